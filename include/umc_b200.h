@@ -1,0 +1,213 @@
+/*
+ * umc_b200.h -- C ABI of the B200 local-update engine.
+ *
+ * This is the boundary the C++23 facade (include/umc/) and any other host
+ * language bind to: plain pointers and sizes, integer status codes, opaque
+ * handles, no C++ or torch types.  It replaces the reference library's
+ * header-only hot path (universal_monte_carlo):
+ *
+ *   tables      PairGraph / square_lattice     lattice/pair_graph.hpp, lattice/square.hpp
+ *               CellComplex / hypercubic_plaquettes  lattice/cell_complex.hpp, lattice/hypercubic.hpp
+ *   models      Ising, VectorSpin<N>, U1Gauge, SUGauge<N>  example/*.hpp
+ *               PairModel / CellModel + terms   model/*.hpp, term/*.hpp
+ *   proposals   Flip, FixedAxis, UniformSphereN, LocalRotation, U1Shift, SUShift  dof/*.hpp
+ *   drivers     Metropolis<M,Q,R>, Wolff<M,A,R>  driver.hpp
+ *   RNG         Pcg32                           rng.hpp
+ *
+ * Errors: every function returns umc_status (0 = OK).  The reference's table
+ * builders throw std::invalid_argument / std::out_of_range / std::overflow_error;
+ * here those become UMC_ERR_INVALID_ARGUMENT / _OUT_OF_RANGE / _OVERFLOW with
+ * the same messages available from umc_last_error() (thread-local).
+ *
+ * Random numbers: every update opens its own reference-semantics Pcg32 keyed by
+ * (seed, counter, tag, id) -- see the package's csrc/umc_rng.cuh -- so a chain
+ * is a pure function of (field, seed, counters) and can be replayed by the
+ * reference driver on the CPU.
+ */
+#ifndef UMC_B200_H
+#define UMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UMC_ABI_VERSION 1
+
+typedef enum umc_status {
+    UMC_OK = 0,
+    UMC_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference builders */
+    UMC_ERR_OUT_OF_RANGE = 2,     /* std::out_of_range                               */
+    UMC_ERR_OVERFLOW = 3,         /* std::overflow_error                             */
+    UMC_ERR_UNSUPPORTED = 4,      /* combination this engine does not provide        */
+    UMC_ERR_CUDA = 5,             /* CUDA runtime error (incl. no device)            */
+    UMC_ERR_DEVICE_TIMEOUT = 6,   /* a bounded device-side wait ran out              */
+    UMC_ERR_OUT_OF_MEMORY = 7,
+    UMC_ERR_STATE = 8             /* call out of order (e.g. records overflowed)     */
+} umc_status;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* umc_last_error(void);
+int umc_abi_version(void);
+/* Number of visible CUDA devices (0 on a host without GPUs). */
+int umc_device_count(int* count);
+
+/* ===================================================================== tables */
+
+typedef struct umc_graph umc_graph;
+
+/* PairGraph(n, edges, symmetric) -- lattice/pair_graph.hpp:49-83.  CSR rows in
+ * edge-list order, duplicates kept, self-loops rejected (INVALID_ARGUMENT),
+ * endpoints >= n rejected (OUT_OF_RANGE), n or 2E beyond uint32 (OVERFLOW). */
+int umc_graph_create(uint64_t n_sites, const uint32_t* edge_i, const uint32_t* edge_j,
+                     uint64_t n_edges, int symmetric, umc_graph** out);
+/* square_lattice(Lx, Ly) -- lattice/square.hpp:15-38. */
+int umc_graph_square(uint64_t Lx, uint64_t Ly, umc_graph** out);
+/* Periodic Lx*Ly*Lz cubic lattice with square_lattice's conventions (site
+ * (z*Ly+y)*Lx+x; per site a +x, +y, +z edge when that extent exceeds 1).  The
+ * reference has no 3D builder; users build the same edge list by hand. */
+int umc_graph_cubic(uint64_t Lx, uint64_t Ly, uint64_t Lz, umc_graph** out);
+void umc_graph_destroy(umc_graph* g);
+/* PairGraph::sites / degree / bonds -- lattice/pair_graph.hpp:86-102. */
+uint64_t umc_graph_sites(const umc_graph* g);
+uint64_t umc_graph_slots(const umc_graph* g);
+int umc_graph_csr(const umc_graph* g, uint32_t* offset /* n+1 */, uint32_t* bonds /* slots */);
+/* Colouring used by the colour passes (no reference counterpart: the reference
+ * sweeps sites in index order, driver.hpp:34).  colour[i] in [0, n_colours);
+ * position[i] = index of site i in colour-major order, which is the order in
+ * which the reference driver reproduces the GPU's updates and the id that keys
+ * site i's random stream.  Any pointer may be NULL. */
+int umc_graph_colouring(const umc_graph* g, uint32_t* n_colours, uint32_t* colour,
+                        uint32_t* position);
+
+typedef struct umc_cells umc_cells;
+
+/* CellComplex<A>(sites, cells) -- lattice/cell_complex.hpp:36-63 (cells is
+ * n_cells*arity site ids, arity in [1, 255]). */
+int umc_cells_create(uint64_t n_sites, uint32_t arity, const uint32_t* cells, uint64_t n_cells,
+                     umc_cells** out);
+/* hypercubic_plaquettes(L) -- lattice/hypercubic.hpp:15-64. */
+int umc_cells_hypercubic(uint64_t L, umc_cells** out);
+/* Periodic 2D plaquettes with the same orientation rule (links mu*L^2+y*L+x,
+ * plaquette [U_0(c), U_1(c+x), U_0(c+y), U_1(c)]); no reference builder. */
+int umc_cells_square_plaquettes(uint64_t L, umc_cells** out);
+void umc_cells_destroy(umc_cells* c);
+/* CellComplex::sites / cells / cell(c) / incident(i) -- lattice/cell_complex.hpp:65-80. */
+uint64_t umc_cells_sites(const umc_cells* c);
+uint64_t umc_cells_count(const umc_cells* c);
+uint32_t umc_cells_arity(const umc_cells* c);
+int umc_cells_table(const umc_cells* c, uint32_t* cells /* n_cells*arity */);
+int umc_cells_incidence(const umc_cells* c, uint64_t* offset /* sites+1 */, uint32_t* inc_cell,
+                        uint8_t* inc_which);
+/* Colouring of the links (no two links of one colour share a cell). */
+int umc_cells_colouring(const umc_cells* c, uint32_t* n_colours, uint32_t* colour,
+                        uint32_t* position);
+
+/* ===================================================================== chains */
+
+/* Models (example/*.hpp, model/*.hpp). */
+#define UMC_MODEL_ISING 1    /* Ising, example/ising.hpp:14-76 (int8 spins, integer J)     */
+#define UMC_MODEL_VECTOR 2   /* VectorSpin<N>, example/vector_spin.hpp:14-83 (N = 1..4)     */
+#define UMC_MODEL_XY_ANGLE 3 /* PairModel<U1Dof, -J cos(ti-tj)>, model/pair.hpp:17-83     */
+#define UMC_MODEL_U1 4       /* U1Gauge / CellModel<U1Dof,U1PlaquetteTerm>, example/u1_gauge.hpp */
+#define UMC_MODEL_SU 5       /* SUGauge<N> / CellModel<SUDof,SUPlaquetteTerm>, example/sun_gauge.hpp */
+
+/* Metropolis proposals (dof/*.hpp). */
+#define UMC_PROPOSAL_FLIP 1     /* Flip, dof/ising.hpp:27-38                 */
+#define UMC_PROPOSAL_SPHERE 2   /* UniformSphereN<N>, dof/vector.hpp:35-61     */
+#define UMC_PROPOSAL_ROTATION 3 /* LocalRotation<N>{delta}, dof/vector.hpp:70-122 */
+#define UMC_PROPOSAL_U1SHIFT 4  /* U1Shift{width}, dof/u1.hpp:35-50          */
+#define UMC_PROPOSAL_SUSHIFT 5  /* SUShift<N>{width}, dof/sun.hpp:163-204     */
+
+/* Wolff reflection axes. */
+#define UMC_AXIS_NONE 0
+#define UMC_AXIS_FIXED 1  /* FixedAxis, dof/ising.hpp:41-49      */
+#define UMC_AXIS_SPHERE 2 /* UniformSphereN<N> as the axis        */
+
+typedef struct umc_chain_desc {
+    int32_t model;          /* UMC_MODEL_*                                        */
+    int32_t components;     /* N of VectorSpin<N> or SU(N); 1 for the others      */
+    const umc_graph* graph; /* spin models                                        */
+    const umc_cells* cells; /* gauge models (arity 4)                              */
+    double coupling;        /* J (Ising: an integer value), or the gauge beta     */
+    int32_t proposal;       /* UMC_PROPOSAL_*                                     */
+    double width;           /* LocalRotation delta, U1Shift / SUShift width       */
+    uint32_t hits;          /* Metropolis hits per site and sweep (>= 1)          */
+    int32_t wolff_axis;     /* UMC_AXIS_*                                         */
+    uint64_t seed;          /* RNG key seed                                       */
+    int32_t device;         /* CUDA device ordinal                                */
+    void* stream;           /* cudaStream_t to run on; NULL: the chain owns one    */
+    uint64_t max_records;   /* per-sweep observable slots on the device (0: 4096) */
+} umc_chain_desc;
+
+typedef struct umc_chain umc_chain;
+
+/* One observable record per sweep (Metropolis) or flip (Wolff), FP64:
+ *   spin models:  [0] E = 0.5 * sum_i energy_at(i)  [1..N] magnetisation sum
+ *                 [7] accepted proposals in the sweep (Wolff: cluster size)
+ *   gauge models: [0] action S = beta * sum_p (1 - P_p)  [1] mean plaquette
+ *                 [2] topological charge (2D U(1))      [7] accepted proposals */
+#define UMC_OBS_STRIDE 8
+
+/* Creates the device chain: the model's field (cold start exactly as the
+ * reference constructors: Ising all +1 example/ising.hpp:24, VectorSpin along
+ * the last axis example/vector_spin.hpp:27-28, gauge links identity
+ * example/sun_gauge.hpp:26 / zero angles), its tables and workspace. */
+int umc_chain_create(const umc_chain_desc* desc, umc_chain** out);
+int umc_chain_destroy(umc_chain* c);
+/* Writes the whole field from host memory in the reference's data() layout:
+ * Ising int8[n]; VectorSpin float[n*N]; XY / U(1) float[n] angles; SU(N)
+ * float[n*N*N*2] (row-major, interleaved re/im).  Equivalent to update(i, .)
+ * for every site. */
+int umc_chain_set_field(umc_chain* c, const void* host_field);
+/* Reads the field back in the same layout (the reference's data()). */
+int umc_chain_get_field(umc_chain* c, void* host_field);
+/* Random start from keyed draws (tag 3, id = site): uniform on the sphere,
+ * uniform angles in [0, 2pi), Haar-random SU(N), random Ising signs. */
+int umc_chain_randomize(umc_chain* c, uint64_t seed);
+/* A driver brings its own proposal and RNG to a model (Metropolis(M&, Q, R,
+ * beta), driver.hpp:22-25; Wolff(M&, A, R, beta), driver.hpp:96-101): these
+ * set the chain's proposal (with its width and hits per site), its Wolff axis
+ * and the seed that keys every random stream. */
+int umc_chain_set_proposal(umc_chain* c, int32_t proposal, double width, uint32_t hits);
+int umc_chain_set_wolff_axis(umc_chain* c, int32_t axis);
+int umc_chain_set_seed(umc_chain* c, uint64_t seed);
+/* Sweep and flip counters (they key the random streams). */
+int umc_chain_counters(const umc_chain* c, uint64_t* sweeps, uint64_t* flips);
+int umc_chain_set_counters(umc_chain* c, uint64_t sweeps, uint64_t flips);
+/* The stream the chain's kernels run on (cudaStream_t). */
+void* umc_chain_stream(const umc_chain* c);
+/* Waits for the chain's queued work and reports any device-side error. */
+int umc_chain_sync(umc_chain* c);
+/* Observables of the current field (one record, see UMC_OBS_STRIDE). */
+int umc_chain_observe(umc_chain* c, double* record);
+
+/* Metropolis::sweep x n -- driver.hpp:29-61.  beta is the driver's beta: the
+ * exponent is -beta * dE (for gauge models put the physical beta in the model
+ * coupling and pass 1.0 here).  records: n x UMC_OBS_STRIDE doubles or NULL.
+ * Blocks until done. */
+int umc_metropolis_run(umc_chain* c, double beta, uint64_t n_sweeps, double* records);
+/* Wolff::flip x n -- driver.hpp:104-190 (single-cluster, reflection axis from
+ * desc.wolff_axis).  sizes: n cluster sizes or NULL; records: n x stride or NULL. */
+int umc_wolff_run(umc_chain* c, double beta, uint64_t n_flips, uint64_t* sizes, double* records);
+/* n x (one Wolff flip, then one Metropolis sweep); one record per step, taken
+ * after the sweep. */
+int umc_hybrid_run(umc_chain* c, double beta, uint64_t n_steps, uint64_t* sizes, double* records);
+/* Asynchronous forms: enqueue on the chain's stream and return.  Records stay
+ * in the device ring (capacity desc.max_records) until umc_chain_fetch. */
+int umc_metropolis_enqueue(umc_chain* c, double beta, uint64_t n_sweeps);
+int umc_wolff_enqueue(umc_chain* c, double beta, uint64_t n_flips);
+int umc_hybrid_enqueue(umc_chain* c, double beta, uint64_t n_steps);
+/* Copies (and releases) the records queued since the last fetch. *n_records
+ * receives their count; records / sizes may be NULL.  Synchronises. */
+int umc_chain_fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t capacity,
+                    uint64_t* n_records);
+/* Wolff::mean_cluster_size bookkeeping -- driver.hpp:193-196. */
+int umc_wolff_stats(const umc_chain* c, uint64_t* flips, double* size_sum);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UMC_B200_H */

@@ -1,0 +1,488 @@
+"""ctypes bindings for the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Two libraries live here:
+
+* ``libumc_oracle.so`` -- the C restatement of the reference algorithms
+  (``umc_oracle.c``); always built by ``make -C oracle oracle``.
+* ``_ref/libumc_ref.so`` -- the reference library's own headers driven through
+  project-written adapters (``ref_harness.cpp``); built where the reference tree
+  is mounted and shipped with the repository snapshot otherwise.
+
+Only tests, the package's smoke check and bench.py's CPU-baseline leg import this
+module.  Every function works on numpy arrays and returns fresh arrays; none of
+them touches a GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libumc_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libumc_ref.so")
+
+TAG_BOND = 1
+TAG_AXIS = 2
+TAG_INIT = 3
+TAG_SWAP = 4
+
+
+def TAG_SITE(h: int = 0) -> int:
+    return 0x100 + h
+
+
+PROP_SPHERE = 0
+PROP_ROTATION = 1
+
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_i8p = np.ctypeslib.ndpointer(np.int8, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+_u32 = C.c_uint32
+_u64 = C.c_uint64
+_i32 = C.c_int32
+_f64 = C.c_double
+_int = C.c_int
+
+
+def build(reference_root: str | None = "/root/reference") -> None:
+    """Builds the oracle (and the reference harness where the tree exists)."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if reference_root and os.path.isfile(os.path.join(reference_root, "driver.hpp")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={reference_root}"], check=True)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+class _Lib:
+    def __init__(self, path: str, prefix: str):
+        self.path = path
+        self.lib = C.CDLL(path)
+        self.prefix = prefix
+
+    def fn(self, name, restype, *argtypes):
+        f = getattr(self.lib, self.prefix + name)
+        f.restype = restype
+        f.argtypes = list(argtypes)
+        return f
+
+
+# --------------------------------------------------------------------- oracle
+class Oracle:
+    """The C restatement (``orc_*``)."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.isfile(path):
+            raise FileNotFoundError(f"oracle library not built: {path} (run make -C oracle oracle)")
+        L = _Lib(path, "orc_")
+        self._L = L
+        self._key_draws = L.fn("key_draws", None, _u64, _u64, _u32, _u32, _u32, _vp)
+        self._pcg_draws = L.fn("pcg32_draws", None, _u64, _u64, _u32, _vp)
+        self._key_seed = L.fn("key_seed", _u64, _u64, _u64, _u32)
+        self._stream_id = L.fn("stream_id", _u32, _u32)
+        self._pair_graph = L.fn("pair_graph", _int, _u64, _vp, _vp, _u64, _int, _vp, _vp, _vp)
+        self._square = L.fn("square_edges", C.c_int64, _u64, _u64, _vp, _vp)
+        self._cubic = L.fn("cubic_edges", C.c_int64, _u64, _u64, _u64, _vp, _vp)
+        self._hyper = L.fn("hypercubic_cells", C.c_int64, _u64, _vp)
+        self._plaq2 = L.fn("square_plaquette_cells", C.c_int64, _u64, _vp)
+        self._incidence = L.fn("cell_incidence", _int, _u64, _u32, _vp, _u64, _vp, _vp, _vp)
+        self._check_col = L.fn("check_colouring", _int, _u64, _vp, _vp, _vp)
+        self._check_cell_col = L.fn("check_cell_colouring", _int, _u64, _u32, _vp, _u64, _vp)
+        self._ising_metro = L.fn("ising_metropolis", None, _u64, _vp, _vp, _i32, _f64, _u64, _u64,
+                                 _u64, _vp, _vp, _vp)
+        self._ising_wolff = L.fn("ising_wolff", None, _u64, _vp, _vp, _vp, _i32, _f64, _u64, _u64,
+                                 _u64, _vp, _vp, _vp, _vp)
+        self._vec_metro = L.fn("vector_metropolis", None, _u32, _u64, _vp, _vp, _f64, _f64, _int,
+                               _f64, _u64, _u64, _u64, _vp, _vp, _vp)
+        self._vec_wolff = L.fn("vector_wolff", None, _u32, _u64, _vp, _vp, _vp, _f64, _f64, _u64,
+                               _u64, _u64, _vp, _vp, _vp, _vp)
+        self._xy_metro = L.fn("xy_metropolis", None, _u64, _vp, _vp, _f64, _f64, _f64, _u64, _u64,
+                              _u64, _vp, _vp, _vp)
+        self._u1_metro = L.fn("u1_metropolis", None, _u64, _vp, _u64, _vp, _vp, _vp, _f64, _f64,
+                              _f64, _u32, _u64, _u64, _u64, _vp, _vp, _vp)
+        self._u1_plaq = L.fn("u1_mean_plaquette", _f64, _u64, _vp, _vp)
+        self._u1_q = L.fn("u1_topological_charge", _f64, _u64, _vp, _vp)
+        self._su_metro = L.fn("su_metropolis", None, _u32, _u64, _vp, _u64, _vp, _vp, _vp, _f64,
+                              _f64, _f64, _u32, _u64, _u64, _u64, _vp, _vp, _vp)
+        self._su_plaq = L.fn("su_mean_plaquette", _f64, _u32, _u64, _vp, _vp)
+        self._su_expm = L.fn("su_expm", None, _u32, _vp, _vp)
+        self._su_unit = L.fn("su_unitarity_error", _f64, _u32, _vp)
+
+    # ---- RNG
+    def key_draws(self, seed, counter, tag, id_, n):
+        out = np.zeros(n, np.uint32)
+        self._key_draws(seed, counter, tag, id_, n, _ptr(out))
+        return out
+
+    def pcg32_draws(self, seed, stream, n):
+        out = np.zeros(n, np.uint32)
+        self._pcg_draws(seed, stream, n, _ptr(out))
+        return out
+
+    def key_seed(self, seed, counter, tag):
+        return int(self._key_seed(seed, counter, tag))
+
+    def stream_id(self, i):
+        return int(self._stream_id(i))
+
+    # ---- tables
+    def pair_graph(self, n, ei, ej, symmetric=True):
+        """CSR of PairGraph(n, edges, symmetric): (status, offset, bonds, slot_edge)."""
+        ei = np.ascontiguousarray(ei, np.uint32)
+        ej = np.ascontiguousarray(ej, np.uint32)
+        offset = np.zeros(n + 1, np.uint32)
+        st = self._pair_graph(n, _ptr(ei), _ptr(ej), len(ei), int(symmetric), _ptr(offset), None, None)
+        if st != 0:
+            return st, None, None, None
+        bonds = np.zeros(int(offset[-1]), np.uint32)
+        slot = np.zeros(int(offset[-1]), np.uint32)
+        self._pair_graph(n, _ptr(ei), _ptr(ej), len(ei), int(symmetric), _ptr(offset), _ptr(bonds), _ptr(slot))
+        return 0, offset, bonds, slot
+
+    def square_edges(self, Lx, Ly):
+        m = self._square(Lx, Ly, None, None)
+        if m < 0:
+            return m, None, None
+        ei = np.zeros(m, np.uint32)
+        ej = np.zeros(m, np.uint32)
+        self._square(Lx, Ly, _ptr(ei), _ptr(ej))
+        return 0, ei, ej
+
+    def cubic_edges(self, Lx, Ly, Lz):
+        m = self._cubic(Lx, Ly, Lz, None, None)
+        if m < 0:
+            return m, None, None
+        ei = np.zeros(m, np.uint32)
+        ej = np.zeros(m, np.uint32)
+        self._cubic(Lx, Ly, Lz, _ptr(ei), _ptr(ej))
+        return 0, ei, ej
+
+    def hypercubic_cells(self, L):
+        m = self._hyper(L, None)
+        cells = np.zeros((m, 4), np.uint32)
+        self._hyper(L, _ptr(cells))
+        return cells
+
+    def square_plaquette_cells(self, L):
+        m = self._plaq2(L, None)
+        cells = np.zeros((m, 4), np.uint32)
+        self._plaq2(L, _ptr(cells))
+        return cells
+
+    def cell_incidence(self, n_sites, cells):
+        cells = np.ascontiguousarray(cells, np.uint32)
+        arity = cells.shape[1]
+        offset = np.zeros(n_sites + 1, np.uint64)
+        st = self._incidence(n_sites, arity, _ptr(cells), cells.shape[0], _ptr(offset), None, None)
+        if st != 0:
+            return st, None, None, None
+        tot = int(offset[-1])
+        inc_cell = np.zeros(tot, np.uint32)
+        inc_which = np.zeros(tot, np.uint8)
+        self._incidence(n_sites, arity, _ptr(cells), cells.shape[0], _ptr(offset), _ptr(inc_cell), _ptr(inc_which))
+        return 0, offset, inc_cell, inc_which
+
+    def check_colouring(self, offset, bonds, colour):
+        colour = np.ascontiguousarray(colour, np.uint32)
+        return bool(self._check_col(len(offset) - 1, _ptr(offset), _ptr(bonds), _ptr(colour)))
+
+    def check_cell_colouring(self, n_sites, cells, colour):
+        cells = np.ascontiguousarray(cells, np.uint32)
+        colour = np.ascontiguousarray(colour, np.uint32)
+        return bool(self._check_cell_col(n_sites, cells.shape[1], _ptr(cells), cells.shape[0], _ptr(colour)))
+
+    # ---- Ising
+    def ising_metropolis(self, offset, bonds, J, beta, seed, sweep0, n_sweeps, spins):
+        s = np.array(spins, np.int8, copy=True)
+        E = np.zeros(n_sweeps)
+        M = np.zeros(n_sweeps)
+        self._ising_metro(len(s), _ptr(offset), _ptr(bonds), J, beta, seed, sweep0, n_sweeps,
+                          _ptr(s), _ptr(E), _ptr(M))
+        return s, E, M
+
+    def ising_wolff(self, offset, bonds, slot_edge, J, beta, seed, flip0, n_flips, spins):
+        s = np.array(spins, np.int8, copy=True)
+        sizes = np.zeros(n_flips, np.uint64)
+        E = np.zeros(n_flips)
+        M = np.zeros(n_flips)
+        self._ising_wolff(len(s), _ptr(offset), _ptr(bonds), _ptr(slot_edge), J, beta, seed, flip0,
+                          n_flips, _ptr(s), _ptr(sizes), _ptr(E), _ptr(M))
+        return s, sizes, E, M
+
+    # ---- VectorSpin
+    def vector_metropolis(self, N, offset, bonds, J, beta, proposal, delta, seed, sweep0, n_sweeps, spins):
+        s = np.array(spins, np.float64, copy=True).reshape(-1)
+        n = s.size // N
+        obs = np.zeros((n_sweeps, N + 1))
+        margin = np.zeros(n)
+        self._vec_metro(N, n, _ptr(offset), _ptr(bonds), J, beta, proposal, delta, seed, sweep0,
+                        n_sweeps, _ptr(s), _ptr(obs), _ptr(margin))
+        return s.reshape(n, N), obs, margin
+
+    def vector_wolff(self, N, offset, bonds, slot_edge, J, beta, seed, flip0, n_flips, spins):
+        s = np.array(spins, np.float64, copy=True).reshape(-1)
+        n = s.size // N
+        sizes = np.zeros(n_flips, np.uint64)
+        obs = np.zeros((n_flips, N + 1))
+        margin = np.zeros(n_flips)
+        self._vec_wolff(N, n, _ptr(offset), _ptr(bonds), _ptr(slot_edge), J, beta, seed, flip0,
+                        n_flips, _ptr(s), _ptr(sizes), _ptr(obs), _ptr(margin))
+        return s.reshape(n, N), sizes, obs, margin
+
+    def xy_metropolis(self, offset, bonds, J, beta, width, seed, sweep0, n_sweeps, theta):
+        t = np.array(theta, np.float64, copy=True)
+        obs = np.zeros((n_sweeps, 3))
+        margin = np.zeros(t.size)
+        self._xy_metro(t.size, _ptr(offset), _ptr(bonds), J, beta, width, seed, sweep0, n_sweeps,
+                       _ptr(t), _ptr(obs), _ptr(margin))
+        return t, obs, margin
+
+    # ---- gauge
+    def u1_metropolis(self, cells, inc, model_beta, driver_beta, width, hits, seed, sweep0,
+                      n_sweeps, theta):
+        cells = np.ascontiguousarray(cells, np.uint32)
+        off, ic, iw = inc
+        t = np.array(theta, np.float64, copy=True)
+        obs = np.zeros((n_sweeps, 2))
+        margin = np.zeros(t.size)
+        self._u1_metro(t.size, _ptr(cells), cells.shape[0], _ptr(off), _ptr(ic), _ptr(iw),
+                       model_beta, driver_beta, width, hits, seed, sweep0, n_sweeps, _ptr(t),
+                       _ptr(obs), _ptr(margin))
+        return t, obs, margin
+
+    def u1_mean_plaquette(self, cells, theta):
+        cells = np.ascontiguousarray(cells, np.uint32)
+        theta = np.ascontiguousarray(theta, np.float64)
+        return self._u1_plaq(cells.shape[0], _ptr(cells), _ptr(theta))
+
+    def u1_topological_charge(self, cells, theta):
+        cells = np.ascontiguousarray(cells, np.uint32)
+        theta = np.ascontiguousarray(theta, np.float64)
+        return self._u1_q(cells.shape[0], _ptr(cells), _ptr(theta))
+
+    def su_metropolis(self, N, cells, inc, model_beta, driver_beta, width, hits, seed, sweep0,
+                      n_sweeps, links):
+        """links: complex array (n_links, N, N)."""
+        cells = np.ascontiguousarray(cells, np.uint32)
+        off, ic, iw = inc
+        l = np.ascontiguousarray(np.array(links, np.complex128, copy=True))
+        n_links = l.shape[0]
+        obs = np.zeros((n_sweeps, 2))
+        margin = np.zeros(n_links)
+        self._su_metro(N, n_links, _ptr(cells), cells.shape[0], _ptr(off), _ptr(ic), _ptr(iw),
+                       model_beta, driver_beta, width, hits, seed, sweep0, n_sweeps, _ptr(l),
+                       _ptr(obs), _ptr(margin))
+        return l, obs, margin
+
+    def su_mean_plaquette(self, N, cells, links):
+        cells = np.ascontiguousarray(cells, np.uint32)
+        l = np.ascontiguousarray(links, np.complex128)
+        return self._su_plaq(N, cells.shape[0], _ptr(cells), _ptr(l))
+
+    def su_expm(self, N, a):
+        a = np.ascontiguousarray(a, np.complex128)
+        out = np.zeros((N, N), np.complex128)
+        self._su_expm(N, _ptr(a), _ptr(out))
+        return out
+
+    def su_unitarity_error(self, N, u):
+        u = np.ascontiguousarray(u, np.complex128)
+        return self._su_unit(N, _ptr(u))
+
+
+# ------------------------------------------------------------------ reference
+class Reference:
+    """The reference headers driven by ref_harness.cpp (``ref_*``)."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.isfile(path):
+            raise FileNotFoundError(f"reference harness not built: {path}")
+        L = _Lib(path, "ref_")
+        self._pcg_draws = L.fn("pcg32_draws", None, _u64, _u64, _u32, _vp)
+        self._key_draws = L.fn("key_draws", None, _u64, _u64, _u32, _u32, _u32, _vp)
+        self._pair_graph = L.fn("pair_graph", _int, _u64, _vp, _vp, _u64, _int, _vp, _vp)
+        self._square = L.fn("square_lattice", _int, _u64, _u64, _vp, _vp)
+        self._hyper = L.fn("hypercubic", _int, _u64, _vp, _vp, _vp, _vp)
+        self._incidence = L.fn("cell_incidence", _int, _u64, _vp, _u64, _vp, _vp, _vp)
+        self._ising_metro = L.fn("ising_metropolis", _int, _u64, _vp, _vp, _u64, _i32, _f64, _u64,
+                                 _u64, _u64, _vp, _vp, _vp)
+        self._ising_wolff = L.fn("ising_wolff", _int, _u64, _vp, _vp, _u64, _i32, _f64, _u64, _u64,
+                                 _u64, _vp, _vp, _vp, _vp)
+        self._vec_metro = L.fn("vector_metropolis", _int, _u32, _u64, _vp, _vp, _u64, _f64, _f64,
+                               _int, _f64, _u64, _u64, _u64, _vp, _vp)
+        self._vec_wolff = L.fn("vector_wolff", _int, _u32, _u64, _vp, _vp, _u64, _f64, _f64, _u64,
+                               _u64, _u64, _vp, _vp, _vp)
+        self._sphere = L.fn("sphere_sample", None, _u32, _u64, _u64, _u32, _u32, _vp)
+        self._xy_metro = L.fn("xy_metropolis", _int, _u64, _vp, _vp, _u64, _f64, _f64, _f64, _u64,
+                              _u64, _u64, _vp, _vp)
+        self._u1_metro = L.fn("u1_metropolis", _int, _u64, _vp, _u64, _f64, _f64, _f64, _u32,
+                              _u64, _u64, _u64, _vp, _vp)
+        self._su_metro = L.fn("su_metropolis", _int, _u32, _u64, _vp, _u64, _f64, _f64, _f64, _u32,
+                              _u64, _u64, _u64, _vp, _vp)
+        self._su_expm = L.fn("su_expm", None, _u32, _vp, _vp)
+        self._su_shift = L.fn("su_shift", None, _u32, _f64, _u64, _u64, _u32, _u32, _vp, _vp)
+        self._bench_o3 = L.fn("bench_o3", _int, _u64, _f64, _u64, _u32, _u64, _vp, _vp)
+        self._bench_ising = L.fn("bench_ising", _int, _u64, _f64, _u64, _u32, _u64, _vp, _vp)
+
+    def pcg32_draws(self, seed, stream, n):
+        out = np.zeros(n, np.uint32)
+        self._pcg_draws(seed, stream, n, _ptr(out))
+        return out
+
+    def key_draws(self, seed, counter, tag, id_, n):
+        out = np.zeros(n, np.uint32)
+        self._key_draws(seed, counter, tag, id_, n, _ptr(out))
+        return out
+
+    def pair_graph(self, n, ei, ej, symmetric=True):
+        ei = np.ascontiguousarray(ei, np.uint32)
+        ej = np.ascontiguousarray(ej, np.uint32)
+        offset = np.zeros(n + 1, np.uint32)
+        st = self._pair_graph(n, _ptr(ei), _ptr(ej), len(ei), int(symmetric), _ptr(offset), None)
+        if st != 0:
+            return st, None, None
+        bonds = np.zeros(int(offset[-1]), np.uint32)
+        self._pair_graph(n, _ptr(ei), _ptr(ej), len(ei), int(symmetric), _ptr(offset), _ptr(bonds))
+        return 0, offset, bonds
+
+    def square_lattice(self, Lx, Ly):
+        n = Lx * Ly
+        offset = np.zeros(n + 1, np.uint32)
+        st = self._square(Lx, Ly, _ptr(offset), None)
+        if st != 0:
+            return st, None, None
+        bonds = np.zeros(int(offset[-1]), np.uint32)
+        self._square(Lx, Ly, _ptr(offset), _ptr(bonds))
+        return 0, offset, bonds
+
+    def hypercubic(self, L):
+        L4 = L ** 4
+        cells = np.zeros((6 * L4, 4), np.uint32)
+        offset = np.zeros(4 * L4 + 1, np.uint64)
+        inc_cell = np.zeros(24 * L4, np.uint32)
+        inc_which = np.zeros(24 * L4, np.uint8)
+        st = self._hyper(L, _ptr(cells), _ptr(offset), _ptr(inc_cell), _ptr(inc_which))
+        return st, cells, offset, inc_cell, inc_which
+
+    def cell_incidence(self, n_sites, cells):
+        cells = np.ascontiguousarray(cells, np.uint32)
+        offset = np.zeros(n_sites + 1, np.uint64)
+        tot = cells.size
+        inc_cell = np.zeros(tot, np.uint32)
+        inc_which = np.zeros(tot, np.uint8)
+        st = self._incidence(n_sites, _ptr(cells), cells.shape[0], _ptr(offset), _ptr(inc_cell), _ptr(inc_which))
+        return st, offset, inc_cell, inc_which
+
+    def ising_metropolis(self, n, ei, ej, J, beta, seed, sweep0, n_sweeps, spins):
+        ei = np.ascontiguousarray(ei, np.uint32)
+        ej = np.ascontiguousarray(ej, np.uint32)
+        s = np.array(spins, np.int8, copy=True)
+        E = np.zeros(n_sweeps)
+        M = np.zeros(n_sweeps)
+        st = self._ising_metro(n, _ptr(ei), _ptr(ej), len(ei), J, beta, seed, sweep0, n_sweeps,
+                               _ptr(s), _ptr(E), _ptr(M))
+        assert st == 0, st
+        return s, E, M
+
+    def ising_wolff(self, n, ei, ej, J, beta, seed, flip0, n_flips, spins):
+        ei = np.ascontiguousarray(ei, np.uint32)
+        ej = np.ascontiguousarray(ej, np.uint32)
+        s = np.array(spins, np.int8, copy=True)
+        sizes = np.zeros(n_flips, np.uint64)
+        E = np.zeros(n_flips)
+        M = np.zeros(n_flips)
+        st = self._ising_wolff(n, _ptr(ei), _ptr(ej), len(ei), J, beta, seed, flip0, n_flips,
+                               _ptr(s), _ptr(sizes), _ptr(E), _ptr(M))
+        assert st == 0, st
+        return s, sizes, E, M
+
+    def vector_metropolis(self, N, n, ei, ej, J, beta, proposal, delta, seed, sweep0, n_sweeps, spins):
+        ei = np.ascontiguousarray(ei, np.uint32)
+        ej = np.ascontiguousarray(ej, np.uint32)
+        s = np.array(spins, np.float64, copy=True).reshape(-1)
+        obs = np.zeros((n_sweeps, N + 1))
+        st = self._vec_metro(N, n, _ptr(ei), _ptr(ej), len(ei), J, beta, proposal, delta, seed,
+                             sweep0, n_sweeps, _ptr(s), _ptr(obs))
+        assert st == 0, st
+        return s.reshape(n, N), obs
+
+    def vector_wolff(self, N, n, ei, ej, J, beta, seed, flip0, n_flips, spins):
+        ei = np.ascontiguousarray(ei, np.uint32)
+        ej = np.ascontiguousarray(ej, np.uint32)
+        s = np.array(spins, np.float64, copy=True).reshape(-1)
+        sizes = np.zeros(n_flips, np.uint64)
+        obs = np.zeros((n_flips, N + 1))
+        st = self._vec_wolff(N, n, _ptr(ei), _ptr(ej), len(ei), J, beta, seed, flip0, n_flips,
+                             _ptr(s), _ptr(sizes), _ptr(obs))
+        assert st == 0, st
+        return s.reshape(n, N), sizes, obs
+
+    def sphere_sample(self, N, seed, counter, tag, id_):
+        out = np.zeros(N)
+        self._sphere(N, seed, counter, tag, id_, _ptr(out))
+        return out
+
+    def xy_metropolis(self, n, ei, ej, J, beta, width, seed, sweep0, n_sweeps, theta):
+        ei = np.ascontiguousarray(ei, np.uint32)
+        ej = np.ascontiguousarray(ej, np.uint32)
+        t = np.array(theta, np.float64, copy=True)
+        obs = np.zeros((n_sweeps, 3))
+        st = self._xy_metro(n, _ptr(ei), _ptr(ej), len(ei), J, beta, width, seed, sweep0, n_sweeps,
+                            _ptr(t), _ptr(obs))
+        assert st == 0, st
+        return t, obs
+
+    def u1_metropolis(self, cells, model_beta, driver_beta, width, hits, seed, sweep0, n_sweeps, theta):
+        cells = np.ascontiguousarray(cells, np.uint32)
+        t = np.array(theta, np.float64, copy=True)
+        obs = np.zeros((n_sweeps, 2))
+        st = self._u1_metro(t.size, _ptr(cells), cells.shape[0], model_beta, driver_beta, width,
+                            hits, seed, sweep0, n_sweeps, _ptr(t), _ptr(obs))
+        assert st == 0, st
+        return t, obs
+
+    def su_metropolis(self, N, cells, model_beta, driver_beta, width, hits, seed, sweep0, n_sweeps, links):
+        cells = np.ascontiguousarray(cells, np.uint32)
+        l = np.ascontiguousarray(np.array(links, np.complex128, copy=True))
+        obs = np.zeros((n_sweeps, 2))
+        st = self._su_metro(N, l.shape[0], _ptr(cells), cells.shape[0], model_beta, driver_beta,
+                            width, hits, seed, sweep0, n_sweeps, _ptr(l), _ptr(obs))
+        assert st == 0, st
+        return l, obs
+
+    def su_expm(self, N, a):
+        a = np.ascontiguousarray(a, np.complex128)
+        out = np.zeros((N, N), np.complex128)
+        self._su_expm(N, _ptr(a), _ptr(out))
+        return out
+
+    def su_shift(self, N, width, seed, counter, tag, id_, cur):
+        cur = np.ascontiguousarray(cur, np.complex128)
+        out = np.zeros((N, N), np.complex128)
+        self._su_shift(N, width, seed, counter, tag, id_, _ptr(cur), _ptr(out))
+        return out
+
+    def bench_o3(self, L, beta, steps, threads, seed=1):
+        su = C.c_double()
+        sec = C.c_double()
+        st = self._bench_o3(L, beta, steps, threads, seed, C.byref(su), C.byref(sec))
+        assert st == 0, st
+        return su.value, sec.value
+
+    def bench_ising(self, L, beta, sweeps, threads, seed=1):
+        su = C.c_double()
+        sec = C.c_double()
+        st = self._bench_ising(L, beta, sweeps, threads, seed, C.byref(su), C.byref(sec))
+        assert st == 0, st
+        return su.value, sec.value
+
+
+def have_reference() -> bool:
+    return os.path.isfile(REF_SO)

@@ -1,0 +1,849 @@
+// ref_harness.cpp -- drives the UNMODIFIED reference library (TEST INFRASTRUCTURE).
+//
+// Compiled against the reference headers where they lie (oracle/Makefile passes
+// -I<reference root>); nothing from the reference is copied here.  The adapters
+// below are ordinary user types that satisfy the reference's own concepts
+// (Proposal dof/proposal.hpp:8-12, ModelLike model.hpp:70-86, WolffModel
+// driver.hpp:73-84).  They only choose WHICH random stream the reference
+// driver reads from:
+//
+//   KeyState / KeyedRng  one reference Pcg32 (rng.hpp:8-44), re-seeded per key
+//                        Pcg32(key_seed(seed, counter, tag), stream_id(id));
+//   Keyed<Q>             a proposal adapter that re-keys on the site index it is
+//                        handed (cur - data(), driver.hpp:35-36) before calling
+//                        the reference proposal;
+//   KeyedWolff<M>        a model adapter that re-keys on the edge id inside
+//                        energy_diff_bond, which the Wolff driver calls right
+//                        before the activation draw (driver.hpp:150-151);
+//   KeyedAxis<A>         re-keys the axis/seed draws of one flip (driver.hpp:110,114);
+//   MultiHit<M>          exposes K pseudo-sites per link so that the reference
+//                        driver performs K Metropolis hits on each link in turn.
+//
+// The exported extern "C" functions mirror oracle/umc_oracle.h with a ref_
+// prefix, plus ref_bench_* entry points that time the reference's own stock
+// path (plain Pcg32, no adapters) for the CPU baseline.
+
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <stdexcept>
+#include <thread>
+#include <vector>
+
+#include <driver.hpp>
+#include <dof/ising.hpp>
+#include <dof/sun.hpp>
+#include <dof/u1.hpp>
+#include <dof/vector.hpp>
+#include <example/ising.hpp>
+#include <example/sun_gauge.hpp>
+#include <example/u1_gauge.hpp>
+#include <example/vector_spin.hpp>
+#include <lattice/cell_complex.hpp>
+#include <lattice/hypercubic.hpp>
+#include <lattice/pair_graph.hpp>
+#include <lattice/square.hpp>
+#include <model/cell.hpp>
+#include <model/pair.hpp>
+#include <rng.hpp>
+#include <term/plaquette.hpp>
+#include <term/sun_plaquette.hpp>
+
+namespace {
+
+constexpr std::uint32_t TAG_BOND = 1;
+constexpr std::uint32_t TAG_AXIS = 2;
+constexpr std::uint32_t tag_site(std::uint32_t h) { return 0x100u + h; }
+
+std::uint64_t mix64(std::uint64_t z)
+{
+    z ^= z >> 30;
+    z *= 0xBF58476D1CE4E5B9ULL;
+    z ^= z >> 27;
+    z *= 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    return z;
+}
+std::uint64_t key_seed(std::uint64_t seed, std::uint64_t counter, std::uint32_t tag)
+{
+    return mix64(mix64(seed ^ (std::uint64_t(tag) << 32)) + counter * 0x9E3779B97F4A7C15ULL);
+}
+std::uint32_t stream_id(std::uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x;
+}
+
+struct KeyState
+{
+    std::uint64_t seed = 0;
+    std::uint64_t counter = 0;
+    Pcg32 gen{0, 0};
+    void open(std::uint32_t tag, std::uint64_t id)
+    {
+        gen = Pcg32(key_seed(seed, counter, tag), stream_id(static_cast<std::uint32_t>(id)));
+    }
+};
+
+struct KeyedRng
+{
+    KeyState* ks;
+    double uni() { return ks->gen.uni(); }
+};
+
+template <class Q, class T>
+struct Keyed
+{
+    Q inner;
+    KeyState* ks;
+    const T* base;
+    std::size_t size;
+    std::uint32_t tag;
+
+    template <class R>
+    void sample(const T* cur, R& rng, T* out) const
+    {
+        ks->open(tag, static_cast<std::size_t>(cur - base) / size);
+        inner.sample(cur, rng, out);
+    }
+    double log_ratio(const T* a, const T* b) const { return inner.log_ratio(a, b); }
+};
+
+template <class A>
+struct KeyedAxis
+{
+    A inner;
+    KeyState* ks;
+    template <class C, class R, class T>
+    void sample(C cur, R& rng, T* out) const
+    {
+        ks->open(TAG_AXIS, 0);
+        inner.sample(cur, rng, out);
+    }
+};
+
+template <class M>
+struct KeyedWolff
+{
+    using value_type = typename M::value_type;
+    using bond_type = typename M::bond_type;
+    static constexpr std::size_t size = M::size;
+
+    M* m;
+    KeyState* ks;
+    const std::uint32_t* slot_edge;
+
+    std::size_t sites() const { return m->sites(); }
+    const value_type* data() const { return m->data(); }
+    double energy_diff_at(std::size_t i, const value_type* p) const { return m->energy_diff_at(i, p); }
+    void update(std::size_t i, const value_type* p) { m->update(i, p); }
+    std::size_t degree(std::size_t i) const { return m->degree(i); }
+    const bond_type* bonds(std::size_t i) const { return m->bonds(i); }
+    double energy_diff_bond(std::size_t i, const bond_type& b, const value_type* p) const
+    {
+        ks->open(TAG_BOND, slot_edge[static_cast<std::size_t>(&b - m->bonds(0))]);
+        return m->energy_diff_bond(i, b, p);
+    }
+};
+
+// K pseudo-sites per link; data() points at a K-times larger dummy buffer so that
+// the driver's pointer arithmetic stays inside an allocation.
+template <class M>
+struct MultiHit
+{
+    using value_type = typename M::value_type;
+    static constexpr std::size_t size = M::size;
+
+    M* m;
+    std::size_t K;
+    std::vector<value_type> dummy;
+
+    std::size_t sites() const { return m->sites() * K; }
+    const value_type* data() const { return dummy.data(); }
+    double energy_diff_at(std::size_t i, const value_type* p) const { return m->energy_diff_at(i / K, p); }
+    void update(std::size_t i, const value_type* p) { m->update(i / K, p); }
+};
+
+// Proposal adapter for MultiHit: keys on (link, hit) and proposes from the
+// inner model's current link rather than the dummy pointer.
+template <class Q, class M>
+struct KeyedHit
+{
+    Q inner;
+    KeyState* ks;
+    const MultiHit<M>* mh;
+
+    template <class R, class T>
+    void sample(const T* cur, R& rng, T* out) const
+    {
+        const std::size_t i = static_cast<std::size_t>(cur - mh->dummy.data()) / M::size;
+        const std::size_t link = i / mh->K, hit = i % mh->K;
+        ks->open(tag_site(static_cast<std::uint32_t>(hit)), link);
+        inner.sample(mh->m->data() + link * M::size, rng, out);
+    }
+    template <class T>
+    double log_ratio(const T* a, const T* b) const { return inner.log_ratio(a, b); }
+};
+
+// Pair term E = -J cos(theta_i - theta_j) for the XY model on angles; a user
+// CellTerm of arity 2 (term/cell.hpp:10-25) for PairModel (model/pair.hpp).
+struct XYAngleTerm
+{
+    using dtype = U1Link;
+    using energy_type = double;
+    static constexpr std::size_t arity = 2;
+    double J = 1.0;
+
+    energy_type energy(const dtype* const* links) const
+    {
+        return -J * std::cos(links[0]->theta - links[1]->theta);
+    }
+    energy_type delta(std::size_t which, const dtype* old, const dtype* nw,
+                      const dtype* const* links) const
+    {
+        const dtype* fixed = links[which == 0 ? 1 : 0];
+        return -J * (std::cos(nw->theta - fixed->theta) - std::cos(old->theta - fixed->theta));
+    }
+};
+static_assert(CellTerm<XYAngleTerm, U1Dof>);
+
+int status_of(const std::exception_ptr& e)
+{
+    try {
+        std::rethrow_exception(e);
+    } catch (const std::out_of_range&) {
+        return -1;
+    } catch (const std::invalid_argument&) {
+        return -2;
+    } catch (const std::overflow_error&) {
+        return -3;
+    } catch (...) {
+        return -4;
+    }
+}
+
+std::vector<PairGraph<>::Edge> make_edges(const std::uint32_t* ei, const std::uint32_t* ej,
+                                          std::uint64_t m)
+{
+    std::vector<PairGraph<>::Edge> edges(m);
+    for (std::uint64_t e = 0; e < m; ++e) edges[e] = {ei[e], ej[e], {}};
+    return edges;
+}
+
+// Slot -> edge-list index, replaying PairGraph's scatter order
+// (lattice/pair_graph.hpp:77-81).
+std::vector<std::uint32_t> slot_edges(const PairGraph<>& g, const std::uint32_t* ei,
+                                      const std::uint32_t* ej, std::uint64_t m, bool symmetric)
+{
+    const std::size_t n = g.sites();
+    std::vector<std::uint32_t> slot;
+    if (n == 0) return slot;
+    const auto* base = g.bonds(0);
+    std::vector<std::size_t> pos(n);
+    std::size_t total = 0;
+    for (std::size_t i = 0; i < n; ++i) {
+        pos[i] = base ? static_cast<std::size_t>(g.bonds(i) - base) : 0;
+        total += g.degree(i);
+    }
+    slot.assign(total, 0);
+    for (std::uint64_t e = 0; e < m; ++e) {
+        slot[pos[ei[e]]++] = static_cast<std::uint32_t>(e);
+        if (symmetric) slot[pos[ej[e]]++] = static_cast<std::uint32_t>(e);
+    }
+    return slot;
+}
+
+template <class M>
+double half_energy_sum(const M& m)
+{
+    double sum = 0.0;
+    for (std::size_t i = 0; i < m.sites(); ++i) sum += m.energy_at(i);
+    return 0.5 * sum;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------- RNG
+extern "C" void ref_pcg32_draws(std::uint64_t seed, std::uint64_t stream, std::uint32_t n, std::uint32_t* out)
+{
+    Pcg32 g(seed, stream);
+    for (std::uint32_t k = 0; k < n; ++k) out[k] = static_cast<std::uint32_t>(g.uni() * 0x1.0p32);
+}
+
+extern "C" void ref_key_draws(std::uint64_t seed, std::uint64_t counter, std::uint32_t tag, std::uint32_t id,
+                   std::uint32_t n, std::uint32_t* out)
+{
+    KeyState ks;
+    ks.seed = seed;
+    ks.counter = counter;
+    ks.open(tag, id);
+    for (std::uint32_t k = 0; k < n; ++k) out[k] = static_cast<std::uint32_t>(ks.gen.uni() * 0x1.0p32);
+}
+
+// ---------------------------------------------------------------------- tables
+extern "C" int ref_pair_graph(std::uint64_t n, const std::uint32_t* ei, const std::uint32_t* ej,
+                   std::uint64_t m, int symmetric, std::uint32_t* offset, std::uint32_t* bonds)
+{
+    try {
+        const auto edges = make_edges(ei, ej, m);
+        PairGraph<> g(n, edges, symmetric != 0);
+        std::uint32_t acc = 0;
+        for (std::size_t i = 0; i < g.sites(); ++i) {
+            offset[i] = acc;
+            for (std::size_t a = 0; a < g.degree(i); ++a) {
+                if (bonds) bonds[acc] = g.bonds(i)[a].j;
+                ++acc;
+            }
+        }
+        offset[g.sites()] = acc;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+extern "C" int ref_square_lattice(std::uint64_t Lx, std::uint64_t Ly, std::uint32_t* offset, std::uint32_t* bonds)
+{
+    try {
+        const auto g = square_lattice(Lx, Ly);
+        std::uint32_t acc = 0;
+        for (std::size_t i = 0; i < g.sites(); ++i) {
+            offset[i] = acc;
+            for (std::size_t a = 0; a < g.degree(i); ++a) {
+                if (bonds) bonds[acc] = g.bonds(i)[a].j;
+                ++acc;
+            }
+        }
+        offset[g.sites()] = acc;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+// Dumps hypercubic_plaquettes(L): cells (6L^4 x 4) and the incidence rows.
+extern "C" int ref_hypercubic(std::uint64_t L, std::uint32_t* cells, std::uint64_t* offset,
+                   std::uint32_t* inc_cell, std::uint8_t* inc_which)
+{
+    try {
+        const auto cc = hypercubic_plaquettes(L);
+        for (std::size_t c = 0; c < cc.cells(); ++c)
+            for (std::size_t k = 0; k < 4; ++k) cells[4 * c + k] = cc.cell(c)[k];
+        std::uint64_t acc = 0;
+        for (std::size_t i = 0; i < cc.sites(); ++i) {
+            offset[i] = acc;
+            for (const auto inc : cc.incident(i)) {
+                inc_cell[acc] = inc.cell;
+                inc_which[acc] = inc.which;
+                ++acc;
+            }
+        }
+        offset[cc.sites()] = acc;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+extern "C" int ref_cell_incidence(std::uint64_t n_sites, const std::uint32_t* cells, std::uint64_t n_cells,
+                       std::uint64_t* offset, std::uint32_t* inc_cell, std::uint8_t* inc_which)
+{
+    try {
+        std::vector<Cell<4>> cl(n_cells);
+        for (std::uint64_t c = 0; c < n_cells; ++c)
+            for (int k = 0; k < 4; ++k) cl[c].sites[k] = cells[4 * c + k];
+        CellComplex<4> cc(n_sites, cl);
+        std::uint64_t acc = 0;
+        for (std::size_t i = 0; i < cc.sites(); ++i) {
+            offset[i] = acc;
+            for (const auto inc : cc.incident(i)) {
+                inc_cell[acc] = inc.cell;
+                inc_which[acc] = inc.which;
+                ++acc;
+            }
+        }
+        offset[cc.sites()] = acc;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+// ----------------------------------------------------------------------- Ising
+extern "C" int ref_ising_metropolis(std::uint64_t n, const std::uint32_t* ei, const std::uint32_t* ej,
+                         std::uint64_t m, std::int32_t J, double beta, std::uint64_t seed,
+                         std::uint64_t sweep0, std::uint64_t n_sweeps, std::int8_t* spins,
+                         double* E_out, double* M_out)
+{
+    try {
+        const auto edges = make_edges(ei, ej, m);
+        Ising model(PairGraph<>(n, edges), J);
+        for (std::size_t i = 0; i < n; ++i) model.update(i, spins + i);
+        KeyState ks;
+        ks.seed = seed;
+        ks.counter = sweep0;
+        Keyed<Flip, IsingSpin> prop{Flip{}, &ks, model.data(), 1, tag_site(0)};
+        Metropolis<Ising, Keyed<Flip, IsingSpin>, KeyedRng> mc(model, prop, KeyedRng{&ks}, beta);
+        std::uint64_t k = 0;
+        mc.sample(n_sweeps, [&](const Ising& mdl) {
+            if (E_out) E_out[k] = half_energy_sum(mdl);
+            if (M_out) {
+                double s = 0.0;
+                for (std::size_t i = 0; i < mdl.sites(); ++i) s += mdl.data()[i];
+                M_out[k] = s;
+            }
+            ++k;
+            ++ks.counter;
+        });
+        std::memcpy(spins, model.data(), n);
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+extern "C" int ref_ising_wolff(std::uint64_t n, const std::uint32_t* ei, const std::uint32_t* ej,
+                    std::uint64_t m, std::int32_t J, double beta, std::uint64_t seed,
+                    std::uint64_t flip0, std::uint64_t n_flips, std::int8_t* spins,
+                    std::uint64_t* sizes, double* E_out, double* M_out)
+{
+    try {
+        const auto edges = make_edges(ei, ej, m);
+        Ising model(PairGraph<>(n, edges), J);
+        for (std::size_t i = 0; i < n; ++i) model.update(i, spins + i);
+        // The model's graph is a copy of this one; slot order is identical.
+        const auto slots = slot_edges(PairGraph<>(n, edges), ei, ej, m, true);
+        KeyState ks;
+        ks.seed = seed;
+        ks.counter = flip0;
+        KeyedWolff<Ising> km{&model, &ks, slots.data()};
+        Wolff<KeyedWolff<Ising>, KeyedAxis<FixedAxis>, KeyedRng> w(
+            km, KeyedAxis<FixedAxis>{FixedAxis{}, &ks}, KeyedRng{&ks}, beta);
+        for (std::uint64_t f = 0; f < n_flips; ++f) {
+            const std::size_t c = w.flip();
+            if (sizes) sizes[f] = c;
+            if (E_out) E_out[f] = half_energy_sum(model);
+            if (M_out) {
+                double s = 0.0;
+                for (std::size_t i = 0; i < n; ++i) s += model.data()[i];
+                M_out[f] = s;
+            }
+            ++ks.counter;
+        }
+        std::memcpy(spins, model.data(), n);
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+// ------------------------------------------------------------------ VectorSpin
+namespace {
+template <std::size_t N>
+void vector_obs(const VectorSpin<N>& m, double* obs)
+{
+    obs[0] = half_energy_sum(m);
+    for (std::size_t k = 0; k < N; ++k) {
+        double s = 0.0;
+        for (std::size_t i = 0; i < m.sites(); ++i) s += m.data()[i * N + k];
+        obs[1 + k] = s;
+    }
+}
+
+template <std::size_t N, class Q>
+void vector_metro_run(VectorSpin<N>& model, Q q, KeyState& ks, double beta, std::uint64_t n_sweeps,
+                      double* obs_out)
+{
+    using KQ = Keyed<Q, double>;
+    KQ prop{q, &ks, model.data(), N, tag_site(0)};
+    Metropolis<VectorSpin<N>, KQ, KeyedRng> mc(model, prop, KeyedRng{&ks}, beta);
+    std::uint64_t k = 0;
+    mc.sample(n_sweeps, [&](const VectorSpin<N>& mdl) {
+        if (obs_out) vector_obs<N>(mdl, obs_out + k * (N + 1));
+        ++k;
+        ++ks.counter;
+    });
+}
+
+template <std::size_t N>
+int vector_metropolis(std::uint64_t n, const std::uint32_t* ei, const std::uint32_t* ej,
+                      std::uint64_t m, double J, double beta, int proposal, double delta,
+                      std::uint64_t seed, std::uint64_t sweep0, std::uint64_t n_sweeps,
+                      double* spins, double* obs_out)
+{
+    const auto edges = make_edges(ei, ej, m);
+    VectorSpin<N> model(PairGraph<>(n, edges), J);
+    for (std::size_t i = 0; i < n; ++i) model.update(i, spins + i * N);
+    KeyState ks;
+    ks.seed = seed;
+    ks.counter = sweep0;
+    if (proposal == 0) {
+        vector_metro_run<N>(model, UniformSphereN<N>{}, ks, beta, n_sweeps, obs_out);
+    } else {
+        if constexpr (N >= 2) vector_metro_run<N>(model, LocalRotation<N>{delta}, ks, beta, n_sweeps, obs_out);
+        else throw std::invalid_argument("LocalRotation needs N >= 2");
+    }
+    std::memcpy(spins, model.data(), n * N * sizeof(double));
+    return 0;
+}
+
+template <std::size_t N>
+int vector_wolff(std::uint64_t n, const std::uint32_t* ei, const std::uint32_t* ej,
+                 std::uint64_t m, double J, double beta, std::uint64_t seed, std::uint64_t flip0,
+                 std::uint64_t n_flips, double* spins, std::uint64_t* sizes, double* obs_out)
+{
+    const auto edges = make_edges(ei, ej, m);
+    VectorSpin<N> model(PairGraph<>(n, edges), J);
+    for (std::size_t i = 0; i < n; ++i) model.update(i, spins + i * N);
+    const auto slots = slot_edges(PairGraph<>(n, edges), ei, ej, m, true);
+    KeyState ks;
+    ks.seed = seed;
+    ks.counter = flip0;
+    KeyedWolff<VectorSpin<N>> km{&model, &ks, slots.data()};
+    using Ax = KeyedAxis<UniformSphereN<N>>;
+    Wolff<KeyedWolff<VectorSpin<N>>, Ax, KeyedRng> w(km, Ax{UniformSphereN<N>{}, &ks}, KeyedRng{&ks}, beta);
+    for (std::uint64_t f = 0; f < n_flips; ++f) {
+        const std::size_t c = w.flip();
+        if (sizes) sizes[f] = c;
+        if (obs_out) vector_obs<N>(model, obs_out + f * (N + 1));
+        ++ks.counter;
+    }
+    std::memcpy(spins, model.data(), n * N * sizeof(double));
+    return 0;
+}
+}  // namespace
+
+extern "C" int ref_vector_metropolis(std::uint32_t N, std::uint64_t n, const std::uint32_t* ei,
+                          const std::uint32_t* ej, std::uint64_t m, double J, double beta,
+                          int proposal, double delta, std::uint64_t seed, std::uint64_t sweep0,
+                          std::uint64_t n_sweeps, double* spins, double* obs_out)
+{
+    try {
+        switch (N) {
+        case 1: return vector_metropolis<1>(n, ei, ej, m, J, beta, proposal, delta, seed, sweep0, n_sweeps, spins, obs_out);
+        case 2: return vector_metropolis<2>(n, ei, ej, m, J, beta, proposal, delta, seed, sweep0, n_sweeps, spins, obs_out);
+        case 3: return vector_metropolis<3>(n, ei, ej, m, J, beta, proposal, delta, seed, sweep0, n_sweeps, spins, obs_out);
+        case 4: return vector_metropolis<4>(n, ei, ej, m, J, beta, proposal, delta, seed, sweep0, n_sweeps, spins, obs_out);
+        default: return -2;
+        }
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+extern "C" int ref_vector_wolff(std::uint32_t N, std::uint64_t n, const std::uint32_t* ei,
+                     const std::uint32_t* ej, std::uint64_t m, double J, double beta,
+                     std::uint64_t seed, std::uint64_t flip0, std::uint64_t n_flips, double* spins,
+                     std::uint64_t* sizes, double* obs_out)
+{
+    try {
+        switch (N) {
+        case 1: return vector_wolff<1>(n, ei, ej, m, J, beta, seed, flip0, n_flips, spins, sizes, obs_out);
+        case 2: return vector_wolff<2>(n, ei, ej, m, J, beta, seed, flip0, n_flips, spins, sizes, obs_out);
+        case 3: return vector_wolff<3>(n, ei, ej, m, J, beta, seed, flip0, n_flips, spins, sizes, obs_out);
+        case 4: return vector_wolff<4>(n, ei, ej, m, J, beta, seed, flip0, n_flips, spins, sizes, obs_out);
+        default: return -2;
+        }
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+extern "C" void ref_sphere_sample(std::uint32_t N, std::uint64_t seed, std::uint64_t counter, std::uint32_t tag,
+                       std::uint32_t id, double* out)
+{
+    KeyState ks;
+    ks.seed = seed;
+    ks.counter = counter;
+    ks.open(tag, id);
+    KeyedRng r{&ks};
+    switch (N) {
+    case 1: UniformSphereN<1>{}.sample(nullptr, r, out); break;
+    case 2: UniformSphereN<2>{}.sample(nullptr, r, out); break;
+    case 3: UniformSphereN<3>{}.sample(nullptr, r, out); break;
+    case 4: UniformSphereN<4>{}.sample(nullptr, r, out); break;
+    default: break;
+    }
+}
+
+// --------------------------------------------------------------------- XY angle
+extern "C" int ref_xy_metropolis(std::uint64_t n, const std::uint32_t* ei, const std::uint32_t* ej,
+                      std::uint64_t m, double J, double beta, double width, std::uint64_t seed,
+                      std::uint64_t sweep0, std::uint64_t n_sweeps, double* theta, double* obs_out)
+{
+    try {
+        using PM = PairModel<U1Dof, XYAngleTerm, PairGraph<>>;
+        const auto edges = make_edges(ei, ej, m);
+        PM model(PairGraph<>(n, edges), XYAngleTerm{J});
+        for (std::size_t i = 0; i < n; ++i) {
+            const U1Link l{theta[i]};
+            model.update(i, &l);
+        }
+        KeyState ks;
+        ks.seed = seed;
+        ks.counter = sweep0;
+        using KQ = Keyed<U1Shift, U1Link>;
+        KQ prop{U1Shift{width}, &ks, model.data(), 1, tag_site(0)};
+        Metropolis<PM, KQ, KeyedRng> mc(model, prop, KeyedRng{&ks}, beta);
+        std::uint64_t k = 0;
+        mc.sample(n_sweeps, [&](const PM& mdl) {
+            if (obs_out) {
+                obs_out[3 * k] = half_energy_sum(mdl);
+                double mx = 0.0, my = 0.0;
+                for (std::size_t i = 0; i < mdl.sites(); ++i) {
+                    mx += std::cos(mdl.data()[i].theta);
+                    my += std::sin(mdl.data()[i].theta);
+                }
+                obs_out[3 * k + 1] = mx;
+                obs_out[3 * k + 2] = my;
+            }
+            ++k;
+            ++ks.counter;
+        });
+        for (std::size_t i = 0; i < n; ++i) theta[i] = model.data()[i].theta;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+// ------------------------------------------------------------------------ U(1)
+extern "C" int ref_u1_metropolis(std::uint64_t n_links, const std::uint32_t* cells, std::uint64_t n_cells,
+                      double model_beta, double driver_beta, double width, std::uint32_t hits,
+                      std::uint64_t seed, std::uint64_t sweep0, std::uint64_t n_sweeps,
+                      double* theta, double* obs_out)
+{
+    try {
+        using CM = CellModel<U1Dof, U1PlaquetteTerm, CellComplex<4>>;
+        std::vector<Cell<4>> cl(n_cells);
+        for (std::uint64_t c = 0; c < n_cells; ++c)
+            for (int k = 0; k < 4; ++k) cl[c].sites[k] = cells[4 * c + k];
+        CM model(CellComplex<4>(n_links, cl), U1PlaquetteTerm{model_beta});
+        for (std::size_t i = 0; i < n_links; ++i) {
+            const U1Link l{theta[i]};
+            model.update(i, &l);
+        }
+        KeyState ks;
+        ks.seed = seed;
+        ks.counter = sweep0;
+        MultiHit<CM> mh{&model, hits, std::vector<U1Link>(n_links * hits)};
+        using KQ = KeyedHit<U1Shift, CM>;
+        Metropolis<MultiHit<CM>, KQ, KeyedRng> mc(mh, KQ{U1Shift{width}, &ks, &mh}, KeyedRng{&ks}, driver_beta);
+        std::uint64_t k = 0;
+        mc.sample(n_sweeps, [&](const MultiHit<CM>&) {
+            if (obs_out) {
+                double sum = 0.0;
+                for (std::size_t c = 0; c < model.cells(); ++c) {
+                    const auto s = model.cell_sites(c);
+                    const U1Link* ls[4] = {model.data() + s[0], model.data() + s[1], model.data() + s[2], model.data() + s[3]};
+                    sum += model.term().cos_plaquette(ls);
+                }
+                const double P = sum / double(model.cells());
+                obs_out[2 * k] = model_beta * double(model.cells()) * (1.0 - P);
+                obs_out[2 * k + 1] = P;
+            }
+            ++k;
+            ++ks.counter;
+        });
+        for (std::size_t i = 0; i < n_links; ++i) theta[i] = model.data()[i].theta;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+// ----------------------------------------------------------------------- SU(N)
+namespace {
+template <std::size_t N>
+int su_metropolis(std::uint64_t n_links, const std::uint32_t* cells, std::uint64_t n_cells,
+                  double model_beta, double driver_beta, double width, std::uint32_t hits,
+                  std::uint64_t seed, std::uint64_t sweep0, std::uint64_t n_sweeps, double* links,
+                  double* obs_out)
+{
+    using CM = CellModel<SUDof<N>, SUPlaquetteTerm<N>, CellComplex<4>>;
+    std::vector<Cell<4>> cl(n_cells);
+    for (std::uint64_t c = 0; c < n_cells; ++c)
+        for (int k = 0; k < 4; ++k) cl[c].sites[k] = cells[4 * c + k];
+    CM model(CellComplex<4>(n_links, cl), SUPlaquetteTerm<N>{model_beta});
+    for (std::size_t i = 0; i < n_links; ++i) {
+        SULink<N> u;
+        for (std::size_t q = 0; q < N * N; ++q) u.m[q] = {links[(i * N * N + q) * 2], links[(i * N * N + q) * 2 + 1]};
+        model.update(i, &u);
+    }
+    KeyState ks;
+    ks.seed = seed;
+    ks.counter = sweep0;
+    MultiHit<CM> mh{&model, hits, std::vector<SULink<N>>(n_links * hits)};
+    using KQ = KeyedHit<SUShift<N>, CM>;
+    Metropolis<MultiHit<CM>, KQ, KeyedRng> mc(mh, KQ{SUShift<N>{width}, &ks, &mh}, KeyedRng{&ks}, driver_beta);
+    std::uint64_t k = 0;
+    mc.sample(n_sweeps, [&](const MultiHit<CM>&) {
+        if (obs_out) {
+            double sum = 0.0;
+            for (std::size_t c = 0; c < model.cells(); ++c) {
+                const auto s = model.cell_sites(c);
+                const SULink<N>* ls[4] = {model.data() + s[0], model.data() + s[1], model.data() + s[2], model.data() + s[3]};
+                sum += model.term().real_plaquette(ls);
+            }
+            const double P = sum / double(model.cells());
+            obs_out[2 * k] = model_beta * double(model.cells()) * (1.0 - P);
+            obs_out[2 * k + 1] = P;
+        }
+        ++k;
+        ++ks.counter;
+    });
+    for (std::size_t i = 0; i < n_links; ++i)
+        for (std::size_t q = 0; q < N * N; ++q) {
+            links[(i * N * N + q) * 2] = model.data()[i].m[q].real();
+            links[(i * N * N + q) * 2 + 1] = model.data()[i].m[q].imag();
+        }
+    return 0;
+}
+}  // namespace
+
+extern "C" int ref_su_metropolis(std::uint32_t N, std::uint64_t n_links, const std::uint32_t* cells,
+                      std::uint64_t n_cells, double model_beta, double driver_beta, double width,
+                      std::uint32_t hits, std::uint64_t seed, std::uint64_t sweep0,
+                      std::uint64_t n_sweeps, double* links, double* obs_out)
+{
+    try {
+        switch (N) {
+        case 2: return su_metropolis<2>(n_links, cells, n_cells, model_beta, driver_beta, width, hits, seed, sweep0, n_sweeps, links, obs_out);
+        case 3: return su_metropolis<3>(n_links, cells, n_cells, model_beta, driver_beta, width, hits, seed, sweep0, n_sweeps, links, obs_out);
+        default: return -2;
+        }
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+extern "C" void ref_su_expm(std::uint32_t N, const double* a, double* out)
+{
+    if (N == 2) {
+        sun_detail::Mat<2> m;
+        for (int q = 0; q < 4; ++q) m[q] = {a[2 * q], a[2 * q + 1]};
+        const auto r = sun_detail::expm<2>(m);
+        for (int q = 0; q < 4; ++q) { out[2 * q] = r.m[q].real(); out[2 * q + 1] = r.m[q].imag(); }
+    } else if (N == 3) {
+        sun_detail::Mat<3> m;
+        for (int q = 0; q < 9; ++q) m[q] = {a[2 * q], a[2 * q + 1]};
+        const auto r = sun_detail::expm<3>(m);
+        for (int q = 0; q < 9; ++q) { out[2 * q] = r.m[q].real(); out[2 * q + 1] = r.m[q].imag(); }
+    }
+}
+
+extern "C" void ref_su_shift(std::uint32_t N, double width, std::uint64_t seed, std::uint64_t counter,
+                  std::uint32_t tag, std::uint32_t id, const double* cur, double* out)
+{
+    KeyState ks;
+    ks.seed = seed;
+    ks.counter = counter;
+    ks.open(tag, id);
+    KeyedRng r{&ks};
+    if (N == 2) {
+        SULink<2> c, o;
+        for (int q = 0; q < 4; ++q) c.m[q] = {cur[2 * q], cur[2 * q + 1]};
+        SUShift<2>{width}.sample(&c, r, &o);
+        for (int q = 0; q < 4; ++q) { out[2 * q] = o.m[q].real(); out[2 * q + 1] = o.m[q].imag(); }
+    } else if (N == 3) {
+        SULink<3> c, o;
+        for (int q = 0; q < 9; ++q) c.m[q] = {cur[2 * q], cur[2 * q + 1]};
+        SUShift<3>{width}.sample(&c, r, &o);
+        for (int q = 0; q < 9; ++q) { out[2 * q] = o.m[q].real(); out[2 * q + 1] = o.m[q].imag(); }
+    }
+}
+
+// -------------------------------------------------------------- CPU baseline
+// Times the reference's stock path: VectorSpin<3> on a periodic L^3 PairGraph,
+// Metropolis with UniformSphereN<3> and a plain Pcg32, alternating one sweep
+// with one Wolff flip (UniformSphereN<3> axis).  One independent chain per
+// thread.  Returns total site-updates (sweep sites + flipped cluster sites)
+// and the wall time of the slowest thread.
+extern "C" int ref_bench_o3(std::uint64_t L, double beta, std::uint64_t steps, std::uint32_t threads,
+                 std::uint64_t seed, double* site_updates, double* seconds)
+{
+    try {
+        std::vector<PairGraph<>::Edge> edges;
+        edges.reserve(3 * L * L * L);
+        for (std::uint64_t z = 0; z < L; ++z)
+            for (std::uint64_t y = 0; y < L; ++y)
+                for (std::uint64_t x = 0; x < L; ++x) {
+                    const auto i = static_cast<std::uint32_t>((z * L + y) * L + x);
+                    edges.push_back({i, static_cast<std::uint32_t>((z * L + y) * L + (x + 1) % L), {}});
+                    edges.push_back({i, static_cast<std::uint32_t>((z * L + (y + 1) % L) * L + x), {}});
+                    edges.push_back({i, static_cast<std::uint32_t>((((z + 1) % L) * L + y) * L + x), {}});
+                }
+        const std::size_t n = L * L * L;
+        std::vector<double> upd(threads, 0.0), secs(threads, 0.0);
+        std::vector<std::thread> pool;
+        for (std::uint32_t t = 0; t < threads; ++t)
+            pool.emplace_back([&, t] {
+                VectorSpin<3> model(PairGraph<>(n, edges), 1.0);
+                Pcg32 init(seed + t, 7);
+                double v[3];
+                for (std::size_t i = 0; i < n; ++i) {
+                    UniformSphereN<3>{}.sample(nullptr, init, v);
+                    model.update(i, v);
+                }
+                Metropolis<VectorSpin<3>, UniformSphereN<3>, Pcg32> mc(model, UniformSphereN<3>{}, Pcg32(seed + t, 1), beta);
+                Wolff<VectorSpin<3>, UniformSphereN<3>, Pcg32> w(model, UniformSphereN<3>{}, Pcg32(seed + t, 2), beta);
+                const auto t0 = std::chrono::steady_clock::now();
+                double u = 0.0;
+                for (std::uint64_t s = 0; s < steps; ++s) {
+                    mc.sweep();
+                    u += double(n);
+                    u += double(w.flip());
+                }
+                const auto t1 = std::chrono::steady_clock::now();
+                upd[t] = u;
+                secs[t] = std::chrono::duration<double>(t1 - t0).count();
+            });
+        for (auto& th : pool) th.join();
+        double total = 0.0, worst = 0.0;
+        for (std::uint32_t t = 0; t < threads; ++t) {
+            total += upd[t];
+            if (secs[t] > worst) worst = secs[t];
+        }
+        *site_updates = total;
+        *seconds = worst;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+// Times the reference's stock Ising Metropolis on an Lx x Ly square_lattice
+// (example/ising.hpp + Flip + Pcg32), one chain per thread, cold start.
+extern "C" int ref_bench_ising(std::uint64_t L, double beta, std::uint64_t sweeps, std::uint32_t threads,
+                    std::uint64_t seed, double* site_updates, double* seconds)
+{
+    try {
+        std::vector<double> secs(threads, 0.0);
+        std::vector<std::thread> pool;
+        for (std::uint32_t t = 0; t < threads; ++t)
+            pool.emplace_back([&, t] {
+                Ising model(square_lattice(L, L), 1);
+                Metropolis<Ising, Flip, Pcg32> mc(model, Flip{}, Pcg32(seed + t, 1), beta);
+                const auto t0 = std::chrono::steady_clock::now();
+                mc.run(sweeps);
+                const auto t1 = std::chrono::steady_clock::now();
+                secs[t] = std::chrono::duration<double>(t1 - t0).count();
+            });
+        for (auto& th : pool) th.join();
+        double worst = 0.0;
+        for (double s : secs) worst = s > worst ? s : worst;
+        *site_updates = double(threads) * double(L * L) * double(sweeps);
+        *seconds = worst;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+

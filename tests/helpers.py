@@ -1,0 +1,98 @@
+"""Shared set-up for the parity tests: lattices, colour-major relabelling and
+seeded states, computed independently of the engine (numpy only)."""
+from __future__ import annotations
+
+import numpy as np
+
+
+def square_edges(Lx: int, Ly: int):
+    """square_lattice's edge list (lattice/square.hpp:27-35)."""
+    ei, ej = [], []
+    for y in range(Ly):
+        for x in range(Lx):
+            i = y * Lx + x
+            if Lx > 1:
+                ei.append(i)
+                ej.append(y * Lx + (x + 1) % Lx)
+            if Ly > 1:
+                ei.append(i)
+                ej.append(((y + 1) % Ly) * Lx + x)
+    return np.array(ei, np.uint32), np.array(ej, np.uint32)
+
+
+def cubic_edges(Lx: int, Ly: int, Lz: int):
+    ei, ej = [], []
+    for z in range(Lz):
+        for y in range(Ly):
+            for x in range(Lx):
+                i = (z * Ly + y) * Lx + x
+                if Lx > 1:
+                    ei.append(i)
+                    ej.append((z * Ly + y) * Lx + (x + 1) % Lx)
+                if Ly > 1:
+                    ei.append(i)
+                    ej.append((z * Ly + (y + 1) % Ly) * Lx + x)
+                if Lz > 1:
+                    ei.append(i)
+                    ej.append((((z + 1) % Lz) * Ly + y) * Lx + x)
+    return np.array(ei, np.uint32), np.array(ej, np.uint32)
+
+
+def checker_position(Lx: int, Ly: int, Lz: int = 1):
+    """Colour-major index of every site of an even periodic lattice:
+    colour (x+y+z)&1 first, then site/2."""
+    n = Lx * Ly * Lz
+    s = np.arange(n)
+    x, y, z = s % Lx, (s // Lx) % Ly, s // (Lx * Ly)
+    c = (x + y + z) & 1
+    return (c * (n // 2) + s // 2).astype(np.uint32)
+
+
+def link_class_position(L: int, dim: int):
+    """Colour-major index of every link of an even periodic plaquette complex
+    (links mu*L^dim + site): class 2*mu + parity, then site/2."""
+    V = L ** dim
+    i = np.arange(dim * V)
+    mu, s = i // V, i % V
+    par = np.zeros_like(s)
+    r = s.copy()
+    for _ in range(dim):
+        par += r % L
+        r //= L
+    cls = 2 * mu + (par & 1)
+    return (cls * (V // 2) + s // 2).astype(np.uint32)
+
+
+def relabel_edges(ei, ej, position):
+    return position[ei].astype(np.uint32), position[ej].astype(np.uint32)
+
+
+def relabel_cells(cells, position):
+    return position[np.asarray(cells)].astype(np.uint32)
+
+
+def to_colour_major(values, position):
+    """values[site] -> out[position[site]]."""
+    out = np.empty_like(values)
+    out[position] = values
+    return out
+
+
+def from_colour_major(values, position):
+    return values[position]
+
+
+def random_unit_vectors(n: int, N: int, seed: int):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(n, N))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return v
+
+
+def square_plaquette_cells(L: int):
+    L2 = L * L
+    cells = []
+    for y in range(L):
+        for x in range(L):
+            cells.append([y * L + x, L2 + y * L + (x + 1) % L, ((y + 1) % L) * L + x, L2 + y * L + x])
+    return np.array(cells, np.uint32)

@@ -1,0 +1,172 @@
+"""The C ABI library on a host without a GPU: it loads, exports every symbol the
+header declares, builds the reference's tables identically, and fails loudly
+(no CPU fallback) when asked to create a chain."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from helpers import checker_position, cubic_edges, link_class_position, square_edges
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    names = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if not h.endswith(".h"):
+            continue
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names |= set(re.findall(r"\b(umc_[a-z0-9_]+)\s*\(", src))
+    return names
+
+
+def test_library_exports_every_declared_symbol(umc):
+    names = _declared_symbols()
+    assert len(names) > 30
+    missing = [n for n in sorted(names) if not hasattr(umc.lib, n)]
+    assert not missing, missing
+
+
+def test_abi_version(umc):
+    assert umc.lib.umc_abi_version() == 1
+
+
+@pytest.mark.parametrize("Lx,Ly", [(1, 1), (1, 4), (2, 2), (4, 4), (3, 5), (8, 6)])
+def test_square_lattice_matches_oracle(umc, oracle, Lx, Ly):
+    g = umc.square_lattice(Lx, Ly)
+    off, bonds = g.csr()
+    _, ei, ej = oracle.square_edges(Lx, Ly)
+    _, off2, bonds2, _ = oracle.pair_graph(Lx * Ly, ei, ej)
+    np.testing.assert_array_equal(off, off2)
+    np.testing.assert_array_equal(bonds, bonds2)
+
+
+def test_square_lattice_matches_reference(umc, golden):
+    for Lx, Ly in [(1, 1), (1, 4), (2, 2), (4, 4), (3, 5)]:
+        off, bonds = umc.square_lattice(Lx, Ly).csr()
+        np.testing.assert_array_equal(off, golden[f"square_{Lx}x{Ly}_off"])
+        np.testing.assert_array_equal(bonds, golden[f"square_{Lx}x{Ly}_bonds"])
+
+
+def test_cubic_lattice_matches_edge_list(umc, oracle):
+    g = umc.cubic_lattice(4, 2, 6)
+    off, bonds = g.csr()
+    ei, ej = cubic_edges(4, 2, 6)
+    _, off2, bonds2, _ = oracle.pair_graph(48, ei, ej)
+    np.testing.assert_array_equal(off, off2)
+    np.testing.assert_array_equal(bonds, bonds2)
+
+
+def test_graph_errors_mirror_reference_exceptions(umc):
+    with pytest.raises(ValueError):
+        umc.PairGraph(2, [[0, 0]])  # self-loop: std::invalid_argument
+    with pytest.raises(IndexError):
+        umc.PairGraph(2, [[0, 2]])  # std::out_of_range
+    with pytest.raises(OverflowError):
+        umc.PairGraph(2**32 + 1, [])  # std::overflow_error
+    with pytest.raises(ValueError):
+        umc.square_lattice(0, 3)
+    with pytest.raises(ValueError):
+        umc.hypercubic_plaquettes(0)
+    with pytest.raises(IndexError):
+        umc.CellComplex(3, [[0, 1, 2, 3]])
+    g = umc.PairGraph(2, [[0, 1], [0, 1]])
+    assert g.degree(0) == 2  # duplicates kept
+    g = umc.PairGraph(3, [])
+    assert g.sites() == 3 and g.degree(1) == 0
+    g = umc.PairGraph(2, [[0, 1]], symmetric=False)
+    assert g.degree(0) == 1 and g.degree(1) == 0
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 1), (2, 2, 1), (6, 4, 1), (4, 4, 4), (2, 6, 8)])
+def test_even_lattices_use_the_checkerboard(umc, dims):
+    g = umc.cubic_lattice(*dims) if dims[2] > 1 else umc.square_lattice(dims[0], dims[1])
+    nc, col, pos = g.colouring()
+    assert nc == 2
+    np.testing.assert_array_equal(pos, checker_position(*dims))
+
+
+@pytest.mark.parametrize("Lx,Ly", [(3, 3), (5, 4), (3, 7)])
+def test_odd_lattices_get_a_valid_colouring(umc, oracle, Lx, Ly):
+    g = umc.square_lattice(Lx, Ly)
+    nc, col, pos = g.colouring()
+    off, bonds = g.csr()
+    assert nc >= 3 and oracle.check_colouring(off, bonds, col)
+    assert sorted(pos) == list(range(Lx * Ly))
+    # colour-major: classes contiguous, ascending site id inside a class
+    order = np.argsort(pos)
+    assert (np.diff(col[order]) >= 0).all()
+    for c in range(nc):
+        sites = order[col[order] == c]
+        assert (np.diff(sites) > 0).all()
+
+
+def test_random_graph_colouring_is_valid(umc, oracle):
+    rng = np.random.default_rng(2)
+    n = 200
+    e = rng.integers(0, n, (700, 2))
+    e = e[e[:, 0] != e[:, 1]]
+    g = umc.PairGraph(n, e)
+    nc, col, pos = g.colouring()
+    off, bonds = g.csr()
+    assert oracle.check_colouring(off, bonds, col)
+    gd = umc.PairGraph(n, e, symmetric=False)
+    _, cold, _ = gd.colouring()
+    sym_off, sym_b = umc.PairGraph(n, e).csr()
+    assert oracle.check_colouring(sym_off, sym_b, cold)
+
+
+def test_hypercubic_matches_reference(umc, golden):
+    c = umc.hypercubic_plaquettes(2)
+    np.testing.assert_array_equal(c.table(), golden["hyper2_cells"])
+    off, ic, iw = c.incidence()
+    np.testing.assert_array_equal(off, golden["hyper2_off"])
+    np.testing.assert_array_equal(ic, golden["hyper2_inc_cell"])
+    np.testing.assert_array_equal(iw, golden["hyper2_inc_which"])
+
+
+@pytest.mark.parametrize("L,dim", [(2, 4), (4, 4), (4, 2), (8, 2)])
+def test_plaquette_complexes_use_direction_parity_classes(umc, oracle, L, dim):
+    c = umc.hypercubic_plaquettes(L) if dim == 4 else umc.square_plaquettes(L)
+    nc, col, pos = c.colouring()
+    assert nc == 2 * dim
+    np.testing.assert_array_equal(pos, link_class_position(L, dim))
+    assert oracle.check_cell_colouring(c.sites(), c.table(), col)
+
+
+def test_odd_plaquette_complex_colouring_is_valid(umc, oracle):
+    c = umc.hypercubic_plaquettes(3)
+    nc, col, _ = c.colouring()
+    assert oracle.check_cell_colouring(c.sites(), c.table(), col)
+    c2 = umc.square_plaquettes(5)
+    _, col2, _ = c2.colouring()
+    assert oracle.check_cell_colouring(c2.sites(), c2.table(), col2)
+
+
+def test_chain_fails_loudly_without_gpu(umc):
+    if umc.device_count() > 0:
+        pytest.skip("a GPU is present")
+    with pytest.raises(umc.UmcError) as e:
+        umc.Chain(umc.MODEL_ISING, graph=umc.square_lattice(4, 4), coupling=1)
+    assert e.value.code == umc.ERR_CUDA
+
+
+def test_ising_thresholds_pin_the_reference_accept_rule():
+    """accept iff draw <= tm1 reproduces log(k 2^-32) < -beta dE exactly."""
+    import math
+
+    for beta, dE in [(0.44, 4), (0.44, 8), (0.3, 4), (1.7, 12), (0.01, 2)]:
+        log_p = -beta * dE + 0.0
+        lo, hi = 0, 1 << 32
+        while hi - lo > 1:
+            mid = (lo + hi) // 2
+            if math.log(mid * 2.0**-32) < log_p:
+                lo = mid
+            else:
+                hi = mid
+        assert math.log(lo * 2.0**-32) < log_p
+        assert not math.log((lo + 1) * 2.0**-32) < log_p

@@ -1,0 +1,652 @@
+"""B200 engine for the local-update hot path of universal_monte_carlo.
+
+The engine is ``libumc_b200.so`` (hand-written sm_100a CUDA behind the C ABI in
+``include/umc_b200.h``).  This module binds that ABI with ctypes and mirrors the
+reference's user-facing names so scripts read like the reference's tests:
+
+=====================  ================================================
+reference              here
+=====================  ================================================
+PairGraph(n, edges)    ``PairGraph(n, edges, symmetric=True)``
+square_lattice(Lx,Ly)  ``square_lattice(Lx, Ly)``
+(3D by hand)           ``cubic_lattice(Lx, Ly, Lz)``
+CellComplex<4>         ``CellComplex(n_sites, cells)``
+hypercubic_plaquettes  ``hypercubic_plaquettes(L)``
+Ising / VectorSpin<N>  ``Ising(graph, J)`` / ``VectorSpin(N, graph, J)``
+XY (angles, PairModel) ``XYAngle(graph, J)``
+U1Gauge / SUGauge<N>   ``U1Gauge(cells, beta)`` / ``SUGauge(N, cells, beta)``
+Metropolis<M,Q,R>      ``Metropolis(model, proposal, rng, beta)``
+Wolff<M,A,R>           ``Wolff(model, axis, rng, beta)``
+Pcg32(seed, stream)    ``Pcg32(seed, stream)`` (keys the counter streams)
+=====================  ================================================
+
+There is no CPU fallback: importing this module fails if the library was not
+built, and creating a model fails (``UmcError``) on a host without a GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libumc_b200.so")
+
+if not os.path.isfile(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `python universal_classical_montecarlo_b200/_build.py`"
+    )
+lib = C.CDLL(LIB_PATH)
+
+# ------------------------------------------------------------------ constants
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_OUT_OF_RANGE = 2
+ERR_OVERFLOW = 3
+ERR_UNSUPPORTED = 4
+ERR_CUDA = 5
+ERR_DEVICE_TIMEOUT = 6
+ERR_OUT_OF_MEMORY = 7
+ERR_STATE = 8
+
+MODEL_ISING = 1
+MODEL_VECTOR = 2
+MODEL_XY_ANGLE = 3
+MODEL_U1 = 4
+MODEL_SU = 5
+
+PROPOSAL_FLIP = 1
+PROPOSAL_SPHERE = 2
+PROPOSAL_ROTATION = 3
+PROPOSAL_U1SHIFT = 4
+PROPOSAL_SUSHIFT = 5
+
+AXIS_NONE = 0
+AXIS_FIXED = 1
+AXIS_SPHERE = 2
+
+OBS_STRIDE = 8
+
+
+class UmcError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[umc status {code}] {msg}")
+        self.code = code
+
+
+def _exc(code: int, msg: str) -> Exception:
+    # the reference builders' exception types
+    if code == ERR_INVALID_ARGUMENT:
+        return ValueError(msg)
+    if code == ERR_OUT_OF_RANGE:
+        return IndexError(msg)
+    if code == ERR_OVERFLOW:
+        return OverflowError(msg)
+    return UmcError(code, msg)
+
+
+_vp = C.c_void_p
+_u32 = C.c_uint32
+_u64 = C.c_uint64
+_i32 = C.c_int32
+_f64 = C.c_double
+_int = C.c_int
+
+
+class ChainDesc(C.Structure):
+    _fields_ = [
+        ("model", _i32),
+        ("components", _i32),
+        ("graph", _vp),
+        ("cells", _vp),
+        ("coupling", _f64),
+        ("proposal", _i32),
+        ("width", _f64),
+        ("hits", _u32),
+        ("wolff_axis", _i32),
+        ("seed", _u64),
+        ("device", _i32),
+        ("stream", _vp),
+        ("max_records", _u64),
+    ]
+
+
+def _decl(name, restype, *args):
+    f = getattr(lib, name)
+    f.restype = restype
+    f.argtypes = list(args)
+    return f
+
+
+_last_error = _decl("umc_last_error", C.c_char_p)
+_decl("umc_abi_version", _int)
+_decl("umc_device_count", _int, C.POINTER(_int))
+_decl("umc_graph_create", _int, _u64, _vp, _vp, _u64, _int, C.POINTER(_vp))
+_decl("umc_graph_square", _int, _u64, _u64, C.POINTER(_vp))
+_decl("umc_graph_cubic", _int, _u64, _u64, _u64, C.POINTER(_vp))
+_decl("umc_graph_destroy", None, _vp)
+_decl("umc_graph_sites", _u64, _vp)
+_decl("umc_graph_slots", _u64, _vp)
+_decl("umc_graph_csr", _int, _vp, _vp, _vp)
+_decl("umc_graph_colouring", _int, _vp, _vp, _vp, _vp)
+_decl("umc_cells_create", _int, _u64, _u32, _vp, _u64, C.POINTER(_vp))
+_decl("umc_cells_hypercubic", _int, _u64, C.POINTER(_vp))
+_decl("umc_cells_square_plaquettes", _int, _u64, C.POINTER(_vp))
+_decl("umc_cells_destroy", None, _vp)
+_decl("umc_cells_sites", _u64, _vp)
+_decl("umc_cells_count", _u64, _vp)
+_decl("umc_cells_arity", _u32, _vp)
+_decl("umc_cells_table", _int, _vp, _vp)
+_decl("umc_cells_incidence", _int, _vp, _vp, _vp, _vp)
+_decl("umc_cells_colouring", _int, _vp, _vp, _vp, _vp)
+_decl("umc_chain_create", _int, C.POINTER(ChainDesc), C.POINTER(_vp))
+_decl("umc_chain_destroy", _int, _vp)
+_decl("umc_chain_set_field", _int, _vp, _vp)
+_decl("umc_chain_get_field", _int, _vp, _vp)
+_decl("umc_chain_randomize", _int, _vp, _u64)
+_decl("umc_chain_set_proposal", _int, _vp, _i32, _f64, _u32)
+_decl("umc_chain_set_wolff_axis", _int, _vp, _i32)
+_decl("umc_chain_set_seed", _int, _vp, _u64)
+_decl("umc_chain_counters", _int, _vp, C.POINTER(_u64), C.POINTER(_u64))
+_decl("umc_chain_set_counters", _int, _vp, _u64, _u64)
+_decl("umc_chain_stream", _vp, _vp)
+_decl("umc_chain_sync", _int, _vp)
+_decl("umc_chain_observe", _int, _vp, _vp)
+_decl("umc_metropolis_run", _int, _vp, _f64, _u64, _vp)
+_decl("umc_wolff_run", _int, _vp, _f64, _u64, _vp, _vp)
+_decl("umc_hybrid_run", _int, _vp, _f64, _u64, _vp, _vp)
+_decl("umc_metropolis_enqueue", _int, _vp, _f64, _u64)
+_decl("umc_wolff_enqueue", _int, _vp, _f64, _u64)
+_decl("umc_hybrid_enqueue", _int, _vp, _f64, _u64)
+_decl("umc_chain_fetch", _int, _vp, _vp, _vp, _u64, C.POINTER(_u64))
+_decl("umc_wolff_stats", _int, _vp, C.POINTER(_u64), C.POINTER(_f64))
+
+
+def check(code: int) -> None:
+    if code != OK:
+        raise _exc(code, (_last_error() or b"").decode())
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def device_count() -> int:
+    n = _int(0)
+    check(lib.umc_device_count(C.byref(n)))
+    return n.value
+
+
+# ===================================================================== tables
+class PairGraph:
+    """PairGraph(n, edges, symmetric) -- lattice/pair_graph.hpp:49-83."""
+
+    def __init__(self, n_sites: int = 0, edges=None, symmetric: bool = True, _handle=None):
+        if _handle is not None:
+            self._h = _handle
+            return
+        e = np.zeros((0, 2), np.uint32) if edges is None else np.asarray(edges)
+        e = np.ascontiguousarray(e.reshape(-1, 2))
+        if e.size and (e.min() < 0 or e.max() > 0xFFFFFFFF):
+            raise IndexError("PairGraph: edge endpoint out of range")
+        ei = np.ascontiguousarray(e[:, 0], np.uint32)
+        ej = np.ascontiguousarray(e[:, 1], np.uint32)
+        h = _vp()
+        check(lib.umc_graph_create(n_sites, _ptr(ei), _ptr(ej), len(ei), int(symmetric), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.umc_graph_destroy(h)
+            self._h = None
+
+    def sites(self) -> int:
+        return int(lib.umc_graph_sites(self._h))
+
+    def csr(self):
+        n = self.sites()
+        off = np.zeros(n + 1, np.uint32)
+        bonds = np.zeros(int(lib.umc_graph_slots(self._h)), np.uint32)
+        check(lib.umc_graph_csr(self._h, _ptr(off), _ptr(bonds)))
+        return off, bonds
+
+    def degree(self, i: int) -> int:
+        off, _ = self.csr()
+        return int(off[i + 1] - off[i])
+
+    def colouring(self):
+        """(n_colours, colour[n], position[n]) of the colour passes."""
+        n = self.sites()
+        nc = _u32(0)
+        col = np.zeros(n, np.uint32)
+        pos = np.zeros(n, np.uint32)
+        check(lib.umc_graph_colouring(self._h, C.byref(nc), _ptr(col), _ptr(pos)))
+        return nc.value, col, pos
+
+
+def square_lattice(Lx: int, Ly: int) -> PairGraph:
+    """square_lattice(Lx, Ly) -- lattice/square.hpp:15-38."""
+    h = _vp()
+    check(lib.umc_graph_square(Lx, Ly, C.byref(h)))
+    return PairGraph(_handle=h)
+
+
+def cubic_lattice(Lx: int, Ly: int, Lz: int) -> PairGraph:
+    """Periodic cubic lattice with square_lattice's conventions (no reference builder)."""
+    h = _vp()
+    check(lib.umc_graph_cubic(Lx, Ly, Lz, C.byref(h)))
+    return PairGraph(_handle=h)
+
+
+class CellComplex:
+    """CellComplex<A>(sites, cells) -- lattice/cell_complex.hpp:36-63."""
+
+    def __init__(self, n_sites: int = 0, cells=None, _handle=None):
+        if _handle is not None:
+            self._h = _handle
+            return
+        c = np.ascontiguousarray(np.asarray(cells), np.uint32)
+        if c.ndim != 2:
+            raise ValueError("cells must be (n_cells, arity)")
+        h = _vp()
+        check(lib.umc_cells_create(n_sites, c.shape[1], _ptr(c), c.shape[0], C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.umc_cells_destroy(h)
+            self._h = None
+
+    def sites(self) -> int:
+        return int(lib.umc_cells_sites(self._h))
+
+    def cells(self) -> int:
+        return int(lib.umc_cells_count(self._h))
+
+    def table(self):
+        a = int(lib.umc_cells_arity(self._h))
+        t = np.zeros((self.cells(), a), np.uint32)
+        check(lib.umc_cells_table(self._h, _ptr(t)))
+        return t
+
+    def incidence(self):
+        n = self.sites()
+        tot = self.cells() * int(lib.umc_cells_arity(self._h))
+        off = np.zeros(n + 1, np.uint64)
+        ic = np.zeros(tot, np.uint32)
+        iw = np.zeros(tot, np.uint8)
+        check(lib.umc_cells_incidence(self._h, _ptr(off), _ptr(ic), _ptr(iw)))
+        return off, ic, iw
+
+    def colouring(self):
+        n = self.sites()
+        nc = _u32(0)
+        col = np.zeros(n, np.uint32)
+        pos = np.zeros(n, np.uint32)
+        check(lib.umc_cells_colouring(self._h, C.byref(nc), _ptr(col), _ptr(pos)))
+        return nc.value, col, pos
+
+
+def hypercubic_plaquettes(L: int) -> CellComplex:
+    """hypercubic_plaquettes(L) -- lattice/hypercubic.hpp:15-64."""
+    h = _vp()
+    check(lib.umc_cells_hypercubic(L, C.byref(h)))
+    return CellComplex(_handle=h)
+
+
+def square_plaquettes(L: int) -> CellComplex:
+    """Periodic 2D plaquette complex with the hypercubic orientation rule."""
+    h = _vp()
+    check(lib.umc_cells_square_plaquettes(L, C.byref(h)))
+    return CellComplex(_handle=h)
+
+
+# ===================================================================== chains
+class Chain:
+    """One model's field on one GPU (the C ABI's umc_chain)."""
+
+    def __init__(self, model: int, *, graph: PairGraph | None = None, cells: CellComplex | None = None,
+                 components: int = 1, coupling: float = 1.0, proposal: int = 0, width: float = 0.0,
+                 hits: int = 1, wolff_axis: int = AXIS_NONE, seed: int = 1, device: int = 0,
+                 stream: int | None = None, max_records: int = 0):
+        d = ChainDesc()
+        d.model = model
+        d.components = components
+        d.graph = graph._h if graph is not None else None
+        d.cells = cells._h if cells is not None else None
+        d.coupling = coupling
+        d.proposal = proposal
+        d.width = width
+        d.hits = hits
+        d.wolff_axis = wolff_axis
+        d.seed = seed
+        d.device = device
+        d.stream = stream
+        d.max_records = max_records
+        h = _vp()
+        check(lib.umc_chain_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.model = model
+        self.components = components
+        self._graph = graph
+        self._cells = cells
+        if model == MODEL_ISING:
+            self.dtype, self.comps = np.int8, 1
+        elif model == MODEL_VECTOR:
+            self.dtype, self.comps = np.float32, components
+        elif model in (MODEL_XY_ANGLE, MODEL_U1):
+            self.dtype, self.comps = np.float32, 1
+        else:
+            self.dtype, self.comps = np.float32, components * components * 2
+        self.n = graph.sites() if graph is not None else cells.sites()
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.umc_chain_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_field(self, field) -> None:
+        a = np.ascontiguousarray(np.asarray(field, self.dtype).reshape(-1))
+        if a.size != self.n * self.comps:
+            raise ValueError(f"field has {a.size} scalars, expected {self.n * self.comps}")
+        check(lib.umc_chain_set_field(self._h, _ptr(a)))
+
+    def get_field(self) -> np.ndarray:
+        a = np.zeros(self.n * self.comps, self.dtype)
+        check(lib.umc_chain_get_field(self._h, _ptr(a)))
+        return a.reshape(self.n, self.comps) if self.comps > 1 else a
+
+    def randomize(self, seed: int) -> None:
+        check(lib.umc_chain_randomize(self._h, seed))
+
+    def set_proposal(self, proposal: int, width: float = 0.0, hits: int = 1) -> None:
+        check(lib.umc_chain_set_proposal(self._h, proposal, width, hits))
+
+    def set_wolff_axis(self, axis: int) -> None:
+        check(lib.umc_chain_set_wolff_axis(self._h, axis))
+
+    def set_seed(self, seed: int) -> None:
+        check(lib.umc_chain_set_seed(self._h, seed))
+
+    def counters(self):
+        s, f = _u64(0), _u64(0)
+        check(lib.umc_chain_counters(self._h, C.byref(s), C.byref(f)))
+        return s.value, f.value
+
+    def set_counters(self, sweeps: int, flips: int) -> None:
+        check(lib.umc_chain_set_counters(self._h, sweeps, flips))
+
+    def stream(self) -> int:
+        return lib.umc_chain_stream(self._h) or 0
+
+    def sync(self) -> None:
+        check(lib.umc_chain_sync(self._h))
+
+    def observe(self) -> np.ndarray:
+        r = np.zeros(OBS_STRIDE)
+        check(lib.umc_chain_observe(self._h, _ptr(r)))
+        return r
+
+    def metropolis(self, beta: float, n: int, records: bool = True):
+        rec = np.zeros((n, OBS_STRIDE)) if records else None
+        check(lib.umc_metropolis_run(self._h, beta, n, _ptr(rec)))
+        return rec
+
+    def wolff(self, beta: float, n: int, records: bool = True):
+        sizes = np.zeros(n, np.uint64)
+        rec = np.zeros((n, OBS_STRIDE)) if records else None
+        check(lib.umc_wolff_run(self._h, beta, n, _ptr(sizes), _ptr(rec)))
+        return sizes, rec
+
+    def hybrid(self, beta: float, n: int):
+        sizes = np.zeros(n, np.uint64)
+        rec = np.zeros((n, OBS_STRIDE))
+        check(lib.umc_hybrid_run(self._h, beta, n, _ptr(sizes), _ptr(rec)))
+        return sizes, rec
+
+    def enqueue_metropolis(self, beta: float, n: int) -> None:
+        check(lib.umc_metropolis_enqueue(self._h, beta, n))
+
+    def enqueue_wolff(self, beta: float, n: int) -> None:
+        check(lib.umc_wolff_enqueue(self._h, beta, n))
+
+    def enqueue_hybrid(self, beta: float, n: int) -> None:
+        check(lib.umc_hybrid_enqueue(self._h, beta, n))
+
+    def fetch(self, capacity: int):
+        rec = np.zeros((capacity, OBS_STRIDE))
+        sizes = np.zeros(capacity, np.uint64)
+        got = _u64(0)
+        check(lib.umc_chain_fetch(self._h, _ptr(rec), _ptr(sizes), capacity, C.byref(got)))
+        return rec[: got.value], sizes[: got.value]
+
+    def wolff_stats(self):
+        f, s = _u64(0), _f64(0)
+        check(lib.umc_wolff_stats(self._h, C.byref(f), C.byref(s)))
+        return f.value, s.value
+
+
+# ========================================================= reference mirror
+class Pcg32:
+    """The driver's RNG argument: (seed, stream) choose the key seed of every
+    counter-keyed stream the driver opens (rng.hpp:14-20 for the generator)."""
+
+    def __init__(self, seed: int, stream: int = 0):
+        self.seed = int(seed)
+        self.stream = int(stream)
+
+    @property
+    def key(self) -> int:
+        return (self.seed ^ ((self.stream * 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF)) & 0xFFFFFFFFFFFFFFFF
+
+
+class Flip:
+    """dof/ising.hpp:27-38."""
+    kind = PROPOSAL_FLIP
+    width = 0.0
+
+
+class FixedAxis:
+    """dof/ising.hpp:41-49."""
+    axis = AXIS_FIXED
+
+
+class UniformSphereN:
+    """dof/vector.hpp:35-61 (also the Wolff axis for VectorSpin)."""
+    kind = PROPOSAL_SPHERE
+    axis = AXIS_SPHERE
+    width = 0.0
+
+    def __init__(self, N: int | None = None):
+        self.N = N
+
+
+class LocalRotation:
+    """dof/vector.hpp:70-122."""
+    kind = PROPOSAL_ROTATION
+
+    def __init__(self, delta: float):
+        self.width = float(delta)
+
+
+class U1Shift:
+    """dof/u1.hpp:35-50."""
+    kind = PROPOSAL_U1SHIFT
+
+    def __init__(self, width: float = 0.5):
+        self.width = float(width)
+
+
+class SUShift:
+    """dof/sun.hpp:163-204."""
+    kind = PROPOSAL_SUSHIFT
+
+    def __init__(self, width: float = 0.3):
+        self.width = float(width)
+
+
+class _Model:
+    _model = 0
+    _components = 1
+
+    def _chain(self, proposal=None, hits=1) -> Chain:
+        if self.chain is None:
+            kind = getattr(proposal, "kind", self._default_proposal)
+            width = getattr(proposal, "width", 0.0)
+            self.chain = Chain(self._model, graph=self._graph, cells=self._cells, components=self._components,
+                               coupling=self._coupling, proposal=kind, width=width, hits=hits, device=self._device)
+        return self.chain
+
+    def data(self) -> np.ndarray:
+        """The field in the reference's data() layout (forces a device copy)."""
+        return self._chain().get_field()
+
+    def update_all(self, field) -> None:
+        self._chain().set_field(field)
+
+    def sites(self) -> int:
+        return self._chain().n
+
+    def observe(self) -> np.ndarray:
+        return self._chain().observe()
+
+
+class Ising(_Model):
+    """Ising(graph, J) -- example/ising.hpp:14-76 (cold start: all +1)."""
+    _model = MODEL_ISING
+    _default_proposal = PROPOSAL_FLIP
+
+    def __init__(self, graph: PairGraph, J: int = 1, device: int = 0):
+        self._graph, self._cells, self._coupling, self._device = graph, None, float(J), device
+        self.chain = None
+
+
+class VectorSpin(_Model):
+    """VectorSpin<N>(graph, J) -- example/vector_spin.hpp:14-83 (FP32 state)."""
+    _model = MODEL_VECTOR
+    _default_proposal = PROPOSAL_SPHERE
+
+    def __init__(self, N: int, graph: PairGraph, J: float = 1.0, device: int = 0):
+        self._graph, self._cells, self._coupling, self._device = graph, None, float(J), device
+        self._components = N
+        self.chain = None
+
+
+def XY(graph: PairGraph, J: float = 1.0, device: int = 0) -> VectorSpin:
+    return VectorSpin(2, graph, J, device)
+
+
+def Heisenberg(graph: PairGraph, J: float = 1.0, device: int = 0) -> VectorSpin:
+    return VectorSpin(3, graph, J, device)
+
+
+class XYAngle(_Model):
+    """XY model on FP32 angles: PairModel<U1Dof, -J cos(ti - tj)> (model/pair.hpp)."""
+    _model = MODEL_XY_ANGLE
+    _default_proposal = PROPOSAL_U1SHIFT
+
+    def __init__(self, graph: PairGraph, J: float = 1.0, device: int = 0):
+        self._graph, self._cells, self._coupling, self._device = graph, None, float(J), device
+        self.chain = None
+
+
+class U1Gauge(_Model):
+    """U(1) gauge theory on a plaquette complex (example/u1_gauge.hpp)."""
+    _model = MODEL_U1
+    _default_proposal = PROPOSAL_U1SHIFT
+
+    def __init__(self, cells: CellComplex, beta: float = 1.0, device: int = 0):
+        self._graph, self._cells, self._coupling, self._device = None, cells, float(beta), device
+        self.chain = None
+
+
+class SUGauge(_Model):
+    """SU(N) gauge theory on a plaquette complex (example/sun_gauge.hpp)."""
+    _model = MODEL_SU
+    _default_proposal = PROPOSAL_SUSHIFT
+
+    def __init__(self, N: int, cells: CellComplex, beta: float = 1.0, device: int = 0):
+        self._graph, self._cells, self._coupling, self._device = None, cells, float(beta), device
+        self._components = N
+        self.chain = None
+
+
+class Metropolis:
+    """Metropolis(model, proposal, rng, beta) -- driver.hpp:17-68."""
+
+    def __init__(self, model: _Model, proposal, rng: Pcg32, beta: float, hits: int = 1):
+        self.model, self.proposal, self.rng, self.beta, self.hits = model, proposal, rng, float(beta), hits
+        self.chain = model._chain(proposal, hits)
+
+    def _arm(self):
+        self.chain.set_proposal(self.proposal.kind, getattr(self.proposal, "width", 0.0), self.hits)
+        self.chain.set_seed(self.rng.key)
+
+    def sweep(self) -> None:
+        self._arm()
+        self.chain.metropolis(self.beta, 1, records=False)
+
+    def run(self, sweeps: int) -> None:
+        self._arm()
+        self.chain.metropolis(self.beta, sweeps, records=False)
+
+    def sample(self, sweeps: int, observe=None) -> np.ndarray:
+        """Runs n sweeps; returns the per-sweep observable records and, if an
+        observe callback is given, calls it once per sweep with the record."""
+        self._arm()
+        rec = self.chain.metropolis(self.beta, sweeps, records=True)
+        if observe is not None:
+            for r in rec:
+                observe(r)
+        return rec
+
+
+class Wolff:
+    """Wolff(model, axis, rng, beta) -- driver.hpp:92-210."""
+
+    def __init__(self, model: _Model, axis, rng: Pcg32, beta: float):
+        self.model, self.axis, self.rng, self.beta = model, axis, rng, float(beta)
+        self.chain = model._chain()
+
+    def _arm(self):
+        self.chain.set_wolff_axis(self.axis.axis)
+        self.chain.set_seed(self.rng.key)
+
+    def flip(self) -> int:
+        self._arm()
+        sizes, _ = self.chain.wolff(self.beta, 1, records=False)
+        return int(sizes[0])
+
+    def sweep(self) -> None:
+        self._arm()
+        touched, n = 0, self.chain.n
+        while touched < n:
+            sizes, _ = self.chain.wolff(self.beta, 1, records=False)
+            touched += int(sizes[0])
+
+    def run(self, sweeps: int) -> None:
+        for _ in range(sweeps):
+            self.sweep()
+
+    def sample(self, flips: int, observe=None):
+        self._arm()
+        sizes, rec = self.chain.wolff(self.beta, flips, records=True)
+        if observe is not None:
+            for r in rec:
+                observe(r)
+        return sizes, rec
+
+    def mean_cluster_size(self) -> float:
+        f, s = self.chain.wolff_stats()
+        return 0.0 if f == 0 else s / f

@@ -1,0 +1,851 @@
+// umc_chain.cu -- device chains: creation, field transfer, the Metropolis /
+// Wolff schedules, observable records, and the chain part of the C ABI.
+//
+// A Metropolis sweep (driver.hpp:29-43) is one kernel per colour class; the
+// last block of the last class folds the sweep's observables into a record.
+// A Wolff flip (driver.hpp:104-162) is a bond-activation + union-find kernel
+// followed by a flip kernel.  All launches go to the chain's stream; the
+// blocking entry points synchronise once at the end and read the device
+// status word, so bounded device-side waits surface as UMC_ERR_DEVICE_TIMEOUT.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <new>
+
+#include "umc_chain.hpp"
+#include "umc_gauge.hpp"
+#include "umc_spin_kernels.cuh"
+
+namespace umc {
+
+void cuda_check(cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) return;
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) throw Error(UMC_ERR_OUT_OF_MEMORY, m);
+    throw Error(UMC_ERR_CUDA, m);
+}
+
+void DevBuf::alloc(size_t b, const char* what)
+{
+    free_();
+    if (b == 0) b = 16;
+    cuda_check(cudaMalloc(&p, b), what);
+    bytes = b;
+}
+
+void DevBuf::free_()
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+std::vector<uint32_t> ising_metropolis_thresholds(int32_t J, double beta, uint32_t D)
+{
+    std::vector<uint32_t> t(2 * size_t(D) + 1);
+    for (int64_t m = -int64_t(D); m <= int64_t(D); ++m) {
+        const int32_t dEi = int32_t(2 * int64_t(J) * m);
+        const double dE = double(dEi);
+        const double log_p = -beta * dE + 0.0;
+        uint32_t tm1;
+        if (log_p >= 0.0) {
+            tm1 = 0xFFFFFFFFu;
+        } else {
+            // largest k with log(k 2^-32) < log_p; k = 0 always qualifies
+            uint64_t lo = 0, hi = uint64_t(1) << 32;
+            while (hi - lo > 1) {
+                const uint64_t mid = (lo + hi) / 2;
+                if (std::log(double(mid) * 0x1.0p-32) < log_p) lo = mid;
+                else hi = mid;
+            }
+            tm1 = uint32_t(lo);
+        }
+        t[size_t(m + D)] = tm1;
+    }
+    return t;
+}
+
+void ising_wolff_thresholds(int32_t J, double beta, unsigned long long cw[2])
+{
+    for (int b = 0; b < 2; ++b) {
+        const int32_t ss = b ? 1 : -1;
+        const int32_t dEi = -J * ((-ss) - ss);  // energy_diff_bond with nb = -s_j
+        const double p = 1.0 - std::exp(-beta * double(dEi));
+        if (!(p > 0.0)) {
+            cw[b] = 0;
+            continue;
+        }
+        uint64_t lo = 0, hi = uint64_t(1) << 32;  // k = 0 qualifies since 0 < p
+        while (hi - lo > 1) {
+            const uint64_t mid = (lo + hi) / 2;
+            if (double(uint32_t(mid)) * 0x1.0p-32 < p) lo = mid;
+            else hi = mid;
+        }
+        cw[b] = lo + 1;
+    }
+}
+
+namespace {
+
+uint32_t grid_for(const umc_chain* c, uint64_t work)
+{
+    const uint64_t b = (work + kBlock - 1) / kBlock;
+    return uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(b, c->max_grid)));
+}
+
+void device_scope(const umc_chain* c) { cuda_check(cudaSetDevice(c->device), "cudaSetDevice"); }
+
+void launch_check(const char* what) { cuda_check(cudaGetLastError(), what); }
+
+template <class T>
+void upload(DevBuf& b, const std::vector<T>& v, cudaStream_t s, const char* what)
+{
+    b.alloc(v.size() * sizeof(T), what);
+    if (!v.empty()) cuda_check(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), what);
+}
+
+Placement placement(const umc_chain* c)
+{
+    Placement pl{};
+    if (c->stencil) {
+        pl.position = nullptr;
+        pl.Lx = uint32_t(c->dims[0]);
+        pl.Ly = uint32_t(c->dims[1]);
+        pl.half = uint32_t(c->n / 2);
+    } else {
+        pl.position = c->position.as<uint32_t>();
+        pl.Lx = pl.Ly = 1;
+        pl.half = 0;
+    }
+    return pl;
+}
+
+bool is_spin(const umc_chain* c)
+{
+    return c->model == UMC_MODEL_ISING || c->model == UMC_MODEL_VECTOR || c->model == UMC_MODEL_XY_ANGLE;
+}
+
+void ensure_csr(umc_chain* c)
+{
+    if (c->off.p) return;
+    upload(c->off, c->h_off, c->stream, "upload CSR offsets");
+    upload(c->adj, c->h_adj, c->stream, "upload CSR bonds");
+    upload(c->slot, c->h_slot, c->stream, "upload CSR edge ids");
+}
+
+void ensure_labels(umc_chain* c)
+{
+    if (c->lab0.p) return;
+    c->lab0.alloc(c->n * 4, "Wolff labels");
+    c->lab1.alloc(c->n * 4, "Wolff labels");
+    const uint32_t g = grid_for(c, c->n);
+    iota_u32<<<g, kBlock, 0, c->stream>>>(c->lab0.as<uint32_t>(), uint32_t(c->n));
+    iota_u32<<<g, kBlock, 0, c->stream>>>(c->lab1.as<uint32_t>(), uint32_t(c->n));
+    launch_check("iota labels");
+}
+
+// Next free record slot on the device (records are fetched in order).
+uint64_t next_record(umc_chain* c)
+{
+    if (c->rec_pending >= c->max_records) c->rec_overflow = true;
+    return (c->rec_pending++) % c->max_records;
+}
+
+double* record_ptr(umc_chain* c, uint64_t r) { return c->records.as<double>() + r * kObs; }
+unsigned long long* size_ptr(umc_chain* c, uint64_t r) { return c->sizes.as<unsigned long long>() + r; }
+
+template <class Topo>
+void launch_ising_generic(umc_chain* c, IsingArgs a, Topo t)
+{
+    const size_t smem = (2 * size_t(a.D) + 1) * sizeof(uint32_t);
+    ising_pass<Topo><<<grid_for(c, a.count), kBlock, smem, c->stream>>>(a, t);
+}
+
+template <int N, class Topo>
+void launch_vector(umc_chain* c, const VecArgs& a, Topo t)
+{
+    const uint32_t g = grid_for(c, a.count);
+    if (c->desc.proposal == UMC_PROPOSAL_ROTATION) vector_pass<N, kPropRotation, Topo><<<g, kBlock, 0, c->stream>>>(a, t);
+    else vector_pass<N, kPropSphere, Topo><<<g, kBlock, 0, c->stream>>>(a, t);
+}
+
+template <class Topo>
+void launch_vector_n(umc_chain* c, const VecArgs& a, Topo t)
+{
+    switch (c->N) {
+    case 1: launch_vector<1>(c, a, t); break;
+    case 2: launch_vector<2>(c, a, t); break;
+    case 3: launch_vector<3>(c, a, t); break;
+    case 4: launch_vector<4>(c, a, t); break;
+    default: throw Error(UMC_ERR_UNSUPPORTED, "VectorSpin<N>: N must be 1..4");
+    }
+}
+
+template <class Topo>
+void spin_pass(umc_chain* c, uint32_t p, double beta, uint64_t kbase, const PassOut& o, Topo t)
+{
+    const uint32_t first = uint32_t(c->class_start[p]);
+    const uint32_t count = uint32_t(c->class_start[p + 1] - c->class_start[p]);
+    if (c->model == UMC_MODEL_ISING) {
+        IsingArgs a{c->field.as<int8_t>(), first, count, kbase, c->tm1.as<uint32_t>(), c->max_degree, c->J_int, o};
+        launch_ising_generic(c, a, t);
+    } else if (c->model == UMC_MODEL_VECTOR) {
+        VecArgs a{c->field.as<float>(), uint32_t(c->n), first, count, kbase, c->J, float(beta), float(c->desc.width), o};
+        launch_vector_n(c, a, t);
+    } else {
+        XYArgs a{c->field.as<float>(), first, count, kbase, c->J, float(beta), float(c->desc.width), o};
+        xy_pass<Topo><<<grid_for(c, count), kBlock, 0, c->stream>>>(a, t);
+    }
+}
+
+void ensure_ising_tables(umc_chain* c, double beta)
+{
+    if (c->model != UMC_MODEL_ISING) return;
+    if (c->tm1_valid && c->tm1_beta == beta) return;
+    c->h_tm1 = ising_metropolis_thresholds(c->J_int, beta, c->max_degree);
+    if (!c->tm1.p || c->tm1.bytes < c->h_tm1.size() * 4) c->tm1.alloc(c->h_tm1.size() * 4, "Ising thresholds");
+    cuda_check(cudaMemcpyAsync(c->tm1.p, c->h_tm1.data(), c->h_tm1.size() * 4, cudaMemcpyHostToDevice, c->stream),
+               "upload Ising thresholds");
+    // the pageable source must stay alive until the copy ran
+    cuda_check(cudaStreamSynchronize(c->stream), "upload Ising thresholds");
+    c->tm1_beta = beta;
+    c->tm1_valid = true;
+}
+
+void observe_into(umc_chain* c, double* rec, unsigned long long* size_slot)
+{
+    ensure_csr(c);
+    const PassOut o{c->ctl.as<DevCtl>(), c->partials.as<double>(), rec, nullptr, kMaxPasses - 1, 1, 1};
+    const uint32_t g = grid_for(c, c->n);
+    switch (c->model) {
+    case UMC_MODEL_ISING:
+        observe_csr<0><<<g, kBlock, 0, c->stream>>>(c->field.p, uint32_t(c->n), c->off.as<uint32_t>(), c->adj.as<uint32_t>(), c->J, o, size_slot);
+        break;
+    case UMC_MODEL_XY_ANGLE:
+        observe_csr<-1><<<g, kBlock, 0, c->stream>>>(c->field.p, uint32_t(c->n), c->off.as<uint32_t>(), c->adj.as<uint32_t>(), c->J, o, size_slot);
+        break;
+    case UMC_MODEL_VECTOR:
+        switch (c->N) {
+        case 1: observe_csr<1><<<g, kBlock, 0, c->stream>>>(c->field.p, uint32_t(c->n), c->off.as<uint32_t>(), c->adj.as<uint32_t>(), c->J, o, size_slot); break;
+        case 2: observe_csr<2><<<g, kBlock, 0, c->stream>>>(c->field.p, uint32_t(c->n), c->off.as<uint32_t>(), c->adj.as<uint32_t>(), c->J, o, size_slot); break;
+        case 3: observe_csr<3><<<g, kBlock, 0, c->stream>>>(c->field.p, uint32_t(c->n), c->off.as<uint32_t>(), c->adj.as<uint32_t>(), c->J, o, size_slot); break;
+        case 4: observe_csr<4><<<g, kBlock, 0, c->stream>>>(c->field.p, uint32_t(c->n), c->off.as<uint32_t>(), c->adj.as<uint32_t>(), c->J, o, size_slot); break;
+        }
+        break;
+    }
+    launch_check("observe");
+}
+
+// One Metropolis sweep of a spin model: one kernel per colour class.
+void spin_sweep(umc_chain* c, double beta, double* rec)
+{
+    ensure_ising_tables(c, beta);
+    const uint64_t kbase = key_base(key_seed(c->desc.seed, c->sweeps, tag_site(0)));
+    const bool fused = c->symmetric;
+    for (uint32_t p = 0; p < c->n_colours; ++p) {
+        const bool last = p + 1 == c->n_colours;
+        const PassOut o{c->ctl.as<DevCtl>(), c->partials.as<double>(), fused ? rec : nullptr, nullptr,
+                        int(p), int(c->n_colours), last ? 1 : 0};
+        if (c->packed_ising) {
+            IsingPackedArgs a{};
+            a.spins = c->field.as<int8_t>();
+            a.H = uint32_t(c->dims[0] / 2);
+            a.Ly = uint32_t(c->dims[1]);
+            a.half = uint32_t(c->n / 2);
+            a.colour = p;
+            a.kbase = kbase;
+            for (int t = 0; t < 5; ++t) a.tm1[t] = c->h_tm1[size_t(int(c->max_degree) + 2 * t - 4)];
+            a.J = c->J_int;
+            a.out = o;
+            const uint32_t g = grid_for(c, c->n / 2 / 16);
+            ising_packed_pass<<<g, kBlock, 0, c->stream>>>(a);
+        } else if (c->stencil) {
+            StencilTopo t{uint32_t(c->dims[0] / 2), uint32_t(c->dims[1]), uint32_t(c->dims[2]), uint32_t(c->n / 2), p,
+                          c->dims[1] > 1 ? 1u : 0u, c->dims[2] > 1 ? 1u : 0u};
+            spin_pass(c, p, beta, kbase, o, t);
+        } else {
+            CsrTopo t{c->off.as<uint32_t>(), c->adj.as<uint32_t>(), uint32_t(c->class_start[p])};
+            spin_pass(c, p, beta, kbase, o, t);
+        }
+        launch_check("Metropolis colour pass");
+    }
+    if (!fused && rec) observe_into(c, rec, nullptr);
+    c->sweeps++;
+}
+
+// One Wolff flip of a spin model.
+void spin_flip(umc_chain* c, double beta, double* rec, unsigned long long* size_slot)
+{
+    if (c->model == UMC_MODEL_XY_ANGLE || c->desc.wolff_axis == UMC_AXIS_NONE)
+        throw Error(UMC_ERR_UNSUPPORTED, "Wolff needs a reflection axis (FixedAxis for Ising, UniformSphereN for VectorSpin)");
+    if (!c->symmetric) throw Error(UMC_ERR_UNSUPPORTED, "Wolff needs a symmetric graph");
+    ensure_csr(c);
+    ensure_labels(c);
+    WolffArgs a{};
+    a.field = c->field.p;
+    a.n = uint32_t(c->n);
+    a.off = c->off.as<uint32_t>();
+    a.adj = c->adj.as<uint32_t>();
+    a.slot = c->slot.as<uint32_t>();
+    // labels of this flip (identity on entry) and of the next one (reset here)
+    uint32_t* cur = (c->lab_cur ? c->lab1 : c->lab0).as<uint32_t>();
+    uint32_t* nxt = (c->lab_cur ? c->lab0 : c->lab1).as<uint32_t>();
+    a.lab = cur;
+    a.lab_next = nxt;
+    a.seed = c->desc.seed;
+    a.flip = c->flips;
+    a.J = c->J;
+    a.beta = float(beta);
+    if (c->model == UMC_MODEL_ISING) {
+        if (!c->cw_valid || c->cw_beta != beta) {
+            ising_wolff_thresholds(c->J_int, beta, c->cw);
+            c->cw_beta = beta;
+            c->cw_valid = true;
+        }
+        a.cw[0] = c->cw[0];
+        a.cw[1] = c->cw[1];
+    }
+    a.ctl = c->ctl.as<DevCtl>();
+    a.size_slot = size_slot;
+    const uint32_t g = grid_for(c, c->n);
+    if (c->model == UMC_MODEL_ISING) {
+        wolff_union<0><<<g, kBlock, 0, c->stream>>>(a);
+        wolff_flip<0><<<g, kBlock, 0, c->stream>>>(a);
+    } else {
+        switch (c->N) {
+        case 1: wolff_union<1><<<g, kBlock, 0, c->stream>>>(a); wolff_flip<1><<<g, kBlock, 0, c->stream>>>(a); break;
+        case 2: wolff_union<2><<<g, kBlock, 0, c->stream>>>(a); wolff_flip<2><<<g, kBlock, 0, c->stream>>>(a); break;
+        case 3: wolff_union<3><<<g, kBlock, 0, c->stream>>>(a); wolff_flip<3><<<g, kBlock, 0, c->stream>>>(a); break;
+        case 4: wolff_union<4><<<g, kBlock, 0, c->stream>>>(a); wolff_flip<4><<<g, kBlock, 0, c->stream>>>(a); break;
+        }
+    }
+    launch_check("Wolff flip");
+    c->lab_cur ^= 1;
+    if (rec) observe_into(c, rec, size_slot);
+    c->flips++;
+}
+
+void check_status(umc_chain* c)
+{
+    unsigned int st = 0;
+    cuda_check(cudaMemcpyAsync(&st, &c->ctl.as<DevCtl>()->status, sizeof st, cudaMemcpyDeviceToHost, c->stream), "read status");
+    cuda_check(cudaStreamSynchronize(c->stream), "synchronise chain");
+    if (st) {
+        const unsigned int zero = 0;
+        cuda_check(cudaMemcpy(&c->ctl.as<DevCtl>()->status, &zero, sizeof zero, cudaMemcpyHostToDevice), "clear status");
+        std::string m = "device-side bound exhausted:";
+        if (st & kDevErrUnionFind) m += " union-find";
+        if (st & kDevErrGeometry) m += " geometry";
+        if (st & kDevErrRetry) m += " proposal-retry";
+        throw Error(UMC_ERR_DEVICE_TIMEOUT, m);
+    }
+}
+
+void fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t capacity, uint64_t* n_out)
+{
+    check_status(c);
+    if (c->rec_overflow) {
+        c->rec_overflow = false;
+        c->rec_pending = 0;
+        throw Error(UMC_ERR_STATE, "observable records overflowed the device ring; fetch more often or raise max_records");
+    }
+    const uint64_t n = c->rec_pending;
+    if ((records || sizes) && n > capacity) throw Error(UMC_ERR_INVALID_ARGUMENT, "record buffer too small");
+    if (records && n)
+        cuda_check(cudaMemcpy(records, c->records.p, n * kObs * sizeof(double), cudaMemcpyDeviceToHost), "fetch records");
+    std::vector<unsigned long long> s(n);
+    if (n) cuda_check(cudaMemcpy(s.data(), c->sizes.p, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "fetch sizes");
+    if (sizes)
+        for (uint64_t k = 0; k < n; ++k) sizes[k] = s[k];
+    if (n_out) *n_out = n;
+    c->rec_pending = 0;
+}
+
+// --------------------------------------------------------------- creation
+
+// Which proposal / axis a model accepts (the reference enforces this through
+// the Proposal concept's value type, dof/proposal.hpp:8-12).
+void validate_proposal(umc_chain* c, int32_t proposal, double width, uint32_t hits)
+{
+    if (!std::isfinite(width)) throw Error(UMC_ERR_INVALID_ARGUMENT, "proposal width must be finite");
+    if (hits == 0 || hits > 0xFF00) throw Error(UMC_ERR_INVALID_ARGUMENT, "hits must be in [1, 65280]");
+    switch (c->model) {
+    case UMC_MODEL_ISING:
+        if (proposal != 0 && proposal != UMC_PROPOSAL_FLIP) throw Error(UMC_ERR_UNSUPPORTED, "Ising takes the Flip proposal");
+        break;
+    case UMC_MODEL_VECTOR:
+        if (c->N < 1 || c->N > 4) throw Error(UMC_ERR_UNSUPPORTED, "VectorSpin<N>: N must be 1..4");
+        if (proposal != UMC_PROPOSAL_SPHERE && proposal != UMC_PROPOSAL_ROTATION)
+            throw Error(UMC_ERR_UNSUPPORTED, "VectorSpin takes UniformSphereN or LocalRotation");
+        if (proposal == UMC_PROPOSAL_ROTATION && c->N < 2) throw Error(UMC_ERR_UNSUPPORTED, "LocalRotation needs N >= 2");
+        break;
+    case UMC_MODEL_XY_ANGLE:
+    case UMC_MODEL_U1:
+        if (proposal != UMC_PROPOSAL_U1SHIFT) throw Error(UMC_ERR_UNSUPPORTED, "angle models take U1Shift");
+        break;
+    case UMC_MODEL_SU:
+        if (proposal != UMC_PROPOSAL_SUSHIFT) throw Error(UMC_ERR_UNSUPPORTED, "SU(N) takes SUShift");
+        break;
+    }
+    if (hits != 1 && c->model != UMC_MODEL_U1 && c->model != UMC_MODEL_SU)
+        throw Error(UMC_ERR_UNSUPPORTED, "multi-hit is provided for the gauge models");
+}
+
+void validate_axis(umc_chain* c, int32_t axis)
+{
+    if (axis == UMC_AXIS_NONE) return;
+    if (c->model == UMC_MODEL_ISING && axis == UMC_AXIS_FIXED) return;
+    if (c->model == UMC_MODEL_VECTOR && axis == UMC_AXIS_SPHERE) return;
+    throw Error(UMC_ERR_UNSUPPORTED, "Wolff axis: FixedAxis for Ising, UniformSphereN for VectorSpin");
+}
+
+void create_chain(const umc_chain_desc* d, umc_chain* c)
+{
+    if (!d) throw Error(UMC_ERR_INVALID_ARGUMENT, "null descriptor");
+    c->desc = *d;
+    c->model = d->model;
+    c->N = d->components <= 0 ? 1 : d->components;
+    c->device = d->device;
+    c->max_records = d->max_records ? d->max_records : 4096;
+    if (c->desc.hits == 0) c->desc.hits = 1;
+    if (c->desc.proposal == 0 && c->model == UMC_MODEL_ISING) c->desc.proposal = UMC_PROPOSAL_FLIP;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        throw Error(UMC_ERR_CUDA, "no CUDA device available");
+    }
+    if (c->device < 0 || c->device >= count) throw Error(UMC_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    cuda_check(cudaSetDevice(c->device), "cudaSetDevice");
+    int sms = 0;
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device), "SM count");
+    c->max_grid = uint32_t(sms) * 8;
+
+    if (is_spin(c)) {
+        const umc_graph* g = d->graph;
+        if (!g) throw Error(UMC_ERR_INVALID_ARGUMENT, "spin models need a graph");
+        c->n = g->n;
+        c->symmetric = g->symmetric;
+        c->n_colours = g->col.n_colours;
+        c->class_start = g->col.class_start;
+        c->stencil = g->stencil;
+        std::memcpy(c->dims, g->dims, sizeof c->dims);
+        c->max_degree = g->max_degree;
+        c->h_off = g->c_offset;
+        c->h_adj = g->c_bonds;
+        c->h_slot = g->c_slot_edge;
+        c->h_position = g->col.position;
+        if (c->n_colours > uint32_t(kMaxPasses - 1))
+            throw Error(UMC_ERR_UNSUPPORTED, "graph needs more colour classes than the engine supports (63)");
+        validate_proposal(c, c->desc.proposal, c->desc.width, c->desc.hits);
+        validate_axis(c, c->desc.wolff_axis);
+        if (c->model == UMC_MODEL_ISING) {
+            if (d->coupling != std::floor(d->coupling) || std::fabs(d->coupling) > 1e6)
+                throw Error(UMC_ERR_INVALID_ARGUMENT, "Ising coupling J must be an integer (example/ising.hpp:18)");
+            if (c->max_degree > 4096) throw Error(UMC_ERR_UNSUPPORTED, "Ising degree above 4096");
+            c->J_int = int32_t(d->coupling);
+            c->J = float(c->J_int);
+            c->elem_bytes = 1;
+            c->comps = 1;
+            c->packed_ising = c->stencil && c->dims[2] == 1 && c->dims[1] >= 2 && (c->dims[0] / 2) % 16 == 0;
+        } else if (c->model == UMC_MODEL_VECTOR) {
+            c->J = float(d->coupling);
+            c->elem_bytes = 4;
+            c->comps = uint32_t(c->N);
+        } else {
+            c->J = float(d->coupling);
+            c->elem_bytes = 4;
+            c->comps = 1;
+        }
+    } else if (c->model == UMC_MODEL_U1 || c->model == UMC_MODEL_SU) {
+        gauge_configure(c);
+    } else {
+        throw Error(UMC_ERR_INVALID_ARGUMENT, "unknown model");
+    }
+    if (c->n > 0xFFFFFFFFull) throw Error(UMC_ERR_OVERFLOW, "site count exceeds uint32_t");
+
+    if (d->stream) {
+        c->stream = static_cast<cudaStream_t>(d->stream);
+    } else {
+        cuda_check(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        c->own_stream = true;
+    }
+    c->field_bytes = size_t(c->n) * c->comps * c->elem_bytes;
+    c->field.alloc(c->field_bytes, "field");
+    c->partials.alloc(size_t(c->max_grid) * kObs * sizeof(double), "partials");
+    c->ctl.alloc(sizeof(DevCtl), "control block");
+    cuda_check(cudaMemsetAsync(c->ctl.p, 0, sizeof(DevCtl), c->stream), "clear control block");
+    c->records.alloc(c->max_records * kObs * sizeof(double), "records");
+    c->sizes.alloc(c->max_records * sizeof(unsigned long long), "cluster sizes");
+    cuda_check(cudaMemsetAsync(c->sizes.p, 0, c->max_records * sizeof(unsigned long long), c->stream), "clear sizes");
+    if (!c->stencil && is_spin(c)) upload(c->position, c->h_position, c->stream, "upload positions");
+    if (!c->stencil && is_spin(c)) ensure_csr(c);
+
+    // cold start, as the reference constructors do
+    if (c->model == UMC_MODEL_ISING) {
+        cuda_check(cudaMemsetAsync(c->field.p, 1, c->field_bytes, c->stream), "cold start");
+    } else if (c->model == UMC_MODEL_VECTOR) {
+        cuda_check(cudaMemsetAsync(c->field.p, 0, c->field_bytes, c->stream), "cold start");
+        std::vector<float> ones(c->n, 1.0f);
+        cuda_check(cudaMemcpyAsync(c->field.as<float>() + (c->N - 1) * c->n, ones.data(), c->n * 4, cudaMemcpyHostToDevice, c->stream),
+                   "cold start");
+        cuda_check(cudaStreamSynchronize(c->stream), "cold start");
+    } else if (c->model == UMC_MODEL_XY_ANGLE) {
+        cuda_check(cudaMemsetAsync(c->field.p, 0, c->field_bytes, c->stream), "cold start");
+    } else {
+        gauge_cold_start(c);
+    }
+    cuda_check(cudaStreamSynchronize(c->stream), "chain creation");
+}
+
+void destroy_chain(umc_chain* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    gauge_release(c);
+    for (DevBuf* b : {&c->field, &c->staging, &c->off, &c->adj, &c->slot, &c->position, &c->lab0, &c->lab1, &c->cells,
+                      &c->inc_off, &c->inc_cell, &c->inc_which, &c->partials, &c->ctl, &c->records, &c->sizes, &c->tm1})
+        b->free_();
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+}
+
+template <class F>
+int guarded(F&& f)
+{
+    try {
+        set_last_error("");
+        f();
+        return UMC_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("out of host memory");
+        return UMC_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return UMC_ERR_INVALID_ARGUMENT;
+    }
+}
+
+void check_beta(double beta)
+{
+    if (!std::isfinite(beta)) throw Error(UMC_ERR_INVALID_ARGUMENT, "beta must be finite");
+}
+
+void enqueue_sweeps(umc_chain* c, double beta, uint64_t n)
+{
+    check_beta(beta);
+    for (uint64_t k = 0; k < n; ++k) {
+        const uint64_t r = next_record(c);
+        if (is_spin(c)) spin_sweep(c, beta, record_ptr(c, r));
+        else gauge_sweep(c, beta, record_ptr(c, r));
+    }
+}
+
+void enqueue_flips(umc_chain* c, double beta, uint64_t n, bool obs)
+{
+    check_beta(beta);
+    if (!is_spin(c)) throw Error(UMC_ERR_UNSUPPORTED, "Wolff is defined for spin models only (driver.hpp:73-84)");
+    for (uint64_t k = 0; k < n; ++k) {
+        const uint64_t r = next_record(c);
+        spin_flip(c, beta, obs ? record_ptr(c, r) : nullptr, size_ptr(c, r));
+    }
+}
+
+void enqueue_hybrid(umc_chain* c, double beta, uint64_t n)
+{
+    check_beta(beta);
+    if (!is_spin(c)) throw Error(UMC_ERR_UNSUPPORTED, "Wolff is defined for spin models only (driver.hpp:73-84)");
+    for (uint64_t k = 0; k < n; ++k) {
+        const uint64_t r = next_record(c);
+        spin_flip(c, beta, nullptr, size_ptr(c, r));
+        spin_sweep(c, beta, record_ptr(c, r));
+    }
+}
+
+// Runs n units in chunks that fit the record ring, copying records out.
+template <class Enq>
+void run_chunked(umc_chain* c, uint64_t n, double* records, uint64_t* sizes, bool count_flips, Enq&& enq)
+{
+    if (c->rec_pending) fetch(c, nullptr, nullptr, 0, nullptr);  // drop stale records
+    uint64_t done = 0;
+    while (done < n) {
+        const uint64_t m = std::min<uint64_t>(n - done, c->max_records);
+        enq(m);
+        std::vector<uint64_t> sz(m);
+        uint64_t got = 0;
+        fetch(c, records ? records + done * kObs : nullptr, sz.data(), m, &got);
+        if (sizes) std::copy(sz.begin(), sz.end(), sizes + done);
+        if (count_flips)
+            for (uint64_t s : sz) {
+                c->wolff_flips_done++;
+                c->wolff_size_sum += double(s);
+            }
+        done += m;
+    }
+}
+
+}  // namespace
+}  // namespace umc
+
+using namespace umc;
+
+extern "C" {
+
+int umc_device_count(int* count)
+{
+    return guarded([&] {
+        if (!count) throw Error(UMC_ERR_INVALID_ARGUMENT, "null count");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) {
+            cudaGetLastError();
+            n = 0;
+        }
+        *count = n;
+    });
+}
+
+int umc_chain_create(const umc_chain_desc* desc, umc_chain** out)
+{
+    return guarded([&] {
+        if (!out) throw Error(UMC_ERR_INVALID_ARGUMENT, "null output handle");
+        *out = nullptr;
+        auto* c = new umc_chain;
+        try {
+            create_chain(desc, c);
+        } catch (...) {
+            destroy_chain(c);
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+int umc_chain_destroy(umc_chain* c)
+{
+    return guarded([&] {
+        destroy_chain(c);
+        delete c;
+    });
+}
+
+int umc_chain_set_field(umc_chain* c, const void* host_field)
+{
+    return guarded([&] {
+        if (!c || !host_field) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        device_scope(c);
+        if (!is_spin(c)) {
+            gauge_set_field(c, host_field);
+            return;
+        }
+        if (!c->staging.p) c->staging.alloc(c->field_bytes, "staging");
+        cuda_check(cudaMemcpyAsync(c->staging.p, host_field, c->field_bytes, cudaMemcpyHostToDevice, c->stream), "upload field");
+        const uint32_t g = grid_for(c, c->n);
+        if (c->elem_bytes == 1)
+            scatter_field<int8_t><<<g, kBlock, 0, c->stream>>>(c->staging.as<int8_t>(), c->field.as<int8_t>(), uint32_t(c->n), 1, placement(c));
+        else
+            scatter_field<float><<<g, kBlock, 0, c->stream>>>(c->staging.as<float>(), c->field.as<float>(), uint32_t(c->n), c->comps, placement(c));
+        launch_check("scatter field");
+        cuda_check(cudaStreamSynchronize(c->stream), "upload field");
+    });
+}
+
+int umc_chain_get_field(umc_chain* c, void* host_field)
+{
+    return guarded([&] {
+        if (!c || !host_field) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        device_scope(c);
+        if (!is_spin(c)) {
+            gauge_get_field(c, host_field);
+            return;
+        }
+        if (!c->staging.p) c->staging.alloc(c->field_bytes, "staging");
+        const uint32_t g = grid_for(c, c->n);
+        if (c->elem_bytes == 1)
+            gather_field<int8_t><<<g, kBlock, 0, c->stream>>>(c->field.as<int8_t>(), c->staging.as<int8_t>(), uint32_t(c->n), 1, placement(c));
+        else
+            gather_field<float><<<g, kBlock, 0, c->stream>>>(c->field.as<float>(), c->staging.as<float>(), uint32_t(c->n), c->comps, placement(c));
+        launch_check("gather field");
+        cuda_check(cudaMemcpyAsync(host_field, c->staging.p, c->field_bytes, cudaMemcpyDeviceToHost, c->stream), "download field");
+        cuda_check(cudaStreamSynchronize(c->stream), "download field");
+    });
+}
+
+int umc_chain_randomize(umc_chain* c, uint64_t seed)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        if (!is_spin(c)) {
+            gauge_randomize(c, seed);
+            return;
+        }
+        const uint32_t g = grid_for(c, c->n);
+        const uint32_t n = uint32_t(c->n);
+        if (c->model == UMC_MODEL_ISING) randomize_spins<0><<<g, kBlock, 0, c->stream>>>(c->field.p, n, seed, placement(c));
+        else if (c->model == UMC_MODEL_XY_ANGLE) randomize_spins<-1><<<g, kBlock, 0, c->stream>>>(c->field.p, n, seed, placement(c));
+        else
+            switch (c->N) {
+            case 1: randomize_spins<1><<<g, kBlock, 0, c->stream>>>(c->field.p, n, seed, placement(c)); break;
+            case 2: randomize_spins<2><<<g, kBlock, 0, c->stream>>>(c->field.p, n, seed, placement(c)); break;
+            case 3: randomize_spins<3><<<g, kBlock, 0, c->stream>>>(c->field.p, n, seed, placement(c)); break;
+            case 4: randomize_spins<4><<<g, kBlock, 0, c->stream>>>(c->field.p, n, seed, placement(c)); break;
+            }
+        launch_check("randomize");
+        cuda_check(cudaStreamSynchronize(c->stream), "randomize");
+    });
+}
+
+int umc_chain_set_proposal(umc_chain* c, int32_t proposal, double width, uint32_t hits)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        validate_proposal(c, proposal, width, hits);
+        c->desc.proposal = proposal;
+        c->desc.width = width;
+        c->desc.hits = hits;
+    });
+}
+
+int umc_chain_set_wolff_axis(umc_chain* c, int32_t axis)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        validate_axis(c, axis);
+        c->desc.wolff_axis = axis;
+    });
+}
+
+int umc_chain_set_seed(umc_chain* c, uint64_t seed)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        c->desc.seed = seed;
+    });
+}
+
+int umc_chain_counters(const umc_chain* c, uint64_t* sweeps, uint64_t* flips)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        if (sweeps) *sweeps = c->sweeps;
+        if (flips) *flips = c->flips;
+    });
+}
+
+int umc_chain_set_counters(umc_chain* c, uint64_t sweeps, uint64_t flips)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        c->sweeps = sweeps;
+        c->flips = flips;
+    });
+}
+
+void* umc_chain_stream(const umc_chain* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int umc_chain_sync(umc_chain* c)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        check_status(c);
+    });
+}
+
+int umc_chain_observe(umc_chain* c, double* record)
+{
+    return guarded([&] {
+        if (!c || !record) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        device_scope(c);
+        if (c->rec_pending) fetch(c, nullptr, nullptr, 0, nullptr);
+        const uint64_t r = next_record(c);
+        if (is_spin(c)) observe_into(c, record_ptr(c, r), nullptr);
+        else gauge_observe(c, record_ptr(c, r));
+        uint64_t got = 0;
+        std::vector<double> buf(kObs);
+        fetch(c, buf.data(), nullptr, 1, &got);
+        std::copy(buf.begin(), buf.end(), record);
+    });
+}
+
+int umc_metropolis_run(umc_chain* c, double beta, uint64_t n_sweeps, double* records)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        run_chunked(c, n_sweeps, records, nullptr, false, [&](uint64_t m) { enqueue_sweeps(c, beta, m); });
+    });
+}
+
+int umc_wolff_run(umc_chain* c, double beta, uint64_t n_flips, uint64_t* sizes, double* records)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        run_chunked(c, n_flips, records, sizes, true, [&](uint64_t m) { enqueue_flips(c, beta, m, records != nullptr); });
+    });
+}
+
+int umc_hybrid_run(umc_chain* c, double beta, uint64_t n_steps, uint64_t* sizes, double* records)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        run_chunked(c, n_steps, records, sizes, true, [&](uint64_t m) { enqueue_hybrid(c, beta, m); });
+    });
+}
+
+int umc_metropolis_enqueue(umc_chain* c, double beta, uint64_t n_sweeps)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        enqueue_sweeps(c, beta, n_sweeps);
+    });
+}
+
+int umc_wolff_enqueue(umc_chain* c, double beta, uint64_t n_flips)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        enqueue_flips(c, beta, n_flips, true);
+    });
+}
+
+int umc_hybrid_enqueue(umc_chain* c, double beta, uint64_t n_steps)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        enqueue_hybrid(c, beta, n_steps);
+    });
+}
+
+int umc_chain_fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t capacity, uint64_t* n_records)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        fetch(c, records, sizes, capacity, n_records);
+    });
+}
+
+int umc_wolff_stats(const umc_chain* c, uint64_t* flips, double* size_sum)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        if (flips) *flips = c->wolff_flips_done;
+        if (size_sum) *size_sum = c->wolff_size_sum;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+// umc_chain.hpp -- the device chain behind the C ABI's umc_chain handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "umc_device.cuh"
+#include "umc_tables.hpp"
+
+namespace umc {
+
+void cuda_check(cudaError_t e, const char* what);
+
+// Device buffer owned by a chain (freed on destruction).
+struct DevBuf
+{
+    void* p = nullptr;
+    size_t bytes = 0;
+    void alloc(size_t b, const char* what);
+    void free_();
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// Ising acceptance thresholds: accept iff draw <= tm1[s*h + D] where the
+// reference would accept iff log_p >= 0 || log(k 2^-32) < log_p with
+// log_p = -beta * (2 J s h) + 0.0 (driver.hpp:39-40, example/ising.hpp:46-56).
+std::vector<uint32_t> ising_metropolis_thresholds(int32_t J, double beta, uint32_t D);
+// Wolff-Ising: activate iff draw < cw[s_i s_j > 0] where the reference
+// activates iff k 2^-32 < 1 - exp(-beta * dE) (driver.hpp:151), dE = 2 J s_i s_j.
+void ising_wolff_thresholds(int32_t J, double beta, unsigned long long cw[2]);
+
+}  // namespace umc
+
+struct umc_chain
+{
+    umc_chain_desc desc{};
+    int model = 0;
+    int N = 1;               // components (VectorSpin<N>, SU(N))
+    uint64_t n = 0;          // sites or links
+    uint32_t n_colours = 0;
+    std::vector<uint64_t> class_start;
+    bool stencil = false;
+    uint64_t dims[3] = {1, 1, 1};
+    bool packed_ising = false;
+    bool symmetric = true;
+    uint32_t max_degree = 0;
+    int32_t J_int = 0;
+    float J = 1.0f;
+
+    // host copies kept for lazy uploads
+    std::vector<uint32_t> h_off, h_adj, h_slot, h_position;
+    // cell-complex models
+    uint64_t n_cells = 0;
+    uint32_t max_incident = 0;
+    uint32_t cell_dim = 0;
+    uint64_t L = 0;
+    std::vector<uint32_t> h_cells;
+    std::vector<uint64_t> h_inc_off;
+    std::vector<uint32_t> h_inc_cell;
+    std::vector<uint8_t> h_inc_which;
+
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    umc::DevBuf field, staging, off, adj, slot, position, lab0, lab1;
+    umc::DevBuf cells, inc_off, inc_cell, inc_which;
+    umc::DevBuf partials, ctl, records, sizes, tm1;
+    size_t field_bytes = 0;
+    size_t elem_bytes = 0;
+    uint32_t comps = 1;  // scalars per site in the host layout
+    uint32_t max_grid = 0;
+
+    uint64_t max_records = 4096;
+    uint64_t rec_pending = 0;
+    bool rec_overflow = false;
+    uint64_t sweeps = 0, flips = 0;
+    int lab_cur = 0;  // which Wolff label buffer is the identity
+    uint64_t wolff_flips_done = 0;
+    double wolff_size_sum = 0.0;
+
+    double tm1_beta = 0.0;
+    bool tm1_valid = false;
+    std::vector<uint32_t> h_tm1;
+    double cw_beta = 0.0;
+    bool cw_valid = false;
+    unsigned long long cw[2] = {0, 0};
+
+    // learned proposal (U(1) only)
+    void* learned = nullptr;
+};

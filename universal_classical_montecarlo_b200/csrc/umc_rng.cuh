@@ -1,0 +1,133 @@
+// umc_rng.cuh -- counter-keyed PCG32, identical on host and device.
+//
+// The reference draws every random number from one sequential Pcg32
+// (rng.hpp:8-44), and how many it draws depends on the data (the accept draw is
+// skipped when log_p >= 0, driver.hpp:40; Wolff draws once per tested bond,
+// driver.hpp:151).  A sequential stream cannot be replayed by thousands of
+// threads, so every update here opens its OWN reference-semantics Pcg32:
+//
+//     Pcg32(key_seed(seed, counter, tag), stream_id(id))
+//
+//     key_seed(s, c, t) = mix64(mix64(s ^ (t << 32)) + c * 0x9E3779B97F4A7C15)
+//     mix64            = splitmix64 finaliser (Steele, Lea & Flood, 2014)
+//     stream_id(id)    = lowbias32(id), a bijection on 32 bits (Wellons, 2018)
+//
+// and consumes its draws in the same order the reference driver would.  The
+// constructor (rng.hpp:14-20) leaves state = (inc + s) * A + inc with
+// inc = 2 * stream + 1, so the first state of a key is affine in stream_id:
+//     state0 = C0 + stream_id * C1,  C0 = (s + 1) * A + 1,  C1 = 2 * A + 2,
+// which costs two integer multiply-adds per site once C0 is known per sweep.
+#pragma once
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define UMC_HD __host__ __device__ __forceinline__
+#else
+#define UMC_HD inline
+#endif
+
+namespace umc {
+
+constexpr uint64_t kPcgMult = 6364136223846793005ULL;  // rng.hpp:34
+constexpr uint64_t kGolden = 0x9E3779B97F4A7C15ULL;
+constexpr uint64_t kStreamStep = 2ULL * kPcgMult + 2ULL;  // C1
+
+// Key tags: which kind of update a key belongs to.
+constexpr uint32_t kTagBond = 1;   // Wolff bond activation, id = edge index
+constexpr uint32_t kTagAxis = 2;   // Wolff axis + seed draw, id = 0
+constexpr uint32_t kTagInit = 3;   // random start, id = site
+constexpr uint32_t kTagSwap = 4;   // replica exchange, id = ladder slot
+constexpr uint32_t kTagLearn = 5;  // learned-proposal training minibatch
+UMC_HD constexpr uint32_t tag_site(uint32_t hit) { return 0x100u + hit; }  // Metropolis hit
+
+UMC_HD uint64_t mix64(uint64_t z)
+{
+    z ^= z >> 30;
+    z *= 0xBF58476D1CE4E5B9ULL;
+    z ^= z >> 27;
+    z *= 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    return z;
+}
+
+UMC_HD uint64_t key_seed(uint64_t seed, uint64_t counter, uint32_t tag)
+{
+    return mix64(mix64(seed ^ (uint64_t(tag) << 32)) + counter * kGolden);
+}
+
+UMC_HD uint32_t stream_id(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x;
+}
+
+// C0 for a given key seed: state0(id) = c0 + stream_id(id) * kStreamStep.
+UMC_HD uint64_t key_base(uint64_t kseed) { return (kseed + 1ULL) * kPcgMult + 1ULL; }
+
+// XSH-RR output of a state (rng.hpp:36-39).
+UMC_HD uint32_t pcg_output(uint64_t old)
+{
+#if defined(__CUDA_ARCH__)
+    const uint32_t lo = uint32_t(old), hi = uint32_t(old >> 32);
+    // x = old ^ (old >> 18) restricted to the bits the output uses
+    const uint32_t xlo = lo ^ __funnelshift_r(lo, hi, 18);
+    const uint32_t xhi = hi ^ (hi >> 18);
+    const uint32_t xs = __funnelshift_r(xlo, xhi, 27);
+    const uint32_t rot = hi >> 27;
+    return __funnelshift_r(xs, xs, rot);
+#else
+    const uint32_t xs = uint32_t(((old >> 18u) ^ old) >> 27u);
+    const uint32_t rot = uint32_t(old >> 59u);
+    return (xs >> rot) | (xs << ((32u - rot) & 31u));
+#endif
+}
+
+// One keyed stream: the reference Pcg32 after construction.
+struct KeyedPcg
+{
+    uint64_t state;
+    uint64_t inc;
+
+    UMC_HD static KeyedPcg open(uint64_t kbase, uint32_t id)
+    {
+        const uint32_t h = stream_id(id);
+        KeyedPcg g;
+        g.state = kbase + uint64_t(h) * kStreamStep;
+        g.inc = (uint64_t(h) << 1) | 1ULL;
+        return g;
+    }
+    UMC_HD static KeyedPcg open_key(uint64_t seed, uint64_t counter, uint32_t tag, uint32_t id)
+    {
+        return open(key_base(key_seed(seed, counter, tag)), id);
+    }
+    // Pcg32::next (rng.hpp:31-40)
+    UMC_HD uint32_t next()
+    {
+        const uint64_t old = state;
+        state = old * kPcgMult + inc;
+        return pcg_output(old);
+    }
+};
+
+// First draw of a key without materialising the stream (one draw per site).
+UMC_HD uint32_t first_draw(uint64_t kbase, uint32_t id)
+{
+    return pcg_output(kbase + uint64_t(stream_id(id)) * kStreamStep);
+}
+
+// ---- conversions of a 32-bit draw k (the reference uses u = k * 2^-32) ----
+// u in FP64, exactly the reference's value.
+UMC_HD double u_f64(uint32_t k) { return double(k) * 0x1.0p-32; }
+// 2u - 1 in FP32 with a single rounding: 2k - 2^32 = 2 (k - 2^31).
+UMC_HD float sym_f32(uint32_t k) { return float(int32_t(k ^ 0x80000000u)) * 0x1.0p-31f; }
+// 2u in FP32 (argument of sincospif for an angle 2 pi u).
+UMC_HD float twice_u_f32(uint32_t k) { return float(k) * 0x1.0p-31f; }
+// u in FP32.
+UMC_HD float u_f32(uint32_t k) { return float(k) * 0x1.0p-32f; }
+
+}  // namespace umc
