@@ -204,6 +204,22 @@ int umc_hybrid_enqueue(umc_chain* c, double beta, uint64_t n_steps);
  * receives their count; records / sizes may be NULL.  Synchronises. */
 int umc_chain_fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t capacity,
                     uint64_t* n_records);
+/* Kernel accounting (no reference counterpart).  Every kernel the chain
+ * launches is counted by kind; with timing enabled each launch is also
+ * bracketed by CUDA events on the chain's stream.  umc_chain_kernel_stats
+ * synchronises and reports, per kind, launches and device milliseconds
+ * (timed launches only); reset != 0 clears both. */
+#define UMC_KERNEL_METROPOLIS 0 /* spin-model colour pass           */
+#define UMC_KERNEL_WOLFF_UNION 1 /* bond activation + union-find     */
+#define UMC_KERNEL_WOLFF_FLIP 2  /* cluster flip                     */
+#define UMC_KERNEL_OBSERVE 3     /* full observable recomputation    */
+#define UMC_KERNEL_GAUGE 4       /* gauge-link colour pass           */
+#define UMC_KERNEL_BATCH 5       /* batched-chain kernels            */
+#define UMC_KERNEL_LEARNED 6     /* learned-proposal kernels         */
+#define UMC_KERNEL_OTHER 7       /* layout, start, reduction helpers */
+#define UMC_KERNEL_KINDS 8
+int umc_chain_set_timing(umc_chain* c, int enable);
+int umc_chain_kernel_stats(umc_chain* c, uint64_t* launches, double* device_ms, int reset);
 /* Wolff::mean_cluster_size bookkeeping -- driver.hpp:193-196. */
 int umc_wolff_stats(const umc_chain* c, uint64_t* flips, double* size_sum);
 

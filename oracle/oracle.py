@@ -328,8 +328,8 @@ class Reference:
                               _u64, _u64, _u64, _vp, _vp)
         self._su_expm = L.fn("su_expm", None, _u32, _vp, _vp)
         self._su_shift = L.fn("su_shift", None, _u32, _f64, _u64, _u64, _u32, _u32, _vp, _vp)
-        self._bench_o3 = L.fn("bench_o3", _int, _u64, _f64, _u64, _u32, _u64, _vp, _vp)
-        self._bench_ising = L.fn("bench_ising", _int, _u64, _f64, _u64, _u32, _u64, _vp, _vp)
+        self._bench_o3 = L.fn("bench_o3", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
+        self._bench_ising = L.fn("bench_ising", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
 
     def pcg32_draws(self, seed, stream, n):
         out = np.zeros(n, np.uint32)
@@ -469,17 +469,19 @@ class Reference:
         self._su_shift(N, width, seed, counter, tag, id_, _ptr(cur), _ptr(out))
         return out
 
-    def bench_o3(self, L, beta, steps, threads, seed=1):
+    def bench_o3(self, L, beta, warmup, steps, threads, seed=1):
+        """Reference stock path, O(3) L^3 (1 Wolff flip + 1 sweep per step):
+        (site-updates, seconds of the slowest thread)."""
         su = C.c_double()
         sec = C.c_double()
-        st = self._bench_o3(L, beta, steps, threads, seed, C.byref(su), C.byref(sec))
+        st = self._bench_o3(L, beta, warmup, steps, threads, seed, C.byref(su), C.byref(sec))
         assert st == 0, st
         return su.value, sec.value
 
-    def bench_ising(self, L, beta, sweeps, threads, seed=1):
+    def bench_ising(self, L, beta, warmup, sweeps, threads, seed=1):
         su = C.c_double()
         sec = C.c_double()
-        st = self._bench_ising(L, beta, sweeps, threads, seed, C.byref(su), C.byref(sec))
+        st = self._bench_ising(L, beta, warmup, sweeps, threads, seed, C.byref(su), C.byref(sec))
         assert st == 0, st
         return su.value, sec.value
 

@@ -761,13 +761,15 @@ extern "C" void ref_su_shift(std::uint32_t N, double width, std::uint64_t seed, 
 }
 
 // -------------------------------------------------------------- CPU baseline
-// Times the reference's stock path: VectorSpin<3> on a periodic L^3 PairGraph,
-// Metropolis with UniformSphereN<3> and a plain Pcg32, alternating one sweep
-// with one Wolff flip (UniformSphereN<3> axis).  One independent chain per
-// thread.  Returns total site-updates (sweep sites + flipped cluster sites)
-// and the wall time of the slowest thread.
-extern "C" int ref_bench_o3(std::uint64_t L, double beta, std::uint64_t steps, std::uint32_t threads,
-                 std::uint64_t seed, double* site_updates, double* seconds)
+// Times the reference's stock path: VectorSpin<3> on a periodic L^3 PairGraph
+// (edges built by hand, as a user of the reference would), Metropolis with
+// UniformSphereN<3> and a plain Pcg32, alternating one sweep with one Wolff
+// flip (UniformSphereN<3> axis).  One independent chain per thread, uniform
+// random start; `warmup` untimed steps, then `steps` timed ones.  Reports the
+// total site-updates (sweep sites + flipped cluster sites) and the wall time of
+// the slowest thread.
+extern "C" int ref_bench_o3(std::uint64_t L, double beta, std::uint64_t warmup, std::uint64_t steps,
+                            std::uint32_t threads, std::uint64_t seed, double* site_updates, double* seconds)
 {
     try {
         std::vector<PairGraph<>::Edge> edges;
@@ -794,12 +796,16 @@ extern "C" int ref_bench_o3(std::uint64_t L, double beta, std::uint64_t steps, s
                 }
                 Metropolis<VectorSpin<3>, UniformSphereN<3>, Pcg32> mc(model, UniformSphereN<3>{}, Pcg32(seed + t, 1), beta);
                 Wolff<VectorSpin<3>, UniformSphereN<3>, Pcg32> w(model, UniformSphereN<3>{}, Pcg32(seed + t, 2), beta);
+                for (std::uint64_t s = 0; s < warmup; ++s) {
+                    (void)w.flip();
+                    mc.sweep();
+                }
                 const auto t0 = std::chrono::steady_clock::now();
                 double u = 0.0;
                 for (std::uint64_t s = 0; s < steps; ++s) {
+                    u += double(w.flip());
                     mc.sweep();
                     u += double(n);
-                    u += double(w.flip());
                 }
                 const auto t1 = std::chrono::steady_clock::now();
                 upd[t] = u;
@@ -819,10 +825,10 @@ extern "C" int ref_bench_o3(std::uint64_t L, double beta, std::uint64_t steps, s
     }
 }
 
-// Times the reference's stock Ising Metropolis on an Lx x Ly square_lattice
+// Times the reference's stock Ising Metropolis on an L x L square_lattice
 // (example/ising.hpp + Flip + Pcg32), one chain per thread, cold start.
-extern "C" int ref_bench_ising(std::uint64_t L, double beta, std::uint64_t sweeps, std::uint32_t threads,
-                    std::uint64_t seed, double* site_updates, double* seconds)
+extern "C" int ref_bench_ising(std::uint64_t L, double beta, std::uint64_t warmup, std::uint64_t sweeps,
+                               std::uint32_t threads, std::uint64_t seed, double* site_updates, double* seconds)
 {
     try {
         std::vector<double> secs(threads, 0.0);
@@ -831,6 +837,7 @@ extern "C" int ref_bench_ising(std::uint64_t L, double beta, std::uint64_t sweep
             pool.emplace_back([&, t] {
                 Ising model(square_lattice(L, L), 1);
                 Metropolis<Ising, Flip, Pcg32> mc(model, Flip{}, Pcg32(seed + t, 1), beta);
+                mc.run(warmup);
                 const auto t0 = std::chrono::steady_clock::now();
                 mc.run(sweeps);
                 const auto t1 = std::chrono::steady_clock::now();
@@ -846,4 +853,3 @@ extern "C" int ref_bench_ising(std::uint64_t L, double beta, std::uint64_t sweep
         return status_of(std::current_exception());
     }
 }
-

@@ -161,6 +161,10 @@ _decl("umc_wolff_enqueue", _int, _vp, _f64, _u64)
 _decl("umc_hybrid_enqueue", _int, _vp, _f64, _u64)
 _decl("umc_chain_fetch", _int, _vp, _vp, _vp, _u64, C.POINTER(_u64))
 _decl("umc_wolff_stats", _int, _vp, C.POINTER(_u64), C.POINTER(_f64))
+_decl("umc_chain_set_timing", _int, _vp, _int)
+_decl("umc_chain_kernel_stats", _int, _vp, _vp, _vp, _int)
+
+KERNEL_KINDS = ["metropolis", "wolff_union", "wolff_flip", "observe", "gauge", "batch", "learned", "other"]
 
 
 def check(code: int) -> None:
@@ -430,6 +434,16 @@ class Chain:
         got = _u64(0)
         check(lib.umc_chain_fetch(self._h, _ptr(rec), _ptr(sizes), capacity, C.byref(got)))
         return rec[: got.value], sizes[: got.value]
+
+    def set_timing(self, enable: bool) -> None:
+        check(lib.umc_chain_set_timing(self._h, int(enable)))
+
+    def kernel_stats(self, reset: bool = False) -> dict:
+        """{kind: (launches, device_ms)} for the chain's kernels."""
+        n = np.zeros(len(KERNEL_KINDS), np.uint64)
+        ms = np.zeros(len(KERNEL_KINDS))
+        check(lib.umc_chain_kernel_stats(self._h, _ptr(n), _ptr(ms), int(reset)))
+        return {k: (int(n[i]), float(ms[i])) for i, k in enumerate(KERNEL_KINDS)}
 
     def wolff_stats(self):
         f, s = _u64(0), _f64(0)

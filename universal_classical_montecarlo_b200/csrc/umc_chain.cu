@@ -90,6 +90,53 @@ void ising_wolff_thresholds(int32_t J, double beta, unsigned long long cw[2])
     }
 }
 
+
+LaunchScope::LaunchScope(umc_chain* chain, int k) : c(chain), kind(k)
+{
+    c->launches[k]++;
+    if (!c->timing) return;
+    if (c->event_pool.size() < 2) {
+        for (int q = 0; q < 64; ++q) {
+            cudaEvent_t e;
+            cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+            c->event_pool.push_back(e);
+        }
+    }
+    a = c->event_pool.back();
+    c->event_pool.pop_back();
+    cuda_check(cudaEventRecord(a, c->stream), "cudaEventRecord");
+}
+
+LaunchScope::~LaunchScope()
+{
+    if (!a) return;
+    cudaEvent_t b = c->event_pool.back();
+    c->event_pool.pop_back();
+    cudaEventRecord(b, c->stream);
+    c->timed.push_back({kind, a, b});
+    // bound the number of outstanding event pairs
+    if (c->timed.size() >= 4096) {
+        try {
+            collect_kernel_times(c);
+        } catch (...) {
+        }
+    }
+}
+
+void collect_kernel_times(umc_chain* c)
+{
+    if (c->timed.empty()) return;
+    cuda_check(cudaStreamSynchronize(c->stream), "synchronise for kernel times");
+    for (auto& t : c->timed) {
+        float ms = 0.f;
+        cuda_check(cudaEventElapsedTime(&ms, t.a, t.b), "cudaEventElapsedTime");
+        c->device_ms[t.kind] += ms;
+        c->event_pool.push_back(t.a);
+        c->event_pool.push_back(t.b);
+    }
+    c->timed.clear();
+}
+
 namespace {
 
 uint32_t grid_for(const umc_chain* c, uint64_t work)
@@ -144,8 +191,10 @@ void ensure_labels(umc_chain* c)
     c->lab0.alloc(c->n * 4, "Wolff labels");
     c->lab1.alloc(c->n * 4, "Wolff labels");
     const uint32_t g = grid_for(c, c->n);
+    LaunchScope ls(c, UMC_KERNEL_OTHER);
     iota_u32<<<g, kBlock, 0, c->stream>>>(c->lab0.as<uint32_t>(), uint32_t(c->n));
     iota_u32<<<g, kBlock, 0, c->stream>>>(c->lab1.as<uint32_t>(), uint32_t(c->n));
+    c->launches[UMC_KERNEL_OTHER]++;
     launch_check("iota labels");
 }
 
@@ -163,6 +212,7 @@ template <class Topo>
 void launch_ising_generic(umc_chain* c, IsingArgs a, Topo t)
 {
     const size_t smem = (2 * size_t(a.D) + 1) * sizeof(uint32_t);
+    LaunchScope ls(c, UMC_KERNEL_METROPOLIS);
     ising_pass<Topo><<<grid_for(c, a.count), kBlock, smem, c->stream>>>(a, t);
 }
 
@@ -170,6 +220,7 @@ template <int N, class Topo>
 void launch_vector(umc_chain* c, const VecArgs& a, Topo t)
 {
     const uint32_t g = grid_for(c, a.count);
+    LaunchScope ls(c, UMC_KERNEL_METROPOLIS);
     if (c->desc.proposal == UMC_PROPOSAL_ROTATION) vector_pass<N, kPropRotation, Topo><<<g, kBlock, 0, c->stream>>>(a, t);
     else vector_pass<N, kPropSphere, Topo><<<g, kBlock, 0, c->stream>>>(a, t);
 }
@@ -199,6 +250,7 @@ void spin_pass(umc_chain* c, uint32_t p, double beta, uint64_t kbase, const Pass
         launch_vector_n(c, a, t);
     } else {
         XYArgs a{c->field.as<float>(), first, count, kbase, c->J, float(beta), float(c->desc.width), o};
+        LaunchScope ls(c, UMC_KERNEL_METROPOLIS);
         xy_pass<Topo><<<grid_for(c, count), kBlock, 0, c->stream>>>(a, t);
     }
 }
@@ -222,6 +274,7 @@ void observe_into(umc_chain* c, double* rec, unsigned long long* size_slot)
     ensure_csr(c);
     const PassOut o{c->ctl.as<DevCtl>(), c->partials.as<double>(), rec, nullptr, kMaxPasses - 1, 1, 1};
     const uint32_t g = grid_for(c, c->n);
+    LaunchScope ls(c, UMC_KERNEL_OBSERVE);
     switch (c->model) {
     case UMC_MODEL_ISING:
         observe_csr<0><<<g, kBlock, 0, c->stream>>>(c->field.p, uint32_t(c->n), c->off.as<uint32_t>(), c->adj.as<uint32_t>(), c->J, o, size_slot);
@@ -263,6 +316,7 @@ void spin_sweep(umc_chain* c, double beta, double* rec)
             a.J = c->J_int;
             a.out = o;
             const uint32_t g = grid_for(c, c->n / 2 / 16);
+            LaunchScope ls(c, UMC_KERNEL_METROPOLIS);
             ising_packed_pass<<<g, kBlock, 0, c->stream>>>(a);
         } else if (c->stencil) {
             StencilTopo t{uint32_t(c->dims[0] / 2), uint32_t(c->dims[1]), uint32_t(c->dims[2]), uint32_t(c->n / 2), p,
@@ -313,15 +367,25 @@ void spin_flip(umc_chain* c, double beta, double* rec, unsigned long long* size_
     a.ctl = c->ctl.as<DevCtl>();
     a.size_slot = size_slot;
     const uint32_t g = grid_for(c, c->n);
-    if (c->model == UMC_MODEL_ISING) {
-        wolff_union<0><<<g, kBlock, 0, c->stream>>>(a);
-        wolff_flip<0><<<g, kBlock, 0, c->stream>>>(a);
-    } else {
-        switch (c->N) {
-        case 1: wolff_union<1><<<g, kBlock, 0, c->stream>>>(a); wolff_flip<1><<<g, kBlock, 0, c->stream>>>(a); break;
-        case 2: wolff_union<2><<<g, kBlock, 0, c->stream>>>(a); wolff_flip<2><<<g, kBlock, 0, c->stream>>>(a); break;
-        case 3: wolff_union<3><<<g, kBlock, 0, c->stream>>>(a); wolff_flip<3><<<g, kBlock, 0, c->stream>>>(a); break;
-        case 4: wolff_union<4><<<g, kBlock, 0, c->stream>>>(a); wolff_flip<4><<<g, kBlock, 0, c->stream>>>(a); break;
+    const int model = c->model == UMC_MODEL_ISING ? 0 : c->N;
+    {
+        LaunchScope ls(c, UMC_KERNEL_WOLFF_UNION);
+        switch (model) {
+        case 0: wolff_union<0><<<g, kBlock, 0, c->stream>>>(a); break;
+        case 1: wolff_union<1><<<g, kBlock, 0, c->stream>>>(a); break;
+        case 2: wolff_union<2><<<g, kBlock, 0, c->stream>>>(a); break;
+        case 3: wolff_union<3><<<g, kBlock, 0, c->stream>>>(a); break;
+        case 4: wolff_union<4><<<g, kBlock, 0, c->stream>>>(a); break;
+        }
+    }
+    {
+        LaunchScope ls(c, UMC_KERNEL_WOLFF_FLIP);
+        switch (model) {
+        case 0: wolff_flip<0><<<g, kBlock, 0, c->stream>>>(a); break;
+        case 1: wolff_flip<1><<<g, kBlock, 0, c->stream>>>(a); break;
+        case 2: wolff_flip<2><<<g, kBlock, 0, c->stream>>>(a); break;
+        case 3: wolff_flip<3><<<g, kBlock, 0, c->stream>>>(a); break;
+        case 4: wolff_flip<4><<<g, kBlock, 0, c->stream>>>(a); break;
         }
     }
     launch_check("Wolff flip");
@@ -508,6 +572,11 @@ void destroy_chain(umc_chain* c)
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     gauge_release(c);
+    for (auto& t : c->timed) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
     for (DevBuf* b : {&c->field, &c->staging, &c->off, &c->adj, &c->slot, &c->position, &c->lab0, &c->lab1, &c->cells,
                       &c->inc_off, &c->inc_cell, &c->inc_which, &c->partials, &c->ctl, &c->records, &c->sizes, &c->tm1})
         b->free_();
@@ -648,6 +717,7 @@ int umc_chain_set_field(umc_chain* c, const void* host_field)
         if (!c->staging.p) c->staging.alloc(c->field_bytes, "staging");
         cuda_check(cudaMemcpyAsync(c->staging.p, host_field, c->field_bytes, cudaMemcpyHostToDevice, c->stream), "upload field");
         const uint32_t g = grid_for(c, c->n);
+        LaunchScope ls(c, UMC_KERNEL_OTHER);
         if (c->elem_bytes == 1)
             scatter_field<int8_t><<<g, kBlock, 0, c->stream>>>(c->staging.as<int8_t>(), c->field.as<int8_t>(), uint32_t(c->n), 1, placement(c));
         else
@@ -668,10 +738,13 @@ int umc_chain_get_field(umc_chain* c, void* host_field)
         }
         if (!c->staging.p) c->staging.alloc(c->field_bytes, "staging");
         const uint32_t g = grid_for(c, c->n);
+        {
+        LaunchScope ls(c, UMC_KERNEL_OTHER);
         if (c->elem_bytes == 1)
             gather_field<int8_t><<<g, kBlock, 0, c->stream>>>(c->field.as<int8_t>(), c->staging.as<int8_t>(), uint32_t(c->n), 1, placement(c));
         else
             gather_field<float><<<g, kBlock, 0, c->stream>>>(c->field.as<float>(), c->staging.as<float>(), uint32_t(c->n), c->comps, placement(c));
+        }
         launch_check("gather field");
         cuda_check(cudaMemcpyAsync(host_field, c->staging.p, c->field_bytes, cudaMemcpyDeviceToHost, c->stream), "download field");
         cuda_check(cudaStreamSynchronize(c->stream), "download field");
@@ -689,6 +762,7 @@ int umc_chain_randomize(umc_chain* c, uint64_t seed)
         }
         const uint32_t g = grid_for(c, c->n);
         const uint32_t n = uint32_t(c->n);
+        LaunchScope ls(c, UMC_KERNEL_OTHER);
         if (c->model == UMC_MODEL_ISING) randomize_spins<0><<<g, kBlock, 0, c->stream>>>(c->field.p, n, seed, placement(c));
         else if (c->model == UMC_MODEL_XY_ANGLE) randomize_spins<-1><<<g, kBlock, 0, c->stream>>>(c->field.p, n, seed, placement(c));
         else
@@ -836,6 +910,32 @@ int umc_chain_fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t cap
         if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
         device_scope(c);
         fetch(c, records, sizes, capacity, n_records);
+    });
+}
+
+int umc_chain_set_timing(umc_chain* c, int enable)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        c->timing = enable != 0;
+    });
+}
+
+int umc_chain_kernel_stats(umc_chain* c, uint64_t* launches, double* device_ms, int reset)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        collect_kernel_times(c);
+        for (int k = 0; k < UMC_KERNEL_KINDS; ++k) {
+            if (launches) launches[k] = c->launches[k];
+            if (device_ms) device_ms[k] = c->device_ms[k];
+            if (reset) {
+                c->launches[k] = 0;
+                c->device_ms[k] = 0.0;
+            }
+        }
     });
 }
 

@@ -92,4 +92,29 @@ struct umc_chain
 
     // learned proposal (U(1) only)
     void* learned = nullptr;
+
+    // kernel accounting
+    bool timing = false;
+    uint64_t launches[UMC_KERNEL_KINDS] = {};
+    double device_ms[UMC_KERNEL_KINDS] = {};
+    struct Timed
+    {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    std::vector<Timed> timed;
+    std::vector<cudaEvent_t> event_pool;
 };
+
+namespace umc {
+// Bracket one kernel launch: counts it and, with timing on, records events.
+struct LaunchScope
+{
+    umc_chain* c;
+    int kind;
+    cudaEvent_t a = nullptr;
+    LaunchScope(umc_chain* chain, int k);
+    ~LaunchScope();
+};
+void collect_kernel_times(umc_chain* c);
+}  // namespace umc

@@ -91,7 +91,7 @@ struct IsingPackedArgs
 __device__ __forceinline__ uint32_t down_bits(uint32_t w) { return (w >> 1) & 0x01010101u; }
 __device__ __forceinline__ uint32_t byte_sum(uint32_t w) { return (w * 0x01010101u) >> 24; }
 
-__global__ void __launch_bounds__(kBlock) ising_packed_pass(IsingPackedArgs a)
+static __global__ void __launch_bounds__(kBlock) ising_packed_pass(IsingPackedArgs a)
 {
     __shared__ uint32_t tm1[5];
     if (threadIdx.x < 5) tm1[threadIdx.x] = a.tm1[threadIdx.x];
@@ -556,7 +556,7 @@ __global__ void __launch_bounds__(kBlock) wolff_flip(WolffArgs a)
     if (threadIdx.x == 0 && cnt[0] > 0.0) atomicAdd(a.size_slot, (unsigned long long)cnt[0]);
 }
 
-__global__ void iota_u32(uint32_t* p, uint32_t n)
+static __global__ void iota_u32(uint32_t* p, uint32_t n)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = i;
 }
