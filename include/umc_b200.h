@@ -223,6 +223,32 @@ int umc_chain_kernel_stats(umc_chain* c, uint64_t* launches, double* device_ms, 
 /* Wolff::mean_cluster_size bookkeeping -- driver.hpp:193-196. */
 int umc_wolff_stats(const umc_chain* c, uint64_t* flips, double* size_sum);
 
+/* ================================================= allocation-free Wolff flip */
+
+/* No counterpart in the reference: an extra entry point for callers that cannot
+ * call cudaMalloc (a host framework whose pool owns all device memory, or a
+ * latency-critical path that must not pay cudaMalloc's device synchronisation).
+ * One single-cluster Wolff flip -- the same kernels and random streams as
+ * umc_wolff_run -- on caller-owned device memory:
+ *   field      Ising int8[n] or VectorSpin<N> float (component c of site k at
+ *              field[c*n + k]), updated in place;
+ *   offset/bonds/slot_edge  symmetric CSR over the same site order (slot_edge =
+ *              index of the input edge that produced each slot, which keys the
+ *              bond draws; the seed site is drawn in this site order);
+ *   model      UMC_MODEL_ISING (FixedAxis) or UMC_MODEL_VECTOR (UniformSphereN axis).
+ * Its scratch (union-find labels and a status word) is a file-scope device
+ * array sized for at most 1,048,576 sites; larger graphs return
+ * UMC_ERR_UNSUPPORTED.  Every GPU that loads the library holds that array
+ * (about 8 MiB) until the process exits.  The first call on a device resolves
+ * the array's address (cudaGetSymbolAddress) with that device current, so make
+ * it before any stream capture.  All calls share the array: each call resets
+ * what must start from a known value, and calls that overlap on the GPU race.
+ * The call synchronises `stream` and returns the cluster size. */
+int umc_wolff_flip_noalloc(int32_t model, int32_t components, void* field, uint64_t n_sites,
+                           const uint32_t* offset, const uint32_t* bonds, const uint32_t* slot_edge,
+                           double coupling, double beta, uint64_t seed, uint64_t flip,
+                           uint64_t* cluster_size, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
