@@ -533,6 +533,9 @@ __global__ void gauge_haar(float* f, uint32_t n, uint64_t seed, const uint32_t* 
                 z.re[q] = re;
                 z.im[q] = im;
             }
+            // classical Gram-Schmidt in FP32 loses orthogonality on badly
+            // conditioned draws: project the result back onto SU(N)
+            reunitarise<N>(z);
             mat_store(z, f, n, k);
         }
     }
