@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", choices=["o3", "ising", "su3"], default="o3",
+                   help="o3: the headline configuration; ising / su3: secondary roofline runs")
     return p.parse_args()
 
 
@@ -132,8 +134,8 @@ def measured_peak_hbm():
 
 def profiled_traffic(kind: str, units: float):
     """DRAM bytes per launch of a kernel from the committed ncu summary
-    (profiles/traffic.txt: '<kind> <bytes per unit>' lines), scaled to this
-    launch's units, or None when no capture was summarised."""
+    (profiles/traffic.txt: '<workload>:<kind> <bytes per launch>' lines), or
+    None when no capture was summarised."""
     path = os.path.join(PROFILES, "traffic.txt")
     try:
         for line in open(path):
@@ -190,6 +192,172 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ workloads
+class O3Hybrid:
+    """Headline workload: O(3) L^3, one Wolff flip + one Metropolis sweep per step."""
+
+    name = "o3"
+    unit = "site-updates/s"
+    dtype = "f32"
+
+    def __init__(self, umc, args, rank, local):
+        self.L = args.L
+        self.n = self.L**3
+        g = umc.cubic_lattice(self.L, self.L, self.L)
+        self.ch = umc.Chain(umc.MODEL_VECTOR, graph=g, components=3, coupling=1.0, proposal=umc.PROPOSAL_SPHERE,
+                            wolff_axis=umc.AXIS_SPHERE, seed=1 + rank, device=local, max_records=8192)
+        self.ch.randomize(1000 + rank)
+        self.flush = True
+
+    def describe(self):
+        return workload(self.L)
+
+    def enqueue(self, k):
+        self.ch.enqueue_hybrid(BETA, k)
+
+    def units(self, rec, sizes):
+        return len(rec) * self.n + float(sizes.sum())
+
+    def bytes_per_launch(self, kind):
+        # algorithmic bytes (DESIGN.md): colour pass 36 B per site-update
+        # (read own + neighbour class, write own; 12 B per FP32 3-vector);
+        # Wolff: bond pass reads each site and its + neighbours once (12 B +
+        # 4 B label write + 1 B crossing mask), flip reads label + spin (16 B)
+        n = self.n
+        return {"metropolis": 36.0 * n / 2, "wolff_union": 17.0 * n, "wolff_flip": 16.0 * n,
+                "wolff_merge": 1.0 * n}.get(kind, 36.0 * n / 2)
+
+    def e2e(self, torch, K):
+        host = torch.empty((self.n, 3), dtype=torch.float32, pin_memory=True)
+        host.numpy()[:] = self.ch.get_field()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u = 0.0
+        for _ in range(K):
+            self.ch.set_field(host.numpy())  # H2D from pinned memory + layout kernel
+            sz, _ = self.ch.hybrid(BETA, 1)  # step + D2H of the record
+            u += self.n + float(sz[0])
+        torch.cuda.synchronize()
+        return {"value": u / (time.perf_counter() - t0), "unit": self.unit, "h2d_bytes_per_step": self.n * 12,
+                "d2h_bytes_per_step": 8 * 8 + 8, "steps": K}
+
+    def cpu(self, seconds):
+        est = reference_o3(self.L, 0, 1, 1)
+        if est is None:
+            return None
+        threads = cpu_threads()
+        steps = max(2, int(seconds / max(est[1], 1e-4)))
+        su, sec = reference_o3(self.L, 1, steps, threads)
+        return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                "sample": f"{steps} steps x {threads} independent {self.L}^3 chains (reference stock driver, "
+                          f"plain Pcg32), {sec:.1f} s"}
+
+
+class IsingSweep:
+    """Plain Ising Metropolis (Flip, J=1, beta=0.44) on an L x L lattice; step =
+    one sweep.  At the default L = 32768 the int8 field is 1 GiB, far above L2."""
+
+    name = "ising"
+    unit = "site-updates/s"
+    dtype = "i8"
+
+    def __init__(self, umc, args, rank, local):
+        self.L = args.L if args.L != L_DEFAULT else 32768
+        self.n = self.L * self.L
+        g = umc.square_lattice(self.L, self.L)
+        self.ch = umc.Chain(umc.MODEL_ISING, graph=g, coupling=1, proposal=umc.PROPOSAL_FLIP, seed=1 + rank,
+                            device=local, max_records=8192)
+        self.ch.randomize(7 + rank)
+        self.flush = self.n < (256 << 20)
+
+    def describe(self):
+        return (f"2D Ising {self.L}x{self.L} periodic, int8 spins, J=1, beta=0.44, Flip, random start; "
+                f"step = 1 Metropolis sweep (packed checkerboard), E and M every sweep")
+
+    def enqueue(self, k):
+        self.ch.enqueue_metropolis(0.44, k)
+
+    def units(self, rec, sizes):
+        return len(rec) * self.n
+
+    def bytes_per_launch(self, kind):
+        return 3.0 * self.n / 2  # read own + other class, write own: 3 B per site-update
+
+    def e2e(self, torch, K):
+        host = torch.empty(self.n, dtype=torch.int8, pin_memory=True)
+        host.numpy()[:] = self.ch.get_field()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(K):
+            self.ch.set_field(host.numpy())
+            self.ch.metropolis(0.44, 1)
+        torch.cuda.synchronize()
+        return {"value": K * self.n / (time.perf_counter() - t0), "unit": self.unit, "h2d_bytes_per_step": self.n,
+                "d2h_bytes_per_step": 64, "steps": K}
+
+    def cpu(self, seconds):
+        from oracle.oracle import Reference, have_reference
+
+        if not have_reference():
+            return None
+        r = Reference()
+        threads = cpu_threads()
+        su, sec = r.bench_ising(64, 0.44, 10, 2000, threads, 1)
+        return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                "sample": f"2000 sweeps x {threads} independent 64x64 chains (reference stock driver)"}
+
+
+class SU3Sweep:
+    """SU(3) Wilson action on the L^4 hypercubic plaquette complex, beta = 5.7 in
+    the model, SUShift width 0.2, 10 hits per link, reunitarisation and the FP64
+    mean plaquette every sweep, Haar hot start; step = one sweep."""
+
+    name = "su3"
+    unit = "link-updates/s"
+    dtype = "f32"
+
+    def __init__(self, umc, args, rank, local):
+        self.L = args.L if args.L != L_DEFAULT else 24
+        cc = umc.hypercubic_plaquettes(self.L)
+        self.n = cc.sites()
+        self.ch = umc.Chain(umc.MODEL_SU, cells=cc, components=3, coupling=5.7, proposal=umc.PROPOSAL_SUSHIFT,
+                            width=0.2, hits=10, seed=1 + rank, device=local, max_records=8192)
+        self.ch.randomize(11 + rank)
+        self.flush = True
+
+    def describe(self):
+        return (f"SU(3) Wilson action {self.L}^4 hypercubic_plaquettes, FP32 links, Haar start, beta=5.7, "
+                f"SUShift 0.2, 10 hits per link, reunitarisation + FP64 mean plaquette every sweep")
+
+    def enqueue(self, k):
+        self.ch.enqueue_metropolis(1.0, k)
+
+    def units(self, rec, sizes):
+        return len(rec) * self.n
+
+    def bytes_per_launch(self, kind):
+        # per (mu, parity) pass: read 4.5 V links + write V/2 (72 B each) = 648 B per link-update
+        return 648.0 * self.n / 8
+
+    def e2e(self, torch, K):
+        host = torch.empty((self.n, 18), dtype=torch.float32, pin_memory=True)
+        host.numpy()[:] = self.ch.get_field()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(K):
+            self.ch.set_field(host.numpy())
+            self.ch.metropolis(1.0, 1)
+        torch.cuda.synchronize()
+        return {"value": K * self.n / (time.perf_counter() - t0), "unit": self.unit,
+                "h2d_bytes_per_step": self.n * 72, "d2h_bytes_per_step": 64, "steps": K}
+
+    def cpu(self, seconds):
+        return None
+
+
+WORKLOADS = {"o3": O3Hybrid, "ising": IsingSweep, "su3": SU3Sweep}
+
+
 # ---------------------------------------------------------------------- umc
 def main():
     args = parse()
@@ -207,25 +375,22 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     import universal_classical_montecarlo_b200 as umc
 
-    L = args.L
-    n = L**3
-    g = umc.cubic_lattice(L, L, L)
-    ch = umc.Chain(umc.MODEL_VECTOR, graph=g, components=3, coupling=1.0, proposal=umc.PROPOSAL_SPHERE,
-                   wolff_axis=umc.AXIS_SPHERE, seed=1 + rank, device=local, max_records=8192)
-    ch.randomize(1000 + rank)
+    wl = WORKLOADS[args.workload](umc, args, rank, local)
+    ch = wl.ch
     stream = torch.cuda.ExternalStream(ch.stream(), device=torch.device("cuda", local))
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if wl.flush else None
 
     def barrier():
         if ws > 1:
             dist.barrier()
 
     # ---- warm-up
-    ch.enqueue_hybrid(BETA, args.warmup)
+    wl.enqueue(args.warmup)
     ch.fetch(8192)
     ch.kernel_stats(reset=True)
 
-    # ---- timed region: K steps, L2 flushed between steps, steps timed on the chain's stream
+    # ---- timed region: K steps (L2 flushed between steps when the state fits
+    # in L2), each step timed with CUDA events on the chain's stream
     K = args.steps
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
@@ -238,20 +403,21 @@ def main():
     done = 0
     with torch.cuda.stream(stream):
         for k in range(K):
-            flush.fill_(k & 0xFF)
+            if flush is not None:
+                flush.fill_(k & 0xFF)
             starts[k].record(stream)
-            ch.enqueue_hybrid(BETA, 1)
+            wl.enqueue(1)
             ends[k].record(stream)
             done += 1
             if done == 4096:  # drain the record ring
                 rec, sizes = ch.fetch(8192)
-                units += len(rec) * n + float(sizes.sum())
+                units += wl.units(rec, sizes)
                 done = 0
     torch.cuda.synchronize()
     clocks = sampler.stop()
     barrier()
     rec, sizes = ch.fetch(8192)
-    units += len(rec) * n + float(sizes.sum())
+    units += wl.units(rec, sizes)
     launches = ch.kernel_stats(reset=True)
     gpu_launches = sum(v[0] for k, v in launches.items())
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
@@ -262,41 +428,23 @@ def main():
     KP = min(K, 2000)
     with torch.cuda.stream(stream):
         for k in range(KP):
-            flush.fill_(k & 0xFF)
-            ch.enqueue_hybrid(BETA, 1)
+            if flush is not None:
+                flush.fill_(k & 0xFF)
+            wl.enqueue(1)
             if (k + 1) % 4096 == 0:
                 ch.fetch(8192)
     ch.fetch(8192)
     per_kind = ch.kernel_stats(reset=True)
     ch.set_timing(False)
-    kind, (nl, ms) = max(((k, v) for k, v in per_kind.items() if v[0] > 0), key=lambda kv: kv[1][1])
+    kind, (nl, ms) = max(((k, v) for k, v in per_kind.items() if v[0] > 0 and k != "other"),
+                         key=lambda kv: kv[1][1])
     avg_s = ms / nl / 1e3
-    # algorithmic bytes per launch: colour pass 36 B per site-update
-    # (read own + neighbour class, write own; 12 B per FP32 3-vector), union-find
-    # 68 B per site (field + CSR + label), flip 20 B per site (+ 12 B per flipped site)
-    per_unit = {"metropolis": (36.0, n / 2), "wolff_union": (68.0, n), "wolff_flip": (20.0, n)}
-    bpu, units_per_launch = per_unit.get(kind, (36.0, n / 2))
-    achieved = bpu * units_per_launch / avg_s / 1e9
+    achieved = wl.bytes_per_launch(kind) / avg_s / 1e9
     peak, peak_src = measured_peak_hbm()
-    traffic = profiled_traffic(kind, units_per_launch)
+    traffic = profiled_traffic(f"{wl.name}:{kind}", 1.0)
 
     # ---- end to end through the C ABI with host buffers
-    e2e = None
-    if not args.no_e2e:
-        host = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
-        host.numpy()[:] = ch.get_field()
-        KE = min(K, 300)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        e_units = 0.0
-        for _ in range(KE):
-            ch.set_field(host.numpy())  # H2D from pinned memory + layout kernel
-            sz, r = ch.hybrid(BETA, 1)  # step + D2H of the record
-            e_units += n + float(sz[0])
-        torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
-        e2e = {"value": e_units / e2e_s, "unit": "site-updates/s", "h2d_bytes_per_step": n * 3 * 4,
-               "d2h_bytes_per_step": 8 * 8 + 8, "steps": KE}
+    e2e = None if args.no_e2e else wl.e2e(torch, min(K, 300))
 
     # ---- aggregate over ranks
     max_ms, tot_units = total_ms, units
@@ -313,15 +461,7 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        threads = cpu_threads()
-        est = reference_o3(L, 0, 1, 1)
-        if est is not None:
-            per_step = est[1]
-            steps = max(2, int(args.cpu_seconds / max(per_step, 1e-4)))
-            su, sec = reference_o3(L, 1, steps, threads)
-            cpu = {"value": su / sec, "unit": "site-updates/s", "cores": threads, "kind": "reference",
-                   "sample": f"{steps} steps x {threads} independent {L}^3 chains (reference stock driver, "
-                             f"plain Pcg32), {sec:.1f} s"}
+        cpu = wl.cpu(args.cpu_seconds)
 
     if ws > 1:
         dist.barrier()
@@ -330,20 +470,21 @@ def main():
         return
     value = tot_units / (max_ms / 1e3)
     line = {
-        "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": ws, "steps": K,
+        "metric": METRIC, "value": value, "unit": wl.unit, "n_gpus": ws, "steps": K,
         "warmup": args.warmup, "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload(L), "L": L, "beta": BETA, "parallelism": f"replicas x{ws}" if ws > 1 else "1 chain",
-                   "l2": "flushed between timed steps (256 MiB write, outside the timed events)",
-                   "units": "Metropolis site-updates + Wolff flipped sites",
-                   "mean_cluster": float(sizes.mean()) if len(sizes) else None},
+        "vs_baseline": None, "dtype": wl.dtype, "data": "synthetic",
+        "config": {"workload": wl.describe(), "L": wl.L, "parallelism": f"replicas x{ws}" if ws > 1 else "1 chain",
+                   "l2": ("flushed between timed steps (256 MiB write, outside the timed events)" if wl.flush
+                          else "state larger than L2, no flush"),
+                   "mean_cluster": float(sizes.mean()) if len(sizes) and wl.name == "o3" else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": kind, "avg_launch_us": avg_s * 1e6,
-                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback 6.65 TB/s"},
+                     "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "of fallback 6.65 TB/s"},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": gpu_launches,
         "kernel_launches": {k: v[0] for k, v in launches.items() if v[0]},
+        "kernel_ms": {k: round(v[1], 4) for k, v in per_kind.items() if v[0]},
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)

@@ -204,6 +204,12 @@ int umc_hybrid_enqueue(umc_chain* c, double beta, uint64_t n_steps);
  * receives their count; records / sizes may be NULL.  Synchronises. */
 int umc_chain_fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t capacity,
                     uint64_t* n_records);
+/* Execution strategy on regular lattices (no reference counterpart): with
+ * fusion on (the default) a Metropolis sweep, a Wolff flip or a hybrid step of
+ * a VectorSpin chain runs as one cooperative kernel whose phases are separated
+ * by a bounded grid barrier; off, each phase is its own kernel.  Both give the
+ * same field; the FP64 observable sums may differ in the last bits. */
+int umc_chain_set_fused(umc_chain* c, int enable);
 /* Kernel accounting (no reference counterpart).  Every kernel the chain
  * launches is counted by kind; with timing enabled each launch is also
  * bracketed by CUDA events on the chain's stream.  umc_chain_kernel_stats
@@ -217,7 +223,9 @@ int umc_chain_fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t cap
 #define UMC_KERNEL_BATCH 5       /* batched-chain kernels            */
 #define UMC_KERNEL_LEARNED 6     /* learned-proposal kernels         */
 #define UMC_KERNEL_OTHER 7       /* layout, start, reduction helpers */
-#define UMC_KERNEL_KINDS 8
+#define UMC_KERNEL_WOLFF_MERGE 8 /* union of tile-crossing bonds     */
+#define UMC_KERNEL_FUSED 9       /* fused step (Wolff + sweep)       */
+#define UMC_KERNEL_KINDS 10
 int umc_chain_set_timing(umc_chain* c, int enable);
 int umc_chain_kernel_stats(umc_chain* c, uint64_t* launches, double* device_ms, int reset);
 /* Wolff::mean_cluster_size bookkeeping -- driver.hpp:193-196. */

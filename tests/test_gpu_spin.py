@@ -236,7 +236,7 @@ def test_vector_metropolis_per_sweep(umc, oracle, N, prop, dims):
         v_o, obs_o, margin = oracle.vector_metropolis(N, off, bonds, 1.0, 0.693, prop, 0.6, 5, sweep, 1, cm)
         rec = ch.metropolis(0.693, 1)
         got = ch.get_field().reshape(n, N)
-        mism += _compare_sweep(got[np.argsort(pos)] if False else got, v_o[pos], margin[pos], *_site_csr(umc, g))
+        mism += _compare_sweep(got, v_o[pos], margin[pos], *_site_csr(umc, g))
         # the fused FP64 record equals the observables of the new state
         e_true = _vector_energy(g, got.astype(np.float64))
         assert abs(rec[0, 0] - e_true) < 1e-5 * max(1.0, abs(e_true))
@@ -384,3 +384,36 @@ def test_invalid_combinations_are_rejected(umc):
         ch.wolff(0.5, 1)  # no axis configured
     with pytest.raises(ValueError):
         ch.metropolis(float("nan"), 1)
+
+
+@pytest.mark.parametrize("dims,N,prop", [((16, 16, 16), 3, "sphere"), ((32, 32, 1), 2, "rotation"),
+                                         ((8, 8, 8), 4, "sphere"), ((6, 4, 2), 3, "rotation"),
+                                         ((64, 64, 64), 3, "sphere")])
+def test_fused_step_matches_multikernel(umc, dims, N, prop):
+    """The one-kernel step (cooperative, grid barrier) and the five-kernel path
+    produce the same field, cluster sizes and accept counts."""
+    g = umc.cubic_lattice(*dims) if dims[2] > 1 else umc.square_lattice(dims[0], dims[1])
+    kind = umc.PROPOSAL_SPHERE if prop == "sphere" else umc.PROPOSAL_ROTATION
+    chains = []
+    for fused in (True, False):
+        ch = umc.Chain(umc.MODEL_VECTOR, graph=g, components=N, coupling=1.0, proposal=kind, width=0.8,
+                       wolff_axis=umc.AXIS_SPHERE, seed=21)
+        ch.set_fused(fused)
+        ch.randomize(4)
+        chains.append(ch)
+    out = []
+    for ch in chains:
+        ch.kernel_stats(reset=True)
+        s1, r1 = ch.hybrid(0.693, 12)
+        r2 = ch.metropolis(0.693, 5)
+        s3, r3 = ch.wolff(0.693, 5)
+        out.append((s1, r1, r2, s3, r3, ch.get_field(), ch.kernel_stats()))
+    a, b = out
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[3], b[3])
+    np.testing.assert_array_equal(a[5], b[5])
+    for ra, rb in ((a[1], b[1]), (a[2], b[2]), (a[4], b[4])):
+        np.testing.assert_array_equal(ra[:, 7], rb[:, 7])
+        np.testing.assert_allclose(ra[:, :5], rb[:, :5], rtol=1e-9, atol=1e-6)
+    assert a[6]["fused"][0] == 12 + 5 + 5 and a[6]["metropolis"][0] == 0
+    assert b[6]["fused"][0] == 0

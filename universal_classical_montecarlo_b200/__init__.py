@@ -162,9 +162,11 @@ _decl("umc_hybrid_enqueue", _int, _vp, _f64, _u64)
 _decl("umc_chain_fetch", _int, _vp, _vp, _vp, _u64, C.POINTER(_u64))
 _decl("umc_wolff_stats", _int, _vp, C.POINTER(_u64), C.POINTER(_f64))
 _decl("umc_chain_set_timing", _int, _vp, _int)
+_decl("umc_chain_set_fused", _int, _vp, _int)
 _decl("umc_chain_kernel_stats", _int, _vp, _vp, _vp, _int)
 
-KERNEL_KINDS = ["metropolis", "wolff_union", "wolff_flip", "observe", "gauge", "batch", "learned", "other"]
+KERNEL_KINDS = ["metropolis", "wolff_union", "wolff_flip", "observe", "gauge", "batch", "learned", "other",
+                "wolff_merge", "fused"]
 
 
 def check(code: int) -> None:
@@ -434,6 +436,9 @@ class Chain:
         got = _u64(0)
         check(lib.umc_chain_fetch(self._h, _ptr(rec), _ptr(sizes), capacity, C.byref(got)))
         return rec[: got.value], sizes[: got.value]
+
+    def set_fused(self, enable: bool) -> None:
+        check(lib.umc_chain_set_fused(self._h, int(enable)))
 
     def set_timing(self, enable: bool) -> None:
         check(lib.umc_chain_set_timing(self._h, int(enable)))

@@ -19,6 +19,8 @@
 #include "umc_chain.hpp"
 #include "umc_gauge.hpp"
 #include "umc_spin_kernels.cuh"
+#include "umc_fused.cuh"
+#include "umc_wolff_tiled.cuh"
 
 namespace umc {
 
@@ -139,6 +141,8 @@ void collect_kernel_times(umc_chain* c)
 
 namespace {
 
+bool fused_step(umc_chain* c, double beta, bool wolff, bool sweep, double* rec, unsigned long long* size_slot);
+
 uint32_t grid_for(const umc_chain* c, uint64_t work)
 {
     const uint64_t b = (work + kBlock - 1) / kBlock;
@@ -180,6 +184,15 @@ bool is_spin(const umc_chain* c)
 void ensure_csr(umc_chain* c)
 {
     if (c->off.p) return;
+    if (c->h_off.empty() && c->n > 0) {
+        // regular lattice created without tables: build them from the extents
+        umc_graph* g = make_cubic(c->dims[0], c->dims[1], c->dims[2]);
+        materialize(g);
+        c->h_off = g->c_offset;
+        c->h_adj = g->c_bonds;
+        c->h_slot = g->c_slot_edge;
+        delete g;
+    }
     upload(c->off, c->h_off, c->stream, "upload CSR offsets");
     upload(c->adj, c->h_adj, c->stream, "upload CSR bonds");
     upload(c->slot, c->h_slot, c->stream, "upload CSR edge ids");
@@ -297,6 +310,7 @@ void observe_into(umc_chain* c, double* rec, unsigned long long* size_slot)
 // One Metropolis sweep of a spin model: one kernel per colour class.
 void spin_sweep(umc_chain* c, double beta, double* rec)
 {
+    if (fused_step(c, beta, false, true, rec, nullptr)) return;
     ensure_ising_tables(c, beta);
     const uint64_t kbase = key_base(key_seed(c->desc.seed, c->sweeps, tag_site(0)));
     const bool fused = c->symmetric;
@@ -320,7 +334,12 @@ void spin_sweep(umc_chain* c, double beta, double* rec)
             ising_packed_pass<<<g, kBlock, 0, c->stream>>>(a);
         } else if (c->stencil) {
             StencilTopo t{uint32_t(c->dims[0] / 2), uint32_t(c->dims[1]), uint32_t(c->dims[2]), uint32_t(c->n / 2), p,
-                          c->dims[1] > 1 ? 1u : 0u, c->dims[2] > 1 ? 1u : 0u};
+                          c->dims[1] > 1 ? 1u : 0u, c->dims[2] > 1 ? 1u : 0u, 0xFFu, 0xFFu};
+            const uint64_t H = c->dims[0] / 2, Ly = c->dims[1];
+            if ((H & (H - 1)) == 0 && (Ly & (Ly - 1)) == 0) {
+                t.hshift = uint32_t(__builtin_ctzll(H));
+                t.yshift = uint32_t(__builtin_ctzll(Ly));
+            }
             spin_pass(c, p, beta, kbase, o, t);
         } else {
             CsrTopo t{c->off.as<uint32_t>(), c->adj.as<uint32_t>(), uint32_t(c->class_start[p])};
@@ -332,12 +351,186 @@ void spin_sweep(umc_chain* c, double beta, double* rec)
     c->sweeps++;
 }
 
+template <int MODEL, int TX, int TY, int TZ>
+void launch_tiled(umc_chain* c, WolffTileArgs& t)
+{
+    t.ntx = uint32_t((t.Lx + TX - 1) / TX);
+    t.nty = uint32_t((t.Ly + TY - 1) / TY);
+    const uint32_t ntz = uint32_t((t.Lz + TZ - 1) / TZ);
+    {
+        LaunchScope ls(c, UMC_KERNEL_WOLFF_UNION);
+        wolff_tile_local<MODEL, TX, TY, TZ><<<t.ntx * t.nty * ntz, TX * TY * TZ, 0, c->stream>>>(t);
+    }
+    const uint32_t g = grid_for(c, c->n);
+    {
+        LaunchScope ls(c, UMC_KERNEL_WOLFF_MERGE);
+        wolff_tile_merge<<<g, kBlock, 0, c->stream>>>(t);
+    }
+    {
+        LaunchScope ls(c, UMC_KERNEL_WOLFF_FLIP);
+        wolff_tile_flip<MODEL><<<g, kBlock, 0, c->stream>>>(t);
+    }
+}
+
+template <int MODEL>
+void launch_tiled_dims(umc_chain* c, WolffTileArgs& t)
+{
+    if (t.Lz > 1) launch_tiled<MODEL, 8, 8, 8>(c, t);
+    else launch_tiled<MODEL, 32, 16, 1>(c, t);
+}
+
+// Wolff flip on a regular lattice: tiled union-find (umc_wolff_tiled.cuh).
+void stencil_flip(umc_chain* c, double beta, unsigned long long* size_slot)
+{
+    if (!c->lab0.p) {
+        c->lab0.alloc(c->n * 4, "Wolff labels");
+        c->lab1.alloc(c->n, "Wolff crossing bonds");
+    }
+    WolffTileArgs t{};
+    t.field = c->field.p;
+    t.label = c->lab0.as<uint32_t>();
+    t.cross = c->lab1.as<uint8_t>();
+    t.n = uint32_t(c->n);
+    t.half = uint32_t(c->n / 2);
+    t.Lx = uint32_t(c->dims[0]);
+    t.Ly = uint32_t(c->dims[1]);
+    t.Lz = uint32_t(c->dims[2]);
+    t.ndir = (t.Lx > 1) + (t.Ly > 1) + (t.Lz > 1);
+    t.seed = c->desc.seed;
+    t.flip = c->flips;
+    t.J = c->J;
+    t.beta = float(beta);
+    if (c->model == UMC_MODEL_ISING) {
+        if (!c->cw_valid || c->cw_beta != beta) {
+            ising_wolff_thresholds(c->J_int, beta, c->cw);
+            c->cw_beta = beta;
+            c->cw_valid = true;
+        }
+        t.cw[0] = c->cw[0];
+        t.cw[1] = c->cw[1];
+    }
+    t.ctl = c->ctl.as<DevCtl>();
+    t.size_slot = size_slot;
+    switch (c->model == UMC_MODEL_ISING ? 0 : c->N) {
+    case 0: launch_tiled_dims<0>(c, t); break;
+    case 1: launch_tiled_dims<1>(c, t); break;
+    case 2: launch_tiled_dims<2>(c, t); break;
+    case 3: launch_tiled_dims<3>(c, t); break;
+    default: launch_tiled_dims<4>(c, t); break;
+    }
+    launch_check("Wolff flip (tiled)");
+}
+
+// Fused step on a regular lattice (umc_fused.cuh): returns false when the
+// chain does not qualify or cooperative launch is unavailable, in which case
+// the caller runs the multi-kernel path.
+template <int N, int TX, int TY, int TZ>
+bool launch_fused_t(umc_chain* c, FusedArgs& a)
+{
+    auto kern = hybrid_fused<N, TX, TY, TZ>;
+    constexpr int T = TX * TY * TZ;
+    if (c->fused_grid < 0) {
+        int coop = 0, nb = 0, sms = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, T, 0) != cudaSuccess) {
+            cudaGetLastError();
+            nb = 0;
+        }
+        c->fused_grid = coop ? std::min<int>(nb * sms, int(c->max_grid)) : 0;
+    }
+    if (c->fused_grid <= 0) return false;
+    a.w.ntx = uint32_t((a.w.Lx + TX - 1) / TX);
+    a.w.nty = uint32_t((a.w.Ly + TY - 1) / TY);
+    void* args[] = {&a};
+    LaunchScope ls(c, UMC_KERNEL_FUSED);
+    const cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kern), dim3(c->fused_grid), dim3(T), args, 0,
+                                                      c->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        c->fused_grid = 0;
+        c->launches[UMC_KERNEL_FUSED]--;
+        return false;
+    }
+    return true;
+}
+
+template <int N>
+bool launch_fused_n(umc_chain* c, FusedArgs& a)
+{
+    if (a.w.Lz > 1) return launch_fused_t<N, 8, 8, 8>(c, a);
+    return launch_fused_t<N, 32, 16, 1>(c, a);
+}
+
+bool fused_step(umc_chain* c, double beta, bool wolff, bool sweep, double* rec, unsigned long long* size_slot)
+{
+    if (!c->fused || !c->stencil || c->model != UMC_MODEL_VECTOR) return false;
+    if (wolff && c->desc.wolff_axis != UMC_AXIS_SPHERE) return false;
+    if (sweep && c->desc.proposal != UMC_PROPOSAL_SPHERE && c->desc.proposal != UMC_PROPOSAL_ROTATION) return false;
+    if (c->dims[0] / 2 > 0xFFFFFFFFull) return false;
+    if (wolff && !c->lab0.p) {
+        c->lab0.alloc(c->n * 4, "Wolff labels");
+        c->lab1.alloc(c->n, "Wolff crossing bonds");
+    }
+    FusedArgs a{};
+    WolffTileArgs& t = a.w;
+    t.field = c->field.p;
+    t.label = c->lab0.as<uint32_t>();
+    t.cross = c->lab1.as<uint8_t>();
+    t.n = uint32_t(c->n);
+    t.half = uint32_t(c->n / 2);
+    t.Lx = uint32_t(c->dims[0]);
+    t.Ly = uint32_t(c->dims[1]);
+    t.Lz = uint32_t(c->dims[2]);
+    t.ndir = (t.Lx > 1) + (t.Ly > 1) + (t.Lz > 1);
+    t.seed = c->desc.seed;
+    t.flip = c->flips;
+    t.J = c->J;
+    t.beta = float(beta);
+    t.ctl = c->ctl.as<DevCtl>();
+    t.size_slot = size_slot;
+    a.bar = &c->ctl.as<DevCtl>()->bar;
+    a.do_wolff = wolff ? 1u : 0u;
+    a.do_sweep = sweep ? 1u : 0u;
+    a.H = uint32_t(c->dims[0] / 2);
+    a.hshift = a.yshift = 0xFFu;
+    const uint64_t H = c->dims[0] / 2, Ly = c->dims[1];
+    if ((H & (H - 1)) == 0 && (Ly & (Ly - 1)) == 0) {
+        a.hshift = uint32_t(__builtin_ctzll(H));
+        a.yshift = uint32_t(__builtin_ctzll(Ly));
+    }
+    a.sweep_kbase = key_base(key_seed(c->desc.seed, c->sweeps, tag_site(0)));
+    a.beta_metro = float(beta);
+    a.proposal = c->desc.proposal == UMC_PROPOSAL_ROTATION ? kPropRotation : kPropSphere;
+    a.delta = float(c->desc.width);
+    a.out = PassOut{c->ctl.as<DevCtl>(), c->partials.as<double>(), sweep ? rec : nullptr, nullptr, kMaxPasses - 2, 1, 1};
+    bool ok = false;
+    switch (c->N) {
+    case 1: ok = launch_fused_n<1>(c, a); break;
+    case 2: ok = launch_fused_n<2>(c, a); break;
+    case 3: ok = launch_fused_n<3>(c, a); break;
+    default: ok = launch_fused_n<4>(c, a); break;
+    }
+    if (!ok) return false;
+    if (wolff) c->flips++;
+    if (sweep) c->sweeps++;
+    return true;
+}
+
 // One Wolff flip of a spin model.
 void spin_flip(umc_chain* c, double beta, double* rec, unsigned long long* size_slot)
 {
     if (c->model == UMC_MODEL_XY_ANGLE || c->desc.wolff_axis == UMC_AXIS_NONE)
         throw Error(UMC_ERR_UNSUPPORTED, "Wolff needs a reflection axis (FixedAxis for Ising, UniformSphereN for VectorSpin)");
     if (!c->symmetric) throw Error(UMC_ERR_UNSUPPORTED, "Wolff needs a symmetric graph");
+    if (c->stencil) {
+        if (!fused_step(c, beta, true, false, nullptr, size_slot)) {
+            stencil_flip(c, beta, size_slot);
+            c->flips++;
+        }
+        if (rec) observe_into(c, rec, size_slot);
+        return;
+    }
     ensure_csr(c);
     ensure_labels(c);
     WolffArgs a{};
@@ -400,12 +593,13 @@ void check_status(umc_chain* c)
     cuda_check(cudaMemcpyAsync(&st, &c->ctl.as<DevCtl>()->status, sizeof st, cudaMemcpyDeviceToHost, c->stream), "read status");
     cuda_check(cudaStreamSynchronize(c->stream), "synchronise chain");
     if (st) {
-        const unsigned int zero = 0;
-        cuda_check(cudaMemcpy(&c->ctl.as<DevCtl>()->status, &zero, sizeof zero, cudaMemcpyHostToDevice), "clear status");
+        // tickets and the barrier may be mid-count after an aborted kernel
+        cuda_check(cudaMemset(c->ctl.p, 0, sizeof(DevCtl)), "clear control block");
         std::string m = "device-side bound exhausted:";
         if (st & kDevErrUnionFind) m += " union-find";
         if (st & kDevErrGeometry) m += " geometry";
         if (st & kDevErrRetry) m += " proposal-retry";
+        if (st & kDevErrBarrier) m += " grid-barrier";
         throw Error(UMC_ERR_DEVICE_TIMEOUT, m);
     }
 }
@@ -499,10 +693,12 @@ void create_chain(const umc_chain_desc* d, umc_chain* c)
         c->stencil = g->stencil;
         std::memcpy(c->dims, g->dims, sizeof c->dims);
         c->max_degree = g->max_degree;
-        c->h_off = g->c_offset;
-        c->h_adj = g->c_bonds;
-        c->h_slot = g->c_slot_edge;
-        c->h_position = g->col.position;
+        if (g->materialized) {
+            c->h_off = g->c_offset;
+            c->h_adj = g->c_bonds;
+            c->h_slot = g->c_slot_edge;
+            c->h_position = g->col.position;
+        }
         if (c->n_colours > uint32_t(kMaxPasses - 1))
             throw Error(UMC_ERR_UNSUPPORTED, "graph needs more colour classes than the engine supports (63)");
         validate_proposal(c, c->desc.proposal, c->desc.width, c->desc.hits);
@@ -633,6 +829,7 @@ void enqueue_hybrid(umc_chain* c, double beta, uint64_t n)
     if (!is_spin(c)) throw Error(UMC_ERR_UNSUPPORTED, "Wolff is defined for spin models only (driver.hpp:73-84)");
     for (uint64_t k = 0; k < n; ++k) {
         const uint64_t r = next_record(c);
+        if (fused_step(c, beta, true, true, record_ptr(c, r), size_ptr(c, r))) continue;
         spin_flip(c, beta, nullptr, size_ptr(c, r));
         spin_sweep(c, beta, record_ptr(c, r));
     }
@@ -910,6 +1107,14 @@ int umc_chain_fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t cap
         if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
         device_scope(c);
         fetch(c, records, sizes, capacity, n_records);
+    });
+}
+
+int umc_chain_set_fused(umc_chain* c, int enable)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        c->fused = enable != 0;
     });
 }
 

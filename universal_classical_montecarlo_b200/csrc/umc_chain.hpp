@@ -90,6 +90,10 @@ struct umc_chain
     bool cw_valid = false;
     unsigned long long cw[2] = {0, 0};
 
+    // one cooperative kernel per step on regular lattices (umc_fused.cuh)
+    bool fused = true;
+    int fused_grid = -1;  // co-resident blocks; 0 = cooperative launch unavailable
+
     // learned proposal (U(1) only)
     void* learned = nullptr;
 

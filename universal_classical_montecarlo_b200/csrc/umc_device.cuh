@@ -26,12 +26,21 @@ constexpr int kBlock = 256;       // threads per block of the update kernels
 constexpr unsigned kDevErrUnionFind = 1u;   // union-find bound exhausted
 constexpr unsigned kDevErrGeometry = 2u;    // index outside a table
 constexpr unsigned kDevErrRetry = 4u;       // proposal retry bound exhausted
+constexpr unsigned kDevErrBarrier = 8u;     // grid barrier wait bound exhausted
+
+// counter + generation of the bounded grid barrier (umc_fused.cuh)
+struct GridBarrier
+{
+    unsigned int count;
+    unsigned int gen;
+};
 
 struct DevCtl
 {
     unsigned int ticket[kMaxPasses];
     unsigned int status;
     unsigned int pad;
+    GridBarrier bar;
     double pass_total[kMaxPasses][kObs];
 };
 
@@ -124,8 +133,17 @@ __device__ void finish_pass(double (&v)[V], const PassOut& o)
 }
 
 // ----------------------------------------------------------------- union-find
-// Labels only ever point to smaller indices, so every find terminates within
-// n steps; the bound exists to turn a logic error into a status bit.
+// Roots are linked by a fixed pseudorandom priority (a bijective hash of the
+// index): the lower-priority root goes under the higher one.  Linking by index
+// instead builds chains as long as a row of merging tiles (T2->T1, T3->T2, ...
+// when the unions run concurrently) and every later find walks them; random
+// priorities give expected logarithmic depth (randomised linking, Goel,
+// Khanna, Larkin & Tarjan 2014).  Labels only ever point to higher priority,
+// so every find terminates within n steps; the bound turns a logic error into
+// a status bit.  The components -- and so the Wolff clusters -- do not depend
+// on the linking order.
+__device__ __forceinline__ uint32_t uf_priority(uint32_t x) { return stream_id(x); }
+
 __device__ __forceinline__ uint32_t uf_find(uint32_t* lab, uint32_t x, uint32_t bound, unsigned* status)
 {
     volatile uint32_t* L = lab;
@@ -146,12 +164,12 @@ __device__ __forceinline__ void uf_union(uint32_t* lab, uint32_t a, uint32_t b, 
     b = uf_find(lab, b, bound, status);
     for (uint32_t it = 0; it < (1u << 22); ++it) {
         if (a == b) return;
-        if (a < b) {
+        if (uf_priority(a) > uf_priority(b)) {
             const uint32_t t = a;
             a = b;
             b = t;
         }
-        // link the larger root under the smaller one
+        // link the lower-priority root under the higher-priority one
         const uint32_t old = atomicCAS(lab + a, a, b);
         if (old == a) return;
         a = uf_find(lab, old, bound, status);

@@ -1,0 +1,255 @@
+// umc_fused.cuh -- one cooperative kernel per step on the regular lattices.
+//
+// On small lattices (64^3 fits in L2) a step is bounded by per-kernel fixed
+// costs, not by work: five launches (Wolff tile labelling, merge, flip, two
+// colour passes) each pay ramp-up, drain and a last-block reduction.  This
+// kernel runs the same phases back to back inside one launch, separated by a
+// grid barrier, with all blocks co-resident (cooperative launch):
+//
+//   A  Wolff: per tile, bond activation + shared-memory union-find  (optional)
+//   B  Wolff: union of tile-crossing bonds on the global labels     (optional)
+//   C  Wolff: reflect the seed's cluster                             (optional)
+//   D  Metropolis pass over colour class 0                           (optional)
+//   E  Metropolis pass over colour class 1, FP64 observables folded  (optional)
+//
+// The per-site arithmetic is shared with the multi-kernel path (same device
+// functions), so results are identical up to the order of the FP64 sums.
+//
+// The grid barrier is bounded: a block that waits longer than kBarrierSpins
+// polls raises kDevErrBarrier and leaves; the others then run out at their own
+// next barrier, so the kernel always terminates.  Data written before a
+// barrier by another block is read with L2-coherent loads (ld.global.cg).
+#pragma once
+
+#include "umc_wolff_tiled.cuh"
+
+namespace umc {
+
+constexpr unsigned kBarrierSpins = 1u << 22;  // x ~64 ns sleep: ~0.3 s
+
+__device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned* status)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile unsigned int* vgen = &b->gen;
+        const unsigned int g = *vgen;
+        __threadfence();
+        if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
+            atomicExch(&b->count, 0u);
+            __threadfence();
+            atomicAdd(&b->gen, 1u);
+        } else {
+            unsigned int it = 0;
+            while (*vgen == g) {
+                if (++it > kBarrierSpins) {
+                    atomicOr(status, kDevErrBarrier);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+struct FusedArgs
+{
+    WolffTileArgs w;  // Wolff phases (w.field is the field)
+    GridBarrier* bar;
+    uint32_t do_wolff, do_sweep;
+    uint32_t H, hshift, yshift;
+    uint64_t sweep_kbase;  // key base of this sweep's site streams
+    float beta_metro;
+    uint32_t proposal;  // kPropSphere / kPropRotation
+    float delta;
+    PassOut out;        // record of the sweep (pass index: dedicated slot)
+};
+
+template <int N>
+__device__ __forceinline__ void fused_site(const FusedArgs& a, const StencilTopo& t, uint32_t k, double* acc)
+{
+    float* f = static_cast<float*>(a.w.field);
+    const uint32_t n = a.w.n;
+    float s[N], h[N];
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+        s[c] = __ldcg(f + c * n + k);
+        h[c] = 0.0f;
+    }
+    t.neighbours(k, [&](uint32_t j, bool) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) h[c] += __ldcg(f + c * n + j);
+    });
+    KeyedPcg g = KeyedPcg::open(a.sweep_kbase, k);
+    float cand[N];
+    bool ok = true;
+    if (a.proposal == kPropSphere) sphere_sample<N>(g, cand);
+    else if constexpr (N >= 2) ok = local_rotation<N>(g, a.delta, s, cand);
+    bool acc_ok = false;
+    if (ok) {
+        const float dE = -a.w.J * (vdot<N>(cand, h) - vdot<N>(s, h));
+        acc_ok = metropolis_accept(g, -a.beta_metro * dE);
+    }
+    if (acc_ok) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+            s[c] = cand[c];
+            f[c * n + k] = cand[c];
+        }
+    }
+    // every bond joins the two classes: count it in the pass of class 1
+    if (t.colour == 1u) acc[0] += double(-a.w.J * vdot<N>(s, h));
+#pragma unroll
+    for (int c = 0; c < N; ++c) acc[1 + c] += double(s[c]);
+    acc[7] += acc_ok ? 1.0 : 0.0;
+}
+
+// MODEL = N >= 1 (VectorSpin<N>).  Block = one tile of TX*TY*TZ threads.
+template <int MODEL, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TX * TY * TZ, 2) hybrid_fused(FusedArgs a)
+{
+    constexpr int N = MODEL;
+    constexpr int T = TX * TY * TZ;
+    __shared__ uint32_t lab[T];
+    __shared__ float r_sh[4];
+    __shared__ uint32_t root_sh;
+    const WolffTileArgs& w = a.w;
+    unsigned* status = &w.ctl->status;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t gtid = blockIdx.x * blockDim.x + tid, gsize = gridDim.x * blockDim.x;
+
+    if (a.do_wolff) {
+        KeyedPcg gax = KeyedPcg::open_key(w.seed, w.flip, kTagAxis, 0);
+        if (tid == 0) {
+            float r[N];
+            sphere_sample<N>(gax, r);
+            for (int c = 0; c < N; ++c) r_sh[c] = r[c];
+            if (blockIdx.x == 0) *w.size_slot = 0ull;
+        }
+        // ---- A: tiles
+        const uint32_t ntz = (w.Lz + TZ - 1) / TZ;
+        const uint32_t ntiles = w.ntx * w.nty * ntz;
+        const uint64_t kb = key_base(key_seed(w.seed, w.flip, kTagBond));
+        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            __syncthreads();
+            lab[tid] = tid;
+            __syncthreads();
+            float r[N];
+#pragma unroll
+            for (int c = 0; c < N; ++c) r[c] = r_sh[c];
+            const uint32_t bx = tile % w.ntx, byz = tile / w.ntx;
+            const uint32_t by = byz % w.nty, bz = byz / w.nty;
+            const uint32_t tx = tid % TX, ty = (tid / TX) % TY, tz = tid / (TX * TY);
+            const uint32_t x = bx * TX + tx, y = by * TY + ty, z = bz * TZ + tz;
+            const bool valid = x < w.Lx && y < w.Ly && z < w.Lz;
+            uint32_t cross = 0, nat = 0;
+            if (valid) {
+                nat = (z * w.Ly + y) * w.Lx + x;
+                float si[N];
+                load_spin<N>(w.field, w.n, colour_major(nat, x, y, z, w.half), si);
+                const float ri = vdot<N>(si, r);
+                uint32_t rank = 0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const uint32_t L = d == 0 ? w.Lx : (d == 1 ? w.Ly : w.Lz);
+                    if (L < 2) continue;
+                    uint32_t xj = x, yj = y, zj = z;
+                    if (d == 0) xj = x + 1 == w.Lx ? 0 : x + 1;
+                    if (d == 1) yj = y + 1 == w.Ly ? 0 : y + 1;
+                    if (d == 2) zj = z + 1 == w.Lz ? 0 : z + 1;
+                    const uint32_t nj = (zj * w.Ly + yj) * w.Lx + xj;
+                    float sj[N];
+                    load_spin<N>(w.field, w.n, colour_major(nj, xj, yj, zj, w.half), sj);
+                    const uint32_t k = first_draw(kb, nat * w.ndir + rank);
+                    ++rank;
+                    if (!wolff_bond_active<N>(w.J, w.beta, w.cw, ri, vdot<N>(sj, r), 0, 0, k)) continue;
+                    if (xj / TX == bx && yj / TY == by && zj / TZ == bz) {
+                        const uint32_t tj = ((zj - bz * TZ) * TY + (yj - by * TY)) * TX + (xj - bx * TX);
+                        smem_union(lab, tid, tj, status);
+                    } else {
+                        cross |= 1u << d;
+                    }
+                }
+            }
+            __syncthreads();
+            if (valid) {
+                const uint32_t root = smem_find(lab, tid);
+                const uint32_t rx = root % TX, ry = (root / TX) % TY, rz = root / (TX * TY);
+                w.label[nat] = ((bz * TZ + rz) * w.Ly + (by * TY + ry)) * w.Lx + (bx * TX + rx);
+                w.cross[nat] = uint8_t(cross);
+            }
+        }
+        if (!grid_barrier(a.bar, status)) return;
+
+        // ---- B: tile-crossing bonds
+        for (uint32_t nat = gtid; nat < w.n; nat += gsize) {
+            const uint32_t cross = __ldcg(w.cross + nat);
+            if (!cross) continue;
+            const uint32_t x = nat % w.Lx, rr = nat / w.Lx, y = rr % w.Ly, z = rr / w.Ly;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (!(cross & (1u << d))) continue;
+                uint32_t xj = x, yj = y, zj = z;
+                if (d == 0) xj = x + 1 == w.Lx ? 0 : x + 1;
+                if (d == 1) yj = y + 1 == w.Ly ? 0 : y + 1;
+                if (d == 2) zj = z + 1 == w.Lz ? 0 : z + 1;
+                uf_union(w.label, nat, (zj * w.Ly + yj) * w.Lx + xj, w.n + 1, status);
+            }
+        }
+        if (!grid_barrier(a.bar, status)) return;
+
+        // ---- C: flip the seed's cluster
+        if (tid == 0) {
+            // seed site: next draw of the axis stream, colour-major -> natural
+            const uint32_t ks = uint32_t(u_f64(gax.next()) * double(w.n));
+            const uint32_t c = ks >= w.half ? 1u : 0u, rank = ks - c * w.half;
+            uint32_t nat = 2 * rank;
+            const uint32_t x = nat % w.Lx, rr = nat / w.Lx, y = rr % w.Ly, z = rr / w.Ly;
+            if (((x + y + z) & 1u) != c) ++nat;
+            root_sh = uf_find(w.label, nat, w.n + 1, status);
+        }
+        __syncthreads();
+        {
+            float r[N];
+#pragma unroll
+            for (int c = 0; c < N; ++c) r[c] = r_sh[c];
+            const uint32_t root = root_sh;
+            double cnt[1] = {0.0};
+            float* f = static_cast<float*>(w.field);
+            for (uint32_t nat = gtid; nat < w.n; nat += gsize) {
+                if (uf_find(w.label, nat, w.n + 1, status) != root) continue;
+                cnt[0] += 1.0;
+                const uint32_t x = nat % w.Lx, rr = nat / w.Lx, y = rr % w.Ly, z = rr / w.Ly;
+                const uint32_t k = colour_major(nat, x, y, z, w.half);
+                float si[N];
+#pragma unroll
+                for (int c = 0; c < N; ++c) si[c] = __ldcg(f + c * w.n + k);
+                const float d = vdot<N>(si, r);
+#pragma unroll
+                for (int c = 0; c < N; ++c) f[c * w.n + k] = si[c] - 2.0f * d * r[c];
+            }
+            block_sum<1>(cnt);
+            if (tid == 0 && cnt[0] > 0.0) atomicAdd(w.size_slot, (unsigned long long)cnt[0]);
+        }
+        if (a.do_sweep && !grid_barrier(a.bar, status)) return;
+    }
+
+    if (a.do_sweep) {
+        double acc[kObs] = {0, 0, 0, 0, 0, 0, 0, 0};
+        StencilTopo t{a.H, w.Ly, w.Lz, w.half, 0u, w.Ly > 1 ? 1u : 0u, w.Lz > 1 ? 1u : 0u, a.hshift, a.yshift};
+        // ---- D: colour class 0
+        for (uint32_t q = gtid; q < w.half; q += gsize) fused_site<N>(a, t, q, acc);
+        if (!grid_barrier(a.bar, status)) return;
+        // ---- E: colour class 1, then the sweep's record
+        t.colour = 1u;
+        for (uint32_t q = gtid; q < w.n - w.half; q += gsize) fused_site<N>(a, t, w.half + q, acc);
+        finish_pass<kObs>(acc, a.out);
+    }
+}
+
+}  // namespace umc

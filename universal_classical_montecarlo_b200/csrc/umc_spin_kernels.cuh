@@ -48,12 +48,23 @@ struct StencilTopo
 {
     uint32_t H, Ly, Lz, half, colour;
     uint32_t hasy, hasz;
+    uint32_t hshift, yshift;  // log2(H), log2(Ly) when both are powers of two, else 0xFF
     template <class F>
     __device__ __forceinline__ void neighbours(uint32_t k, F&& f) const
     {
         const uint32_t j = k - colour * half;
-        const uint32_t row = j / H, i = j - row * H;
-        const uint32_t y = row % Ly, z = row / Ly;
+        uint32_t row, i, y, z;
+        if (hshift != 0xFFu) {  // uniform branch: shifts instead of integer division
+            row = j >> hshift;
+            i = j & (H - 1);
+            y = row & (Ly - 1);
+            z = row >> yshift;
+        } else {
+            row = j / H;
+            i = j - row * H;
+            y = row % Ly;
+            z = row / Ly;
+        }
         const uint32_t p = (y + z + colour) & 1u;
         const uint32_t ob = (1u - colour) * half;
         const bool early = colour == 1u;
@@ -201,13 +212,16 @@ __device__ __forceinline__ void sphere_sample(KeyedPcg& g, float* out)
     if constexpr (N == 1) {
         out[0] = g.next() < 0x80000000u ? -1.0f : 1.0f;  // u < 0.5
     } else if constexpr (N == 2) {
+        // angle 2 pi u = a + pi with a = pi (2u - 1) in [-pi, pi), where the
+        // hardware sine/cosine are accurate to ~4e-7
         float sn, cs;
-        sincospif(twice_u_f32(g.next()), &sn, &cs);
-        out[0] = cs;
-        out[1] = sn;
+        __sincosf(3.14159265358979f * sym_f32(g.next()), &sn, &cs);
+        out[0] = -cs;
+        out[1] = -sn;
     } else {
         const float z = sym_f32(g.next());
-        const float r = sqrtf((1.0f - z) * (1.0f + z));
+        const float w = (1.0f - z) * (1.0f + z);
+        const float r = w > 0.0f ? w * rsqrtf(w) : 0.0f;
         sphere_sample<N - 1>(g, out);
 #pragma unroll
         for (int k = 0; k < N - 1; ++k) out[k] *= r;
@@ -251,7 +265,7 @@ __device__ __forceinline__ bool local_rotation(KeyedPcg& g, float delta, const f
     if (!ok) return false;
     const float th = delta * sym_f32(g.next());
     float sn, cs;
-    sincosf(th, &sn, &cs);
+    __sincosf(th, &sn, &cs);
     const float cu = vdot<N>(u, cur), cv = vdot<N>(v, cur);
 #pragma unroll
     for (int k = 0; k < N; ++k) out[k] = cur[k] + (cs - 1.0f) * (cu * u[k] + cv * v[k]) + sn * (cu * v[k] - cv * u[k]);
@@ -269,7 +283,7 @@ __device__ __forceinline__ float u1_shift(KeyedPcg& g, float width, float cur)
 __device__ __forceinline__ bool metropolis_accept(KeyedPcg& g, float log_p)
 {
     if (log_p >= 0.0f) return true;
-    return logf(u_f32(g.next())) < log_p;
+    return u_f32(g.next()) < __expf(log_p);  // log(u) < log_p, monotone-equivalent
 }
 
 // ------------------------------------------------------ VectorSpin<N> pass
@@ -355,7 +369,7 @@ __global__ void __launch_bounds__(kBlock) xy_pass(XYArgs a, Topo t)
         float C = 0.f, S = 0.f, Ce = 0.f, Se = 0.f;
         t.neighbours(k, [&](uint32_t j, bool early) {
             float sn, cs;
-            sincosf(a.th[j], &sn, &cs);
+            __sincosf(a.th[j], &sn, &cs);
             C += cs;
             S += sn;
             Ce += early ? cs : 0.f;
@@ -365,8 +379,8 @@ __global__ void __launch_bounds__(kBlock) xy_pass(XYArgs a, Topo t)
         KeyedPcg g = KeyedPcg::open(a.kbase, k);
         const float p = u1_shift(g, a.width, th);
         float so, co, sp, cp;
-        sincosf(th, &so, &co);
-        sincosf(p, &sp, &cp);
+        __sincosf(th, &so, &co);
+        __sincosf(p, &sp, &cp);
         const float dE = -a.J * ((cp - co) * C + (sp - so) * S);
         const bool ok = metropolis_accept(g, -a.beta * dE);
         if (ok) {
@@ -455,6 +469,23 @@ struct WolffArgs
     unsigned long long* size_slot;
 };
 
+// Activation of one bond (driver.hpp:150-151): uni() < 1 - exp(-beta dE).
+// The reference's energy_diff_bond, -J (nb.s_i - s_j.s_i) with the reflected
+// nb = s_j - 2 (s_j.r) r, equals 2 J (r.s_i)(r.s_j); that symmetric form is
+// used so the decision does not depend on which end reaches the bond first.
+// Ising compares the draw with integer thresholds (exact); ri, rj unused.
+template <int MODEL>
+__device__ __forceinline__ bool wolff_bond_active(float J, float beta, const unsigned long long* cw, float ri, float rj,
+                                                  int si, int sj, uint32_t k)
+{
+    if constexpr (MODEL == 0) {
+        return uint64_t(k) < cw[si * sj > 0 ? 1 : 0];
+    } else {
+        const float dE = 2.0f * J * (ri * rj);
+        return u_f32(k) < 1.0f - __expf(-beta * dE);
+    }
+}
+
 // Axis and seed site of one flip (driver.hpp:110-115), from the axis key.
 template <int MODEL>
 __device__ __forceinline__ uint32_t wolff_axis(const WolffArgs& a, float* r)
@@ -490,27 +521,23 @@ __global__ void __launch_bounds__(kBlock) wolff_union(WolffArgs a)
                 const uint32_t j = a.adj[q];
                 if (j <= i) continue;
                 const uint32_t k = first_draw(kb, a.slot[q]);
-                if (uint64_t(k) < a.cw[si * int32_t(s[j]) > 0 ? 1 : 0]) uf_union(a.lab, i, j, a.n + 1, &a.ctl->status);
+                if (wolff_bond_active<0>(a.J, a.beta, a.cw, 0.f, 0.f, si, s[j], k)) uf_union(a.lab, i, j, a.n + 1, &a.ctl->status);
             }
         } else {
             const float* f = static_cast<const float*>(a.field);
             float si[N];
 #pragma unroll
             for (int c = 0; c < N; ++c) si[c] = f[c * a.n + i];
+            const float ri = vdot<N>(si, r);
             for (uint32_t q = a0; q < a1; ++q) {
                 const uint32_t j = a.adj[q];
                 if (j <= i) continue;
-                float t[N], nb[N];
+                float t[N];
 #pragma unroll
                 for (int c = 0; c < N; ++c) t[c] = f[c * a.n + j];
-                const float d = vdot<N>(t, r);
-#pragma unroll
-                for (int c = 0; c < N; ++c) nb[c] = t[c] - 2.0f * d * r[c];
-                // energy_diff_bond, example/vector_spin.hpp:63-69
-                const float dE = -a.J * (vdot<N>(nb, si) - vdot<N>(t, si));
-                const float p = 1.0f - expf(-a.beta * dE);
                 const uint32_t k = first_draw(kb, a.slot[q]);
-                if (u_f32(k) < p) uf_union(a.lab, i, j, a.n + 1, &a.ctl->status);
+                if (wolff_bond_active<MODEL>(a.J, a.beta, a.cw, ri, vdot<N>(t, r), 0, 0, k))
+                    uf_union(a.lab, i, j, a.n + 1, &a.ctl->status);
             }
         }
     }

@@ -99,10 +99,11 @@ Colouring colour_graph(uint64_t n, const std::vector<uint32_t>& off, const std::
 void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 const char* last_error() { return g_last_error.c_str(); }
 
-umc_graph* make_graph(uint64_t n, const uint32_t* ei, const uint32_t* ej, uint64_t m, bool symmetric,
-                      Lattice kind, const uint64_t dims[3])
+namespace {
+// Fills g's tables from an edge list (lattice/pair_graph.hpp:49-83: same
+// checks, same exceptions); g->kind and g->dims must already be set.
+void fill_graph(umc_graph* g, uint64_t n, const uint32_t* ei, const uint32_t* ej, uint64_t m, bool symmetric)
 {
-    // lattice/pair_graph.hpp:49-83: same checks, same exceptions.
     if (n > kMax32) throw Error(UMC_ERR_OVERFLOW, "PairGraph: site count exceeds uint32_t");
     if (m && (!ei || !ej)) throw Error(UMC_ERR_INVALID_ARGUMENT, "PairGraph: null edge arrays");
     std::vector<uint64_t> degree(n, 0);
@@ -112,11 +113,9 @@ umc_graph* make_graph(uint64_t n, const uint32_t* ei, const uint32_t* ej, uint64
         ++degree[ei[e]];
         if (symmetric) ++degree[ej[e]];
     }
-    auto* g = new umc_graph;
     g->n = n;
     g->symmetric = symmetric;
-    g->kind = kind;
-    if (dims) std::memcpy(g->dims, dims, sizeof g->dims);
+    g->max_degree = 0;
     g->ei.assign(ei, ei + m);
     g->ej.assign(ej, ej + m);
     g->offset.assign(n + 1, 0);
@@ -124,10 +123,7 @@ umc_graph* make_graph(uint64_t n, const uint32_t* ei, const uint32_t* ej, uint64
     for (uint64_t i = 0; i < n; ++i) {
         g->offset[i] = uint32_t(total);
         total += degree[i];
-        if (total > kMax32) {
-            delete g;
-            throw Error(UMC_ERR_OVERFLOW, "PairGraph: bond count exceeds uint32_t");
-        }
+        if (total > kMax32) throw Error(UMC_ERR_OVERFLOW, "PairGraph: bond count exceeds uint32_t");
         g->max_degree = std::max<uint32_t>(g->max_degree, uint32_t(degree[i]));
     }
     if (n) g->offset[n] = uint32_t(total);
@@ -186,7 +182,7 @@ umc_graph* make_graph(uint64_t n, const uint32_t* ei, const uint32_t* ej, uint64
     // The regular-lattice kernels reproduce this graph exactly when every
     // extent is 1 or even (x even >= 2): then the two-colouring is
     // (x + y + z) & 1 and colour-major index = colour * n/2 + site/2.
-    if (kind == Lattice::Square || kind == Lattice::Cubic) {
+    if (g->kind == Lattice::Square || g->kind == Lattice::Cubic) {
         const uint64_t Lx = g->dims[0], Ly = g->dims[1], Lz = g->dims[2];
         bool ok = Lx >= 2 && Lx % 2 == 0 && (Ly == 1 || Ly % 2 == 0) && (Lz == 1 || Lz % 2 == 0);
         if (ok && g->col.n_colours == 2) {
@@ -200,36 +196,16 @@ umc_graph* make_graph(uint64_t n, const uint32_t* ei, const uint32_t* ej, uint64
         }
         g->stencil = ok;
     }
-    return g;
+    g->materialized = true;
 }
 
-umc_graph* make_square(uint64_t Lx, uint64_t Ly)
+// Edge list of the periodic square / cubic builders (lattice/square.hpp:27-35,
+// extended to z): per site a +x, +y, +z edge when that extent exceeds 1.
+void lattice_edges(uint64_t Lx, uint64_t Ly, uint64_t Lz, std::vector<uint32_t>& ei, std::vector<uint32_t>& ej)
 {
-    // lattice/square.hpp:15-38
-    if (Lx == 0 || Ly == 0) throw Error(UMC_ERR_INVALID_ARGUMENT, "square_lattice: Lx and Ly must be positive");
-    if (Lx > std::numeric_limits<uint64_t>::max() / Ly) throw Error(UMC_ERR_OVERFLOW, "square_lattice: site count overflows size_t");
-    const uint64_t n = Lx * Ly;
-    if (n > kMax32) throw Error(UMC_ERR_OVERFLOW, "square_lattice: site count exceeds uint32_t");
-    std::vector<uint32_t> ei, ej;
-    ei.reserve(2 * n);
-    ej.reserve(2 * n);
-    for (uint64_t y = 0; y < Ly; ++y)
-        for (uint64_t x = 0; x < Lx; ++x) {
-            const uint32_t i = uint32_t(y * Lx + x);
-            if (Lx > 1) { ei.push_back(i); ej.push_back(uint32_t(y * Lx + (x + 1) % Lx)); }
-            if (Ly > 1) { ei.push_back(i); ej.push_back(uint32_t(((y + 1) % Ly) * Lx + x)); }
-        }
-    const uint64_t dims[3] = {Lx, Ly, 1};
-    return make_graph(n, ei.data(), ej.data(), ei.size(), true, Lattice::Square, dims);
-}
-
-umc_graph* make_cubic(uint64_t Lx, uint64_t Ly, uint64_t Lz)
-{
-    if (Lx == 0 || Ly == 0 || Lz == 0) throw Error(UMC_ERR_INVALID_ARGUMENT, "cubic_lattice: extents must be positive");
-    if (Lx > kMax32 || Ly > kMax32 || Lz > kMax32 || Lx * Ly > kMax32 || Lx * Ly * Lz > kMax32)
-        throw Error(UMC_ERR_OVERFLOW, "cubic_lattice: site count exceeds uint32_t");
     const uint64_t n = Lx * Ly * Lz;
-    std::vector<uint32_t> ei, ej;
+    ei.clear();
+    ej.clear();
     ei.reserve(3 * n);
     ej.reserve(3 * n);
     for (uint64_t z = 0; z < Lz; ++z)
@@ -240,8 +216,82 @@ umc_graph* make_cubic(uint64_t Lx, uint64_t Ly, uint64_t Lz)
                 if (Ly > 1) { ei.push_back(i); ej.push_back(uint32_t((z * Ly + (y + 1) % Ly) * Lx + x)); }
                 if (Lz > 1) { ei.push_back(i); ej.push_back(uint32_t((((z + 1) % Lz) * Ly + y) * Lx + x)); }
             }
-    const uint64_t dims[3] = {Lx, Ly, Lz};
-    return make_graph(n, ei.data(), ej.data(), ei.size(), true, Lattice::Cubic, dims);
+}
+
+// A regular lattice whose kernels need no table: keep n, extents, degree and
+// the two colour classes; the tables are built on first request.
+umc_graph* make_regular(Lattice kind, uint64_t Lx, uint64_t Ly, uint64_t Lz)
+{
+    const uint64_t n = Lx * Ly * Lz;
+    const uint64_t ndir = (Lx > 1) + (Ly > 1) + (Lz > 1);
+    if (2 * ndir * n > kMax32) throw Error(UMC_ERR_OVERFLOW, "PairGraph: bond count exceeds uint32_t");
+    const bool closed = Lx >= 2 && Lx % 2 == 0 && (Ly == 1 || Ly % 2 == 0) && (Lz == 1 || Lz % 2 == 0);
+    auto* g = new umc_graph;
+    g->kind = kind;
+    g->dims[0] = Lx;
+    g->dims[1] = Ly;
+    g->dims[2] = Lz;
+    if (!closed) {
+        std::vector<uint32_t> ei, ej;
+        lattice_edges(Lx, Ly, Lz, ei, ej);
+        try {
+            fill_graph(g, n, ei.data(), ej.data(), ei.size(), true);
+        } catch (...) {
+            delete g;
+            throw;
+        }
+        return g;
+    }
+    g->n = n;
+    g->symmetric = true;
+    g->max_degree = uint32_t(2 * ndir);
+    g->col.n_colours = 2;
+    g->col.class_start = {0, n / 2, n};
+    g->stencil = true;
+    g->materialized = false;
+    return g;
+}
+}  // namespace
+
+umc_graph* make_graph(uint64_t n, const uint32_t* ei, const uint32_t* ej, uint64_t m, bool symmetric,
+                      Lattice kind, const uint64_t dims[3])
+{
+    auto* g = new umc_graph;
+    g->kind = kind;
+    if (dims) std::memcpy(g->dims, dims, sizeof g->dims);
+    try {
+        fill_graph(g, n, ei, ej, m, symmetric);
+    } catch (...) {
+        delete g;
+        throw;
+    }
+    return g;
+}
+
+void materialize(const umc_graph* cg)
+{
+    if (cg->materialized) return;
+    auto* g = const_cast<umc_graph*>(cg);  // the lazy tables are a cache of the extents
+    std::vector<uint32_t> ei, ej;
+    lattice_edges(g->dims[0], g->dims[1], g->dims[2], ei, ej);
+    fill_graph(g, g->n, ei.data(), ej.data(), ei.size(), true);
+}
+
+umc_graph* make_square(uint64_t Lx, uint64_t Ly)
+{
+    // lattice/square.hpp:15-38
+    if (Lx == 0 || Ly == 0) throw Error(UMC_ERR_INVALID_ARGUMENT, "square_lattice: Lx and Ly must be positive");
+    if (Lx > std::numeric_limits<uint64_t>::max() / Ly) throw Error(UMC_ERR_OVERFLOW, "square_lattice: site count overflows size_t");
+    if (Lx * Ly > kMax32) throw Error(UMC_ERR_OVERFLOW, "square_lattice: site count exceeds uint32_t");
+    return make_regular(Lattice::Square, Lx, Ly, 1);
+}
+
+umc_graph* make_cubic(uint64_t Lx, uint64_t Ly, uint64_t Lz)
+{
+    if (Lx == 0 || Ly == 0 || Lz == 0) throw Error(UMC_ERR_INVALID_ARGUMENT, "cubic_lattice: extents must be positive");
+    if (Lx > kMax32 || Ly > kMax32 || Lz > kMax32 || Lx * Ly > kMax32 || Lx * Ly * Lz > kMax32)
+        throw Error(UMC_ERR_OVERFLOW, "cubic_lattice: site count exceeds uint32_t");
+    return make_regular(Lattice::Cubic, Lx, Ly, Lz);
 }
 
 umc_cells* make_cells(uint64_t n_sites, uint32_t arity, const uint32_t* cells, uint64_t n_cells,
@@ -460,12 +510,17 @@ int umc_graph_cubic(uint64_t Lx, uint64_t Ly, uint64_t Lz, umc_graph** out)
 
 void umc_graph_destroy(umc_graph* g) { delete g; }
 uint64_t umc_graph_sites(const umc_graph* g) { return g ? g->n : 0; }
-uint64_t umc_graph_slots(const umc_graph* g) { return g ? g->bonds.size() : 0; }
+uint64_t umc_graph_slots(const umc_graph* g)
+{
+    if (!g) return 0;
+    return g->materialized ? g->bonds.size() : g->n * g->max_degree;
+}
 
 int umc_graph_csr(const umc_graph* g, uint32_t* offset, uint32_t* bonds)
 {
     return guarded([&] {
         if (!g) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "null graph");
+        umc::materialize(g);
         if (offset) std::copy(g->offset.begin(), g->offset.end(), offset);
         if (bonds) std::copy(g->bonds.begin(), g->bonds.end(), bonds);
     });
@@ -475,6 +530,7 @@ int umc_graph_colouring(const umc_graph* g, uint32_t* n_colours, uint32_t* colou
 {
     return guarded([&] {
         if (!g) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "null graph");
+        umc::materialize(g);
         fill_colouring(g->col, n_colours, colour, position);
     });
 }

@@ -47,6 +47,10 @@ struct umc_graph
     uint32_t max_degree = 0;
     // true when the regular-lattice stencil kernels reproduce this graph exactly
     bool stencil = false;
+    // regular lattices keep only their extents until a table is asked for
+    // (edge list, CSR, colouring arrays); n, degree and the colour classes are
+    // known in closed form
+    bool materialized = true;
 };
 
 // CellComplex<A> (lattice/cell_complex.hpp:21-87) plus the colour-major copy.
@@ -77,6 +81,8 @@ umc_graph* make_graph(uint64_t n, const uint32_t* ei, const uint32_t* ej, uint64
                       Lattice kind, const uint64_t dims[3]);
 umc_graph* make_square(uint64_t Lx, uint64_t Ly);
 umc_graph* make_cubic(uint64_t Lx, uint64_t Ly, uint64_t Lz);
+// Builds the edge list, CSR and colouring of a lazily created regular lattice.
+void materialize(const umc_graph* g);
 umc_cells* make_cells(uint64_t n_sites, uint32_t arity, const uint32_t* cells, uint64_t n_cells,
                       Lattice kind, uint64_t L, uint32_t dim);
 umc_cells* make_hypercubic(uint64_t L);
