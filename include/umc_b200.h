@@ -231,6 +231,60 @@ int umc_chain_kernel_stats(umc_chain* c, uint64_t* launches, double* device_ms, 
 /* Wolff::mean_cluster_size bookkeeping -- driver.hpp:193-196. */
 int umc_wolff_stats(const umc_chain* c, uint64_t* flips, double* size_sum);
 
+/* ============================================================ batched chains */
+
+/* Many independent XY chains (the angle model of UMC_MODEL_XY_ANGLE with
+ * U1Shift) on periodic L x L lattices, organised in replica-exchange ladders.
+ * No reference counterpart: the reference runs one chain per driver object
+ * (driver.hpp:17-68).  Chain c = ladder * replicas + k starts at temperature
+ * slot k of its ladder; every segment runs sweeps_per_exchange Metropolis
+ * sweeps of every chain at the beta of the slot it holds, then one exchange
+ * round per ladder: slots (k, k+1), k of the round's parity, swap their chains
+ * iff (beta_k - beta_{k+1})(E_k - E_{k+1}) >= 0 or log(u) < that product. */
+typedef struct umc_batch_desc {
+    uint32_t n_ladders;
+    uint32_t replicas;            /* temperature slots per ladder (<= 64)        */
+    const uint32_t* L;            /* side per ladder: even, in [2, 4096]         */
+    const double* betas;          /* n_ladders * replicas inverse temperatures   */
+    double coupling;              /* J                                           */
+    double width;                 /* U1Shift width                               */
+    uint32_t sweeps_per_exchange; /* 0: 10                                       */
+    uint64_t seed;
+    int32_t device;
+    void* stream;                 /* NULL: the batch owns one                    */
+    uint64_t max_records;         /* segments kept on the device (0: 1024)       */
+} umc_batch_desc;
+
+typedef struct umc_batch umc_batch;
+
+int umc_batch_create(const umc_batch_desc* desc, umc_batch** out);
+int umc_batch_destroy(umc_batch* b);
+/* Uniform angles 2 pi u on every chain (keys derived from seed and chain). */
+int umc_batch_randomize(umc_batch* b, uint64_t seed);
+/* One chain's angles in natural site order y*L + x. */
+int umc_batch_set_field(umc_batch* b, uint32_t chain, const float* theta);
+int umc_batch_get_field(umc_batch* b, uint32_t chain, float* theta);
+/* Queue n segments (a captured CUDA graph per segment). */
+int umc_batch_enqueue(umc_batch* b, uint64_t n_segments);
+/* Copy the records of the segments queued since the last fetch:
+ * n_records x (n_ladders * replicas) x UMC_OBS_STRIDE doubles, by temperature
+ * slot: [E, Mx, My, chain, beta, swap of (k, k+1) accepted, accepted
+ * updates, 0] taken at the end of the segment, before the exchange. */
+int umc_batch_fetch(umc_batch* b, double* records, uint64_t capacity, uint64_t* n_records);
+/* enqueue + fetch in chunks of max_records; records may be NULL. */
+int umc_batch_run(umc_batch* b, uint64_t n_segments, double* records);
+int umc_batch_counters(const umc_batch* b, uint64_t* sweeps, uint64_t* rounds, uint64_t* swaps_accepted);
+/* holder[l * replicas + k] = chain at slot k of ladder l. */
+int umc_batch_temperature_map(const umc_batch* b, uint32_t* holder);
+/* chain_seeds[c] keys chain c's site streams; ladder_seeds[l] its swaps. */
+int umc_batch_seeds(const umc_batch* b, uint64_t* chain_seeds, uint64_t* ladder_seeds);
+/* Launch shape the autotuner chose for the ladders of side L. */
+int umc_batch_config(const umc_batch* b, uint32_t L, uint32_t* chains_per_cta, uint32_t* ctas_per_chain,
+                     uint32_t* block);
+int umc_batch_sites(const umc_batch* b, uint64_t* total_sites, uint64_t* kernel_launches);
+/* The stream the batch's segments run on (cudaStream_t). */
+void* umc_batch_stream(const umc_batch* b);
+
 /* ================================================= allocation-free Wolff flip */
 
 /* No counterpart in the reference: an extra entry point for callers that cannot

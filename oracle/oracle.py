@@ -114,6 +114,7 @@ class Oracle:
         self._su_plaq = L.fn("su_mean_plaquette", _f64, _u32, _u64, _vp, _vp)
         self._su_expm = L.fn("su_expm", None, _u32, _vp, _vp)
         self._su_unit = L.fn("su_unitarity_error", _f64, _u32, _vp)
+        self._rex = L.fn("replica_exchange", _int, _u32, _vp, _vp, _vp, _u64, _u64, _u32, _vp)
 
     # ---- RNG
     def key_draws(self, seed, counter, tag, id_, n):
@@ -296,6 +297,15 @@ class Oracle:
         u = np.ascontiguousarray(u, np.complex128)
         return self._su_unit(N, _ptr(u))
 
+    def replica_exchange(self, betas, holder, energy, seed, round_, parity):
+        """One exchange round: returns (new holder, accepted flags per slot)."""
+        betas = np.ascontiguousarray(betas, np.float64)
+        h = np.array(holder, np.uint32, copy=True)
+        e = np.ascontiguousarray(energy, np.float64)
+        acc = np.zeros(len(h), np.uint8)
+        self._rex(len(h), _ptr(betas), _ptr(h), _ptr(e), seed, round_, parity, _ptr(acc))
+        return h, acc
+
 
 # ------------------------------------------------------------------ reference
 class Reference:
@@ -330,6 +340,7 @@ class Reference:
         self._su_shift = L.fn("su_shift", None, _u32, _f64, _u64, _u64, _u32, _u32, _vp, _vp)
         self._bench_o3 = L.fn("bench_o3", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._bench_ising = L.fn("bench_ising", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
+        self._bench_xy = L.fn("bench_xy", _int, _u64, _f64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
 
     def pcg32_draws(self, seed, stream, n):
         out = np.zeros(n, np.uint32)
@@ -484,6 +495,17 @@ class Reference:
         st = self._bench_ising(L, beta, warmup, sweeps, threads, seed, C.byref(su), C.byref(sec))
         assert st == 0, st
         return su.value, sec.value
+
+
+def _bench_xy(self, L, beta, width, warmup, sweeps, threads, seed=1):
+    su = C.c_double()
+    sec = C.c_double()
+    st = self._bench_xy(L, beta, width, warmup, sweeps, threads, seed, C.byref(su), C.byref(sec))
+    assert st == 0, st
+    return su.value, sec.value
+
+
+Reference.bench_xy = _bench_xy
 
 
 def have_reference() -> bool:

@@ -853,3 +853,39 @@ extern "C" int ref_bench_ising(std::uint64_t L, double beta, std::uint64_t warmu
         return status_of(std::current_exception());
     }
 }
+
+// Times the reference's stock XY model on angles: PairModel<U1Dof, -J cos> on an
+// L x L square_lattice with U1Shift{width} and a plain Pcg32, one chain per
+// thread, uniform random start.
+extern "C" int ref_bench_xy(std::uint64_t L, double beta, double width, std::uint64_t warmup, std::uint64_t sweeps,
+                            std::uint32_t threads, std::uint64_t seed, double* site_updates, double* seconds)
+{
+    try {
+        using PM = PairModel<U1Dof, XYAngleTerm, PairGraph<>>;
+        std::vector<double> secs(threads, 0.0);
+        std::vector<std::thread> pool;
+        for (std::uint32_t t = 0; t < threads; ++t)
+            pool.emplace_back([&, t] {
+                PM model(square_lattice(L, L), XYAngleTerm{1.0});
+                Pcg32 init(seed + t, 9);
+                for (std::size_t i = 0; i < model.sites(); ++i) {
+                    const U1Link l{6.283185307179586 * init.uni()};
+                    model.update(i, &l);
+                }
+                Metropolis<PM, U1Shift, Pcg32> mc(model, U1Shift{width}, Pcg32(seed + t, 1), beta);
+                mc.run(warmup);
+                const auto t0 = std::chrono::steady_clock::now();
+                mc.run(sweeps);
+                const auto t1 = std::chrono::steady_clock::now();
+                secs[t] = std::chrono::duration<double>(t1 - t0).count();
+            });
+        for (auto& th : pool) th.join();
+        double worst = 0.0;
+        for (double x : secs) worst = x > worst ? x : worst;
+        *site_updates = double(threads) * double(L * L) * double(sweeps);
+        *seconds = worst;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}

@@ -612,6 +612,31 @@ void orc_xy_metropolis(uint64_t n, const uint32_t* offset, const uint32_t* bonds
     }
 }
 
+/* ------------------------------------------------------- replica exchange */
+
+/* Parallel tempering swap between neighbouring temperature slots (project-
+ * defined; the reference has none): detailed balance for the joint ensemble
+ * with acceptance min(1, exp((beta_k - beta_{k+1}) (E_k - E_{k+1}))). */
+int orc_replica_exchange(uint32_t R, const double* betas, uint32_t* holder, const double* energy,
+                         uint64_t seed, uint64_t round, uint32_t parity, uint8_t* accepted)
+{
+    int n = 0;
+    for (uint32_t k = parity; k + 1 < R; k += 2) {
+        const uint32_t a = holder[k], b = holder[k + 1];
+        const double delta = (betas[k] - betas[k + 1]) * (energy[a] - energy[b]);
+        orc_pcg32 g;
+        orc_key_open(&g, seed, round, ORC_TAG_SWAP, k);
+        const int acc = delta >= 0.0 || log(orc_pcg32_uni(&g)) < delta;
+        if (accepted) accepted[k] = (uint8_t)acc;
+        if (acc) {
+            holder[k] = b;
+            holder[k + 1] = a;
+            ++n;
+        }
+    }
+    return n;
+}
+
 /* --------------------------------------------------------------------- U(1) */
 
 /* plaquette(t0..t3), dof/u1.hpp:18-21. */

@@ -127,6 +127,17 @@ void orc_xy_metropolis(uint64_t n, const uint32_t* offset, const uint32_t* bonds
                        double beta, double width, uint64_t seed, uint64_t sweep0,
                        uint64_t n_sweeps, double* theta, double* obs_out, double* margin_out);
 
+/* ---- replica exchange (no reference counterpart) ------------------------------
+ * One exchange round of a ladder of R replicas (temperature slots 0..R-1 with
+ * inverse temperatures betas[k]).  holder[k] = chain currently at slot k,
+ * energy[c] = energy of chain c.  Pairs (k, k+1) with k = parity, parity+2, ...
+ * are proposed; the swap is accepted iff Delta >= 0 or log(u) < Delta with
+ * Delta = (betas[k] - betas[k+1]) * (energy[holder[k]] - energy[holder[k+1]])
+ * and u the first draw of key (seed, round, ORC_TAG_SWAP, k).  accepted[k]
+ * (may be NULL) receives 1/0 per proposed pair.  Returns the number accepted. */
+int orc_replica_exchange(uint32_t R, const double* betas, uint32_t* holder, const double* energy,
+                         uint64_t seed, uint64_t round, uint32_t parity, uint8_t* accepted);
+
 /* ---- U(1) gauge on a cell complex (example/u1_gauge.hpp, model/cell.hpp + term/plaquette.hpp)
  * theta: n_links angles.  model_beta multiplies the action, driver_beta the exponent.
  * hits: number of U1Shift hits per link (multi-hit; 1 = the reference sweep).

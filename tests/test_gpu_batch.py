@@ -1,0 +1,105 @@
+"""Batched XY chains with replica-exchange ladders (umc_batch_*), through the C ABI.
+
+Every chain is checked segment by segment against the single-chain oracle
+(the reference's PairModel / U1Shift arithmetic on a checkerboard-relabelled
+square lattice, keyed by the chain's seed) and the exchange round against the
+oracle's swap rule, both from identical states.
+"""
+import numpy as np
+import pytest
+
+from helpers import checker_position, relabel_edges, square_edges
+
+pytestmark = pytest.mark.gpu
+
+TOL = 4e-5     # radians after one segment (10 sweeps)
+MARGIN = 1e-3
+
+
+def _geometric(lo, hi, R):
+    return lo * (hi / lo) ** (np.arange(R) / max(1, R - 1))
+
+
+def test_batch_segments_match_oracle(umc, oracle):
+    Ls = [8, 16, 12]
+    R, S = 4, 3
+    betas = np.stack([_geometric(0.8, 1.3, R)] * len(Ls))
+    b = umc.Batch(Ls, betas, coupling=1.0, width=1.0, sweeps_per_exchange=S, seed=7)
+    b.randomize(3)
+    cseeds, lseeds = b.seeds()
+    csr = {}
+    for L in set(Ls):
+        pos = checker_position(L, L)
+        ei, ej = relabel_edges(*square_edges(L, L), pos)
+        st, off, bonds, _ = oracle.pair_graph(L * L, ei, ej)
+        csr[L] = (pos, off, bonds)
+    for seg in range(3):
+        holder = b.temperature_map()
+        fields = [b.get_field(c).astype(np.float64) for c in range(b.n_chains)]
+        energies = np.zeros(b.n_chains)
+        expect = []
+        near = False
+        for c in range(b.n_chains):
+            l, L = c // R, b.chain_side(c)
+            slot = int(np.nonzero(holder[l] == c)[0][0])
+            pos, off, bonds = csr[L]
+            cm = np.empty(L * L)
+            cm[pos] = fields[c]
+            t_o, obs, margin = oracle.xy_metropolis(off, bonds, 1.0, betas[l, slot], 1.0, int(cseeds[c]), seg * S, S, cm)
+            near |= bool((np.abs(margin) < MARGIN).any())
+            energies[c] = obs[-1, 0]
+            expect.append(t_o[pos])
+        rec = b.run(1)
+        for c in range(b.n_chains):
+            got = b.get_field(c).astype(np.float64)
+            d = np.abs(np.angle(np.exp(1j * (got - expect[c]))))
+            if not near:
+                assert d.max() < TOL, (seg, c, d.max())
+        # exchange round: the oracle's rule on the oracle energies
+        new_holder = b.temperature_map()
+        for l in range(len(Ls)):
+            h_o, acc = oracle.replica_exchange(betas[l], holder[l], energies, int(lseeds[l]), seg, seg & 1)
+            np.testing.assert_array_equal(new_holder[l], h_o)
+        # records: slot k's energy is the energy of its holder before the exchange
+        for l in range(len(Ls)):
+            for k in range(R):
+                c = int(rec[0, l, k, 3])
+                assert c == holder[l, k]
+                assert abs(rec[0, l, k, 0] - energies[c]) < 1e-3 * max(1, abs(energies[c]))
+    s, r, w = b.counters()
+    assert (s, r) == (3 * S, 3)
+
+
+def test_batch_is_deterministic_and_config_independent(umc):
+    Ls = [16, 32, 64, 128, 256, 32]
+    R = 8
+    betas = np.stack([_geometric(0.8, 1.3, R)] * len(Ls))
+    a = umc.Batch(Ls, betas, seed=11)
+    b = umc.Batch(Ls, betas, seed=11)
+    for x in (a, b):
+        x.randomize(5)
+    ra, rb = a.run(6), b.run(6)
+    np.testing.assert_array_equal(ra, rb)
+    for c in (0, R * 4, a.n_chains - 1):
+        np.testing.assert_array_equal(a.get_field(c), b.get_field(c))
+    sw = a.counters()
+    assert sw[0] == 60 and sw[1] == 6 and sw[2] > 0
+    assert np.isfinite(ra).all()
+    # every temperature slot is held by exactly one chain of its ladder
+    h = a.temperature_map()
+    for l in range(len(Ls)):
+        assert sorted(h[l]) == list(range(l * R, (l + 1) * R))
+    assert a.config(256)["block"] in (256, 512, 1024)
+
+
+def test_batch_energy_per_site_orders_with_beta(umc):
+    # hotter slots carry higher energy on average (a sanity check of the ladder)
+    R = 8
+    betas = np.stack([_geometric(0.5, 1.5, R)] * 2)
+    b = umc.Batch([32, 32], betas, seed=3)
+    b.randomize(1)
+    b.run(20)
+    rec = b.run(40)
+    e = rec[:, :, :, 0].mean(axis=0) / (32 * 32)
+    assert (np.diff(e, axis=1) < 0.02).all()
+    assert e[0, 0] > e[0, -1]

@@ -163,6 +163,38 @@ _decl("umc_chain_fetch", _int, _vp, _vp, _vp, _u64, C.POINTER(_u64))
 _decl("umc_wolff_stats", _int, _vp, C.POINTER(_u64), C.POINTER(_f64))
 _decl("umc_chain_set_timing", _int, _vp, _int)
 _decl("umc_chain_set_fused", _int, _vp, _int)
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [
+        ("n_ladders", _u32),
+        ("replicas", _u32),
+        ("L", _vp),
+        ("betas", _vp),
+        ("coupling", _f64),
+        ("width", _f64),
+        ("sweeps_per_exchange", _u32),
+        ("seed", _u64),
+        ("device", _i32),
+        ("stream", _vp),
+        ("max_records", _u64),
+    ]
+
+
+_decl("umc_batch_create", _int, C.POINTER(BatchDesc), C.POINTER(_vp))
+_decl("umc_batch_destroy", _int, _vp)
+_decl("umc_batch_randomize", _int, _vp, _u64)
+_decl("umc_batch_set_field", _int, _vp, _u32, _vp)
+_decl("umc_batch_get_field", _int, _vp, _u32, _vp)
+_decl("umc_batch_enqueue", _int, _vp, _u64)
+_decl("umc_batch_fetch", _int, _vp, _vp, _u64, C.POINTER(_u64))
+_decl("umc_batch_run", _int, _vp, _u64, _vp)
+_decl("umc_batch_counters", _int, _vp, C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64))
+_decl("umc_batch_temperature_map", _int, _vp, _vp)
+_decl("umc_batch_seeds", _int, _vp, _vp, _vp)
+_decl("umc_batch_config", _int, _vp, _u32, C.POINTER(_u32), C.POINTER(_u32), C.POINTER(_u32))
+_decl("umc_batch_sites", _int, _vp, C.POINTER(_u64), C.POINTER(_u64))
+_decl("umc_batch_stream", _vp, _vp)
 _decl("umc_chain_kernel_stats", _int, _vp, _vp, _vp, _int)
 
 KERNEL_KINDS = ["metropolis", "wolff_union", "wolff_flip", "observe", "gauge", "batch", "learned", "other",
@@ -454,6 +486,101 @@ class Chain:
         f, s = _u64(0), _f64(0)
         check(lib.umc_wolff_stats(self._h, C.byref(f), C.byref(s)))
         return f.value, s.value
+
+
+class Batch:
+    """Independent XY chains in replica-exchange ladders (umc_batch_*)."""
+
+    def __init__(self, L, betas, *, coupling=1.0, width=1.0, sweeps_per_exchange=10, seed=1, device=0,
+                 max_records=1024):
+        L = np.ascontiguousarray(L, np.uint32)
+        betas = np.ascontiguousarray(betas, np.float64)
+        if betas.ndim != 2 or betas.shape[0] != len(L):
+            raise ValueError("betas must be (n_ladders, replicas)")
+        d = BatchDesc()
+        d.n_ladders, d.replicas = betas.shape
+        d.L = L.ctypes.data_as(_vp)
+        d.betas = betas.ctypes.data_as(_vp)
+        d.coupling, d.width = coupling, width
+        d.sweeps_per_exchange = sweeps_per_exchange
+        d.seed, d.device, d.stream, d.max_records = seed, device, None, max_records
+        h = _vp()
+        check(lib.umc_batch_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.L = L.copy()
+        self.betas = betas.copy()
+        self.n_ladders, self.R = betas.shape
+        self.n_chains = self.n_ladders * self.R
+        self.sweeps_per_exchange = sweeps_per_exchange
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.umc_batch_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def chain_side(self, c):
+        return int(self.L[c // self.R])
+
+    def randomize(self, seed):
+        check(lib.umc_batch_randomize(self._h, seed))
+
+    def set_field(self, chain, theta):
+        a = np.ascontiguousarray(theta, np.float32).reshape(-1)
+        if a.size != self.chain_side(chain) ** 2:
+            raise ValueError("wrong field size")
+        check(lib.umc_batch_set_field(self._h, chain, _ptr(a)))
+
+    def get_field(self, chain):
+        a = np.zeros(self.chain_side(chain) ** 2, np.float32)
+        check(lib.umc_batch_get_field(self._h, chain, _ptr(a)))
+        return a
+
+    def run(self, n_segments):
+        rec = np.zeros((n_segments, self.n_chains, OBS_STRIDE))
+        check(lib.umc_batch_run(self._h, n_segments, _ptr(rec)))
+        return rec.reshape(n_segments, self.n_ladders, self.R, OBS_STRIDE)
+
+    def enqueue(self, n_segments):
+        check(lib.umc_batch_enqueue(self._h, n_segments))
+
+    def fetch(self, capacity):
+        rec = np.zeros((capacity, self.n_chains, OBS_STRIDE))
+        got = _u64(0)
+        check(lib.umc_batch_fetch(self._h, _ptr(rec), capacity, C.byref(got)))
+        return rec[: got.value].reshape(-1, self.n_ladders, self.R, OBS_STRIDE)
+
+    def counters(self):
+        s, r, w = _u64(0), _u64(0), _u64(0)
+        check(lib.umc_batch_counters(self._h, C.byref(s), C.byref(r), C.byref(w)))
+        return s.value, r.value, w.value
+
+    def temperature_map(self):
+        h = np.zeros(self.n_chains, np.uint32)
+        check(lib.umc_batch_temperature_map(self._h, _ptr(h)))
+        return h.reshape(self.n_ladders, self.R)
+
+    def seeds(self):
+        cs = np.zeros(self.n_chains, np.uint64)
+        ls = np.zeros(self.n_ladders, np.uint64)
+        check(lib.umc_batch_seeds(self._h, _ptr(cs), _ptr(ls)))
+        return cs, ls
+
+    def config(self, L):
+        a, b, c = _u32(0), _u32(0), _u32(0)
+        check(lib.umc_batch_config(self._h, L, C.byref(a), C.byref(b), C.byref(c)))
+        return {"chains_per_cta": a.value, "ctas_per_chain": b.value, "block": c.value}
+
+    def sites(self):
+        t, k = _u64(0), _u64(0)
+        check(lib.umc_batch_sites(self._h, C.byref(t), C.byref(k)))
+        return t.value, k.value
+
+    def stream(self) -> int:
+        return lib.umc_batch_stream(self._h) or 0
 
 
 # ========================================================= reference mirror

@@ -1,0 +1,813 @@
+// umc_batch.cu -- many independent XY chains with replica-exchange ladders.
+//
+// The reference drives one chain per driver object (driver.hpp:17-68) and has
+// no notion of batching or parallel tempering; this is the engine's batched
+// form of its XY angle model (PairModel<U1Dof, -J cos(ti - tj)> + U1Shift).
+//
+// Layout: every chain is a periodic L x L lattice (L even, one L per ladder) in
+// the two-colour layout of umc_spin_kernels.cuh (colour c, site/2); all chains
+// sit back to back in one FP32 buffer.  Chain c belongs to ladder c / R and
+// starts at temperature slot c % R.
+//
+// One segment = S sweeps of every chain (each chain at the beta of the slot it
+// holds) followed by one exchange round per ladder.  A segment is one kernel
+// per lattice-size group -- the groups run as parallel branches of a CUDA
+// graph -- plus one swap kernel.  Within a group a CTA either owns several
+// small chains (chains per CTA, cpc) or a cluster of CTAs shares one large
+// chain (CTAs per chain, cpk) and synchronises with the hardware cluster
+// barrier.  cpc / cpk / block size come from a short autotuning run per group.
+//
+// Keys: site k of chain c at sweep s draws from (chain_seed[c], s, site tag, k),
+// exactly the stream a single XY chain with seed chain_seed[c] would use, so a
+// chain's trajectory can be replayed by the single-chain oracle.  The swap of
+// slots (k, k+1) in ladder l at round r draws from (ladder_seed[l], r, 4, k).
+
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "umc_chain.hpp"
+#include "umc_spin_kernels.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace umc {
+namespace {
+
+constexpr uint32_t kMaxCpc = 64;       // chains per CTA
+constexpr uint32_t kMaxRungs = 64;     // replicas per ladder
+constexpr uint32_t kMaxShares = 8;     // CTAs per chain (cluster size)
+constexpr unsigned kBatchErrRecords = 1u;
+
+struct BatchCounters
+{
+    unsigned long long sweep;     // sweeps done by every chain
+    unsigned long long round;     // exchange rounds done
+    unsigned long long rec;       // records written since the last fetch
+    unsigned long long capacity;  // record slots
+    unsigned int status;
+    unsigned int pad;
+};
+
+struct SegArgs
+{
+    float* theta;
+    const unsigned long long* off;  // per chain
+    const uint32_t* chains;         // chain ids of this group
+    uint32_t n_chains;              // in this group
+    uint32_t L, H, half;
+    uint32_t cpc, cpk;
+    uint32_t sweeps;
+    const BatchCounters* ctr;
+    const uint32_t* slot_of_chain;
+    const double* betas;  // betas[ladder * R + slot]
+    uint32_t R;
+    const unsigned long long* chain_seed;
+    float J, width;
+    double* part;  // per chain, kMaxShares shares: [E, Mx, My, accepted]
+};
+
+template <bool CG>
+__device__ __forceinline__ float ldf(const float* p)
+{
+    if constexpr (CG) return __ldcg(p);
+    else return *p;
+}
+
+// One XY site update (the body of xy_pass in umc_spin_kernels.cuh) on chain
+// data `th`; neighbours through L1 inside one CTA, through L2 in a cluster.
+template <bool CLUSTER>
+__device__ __forceinline__ bool xy_update(const SegArgs& a, float* th, uint32_t colour, uint32_t y, uint32_t i,
+                                          uint64_t kbase, float beta)
+{
+    const uint32_t L = a.L, H = a.H;
+    const uint32_t p = (y + colour) & 1u;
+    const float* other = th + (1u - colour) * a.half;
+    float* own = th + colour * a.half;
+    const uint32_t ym = y == 0 ? L - 1 : y - 1, yp = y + 1 == L ? 0u : y + 1;
+    const uint32_t i2 = p ? (i + 1 == H ? 0u : i + 1) : (i == 0 ? H - 1 : i - 1);
+    const float nb[4] = {ldf<CLUSTER>(other + y * H + i), ldf<CLUSTER>(other + y * H + i2),
+                         ldf<CLUSTER>(other + ym * H + i), ldf<CLUSTER>(other + yp * H + i)};
+    float C = 0.f, S = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float sn, cs;
+        __sincosf(nb[q], &sn, &cs);
+        C += cs;
+        S += sn;
+    }
+    const uint32_t k = colour * a.half + y * H + i;
+    const float t = ldf<CLUSTER>(own + y * H + i);
+    KeyedPcg g = KeyedPcg::open(kbase, k);
+    const float prop = u1_shift(g, a.width, t);
+    float so, co, sp, cp;
+    __sincosf(t, &so, &co);
+    __sincosf(prop, &sp, &cp);
+    const float dE = -a.J * ((cp - co) * C + (sp - so) * S);
+    if (!metropolis_accept(g, -beta * dE)) return false;
+    own[y * H + i] = prop;
+    return true;
+}
+
+template <bool CLUSTER>
+__global__ void __launch_bounds__(1024) xy_batch_segment(SegArgs a)
+{
+    __shared__ unsigned int accepted[kMaxCpc];
+    const uint64_t sweep0 = a.ctr->sweep;
+    const uint32_t H = a.H, half = a.half;
+    uint32_t chain_lo, chain_n, row_lo, row_n, share = 0;
+    if (CLUSTER) {
+        chain_lo = blockIdx.x / a.cpk;
+        chain_n = 1;
+        share = blockIdx.x % a.cpk;
+        row_n = a.L / a.cpk;
+        row_lo = share * row_n;
+    } else {
+        chain_lo = blockIdx.x * a.cpc;
+        chain_n = min(a.cpc, a.n_chains - chain_lo);
+        row_lo = 0;
+        row_n = a.L;
+    }
+    if (threadIdx.x < kMaxCpc) accepted[threadIdx.x] = 0u;
+    __syncthreads();
+    const uint32_t per_chain = row_n * H;  // sites of one colour per chain share
+    const uint32_t work = chain_n * per_chain;
+    for (uint32_t s = 0; s < a.sweeps; ++s) {
+        for (uint32_t colour = 0; colour < 2; ++colour) {
+            for (uint32_t w = threadIdx.x; w < work; w += blockDim.x) {
+                const uint32_t ci = w / per_chain, r = w - ci * per_chain;
+                const uint32_t chain = a.chains[chain_lo + ci];
+                const uint32_t y = row_lo + r / H, i = r % H;
+                const float beta = float(a.betas[(chain / a.R) * a.R + a.slot_of_chain[chain]]);
+                const uint64_t kbase = key_base(key_seed(a.chain_seed[chain], sweep0 + s, tag_site(0)));
+                if (xy_update<CLUSTER>(a, a.theta + a.off[chain], colour, y, i, kbase, beta))
+                    atomicAdd(&accepted[ci], 1u);
+            }
+            if constexpr (CLUSTER) cg::this_cluster().sync();
+            else __syncthreads();
+        }
+    }
+    // observables of this CTA's share, per chain, in FP64 (fixed-order sums)
+    for (uint32_t ci = 0; ci < chain_n; ++ci) {
+        const uint32_t chain = a.chains[chain_lo + ci];
+        const float* th = a.theta + a.off[chain];
+        double v[3] = {0, 0, 0};
+        for (uint32_t r = threadIdx.x; r < per_chain; r += blockDim.x) {
+            const uint32_t y = row_lo + r / H, i = r % H;
+            // colour-1 site: its four bonds, all to colour 0, carry every bond once
+            const uint32_t p = (y + 1u) & 1u;
+            const uint32_t ym = y == 0 ? a.L - 1 : y - 1, yp = y + 1 == a.L ? 0u : y + 1;
+            const uint32_t i2 = p ? (i + 1 == H ? 0u : i + 1) : (i == 0 ? H - 1 : i - 1);
+            const float t1 = ldf<CLUSTER>(th + half + y * H + i);
+            const float e = cosf(t1 - ldf<CLUSTER>(th + y * H + i)) + cosf(t1 - ldf<CLUSTER>(th + y * H + i2)) +
+                            cosf(t1 - ldf<CLUSTER>(th + ym * H + i)) + cosf(t1 - ldf<CLUSTER>(th + yp * H + i));
+            v[0] += double(-a.J * e);
+            float sn, cs;
+            sincosf(t1, &sn, &cs);
+            v[1] += double(cs);
+            v[2] += double(sn);
+            sincosf(ldf<CLUSTER>(th + y * H + i), &sn, &cs);
+            v[1] += double(cs);
+            v[2] += double(sn);
+        }
+        block_sum<3>(v);
+        if (threadIdx.x == 0) {
+            double* out = a.part + (uint64_t(chain) * kMaxShares + share) * 4;
+            out[0] = v[0];
+            out[1] = v[1];
+            out[2] = v[2];
+            out[3] = double(accepted[ci]);
+        }
+    }
+}
+
+// One exchange round per ladder (one thread per ladder), after writing the
+// segment's record [E, Mx, My, chain, beta, swap accepted, accepted updates, 0]
+// for every temperature slot.
+__global__ void xy_batch_swap(BatchCounters* ctr, uint32_t n_ladders, uint32_t R, const uint32_t* cpk_of_chain,
+                              const double* part, const double* betas, uint32_t* holder, uint32_t* slot_of_chain,
+                              const unsigned long long* ladder_seed, double* records, unsigned long long* swaps,
+                              uint32_t sweeps)
+{
+    const unsigned long long round = ctr->round;
+    const unsigned long long rec = ctr->rec;
+    const bool keep = rec < ctr->capacity;
+    __syncthreads();
+    for (uint32_t l = threadIdx.x; l < n_ladders; l += blockDim.x) {
+        double E[kMaxRungs];
+        for (uint32_t q = 0; q < R; ++q) {
+            const uint32_t c = l * R + q, k = cpk_of_chain[c];
+            double e = 0.0;
+            for (uint32_t r = 0; r < k; ++r) e += part[(uint64_t(c) * kMaxShares + r) * 4];
+            E[q] = e;
+        }
+        for (uint32_t k = 0; k < R && keep; ++k) {
+            const uint32_t c = holder[l * R + k], nk = cpk_of_chain[c];
+            double mx = 0.0, my = 0.0, acc = 0.0;
+            for (uint32_t r = 0; r < nk; ++r) {
+                mx += part[(uint64_t(c) * kMaxShares + r) * 4 + 1];
+                my += part[(uint64_t(c) * kMaxShares + r) * 4 + 2];
+                acc += part[(uint64_t(c) * kMaxShares + r) * 4 + 3];
+            }
+            double* out = records + ((rec * n_ladders + l) * R + k) * kObs;
+            out[0] = E[c - l * R];
+            out[1] = mx;
+            out[2] = my;
+            out[3] = double(c);
+            out[4] = betas[l * R + k];
+            out[5] = 0.0;
+            out[6] = acc;
+            out[7] = 0.0;
+        }
+        const uint32_t parity = uint32_t(round & 1ull);
+        const uint64_t kb = key_base(key_seed(ladder_seed[l], round, kTagSwap));
+        for (uint32_t k = parity; k + 1 < R; k += 2) {
+            const uint32_t a = holder[l * R + k], b = holder[l * R + k + 1];
+            const double delta = (betas[l * R + k] - betas[l * R + k + 1]) * (E[a - l * R] - E[b - l * R]);
+            const bool acc = delta >= 0.0 || log(u_f64(first_draw(kb, k))) < delta;
+            if (keep) records[((rec * n_ladders + l) * R + k) * kObs + 5] = acc ? 1.0 : 0.0;
+            if (acc) {
+                holder[l * R + k] = b;
+                holder[l * R + k + 1] = a;
+                slot_of_chain[a] = k + 1;
+                slot_of_chain[b] = k;
+                atomicAdd(swaps, 1ull);
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctr->round = round + 1;
+        ctr->sweep += sweeps;
+        if (keep) ctr->rec = rec + 1;
+        else ctr->status |= kBatchErrRecords;
+    }
+}
+
+// Random start: angle 2 pi u from key (chain_seed, 0, init tag, natural site id).
+__global__ void xy_batch_randomize(float* theta, const unsigned long long* off, const uint32_t* Ls, uint32_t n_chains,
+                                   const unsigned long long* chain_seed)
+{
+    const uint32_t c = blockIdx.y;
+    if (c >= n_chains) return;
+    const uint32_t L = Ls[c], n = L * L, half = n / 2;
+    const uint64_t kb = key_base(key_seed(chain_seed[c], 0, kTagInit));
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const uint32_t x = s % L, y = s / L;
+        const uint32_t k = ((x + y) & 1u) * half + (s >> 1);
+        theta[off[c] + k] = twice_u_f32(first_draw(kb, s)) * 3.14159265358979f;
+    }
+}
+
+struct GroupCfg
+{
+    uint32_t cpc = 1, cpk = 1, block = 256;
+};
+
+std::mutex g_tune_mutex;
+std::map<std::string, GroupCfg> g_tune_cache;
+
+}  // namespace
+}  // namespace umc
+
+// ============================================================== batch object
+
+struct umc_batch
+{
+    umc_batch_desc desc{};
+    uint32_t n_ladders = 0, R = 0, n_chains = 0;
+    std::vector<uint32_t> L;  // per chain
+    std::vector<unsigned long long> off, chain_seed, ladder_seed;
+    std::vector<double> betas;
+    struct Group
+    {
+        uint32_t L = 0;
+        std::vector<uint32_t> chains;
+        umc::GroupCfg cfg;
+        umc::DevBuf chains_dev;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t done = nullptr;
+    };
+    std::vector<Group> groups;
+    std::vector<uint32_t> cpk_of_chain;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t fork = nullptr;
+    umc::DevBuf theta, off_dev, seeds_dev, lseeds_dev, betas_dev, holder_dev, slot_dev, cpk_dev, part, records, ctr,
+        swaps, Ls_dev;
+    uint64_t total_sites = 0;
+    uint64_t max_records = 0;
+    uint32_t sweeps_per_exchange = 10;
+    cudaGraphExec_t graph = nullptr;
+    uint64_t launches = 0;
+};
+
+namespace umc {
+namespace {
+
+void batch_scope(const umc_batch* b) { cuda_check(cudaSetDevice(b->device), "cudaSetDevice"); }
+
+SegArgs seg_args(umc_batch* b, umc_batch::Group& g, float* theta)
+{
+    SegArgs a{};
+    a.theta = theta;
+    a.off = b->off_dev.as<unsigned long long>();
+    a.chains = g.chains_dev.as<uint32_t>();
+    a.n_chains = uint32_t(g.chains.size());
+    a.L = g.L;
+    a.H = g.L / 2;
+    a.half = g.L * g.L / 2;
+    a.cpc = g.cfg.cpc;
+    a.cpk = g.cfg.cpk;
+    a.sweeps = b->sweeps_per_exchange;
+    a.ctr = b->ctr.as<BatchCounters>();
+    a.slot_of_chain = b->slot_dev.as<uint32_t>();
+    a.betas = b->betas_dev.as<double>();
+    a.R = b->R;
+    a.chain_seed = b->seeds_dev.as<unsigned long long>();
+    a.J = float(b->desc.coupling);
+    a.width = float(b->desc.width);
+    a.part = b->part.as<double>();
+    return a;
+}
+
+void launch_segment(umc_batch* b, umc_batch::Group& g, const GroupCfg& cfg, float* theta, cudaStream_t st)
+{
+    SegArgs a = seg_args(b, g, theta);
+    a.cpc = cfg.cpc;
+    a.cpk = cfg.cpk;
+    const uint32_t nc = uint32_t(g.chains.size());
+    if (cfg.cpk > 1) {
+        cudaLaunchConfig_t lc{};
+        lc.gridDim = dim3(nc * cfg.cpk);
+        lc.blockDim = dim3(cfg.block);
+        lc.dynamicSmemBytes = 0;
+        lc.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cfg.cpk;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        cuda_check(cudaLaunchKernelEx(&lc, xy_batch_segment<true>, a), "batch segment (cluster)");
+    } else {
+        const uint32_t grid = (nc + cfg.cpc - 1) / cfg.cpc;
+        xy_batch_segment<false><<<grid, cfg.block, 0, st>>>(a);
+        cuda_check(cudaGetLastError(), "batch segment");
+    }
+    b->launches++;
+}
+
+// Candidate launch shapes for chains of side L.
+std::vector<GroupCfg> candidates(uint32_t L, uint32_t n_chains)
+{
+    std::vector<GroupCfg> out;
+    const uint32_t half = L * L / 2;
+    for (uint32_t block : {256u, 512u, 1024u}) {
+        for (uint32_t cpc = 1; cpc <= kMaxCpc && cpc <= n_chains; cpc *= 2) {
+            if (cpc > 1 && cpc * half > 8u * block * 4u) break;  // keep a CTA's share moderate
+            out.push_back({cpc, 1, block});
+        }
+        for (uint32_t cpk = 2; cpk <= kMaxShares; cpk *= 2)
+            if (L % cpk == 0 && (L / cpk) >= 2 && half >= cpk * block) out.push_back({1, cpk, block});
+    }
+    return out;
+}
+
+// Times each candidate on a scratch copy of the group's chains (state untouched).
+GroupCfg autotune(umc_batch* b, umc_batch::Group& g)
+{
+    cudaDeviceProp prop{};
+    cuda_check(cudaGetDeviceProperties(&prop, b->device), "device properties");
+    const std::string key = std::string(prop.name) + "/L" + std::to_string(g.L) + "/n" + std::to_string(g.chains.size()) +
+                            "/s" + std::to_string(b->sweeps_per_exchange);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) return it->second;
+    }
+    DevBuf scratch;
+    scratch.alloc(b->theta.bytes, "autotune scratch");
+    cuda_check(cudaMemcpyAsync(scratch.p, b->theta.p, b->theta.bytes, cudaMemcpyDeviceToDevice, b->stream), "autotune copy");
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "event");
+    cuda_check(cudaEventCreate(&e1), "event");
+    GroupCfg best;
+    float best_ms = 1e30f;
+    for (const GroupCfg& cfg : candidates(g.L, uint32_t(g.chains.size()))) {
+        // warm once, then time two launches
+        try {
+            launch_segment(b, g, cfg, scratch.as<float>(), b->stream);
+        } catch (const Error&) {
+            cudaGetLastError();
+            continue;
+        }
+        cuda_check(cudaEventRecord(e0, b->stream), "event");
+        launch_segment(b, g, cfg, scratch.as<float>(), b->stream);
+        launch_segment(b, g, cfg, scratch.as<float>(), b->stream);
+        cuda_check(cudaEventRecord(e1, b->stream), "event");
+        cuda_check(cudaEventSynchronize(e1), "autotune");
+        float ms = 0;
+        cuda_check(cudaEventElapsedTime(&ms, e0, e1), "autotune");
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = cfg;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    scratch.free_();
+    b->launches = 0;
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = best;
+    return best;
+}
+
+void build_graph(umc_batch* b)
+{
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    cudaGraph_t graph;
+    cuda_check(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cuda_check(cudaEventRecord(b->fork, b->stream), "fork");
+    for (auto& g : b->groups) {
+        cuda_check(cudaStreamWaitEvent(g.stream, b->fork, 0), "fork wait");
+        launch_segment(b, g, g.cfg, b->theta.as<float>(), g.stream);
+        cuda_check(cudaEventRecord(g.done, g.stream), "join");
+        cuda_check(cudaStreamWaitEvent(b->stream, g.done, 0), "join wait");
+    }
+    xy_batch_swap<<<1, 64, 0, b->stream>>>(b->ctr.as<BatchCounters>(), b->n_ladders, b->R, b->cpk_dev.as<uint32_t>(),
+                                             b->part.as<double>(), b->betas_dev.as<double>(), b->holder_dev.as<uint32_t>(),
+                                             b->slot_dev.as<uint32_t>(), b->lseeds_dev.as<unsigned long long>(),
+                                             b->records.as<double>(), b->swaps.as<unsigned long long>(),
+                                             b->sweeps_per_exchange);
+    cuda_check(cudaGetLastError(), "swap kernel");
+    cuda_check(cudaStreamEndCapture(b->stream, &graph), "end capture");
+    cuda_check(cudaGraphInstantiate(&b->graph, graph, 0), "instantiate graph");
+    cudaGraphDestroy(graph);
+}
+
+void create_batch(const umc_batch_desc* d, umc_batch* b)
+{
+    if (!d) throw Error(UMC_ERR_INVALID_ARGUMENT, "null descriptor");
+    b->desc = *d;
+    b->n_ladders = d->n_ladders;
+    b->R = d->replicas;
+    if (b->n_ladders == 0 || b->R == 0) throw Error(UMC_ERR_INVALID_ARGUMENT, "need at least one ladder and one replica");
+    if (b->R > kMaxRungs) throw Error(UMC_ERR_UNSUPPORTED, "at most 64 replicas per ladder");
+    if (!d->L || !d->betas) throw Error(UMC_ERR_INVALID_ARGUMENT, "null L or betas");
+    if (!std::isfinite(d->coupling) || !std::isfinite(d->width)) throw Error(UMC_ERR_INVALID_ARGUMENT, "J and width must be finite");
+    b->sweeps_per_exchange = d->sweeps_per_exchange ? d->sweeps_per_exchange : 10;
+    b->n_chains = b->n_ladders * b->R;
+    b->device = d->device;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        throw Error(UMC_ERR_CUDA, "no CUDA device available");
+    }
+    if (b->device < 0 || b->device >= count) throw Error(UMC_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    batch_scope(b);
+    b->betas.assign(d->betas, d->betas + b->n_chains);
+    for (double beta : b->betas)
+        if (!std::isfinite(beta)) throw Error(UMC_ERR_INVALID_ARGUMENT, "betas must be finite");
+    b->L.resize(b->n_chains);
+    b->off.resize(b->n_chains);
+    b->chain_seed.resize(b->n_chains);
+    b->ladder_seed.resize(b->n_ladders);
+    uint64_t acc = 0;
+    std::map<uint32_t, std::vector<uint32_t>> by_L;
+    for (uint32_t l = 0; l < b->n_ladders; ++l) {
+        const uint64_t L = d->L[l];
+        if (L < 2 || L % 2 || L > 4096) throw Error(UMC_ERR_INVALID_ARGUMENT, "ladder side L must be even, in [2, 4096]");
+        b->ladder_seed[l] = mix64(d->seed + 0xD1B54A32D192ED03ULL * (l + 1));
+        for (uint32_t k = 0; k < b->R; ++k) {
+            const uint32_t c = l * b->R + k;
+            b->L[c] = uint32_t(L);
+            b->off[c] = acc;
+            acc += L * L;
+            b->chain_seed[c] = mix64(d->seed + kGolden * (c + 1ull));
+            by_L[uint32_t(L)].push_back(c);
+        }
+    }
+    b->total_sites = acc;
+    if (acc > (1ull << 34)) throw Error(UMC_ERR_OVERFLOW, "too many sites in the batch");
+    if (d->stream) {
+        b->stream = static_cast<cudaStream_t>(d->stream);
+    } else {
+        cuda_check(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream");
+        b->own_stream = true;
+    }
+    cuda_check(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "event");
+    b->max_records = d->max_records ? d->max_records : 1024;
+    auto up = [&](DevBuf& buf, const void* p, size_t bytes, const char* what) {
+        buf.alloc(bytes, what);
+        cuda_check(cudaMemcpy(buf.p, p, bytes, cudaMemcpyHostToDevice), what);
+    };
+    b->theta.alloc(acc * sizeof(float), "batch field");
+    cuda_check(cudaMemset(b->theta.p, 0, acc * sizeof(float)), "zero field");
+    up(b->off_dev, b->off.data(), b->off.size() * 8, "offsets");
+    up(b->seeds_dev, b->chain_seed.data(), b->chain_seed.size() * 8, "chain seeds");
+    up(b->lseeds_dev, b->ladder_seed.data(), b->ladder_seed.size() * 8, "ladder seeds");
+    up(b->betas_dev, b->betas.data(), b->betas.size() * 8, "betas");
+    up(b->Ls_dev, b->L.data(), b->L.size() * 4, "sides");
+    std::vector<uint32_t> holder(b->n_chains), slot(b->n_chains);
+    for (uint32_t c = 0; c < b->n_chains; ++c) holder[c] = slot[c] = c % b->R;
+    for (uint32_t c = 0; c < b->n_chains; ++c) holder[c] = c;  // slot k of ladder l held by chain l*R+k
+    up(b->holder_dev, holder.data(), holder.size() * 4, "holders");
+    up(b->slot_dev, slot.data(), slot.size() * 4, "slots");
+    b->records.alloc(b->max_records * b->n_chains * kObs * sizeof(double), "batch records");
+    b->swaps.alloc(8, "swap counter");
+    cuda_check(cudaMemset(b->swaps.p, 0, 8), "swap counter");
+    BatchCounters c0{};
+    c0.capacity = b->max_records;
+    up(b->ctr, &c0, sizeof c0, "counters");
+
+    // groups and their launch shapes
+    b->cpk_of_chain.assign(b->n_chains, 1);
+    for (auto& [L, chains] : by_L) {
+        b->groups.emplace_back();
+        auto& g = b->groups.back();
+        g.L = L;
+        g.chains = chains;
+        up(g.chains_dev, chains.data(), chains.size() * 4, "group chains");
+        cuda_check(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking), "group stream");
+        cuda_check(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming), "event");
+    }
+    // shares of the energy partials need the largest cpk first: tune, then size
+    b->part.alloc(uint64_t(b->n_chains) * kMaxShares * 4 * sizeof(double), "partials");
+    for (auto& g : b->groups) {
+        g.cfg = autotune(b, g);
+        for (uint32_t c : g.chains) b->cpk_of_chain[c] = g.cfg.cpk;
+    }
+    up(b->cpk_dev, b->cpk_of_chain.data(), b->cpk_of_chain.size() * 4, "cpk");
+    cuda_check(cudaMemset(b->ctr.p, 0, sizeof(BatchCounters)), "counters");
+    cuda_check(cudaMemcpy(&b->ctr.as<BatchCounters>()->capacity, &b->max_records, 8, cudaMemcpyHostToDevice), "capacity");
+    build_graph(b);
+}
+
+void destroy_batch(umc_batch* b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (auto& g : b->groups) {
+        if (g.stream) cudaStreamDestroy(g.stream);
+        if (g.done) cudaEventDestroy(g.done);
+        g.chains_dev.free_();
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    for (DevBuf* x : {&b->theta, &b->off_dev, &b->seeds_dev, &b->lseeds_dev, &b->betas_dev, &b->holder_dev, &b->slot_dev,
+                      &b->cpk_dev, &b->part, &b->records, &b->ctr, &b->swaps, &b->Ls_dev})
+        x->free_();
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+}
+
+template <class F>
+int bguard(F&& f)
+{
+    try {
+        set_last_error("");
+        f();
+        return UMC_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return UMC_ERR_INVALID_ARGUMENT;
+    }
+}
+
+// chain-local natural order <-> two-colour order
+void to_colour_major(const float* src, float* dst, uint32_t L)
+{
+    const uint32_t half = L * L / 2;
+    for (uint32_t s = 0; s < L * L; ++s) {
+        const uint32_t x = s % L, y = s / L;
+        dst[((x + y) & 1u) * half + s / 2] = src[s];
+    }
+}
+
+void from_colour_major(const float* src, float* dst, uint32_t L)
+{
+    const uint32_t half = L * L / 2;
+    for (uint32_t s = 0; s < L * L; ++s) {
+        const uint32_t x = s % L, y = s / L;
+        dst[s] = src[((x + y) & 1u) * half + s / 2];
+    }
+}
+
+}  // namespace
+}  // namespace umc
+
+using namespace umc;
+
+extern "C" {
+
+int umc_batch_create(const umc_batch_desc* desc, umc_batch** out)
+{
+    return bguard([&] {
+        if (!out) throw Error(UMC_ERR_INVALID_ARGUMENT, "null output handle");
+        *out = nullptr;
+        auto* b = new umc_batch;
+        try {
+            create_batch(desc, b);
+        } catch (...) {
+            destroy_batch(b);
+            delete b;
+            throw;
+        }
+        *out = b;
+    });
+}
+
+int umc_batch_destroy(umc_batch* b)
+{
+    return bguard([&] {
+        destroy_batch(b);
+        delete b;
+    });
+}
+
+int umc_batch_randomize(umc_batch* b, uint64_t seed)
+{
+    return bguard([&] {
+        if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
+        batch_scope(b);
+        // per-chain init keys derive from the run seed and the chain index
+        std::vector<unsigned long long> s(b->n_chains);
+        for (uint32_t c = 0; c < b->n_chains; ++c) s[c] = mix64(seed + kGolden * (c + 1ull));
+        DevBuf sd;
+        sd.alloc(s.size() * 8, "init seeds");
+        cuda_check(cudaMemcpy(sd.p, s.data(), s.size() * 8, cudaMemcpyHostToDevice), "init seeds");
+        const uint32_t maxL = *std::max_element(b->L.begin(), b->L.end());
+        xy_batch_randomize<<<dim3((maxL * maxL + 255) / 256, b->n_chains), 256, 0, b->stream>>>(
+            b->theta.as<float>(), b->off_dev.as<unsigned long long>(), b->Ls_dev.as<uint32_t>(), b->n_chains,
+            sd.as<unsigned long long>());
+        cuda_check(cudaGetLastError(), "randomize");
+        cuda_check(cudaStreamSynchronize(b->stream), "randomize");
+    });
+}
+
+int umc_batch_set_field(umc_batch* b, uint32_t chain, const float* theta)
+{
+    return bguard([&] {
+        if (!b || !theta) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (chain >= b->n_chains) throw Error(UMC_ERR_OUT_OF_RANGE, "chain index out of range");
+        batch_scope(b);
+        const uint32_t L = b->L[chain];
+        std::vector<float> tmp(size_t(L) * L);
+        to_colour_major(theta, tmp.data(), L);
+        cuda_check(cudaStreamSynchronize(b->stream), "sync");
+        cuda_check(cudaMemcpy(b->theta.as<float>() + b->off[chain], tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice),
+                   "upload chain");
+    });
+}
+
+int umc_batch_get_field(umc_batch* b, uint32_t chain, float* theta)
+{
+    return bguard([&] {
+        if (!b || !theta) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (chain >= b->n_chains) throw Error(UMC_ERR_OUT_OF_RANGE, "chain index out of range");
+        batch_scope(b);
+        const uint32_t L = b->L[chain];
+        std::vector<float> tmp(size_t(L) * L);
+        cuda_check(cudaStreamSynchronize(b->stream), "sync");
+        cuda_check(cudaMemcpy(tmp.data(), b->theta.as<float>() + b->off[chain], tmp.size() * 4, cudaMemcpyDeviceToHost),
+                   "download chain");
+        from_colour_major(tmp.data(), theta, L);
+    });
+}
+
+int umc_batch_enqueue(umc_batch* b, uint64_t n_segments)
+{
+    return bguard([&] {
+        if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
+        batch_scope(b);
+        for (uint64_t s = 0; s < n_segments; ++s) cuda_check(cudaGraphLaunch(b->graph, b->stream), "segment graph");
+        b->launches += n_segments * (b->groups.size() + 1);
+    });
+}
+
+int umc_batch_fetch(umc_batch* b, double* records, uint64_t capacity, uint64_t* n_records)
+{
+    return bguard([&] {
+        if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
+        batch_scope(b);
+        cuda_check(cudaStreamSynchronize(b->stream), "sync");
+        BatchCounters c{};
+        cuda_check(cudaMemcpy(&c, b->ctr.p, sizeof c, cudaMemcpyDeviceToHost), "counters");
+        if (c.status & kBatchErrRecords) {
+            const unsigned int zero = 0;
+            cuda_check(cudaMemcpy(&b->ctr.as<BatchCounters>()->status, &zero, 4, cudaMemcpyHostToDevice), "status");
+            const unsigned long long z = 0;
+            cuda_check(cudaMemcpy(&b->ctr.as<BatchCounters>()->rec, &z, 8, cudaMemcpyHostToDevice), "records");
+            throw Error(UMC_ERR_STATE, "batch records overflowed; fetch more often or raise max_records");
+        }
+        if (records && c.rec > capacity) throw Error(UMC_ERR_INVALID_ARGUMENT, "record buffer too small");
+        if (records && c.rec)
+            cuda_check(cudaMemcpy(records, b->records.p, c.rec * b->n_chains * kObs * sizeof(double), cudaMemcpyDeviceToHost),
+                       "records");
+        if (n_records) *n_records = c.rec;
+        const unsigned long long z = 0;
+        cuda_check(cudaMemcpy(&b->ctr.as<BatchCounters>()->rec, &z, 8, cudaMemcpyHostToDevice), "reset records");
+    });
+}
+
+int umc_batch_run(umc_batch* b, uint64_t n_segments, double* records)
+{
+    return bguard([&] {
+        if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
+        uint64_t done = 0;
+        {
+            uint64_t got = 0;  // drop records queued before this call
+            const int st = umc_batch_fetch(b, nullptr, 0, &got);
+            if (st != UMC_OK) throw Error(st, umc_last_error());
+        }
+        while (done < n_segments) {
+            const uint64_t m = std::min<uint64_t>(n_segments - done, b->max_records);
+            int st = umc_batch_enqueue(b, m);
+            if (st != UMC_OK) throw Error(st, umc_last_error());
+            uint64_t got = 0;
+            st = umc_batch_fetch(b, records ? records + done * b->n_chains * kObs : nullptr, m, &got);
+            if (st != UMC_OK) throw Error(st, umc_last_error());
+            done += m;
+        }
+    });
+}
+
+int umc_batch_counters(const umc_batch* b, uint64_t* sweeps, uint64_t* rounds, uint64_t* swaps_accepted)
+{
+    return bguard([&] {
+        if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
+        batch_scope(b);
+        cuda_check(cudaStreamSynchronize(b->stream), "sync");
+        BatchCounters c{};
+        cuda_check(cudaMemcpy(&c, b->ctr.p, sizeof c, cudaMemcpyDeviceToHost), "counters");
+        unsigned long long sw = 0;
+        cuda_check(cudaMemcpy(&sw, b->swaps.p, 8, cudaMemcpyDeviceToHost), "swaps");
+        if (sweeps) *sweeps = c.sweep;
+        if (rounds) *rounds = c.round;
+        if (swaps_accepted) *swaps_accepted = sw;
+    });
+}
+
+int umc_batch_temperature_map(const umc_batch* b, uint32_t* holder)
+{
+    return bguard([&] {
+        if (!b || !holder) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        batch_scope(b);
+        cuda_check(cudaStreamSynchronize(b->stream), "sync");
+        cuda_check(cudaMemcpy(holder, b->holder_dev.p, b->n_chains * 4, cudaMemcpyDeviceToHost), "holders");
+    });
+}
+
+int umc_batch_seeds(const umc_batch* b, uint64_t* chain_seeds, uint64_t* ladder_seeds)
+{
+    return bguard([&] {
+        if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
+        if (chain_seeds) std::copy(b->chain_seed.begin(), b->chain_seed.end(), chain_seeds);
+        if (ladder_seeds) std::copy(b->ladder_seed.begin(), b->ladder_seed.end(), ladder_seeds);
+    });
+}
+
+int umc_batch_config(const umc_batch* b, uint32_t L, uint32_t* chains_per_cta, uint32_t* ctas_per_chain, uint32_t* block)
+{
+    return bguard([&] {
+        if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
+        for (const auto& g : b->groups)
+            if (g.L == L) {
+                if (chains_per_cta) *chains_per_cta = g.cfg.cpc;
+                if (ctas_per_chain) *ctas_per_chain = g.cfg.cpk;
+                if (block) *block = g.cfg.block;
+                return;
+            }
+        throw Error(UMC_ERR_OUT_OF_RANGE, "no ladder with that side");
+    });
+}
+
+int umc_batch_sites(const umc_batch* b, uint64_t* total_sites, uint64_t* kernel_launches)
+{
+    return bguard([&] {
+        if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
+        if (total_sites) *total_sites = b->total_sites;
+        if (kernel_launches) *kernel_launches = b->launches;
+    });
+}
+
+void* umc_batch_stream(const umc_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
+
+}  // extern "C"
