@@ -311,6 +311,18 @@ int umc_wolff_flip_noalloc(int32_t model, int32_t components, void* field, uint6
                            double coupling, double beta, uint64_t seed, uint64_t flip,
                            uint64_t* cluster_size, void* stream);
 
+/* ================================================= series statistics (host) */
+
+/* No counterpart in the reference (its tests compare chain means against fixed
+ * tolerances, test/model_check.cpp:171-222).  Integrated autocorrelation time
+ * of a series with Sokal's automatic window: tau(W) = 1/2 + sum_{t<=W} rho(t),
+ * W the first window with W >= c * tau(W) (c <= 0 selects 6).  tau_err is the
+ * Madras-Sokal estimate tau * sqrt(2 (2W+1) / n).  Any output may be NULL. */
+int umc_tau_int(const double* x, uint64_t n, double c, double* tau, double* tau_err, uint64_t* window);
+/* Mean and its standard error from the means of floor(n/bin) bins of `bin`
+ * consecutive values (at least two bins). */
+int umc_binning_error(const double* x, uint64_t n, uint64_t bin, double* mean, double* err);
+
 #ifdef __cplusplus
 }
 #endif

@@ -216,6 +216,29 @@ def device_count() -> int:
     return n.value
 
 
+# ================================================================= statistics
+_decl("umc_tau_int", _int, _vp, _u64, _f64, C.POINTER(_f64), C.POINTER(_f64), C.POINTER(_u64))
+_decl("umc_binning_error", _int, _vp, _u64, _u64, C.POINTER(_f64), C.POINTER(_f64))
+
+
+def tau_int(series, c: float = 6.0):
+    """Integrated autocorrelation time with Sokal's automatic window.
+
+    Returns ``(tau, tau_err, window)``; tau = 1/2 + sum_{t<=W} rho(t)."""
+    x = np.ascontiguousarray(series, dtype=np.float64)
+    t, e, w = _f64(), _f64(), _u64()
+    check(lib.umc_tau_int(_ptr(x), x.size, c, C.byref(t), C.byref(e), C.byref(w)))
+    return t.value, e.value, w.value
+
+
+def binning_error(series, bin: int):
+    """Mean and its standard error from bins of ``bin`` consecutive values."""
+    x = np.ascontiguousarray(series, dtype=np.float64)
+    m, e = _f64(), _f64()
+    check(lib.umc_binning_error(_ptr(x), x.size, bin, C.byref(m), C.byref(e)))
+    return m.value, e.value
+
+
 # ===================================================================== tables
 class PairGraph:
     """PairGraph(n, edges, symmetric) -- lattice/pair_graph.hpp:49-83."""

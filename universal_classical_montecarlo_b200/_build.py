@@ -26,7 +26,7 @@ NVCC_FLAGS = ["-std=c++20", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-r
 CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-Wall", "-Wextra", f"-I{INCLUDE}", f"-I{CUDA_HOME}/include"]
 
 CU_SOURCES = ["umc_chain.cu", "umc_gauge.cu", "umc_batch.cu", "umc_learn.cu", "umc_noalloc.cu"]
-CXX_SOURCES = ["umc_tables.cpp"]
+CXX_SOURCES = ["umc_tables.cpp", "umc_stats.cpp"]
 
 
 def _sources():
