@@ -115,6 +115,18 @@ class Oracle:
         self._su_expm = L.fn("su_expm", None, _u32, _vp, _vp)
         self._su_unit = L.fn("su_unitarity_error", _f64, _u32, _vp)
         self._rex = L.fn("replica_exchange", _int, _u32, _vp, _vp, _vp, _u64, _u64, _u32, _vp)
+        self._bf16 = L.fn("bf16", _f64, _f64)
+        self._log_i0 = L.fn("log_i0", _f64, _f64)
+        self._i1_i0 = L.fn("i1_over_i0", _f64, _f64)
+        self._mlp_fwd = L.fn("mlp_forward", None, _vp, _u64, _vp, _int, _vp)
+        self._mixture = L.fn("vm_mixture", None, _vp, _vp, _vp, _vp, _vp)
+        self._mix_logpdf = L.fn("vm_mixture_logpdf", _f64, _vp, _vp, _vp, _vp, _f64)
+        self._mlp_grad = L.fn("mlp_loss_grad", _f64, _vp, _u64, _vp, _vp, _int, _vp)
+        self._adam = L.fn("adam_step", None, _u64, _vp, _vp, _vp, _vp, _u64, _f64, _f64, _f64, _f64)
+        self._u1_learned = L.fn("u1_learned_metropolis", None, _u64, _vp, _u64, _vp, _vp, _vp, _vp,
+                                _vp, _f64, _f64, _u64, _u64, _u64, _vp, _vp, _vp, _vp, _vp)
+        self._vm_sample_keyed = L.fn("vm_sample", _int, _vp, _f64, _vp)
+        self._key_open = L.fn("key_open", None, _vp, _u64, _u64, _u32, _u32)
 
     # ---- RNG
     def key_draws(self, seed, counter, tag, id_, n):
@@ -297,6 +309,75 @@ class Oracle:
         u = np.ascontiguousarray(u, np.complex128)
         return self._su_unit(N, _ptr(u))
 
+    # ---- learned proposal
+    MLP_PARAMS = 5456
+    TAG_LEARN = 5
+    TAG_LEARNED = 6
+
+    def bf16(self, v):
+        return self._bf16(float(v))
+
+    def log_i0(self, x):
+        return self._log_i0(float(x))
+
+    def i1_over_i0(self, x):
+        return self._i1_i0(float(x))
+
+    def mlp_forward(self, params, x, emulate=True):
+        p = np.ascontiguousarray(params, np.float64)
+        x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+        out = np.zeros((x.shape[0], 16))
+        self._mlp_fwd(_ptr(p), x.shape[0], _ptr(x), int(emulate), _ptr(out))
+        return out
+
+    def vm_mixture(self, out16):
+        o = np.ascontiguousarray(out16, np.float64)
+        w, mu, k, li = (np.zeros(4) for _ in range(4))
+        self._mixture(_ptr(o), _ptr(w), _ptr(mu), _ptr(k), _ptr(li))
+        return w, mu, k, li
+
+    def vm_mixture_logpdf(self, out16, theta):
+        w, mu, k, li = self.vm_mixture(out16)
+        return self._mix_logpdf(_ptr(w), _ptr(mu), _ptr(k), _ptr(li), float(theta))
+
+    def vm_sample(self, kappa, seed, counter, tag, id_):
+        """Best-Fisher sample around 0 from the keyed stream (None if all trials fail)."""
+        g = (C.c_uint64 * 2)()
+        self._key_open(g, seed, counter, tag, id_)
+        a = C.c_double(0.0)
+        ok = self._vm_sample_keyed(g, float(kappa), C.byref(a))
+        return a.value if ok else None
+
+    def mlp_loss_grad(self, params, x, theta, emulate=True, grad=True):
+        p = np.ascontiguousarray(params, np.float64)
+        x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+        t = np.ascontiguousarray(theta, np.float64)
+        g = np.zeros(p.size) if grad else None
+        loss = self._mlp_grad(_ptr(p), x.shape[0], _ptr(x), _ptr(t), int(emulate), _ptr(g))
+        return loss, g
+
+    def adam_step(self, p, g, m, v, t, lr, b1=0.9, b2=0.999, eps=1e-8):
+        p, m, v = (np.array(a, np.float64, copy=True) for a in (p, m, v))
+        g = np.ascontiguousarray(g, np.float64)
+        self._adam(p.size, _ptr(p), _ptr(g), _ptr(m), _ptr(v), t, lr, b1, b2, eps)
+        return p, m, v
+
+    def u1_learned_metropolis(self, cells, inc, params, model_beta, driver_beta, seed, sweep0,
+                              n_sweeps, theta, given_out=None):
+        cells = np.ascontiguousarray(cells, np.uint32)
+        off, ic, iw = inc
+        t = np.array(theta, np.float64, copy=True)
+        p = np.ascontiguousarray(params, np.float64)
+        given = None if given_out is None else np.ascontiguousarray(given_out, np.float64)
+        obs = np.zeros((n_sweeps, 3))
+        margin = np.zeros(t.size)
+        dump = np.zeros((t.size, 16))
+        acc = np.zeros(t.size, np.uint8)
+        self._u1_learned(t.size, _ptr(cells), cells.shape[0], _ptr(off), _ptr(ic), _ptr(iw),
+                         _ptr(p), _ptr(given), model_beta, driver_beta, seed, sweep0, n_sweeps,
+                         _ptr(t), _ptr(obs), _ptr(margin), _ptr(dump), _ptr(acc))
+        return t, obs, margin, dump, acc
+
     def replica_exchange(self, betas, holder, energy, seed, round_, parity):
         """One exchange round: returns (new holder, accepted flags per slot)."""
         betas = np.ascontiguousarray(betas, np.float64)
@@ -334,6 +415,8 @@ class Reference:
                               _u64, _u64, _vp, _vp)
         self._u1_metro = L.fn("u1_metropolis", _int, _u64, _vp, _u64, _f64, _f64, _f64, _u32,
                               _u64, _u64, _u64, _vp, _vp)
+        self._u1_learned = L.fn("u1_learned_metropolis", _int, _u64, _vp, _u64, _vp, _vp, _vp, _vp,
+                                _f64, _f64, _u64, _u64, _u64, _vp, _vp)
         self._su_metro = L.fn("su_metropolis", _int, _u32, _u64, _vp, _u64, _f64, _f64, _f64, _u32,
                               _u64, _u64, _u64, _vp, _vp)
         self._su_expm = L.fn("su_expm", None, _u32, _vp, _vp)
@@ -447,6 +530,19 @@ class Reference:
         obs = np.zeros((n_sweeps, 3))
         st = self._xy_metro(n, _ptr(ei), _ptr(ej), len(ei), J, beta, width, seed, sweep0, n_sweeps,
                             _ptr(t), _ptr(obs))
+        assert st == 0, st
+        return t, obs
+
+    def u1_learned_metropolis(self, cells, inc, params, model_beta, driver_beta, seed, sweep0,
+                              n_sweeps, theta):
+        """Reference Metropolis driver with the learned proposal adapter; obs = mean plaquette."""
+        cells = np.ascontiguousarray(cells, np.uint32)
+        off, ic, iw = inc
+        t = np.array(theta, np.float64, copy=True)
+        p = np.ascontiguousarray(params, np.float64)
+        obs = np.zeros(n_sweeps)
+        st = self._u1_learned(t.size, _ptr(cells), cells.shape[0], _ptr(off), _ptr(ic), _ptr(iw),
+                              _ptr(p), model_beta, driver_beta, seed, sweep0, n_sweeps, _ptr(t), _ptr(obs))
         assert st == 0, st
         return t, obs
 

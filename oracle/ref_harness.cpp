@@ -52,6 +52,8 @@
 #include <term/plaquette.hpp>
 #include <term/sun_plaquette.hpp>
 
+#include "umc_oracle.h"
+
 namespace {
 
 constexpr std::uint32_t TAG_BOND = 1;
@@ -884,6 +886,117 @@ extern "C" int ref_bench_xy(std::uint64_t L, double beta, double width, std::uin
         for (double x : secs) worst = x > worst ? x : worst;
         *site_updates = double(threads) * double(L * L) * double(sweeps);
         *seconds = worst;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+// ------------------------------------------------------- learned U(1) proposal
+// A user Proposal (dof/proposal.hpp:8-12) whose density depends on the link's
+// staple.  It finds the link from cur - data() (the driver hands it the model's
+// own storage, driver.hpp:35-36), evaluates the oracle's network and mixture
+// for that staple, samples with the oracle's Best-Fisher trial fed by the
+// reference Pcg32 (each uni() is k 2^-32, so k is recovered exactly), and
+// returns log q(old) - log q(new).  The reference Metropolis driver supplies
+// dE (CellModel::energy_diff_at) and the accept step, so this pins the
+// learned update's composition against the reference driver itself.
+struct LearnedU1
+{
+    KeyState* ks;
+    const U1Link* base;
+    const std::uint32_t* cells;
+    const std::uint64_t* inc_off;
+    const std::uint32_t* inc_cell;
+    const std::uint8_t* inc_which;
+    const double* params;
+    mutable double w[4], mu[4], kappa[4], li[4];
+    mutable bool moved = false;
+
+    static std::uint32_t raw(double u) { return static_cast<std::uint32_t>(u * 4294967296.0); }
+
+    template <class R>
+    void sample(const U1Link* cur, R& rng, U1Link* out) const
+    {
+        const std::size_t i = static_cast<std::size_t>(cur - base);
+        ks->open(6u, i);
+        double Sr = 0.0, Si = 0.0;
+        for (std::uint64_t a = inc_off[i]; a < inc_off[i + 1]; ++a) {
+            const std::uint32_t* q = cells + 4 * std::uint64_t(inc_cell[a]);
+            const double t0 = base[q[0]].theta, t1 = base[q[1]].theta, t2 = base[q[2]].theta,
+                         t3 = base[q[3]].theta;
+            double phi;
+            switch (inc_which[a]) {
+            case 0: phi = t1 - t2 - t3; break;
+            case 1: phi = t0 - t2 - t3; break;
+            case 2: phi = t3 - t0 - t1; break;
+            default: phi = t2 - t0 - t1; break;
+            }
+            Sr += std::cos(phi);
+            Si += std::sin(phi);
+        }
+        double x[3], o[16];
+        orc_u1_features(Sr, Si, x);
+        orc_mlp_forward(params, 1, x, 1, o);
+        orc_vm_mixture(o, w, mu, kappa, li);
+        const int k = orc_vm_pick(w, raw(rng.uni()));
+        moved = false;
+        out->theta = cur->theta;
+        for (int t = 0; t < ORC_VM_TRIES; ++t) {
+            const std::uint32_t d1 = raw(rng.uni()), d2 = raw(rng.uni()), d3 = raw(rng.uni());
+            double a;
+            if (orc_vm_trial(kappa[k], d1, d2, d3, &a)) {
+                out->theta = std::remainder(mu[k] + a, 2.0 * 3.14159265358979323846);
+                moved = true;
+                break;
+            }
+        }
+    }
+    double log_ratio(const U1Link* cur, const U1Link* prop) const
+    {
+        if (!moved) return 0.0;
+        return orc_vm_mixture_logpdf(w, mu, kappa, li, cur->theta) -
+               orc_vm_mixture_logpdf(w, mu, kappa, li, prop->theta);
+    }
+};
+
+extern "C" int ref_u1_learned_metropolis(std::uint64_t n_links, const std::uint32_t* cells,
+                                         std::uint64_t n_cells, const std::uint64_t* inc_off,
+                                         const std::uint32_t* inc_cell, const std::uint8_t* inc_which,
+                                         const double* params, double model_beta, double driver_beta,
+                                         std::uint64_t seed, std::uint64_t sweep0, std::uint64_t n_sweeps,
+                                         double* theta, double* obs_out)
+{
+    try {
+        using CM = CellModel<U1Dof, U1PlaquetteTerm, CellComplex<4>>;
+        std::vector<Cell<4>> cl(n_cells);
+        for (std::uint64_t c = 0; c < n_cells; ++c)
+            for (int k = 0; k < 4; ++k) cl[c].sites[k] = cells[4 * c + k];
+        CM model(CellComplex<4>(n_links, cl), U1PlaquetteTerm{model_beta});
+        for (std::size_t i = 0; i < n_links; ++i) {
+            const U1Link l{theta[i]};
+            model.update(i, &l);
+        }
+        KeyState ks;
+        ks.seed = seed;
+        ks.counter = sweep0;
+        LearnedU1 prop{&ks, model.data(), cells, inc_off, inc_cell, inc_which, params, {}, {}, {}, {}};
+        Metropolis<CM, LearnedU1, KeyedRng> mc(model, prop, KeyedRng{&ks}, driver_beta);
+        std::uint64_t k = 0;
+        mc.sample(n_sweeps, [&](const CM& m) {
+            if (obs_out) {
+                double sum = 0.0;
+                for (std::size_t c = 0; c < m.cells(); ++c) {
+                    const auto s = m.cell_sites(c);
+                    const U1Link* ls[4] = {m.data() + s[0], m.data() + s[1], m.data() + s[2], m.data() + s[3]};
+                    sum += m.term().cos_plaquette(ls);
+                }
+                obs_out[k] = sum / double(m.cells());
+            }
+            ++k;
+            ++ks.counter;
+        });
+        for (std::size_t i = 0; i < n_links; ++i) theta[i] = model.data()[i].theta;
         return 0;
     } catch (...) {
         return status_of(std::current_exception());

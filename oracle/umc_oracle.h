@@ -168,6 +168,66 @@ void orc_su_expm(uint32_t N, const double* a, double* out);
 /* max_ij |(U^dagger U - I)_ij| (dof/sun.hpp:43-54). */
 double orc_su_unitarity_error(uint32_t N, const double* u);
 
+/* ---- learned U(1) proposal (umc_oracle_learn.c; no reference counterpart) -------
+ * Parameters: FP32 master values packed W1[3][64], b1[64], W2[64][64], b2[64],
+ * W3[64][16], b3[16] (row = input unit).  Outputs per link: 4 components x
+ * (logit, u, v, pre-softplus concentration), mean = atan2(v, u). */
+#define ORC_TAG_LEARN 5u   /* training minibatch selection */
+#define ORC_TAG_LEARNED 6u /* learned Metropolis-Hastings update, id = link */
+#define ORC_MLP_IN 3
+#define ORC_MLP_HIDDEN 64
+#define ORC_MLP_OUT 16
+#define ORC_MLP_W1 0
+#define ORC_MLP_B1 (ORC_MLP_W1 + ORC_MLP_IN * ORC_MLP_HIDDEN)
+#define ORC_MLP_W2 (ORC_MLP_B1 + ORC_MLP_HIDDEN)
+#define ORC_MLP_B2 (ORC_MLP_W2 + ORC_MLP_HIDDEN * ORC_MLP_HIDDEN)
+#define ORC_MLP_W3 (ORC_MLP_B2 + ORC_MLP_HIDDEN)
+#define ORC_MLP_B3 (ORC_MLP_W3 + ORC_MLP_HIDDEN * ORC_MLP_OUT)
+#define ORC_MLP_PARAMS (ORC_MLP_B3 + ORC_MLP_OUT)
+#define ORC_VM_COMPONENTS 4
+#define ORC_VM_KAPPA_MIN 1e-4
+#define ORC_VM_KAPPA_MAX 80.0
+#define ORC_VM_TRIES 32
+
+double orc_bf16(double v);
+double orc_log_i0(double x);
+double orc_i1_over_i0(double x);
+/* x[3] = (cos a, sin a, |S|) of the staple sum S = Sr + i Si ((1, 0, 0) for S = 0). */
+void orc_u1_features(double Sr, double Si, double* x);
+/* out[n][16]; emulate != 0 rounds operands to BF16 as the tensor-core path does. */
+void orc_mlp_forward(const double* params, uint64_t n, const double* x, int emulate, double* out);
+/* Mixture parameters of one output row; log_i0 may be NULL. */
+void orc_vm_mixture(const double* out16, double* w, double* mu, double* kappa, double* log_i0);
+double orc_vm_mixture_logpdf(const double* w, const double* mu, const double* kappa,
+                             const double* log_i0, double theta);
+/* Best-Fisher sample around 0; returns 0 if every trial was rejected. */
+int orc_vm_sample(orc_pcg32* g, double kappa, double* angle);
+/* One Best-Fisher trial from three raw draws (d3's top bit picks the sign). */
+int orc_vm_trial(double kappa, uint32_t d1, uint32_t d2, uint32_t d3, double* angle);
+/* Component index from one raw draw: smallest k with u < w_0 + ... + w_k. */
+int orc_vm_pick(const double* w, uint32_t d0);
+int orc_vm_mixture_sample(orc_pcg32* g, const double* w, const double* mu, const double* kappa,
+                          double* theta);
+/* Mean negative log-likelihood of targets theta[n] under the mixture the network
+ * gives for x[n][3]; grad (may be NULL) receives its gradient (ORC_MLP_PARAMS). */
+double orc_mlp_loss_grad(const double* params, uint64_t n, const double* x, const double* theta,
+                         int emulate, double* grad);
+/* One Adam step (Kingma & Ba 2015) with bias correction at step t >= 1. */
+void orc_adam_step(uint64_t n, double* p, const double* g, double* m, double* v, uint64_t t,
+                   double lr, double b1, double b2, double eps);
+/* Learned-proposal Metropolis-Hastings sweeps of U(1) links in index order
+ * (tables relabelled colour-major by the caller).  given_out (n_links x 16, one
+ * sweep only) replaces the network's outputs; out_dump receives the outputs of
+ * the last sweep.  obs per sweep: [S, mean plaquette, Q].  margin_out: log u -
+ * log_p of the accept test (+inf when accepted without a draw or no proposal). */
+void orc_u1_learned_metropolis(uint64_t n_links, const uint32_t* cells, uint64_t n_cells,
+                               const uint64_t* inc_offset, const uint32_t* inc_cell,
+                               const uint8_t* inc_which, const double* params,
+                               const double* given_out, double model_beta, double driver_beta,
+                               uint64_t seed, uint64_t sweep0, uint64_t n_sweeps, double* theta,
+                               double* obs_out, double* margin_out, double* out_dump,
+                               uint8_t* accepted);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,3 +96,16 @@ def square_plaquette_cells(L: int):
         for x in range(L):
             cells.append([y * L + x, L2 + y * L + (x + 1) % L, ((y + 1) % L) * L + x, L2 + y * L + x])
     return np.array(cells, np.uint32)
+
+
+def mlp_init(seed: int, scale: float = 1.0):
+    """Random parameters of the 3-64-64-16 proposal network (He-style scale),
+    packed W1[3][64], b1, W2[64][64], b2, W3[64][16], b3."""
+    rng = np.random.default_rng(seed)
+    W1 = rng.standard_normal((3, 64)) * np.sqrt(2 / 3) * scale
+    b1 = rng.standard_normal(64) * 0.1
+    W2 = rng.standard_normal((64, 64)) * np.sqrt(2 / 64) * scale
+    b2 = rng.standard_normal(64) * 0.1
+    W3 = rng.standard_normal((64, 16)) * np.sqrt(1 / 64) * scale
+    b3 = rng.standard_normal(16) * 0.1
+    return np.concatenate([W1.ravel(), b1, W2.ravel(), b2, W3.ravel(), b3]).astype(np.float32).astype(np.float64)
