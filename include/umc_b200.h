@@ -311,6 +311,99 @@ int umc_wolff_flip_noalloc(int32_t model, int32_t components, void* field, uint6
                            double coupling, double beta, uint64_t seed, uint64_t flip,
                            uint64_t* cluster_size, void* stream);
 
+/* ======================================= batched 2D U(1) chains, learned proposal */
+
+/* No counterpart in the reference (which has one chain per driver object and no
+ * learned proposals).  A chain is the reference's U(1) plaquette model
+ * (model/cell.hpp:64-78 with term/plaquette.hpp:34-47, S = beta sum_p (1 -
+ * cos theta_p)) on the periodic L x L square-plaquette complex (links
+ * mu L^2 + y L + x; plaquette (x, y) = [(0,x,y), (1,x+1,y), (0,x,y+1), (1,x,y)])
+ * under the Metropolis rule of driver.hpp:29-42.  Chain c draws with seed
+ * mix64(seed + 0x9E3779B97F4A7C15 (c + 1)), so with the plain proposal
+ * (U1Shift, dof/u1.hpp:36-52) it replays the single-chain U(1) sweep of that
+ * seed on the colour-major relabelled complex.  With a network the proposal is
+ * a 4-component von Mises mixture the network computes from the link's staple,
+ * accepted with min(1, exp(-beta dE + log q(old) - log q(new))) in FP64 (the
+ * Proposal contract of dof/proposal.hpp:5-12). */
+typedef struct umc_u1batch umc_u1batch;
+typedef struct umc_mlp umc_mlp;
+
+typedef struct umc_u1batch_desc {
+    uint32_t n_chains;
+    uint32_t L;            /* even, 4 .. 96 (a chain is held in shared memory) */
+    double beta;           /* Wilson coupling */
+    double width;          /* U1Shift width of the plain proposal */
+    uint64_t seed;
+    int32_t device;
+    void* stream;          /* cudaStream_t, NULL = own stream */
+    uint64_t max_records;  /* record slots (sweeps) between fetches; 0 = 1024 */
+} umc_u1batch_desc;
+
+/* Record per sweep and chain: [S, mean plaquette, topological charge
+ * Q = sum_p remainder(theta_p, 2 pi) / 2 pi, accepted updates], laid out
+ * [sweep][chain][4]. */
+#define UMC_U1_RECORD 4
+
+int umc_u1batch_create(const umc_u1batch_desc* desc, umc_u1batch** out);
+int umc_u1batch_destroy(umc_u1batch* b);
+/* Hot start: link i of chain c = pi (2u - 1), u the first draw of key
+ * (mix64(seed + golden (c + 1)), 0, init tag, i).  Creation leaves a cold start. */
+int umc_u1batch_randomize(umc_u1batch* b, uint64_t seed);
+/* Angles of one chain in the natural link order (2 L^2 floats). */
+int umc_u1batch_set_field(umc_u1batch* b, uint32_t chain, const float* theta);
+int umc_u1batch_get_field(umc_u1batch* b, uint32_t chain, float* theta);
+/* n sweeps of every chain: plain U1Shift when net is NULL, else the learned proposal. */
+int umc_u1batch_enqueue(umc_u1batch* b, uint64_t n_sweeps, const umc_mlp* net);
+int umc_u1batch_fetch(umc_u1batch* b, double* records, uint64_t max_sweeps, uint64_t* n_sweeps);
+int umc_u1batch_run(umc_u1batch* b, uint64_t n_sweeps, const umc_mlp* net, double* records);
+/* One learned sweep; outputs receives chain 0's 16 network outputs per link
+ * (natural link order), as the sweep computed them. */
+int umc_u1batch_run_dump(umc_u1batch* b, const umc_mlp* net, float* outputs);
+int umc_u1batch_counters(const umc_u1batch* b, uint64_t* sweeps, uint64_t* kernel_launches);
+int umc_u1batch_set_counter(umc_u1batch* b, uint64_t sweeps);
+int umc_u1batch_seeds(const umc_u1batch* b, uint64_t* chain_seeds);
+/* Resident CTAs of the plain and learned kernels (one chain per CTA at a time). */
+int umc_u1batch_config(const umc_u1batch* b, uint32_t* plain_grid, uint32_t* learned_grid);
+void* umc_u1batch_stream(const umc_u1batch* b);
+
+/* The proposal network: x = (cos a, sin a, |S|) of the staple sum S -> ReLU 64
+ * -> ReLU 64 -> 16 outputs, component k = (logit, u, v, rho): weight
+ * softmax(logit), mean atan2(v, u), concentration clamp(softplus(rho), 1e-4,
+ * 80).  BF16 tensor-core products with FP32 accumulation; FP32 master
+ * parameters packed W1[3][64], b1[64], W2[64][64], b2[64], W3[64][16], b3[16]. */
+#define UMC_MLP_PARAMS 5456
+
+typedef struct umc_mlp_desc {
+    uint64_t seed;         /* initial parameters and training minibatches */
+    int32_t device;
+    void* stream;
+    uint64_t max_configs;  /* training configurations held on the device (0 = none) */
+    uint32_t L;            /* their lattice side */
+} umc_mlp_desc;
+
+int umc_mlp_create(const umc_mlp_desc* desc, umc_mlp** out);
+int umc_mlp_destroy(umc_mlp* n);
+int umc_mlp_set_params(umc_mlp* n, const float* params);  /* also resets Adam */
+int umc_mlp_get_params(umc_mlp* n, float* params);
+/* out[n][16] for inputs x[n][3] (host arrays). */
+int umc_mlp_forward(umc_mlp* n, const float* x, uint64_t count, float* out);
+/* Mean negative log-likelihood of angles theta[n] given inputs x[n][3], and its
+ * gradient (UMC_MLP_PARAMS floats); either output may be NULL. */
+int umc_mlp_loss_grad(umc_mlp* n, const float* x, const float* theta, uint64_t count, double* loss, float* grad);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with a given gradient. */
+int umc_mlp_apply_gradient(umc_mlp* n, const float* grad, double lr);
+/* Appends the batch's current configurations (one per chain) to the dataset. */
+int umc_mlp_add_configs(umc_mlp* n, umc_u1batch* b);
+int umc_mlp_configs(const umc_mlp* n, uint64_t* count);
+int umc_mlp_clear_configs(umc_mlp* n);
+/* steps Adam steps on minibatches of `batch` links drawn uniformly from the
+ * dataset (key (seed, step, learn tag, sample)); losses[step] = minibatch mean
+ * NLL before the step (may be NULL).  Do not train a network while a batch
+ * that uses it is still running. */
+int umc_mlp_train(umc_mlp* n, uint64_t steps, uint32_t batch, double lr, double* losses);
+int umc_mlp_counters(const umc_mlp* n, uint64_t* steps, uint64_t* kernel_launches);
+void* umc_mlp_stream(const umc_mlp* n);
+
 /* ================================================= series statistics (host) */
 
 /* No counterpart in the reference (its tests compare chain means against fixed

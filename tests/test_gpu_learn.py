@@ -1,0 +1,189 @@
+"""GPU parity of the learned U(1) proposal and the batched U(1) chains.
+
+- the tensor-core forward and gradient against the FP64 oracle network (which
+  rounds the same operands to BF16), Adam against the oracle's Adam;
+- one plain batched sweep per chain against the single-chain oracle with that
+  chain's seed (near-margin decisions exempted and counted);
+- one learned sweep given the network outputs the GPU computed: proposals and
+  decisions against the oracle's Metropolis-Hastings step;
+- long learned chains sample the exact 2D U(1) torus distribution;
+- training on plain-chain configurations lowers the loss to the exact
+  conditional's entropy and lowers the plaquette's autocorrelation time.
+"""
+import numpy as np
+import pytest
+
+from helpers import link_class_position, mlp_init, relabel_cells, square_plaquette_cells
+from test_oracle_learn import torus_plaquette
+
+pytestmark = pytest.mark.gpu
+
+MARGIN = 1e-3
+
+
+def _tables(oracle, L):
+    pos = link_class_position(L, 2)
+    cells = relabel_cells(square_plaquette_cells(L), pos)
+    inc = oracle.cell_incidence(2 * L * L, cells)[1:]
+    return pos, cells, inc
+
+
+def _inputs(n, seed):
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(-np.pi, np.pi, n)
+    r = rng.uniform(0, 2, n)
+    return np.stack([np.cos(a), np.sin(a), r], 1).astype(np.float32), rng.uniform(-np.pi, np.pi, n).astype(np.float32)
+
+
+def test_forward_matches_oracle(umc, oracle):
+    P = mlp_init(21).astype(np.float32)
+    net = umc.ProposalNet(1)
+    net.set_params(P)
+    x, _ = _inputs(1000, 1)  # not a multiple of the 128-row tile
+    got = net.forward(x)
+    ref = oracle.mlp_forward(P.astype(np.float64), x.astype(np.float64), emulate=True)
+    err = np.abs(got - ref)
+    # BF16 rounding of a hidden unit may flip where FP32 and FP64 sums straddle
+    # a rounding boundary; everything else agrees to FP32 accumulation error.
+    assert np.quantile(err, 0.99) < 1e-4, np.quantile(err, 0.99)
+    assert err.max() < 0.05 * (1 + np.abs(ref).max())
+
+
+def test_loss_and_gradient_match_oracle(umc, oracle):
+    P = mlp_init(22).astype(np.float32)
+    net = umc.ProposalNet(1)
+    net.set_params(P)
+    x, th = _inputs(4096, 2)
+    loss, g = net.loss_grad(x, th)
+    lo, go = oracle.mlp_loss_grad(P.astype(np.float64), x.astype(np.float64), th.astype(np.float64), emulate=True)
+    assert loss == pytest.approx(lo, rel=1e-4)
+    # backward operands are BF16 on the GPU: compare each parameter block in norm
+    for a, b in [(0, 192), (192, 256), (256, 4352), (4352, 4416), (4416, 5440), (5440, 5456)]:
+        rel = np.linalg.norm(g[a:b] - go[a:b]) / np.linalg.norm(go[a:b])
+        assert rel < 2e-2, (a, b, rel)
+    cos = g @ go / np.linalg.norm(g) / np.linalg.norm(go)
+    assert cos > 0.9995
+
+
+def test_adam_matches_oracle(umc, oracle):
+    P = mlp_init(23).astype(np.float32)
+    net = umc.ProposalNet(1)
+    net.set_params(P)
+    rng = np.random.default_rng(3)
+    p, m, v = P.astype(np.float64), np.zeros(P.size), np.zeros(P.size)
+    for t in range(1, 4):
+        g = rng.standard_normal(P.size).astype(np.float32)
+        net.apply_gradient(g, 1e-3)
+        p, m, v = oracle.adam_step(p, g.astype(np.float64), m, v, t, 1e-3)
+    np.testing.assert_allclose(net.get_params(), p, rtol=1e-5, atol=1e-6)
+    assert net.counters()[0] == 3
+
+
+@pytest.mark.parametrize("L,beta", [(8, 2.0), (6, 0.7), (16, 5.0)])
+def test_plain_sweep_matches_single_chain_oracle(umc, oracle, L, beta):
+    pos, cells, inc = _tables(oracle, L)
+    b = umc.U1Batch(3, L, beta, width=0.5, seed=17)
+    b.randomize(5)
+    seeds = b.seeds()
+    skipped = total = 0
+    for sweep in range(2):
+        start = [b.get_field(c).astype(np.float64) for c in range(3)]
+        rec = b.run(1)
+        for c in range(3):
+            cm = np.empty(2 * L * L)
+            cm[pos] = start[c]
+            t_o, obs, margin = oracle.u1_metropolis(cells, inc, beta, 1.0, 0.5, 1, int(seeds[c]), sweep, 1, cm)
+            got = np.empty(2 * L * L)
+            got[pos] = b.get_field(c)
+            near = np.abs(margin) < MARGIN
+            d = np.abs(np.remainder(got - t_o + np.pi, 2 * np.pi) - np.pi)
+            bad = (d > 1e-4) & ~near
+            total += got.size
+            skipped += int(near.sum())
+            assert bad.sum() <= 2 * near.sum(), (c, np.flatnonzero(bad)[:8])
+            assert rec[0, c, 1] == pytest.approx(oracle.u1_mean_plaquette(cells, got), abs=1e-5)
+            assert rec[0, c, 2] == pytest.approx(oracle.u1_topological_charge(cells, got), abs=1e-3)
+    assert skipped < 0.01 * total
+
+
+@pytest.mark.parametrize("L,beta", [(8, 2.0), (16, 6.0)])
+def test_learned_sweep_matches_oracle_given_outputs(umc, oracle, L, beta):
+    pos, cells, inc = _tables(oracle, L)
+    P = mlp_init(24).astype(np.float32)
+    net = umc.ProposalNet(1)
+    net.set_params(P)
+    b = umc.U1Batch(2, L, beta, seed=9)
+    b.randomize(2)
+    seed0 = int(b.seeds()[0])
+    start = b.get_field(0).astype(np.float64)
+    out = b.run_dump(net)  # natural link order
+    cm = np.empty(2 * L * L)
+    cm[pos] = start
+    given = np.empty((2 * L * L, 16))
+    given[pos] = out
+    t_o, obs, margin, dump, acc = oracle.u1_learned_metropolis(cells, inc, P.astype(np.float64), beta, 1.0, seed0, 0,
+                                                               1, cm, given_out=given)
+    got = np.empty(2 * L * L)
+    got[pos] = b.get_field(0)
+    d = np.abs(np.remainder(got - t_o + np.pi, 2 * np.pi) - np.pi)
+    near = np.abs(margin) < MARGIN
+    bad = (d > 1e-3) & ~near
+    assert bad.sum() <= 2 + 2 * near.sum(), np.flatnonzero(bad)[:8]
+    assert 0.2 < acc.mean() <= 1.0
+    # the outputs themselves: the oracle network on the features the GPU saw
+    # (first colour class only: its staples are untouched by the sweep)
+    half = L * L // 2
+    _, _, _, dump0, _ = oracle.u1_learned_metropolis(cells, inc, P.astype(np.float64), beta, 1.0, seed0, 0, 1, cm)
+    err = np.abs(dump0[:half] - given[:half])
+    assert np.quantile(err, 0.99) < 1e-3 and err.max() < 0.1
+
+
+def test_learned_chains_sample_the_exact_distribution(umc):
+    """Detailed balance with an untrained network: mean plaquette of 128
+    chains (4 x 4 torus, beta 1.5) equals the exact value."""
+    L, beta = 4, 1.5
+    net = umc.ProposalNet(5)
+    b = umc.U1Batch(128, L, beta, seed=3, max_records=4000)
+    b.randomize(1)
+    b.run(200, net, records=False)
+    rec = b.run(3000, net)
+    per_chain = rec[:, :, 1].mean(0)
+    m, err = per_chain.mean(), per_chain.std(ddof=1) / np.sqrt(per_chain.size)
+    exact = torus_plaquette(beta, L * L)
+    assert abs(m - exact) < 4 * err + 2e-4, (m, err, exact)
+    plain = umc.U1Batch(128, L, beta, seed=4, max_records=4000)
+    plain.randomize(2)
+    plain.run(200, records=False)
+    pc = plain.run(3000)[:, :, 1].mean(0)
+    assert abs(pc.mean() - exact) < 4 * pc.std(ddof=1) / np.sqrt(pc.size) + 2e-4
+
+
+def test_training_learns_the_conditional_and_reduces_tau(umc):
+    L, beta = 16, 4.0
+    plain = umc.U1Batch(256, L, beta, seed=11, max_records=4096)
+    plain.randomize(3)
+    plain.run(300, records=False)
+    net = umc.ProposalNet(7, max_configs=256 * 20, L=L)
+    for _ in range(20):
+        plain.run(5, records=False)
+        net.add_configs(plain)
+    assert net.configs() == 256 * 20
+    losses = net.train(400, batch=8192, lr=3e-3)
+    assert np.all(np.isfinite(losses))
+    assert losses[-20:].mean() < losses[:5].mean() - 0.3
+    # exact conditional: von Mises(kappa = beta |S|): entropy log(2 pi I0) - kappa A
+    learned = umc.U1Batch(256, L, beta, seed=12, max_records=4096)
+    for c in range(256):
+        learned.set_field(c, plain.get_field(c))
+    rec_l = learned.run(2000, net)
+    rec_p = plain.run(2000)
+    acc_l = rec_l[:, :, 3].mean() / (2 * L * L)
+    acc_p = rec_p[:, :, 3].mean() / (2 * L * L)
+    assert acc_l > 0.85 and acc_l > acc_p
+    tl = np.mean([umc.tau_int(rec_l[:, c, 1])[0] for c in range(0, 256, 8)])
+    tp = np.mean([umc.tau_int(rec_p[:, c, 1])[0] for c in range(0, 256, 8)])
+    assert tl < 0.8 * tp, (tl, tp)
+    # matched observables within the statistical error
+    pl, pp = rec_l[:, :, 1].mean(0), rec_p[:, :, 1].mean(0)
+    err = np.hypot(pl.std(ddof=1), pp.std(ddof=1)) / np.sqrt(256)
+    assert abs(pl.mean() - pp.mean()) < 4 * err

@@ -406,9 +406,9 @@ class Chain:
 
     def close(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:  # module globals are gone at interpreter exit
             lib.umc_chain_destroy(h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         self.close()
@@ -538,9 +538,9 @@ class Batch:
 
     def close(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:  # module globals are gone at interpreter exit
             lib.umc_batch_destroy(h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         self.close()
@@ -604,6 +604,213 @@ class Batch:
 
     def stream(self) -> int:
         return lib.umc_batch_stream(self._h) or 0
+
+
+# ============================================== batched U(1), learned proposal
+class U1BatchDesc(C.Structure):
+    _fields_ = [
+        ("n_chains", _u32),
+        ("L", _u32),
+        ("beta", _f64),
+        ("width", _f64),
+        ("seed", _u64),
+        ("device", _i32),
+        ("stream", _vp),
+        ("max_records", _u64),
+    ]
+
+
+class MlpDesc(C.Structure):
+    _fields_ = [
+        ("seed", _u64),
+        ("device", _i32),
+        ("stream", _vp),
+        ("max_configs", _u64),
+        ("L", _u32),
+    ]
+
+
+MLP_PARAMS = 5456
+U1_RECORD = 4
+_decl("umc_u1batch_create", _int, C.POINTER(U1BatchDesc), C.POINTER(_vp))
+_decl("umc_u1batch_destroy", _int, _vp)
+_decl("umc_u1batch_randomize", _int, _vp, _u64)
+_decl("umc_u1batch_set_field", _int, _vp, _u32, _vp)
+_decl("umc_u1batch_get_field", _int, _vp, _u32, _vp)
+_decl("umc_u1batch_enqueue", _int, _vp, _u64, _vp)
+_decl("umc_u1batch_fetch", _int, _vp, _vp, _u64, C.POINTER(_u64))
+_decl("umc_u1batch_run", _int, _vp, _u64, _vp, _vp)
+_decl("umc_u1batch_run_dump", _int, _vp, _vp, _vp)
+_decl("umc_u1batch_counters", _int, _vp, C.POINTER(_u64), C.POINTER(_u64))
+_decl("umc_u1batch_set_counter", _int, _vp, _u64)
+_decl("umc_u1batch_seeds", _int, _vp, _vp)
+_decl("umc_u1batch_config", _int, _vp, C.POINTER(_u32), C.POINTER(_u32))
+_decl("umc_u1batch_stream", _vp, _vp)
+_decl("umc_mlp_create", _int, C.POINTER(MlpDesc), C.POINTER(_vp))
+_decl("umc_mlp_destroy", _int, _vp)
+_decl("umc_mlp_set_params", _int, _vp, _vp)
+_decl("umc_mlp_get_params", _int, _vp, _vp)
+_decl("umc_mlp_forward", _int, _vp, _vp, _u64, _vp)
+_decl("umc_mlp_loss_grad", _int, _vp, _vp, _vp, _u64, C.POINTER(_f64), _vp)
+_decl("umc_mlp_apply_gradient", _int, _vp, _vp, _f64)
+_decl("umc_mlp_add_configs", _int, _vp, _vp)
+_decl("umc_mlp_configs", _int, _vp, C.POINTER(_u64))
+_decl("umc_mlp_clear_configs", _int, _vp)
+_decl("umc_mlp_train", _int, _vp, _u64, _u32, _f64, _vp)
+_decl("umc_mlp_counters", _int, _vp, C.POINTER(_u64), C.POINTER(_u64))
+_decl("umc_mlp_stream", _vp, _vp)
+
+
+class ProposalNet:
+    """The learned proposal's network (umc_mlp_*): staple features -> 4-component
+    von Mises mixture, BF16 tensor-core forward/backward, Adam on FP32 masters.
+    With max_configs > 0 it holds that many L x L training configurations."""
+
+    def __init__(self, seed=1, *, device=0, max_configs=0, L=0):
+        d = MlpDesc()
+        d.seed, d.device, d.stream, d.max_configs, d.L = seed, device, None, max_configs, L
+        h = _vp()
+        check(lib.umc_mlp_create(C.byref(d), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h and lib is not None:  # module globals are gone at interpreter exit
+            lib.umc_mlp_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_params(self, p):
+        a = np.ascontiguousarray(p, np.float32)
+        if a.size != MLP_PARAMS:
+            raise ValueError("wrong parameter count")
+        check(lib.umc_mlp_set_params(self._h, _ptr(a)))
+
+    def get_params(self):
+        a = np.zeros(MLP_PARAMS, np.float32)
+        check(lib.umc_mlp_get_params(self._h, _ptr(a)))
+        return a
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, 3)
+        out = np.zeros((x.shape[0], 16), np.float32)
+        check(lib.umc_mlp_forward(self._h, _ptr(x), x.shape[0], _ptr(out)))
+        return out
+
+    def loss_grad(self, x, theta):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(theta, np.float32)
+        g = np.zeros(MLP_PARAMS, np.float32)
+        loss = _f64(0)
+        check(lib.umc_mlp_loss_grad(self._h, _ptr(x), _ptr(t), x.shape[0], C.byref(loss), _ptr(g)))
+        return loss.value, g
+
+    def apply_gradient(self, g, lr):
+        a = np.ascontiguousarray(g, np.float32)
+        check(lib.umc_mlp_apply_gradient(self._h, _ptr(a), lr))
+
+    def add_configs(self, batch: "U1Batch"):
+        check(lib.umc_mlp_add_configs(self._h, batch._h))
+
+    def configs(self) -> int:
+        n = _u64(0)
+        check(lib.umc_mlp_configs(self._h, C.byref(n)))
+        return n.value
+
+    def clear_configs(self):
+        check(lib.umc_mlp_clear_configs(self._h))
+
+    def train(self, steps, batch=8192, lr=1e-3):
+        losses = np.zeros(steps)
+        check(lib.umc_mlp_train(self._h, steps, batch, lr, _ptr(losses)))
+        return losses
+
+    def counters(self):
+        s, k = _u64(0), _u64(0)
+        check(lib.umc_mlp_counters(self._h, C.byref(s), C.byref(k)))
+        return s.value, k.value
+
+
+class U1Batch:
+    """Independent 2D U(1) chains (umc_u1batch_*): plain U1Shift Metropolis, or
+    Metropolis-Hastings with a ProposalNet.  Records per sweep and chain:
+    [S, mean plaquette, Q, accepted]."""
+
+    def __init__(self, n_chains, L, beta, *, width=0.5, seed=1, device=0, max_records=1024):
+        d = U1BatchDesc()
+        d.n_chains, d.L, d.beta, d.width = n_chains, L, beta, width
+        d.seed, d.device, d.stream, d.max_records = seed, device, None, max_records
+        h = _vp()
+        check(lib.umc_u1batch_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.n_chains, self.L, self.beta, self.width = n_chains, L, beta, width
+        self.max_records = max_records or 1024
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h and lib is not None:  # module globals are gone at interpreter exit
+            lib.umc_u1batch_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def randomize(self, seed):
+        check(lib.umc_u1batch_randomize(self._h, seed))
+
+    def set_field(self, chain, theta):
+        a = np.ascontiguousarray(theta, np.float32).reshape(-1)
+        if a.size != 2 * self.L * self.L:
+            raise ValueError("wrong field size")
+        check(lib.umc_u1batch_set_field(self._h, chain, _ptr(a)))
+
+    def get_field(self, chain):
+        a = np.zeros(2 * self.L * self.L, np.float32)
+        check(lib.umc_u1batch_get_field(self._h, chain, _ptr(a)))
+        return a
+
+    def run(self, n_sweeps, net: ProposalNet | None = None, records=True):
+        rec = np.zeros((n_sweeps, self.n_chains, U1_RECORD)) if records else None
+        check(lib.umc_u1batch_run(self._h, n_sweeps, net._h if net else None, _ptr(rec)))
+        return rec
+
+    def enqueue(self, n_sweeps, net: ProposalNet | None = None):
+        check(lib.umc_u1batch_enqueue(self._h, n_sweeps, net._h if net else None))
+
+    def fetch(self, capacity=None):
+        capacity = capacity or self.max_records
+        rec = np.zeros((capacity, self.n_chains, U1_RECORD))
+        got = _u64(0)
+        check(lib.umc_u1batch_fetch(self._h, _ptr(rec), capacity, C.byref(got)))
+        return rec[: got.value]
+
+    def run_dump(self, net: ProposalNet):
+        out = np.zeros((2 * self.L * self.L, 16), np.float32)
+        check(lib.umc_u1batch_run_dump(self._h, net._h, _ptr(out)))
+        return out
+
+    def counters(self):
+        s, k = _u64(0), _u64(0)
+        check(lib.umc_u1batch_counters(self._h, C.byref(s), C.byref(k)))
+        return s.value, k.value
+
+    def set_counter(self, sweeps):
+        check(lib.umc_u1batch_set_counter(self._h, sweeps))
+
+    def seeds(self):
+        s = np.zeros(self.n_chains, np.uint64)
+        check(lib.umc_u1batch_seeds(self._h, _ptr(s)))
+        return s
+
+    def config(self):
+        a, b = _u32(0), _u32(0)
+        check(lib.umc_u1batch_config(self._h, C.byref(a), C.byref(b)))
+        return {"plain_grid": a.value, "learned_grid": b.value}
+
+    def stream(self) -> int:
+        return lib.umc_u1batch_stream(self._h) or 0
 
 
 # ========================================================= reference mirror
