@@ -49,8 +49,10 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", choices=["o3", "ising", "su3", "xybatch"], default="o3",
-                   help="o3: the headline configuration; ising / su3: secondary roofline runs")
+    p.add_argument("--workload", choices=["o3", "ising", "su3", "xybatch", "u1learned"], default="o3",
+                   help="o3: the headline configuration; ising / su3 / xybatch: secondary roofline runs; "
+                        "u1learned: the learned-proposal study (effective samples/s)")
+    p.add_argument("--no-learned", action="store_true", help="skip the learned-proposal summary of the o3 line")
     return p.parse_args()
 
 
@@ -255,14 +257,15 @@ class O3Hybrid:
 
 class IsingSweep:
     """Plain Ising Metropolis (Flip, J=1, beta=0.44) on an L x L lattice; step =
-    one sweep.  At the default L = 32768 the int8 field is 1 GiB, far above L2."""
+    one sweep.  At the default L = 32000 the int8 field is 0.95 GiB, far above L2
+    (32768 would exceed the reference's uint32 bond count)."""
 
     name = "ising"
     unit = "site-updates/s"
     dtype = "i8"
 
     def __init__(self, umc, args, rank, local):
-        self.L = args.L if args.L != L_DEFAULT else 32768
+        self.L = args.L if args.L != L_DEFAULT else 32000
         self.n = self.L * self.L
         g = umc.square_lattice(self.L, self.L)
         self.ch = umc.Chain(umc.MODEL_ISING, graph=g, coupling=1, proposal=umc.PROPOSAL_FLIP, seed=1 + rank,
@@ -424,6 +427,140 @@ class XYBatch:
                           f"U1Shift, stock driver), {sec:.1f} s"}
 
 
+# ------------------------------------------------------- learned U(1) study
+LEARN_BETAS = (2.0, 4.0, 6.0, 8.0)
+
+
+def _timed_sweeps(torch, b, n, net, chunk=100):
+    """n sweeps of every chain of the batch in launches of `chunk` sweeps, each
+    launch timed with CUDA events on the batch's stream and preceded (outside
+    the events) by a 256 MiB write that evicts the chains from L2."""
+    import numpy as np
+
+    s = torch.cuda.ExternalStream(b.stream())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    recs, ms = [], 0.0
+    done = 0
+    torch.cuda.synchronize()
+    while done < n:
+        k = min(chunk, n - done)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(s):
+            flush.fill_(done & 0xFF)
+            e0.record(s)
+            b.enqueue(k, net)
+            e1.record(s)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        recs.append(b.fetch(k))
+        done += k
+    return np.concatenate(recs), ms / n
+
+
+def _chain_ms_per_sweep(torch, ch, n):
+    s = torch.cuda.ExternalStream(ch.stream())
+    ch.enqueue_metropolis(1.0, 20)
+    ch.fetch(8192)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    ch.enqueue_metropolis(1.0, n)
+    e1.record(s)
+    e1.synchronize()
+    ch.fetch(8192)
+    return e0.elapsed_time(e1) / n
+
+
+def torus_plaquette(beta, n_plaq):
+    """Exact <cos theta_p> of 2D U(1) (Wilson action) on a periodic torus of
+    n_plaq plaquettes: Z = sum_n I_n(beta)^n_plaq (character expansion), so
+    <P> = sum_n I_n^(n_plaq - 1) I_n' / sum_n I_n^n_plaq, I_n' = (I_{n-1} + I_{n+1}) / 2."""
+    import numpy as np
+    import scipy.special as sp
+
+    ns = np.arange(-60, 61)
+    li = np.log(sp.ive(ns, beta))
+    ld = np.log(0.5 * (sp.ive(ns - 1, beta) + sp.ive(ns + 1, beta)))
+    a = (n_plaq - 1) * li + ld
+    b = n_plaq * li
+    lse = lambda v: v.max() + np.log(np.exp(v - v.max()).sum())
+    return float(np.exp(lse(a) - lse(b)))
+
+
+def learned_study(umc, torch, betas=LEARN_BETAS, L=64, chains=444, n_configs=20000, train_steps=1500,
+                  batch=16384, lr=3e-3, therm=3000, meas=4000, seed=1):
+    """Effective independent samples per second of the plaquette P and the
+    topological charge Q on 2D U(1) L x L, for plain U1Shift(0.5) Metropolis on
+    one chain (the faster of the single-chain engine and the batch kernel with
+    one chain), plain batched, and learned batched (the network trained on
+    n_configs plain-chain configurations of the same beta).  Effective samples
+    per second = chains x sweeps per second / (2 tau_int), tau_int pooled over
+    the chains (umc.tau_int_multi)."""
+    import numpy as np
+
+    out = {}
+    for beta in betas:
+        t_start = time.perf_counter()
+        plain = umc.U1Batch(chains, L, beta, width=0.5, seed=seed, max_records=max(meas, 200))
+        plain.randomize(seed + 100)
+        plain.run(therm, records=False)
+        snaps = -(-n_configs // chains)
+        net = umc.ProposalNet(seed + 7, max_configs=snaps * chains, L=L)
+        for _ in range(snaps):
+            plain.run(5, records=False)
+            net.add_configs(plain)
+        t0 = time.perf_counter()
+        losses = net.train(train_steps, batch=batch, lr=lr)
+        train_s = time.perf_counter() - t0
+        learned = umc.U1Batch(chains, L, beta, seed=seed + 1, max_records=max(meas, 200))
+        for c in range(chains):
+            learned.set_field(c, plain.get_field(c))
+        learned.run(20, net, records=False)
+        rec_p, ms_p = _timed_sweeps(torch, plain, meas, None)
+        rec_l, ms_l = _timed_sweeps(torch, learned, meas, net)
+        one = umc.U1Batch(1, L, beta, width=0.5, seed=seed, max_records=1000)
+        one.set_field(0, plain.get_field(0))
+        _, ms_one = _timed_sweeps(torch, one, 1000, None, chunk=1000)
+        ch = umc.Chain(umc.MODEL_U1, cells=umc.square_plaquettes(L), coupling=beta, proposal=umc.PROPOSAL_U1SHIFT,
+                       width=0.5, seed=seed, max_records=8192)
+        ch.set_field(plain.get_field(0))
+        ms_chain = _chain_ms_per_sweep(torch, ch, 1000)
+        ms_single = min(ms_one, ms_chain)
+        row = {"ms_per_sweep": {"plain_single_chain": ms_single, "plain_single_chain_engine": ms_chain,
+                                "plain_batch_kernel_one_chain": ms_one, "plain_batched": ms_p,
+                                "learned_batched": ms_l},
+               "acceptance": {"plain": float(rec_p[:, :, 3].mean() / (2 * L * L)),
+                              "learned": float(rec_l[:, :, 3].mean() / (2 * L * L))},
+               "train": {"configs": net.configs(), "steps": train_steps, "batch": batch, "lr": lr,
+                         "loss_first": float(losses[0]), "loss_last": float(np.mean(losses[-20:])),
+                         "seconds": train_s}}
+        for name, idx in (("plaquette", 1), ("Q", 2)):
+            tp, ep, wp = umc.tau_int_multi(rec_p[:, :, idx].T)
+            tl, el, wl = umc.tau_int_multi(rec_l[:, :, idx].T)
+            mp, ml = rec_p[:, :, idx].mean(0), rec_l[:, :, idx].mean(0)
+            err = float(np.hypot(mp.std(ddof=1), ml.std(ddof=1)) / np.sqrt(chains))
+            eff = {"plain_single_chain": 1e3 / ms_single / (2 * tp),
+                   "plain_batched": chains * 1e3 / ms_p / (2 * tp),
+                   "learned_batched": chains * 1e3 / ms_l / (2 * tl)}
+            if name == "plaquette":
+                exact = torus_plaquette(beta, L * L)
+                row["exact_plaquette"] = exact
+                row["z_vs_exact"] = {"plain": float((mp.mean() - exact) / (mp.std(ddof=1) / np.sqrt(chains))),
+                                     "learned": float((ml.mean() - exact) / (ml.std(ddof=1) / np.sqrt(chains)))}
+            row[name] = {"tau_int": {"plain": tp, "plain_err": ep, "learned": tl, "learned_err": el},
+                         "tau_converged": {"plain": wp < meas // 2, "learned": wl < meas // 2},
+                         "effective_samples_per_s": eff,
+                         "learned_batched_over_plain_single": eff["learned_batched"] / eff["plain_single_chain"],
+                         "learned_over_plain_at_equal_batch": eff["learned_batched"] / eff["plain_batched"],
+                         "mean": {"plain": float(mp.mean()), "learned": float(ml.mean()),
+                                  "z": float((ml.mean() - mp.mean()) / err) if err > 0 else 0.0}}
+        row["seconds"] = time.perf_counter() - t_start
+        out[f"beta={beta:g}"] = row
+        for o in (plain, learned, one, net):
+            o.close()
+    return out
+
+
 class _BatchAsChain:
     """The few chain methods the timing loop uses, for a batch."""
 
@@ -452,11 +589,40 @@ class _BatchAsChain:
 WORKLOADS = {"o3": O3Hybrid, "ising": IsingSweep, "su3": SU3Sweep, "xybatch": XYBatch}
 
 
+def run_learned(args):
+    """--workload u1learned: the full study, one JSON line."""
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(0)
+    import universal_classical_montecarlo_b200 as umc
+
+    sampler = ClockSampler("GPU-" + str(torch.cuda.get_device_properties(0).uuid))
+    sampler.start()
+    time.sleep(0.3)
+    study = learned_study(umc, torch, meas=args.steps if args.steps != 4000 else 4000)
+    clocks = sampler.stop()
+    eff = [row["plaquette"]["effective_samples_per_s"]["learned_batched"] for row in study.values()]
+    line = {"metric": METRIC, "value": float(np.exp(np.mean(np.log(eff)))),
+            "unit": "effective samples/s (plaquette, geometric mean over beta)", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "learned proposal on 2D U(1) 64x64, beta in {2,4,6,8}, 444 chains per batch, "
+                                   "plain U1Shift 0.5 vs MLP 3-64-64-16 (BF16 tcgen05) 4-component von Mises "
+                                   "mixture trained on 20000 plain-chain configurations per beta",
+                       "l2": "256 MiB flush between timed launches of 100 sweeps"},
+            "per_beta": study, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------------- umc
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "u1learned":
+        run_learned(args)
         return
     ws, rank, local = rank_info()
     import torch

@@ -412,6 +412,13 @@ void* umc_mlp_stream(const umc_mlp* n);
  * W the first window with W >= c * tau(W) (c <= 0 selects 6).  tau_err is the
  * Madras-Sokal estimate tau * sqrt(2 (2W+1) / n).  Any output may be NULL. */
 int umc_tau_int(const double* x, uint64_t n, double c, double* tau, double* tau_err, uint64_t* window);
+/* The same for `series` independent chains of `length` values each (x laid out
+ * [series][length]): every series is centred on its own mean and the
+ * autocovariances are averaged over the series (a chain frozen at a constant
+ * value contributes nothing; all frozen gives tau = 0.5, window 0).  The error
+ * uses the pooled count series * length. */
+int umc_tau_int_multi(const double* x, uint64_t series, uint64_t length, double c, double* tau, double* tau_err,
+                      uint64_t* window);
 /* Mean and its standard error from the means of floor(n/bin) bins of `bin`
  * consecutive values (at least two bins). */
 int umc_binning_error(const double* x, uint64_t n, uint64_t bin, double* mean, double* err);

@@ -87,6 +87,7 @@ class Oracle:
         self._pcg_draws = L.fn("pcg32_draws", None, _u64, _u64, _u32, _vp)
         self._key_seed = L.fn("key_seed", _u64, _u64, _u64, _u32)
         self._stream_id = L.fn("stream_id", _u32, _u32)
+        self._id_seed = L.fn("id_seed", _u64, _u64, _u32)
         self._pair_graph = L.fn("pair_graph", _int, _u64, _vp, _vp, _u64, _int, _vp, _vp, _vp)
         self._square = L.fn("square_edges", C.c_int64, _u64, _u64, _vp, _vp)
         self._cubic = L.fn("cubic_edges", C.c_int64, _u64, _u64, _u64, _vp, _vp)
@@ -144,6 +145,9 @@ class Oracle:
 
     def stream_id(self, i):
         return int(self._stream_id(i))
+
+    def id_seed(self, kseed, i):
+        return int(self._id_seed(kseed, i))
 
     # ---- tables
     def pair_graph(self, n, ei, ej, symmetric=True):

@@ -8,7 +8,7 @@
 // driver reads from:
 //
 //   KeyState / KeyedRng  one reference Pcg32 (rng.hpp:8-44), re-seeded per key
-//                        Pcg32(key_seed(seed, counter, tag), stream_id(id));
+//                        Pcg32(id_seed(key_seed(seed, counter, tag), id), 0);
 //   Keyed<Q>             a proposal adapter that re-keys on the site index it is
 //                        handed (cur - data(), driver.hpp:35-36) before calling
 //                        the reference proposal;
@@ -73,16 +73,6 @@ std::uint64_t key_seed(std::uint64_t seed, std::uint64_t counter, std::uint32_t 
 {
     return mix64(mix64(seed ^ (std::uint64_t(tag) << 32)) + counter * 0x9E3779B97F4A7C15ULL);
 }
-std::uint32_t stream_id(std::uint32_t x)
-{
-    x ^= x >> 16;
-    x *= 0x7feb352dU;
-    x ^= x >> 15;
-    x *= 0x846ca68bU;
-    x ^= x >> 16;
-    return x;
-}
-
 struct KeyState
 {
     std::uint64_t seed = 0;
@@ -90,7 +80,9 @@ struct KeyState
     Pcg32 gen{0, 0};
     void open(std::uint32_t tag, std::uint64_t id)
     {
-        gen = Pcg32(key_seed(seed, counter, tag), stream_id(static_cast<std::uint32_t>(id)));
+        gen = Pcg32(mix64(key_seed(seed, counter, tag) + (std::uint64_t(static_cast<std::uint32_t>(id)) + 1) *
+                                                              0x9E3779B97F4A7C15ULL),
+                    0);
     }
 };
 
@@ -113,6 +105,27 @@ struct Keyed
     void sample(const T* cur, R& rng, T* out) const
     {
         ks->open(tag, static_cast<std::size_t>(cur - base) / size);
+        inner.sample(cur, rng, out);
+    }
+    double log_ratio(const T* a, const T* b) const { return inner.log_ratio(a, b); }
+};
+
+// One draw per site, 16 sites per stream: re-keys on site / 16 and skips to
+// output site % 16 before the reference proposal runs (used with Flip, which
+// draws nothing, so the driver's accept draw is that output).
+template <class Q, class T>
+struct KeyedGroup
+{
+    Q inner;
+    KeyState* ks;
+    const T* base;
+
+    template <class R>
+    void sample(const T* cur, R& rng, T* out) const
+    {
+        const std::size_t i = static_cast<std::size_t>(cur - base);
+        ks->open(tag_site(0), i / 16);
+        for (std::size_t q = 0; q < i % 16; ++q) (void)ks->gen.uni();
         inner.sample(cur, rng, out);
     }
     double log_ratio(const T* a, const T* b) const { return inner.log_ratio(a, b); }
@@ -391,8 +404,8 @@ extern "C" int ref_ising_metropolis(std::uint64_t n, const std::uint32_t* ei, co
         KeyState ks;
         ks.seed = seed;
         ks.counter = sweep0;
-        Keyed<Flip, IsingSpin> prop{Flip{}, &ks, model.data(), 1, tag_site(0)};
-        Metropolis<Ising, Keyed<Flip, IsingSpin>, KeyedRng> mc(model, prop, KeyedRng{&ks}, beta);
+        KeyedGroup<Flip, IsingSpin> prop{Flip{}, &ks, model.data()};
+        Metropolis<Ising, KeyedGroup<Flip, IsingSpin>, KeyedRng> mc(model, prop, KeyedRng{&ks}, beta);
         std::uint64_t k = 0;
         mc.sample(n_sweeps, [&](const Ising& mdl) {
             if (E_out) E_out[k] = half_energy_sum(mdl);

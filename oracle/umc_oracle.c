@@ -55,7 +55,8 @@ uint64_t orc_key_seed(uint64_t seed, uint64_t counter, uint32_t tag)
     return orc_mix64(orc_mix64(seed ^ ((uint64_t)tag << 32)) + counter * 0x9E3779B97F4A7C15ULL);
 }
 
-/* lowbias32 integer hash (C. Wellons, 2018); every step is invertible. */
+/* lowbias32 integer hash (C. Wellons, 2018); every step is invertible.  The
+ * GPU's union-find linking priority of a site. */
 uint32_t orc_stream_id(uint32_t x)
 {
     x ^= x >> 16;
@@ -66,9 +67,14 @@ uint32_t orc_stream_id(uint32_t x)
     return x;
 }
 
+uint64_t orc_id_seed(uint64_t kseed, uint32_t id)
+{
+    return orc_mix64(kseed + ((uint64_t)id + 1ULL) * 0x9E3779B97F4A7C15ULL);
+}
+
 void orc_key_open(orc_pcg32* g, uint64_t seed, uint64_t counter, uint32_t tag, uint32_t id)
 {
-    orc_pcg32_seed(g, orc_key_seed(seed, counter, tag), orc_stream_id(id));
+    orc_pcg32_seed(g, orc_id_seed(orc_key_seed(seed, counter, tag), id), 0);
 }
 
 void orc_key_draws(uint64_t seed, uint64_t counter, uint32_t tag, uint32_t id, uint32_t n,
@@ -312,8 +318,10 @@ void orc_ising_metropolis(uint64_t n, const uint32_t* offset, const uint32_t* bo
     for (uint64_t k = 0; k < n_sweeps; ++k) {
         const uint64_t counter = sweep0 + k;
         for (uint64_t i = 0; i < n; ++i) {
+            /* one draw per site: output i % 16 of the stream of id i / 16 */
             orc_pcg32 g;
-            orc_key_open(&g, seed, counter, ORC_TAG_SITE(0), (uint32_t)i);
+            orc_key_open(&g, seed, counter, ORC_TAG_SITE(0), (uint32_t)(i / ORC_GROUP_SITES));
+            for (uint64_t q = 0; q < i % ORC_GROUP_SITES; ++q) orc_pcg32_next(&g);
             const int8_t old = s[i];
             const int8_t p = (int8_t)(-old);
             int32_t d = 0;
@@ -409,10 +417,12 @@ void orc_sphere_sample(uint32_t N, orc_pcg32* g, double* out)
     }
 }
 
-/* LocalRotation<N, double>::sample, dof/vector.hpp:70-122. */
-static void local_rotation(uint32_t N, double delta, orc_pcg32* g, const double* cur, double* out)
+/* LocalRotation<N, double>::sample, dof/vector.hpp:70-122.  Returns |v - (v.u) u|
+ * of the accepted frame: rounding of u and v (FP32 on the GPU) is amplified by
+ * its inverse in the normalised second axis. */
+static double local_rotation(uint32_t N, double delta, orc_pcg32* g, const double* cur, double* out)
 {
-    double u[8] = {0}, v[8] = {0};
+    double u[8] = {0}, v[8] = {0}, frame = 0.0;
     orc_sphere_sample(N, g, u);
     const double eps = 64.0 * 2.220446049250313080847263336181640625e-16;
     for (;;) {
@@ -427,6 +437,7 @@ static void local_rotation(uint32_t N, double delta, orc_pcg32* g, const double*
         if (r2 > eps) {
             const double inv = 1.0 / sqrt(r2);
             for (uint32_t k = 0; k < N; ++k) v[k] *= inv;
+            frame = sqrt(r2);
             break;
         }
     }
@@ -440,6 +451,7 @@ static void local_rotation(uint32_t N, double delta, orc_pcg32* g, const double*
     }
     for (uint32_t k = 0; k < N; ++k)
         out[k] = cur[k] + (c - 1.0) * (cu * u[k] + cv * v[k]) + sn * (cu * v[k] - cv * u[k]);
+    return frame;
 }
 
 /* VectorSpin<N>::energy_at, example/vector_spin.hpp:39-47. */
@@ -473,8 +485,9 @@ void orc_vector_metropolis(uint32_t N, uint64_t n, const uint32_t* offset, const
             orc_pcg32 g;
             orc_key_open(&g, seed, counter, ORC_TAG_SITE(0), (uint32_t)i);
             double* cur = s + i * N;
+            double frame = 1.0;
             if (proposal == ORC_PROP_SPHERE) orc_sphere_sample(N, &g, cand);
-            else local_rotation(N, delta, &g, cur, cand);
+            else frame = local_rotation(N, delta, &g, cur, cand);
             double d = 0.0;
             for (uint32_t a = offset[i]; a < offset[i + 1]; ++a) {
                 const double* sj = s + (uint64_t)bonds[a] * N;
@@ -489,6 +502,9 @@ void orc_vector_metropolis(uint32_t N, uint64_t n, const uint32_t* offset, const
                 margin = lu - log_p;
                 accept = lu < log_p;
             }
+            /* an ill-conditioned rotation frame makes the candidate itself
+             * precision-sensitive: report it like a near-threshold decision */
+            if (frame < ORC_FRAME_TOL) margin = 0.0;
             if (margin_out && k + 1 == n_sweeps) margin_out[i] = margin;
             if (accept) memcpy(cur, cand, N * sizeof(double));
         }

@@ -15,10 +15,10 @@
  * Conventions shared with the GPU path
  * ------------------------------------
  *  - Every random draw comes from a reference PCG32 (rng.hpp:8-44) constructed
- *    per key:  Pcg32(key_seed(seed, counter, tag), stream_id(id)),
+ *    per key:  Pcg32(id_seed(key_seed(seed, counter, tag), id), 0),
  *      key_seed(s,c,t) = mix64(mix64(s ^ (t << 32)) + c * 0x9E3779B97F4A7C15)
+ *      id_seed(k,id)   = mix64(k + (id + 1) * 0x9E3779B97F4A7C15)
  *      mix64           = splitmix64 finaliser (Steele, Lea, Flood 2014)
- *      stream_id(id)   = lowbias32(id) (a bijection on 32 bits, Wellons 2018)
  *    and draws are consumed sequentially inside the key, exactly as the
  *    reference driver would consume them from one Pcg32.
  *  - counter = sweep index for Metropolis, flip index for Wolff.
@@ -55,7 +55,8 @@ uint32_t orc_pcg32_next(orc_pcg32* g);
 double   orc_pcg32_uni(orc_pcg32* g);
 uint64_t orc_mix64(uint64_t z);
 uint64_t orc_key_seed(uint64_t seed, uint64_t counter, uint32_t tag);
-uint32_t orc_stream_id(uint32_t id);
+uint64_t orc_id_seed(uint64_t kseed, uint32_t id);
+uint32_t orc_stream_id(uint32_t id); /* lowbias32: union-find linking priority */
 void     orc_key_open(orc_pcg32* g, uint64_t seed, uint64_t counter, uint32_t tag, uint32_t id);
 /* n raw 32-bit outputs of the keyed stream */
 void     orc_key_draws(uint64_t seed, uint64_t counter, uint32_t tag, uint32_t id,
@@ -94,7 +95,10 @@ int orc_check_cell_colouring(uint64_t n_sites, uint32_t arity, const uint32_t* c
 
 /* ---- Ising (example/ising.hpp) under Metropolis / Wolff (driver.hpp) ----------
  * spins: int8 in {-1,+1}, updated in place.  E_out / M_out: one entry per sweep
- * or flip (may be NULL); E = 0.5 * sum_i energy_at(i). */
+ * or flip (may be NULL); E = 0.5 * sum_i energy_at(i).  Metropolis draws one
+ * uniform per site (Flip draws none): site i reads output i % ORC_GROUP_SITES of
+ * the keyed stream of id i / ORC_GROUP_SITES. */
+#define ORC_GROUP_SITES 16
 void orc_ising_metropolis(uint64_t n, const uint32_t* offset, const uint32_t* bonds, int32_t J,
                           double beta, uint64_t seed, uint64_t sweep0, uint64_t n_sweeps,
                           int8_t* spins, double* E_out, double* M_out);
@@ -107,9 +111,12 @@ void orc_ising_wolff(uint64_t n, const uint32_t* offset, const uint32_t* bonds,
  * spins: n*N doubles.  proposal: 0 = UniformSphereN<N>, 1 = LocalRotation<N>{delta}.
  * obs_out (may be NULL): per sweep/flip, [E, M_0 .. M_{N-1}]  (stride N+1).
  * margin_out (may be NULL): per site of the LAST sweep, log(u) - log_p of the
- * accept test (+inf when log_p >= 0, i.e. accepted without a draw). */
+ * accept test (+inf when log_p >= 0, i.e. accepted without a draw), and 0 when
+ * the LocalRotation frame was ill-conditioned (|v - (v.u) u| < ORC_FRAME_TOL:
+ * FP32 rounding of u, v grows by 1/|v - (v.u) u| in the candidate). */
 #define ORC_PROP_SPHERE 0
 #define ORC_PROP_ROTATION 1
+#define ORC_FRAME_TOL 0.1
 void orc_vector_metropolis(uint32_t N, uint64_t n, const uint32_t* offset, const uint32_t* bonds,
                            double J, double beta, int proposal, double delta, uint64_t seed,
                            uint64_t sweep0, uint64_t n_sweeps, double* spins, double* obs_out,

@@ -37,10 +37,10 @@ def test_keyed_streams_match_reference(oracle, golden):
 
 
 def test_keyed_stream_is_reference_pcg32(oracle):
-    # a keyed stream is exactly Pcg32(key_seed, stream_id(id)) of rng.hpp
+    # a keyed stream is exactly Pcg32(id_seed(key_seed, id), 0) of rng.hpp
     for s, c, t, i in [(1, 0, TAG_SITE(0), 5), (77, 9, 2, 0), (3, 2**40, 1, 2**32 - 1)]:
-        np.testing.assert_array_equal(oracle.key_draws(s, c, t, i, 8),
-                                      oracle.pcg32_draws(oracle.key_seed(s, c, t), oracle.stream_id(i), 8))
+        ks = oracle.key_seed(s, c, t)
+        np.testing.assert_array_equal(oracle.key_draws(s, c, t, i, 8), oracle.pcg32_draws(oracle.id_seed(ks, i), 0, 8))
 
 
 def test_stream_id_is_a_bijection_on_a_sample(oracle):

@@ -68,3 +68,18 @@ def test_constant_series_and_errors(umc):
         umc.binning_error(np.ones(10), 6)
     with pytest.raises(ValueError):
         umc.binning_error(np.ones(10), 0)
+
+
+def test_tau_multi_pools_chains(umc):
+    rho = 0.8
+    x = np.stack([_ar1(rho, 20_000, 100 + s) + s for s in range(16)])  # different means per chain
+    t, e, w = umc.tau_int_multi(x)
+    exact = (1 + rho) / (2 * (1 - rho))
+    assert abs(t - exact) < 4 * e + 0.02 * exact, (t, e)
+    t1, _, _ = umc.tau_int(x[3])
+    assert abs(t1 - exact) < 0.2 * exact
+    # frozen chains contribute nothing
+    xf = np.concatenate([x, np.full((16, 20_000), 3.0)])
+    tf, _, _ = umc.tau_int_multi(xf)
+    assert tf == pytest.approx(t, rel=1e-9)
+    assert umc.tau_int_multi(np.ones((3, 10)))[0] == 0.5

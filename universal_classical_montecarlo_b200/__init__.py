@@ -231,6 +231,21 @@ def tau_int(series, c: float = 6.0):
     return t.value, e.value, w.value
 
 
+_decl("umc_tau_int_multi", _int, _vp, _u64, _u64, _f64, C.POINTER(_f64), C.POINTER(_f64), C.POINTER(_u64))
+
+
+def tau_int_multi(series, c: float = 6.0):
+    """Pooled tau_int of independent chains: ``series`` is (chains, length).
+    Returns ``(tau, tau_err, window)``; window == length // 2 means the estimate
+    did not converge inside the series."""
+    x = np.ascontiguousarray(series, dtype=np.float64)
+    if x.ndim != 2:
+        raise ValueError("series must be (chains, length)")
+    t, e, w = _f64(), _f64(), _u64()
+    check(lib.umc_tau_int_multi(_ptr(x), x.shape[0], x.shape[1], c, C.byref(t), C.byref(e), C.byref(w)))
+    return t.value, e.value, w.value
+
+
 def binning_error(series, bin: int):
     """Mean and its standard error from bins of ``bin`` consecutive values."""
     x = np.ascontiguousarray(series, dtype=np.float64)

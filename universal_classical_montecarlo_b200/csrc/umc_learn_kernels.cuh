@@ -456,23 +456,70 @@ __device__ __forceinline__ void chain_record(const U1BatchArgs& a, const float* 
     }
 }
 
+// Mixture parameters as the sampler uses them: weights, log weights,
+// concentrations and mean directions (cos mu, sin mu) = (u, v) / |(u, v)|
+// ((1, 0) when u = v = 0, matching atan2(0, 0) = 0).
+struct MixtureDir
+{
+    float w[kComp], lw[kComp], kappa[kComp], cu[kComp], su[kComp];
+};
+
+__device__ __forceinline__ void mixture_dir(const float o[16], MixtureDir& m)
+{
+    float mx = o[0];
+#pragma unroll
+    for (int k = 1; k < kComp; ++k) mx = fmaxf(mx, o[4 * k]);
+    float z = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kComp; ++k) {
+        m.w[k] = expf(o[4 * k] - mx);
+        z += m.w[k];
+    }
+    const float lz = logf(z), iz = 1.0f / z;
+#pragma unroll
+    for (int k = 0; k < kComp; ++k) {
+        m.w[k] *= iz;
+        m.lw[k] = (o[4 * k] - mx) - lz;
+        m.kappa[k] = fminf(fmaxf(softplus_f(o[4 * k + 3]), kKappaMin), kKappaMax);
+        const float u = o[4 * k + 1], v = o[4 * k + 2], rr = u * u + v * v;
+        const float n = rr > 0.0f ? rsqrtf(rr) : 0.0f;
+        m.cu[k] = rr > 0.0f ? u * n : 1.0f;
+        m.su[k] = v * n;
+    }
+}
+
 // The learned Metropolis-Hastings step of link k (colour-major) given the
 // network outputs o and the staple sum: component by inverse CDF, Best-Fisher
-// angle, dE as the plain model computes it, and the log proposal ratio
-// log q(old) - log q(new) summed in FP64.  Returns true if accepted.
+// angle around mu = atan2(v, u), dE as the plain model computes it, and
+//   log_p = -beta dE + log q(old) - log q(new)
+// with log q(t) = logsumexp_k(log w_k - log I0(kappa_k) + kappa_k cos(t - mu_k))
+// (the common log 2 pi cancels).  The per-component terms are FP32 -- their
+// error, about kappa 1e-7, is the size of the FP32 angle quantisation of the
+// proposal itself -- and log_p is formed in FP64.  Returns true if accepted.
 __device__ __forceinline__ bool learned_update(const U1BatchArgs& a, float* th, uint32_t k, const float o[16],
                                                float Sr, float Si, uint64_t kbase)
 {
-    Mixture m;
-    mixture_of(o, m);
+    MixtureDir m;
+    mixture_dir(o, m);
     KeyedPcg r = KeyedPcg::open(kbase, k);
-    const int comp = pick_component(m, r.next());
-    float kc = m.kappa[0], mc = m.mu[0];
+    const float u0 = u_f32(r.next());
+    int comp = kComp - 1;
+    {
+        // smallest kk with u0 < w_0 + ... + w_kk
+        float c = 0.0f;
+#pragma unroll
+        for (int kk = 0; kk < kComp - 1; ++kk) {
+            c += m.w[kk];
+            if (comp == kComp - 1 && u0 < c) comp = kk;
+        }
+    }
+    float kc = m.kappa[0], uc = o[1], vc = o[2];
 #pragma unroll
     for (int kk = 1; kk < kComp; ++kk)
         if (comp == kk) {
             kc = m.kappa[kk];
-            mc = m.mu[kk];
+            uc = o[4 * kk + 1];
+            vc = o[4 * kk + 2];
         }
     float ang = 0.0f;
     bool moved = false;
@@ -482,28 +529,27 @@ __device__ __forceinline__ bool learned_update(const U1BatchArgs& a, float* th, 
     }
     if (!moved) return false;
     const float tcur = th[k];
-    const float p = remainderf(mc + ang, 6.283185307179586f);
+    const float p = remainderf(atan2f(vc, uc) + ang, 6.283185307179586f);
     float so, co, sp, cp;
     sincosf(tcur, &so, &co);
     sincosf(p, &sp, &cp);
     const float dE = a.model_beta * ((co - cp) * Sr - (so - sp) * Si);
-    double lo[kComp], ln[kComp], mo = -1e300, mn = -1e300;
+    float lo[kComp], ln[kComp], mo = -3.0e38f, mn = -3.0e38f;
 #pragma unroll
     for (int kk = 0; kk < kComp; ++kk) {
-        const double base = m.lwd[kk] - double(logf(cyl_bessel_i0f(m.kappa[kk])));
-        const double kap = double(m.kappa[kk]), mu = double(m.mu[kk]);
-        lo[kk] = base + kap * cos(double(tcur) - mu);
-        ln[kk] = base + kap * cos(double(p) - mu);
-        mo = fmax(mo, lo[kk]);
-        mn = fmax(mn, ln[kk]);
+        const float base = m.lw[kk] - logf(cyl_bessel_i0f(m.kappa[kk]));
+        lo[kk] = base + m.kappa[kk] * (co * m.cu[kk] + so * m.su[kk]);
+        ln[kk] = base + m.kappa[kk] * (cp * m.cu[kk] + sp * m.su[kk]);
+        mo = fmaxf(mo, lo[kk]);
+        mn = fmaxf(mn, ln[kk]);
     }
-    double so_ = 0.0, sn_ = 0.0;
+    float so_ = 0.0f, sn_ = 0.0f;
 #pragma unroll
     for (int kk = 0; kk < kComp; ++kk) {
-        so_ += exp(lo[kk] - mo);
-        sn_ += exp(ln[kk] - mn);
+        so_ += expf(lo[kk] - mo);
+        sn_ += expf(ln[kk] - mn);
     }
-    const double lr = (mo - mn) + log(so_ / sn_);
+    const double lr = (double(mo) - double(mn)) + log(double(so_) / double(sn_));
     const double log_p = -double(a.driver_beta) * double(dE) + lr;
     if (log_p >= 0.0 || log(u_f64(r.next())) < log_p) {
         th[k] = p;

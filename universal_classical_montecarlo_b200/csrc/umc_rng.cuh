@@ -6,17 +6,24 @@
 // driver.hpp:151).  A sequential stream cannot be replayed by thousands of
 // threads, so every update here opens its OWN reference-semantics Pcg32:
 //
-//     Pcg32(key_seed(seed, counter, tag), stream_id(id))
+//     Pcg32(id_seed(key_seed(seed, counter, tag), id), 0)
 //
 //     key_seed(s, c, t) = mix64(mix64(s ^ (t << 32)) + c * 0x9E3779B97F4A7C15)
-//     mix64            = splitmix64 finaliser (Steele, Lea & Flood, 2014)
-//     stream_id(id)    = lowbias32(id), a bijection on 32 bits (Wellons, 2018)
+//     id_seed(k, id)    = mix64(k + (id + 1) * 0x9E3779B97F4A7C15)
+//     mix64             = splitmix64 finaliser (Steele, Lea & Flood, 2014)
 //
-// and consumes its draws in the same order the reference driver would.  The
-// constructor (rng.hpp:14-20) leaves state = (inc + s) * A + inc with
-// inc = 2 * stream + 1, so the first state of a key is affine in stream_id:
-//     state0 = C0 + stream_id * C1,  C0 = (s + 1) * A + 1,  C1 = 2 * A + 2,
-// which costs two integer multiply-adds per site once C0 is known per sweep.
+// and consumes its draws in the same order the reference driver would.  With
+// stream 0 the constructor (rng.hpp:14-20) leaves state = (s + 1) * A + 1 and
+// increment 1.
+//
+// Why the id goes into the seed: an earlier keying gave every id of a key the
+// SAME seed and a per-id increment (stream = a 32-bit hash of id).  Then the
+// first states of two ids differ by an offset that depends on the two ids only,
+// identical at every sweep, and the small correlation between the XSH-RR
+// outputs of states a fixed offset apart never averages out: plain U(1)
+// Metropolis on a 4 x 4 torus at beta = 1 settled 2.5e-3 (7 sigma) below the
+// exact plaquette.  Hashing (key, id) into the seed gives every update an
+// independent state at every sweep.
 #pragma once
 
 #include <stdint.h>
@@ -31,7 +38,6 @@ namespace umc {
 
 constexpr uint64_t kPcgMult = 6364136223846793005ULL;  // rng.hpp:34
 constexpr uint64_t kGolden = 0x9E3779B97F4A7C15ULL;
-constexpr uint64_t kStreamStep = 2ULL * kPcgMult + 2ULL;  // C1
 
 // Key tags: which kind of update a key belongs to.
 constexpr uint32_t kTagBond = 1;   // Wolff bond activation, id = edge index
@@ -56,6 +62,8 @@ UMC_HD uint64_t key_seed(uint64_t seed, uint64_t counter, uint32_t tag)
     return mix64(mix64(seed ^ (uint64_t(tag) << 32)) + counter * kGolden);
 }
 
+// lowbias32 (Wellons, 2018), a bijection on 32 bits; the union-find linking
+// priority of a site (umc_device.cuh).
 UMC_HD uint32_t stream_id(uint32_t x)
 {
     x ^= x >> 16;
@@ -66,8 +74,14 @@ UMC_HD uint32_t stream_id(uint32_t x)
     return x;
 }
 
-// C0 for a given key seed: state0(id) = c0 + stream_id(id) * kStreamStep.
-UMC_HD uint64_t key_base(uint64_t kseed) { return (kseed + 1ULL) * kPcgMult + 1ULL; }
+// Per-key base of the ids' seeds (the key seed itself).
+UMC_HD uint64_t key_base(uint64_t kseed) { return kseed; }
+
+// Seed of id's stream under a key.
+UMC_HD uint64_t id_seed(uint64_t kbase, uint32_t id) { return mix64(kbase + (uint64_t(id) + 1ULL) * kGolden); }
+
+// First state of Pcg32(seed, 0): (seed + 1) * A + 1.
+UMC_HD uint64_t first_state(uint64_t seed) { return (seed + 1ULL) * kPcgMult + 1ULL; }
 
 // XSH-RR output of a state (rng.hpp:36-39).
 UMC_HD uint32_t pcg_output(uint64_t old)
@@ -95,10 +109,9 @@ struct KeyedPcg
 
     UMC_HD static KeyedPcg open(uint64_t kbase, uint32_t id)
     {
-        const uint32_t h = stream_id(id);
         KeyedPcg g;
-        g.state = kbase + uint64_t(h) * kStreamStep;
-        g.inc = (uint64_t(h) << 1) | 1ULL;
+        g.state = first_state(id_seed(kbase, id));
+        g.inc = 1ULL;
         return g;
     }
     UMC_HD static KeyedPcg open_key(uint64_t seed, uint64_t counter, uint32_t tag, uint32_t id)
@@ -115,9 +128,51 @@ struct KeyedPcg
 };
 
 // First draw of a key without materialising the stream (one draw per site).
-UMC_HD uint32_t first_draw(uint64_t kbase, uint32_t id)
+UMC_HD uint32_t first_draw(uint64_t kbase, uint32_t id) { return pcg_output(first_state(id_seed(kbase, id))); }
+
+// ---- one draw per site, 16 sites per stream ------------------------------------
+// Ising Metropolis draws exactly one uniform per site (Flip proposes without a
+// draw).  There site k reads output (k % 16) of the stream of id k / 16: one
+// hash per 16 sites, and consecutive outputs of one Pcg32 within a group.
+constexpr uint32_t kGroupSites = 16;
+
+// Jump table of Pcg32 stream 0 (increment 1): state_j = A^j state_0 + C_j with
+// C_j = A^0 + ... + A^(j-1), all mod 2^64.
+struct PcgJump
 {
-    return pcg_output(kbase + uint64_t(stream_id(id)) * kStreamStep);
+    uint64_t mul[kGroupSites], add[kGroupSites];
+    constexpr PcgJump() : mul(), add()
+    {
+        uint64_t m = 1, c = 0;
+        for (uint32_t j = 0; j < kGroupSites; ++j) {
+            mul[j] = m;
+            add[j] = c;
+            c = c * kPcgMult + 1ULL;
+            m = m * kPcgMult;
+        }
+    }
+};
+constexpr PcgJump kPcgJump{};
+
+// Advance a stream-0 state by j < 16 outputs: four conditional jumps by 1, 2,
+// 4 and 8 steps with compile-time constants (no table in memory).
+UMC_HD uint64_t pcg_advance(uint64_t st, uint32_t j)
+{
+    constexpr uint64_t m1 = kPcgJump.mul[1], a1 = kPcgJump.add[1];
+    constexpr uint64_t m2 = kPcgJump.mul[2], a2 = kPcgJump.add[2];
+    constexpr uint64_t m4 = kPcgJump.mul[4], a4 = kPcgJump.add[4];
+    constexpr uint64_t m8 = kPcgJump.mul[8], a8 = kPcgJump.add[8];
+    if (j & 1u) st = st * m1 + a1;
+    if (j & 2u) st = st * m2 + a2;
+    if (j & 4u) st = st * m4 + a4;
+    if (j & 8u) st = st * m8 + a8;
+    return st;
+}
+
+// The draw of site k under a key (one draw per site).
+UMC_HD uint32_t group_draw(uint64_t kbase, uint32_t k)
+{
+    return pcg_output(pcg_advance(first_state(id_seed(kbase, k / kGroupSites)), k % kGroupSites));
 }
 
 // ---- conversions of a 32-bit draw k (the reference uses u = k * 2^-32) ----

@@ -128,6 +128,9 @@ static __global__ void __launch_bounds__(kBlock) ising_packed_pass(IsingPackedAr
         const uint32_t uw[4] = {u4.x, u4.y, u4.z, u4.w};
         const uint32_t dw[4] = {d4.x, d4.y, d4.z, d4.w};
         uint32_t out[4];
+        // the 16 sites of this vector are one group: consecutive outputs of the
+        // stream of id (class offset + base) / 16
+        KeyedPcg rng = KeyedPcg::open(a.kbase, (idbase + base) / kGroupSites);
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
             // second horizontal neighbour: byte k-1 (p == 0) or k+1 (p == 1)
@@ -142,7 +145,7 @@ static __global__ void __launch_bounds__(kBlock) ising_packed_pass(IsingPackedAr
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
                 const uint32_t tb = (t >> (8 * b)) & 0xFFu;
-                const uint32_t r = first_draw(a.kbase, idbase + base + 4 * w + b);
+                const uint32_t r = rng.next();
                 fm |= (r <= tm1[tb] ? 0xFEu : 0u) << (8 * b);
             }
             const uint32_t ns = sw[w] ^ fm;
@@ -191,7 +194,7 @@ __global__ void __launch_bounds__(kBlock) ising_pass(IsingArgs a, Topo t)
             he += early ? sj : 0;
         });
         const int32_t s = a.spins[k];
-        const uint32_t r = first_draw(a.kbase, k);
+        const uint32_t r = group_draw(a.kbase, k);
         const bool flip = r <= tm1s[s * h + int32_t(a.D)];
         const int32_t ns = flip ? -s : s;
         if (flip) a.spins[k] = int8_t(ns);

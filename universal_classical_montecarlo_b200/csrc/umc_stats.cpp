@@ -73,6 +73,44 @@ int umc_tau_int(const double* x, uint64_t n, double c, double* tau, double* tau_
     });
 }
 
+int umc_tau_int_multi(const double* x, uint64_t series, uint64_t length, double c, double* tau, double* tau_err,
+                      uint64_t* window)
+{
+    return umc::sguard([&] {
+        if (!x || series == 0 || length < 4) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "need series of at least 4 values");
+        if (!(c > 0.0)) c = 6.0;
+        // each series centred on its own mean; autocovariances pooled over series
+        std::vector<double> d(series * length);
+        for (uint64_t s = 0; s < series; ++s) {
+            double m = 0.0;
+            for (uint64_t i = 0; i < length; ++i) m += x[s * length + i];
+            m /= double(length);
+            for (uint64_t i = 0; i < length; ++i) d[s * length + i] = x[s * length + i] - m;
+        }
+        auto cov = [&](uint64_t t) {
+            double a = 0.0;
+            for (uint64_t s = 0; s < series; ++s) {
+                const double* r = d.data() + s * length;
+                for (uint64_t i = 0; i + t < length; ++i) a += r[i] * r[i + t];
+            }
+            return a / double(series * (length - t));
+        };
+        const double c0 = cov(0);
+        double t = 0.5;
+        uint64_t W = 0;
+        if (c0 > 0.0) {
+            for (uint64_t w = 1; w <= length / 2; ++w) {
+                t += cov(w) / c0;
+                W = w;
+                if (double(w) >= c * t) break;
+            }
+        }
+        if (tau) *tau = t;
+        if (tau_err) *tau_err = t * std::sqrt(2.0 * (2.0 * double(W) + 1.0) / double(series * length));
+        if (window) *window = W;
+    });
+}
+
 int umc_binning_error(const double* x, uint64_t n, uint64_t bin, double* mean, double* err)
 {
     return umc::sguard([&] {
