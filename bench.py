@@ -225,9 +225,12 @@ class O3Hybrid:
         # (read own + neighbour class, write own; 12 B per FP32 3-vector);
         # Wolff: bond pass reads each site and its + neighbours once (12 B +
         # 4 B label write + 1 B crossing mask), flip reads label + spin (16 B)
+        # fused step (one launch): sweep 36 B + bond/label pass 17 B + merge 1 B
+        # + flip label read 4 B per site, and 24 B per cluster site
         n = self.n
-        return {"metropolis": 36.0 * n / 2, "wolff_union": 17.0 * n, "wolff_flip": 16.0 * n,
-                "wolff_merge": 1.0 * n}.get(kind, 36.0 * n / 2)
+        c = getattr(self, "mean_cluster", 0.0)
+        return {"metropolis": 36.0 * n / 2, "wolff_union": 17.0 * n, "wolff_flip": 4.0 * n + 24.0 * c,
+                "wolff_merge": 1.0 * n, "fused": 58.0 * n + 24.0 * c}.get(kind, 36.0 * n / 2)
 
     def e2e(self, torch, K):
         host = torch.empty((self.n, 3), dtype=torch.float32, pin_memory=True)
@@ -488,7 +491,7 @@ def torus_plaquette(beta, n_plaq):
 
 
 def learned_study(umc, torch, betas=LEARN_BETAS, L=64, chains=444, n_configs=20000, train_steps=1500,
-                  batch=16384, lr=3e-3, therm=3000, meas=4000, seed=1):
+                  batch=16384, lr=3e-3, therm=20000, meas=4000, seed=1):
     """Effective independent samples per second of the plaquette P and the
     topological charge Q on 2D U(1) L x L, for plain U1Shift(0.5) Metropolis on
     one chain (the faster of the single-chain engine and the batch kernel with
@@ -702,6 +705,8 @@ def main():
         ch.fetch(8192)
         per_kind = ch.kernel_stats(reset=True)
     ch.set_timing(False)
+    if wl.name == "o3" and len(sizes):
+        wl.mean_cluster = float(sizes.mean())
     kind, (nl, ms) = max(((k, v) for k, v in per_kind.items() if v[0] > 0 and k != "other"),
                          key=lambda kv: kv[1][1])
     avg_s = ms / nl / 1e3
@@ -729,6 +734,25 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         cpu = wl.cpu(args.cpu_seconds)
 
+    # the learned-proposal study (2D U(1) 64x64, beta 2..8), summarised
+    learned = None
+    if rank == 0 and wl.name == "o3" and not args.no_learned:
+        study = learned_study(umc, torch, meas=2000)
+        learned = {"workload": "2D U(1) 64x64, 444 chains, U1Shift 0.5 vs learned 4-component von Mises mixture "
+                               "(MLP 3-64-64-16, BF16 tcgen05), 20000 training configurations per beta",
+                   "unit": "effective samples/s",
+                   "per_beta": {b: {"learned_batched_over_plain_single": {o: row[o]["learned_batched_over_plain_single"]
+                                                                          for o in ("plaquette", "Q")},
+                                    "learned_over_plain_at_equal_batch": {o: row[o]["learned_over_plain_at_equal_batch"]
+                                                                          for o in ("plaquette", "Q")},
+                                    "effective_samples_per_s": {o: row[o]["effective_samples_per_s"]
+                                                                for o in ("plaquette", "Q")},
+                                    "tau_int": {o: row[o]["tau_int"] for o in ("plaquette", "Q")},
+                                    "tau_converged": {o: row[o]["tau_converged"] for o in ("plaquette", "Q")},
+                                    "z_vs_exact_plaquette": row["z_vs_exact"],
+                                    "acceptance": row["acceptance"]}
+                                for b, row in study.items()}}
+
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -753,6 +777,8 @@ def main():
         "kernel_ms": {k: round(v[1], 4) for k, v in per_kind.items() if v[0]},
         "clocks": clocks,
     }
+    if learned is not None:
+        line["learned_u1"] = learned
     print(json.dumps(line), flush=True)
 
 
