@@ -1,0 +1,104 @@
+// umc/detail.hpp -- status codes -> the reference's exception types, handle
+// ownership, and the host/device field synchronisation shared by the models.
+#pragma once
+
+#include <umc_b200.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace umc::gpu::detail {
+
+// Builder errors keep the reference's exception classes (lattice/*.hpp);
+// everything else (CUDA, device timeouts, misuse) is a runtime_error.
+inline void check(int status)
+{
+    if (status == UMC_OK) return;
+    const std::string msg = umc_last_error();
+    switch (status) {
+    case UMC_ERR_INVALID_ARGUMENT: throw std::invalid_argument(msg);
+    case UMC_ERR_OUT_OF_RANGE: throw std::out_of_range(msg);
+    case UMC_ERR_OVERFLOW: throw std::overflow_error(msg);
+    default: throw std::runtime_error("umc status " + std::to_string(status) + ": " + msg);
+    }
+}
+
+struct GraphFree
+{
+    void operator()(umc_graph* g) const noexcept { umc_graph_destroy(g); }
+};
+struct CellsFree
+{
+    void operator()(umc_cells* c) const noexcept { umc_cells_destroy(c); }
+};
+struct ChainFree
+{
+    void operator()(umc_chain* c) const noexcept { umc_chain_destroy(c); }
+};
+using ChainPtr = std::unique_ptr<umc_chain, ChainFree>;
+
+inline ChainPtr make_chain(const umc_chain_desc& d)
+{
+    umc_chain* c = nullptr;
+    check(umc_chain_create(&d, &c));
+    return ChainPtr(c);
+}
+
+// A model's field on the host as scalars HS in the reference's data() layout,
+// plus which device chain holds the newest copy.  Drivers call attach() before
+// they run and mark_device() after; data() and update() call ensure_host()
+// first.  DevT is the scalar type of the C ABI's set_field/get_field layout
+// (int8 Ising spins, FP32 otherwise).
+template <class HS, class DevT>
+class Field
+{
+public:
+    void attach(umc_chain* c) const
+    {
+        if (owner_ == c) return;
+        ensure_host();
+        std::vector<DevT> dev(host_.size());
+        for (std::size_t k = 0; k < host_.size(); ++k) dev[k] = static_cast<DevT>(host_[k]);
+        check(umc_chain_set_field(c, dev.data()));
+        owner_ = c;
+        host_valid_ = true;
+    }
+    void mark_device(umc_chain* c) const
+    {
+        owner_ = c;
+        host_valid_ = false;
+    }
+    // A driver going away keeps its results in the host copy.
+    void detach(umc_chain* c) const noexcept
+    {
+        if (owner_ != c) return;
+        try {
+            ensure_host();
+        } catch (...) {
+        }
+        owner_ = nullptr;
+        host_valid_ = true;
+    }
+
+protected:
+    void ensure_host() const
+    {
+        if (host_valid_ || !owner_) return;
+        std::vector<DevT> dev(host_.size());
+        check(umc_chain_get_field(owner_, dev.data()));
+        for (std::size_t k = 0; k < host_.size(); ++k) host_[k] = static_cast<HS>(dev[k]);
+        host_valid_ = true;
+    }
+    // After a host-side write the host copy is the newest.
+    void host_written() const { owner_ = nullptr; }
+
+    mutable std::vector<HS> host_;
+    mutable umc_chain* owner_ = nullptr;
+    mutable bool host_valid_ = true;
+};
+
+}  // namespace umc::gpu::detail

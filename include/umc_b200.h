@@ -8,9 +8,9 @@
  *
  *   tables      PairGraph / square_lattice     lattice/pair_graph.hpp, lattice/square.hpp
  *               CellComplex / hypercubic_plaquettes  lattice/cell_complex.hpp, lattice/hypercubic.hpp
- *   models      Ising, VectorSpin<N>, U1Gauge, SUGauge<N>  example/*.hpp
- *               PairModel / CellModel + terms   model/*.hpp, term/*.hpp
- *   proposals   Flip, FixedAxis, UniformSphereN, LocalRotation, U1Shift, SUShift  dof/*.hpp
+ *   models      Ising, VectorSpin<N>, U1Gauge, SUGauge<N>  example/ headers
+ *               PairModel / CellModel + terms   model/ and term/ headers
+ *   proposals   Flip, FixedAxis, UniformSphereN, LocalRotation, U1Shift, SUShift  dof/ headers
  *   drivers     Metropolis<M,Q,R>, Wolff<M,A,R>  driver.hpp
  *   RNG         Pcg32                           rng.hpp
  *
@@ -107,14 +107,14 @@ int umc_cells_colouring(const umc_cells* c, uint32_t* n_colours, uint32_t* colou
 
 /* ===================================================================== chains */
 
-/* Models (example/*.hpp, model/*.hpp). */
+/* Models (example/ and model/ headers). */
 #define UMC_MODEL_ISING 1    /* Ising, example/ising.hpp:14-76 (int8 spins, integer J)     */
 #define UMC_MODEL_VECTOR 2   /* VectorSpin<N>, example/vector_spin.hpp:14-83 (N = 1..4)     */
 #define UMC_MODEL_XY_ANGLE 3 /* PairModel<U1Dof, -J cos(ti-tj)>, model/pair.hpp:17-83     */
 #define UMC_MODEL_U1 4       /* U1Gauge / CellModel<U1Dof,U1PlaquetteTerm>, example/u1_gauge.hpp */
 #define UMC_MODEL_SU 5       /* SUGauge<N> / CellModel<SUDof,SUPlaquetteTerm>, example/sun_gauge.hpp */
 
-/* Metropolis proposals (dof/*.hpp). */
+/* Metropolis proposals (dof/ headers). */
 #define UMC_PROPOSAL_FLIP 1     /* Flip, dof/ising.hpp:27-38                 */
 #define UMC_PROPOSAL_SPHERE 2   /* UniformSphereN<N>, dof/vector.hpp:35-61     */
 #define UMC_PROPOSAL_ROTATION 3 /* LocalRotation<N>{delta}, dof/vector.hpp:70-122 */
