@@ -318,7 +318,31 @@ void spin_sweep(umc_chain* c, double beta, double* rec)
         const bool last = p + 1 == c->n_colours;
         const PassOut o{c->ctl.as<DevCtl>(), c->partials.as<double>(), fused ? rec : nullptr, nullptr,
                         int(p), int(c->n_colours), last ? 1 : 0};
-        if (c->packed_ising) {
+        uint32_t tm[5] = {0, 0, 0, 0, 0};
+        if (c->packed_ising)
+            for (int t = 0; t < 5; ++t) tm[t] = c->h_tm1[size_t(int(c->max_degree) + 2 * t - 4)];
+        const uint32_t vpr = uint32_t(c->dims[0] / 2 / 16);
+        const bool fast = c->packed_ising && tm[0] == 0xFFFFFFFFu && tm[1] == 0xFFFFFFFFu && tm[2] == 0xFFFFFFFFu &&
+                          tm[4] <= tm[3] && vpr < (1u << 15) && c->n / 2 / 16 < (uint64_t(1) << 25);
+        if (fast) {
+            IsingFastArgs a{};
+            a.spins = c->field.as<int8_t>();
+            a.H = uint32_t(c->dims[0] / 2);
+            a.Ly = uint32_t(c->dims[1]);
+            a.half = uint32_t(c->n / 2);
+            a.colour = p;
+            a.vpr = vpr;
+            a.vmagic = ((uint64_t(1) << 40) / vpr) + 1;
+            a.kbase = kbase;
+            a.T3 = tm[3];
+            a.T4 = tm[4];
+            a.J = c->J_int;
+            a.out = o;
+            const uint32_t g = grid_for(c, c->n / 2 / 16);
+            LaunchScope ls(c, UMC_KERNEL_METROPOLIS);
+            if (p == 1) ising_fast_pass<true><<<g, kBlock, 0, c->stream>>>(a);
+            else ising_fast_pass<false><<<g, kBlock, 0, c->stream>>>(a);
+        } else if (c->packed_ising) {
             IsingPackedArgs a{};
             a.spins = c->field.as<int8_t>();
             a.H = uint32_t(c->dims[0] / 2);
@@ -326,7 +350,7 @@ void spin_sweep(umc_chain* c, double beta, double* rec)
             a.half = uint32_t(c->n / 2);
             a.colour = p;
             a.kbase = kbase;
-            for (int t = 0; t < 5; ++t) a.tm1[t] = c->h_tm1[size_t(int(c->max_degree) + 2 * t - 4)];
+            for (int t = 0; t < 5; ++t) a.tm1[t] = tm[t];
             a.J = c->J_int;
             a.out = o;
             const uint32_t g = grid_for(c, c->n / 2 / 16);

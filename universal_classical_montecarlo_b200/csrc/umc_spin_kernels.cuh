@@ -165,6 +165,109 @@ static __global__ void __launch_bounds__(kBlock) ising_packed_pass(IsingPackedAr
     finish_pass<kObs>(v, a.out);
 }
 
+// --------------------------------------- Ising, packed 2D stencil, J > 0
+//
+// The same pass for the usual sign of J (ferromagnet): only a site with at
+// most one anti-aligned neighbour can be rejected (dE = 8J with none, 4J with
+// one), so the decision per site is
+//     flip  <=>  anti + [r <= T(dE=4J)] + [r <= T(dE=8J)] >= 2,
+// evaluated four sites at a time on bytes.  The arithmetic is arranged for the
+// FMA pipe where it can be (multiply-high shifts, wide multiply-adds for the
+// comparisons), the integer ALU being the limiting pipe of this kernel.
+struct IsingFastArgs
+{
+    int8_t* spins;
+    uint32_t H, Ly, half, colour, vpr;
+    uint64_t vmagic;  // row of vector v = (v * vmagic) >> 40 (exact for v < 2^25, vpr < 2^15)
+    uint64_t kbase;
+    uint32_t T3, T4;  // accept iff draw <= T for dE = 4J, 8J (T4 <= T3)
+    int32_t J;
+    PassOut out;
+};
+
+// XSH-RR output of state (hi:lo): rotr32(uint32(s >> 27) ^ uint32(s >> 45), s >> 59),
+// with the right shifts of hi as multiply-highs.
+__device__ __forceinline__ uint32_t pcg_output_split(uint32_t lo, uint32_t hi)
+{
+    const uint32_t xs = __funnelshift_r(lo, hi, 27) ^ __umulhi(hi, 1u << 19);
+    return __funnelshift_r(xs, xs, __umulhi(hi, 32u));
+}
+
+// hi32(a * b + c) with one wide multiply-add.
+__device__ __forceinline__ uint32_t mad_wide_hi(uint32_t a, uint32_t b, uint32_t c)
+{
+    uint64_t w;
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(w) : "r"(a), "r"(b), "l"(uint64_t(c)));
+    return uint32_t(w >> 32);
+}
+
+// ENERGY: the pass of class 1, which also sums s_k h_k (every bond once).
+template <bool ENERGY>
+__global__ void __launch_bounds__(kBlock) ising_fast_pass(IsingFastArgs a)
+{
+    int64_t e_acc = 0, m_acc = 0, n_acc = 0;
+    const uint32_t nvec = a.half >> 4;
+    const int8_t* other = a.spins + (1u - a.colour) * a.half;
+    int8_t* own = a.spins + a.colour * a.half;
+    const uint32_t gbase = (a.colour * a.half) >> 4;  // stream id of this class's first vector
+    constexpr uint32_t M2 = 0x02020202u;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nvec; v += gridDim.x * blockDim.x) {
+        const uint32_t y = uint32_t((uint64_t(v) * a.vmagic) >> 40);
+        const uint32_t i0 = (v - y * a.vpr) << 4;
+        const uint32_t base = v << 4;
+        const uint32_t p = (y + a.colour) & 1u;
+        const uint32_t ym = y == 0 ? a.Ly - 1 : y - 1, yp = y + 1 == a.Ly ? 0u : y + 1;
+        const uint4 s4 = *reinterpret_cast<const uint4*>(own + base);
+        const uint4 m4 = *reinterpret_cast<const uint4*>(other + base);
+        const uint4 u4 = *reinterpret_cast<const uint4*>(other + yp * a.H + i0);
+        const uint4 d4 = *reinterpret_cast<const uint4*>(other + ym * a.H + i0);
+        const uint32_t xe = p ? (i0 + 16 == a.H ? 0u : i0 + 16) : (i0 == 0 ? a.H - 1 : i0 - 1);
+        const uint32_t extra = uint32_t(uint8_t(other[y * a.H + xe]));
+        const uint32_t sw[4] = {s4.x, s4.y, s4.z, s4.w};
+        const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
+        const uint32_t uw[4] = {u4.x, u4.y, u4.z, u4.w};
+        const uint32_t dw[4] = {d4.x, d4.y, d4.z, d4.w};
+        uint64_t st = first_state(id_seed(a.kbase, gbase + v));
+        uint32_t out[4], acc_f = 0, acc_dn = 0, acc_e = 0;
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            const uint32_t h2 = p ? __byte_perm(mw[w], w == 3 ? extra : mw[w + 1], 0x4321)
+                                  : __byte_perm(w == 0 ? (extra << 24) : mw[w - 1], mw[w], 0x6543);
+            const uint32_t s = sw[w];
+            // twice the number of neighbours whose spin differs from the site's
+            const uint32_t A2 = ((mw[w] ^ s) & M2) + ((h2 ^ s) & M2) + ((uw[w] ^ s) & M2) + ((dw[w] ^ s) & M2);
+            // byte b: A2 + 2 ([r <= T3] + [r <= T4]) + 12, flip iff >= 16
+            uint32_t X = A2 + 0x0C0C0C0Cu;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const uint32_t r = pcg_output_split(uint32_t(st), uint32_t(st >> 32));
+                st = st * kPcgMult + 1ULL;
+                // hi32(r (2^32 - 1) + T) = r - [r > T], so 2 [r <= T] = 2 + 2 hi32 - 2 r
+                const uint32_t h3 = mad_wide_hi(r, 0xFFFFFFFFu, a.T3);
+                const uint32_t h4 = mad_wide_hi(r, 0xFFFFFFFFu, a.T4);
+                X += (4u + 2u * (h3 + h4) - 4u * r) << (8 * b);
+            }
+            const uint32_t g = (X & 0x10101010u) >> 4;  // 1 per flipped site
+            const uint32_t gm = g * 0xFFu;
+            const uint32_t ns = s ^ (gm - g);           // flipped bytes ^= 0xFE
+            out[w] = ns;
+            acc_f += g;
+            acc_dn += ns & M2;                          // twice the new down count
+            if constexpr (ENERGY) {
+                // twice the anti-aligned count of the new spin
+                acc_e += (A2 & ~gm) | ((0x08080808u - A2) & gm);
+            }
+        }
+        *reinterpret_cast<uint4*>(own + base) = make_uint4(out[0], out[1], out[2], out[3]);
+        n_acc += byte_sum(acc_f);
+        m_acc += 16 - int32_t(byte_sum(acc_dn));
+        // sum_k s_k h_k = sum_k (4 - 2 anti_k)
+        if constexpr (ENERGY) e_acc += 64 - int32_t(byte_sum(acc_e));
+    }
+    double v[kObs] = {ENERGY ? double(-int64_t(a.J) * e_acc) : 0.0, double(m_acc), 0, 0, 0, 0, 0, double(n_acc)};
+    finish_pass<kObs>(v, a.out);
+}
+
 // ----------------------------------------------------- Ising, any topology
 
 struct IsingArgs
