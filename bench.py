@@ -62,6 +62,23 @@ def workload(L):
             f"(UniformSphereN<3>), E and M reduced in FP64 every step")
 
 
+def aggregate_ranks(dist, torch, device, total_ms, units, e2e_value=None):
+    """Whole-job figures of a replicas run: the slowest rank's device time
+    (max), the units all ranks processed (sum) and, when given, the sum of the
+    ranks' end-to-end throughputs.  Every rank makes the same collective calls
+    in the same order (e2e_value is None on all ranks or on none)."""
+    t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+    u = torch.tensor([units], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    e2e_sum = None
+    if e2e_value is not None:
+        ev = torch.tensor([e2e_value], dtype=torch.float64, device=device)
+        dist.all_reduce(ev, op=dist.ReduceOp.SUM)
+        e2e_sum = float(ev.item())
+    return float(t.item()), float(u.item()), e2e_sum
+
+
 def rank_info():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -720,15 +737,10 @@ def main():
     # ---- aggregate over ranks
     max_ms, tot_units = total_ms, units
     if ws > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        u = torch.tensor([units], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(u, op=dist.ReduceOp.SUM)
-        max_ms, tot_units = float(t.item()), float(u.item())
+        max_ms, tot_units, e2e_sum = aggregate_ranks(dist, torch, "cuda", total_ms, units,
+                                                     None if e2e is None else e2e["value"])
         if e2e is not None:
-            ev = torch.tensor([e2e["value"]], dtype=torch.float64, device="cuda")
-            dist.all_reduce(ev, op=dist.ReduceOp.SUM)
-            e2e["value"] = float(ev.item())
+            e2e["value"] = e2e_sum
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

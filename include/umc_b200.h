@@ -404,6 +404,17 @@ int umc_mlp_train(umc_mlp* n, uint64_t steps, uint32_t batch, double lr, double*
 int umc_mlp_counters(const umc_mlp* n, uint64_t* steps, uint64_t* kernel_launches);
 void* umc_mlp_stream(const umc_mlp* n);
 
+/* ================================================================ self-test */
+
+/* No counterpart in the reference.  Every device-side wait of the engine (grid
+ * barrier, union-find, tensor-core mbarriers) has an iteration limit; on expiry
+ * the kernel records a status bit and returns, and the call that launched it
+ * returns UMC_ERR_DEVICE_TIMEOUT with the context still usable.  This runs the
+ * engine's grid barrier on a barrier whose generation never advances (about
+ * 0.3 s), reports the status bits the kernel left (8 = grid barrier) and
+ * returns UMC_ERR_DEVICE_TIMEOUT after checking that the device still answers. */
+int umc_selftest_barrier_timeout(int32_t device, uint32_t* status_bits);
+
 /* ================================================= series statistics (host) */
 
 /* No counterpart in the reference (its tests compare chain means against fixed

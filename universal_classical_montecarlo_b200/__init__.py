@@ -216,6 +216,19 @@ def device_count() -> int:
     return n.value
 
 
+# ================================================================== self-test
+_decl("umc_selftest_barrier_timeout", _int, _i32, C.POINTER(_u32))
+
+
+def selftest_barrier_timeout(device: int = 0):
+    """Runs the engine's bounded grid barrier on a barrier that never completes.
+    Returns (status code, status bits): ERR_DEVICE_TIMEOUT and bit 8 when the
+    bound works."""
+    bits = _u32(0)
+    code = lib.umc_selftest_barrier_timeout(device, C.byref(bits))
+    return code, bits.value
+
+
 # ================================================================= statistics
 _decl("umc_tau_int", _int, _vp, _u64, _f64, C.POINTER(_f64), C.POINTER(_f64), C.POINTER(_u64))
 _decl("umc_binning_error", _int, _vp, _u64, _u64, C.POINTER(_f64), C.POINTER(_f64))

@@ -882,11 +882,43 @@ void run_chunked(umc_chain* c, uint64_t n, double* records, uint64_t* sizes, boo
 }
 
 }  // namespace
+// Self-test of the bounded grid barrier: the barrier's arrival count starts
+// far from gridDim - 1, so its generation never advances and every block runs
+// into kBarrierSpins.
+static __global__ void barrier_selftest(GridBarrier* b, unsigned* status) { grid_barrier(b, status); }
+
 }  // namespace umc
 
 using namespace umc;
 
 extern "C" {
+
+int umc_selftest_barrier_timeout(int32_t device, uint32_t* status_bits)
+{
+    return guarded([&] {
+        cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        struct Cells
+        {
+            GridBarrier bar;
+            unsigned status;
+        };
+        DevBuf buf;
+        buf.alloc(sizeof(Cells), "self-test barrier");
+        const Cells init{{0xF0000000u, 0u}, 0u};
+        cuda_check(cudaMemcpy(buf.p, &init, sizeof init, cudaMemcpyHostToDevice), "self-test set-up");
+        Cells* d = buf.as<Cells>();
+        barrier_selftest<<<2, 32>>>(&d->bar, &d->status);
+        cuda_check(cudaGetLastError(), "self-test launch");
+        Cells got{};
+        cuda_check(cudaMemcpy(&got, buf.p, sizeof got, cudaMemcpyDeviceToHost), "self-test result");
+        // the context still answers: a trivial operation after the timed-out kernel
+        cuda_check(cudaMemset(buf.p, 0, sizeof(Cells)), "context check");
+        cuda_check(cudaDeviceSynchronize(), "context check");
+        if (status_bits) *status_bits = got.status;
+        if (got.status & kDevErrBarrier)
+            throw Error(UMC_ERR_DEVICE_TIMEOUT, "grid barrier wait bound exhausted (self-test)");
+    });
+}
 
 int umc_device_count(int* count)
 {

@@ -162,6 +162,99 @@ __device__ __forceinline__ void mat_expm(const Mat<N>& a, Mat<N>& result)
     }
 }
 
+// exp(i X) for a traceless Hermitian X in closed form (the reference sums the
+// Taylor series with scaling and squaring, dof/sun.hpp:118-146; both agree to
+// FP32 rounding).  SU(2): X^2 = |q|^2 I, so exp(iX) = cos|q| I + i sin|q|/|q| X.
+// SU(3): Cayley-Hamilton, exp(iX) = f0 I + f1 X + f2 X^2 with f_j from
+// c0 = det X and c1 = tr X^2 / 2 (Morningstar & Peardon, Phys. Rev. D 69,
+// 054501 (2004)), using f_j(-c0) = (-1)^j conj f_j(c0) so that the
+// denominator 9u^2 - w^2 stays >= 2 c1.  Other N: the Taylor series.
+template <int N>
+__device__ __forceinline__ void su_exp_i(const Mat<N>& x, Mat<N>& e)
+{
+    if constexpr (N == 2) {
+        const float q2 = x.re[0] * x.re[0] + x.re[1] * x.re[1] + x.im[1] * x.im[1];
+        const float q = sqrtf(q2);
+        float sn, cs;
+        sincosf(q, &sn, &cs);
+        const float sq = q > 1e-3f ? sn / q : 1.f - q2 * (1.f / 6.f);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            e.re[k] = (k == 0 || k == 3 ? cs : 0.f) - sq * x.im[k];
+            e.im[k] = sq * x.re[k];
+        }
+    } else if constexpr (N == 3) {
+        Mat<3> x2;
+        mat_mul<3, false, false>(x, x, x2);
+        const float c1 = 0.5f * (x2.re[0] + x2.re[4] + x2.re[8]);
+        if (c1 < 1e-8f) {  // exp(iX) = I + iX - X^2/2 + O(|X|^3)
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                e.re[k] = (k % 4 == 0 ? 1.f : 0.f) - x.im[k] - 0.5f * x2.re[k];
+                e.im[k] = x.re[k] - 0.5f * x2.im[k];
+            }
+            return;
+        }
+        float tr3 = 0.f;  // tr(X X^2) = 3 det X
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) tr3 += x.re[i * 3 + j] * x2.re[j * 3 + i] - x.im[i * 3 + j] * x2.im[j * 3 + i];
+        const float c0 = tr3 * (1.f / 3.f);
+        const bool neg = c0 < 0.f;
+        // theta = acos(|c0| / c0_max), c0_max = 2 (c1 / 3)^(3/2)
+        const float c13 = c1 * (1.f / 3.f);
+        const float th = acosf(fminf(fabsf(c0) / (2.f * c13 * sqrtf(c13)), 1.f));
+        float s3, c3;
+        sincosf(th * (1.f / 3.f), &s3, &c3);
+        const float u = sqrtf(c1 * (1.f / 3.f)) * c3, w = sqrtf(c1) * s3;
+        const float w2 = w * w, u2 = u * u;
+        const float xi = fabsf(w) < 0.05f ? 1.f - w2 * (1.f / 6.f) * (1.f - w2 * (1.f / 20.f) * (1.f - w2 * (1.f / 42.f)))
+                                          : sinf(w) / w;
+        float s2u, c2u, su, cu, sw, cw;
+        sincosf(2.f * u, &s2u, &c2u);
+        sincosf(u, &su, &cu);
+        sincosf(w, &sw, &cw);
+        (void)sw;  // sin w enters through xi
+        // e^{-iu} = (cu, -su)
+        auto emiu = [&](float ar, float ai, float& rr, float& ri) {  // e^{-iu} (ar + i ai)
+            rr = cu * ar + su * ai;
+            ri = cu * ai - su * ar;
+        };
+        float h0r, h0i, h1r, h1i, h2r, h2i, tr, ti;
+        emiu(8.f * u2 * cw, 2.f * u * (3.f * u2 + w2) * xi, tr, ti);
+        h0r = (u2 - w2) * c2u + tr;
+        h0i = (u2 - w2) * s2u + ti;
+        emiu(2.f * u * cw, -(3.f * u2 - w2) * xi, tr, ti);
+        h1r = 2.f * u * c2u - tr;
+        h1i = 2.f * u * s2u - ti;
+        emiu(cw, 3.f * u * xi, tr, ti);
+        h2r = c2u - tr;
+        h2i = s2u - ti;
+        const float id = 1.f / (9.f * u2 - w2);
+        float f0r = h0r * id, f0i = h0i * id, f1r = h1r * id, f1i = h1i * id, f2r = h2r * id, f2i = h2i * id;
+        if (neg) {  // f_j(-c0) = (-1)^j conj f_j(c0)
+            f0i = -f0i;
+            f1r = -f1r;
+            f2i = -f2i;
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const float d = k % 4 == 0 ? 1.f : 0.f;
+            e.re[k] = f0r * d + f1r * x.re[k] - f1i * x.im[k] + f2r * x2.re[k] - f2i * x2.im[k];
+            e.im[k] = f0i * d + f1r * x.im[k] + f1i * x.re[k] + f2r * x2.im[k] + f2i * x2.re[k];
+        }
+    } else {
+        Mat<N> a;
+#pragma unroll
+        for (int q = 0; q < N * N; ++q) {  // a = i x
+            a.re[q] = -x.im[q];
+            a.im[q] = x.re[q];
+        }
+        mat_expm<N>(a, e);
+    }
+}
+
 // SUShift<N>::sample (dof/sun.hpp:163-204): traceless Hermitian X from N + N(N-1)
 // keyed uniforms (diagonal first, then (a, b) per upper pair), U' = U exp(iX).
 template <int N>
@@ -189,13 +282,8 @@ __device__ __forceinline__ void su_shift(KeyedPcg& g, float width, const Mat<N>&
         }
 #pragma unroll
     for (int i = 0; i < N; ++i) x.re[i * N + i] -= tr / float(N);
-    Mat<N> a, e;
-#pragma unroll
-    for (int q = 0; q < N * N; ++q) {  // a = i x
-        a.re[q] = -x.im[q];
-        a.im[q] = x.re[q];
-    }
-    mat_expm<N>(a, e);
+    Mat<N> e;
+    su_exp_i<N>(x, e);
     mat_mul<N, false, false>(cur, e, out);
 }
 
