@@ -60,9 +60,18 @@ constexpr uint32_t IMG_BYTES = IMG_B2T + 8192;
 
 // Tensor-memory columns.  The output layer reuses the first layer's columns
 // (read out before the second product is issued), so a forward needs 128.
+// The sampler's second layer also reuses them (64 columns per tile group);
+// training keeps z2 / dH2 at column 64.
 constexpr uint32_t TM_Z1 = 0, TM_Z2 = 64, TM_O = 0;     // forward (and dH1 / dH2)
 constexpr uint32_t TM_G1 = 128, TM_G2 = 288;            // weight-gradient accumulators (144 + 80)
-constexpr uint32_t kFwdCols = 128, kTrainCols = 512;
+constexpr uint32_t kFwdCols = 64, kTrainCols = 512;
+// tcgen05.alloc takes a power of two >= 32 columns
+__host__ __device__ constexpr uint32_t alloc_cols(uint32_t c)
+{
+    uint32_t p = 32;
+    while (p < c) p <<= 1;
+    return p;
+}
 // Dynamic shared memory of the forward kernels is at least this, so that at
 // most three of their CTAs (3 x 128 TMEM columns) share an SM.
 constexpr uint32_t kFwdMinSmem = 58 * 1024;
@@ -140,6 +149,7 @@ struct Tile
     uint32_t phase;
     uint32_t row;        // this thread's row, 0..127
     uint32_t bar;        // named barrier id of the group (1..15)
+    uint32_t z2col;      // TMEM column of the second layer's accumulator
 };
 
 // Waits for the next MMA completion; records a timeout in *fail.
@@ -181,6 +191,31 @@ __device__ __forceinline__ uint64_t layer_epilogue(const Tile& t, uint32_t col, 
     return mask;
 }
 
+// The same epilogue without the mask (sampler and forward): bias added in FP32,
+// then BF16 rounding and ReLU on packed pairs (relu(bf16(z)) = bf16(relu(z))).
+__device__ __forceinline__ void layer_epilogue_fast(const Tile& t, uint32_t col, const float* bias, uint8_t* dst)
+{
+    const __nv_bfloat162 zero = __float2bfloat162_rn(0.0f);
+    const uint32_t row = t.row;
+#pragma unroll
+    for (uint32_t c = 0; c < 4; ++c) {
+        float v[16];
+        tc::tmem_ld16(tc::tmem_lane_addr(t.tmem, col + 16 * c), v);
+        tc::tmem_wait_ld();
+        uint32_t w[8];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float4 b = reinterpret_cast<const float4*>(bias + 16 * c)[q];
+            __nv_bfloat162 p0 = __hmax2(__floats2bfloat162_rn(v[4 * q] + b.x, v[4 * q + 1] + b.y), zero);
+            __nv_bfloat162 p1 = __hmax2(__floats2bfloat162_rn(v[4 * q + 2] + b.z, v[4 * q + 3] + b.w), zero);
+            w[2 * q] = *reinterpret_cast<uint32_t*>(&p0);
+            w[2 * q + 1] = *reinterpret_cast<uint32_t*>(&p1);
+        }
+        *reinterpret_cast<uint4*>(dst + tc::kmajor_offset(kTile, row, 16 * c)) = make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4*>(dst + tc::kmajor_offset(kTile, row, 16 * c + 8)) = make_uint4(w[4], w[5], w[6], w[7]);
+    }
+}
+
 // Forward pass of one tile: x (this thread's row) -> o[16].  All 128 threads
 // call it.  h1 goes to t.H1, h2 to t.H2; masks receive the ReLU masks.
 // Returns true (uniformly) on a wait timeout.
@@ -202,17 +237,20 @@ __device__ bool tile_forward(Tile& t, const float x[3], float o[16], uint64_t* m
         tc::mma_commit(t.mbar);
     }
     tile_wait(t, fail);
-    const uint64_t m1 = layer_epilogue(t, TM_Z1, bias, t.H1);
+    uint64_t m1 = 0, m2 = 0;
+    if (masks) m1 = layer_epilogue(t, TM_Z1, bias, t.H1);
+    else layer_epilogue_fast(t, TM_Z1, bias, t.H1);
     if (tile_sync(t, fail)) return true;
     if (row == 0) {
         tc::fence_after();
         for (uint32_t s = 0; s < 4; ++s)
-            tc::mma_bf16(t.tmem + TM_Z2, tc::operand_desc(tc::smem_addr(t.H1), kTile, s),
+            tc::mma_bf16(t.tmem + t.z2col, tc::operand_desc(tc::smem_addr(t.H1), kTile, s),
                          tc::operand_desc(ximg + IMG_B2, 64, s), tc::idesc_bf16(128, 64), s > 0);
         tc::mma_commit(t.mbar);
     }
     tile_wait(t, fail);
-    const uint64_t m2 = layer_epilogue(t, TM_Z2, bias + 64, t.H2);
+    if (masks) m2 = layer_epilogue(t, t.z2col, bias + 64, t.H2);
+    else layer_epilogue_fast(t, t.z2col, bias + 64, t.H2);
     if (tile_sync(t, fail)) return true;
     if (row == 0) {
         tc::fence_after();
@@ -605,7 +643,7 @@ __global__ void __launch_bounds__(256) u1_plain_batch(U1BatchArgs a)
 // mbarriers and the TMEM address slot, then the chain's angles.  The total is
 // padded so that the CTAs one SM can hold never ask for more than 512 TMEM
 // columns between them.
-constexpr uint32_t kGroups = 4;  // tile groups of the learned sampler
+constexpr uint32_t kGroups = 6;  // tile groups of the learned sampler (768 threads, 6 x 64 TMEM columns)
 
 struct LearnSmem
 {
@@ -620,7 +658,7 @@ struct LearnSmem
         p.bar = p.X + groups * p.group_bytes;
         p.field = p.bar + 128;
         p.total = p.field + 2u * L * L * 4u;
-        const uint32_t per_sm = 512u / (groups * kFwdCols);  // CTAs whose TMEM fits one SM
+        const uint32_t per_sm = 512u / alloc_cols(groups * kFwdCols);  // CTAs whose TMEM fits one SM
         const uint32_t floor_bytes = 228u * 1024u / (per_sm + 1) + 1024u;
         if (p.total < floor_bytes) p.total = floor_bytes;
         return p;
@@ -644,12 +682,12 @@ __global__ void __launch_bounds__(kTile * kGroups, 1) u1_learned_batch(U1BatchAr
         reinterpret_cast<uint4*>(img)[i] = reinterpret_cast<const uint4*>(a.img)[i];
     if (t == 0)
         for (uint32_t g = 0; g < kGroups; ++g) tc::mbar_init(mbar + g, 1);
-    if (t < 32) tc::tmem_alloc(tslot, kFwdCols * kGroups);
+    if (t < 32) tc::tmem_alloc(tslot, alloc_cols(kFwdCols * kGroups));
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
     uint8_t* gx = smem + sp.X + grp * sp.group_bytes;
-    Tile tl{img, gx, gx + kTile * 32, gx + kTile * 32, mbar + grp, *tslot + grp * kFwdCols, 0u, t % kTile, 1u + grp};
+    Tile tl{img, gx, gx + kTile * 32, gx + kTile * 32, mbar + grp, *tslot + grp * kFwdCols, 0u, t % kTile, 1u + grp, 0u};
 
     const Lat2 g{a.L, a.L / 2, a.L * a.L / 2};
     const uint32_t nl = 2 * a.L * a.L;
@@ -692,7 +730,7 @@ __global__ void __launch_bounds__(kTile * kGroups, 1) u1_learned_batch(U1BatchAr
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
-    if (t < 32) tc::tmem_dealloc(*tslot, kFwdCols * kGroups);
+    if (t < 32) tc::tmem_dealloc(*tslot, alloc_cols(kFwdCols * kGroups));
 }
 
 // ------------------------------------------------------------ forward (tests)
@@ -713,7 +751,7 @@ __global__ void __launch_bounds__(kTile) mlp_forward_kernel(const uint8_t* gimg,
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
-    Tile tl{img, smem + sp.X, smem + sp.H, smem + sp.H, mbar, *tslot, 0u, t, 1u};
+    Tile tl{img, smem + sp.X, smem + sp.H, smem + sp.H, mbar, *tslot, 0u, t, 1u, 0u};
     const uint32_t tiles = (n + kTile - 1) / kTile;
     bool failed = false;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
@@ -820,7 +858,7 @@ __global__ void __launch_bounds__(kTile) mlp_train_kernel(TrainArgs a)
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
-    Tile tl{img, smem + sp.X, smem + sp.H1, smem + sp.H2, mbar, *tslot, 0u, t, 1u};
+    Tile tl{img, smem + sp.X, smem + sp.H1, smem + sp.H2, mbar, *tslot, 0u, t, 1u, TM_Z2};
     const uint32_t ximg = tc::smem_addr(img);
 
     const uint32_t tiles = (a.n + kTile - 1) / kTile;
