@@ -479,10 +479,33 @@ bool launch_fused_t(umc_chain* c, FusedArgs& a)
     return true;
 }
 
+// Bound on the + bonds that can leave a TX x TY x TZ tile: in direction d
+// only the sites of the last plane of each tile, ceil(L_d / T_d) planes of
+// n / L_d sites.
+uint64_t crossing_capacity(const umc_chain* c, uint32_t TX, uint32_t TY, uint32_t TZ)
+{
+    const uint64_t T[3] = {TX, TY, TZ};
+    uint64_t cap = 0;
+    for (int d = 0; d < 3; ++d) {
+        const uint64_t L = c->dims[d];
+        if (L < 2) continue;
+        cap += (L + T[d] - 1) / T[d] * (c->n / L);
+    }
+    return cap;
+}
+
 template <int N>
 bool launch_fused_n(umc_chain* c, FusedArgs& a)
 {
-    if (a.w.Lz > 1) return launch_fused_t<N, 8, 8, 8>(c, a);
+    const bool three = a.w.Lz > 1;
+    const uint64_t cap = three ? crossing_capacity(c, 8, 8, 8) : crossing_capacity(c, 32, 16, 1);
+    if (a.do_wolff) {
+        if (c->n >= (uint64_t(1) << 30)) return false;  // list entries are site * 4 + direction
+        if (c->xlist.bytes < cap * 4) c->xlist.alloc(cap * 4, "Wolff crossing-bond list");
+        a.xlist = c->xlist.as<uint32_t>();
+        a.xcap = uint32_t(cap);
+    }
+    if (three) return launch_fused_t<N, 8, 8, 8>(c, a);
     return launch_fused_t<N, 32, 16, 1>(c, a);
 }
 
@@ -797,7 +820,7 @@ void destroy_chain(umc_chain* c)
         cudaEventDestroy(t.b);
     }
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
-    for (DevBuf* b : {&c->field, &c->staging, &c->off, &c->adj, &c->slot, &c->position, &c->lab0, &c->lab1, &c->cells,
+    for (DevBuf* b : {&c->field, &c->staging, &c->off, &c->adj, &c->slot, &c->position, &c->lab0, &c->lab1, &c->xlist, &c->cells,
                       &c->inc_off, &c->inc_cell, &c->inc_which, &c->partials, &c->ctl, &c->records, &c->sizes, &c->tm1})
         b->free_();
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);

@@ -67,7 +67,7 @@ struct umc_chain
     cudaStream_t stream = nullptr;
     bool own_stream = false;
 
-    umc::DevBuf field, staging, off, adj, slot, position, lab0, lab1;
+    umc::DevBuf field, staging, off, adj, slot, position, lab0, lab1, xlist;
     umc::DevBuf cells, inc_off, inc_cell, inc_which;
     umc::DevBuf partials, ctl, records, sizes, tm1;
     size_t field_bytes = 0;

@@ -39,7 +39,7 @@ struct DevCtl
 {
     unsigned int ticket[kMaxPasses];
     unsigned int status;
-    unsigned int pad;
+    unsigned int xcount;  // entries of the fused Wolff step's crossing-bond list
     GridBarrier bar;
     double pass_total[kMaxPasses][kObs];
 };

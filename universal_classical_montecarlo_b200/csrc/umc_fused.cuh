@@ -68,6 +68,8 @@ struct FusedArgs
     uint32_t proposal;  // kPropSphere / kPropRotation
     float delta;
     PassOut out;        // record of the sweep (pass index: dedicated slot)
+    uint32_t* xlist;    // activated tile-crossing bonds, site * 4 + direction
+    uint32_t xcap;      // its capacity (>= every + bond that can leave a tile)
 };
 
 template <int N>
@@ -118,6 +120,7 @@ __global__ void __launch_bounds__(TX * TY * TZ, 2) hybrid_fused(FusedArgs a)
     __shared__ uint32_t lab[T];
     __shared__ float r_sh[4];
     __shared__ uint32_t root_sh;
+    __shared__ uint32_t xs_cnt, xs_base;
     const WolffTileArgs& w = a.w;
     unsigned* status = &w.ctl->status;
     const uint32_t tid = threadIdx.x;
@@ -176,34 +179,47 @@ __global__ void __launch_bounds__(TX * TY * TZ, 2) hybrid_fused(FusedArgs a)
                     }
                 }
             }
+            // compact this tile's activated crossing bonds into the global list:
+            // one atomic per block, then each thread writes its bonds
+            if (tid == 0) xs_cnt = 0;
+            __syncthreads();
+            const uint32_t nc = __popc(cross);
+            const uint32_t off = nc ? atomicAdd(&xs_cnt, nc) : 0u;
+            __syncthreads();
+            if (tid == 0) xs_base = xs_cnt ? atomicAdd(&w.ctl->xcount, xs_cnt) : 0u;
             __syncthreads();
             if (valid) {
                 const uint32_t root = smem_find(lab, tid);
                 const uint32_t rx = root % TX, ry = (root / TX) % TY, rz = root / (TX * TY);
                 w.label[nat] = ((bz * TZ + rz) * w.Ly + (by * TY + ry)) * w.Lx + (bx * TX + rx);
-                w.cross[nat] = uint8_t(cross);
-            }
-        }
-        if (!grid_barrier(a.bar, status)) return;
-
-        // ---- B: tile-crossing bonds
-        for (uint32_t nat = gtid; nat < w.n; nat += gsize) {
-            const uint32_t cross = __ldcg(w.cross + nat);
-            if (!cross) continue;
-            const uint32_t x = nat % w.Lx, rr = nat / w.Lx, y = rr % w.Ly, z = rr / w.Ly;
+                uint32_t slot = xs_base + off;
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                if (!(cross & (1u << d))) continue;
-                uint32_t xj = x, yj = y, zj = z;
-                if (d == 0) xj = x + 1 == w.Lx ? 0 : x + 1;
-                if (d == 1) yj = y + 1 == w.Ly ? 0 : y + 1;
-                if (d == 2) zj = z + 1 == w.Lz ? 0 : z + 1;
-                uf_union(w.label, nat, (zj * w.Ly + yj) * w.Lx + xj, w.n + 1, status);
+                for (int d = 0; d < 3; ++d) {
+                    if (!(cross & (1u << d))) continue;
+                    if (slot < a.xcap) a.xlist[slot] = nat * 4u + uint32_t(d);
+                    else atomicOr(status, kDevErrGeometry);
+                    ++slot;
+                }
             }
         }
         if (!grid_barrier(a.bar, status)) return;
 
-        // ---- C: flip the seed's cluster
+        // ---- B: tile-crossing bonds, one list entry per thread
+        const uint32_t xcount = min(__ldcg(&w.ctl->xcount), a.xcap);
+        for (uint32_t i = gtid; i < xcount; i += gsize) {
+            const uint32_t e = __ldcg(a.xlist + i);
+            const uint32_t nat = e >> 2, d = e & 3u;
+            const uint32_t x = nat % w.Lx, rr = nat / w.Lx, y = rr % w.Ly, z = rr / w.Ly;
+            uint32_t xj = x, yj = y, zj = z;
+            if (d == 0) xj = x + 1 == w.Lx ? 0 : x + 1;
+            if (d == 1) yj = y + 1 == w.Ly ? 0 : y + 1;
+            if (d == 2) zj = z + 1 == w.Lz ? 0 : z + 1;
+            uf_union(w.label, nat, (zj * w.Ly + yj) * w.Lx + xj, w.n + 1, status);
+        }
+        if (!grid_barrier(a.bar, status)) return;
+
+        // ---- C: flip the seed's cluster (the list is consumed: reset it)
+        if (gtid == 0) w.ctl->xcount = 0u;
         if (tid == 0) {
             // seed site: next draw of the axis stream, colour-major -> natural
             const uint32_t ks = uint32_t(u_f64(gax.next()) * double(w.n));
