@@ -448,11 +448,11 @@ void stencil_flip(umc_chain* c, double beta, unsigned long long* size_slot)
 // Fused step on a regular lattice (umc_fused.cuh): returns false when the
 // chain does not qualify or cooperative launch is unavailable, in which case
 // the caller runs the multi-kernel path.
-template <int N, int TX, int TY, int TZ>
+template <int N, int TX, int TY, int TZ, int SPT>
 bool launch_fused_t(umc_chain* c, FusedArgs& a)
 {
-    auto kern = hybrid_fused<N, TX, TY, TZ>;
-    constexpr int T = TX * TY * TZ;
+    auto kern = hybrid_fused<N, TX, TY, TZ, SPT>;
+    constexpr int T = TX * TY * TZ / SPT;  // threads per block
     if (c->fused_grid < 0) {
         int coop = 0, nb = 0, sms = 0;
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
@@ -505,8 +505,8 @@ bool launch_fused_n(umc_chain* c, FusedArgs& a)
         a.xlist = c->xlist.as<uint32_t>();
         a.xcap = uint32_t(cap);
     }
-    if (three) return launch_fused_t<N, 8, 8, 8>(c, a);
-    return launch_fused_t<N, 32, 16, 1>(c, a);
+    if (three) return launch_fused_t<N, 8, 8, 8, 2>(c, a);
+    return launch_fused_t<N, 32, 16, 1, 2>(c, a);
 }
 
 bool fused_step(umc_chain* c, double beta, bool wolff, bool sweep, double* rec, unsigned long long* size_slot)
@@ -905,10 +905,13 @@ void run_chunked(umc_chain* c, uint64_t n, double* records, uint64_t* sizes, boo
 }
 
 }  // namespace
-// Self-test of the bounded grid barrier: the barrier's arrival count starts
-// far from gridDim - 1, so its generation never advances and every block runs
+// Self-test of the bounded grid barrier: a grid of two blocks of which only
+// the first arrives, so the count never reaches gridDim and that block runs
 // into kBarrierSpins.
-static __global__ void barrier_selftest(GridBarrier* b, unsigned* status) { grid_barrier(b, status); }
+static __global__ void barrier_selftest(GridBarrier* b, unsigned* status)
+{
+    if (blockIdx.x == 0) grid_barrier(b, status);
+}
 
 }  // namespace umc
 
@@ -927,7 +930,7 @@ int umc_selftest_barrier_timeout(int32_t device, uint32_t* status_bits)
         };
         DevBuf buf;
         buf.alloc(sizeof(Cells), "self-test barrier");
-        const Cells init{{0xF0000000u, 0u}, 0u};
+        const Cells init{{0u, 0u}, 0u};
         cuda_check(cudaMemcpy(buf.p, &init, sizeof init, cudaMemcpyHostToDevice), "self-test set-up");
         Cells* d = buf.as<Cells>();
         barrier_selftest<<<2, 32>>>(&d->bar, &d->status);

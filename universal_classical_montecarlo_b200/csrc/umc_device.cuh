@@ -29,10 +29,13 @@ constexpr unsigned kDevErrRetry = 4u;       // proposal retry bound exhausted
 constexpr unsigned kDevErrBarrier = 8u;     // grid barrier wait bound exhausted
 
 // counter + generation of the bounded grid barrier (umc_fused.cuh)
+// Grid barrier of a cooperative launch: count only grows within a launch
+// (barrier k completes at k * gridDim arrivals); the last block to retire
+// resets both words for the next launch.
 struct GridBarrier
 {
     unsigned int count;
-    unsigned int gen;
+    unsigned int done;
 };
 
 struct DevCtl
@@ -156,6 +159,35 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t* lab, uint32_t x, uint32_t 
     }
     atomicOr(status, kDevErrUnionFind);
     return x;
+}
+
+// Two finds walked in lockstep (independent load chains overlap their
+// latency); same path halving and bound as uf_find.
+__device__ __forceinline__ void uf_find2(uint32_t* lab, uint32_t x0, uint32_t x1, uint32_t bound, unsigned* status,
+                                         uint32_t& r0, uint32_t& r1)
+{
+    volatile uint32_t* L = lab;
+    bool d0 = false, d1 = false;
+    for (uint32_t it = 0; it < bound; ++it) {
+        const uint32_t p0 = d0 ? x0 : L[x0];
+        const uint32_t p1 = d1 ? x1 : L[x1];
+        d0 = d0 || p0 == x0;
+        d1 = d1 || p1 == x1;
+        if (d0 && d1) {
+            r0 = x0;
+            r1 = x1;
+            return;
+        }
+        const uint32_t g0 = d0 ? x0 : L[p0];
+        const uint32_t g1 = d1 ? x1 : L[p1];
+        if (!d0 && g0 != p0) L[x0] = g0;
+        if (!d1 && g1 != p1) L[x1] = g1;
+        if (!d0) x0 = g0;
+        if (!d1) x1 = g1;
+    }
+    atomicOr(status, kDevErrUnionFind);
+    r0 = x0;
+    r1 = x1;
 }
 
 __device__ __forceinline__ void uf_union(uint32_t* lab, uint32_t a, uint32_t b, uint32_t bound, unsigned* status)

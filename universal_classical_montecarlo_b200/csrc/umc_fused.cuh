@@ -7,7 +7,8 @@
 // grid barrier, with all blocks co-resident (cooperative launch):
 //
 //   A  Wolff: per tile, bond activation + shared-memory union-find  (optional)
-//   B  Wolff: union of tile-crossing bonds on the global labels     (optional)
+//   B  Wolff: union of the activated tile-crossing bonds, compacted
+//      into a list in A, on the global labels                       (optional)
 //   C  Wolff: reflect the seed's cluster                             (optional)
 //   D  Metropolis pass over colour class 0                           (optional)
 //   E  Metropolis pass over colour class 1, FP64 observables folded  (optional)
@@ -25,7 +26,10 @@
 
 namespace umc {
 
-constexpr unsigned kBarrierSpins = 1u << 22;  // x ~64 ns sleep: ~0.3 s
+// polls: the first kBarrierHot back to back (a balanced phase ends within a
+// few L2 round trips), then with a 64 ns sleep; the bound is ~0.3 s
+constexpr unsigned kBarrierSpins = 1u << 22;
+constexpr unsigned kBarrierHot = 256u;
 
 __device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned* status)
 {
@@ -33,28 +37,37 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned* status)
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
-        volatile unsigned int* vgen = &b->gen;
-        const unsigned int g = *vgen;
         __threadfence();
-        if (atomicAdd(&b->count, 1u) == gridDim.x - 1) {
-            atomicExch(&b->count, 0u);
-            __threadfence();
-            atomicAdd(&b->gen, 1u);
-        } else {
-            unsigned int it = 0;
-            while (*vgen == g) {
-                if (++it > kBarrierSpins) {
-                    atomicOr(status, kDevErrBarrier);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
+        // arrival; this barrier completes when count reaches the next
+        // multiple of gridDim (one round trip, no generation word to update)
+        const unsigned int old = atomicAdd(&b->count, 1u);
+        const unsigned int target = (old / gridDim.x + 1u) * gridDim.x;
+        volatile unsigned int* cnt = &b->count;
+        unsigned int it = 0;
+        while (*cnt < target) {
+            if (++it > kBarrierSpins) {
+                atomicOr(status, kDevErrBarrier);
+                ok = 0;
+                break;
             }
+            if (it > kBarrierHot) __nanosleep(64);
         }
         __threadfence();
     }
     __syncthreads();
     return ok != 0;
+}
+
+// Once per block after its last barrier: the last block to get here has seen
+// every other block leave its polls, so it can reset the counter for the next
+// launch (stream-ordered after this one).  A block that left on a barrier
+// error does not retire; the host clears the control block on that error.
+__device__ __forceinline__ void grid_barrier_retire(GridBarrier* b)
+{
+    if (threadIdx.x == 0 && atomicAdd(&b->done, 1u) == gridDim.x - 1) {
+        b->count = 0u;
+        b->done = 0u;
+    }
 }
 
 struct FusedArgs
@@ -111,12 +124,17 @@ __device__ __forceinline__ void fused_site(const FusedArgs& a, const StencilTopo
     acc[7] += acc_ok ? 1.0 : 0.0;
 }
 
-// MODEL = N >= 1 (VectorSpin<N>).  Block = one tile of TX*TY*TZ threads.
-template <int MODEL, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX * TY * TZ, 2) hybrid_fused(FusedArgs a)
+// MODEL = N >= 1 (VectorSpin<N>).  Phase A: one tile of TX*TY*TZ sites per
+// block and iteration, SPT sites per thread (local ids tid + u * blockDim).
+// Each thread first activates the bonds of all its sites (their loads and
+// draws overlap), then does the shared-memory unions.
+template <int MODEL, int TX, int TY, int TZ, int SPT>
+__global__ void __launch_bounds__(TX * TY * TZ / SPT, 2 * SPT) hybrid_fused(FusedArgs a)
 {
     constexpr int N = MODEL;
     constexpr int T = TX * TY * TZ;
+    constexpr int BT = T / SPT;
+    static_assert(T % SPT == 0, "sites per thread must divide the tile");
     __shared__ uint32_t lab[T];
     __shared__ float r_sh[4];
     __shared__ uint32_t root_sh;
@@ -140,25 +158,33 @@ __global__ void __launch_bounds__(TX * TY * TZ, 2) hybrid_fused(FusedArgs a)
         const uint64_t kb = key_base(key_seed(w.seed, w.flip, kTagBond));
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             __syncthreads();
-            lab[tid] = tid;
+#pragma unroll
+            for (int u = 0; u < SPT; ++u) lab[tid + u * BT] = tid + u * BT;
             __syncthreads();
             float r[N];
 #pragma unroll
             for (int c = 0; c < N; ++c) r[c] = r_sh[c];
             const uint32_t bx = tile % w.ntx, byz = tile / w.ntx;
             const uint32_t by = byz % w.nty, bz = byz / w.nty;
-            const uint32_t tx = tid % TX, ty = (tid / TX) % TY, tz = tid / (TX * TY);
-            const uint32_t x = bx * TX + tx, y = by * TY + ty, z = bz * TZ + tz;
-            const bool valid = x < w.Lx && y < w.Ly && z < w.Lz;
-            uint32_t cross = 0, nat = 0;
-            if (valid) {
-                nat = (z * w.Ly + y) * w.Lx + x;
+            uint32_t nat[SPT], cross[SPT], inner[SPT], tjs[SPT][3];
+            // bond activation of every site of this thread
+#pragma unroll
+            for (int u = 0; u < SPT; ++u) {
+                const uint32_t lid = tid + u * BT;
+                const uint32_t tx = lid % TX, ty = (lid / TX) % TY, tz = lid / (TX * TY);
+                const uint32_t x = bx * TX + tx, y = by * TY + ty, z = bz * TZ + tz;
+                cross[u] = 0;
+                inner[u] = 0;
+                nat[u] = 0xFFFFFFFFu;
+                if (!(x < w.Lx && y < w.Ly && z < w.Lz)) continue;
+                nat[u] = (z * w.Ly + y) * w.Lx + x;
                 float si[N];
-                load_spin<N>(w.field, w.n, colour_major(nat, x, y, z, w.half), si);
+                load_spin<N>(w.field, w.n, colour_major(nat[u], x, y, z, w.half), si);
                 const float ri = vdot<N>(si, r);
                 uint32_t rank = 0;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
+                    tjs[u][d] = 0;
                     const uint32_t L = d == 0 ? w.Lx : (d == 1 ? w.Ly : w.Lz);
                     if (L < 2) continue;
                     uint32_t xj = x, yj = y, zj = z;
@@ -168,35 +194,45 @@ __global__ void __launch_bounds__(TX * TY * TZ, 2) hybrid_fused(FusedArgs a)
                     const uint32_t nj = (zj * w.Ly + yj) * w.Lx + xj;
                     float sj[N];
                     load_spin<N>(w.field, w.n, colour_major(nj, xj, yj, zj, w.half), sj);
-                    const uint32_t k = first_draw(kb, nat * w.ndir + rank);
+                    const uint32_t k = first_draw(kb, nat[u] * w.ndir + rank);
                     ++rank;
                     if (!wolff_bond_active<N>(w.J, w.beta, w.cw, ri, vdot<N>(sj, r), 0, 0, k)) continue;
                     if (xj / TX == bx && yj / TY == by && zj / TZ == bz) {
-                        const uint32_t tj = ((zj - bz * TZ) * TY + (yj - by * TY)) * TX + (xj - bx * TX);
-                        smem_union(lab, tid, tj, status);
+                        tjs[u][d] = ((zj - bz * TZ) * TY + (yj - by * TY)) * TX + (xj - bx * TX);
+                        inner[u] |= 1u << d;
                     } else {
-                        cross |= 1u << d;
+                        cross[u] |= 1u << d;
                     }
                 }
             }
+            // unions inside the tile
+#pragma unroll
+            for (int u = 0; u < SPT; ++u)
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    if (inner[u] & (1u << d)) smem_union(lab, tid + u * BT, tjs[u][d], status);
             // compact this tile's activated crossing bonds into the global list:
             // one atomic per block, then each thread writes its bonds
             if (tid == 0) xs_cnt = 0;
             __syncthreads();
-            const uint32_t nc = __popc(cross);
+            uint32_t nc = 0;
+#pragma unroll
+            for (int u = 0; u < SPT; ++u) nc += __popc(cross[u]);
             const uint32_t off = nc ? atomicAdd(&xs_cnt, nc) : 0u;
             __syncthreads();
             if (tid == 0) xs_base = xs_cnt ? atomicAdd(&w.ctl->xcount, xs_cnt) : 0u;
             __syncthreads();
-            if (valid) {
-                const uint32_t root = smem_find(lab, tid);
+            uint32_t slot = xs_base + off;
+#pragma unroll
+            for (int u = 0; u < SPT; ++u) {
+                if (nat[u] == 0xFFFFFFFFu) continue;
+                const uint32_t root = smem_find(lab, tid + u * BT);
                 const uint32_t rx = root % TX, ry = (root / TX) % TY, rz = root / (TX * TY);
-                w.label[nat] = ((bz * TZ + rz) * w.Ly + (by * TY + ry)) * w.Lx + (bx * TX + rx);
-                uint32_t slot = xs_base + off;
+                w.label[nat[u]] = ((bz * TZ + rz) * w.Ly + (by * TY + ry)) * w.Lx + (bx * TX + rx);
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    if (!(cross & (1u << d))) continue;
-                    if (slot < a.xcap) a.xlist[slot] = nat * 4u + uint32_t(d);
+                    if (!(cross[u] & (1u << d))) continue;
+                    if (slot < a.xcap) a.xlist[slot] = nat[u] * 4u + uint32_t(d);
                     else atomicOr(status, kDevErrGeometry);
                     ++slot;
                 }
@@ -237,17 +273,25 @@ __global__ void __launch_bounds__(TX * TY * TZ, 2) hybrid_fused(FusedArgs a)
             const uint32_t root = root_sh;
             double cnt[1] = {0.0};
             float* f = static_cast<float*>(w.field);
-            for (uint32_t nat = gtid; nat < w.n; nat += gsize) {
-                if (uf_find(w.label, nat, w.n + 1, status) != root) continue;
-                cnt[0] += 1.0;
-                const uint32_t x = nat % w.Lx, rr = nat / w.Lx, y = rr % w.Ly, z = rr / w.Ly;
-                const uint32_t k = colour_major(nat, x, y, z, w.half);
-                float si[N];
+            // two sites per thread and iteration, their finds walked together
+            for (uint32_t n0 = gtid; n0 < w.n; n0 += 2 * gsize) {
+                const uint32_t n1 = n0 + gsize;
+                uint32_t r0, r1;
+                uf_find2(w.label, n0, n1 < w.n ? n1 : n0, w.n + 1, status, r0, r1);
 #pragma unroll
-                for (int c = 0; c < N; ++c) si[c] = __ldcg(f + c * w.n + k);
-                const float d = vdot<N>(si, r);
+                for (int u = 0; u < 2; ++u) {
+                    const uint32_t nat = u ? n1 : n0;
+                    if ((u ? r1 : r0) != root || nat >= w.n) continue;
+                    cnt[0] += 1.0;
+                    const uint32_t x = nat % w.Lx, rr = nat / w.Lx, y = rr % w.Ly, z = rr / w.Ly;
+                    const uint32_t k = colour_major(nat, x, y, z, w.half);
+                    float si[N];
 #pragma unroll
-                for (int c = 0; c < N; ++c) f[c * w.n + k] = si[c] - 2.0f * d * r[c];
+                    for (int c = 0; c < N; ++c) si[c] = __ldcg(f + c * w.n + k);
+                    reflect<N>(si, r);
+#pragma unroll
+                    for (int c = 0; c < N; ++c) f[c * w.n + k] = si[c];
+                }
             }
             block_sum<1>(cnt);
             if (tid == 0 && cnt[0] > 0.0) atomicAdd(w.size_slot, (unsigned long long)cnt[0]);
@@ -266,6 +310,7 @@ __global__ void __launch_bounds__(TX * TY * TZ, 2) hybrid_fused(FusedArgs a)
         for (uint32_t q = gtid; q < w.n - w.half; q += gsize) fused_site<N>(a, t, w.half + q, acc);
         finish_pass<kObs>(acc, a.out);
     }
+    grid_barrier_retire(a.bar);
 }
 
 }  // namespace umc

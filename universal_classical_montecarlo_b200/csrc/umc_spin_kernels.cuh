@@ -344,6 +344,16 @@ __device__ __forceinline__ float vdot(const float* a, const float* b)
     return s;
 }
 
+// Wolff reflection s - 2 (s.r) r in FP32, rounded the same way wherever a
+// cluster is flipped (one fused multiply-add per component).
+template <int N>
+__device__ __forceinline__ void reflect(float* s, const float* r)
+{
+    const float d2 = 2.0f * vdot<N>(s, r);
+#pragma unroll
+    for (int c = 0; c < N; ++c) s[c] = __fmaf_rn(-d2, r[c], s[c]);
+}
+
 // LocalRotation<N>::sample (dof/vector.hpp:70-122) in FP32.  The retry loop
 // is bounded; running out flags the chain and leaves the site unchanged.
 template <int N>
@@ -678,9 +688,9 @@ __global__ void __launch_bounds__(kBlock) wolff_flip(WolffArgs a)
                 float si[N];
 #pragma unroll
                 for (int c = 0; c < N; ++c) si[c] = f[c * a.n + i];
-                const float d = vdot<N>(si, r);
+                reflect<N>(si, r);
 #pragma unroll
-                for (int c = 0; c < N; ++c) f[c * a.n + i] = si[c] - 2.0f * d * r[c];
+                for (int c = 0; c < N; ++c) f[c * a.n + i] = si[c];
             }
         }
         a.lab_next[i] = i;

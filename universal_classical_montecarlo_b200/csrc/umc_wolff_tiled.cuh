@@ -211,9 +211,9 @@ __global__ void __launch_bounds__(kBlock) wolff_tile_flip(WolffTileArgs a)
             float si[N];
 #pragma unroll
             for (int c = 0; c < N; ++c) si[c] = f[c * a.n + k];
-            const float d = vdot<N>(si, r);
+            reflect<N>(si, r);
 #pragma unroll
-            for (int c = 0; c < N; ++c) f[c * a.n + k] = si[c] - 2.0f * d * r[c];
+            for (int c = 0; c < N; ++c) f[c * a.n + k] = si[c];
         }
     }
     block_sum<1>(cnt);
