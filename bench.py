@@ -242,12 +242,13 @@ class O3Hybrid:
         # (read own + neighbour class, write own; 12 B per FP32 3-vector);
         # Wolff: bond pass reads each site and its + neighbours once (12 B +
         # 4 B label write + 1 B crossing mask), flip reads label + spin (16 B)
-        # fused step (one launch): sweep 36 B + bond/label pass 17 B + merge 1 B
-        # + flip label read 4 B per site, and 24 B per cluster site
+        # fused step (one launch): sweep 36 B + bond/label pass 16 B (spins read
+        # once, label written) + flip label read 4 B per site, and 24 B per
+        # cluster site (the crossing-bond list is not counted)
         n = self.n
         c = getattr(self, "mean_cluster", 0.0)
         return {"metropolis": 36.0 * n / 2, "wolff_union": 17.0 * n, "wolff_flip": 4.0 * n + 24.0 * c,
-                "wolff_merge": 1.0 * n, "fused": 58.0 * n + 24.0 * c}.get(kind, 36.0 * n / 2)
+                "wolff_merge": 1.0 * n, "fused": 56.0 * n + 24.0 * c}.get(kind, 36.0 * n / 2)
 
     def e2e(self, torch, K):
         host = torch.empty((self.n, 3), dtype=torch.float32, pin_memory=True)
