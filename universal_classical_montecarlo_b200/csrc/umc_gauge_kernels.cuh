@@ -184,8 +184,33 @@ __device__ __forceinline__ void su_exp_i(const Mat<N>& x, Mat<N>& e)
             e.im[k] = sq * x.re[k];
         }
     } else if constexpr (N == 3) {
+        // X^2 of a Hermitian X is Hermitian: the diagonal is real and the
+        // lower triangle is the conjugate of the upper one
         Mat<3> x2;
-        mat_mul<3, false, false>(x, x, x2);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            float d = 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) d = fmaf(x.re[i * 3 + k], x.re[i * 3 + k], fmaf(x.im[i * 3 + k], x.im[i * 3 + k], d));
+            x2.re[i * 4] = d;
+            x2.im[i * 4] = 0.f;
+#pragma unroll
+            for (int j = i + 1; j < 3; ++j) {
+                // (X^2)_ij = sum_k x_ik conj(x_jk)
+                float sr = 0.f, si = 0.f;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float ar = x.re[i * 3 + k], ai = x.im[i * 3 + k];
+                    const float br = x.re[j * 3 + k], bi = x.im[j * 3 + k];
+                    sr = fmaf(ar, br, fmaf(ai, bi, sr));
+                    si = fmaf(ai, br, fmaf(-ar, bi, si));
+                }
+                x2.re[i * 3 + j] = sr;
+                x2.im[i * 3 + j] = si;
+                x2.re[j * 3 + i] = sr;
+                x2.im[j * 3 + i] = -si;
+            }
+        }
         const float c1 = 0.5f * (x2.re[0] + x2.re[4] + x2.re[8]);
         if (c1 < 1e-8f) {  // exp(iX) = I + iX - X^2/2 + O(|X|^3)
 #pragma unroll
@@ -195,11 +220,17 @@ __device__ __forceinline__ void su_exp_i(const Mat<N>& x, Mat<N>& e)
             }
             return;
         }
-        float tr3 = 0.f;  // tr(X X^2) = 3 det X
+        // tr(X X^2) = 3 det X; both Hermitian, so the sum over i != j is twice
+        // the real part over i < j
+        float off = 0.f, tr3 = 0.f;
 #pragma unroll
-        for (int i = 0; i < 3; ++i)
+        for (int i = 0; i < 3; ++i) {
+            tr3 = fmaf(x.re[i * 4], x2.re[i * 4], tr3);
 #pragma unroll
-            for (int j = 0; j < 3; ++j) tr3 += x.re[i * 3 + j] * x2.re[j * 3 + i] - x.im[i * 3 + j] * x2.im[j * 3 + i];
+            for (int j = i + 1; j < 3; ++j)
+                off = fmaf(x.re[i * 3 + j], x2.re[i * 3 + j], fmaf(x.im[i * 3 + j], x2.im[i * 3 + j], off));
+        }
+        tr3 = fmaf(2.f, off, tr3);
         const float c0 = tr3 * (1.f / 3.f);
         const bool neg = c0 < 0.f;
         // theta = acos(|c0| / c0_max), c0_max = 2 (c1 / 3)^(3/2)
@@ -209,13 +240,13 @@ __device__ __forceinline__ void su_exp_i(const Mat<N>& x, Mat<N>& e)
         sincosf(th * (1.f / 3.f), &s3, &c3);
         const float u = sqrtf(c1 * (1.f / 3.f)) * c3, w = sqrtf(c1) * s3;
         const float w2 = w * w, u2 = u * u;
-        const float xi = fabsf(w) < 0.05f ? 1.f - w2 * (1.f / 6.f) * (1.f - w2 * (1.f / 20.f) * (1.f - w2 * (1.f / 42.f)))
-                                          : sinf(w) / w;
-        float s2u, c2u, su, cu, sw, cw;
-        sincosf(2.f * u, &s2u, &c2u);
+        float su, cu, sw, cw;
         sincosf(u, &su, &cu);
         sincosf(w, &sw, &cw);
-        (void)sw;  // sin w enters through xi
+        // sin 2u, cos 2u by the double-angle formulas
+        const float s2u = 2.f * su * cu, c2u = fmaf(cu, cu, -su * su);
+        const float xi = fabsf(w) < 0.05f ? 1.f - w2 * (1.f / 6.f) * (1.f - w2 * (1.f / 20.f) * (1.f - w2 * (1.f / 42.f)))
+                                          : sw / w;
         // e^{-iu} = (cu, -su)
         auto emiu = [&](float ar, float ai, float& rr, float& ri) {  // e^{-iu} (ar + i ai)
             rr = cu * ar + su * ai;
@@ -359,8 +390,26 @@ struct GaugeArgs
     PassOut out;
 };
 
+// Key base of hit h of this sweep (the same for every link): the first
+// kHitKeys are computed once per block into shared memory.
+constexpr uint32_t kHitKeys = 32;
+
+__device__ __forceinline__ void hit_keys_init(uint64_t* keys, const GaugeArgs& a)
+{
+    for (uint32_t h = threadIdx.x; h < a.hits && h < kHitKeys; h += blockDim.x)
+        keys[h] = key_base(key_seed(a.seed, a.sweep, tag_site(h)));
+    __syncthreads();
+}
+
+__device__ __forceinline__ uint64_t hit_key(const uint64_t* keys, const GaugeArgs& a, uint32_t h)
+{
+    return h < kHitKeys ? keys[h] : key_base(key_seed(a.seed, a.sweep, tag_site(h)));
+}
+
 static __global__ void __launch_bounds__(kBlock) u1_pass(GaugeArgs a)
 {
+    __shared__ uint64_t keys[kHitKeys];
+    hit_keys_init(keys, a);
     double acc[kObs] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < a.count; q += gridDim.x * blockDim.x) {
         const uint32_t k = a.first + q;
@@ -386,7 +435,7 @@ static __global__ void __launch_bounds__(kBlock) u1_pass(GaugeArgs a)
         sincosf(th, &so, &co);
         uint32_t accepted = 0;
         for (uint32_t h = 0; h < a.hits; ++h) {
-            KeyedPcg g = KeyedPcg::open(key_base(key_seed(a.seed, a.sweep, tag_site(h))), k);
+            KeyedPcg g = KeyedPcg::open(hit_key(keys, a, h), k);
             const float p = u1_shift(g, a.width, th);
             float sp, cp;
             sincosf(p, &sp, &cp);
@@ -406,8 +455,10 @@ static __global__ void __launch_bounds__(kBlock) u1_pass(GaugeArgs a)
 }
 
 template <int N>
-__global__ void __launch_bounds__(kBlock) su_pass(GaugeArgs a)
+__global__ void __launch_bounds__(kBlock, 3) su_pass(GaugeArgs a)
 {
+    __shared__ uint64_t keys[kHitKeys];
+    hit_keys_init(keys, a);
     double acc[kObs] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < a.count; q += gridDim.x * blockDim.x) {
         const uint32_t k = a.first + q;
@@ -455,7 +506,7 @@ __global__ void __launch_bounds__(kBlock) su_pass(GaugeArgs a)
         uint32_t accepted = 0;
         const float coef = a.model_beta / float(N);
         for (uint32_t h = 0; h < a.hits; ++h) {
-            KeyedPcg g = KeyedPcg::open(key_base(key_seed(a.seed, a.sweep, tag_site(h))), k);
+            KeyedPcg g = KeyedPcg::open(hit_key(keys, a, h), k);
             su_shift<N>(g, a.width, U, V);
             const float tr_new = re_tr_mul<N>(V, A);
             const float dE = coef * (tr_old - tr_new);
