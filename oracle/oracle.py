@@ -426,6 +426,8 @@ class Reference:
         self._su_expm = L.fn("su_expm", None, _u32, _vp, _vp)
         self._su_shift = L.fn("su_shift", None, _u32, _f64, _u64, _u64, _u32, _u32, _vp, _vp)
         self._bench_o3 = L.fn("bench_o3", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
+        self._stock_o3 = L.fn("stock_o3_chain", _int, _u64, _f64, _u64, _u64, _u64, _vp)
+        self._stock_su3 = L.fn("stock_su3_chain", _int, _u64, _f64, _f64, _u64, _u32, _u64, _u64, _vp)
         self._bench_ising = L.fn("bench_ising", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._bench_xy = L.fn("bench_xy", _int, _u64, _f64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
 
@@ -579,6 +581,23 @@ class Reference:
         out = np.zeros((N, N), np.complex128)
         self._su_shift(N, width, seed, counter, tag, id_, _ptr(cur), _ptr(out))
         return out
+
+    def stock_o3_chain(self, L, beta, seed, warmup, steps):
+        """The reference's own O(3) L^3 chain (plain Pcg32; 1 Wolff flip + 1
+        sweep per step): per-step [E, Mx, My, Mz] after `warmup` steps."""
+        obs = np.zeros((steps, 4))
+        st = self._stock_o3(L, beta, seed, warmup, steps, _ptr(obs))
+        assert st == 0, st
+        return obs
+
+    def stock_su3_chain(self, L, beta, width, seed, chains, warmup, sweeps):
+        """The reference's own SU(3) L^4 chains (SUGauge<3>, SUShift, 1 hit,
+        plain Pcg32 seeded seed + c), one per thread: (chains, sweeps) mean
+        plaquettes after `warmup`."""
+        plaq = np.zeros((chains, sweeps))
+        st = self._stock_su3(L, beta, width, seed, chains, warmup, sweeps, _ptr(plaq))
+        assert st == 0, st
+        return plaq
 
     def bench_o3(self, L, beta, warmup, steps, threads, seed=1):
         """Reference stock path, O(3) L^3 (1 Wolff flip + 1 sweep per step):

@@ -840,6 +840,76 @@ extern "C" int ref_bench_o3(std::uint64_t L, double beta, std::uint64_t warmup, 
     }
 }
 
+// The reference's stock O(3) chain as a user would run it (same set-up as
+// ref_bench_o3, one chain): per step one Wolff flip then one Metropolis sweep,
+// plain Pcg32 streams; after `warmup` steps it records [E, Mx, My, Mz] of every
+// step into obs (steps x 4).  The statistical check against the GPU chain.
+extern "C" int ref_stock_o3_chain(std::uint64_t L, double beta, std::uint64_t seed, std::uint64_t warmup,
+                                  std::uint64_t steps, double* obs)
+{
+    try {
+        std::vector<PairGraph<>::Edge> edges;
+        edges.reserve(3 * L * L * L);
+        for (std::uint64_t z = 0; z < L; ++z)
+            for (std::uint64_t y = 0; y < L; ++y)
+                for (std::uint64_t x = 0; x < L; ++x) {
+                    const auto i = static_cast<std::uint32_t>((z * L + y) * L + x);
+                    edges.push_back({i, static_cast<std::uint32_t>((z * L + y) * L + (x + 1) % L), {}});
+                    edges.push_back({i, static_cast<std::uint32_t>((z * L + (y + 1) % L) * L + x), {}});
+                    edges.push_back({i, static_cast<std::uint32_t>((((z + 1) % L) * L + y) * L + x), {}});
+                }
+        const std::size_t n = L * L * L;
+        VectorSpin<3> model(PairGraph<>(n, edges), 1.0);
+        Pcg32 init(seed, 7);
+        double v[3];
+        for (std::size_t i = 0; i < n; ++i) {
+            UniformSphereN<3>{}.sample(nullptr, init, v);
+            model.update(i, v);
+        }
+        Metropolis<VectorSpin<3>, UniformSphereN<3>, Pcg32> mc(model, UniformSphereN<3>{}, Pcg32(seed, 1), beta);
+        Wolff<VectorSpin<3>, UniformSphereN<3>, Pcg32> w(model, UniformSphereN<3>{}, Pcg32(seed, 2), beta);
+        for (std::uint64_t s = 0; s < warmup + steps; ++s) {
+            (void)w.flip();
+            mc.sweep();
+            if (s >= warmup) vector_obs<3>(model, obs + (s - warmup) * 4);
+        }
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+// The reference's stock SU(3) chains: example/sun_gauge.hpp's SUGauge<3> on
+// hypercubic_plaquettes(L) (cold start, model beta), Metropolis with
+// SUShift<3>{width}, one hit per link, driver beta 1 and a plain Pcg32 (seed +
+// c for chain c), one chain per thread; after `warmup` sweeps each records the
+// mean plaquette of every sweep into plaq[c * sweeps + k].
+extern "C" int ref_stock_su3_chain(std::uint64_t L, double beta, double width, std::uint64_t seed,
+                                   std::uint32_t chains, std::uint64_t warmup, std::uint64_t sweeps, double* plaq)
+{
+    try {
+        std::vector<std::thread> pool;
+        std::atomic<int> failed{0};
+        for (std::uint32_t c = 0; c < chains; ++c)
+            pool.emplace_back([&, c] {
+                try {
+                    SUGauge<3> model(L, beta);
+                    Metropolis<SUGauge<3>, SUShift<3>, Pcg32> mc(model, SUShift<3>{width}, Pcg32(seed + c, 1), 1.0);
+                    mc.run(warmup);
+                    double* out = plaq + std::uint64_t(c) * sweeps;
+                    std::uint64_t k = 0;
+                    mc.sample(sweeps, [&](const SUGauge<3>& m) { out[k++] = m.mean_plaquette(); });
+                } catch (...) {
+                    failed = 1;
+                }
+            });
+        for (auto& th : pool) th.join();
+        return failed ? -1 : 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
 // Times the reference's stock Ising Metropolis on an L x L square_lattice
 // (example/ising.hpp + Flip + Pcg32), one chain per thread, cold start.
 extern "C" int ref_bench_ising(std::uint64_t L, double beta, std::uint64_t warmup, std::uint64_t sweeps,

@@ -1,0 +1,93 @@
+"""Statistical parity with the reference's own chains.
+
+The reference runs here as its users run it: the stock driver (driver.hpp),
+example/vector_spin.hpp or example/sun_gauge.hpp, a plain sequential Pcg32 and
+FP64 state (oracle/_ref, ref_stock_*_chain).  The GPU chains use keyed streams,
+colour passes and FP32 state, so trajectories differ; the distributions must
+not.  Each observable is compared as z = |a - b| / sqrt(ea^2 + eb^2) with
+binned standard errors on both sides, at fixed seeds (the outcome is
+deterministic).
+
+- O(3) 8^3, beta = 0.693, one Wolff flip + one sweep per step: E per site,
+  |m| and chi = n (<m^2> - <|m|>^2);
+- SU(3) 4^4, beta = 5.7, SUShift 0.2: mean plaquette (10 hits per link on the
+  GPU, the reference's single hit: the same equilibrium distribution).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+Z_MAX = 3.0
+
+
+def _mean_err(umc, x, n_bins=40):
+    x = np.asarray(x, np.float64)
+    return umc.binning_error(x, max(1, x.size // n_bins))
+
+
+def _chi_err(m, n, n_bins=40):
+    """chi = n (<m^2> - <m>^2) of the series m, jackknife error over bins."""
+    m = np.asarray(m, np.float64)
+    b = m.size // n_bins
+    m = m[: b * n_bins].reshape(n_bins, b)
+    s1, s2 = m.sum(axis=1), (m * m).sum(axis=1)
+    tot = m.size
+
+    def chi(a1, a2, cnt):
+        return n * (a2 / cnt - (a1 / cnt) ** 2)
+
+    full = chi(s1.sum(), s2.sum(), tot)
+    jk = np.array([chi(s1.sum() - s1[i], s2.sum() - s2[i], tot - b) for i in range(n_bins)])
+    err = np.sqrt((n_bins - 1) / n_bins * ((jk - jk.mean()) ** 2).sum())
+    return full, err
+
+
+def _z(a, ea, b, eb):
+    return abs(a - b) / np.sqrt(ea * ea + eb * eb)
+
+
+def test_o3_hybrid_chain_matches_reference_chain(umc, ref):
+    L, beta, n = 8, 0.693, 512
+    warm, steps = 1000, 20000
+    ch = umc.Chain(umc.MODEL_VECTOR, graph=umc.cubic_lattice(L, L, L), components=3, coupling=1.0,
+                   proposal=umc.PROPOSAL_SPHERE, wolff_axis=umc.AXIS_SPHERE, seed=31)
+    ch.randomize(5)
+    ch.hybrid(beta, warm)
+    _, rec = ch.hybrid(beta, steps)
+    g_e = rec[:, 0] / n
+    g_m = np.linalg.norm(rec[:, 1:4], axis=1) / n
+    obs = ref.stock_o3_chain(L, beta, 5, warm, steps)
+    r_e = obs[:, 0] / n
+    r_m = np.linalg.norm(obs[:, 1:4], axis=1) / n
+
+    zs = {}
+    for name, a, b in (("E/site", g_e, r_e), ("|m|", g_m, r_m)):
+        (ma, ea), (mb, eb) = _mean_err(umc, a), _mean_err(umc, b)
+        zs[name] = (_z(ma, ea, mb, eb), ma, mb)
+    (ca, eca), (cb, ecb) = _chi_err(g_m, n), _chi_err(r_m, n)
+    zs["chi"] = (_z(ca, eca, cb, ecb), ca, cb)
+    print("O(3) 8^3 z, gpu, reference:", zs)
+    for name, (z, a, b) in zs.items():
+        assert z < Z_MAX, (name, z, a, b)
+
+
+def test_su3_chain_matches_reference_chain(umc, ref):
+    """The plaquette of 1-hit Metropolis decorrelates slowly here (tau_int of
+    about 100 sweeps), so the reference side is 16 independent chains, one per
+    thread, and its error the scatter of their means; the GPU side is one long
+    10-hit chain (tau_int about 14) with the Sokal-window error.  A warm-up of
+    500 sweeps from the cold start still left the reference chains about
+    0.003 high."""
+    L, beta, width = 4, 5.7, 0.2
+    ch = umc.Chain(umc.MODEL_SU, cells=umc.hypercubic_plaquettes(L), components=3, coupling=beta,
+                   proposal=umc.PROPOSAL_SUSHIFT, width=width, hits=10, seed=17)
+    ch.metropolis(1.0, 500)
+    g_p = ch.metropolis(1.0, 20000)[:, 1]
+    tau = umc.tau_int(g_p)[0]
+    ma, ea = g_p.mean(), g_p.std() * np.sqrt(2 * tau / g_p.size)
+    # cold starts: 3000 sweeps (some 25 tau) before recording
+    r = ref.stock_su3_chain(L, beta, width, 5, 16, 3000, 1500).mean(axis=1)
+    mb, eb = r.mean(), r.std(ddof=1) / np.sqrt(r.size)
+    print("SU(3) 4^4 plaquette z, gpu, reference:", _z(ma, ea, mb, eb), (ma, ea), (mb, eb))
+    assert _z(ma, ea, mb, eb) < Z_MAX, (ma, ea, mb, eb)
