@@ -634,11 +634,8 @@ void spin_flip(umc_chain* c, double beta, double* rec, unsigned long long* size_
     c->flips++;
 }
 
-void check_status(umc_chain* c)
+void raise_status(umc_chain* c, unsigned int st)
 {
-    unsigned int st = 0;
-    cuda_check(cudaMemcpyAsync(&st, &c->ctl.as<DevCtl>()->status, sizeof st, cudaMemcpyDeviceToHost, c->stream), "read status");
-    cuda_check(cudaStreamSynchronize(c->stream), "synchronise chain");
     if (st) {
         // tickets and the barrier may be mid-count after an aborted kernel
         cuda_check(cudaMemset(c->ctl.p, 0, sizeof(DevCtl)), "clear control block");
@@ -651,9 +648,40 @@ void check_status(umc_chain* c)
     }
 }
 
+void check_status(umc_chain* c)
+{
+    unsigned int st = 0;
+    cuda_check(cudaMemcpyAsync(&st, &c->ctl.as<DevCtl>()->status, sizeof st, cudaMemcpyDeviceToHost, c->stream), "read status");
+    cuda_check(cudaStreamSynchronize(c->stream), "synchronise chain");
+    raise_status(c, st);
+}
+
+// Status word, pending records and cluster sizes in one round trip: async
+// copies into the chain's pinned stage, one synchronisation, then host copies.
 void fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t capacity, uint64_t* n_out)
 {
-    check_status(c);
+    const uint64_t pend = c->rec_overflow ? 0 : c->rec_pending;
+    const size_t need = 16 + size_t(c->max_records) * (kObs * sizeof(double) + sizeof(unsigned long long));
+    if (c->host_stage_bytes < need) {
+        if (c->host_stage) cudaFreeHost(c->host_stage);
+        c->host_stage = nullptr;
+        c->host_stage_bytes = 0;
+        cuda_check(cudaHostAlloc(&c->host_stage, need, cudaHostAllocDefault), "pinned record stage");
+        c->host_stage_bytes = need;
+    }
+    uint8_t* stage = static_cast<uint8_t*>(c->host_stage);
+    unsigned int* st = reinterpret_cast<unsigned int*>(stage);
+    double* rec = reinterpret_cast<double*>(stage + 16);
+    unsigned long long* sz = reinterpret_cast<unsigned long long*>(stage + 16 + size_t(c->max_records) * kObs * sizeof(double));
+    cuda_check(cudaMemcpyAsync(st, &c->ctl.as<DevCtl>()->status, sizeof *st, cudaMemcpyDeviceToHost, c->stream), "read status");
+    if (pend) {
+        cuda_check(cudaMemcpyAsync(rec, c->records.p, pend * kObs * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+                   "fetch records");
+        cuda_check(cudaMemcpyAsync(sz, c->sizes.p, pend * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream),
+                   "fetch sizes");
+    }
+    cuda_check(cudaStreamSynchronize(c->stream), "synchronise chain");
+    raise_status(c, *st);
     if (c->rec_overflow) {
         c->rec_overflow = false;
         c->rec_pending = 0;
@@ -661,12 +689,9 @@ void fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t capacity, ui
     }
     const uint64_t n = c->rec_pending;
     if ((records || sizes) && n > capacity) throw Error(UMC_ERR_INVALID_ARGUMENT, "record buffer too small");
-    if (records && n)
-        cuda_check(cudaMemcpy(records, c->records.p, n * kObs * sizeof(double), cudaMemcpyDeviceToHost), "fetch records");
-    std::vector<unsigned long long> s(n);
-    if (n) cuda_check(cudaMemcpy(s.data(), c->sizes.p, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "fetch sizes");
+    if (records && n) std::memcpy(records, rec, n * kObs * sizeof(double));
     if (sizes)
-        for (uint64_t k = 0; k < n; ++k) sizes[k] = s[k];
+        for (uint64_t k = 0; k < n; ++k) sizes[k] = sz[k];
     if (n_out) *n_out = n;
     c->rec_pending = 0;
 }
@@ -820,6 +845,9 @@ void destroy_chain(umc_chain* c)
         cudaEventDestroy(t.b);
     }
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+    if (c->upload_done) cudaEventDestroy(c->upload_done);
+    if (c->host_stage) cudaFreeHost(c->host_stage);
+    c->host_stage = nullptr;
     for (DevBuf* b : {&c->field, &c->staging, &c->off, &c->adj, &c->slot, &c->position, &c->lab0, &c->lab1, &c->xlist, &c->cells,
                       &c->inc_off, &c->inc_cell, &c->inc_which, &c->partials, &c->ctl, &c->records, &c->sizes, &c->tm1})
         b->free_();
@@ -994,7 +1022,9 @@ int umc_chain_set_field(umc_chain* c, const void* host_field)
             return;
         }
         if (!c->staging.p) c->staging.alloc(c->field_bytes, "staging");
+        if (!c->upload_done) cuda_check(cudaEventCreateWithFlags(&c->upload_done, cudaEventDisableTiming), "upload event");
         cuda_check(cudaMemcpyAsync(c->staging.p, host_field, c->field_bytes, cudaMemcpyHostToDevice, c->stream), "upload field");
+        cuda_check(cudaEventRecord(c->upload_done, c->stream), "upload field");
         const uint32_t g = grid_for(c, c->n);
         LaunchScope ls(c, UMC_KERNEL_OTHER);
         if (c->elem_bytes == 1)
@@ -1002,7 +1032,9 @@ int umc_chain_set_field(umc_chain* c, const void* host_field)
         else
             scatter_field<float><<<g, kBlock, 0, c->stream>>>(c->staging.as<float>(), c->field.as<float>(), uint32_t(c->n), c->comps, placement(c));
         launch_check("scatter field");
-        cuda_check(cudaStreamSynchronize(c->stream), "upload field");
+        // the caller's buffer is free once the copy has landed; the scatter
+        // is stream-ordered before any later work on the chain
+        cuda_check(cudaEventSynchronize(c->upload_done), "upload field");
     });
 }
 

@@ -76,6 +76,11 @@ struct umc_chain
     uint32_t max_grid = 0;
 
     uint64_t max_records = 4096;
+    // pinned host image of [status | records | sizes]: a fetch is one round
+    // trip (three async copies, one stream synchronisation)
+    void* host_stage = nullptr;
+    size_t host_stage_bytes = 0;
+    cudaEvent_t upload_done = nullptr;  // set_field waits on the copy, not the scatter
     uint64_t rec_pending = 0;
     bool rec_overflow = false;
     uint64_t sweeps = 0, flips = 0;
