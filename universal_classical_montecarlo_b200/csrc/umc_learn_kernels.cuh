@@ -587,13 +587,35 @@ __device__ __forceinline__ bool learned_update(const U1BatchArgs& a, float* th, 
         so_ += expf(lo[kk] - mo);
         sn_ += expf(ln[kk] - mn);
     }
-    const double lr = (double(mo) - double(mn)) + log(double(so_) / double(sn_));
-    const double log_p = -double(a.driver_beta) * double(dE) + lr;
-    if (log_p >= 0.0 || log(u_f64(r.next())) < log_p) {
-        th[k] = p;
-        return true;
+    // MH test: log_p = -beta dE + log q(old|new) - log q(new|old) in FP64, accept
+    // iff log_p >= 0 or log u < log_p (driver.hpp:36-41).  The same comparisons
+    // are made first in FP32 with error bounds far above FP32 round-off (2^-18
+    // of the terms' magnitude for log_p, 2^-17 of |log u| + 1 for log u); only
+    // a decision inside those bounds evaluates the FP64 expressions, so every
+    // decision is the FP64 one.
+    const float bdE = a.driver_beta * dE;
+    const float lp = (-bdE + (mo - mn)) + (logf(so_) - logf(sn_));
+    const float ep = ldexpf(4.0f + fabsf(mo) + fabsf(mn) + fabsf(bdE), -18);
+    auto log_p64 = [&] {
+        const double lr = (double(mo) - double(mn)) + log(double(so_) / double(sn_));
+        return -double(a.driver_beta) * double(dE) + lr;
+    };
+    bool accept;
+    if (lp >= ep) {
+        accept = true;
+    } else if (lp <= -ep) {
+        const uint32_t kd = r.next();
+        const float lu = logf(u_f32(kd));
+        const float eu = ldexpf(1.0f + fabsf(lu), -17);
+        if (lu + eu < lp - ep) accept = true;
+        else if (lu - eu > lp + ep) accept = false;
+        else accept = log(u_f64(kd)) < log_p64();
+    } else {
+        const double lp64 = log_p64();
+        accept = lp64 >= 0.0 || log(u_f64(r.next())) < lp64;
     }
-    return false;
+    if (accept) th[k] = p;
+    return accept;
 }
 
 // Plain U1Shift Metropolis, one CTA per chain at a time, chain in shared memory.
