@@ -522,8 +522,12 @@ def learned_study(umc, torch, betas=LEARN_BETAS, L=64, chains=444, n_configs=200
     out = {}
     for beta in betas:
         t_start = time.perf_counter()
+        # cold start (all angles 0), as the reference's U1Gauge constructs its
+        # links (example/u1_gauge.hpp:23-25).  A hot start leaves each chain
+        # with a topological charge of order sqrt(V / 12) that local updates
+        # cannot shed at beta >= 6; the excess action then biases the
+        # plaquette low by several standard errors.
         plain = umc.U1Batch(chains, L, beta, width=0.5, seed=seed, max_records=max(meas, 200))
-        plain.randomize(seed + 100)
         plain.run(therm, records=False)
         snaps = -(-n_configs // chains)
         net = umc.ProposalNet(seed + 7, max_configs=snaps * chains, L=L)
