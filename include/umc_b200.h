@@ -164,6 +164,19 @@ int umc_chain_destroy(umc_chain* c);
 int umc_chain_set_field(umc_chain* c, const void* host_field);
 /* Reads the field back in the same layout (the reference's data()). */
 int umc_chain_get_field(umc_chain* c, void* host_field);
+/* Asynchronous umc_chain_set_field (spin models): the copy runs on a second
+ * stream into one of two staging buffers and the layout pass follows on the
+ * chain's stream, so the upload of the next configuration overlaps the work
+ * queued before it.  Returns at once; host_field (pinned memory, for the copy
+ * to be asynchronous) must stay unchanged until the next synchronising call
+ * (umc_chain_sync, _fetch, _get_field, a *_run).  The reference sets a field
+ * only through its model's update(i, .) (model.hpp:70-86). */
+int umc_chain_upload_async(umc_chain* c, const void* host_field);
+/* With streaming on, every record (and cluster size) is copied to pinned host
+ * memory as soon as its step has run, on the chain's stream; umc_chain_fetch
+ * then only waits.  This is how the reference's sample(n, observe) sees each
+ * sweep's observables as it ends (driver.hpp:54-61, :182-190). */
+int umc_chain_set_record_streaming(umc_chain* c, int enable);
 /* Random start from keyed draws (tag 3, id = site): uniform on the sphere,
  * uniform angles in [0, 2pi), Haar-random SU(N), random Ising signs. */
 int umc_chain_randomize(umc_chain* c, uint64_t seed);

@@ -144,6 +144,8 @@ _decl("umc_chain_create", _int, C.POINTER(ChainDesc), C.POINTER(_vp))
 _decl("umc_chain_destroy", _int, _vp)
 _decl("umc_chain_set_field", _int, _vp, _vp)
 _decl("umc_chain_get_field", _int, _vp, _vp)
+_decl("umc_chain_upload_async", _int, _vp, _vp)
+_decl("umc_chain_set_record_streaming", _int, _vp, _int)
 _decl("umc_chain_randomize", _int, _vp, _u64)
 _decl("umc_chain_set_proposal", _int, _vp, _i32, _f64, _u32)
 _decl("umc_chain_set_wolff_axis", _int, _vp, _i32)
@@ -431,12 +433,14 @@ class Chain:
         else:
             self.dtype, self.comps = np.float32, components * components * 2
         self.n = graph.sites() if graph is not None else cells.sites()
+        self._inflight = []  # host arrays of uploads that may still be copying
 
     def close(self):
         h = getattr(self, "_h", None)
         if h and lib is not None:  # module globals are gone at interpreter exit
             lib.umc_chain_destroy(h)
         self._h = None
+        self._inflight = []
 
     def __del__(self):
         self.close()
@@ -451,7 +455,23 @@ class Chain:
             raise ValueError(f"field has {a.size} scalars, expected {self.n * self.comps}")
         check(lib.umc_chain_set_field(self._h, _ptr(a)))
 
+    def upload_async(self, field) -> None:
+        """umc_chain_upload_async: the array is kept alive until the next
+        synchronising call; pinned memory (torch pin_memory) makes the copy
+        asynchronous."""
+        a = np.asarray(field)
+        if a.dtype != self.dtype or not a.flags.c_contiguous:
+            raise ValueError(f"upload_async needs a C-contiguous {np.dtype(self.dtype).name} array")
+        if a.size != self.n * self.comps:
+            raise ValueError(f"field has {a.size} scalars, expected {self.n * self.comps}")
+        check(lib.umc_chain_upload_async(self._h, _ptr(a)))
+        self._inflight.append(a)
+
+    def set_record_streaming(self, enable: bool) -> None:
+        check(lib.umc_chain_set_record_streaming(self._h, int(enable)))
+
     def get_field(self) -> np.ndarray:
+        self._inflight = []
         a = np.zeros(self.n * self.comps, self.dtype)
         check(lib.umc_chain_get_field(self._h, _ptr(a)))
         return a.reshape(self.n, self.comps) if self.comps > 1 else a
@@ -481,6 +501,7 @@ class Chain:
 
     def sync(self) -> None:
         check(lib.umc_chain_sync(self._h))
+        self._inflight = []
 
     def observe(self) -> np.ndarray:
         r = np.zeros(OBS_STRIDE)
@@ -518,6 +539,7 @@ class Chain:
         sizes = np.zeros(capacity, np.uint64)
         got = _u64(0)
         check(lib.umc_chain_fetch(self._h, _ptr(rec), _ptr(sizes), capacity, C.byref(got)))
+        self._inflight = []
         return rec[: got.value], sizes[: got.value]
 
     def set_fused(self, enable: bool) -> None:

@@ -656,28 +656,63 @@ void check_status(umc_chain* c)
     raise_status(c, st);
 }
 
-// Status word, pending records and cluster sizes in one round trip: async
-// copies into the chain's pinned stage, one synchronisation, then host copies.
-void fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t capacity, uint64_t* n_out)
+// The chain's pinned host image [status | records | sizes].
+struct Stage
 {
-    const uint64_t pend = c->rec_overflow ? 0 : c->rec_pending;
+    unsigned int* status;
+    double* rec;
+    unsigned long long* sz;
+};
+
+Stage host_stage(umc_chain* c)
+{
     const size_t need = 16 + size_t(c->max_records) * (kObs * sizeof(double) + sizeof(unsigned long long));
     if (c->host_stage_bytes < need) {
+        cuda_check(cudaStreamSynchronize(c->stream), "synchronise chain");
         if (c->host_stage) cudaFreeHost(c->host_stage);
         c->host_stage = nullptr;
         c->host_stage_bytes = 0;
+        c->streamed = 0;
         cuda_check(cudaHostAlloc(&c->host_stage, need, cudaHostAllocDefault), "pinned record stage");
         c->host_stage_bytes = need;
     }
     uint8_t* stage = static_cast<uint8_t*>(c->host_stage);
-    unsigned int* st = reinterpret_cast<unsigned int*>(stage);
-    double* rec = reinterpret_cast<double*>(stage + 16);
-    unsigned long long* sz = reinterpret_cast<unsigned long long*>(stage + 16 + size_t(c->max_records) * kObs * sizeof(double));
+    return {reinterpret_cast<unsigned int*>(stage), reinterpret_cast<double*>(stage + 16),
+            reinterpret_cast<unsigned long long*>(stage + 16 + size_t(c->max_records) * kObs * sizeof(double))};
+}
+
+// After the unit that writes ring slot r has been enqueued: with record
+// streaming on, its record and size go to the pinned stage right behind it.
+void record_done(umc_chain* c, uint64_t r)
+{
+    if (!c->stream_records || c->rec_overflow || r != c->streamed) return;
+    const Stage h = host_stage(c);
+    cuda_check(cudaMemcpyAsync(h.rec + r * kObs, c->records.as<double>() + r * kObs, kObs * sizeof(double),
+                               cudaMemcpyDeviceToHost, c->stream), "stream record");
+    cuda_check(cudaMemcpyAsync(h.sz + r, c->sizes.as<unsigned long long>() + r, sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, c->stream), "stream record");
+    c->streamed = r + 1;
+}
+
+// Status word, pending records and cluster sizes in one round trip: async
+// copies into the chain's pinned stage (only the records not streamed there
+// already), one synchronisation, then host copies.
+void fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t capacity, uint64_t* n_out)
+{
+    const uint64_t pend = c->rec_overflow ? 0 : c->rec_pending;
+    const Stage h = host_stage(c);
+    unsigned int* st = h.status;
+    double* rec = h.rec;
+    unsigned long long* sz = h.sz;
+    const uint64_t from = std::min(c->streamed, pend);
+    c->streamed = 0;
     cuda_check(cudaMemcpyAsync(st, &c->ctl.as<DevCtl>()->status, sizeof *st, cudaMemcpyDeviceToHost, c->stream), "read status");
-    if (pend) {
-        cuda_check(cudaMemcpyAsync(rec, c->records.p, pend * kObs * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+    if (pend > from) {
+        cuda_check(cudaMemcpyAsync(rec + from * kObs, c->records.as<double>() + from * kObs,
+                                   (pend - from) * kObs * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
                    "fetch records");
-        cuda_check(cudaMemcpyAsync(sz, c->sizes.p, pend * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream),
+        cuda_check(cudaMemcpyAsync(sz + from, c->sizes.as<unsigned long long>() + from,
+                                   (pend - from) * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream),
                    "fetch sizes");
     }
     cuda_check(cudaStreamSynchronize(c->stream), "synchronise chain");
@@ -846,6 +881,15 @@ void destroy_chain(umc_chain* c)
     }
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
     if (c->upload_done) cudaEventDestroy(c->upload_done);
+    for (int q = 0; q < 2; ++q) {
+        if (c->up_copied[q]) cudaEventDestroy(c->up_copied[q]);
+        if (c->up_consumed[q]) cudaEventDestroy(c->up_consumed[q]);
+        c->up_staging[q].free_();
+    }
+    if (c->up_stream) {
+        cudaStreamSynchronize(c->up_stream);
+        cudaStreamDestroy(c->up_stream);
+    }
     if (c->host_stage) cudaFreeHost(c->host_stage);
     c->host_stage = nullptr;
     for (DevBuf* b : {&c->field, &c->staging, &c->off, &c->adj, &c->slot, &c->position, &c->lab0, &c->lab1, &c->xlist, &c->cells,
@@ -885,6 +929,7 @@ void enqueue_sweeps(umc_chain* c, double beta, uint64_t n)
         const uint64_t r = next_record(c);
         if (is_spin(c)) spin_sweep(c, beta, record_ptr(c, r));
         else gauge_sweep(c, beta, record_ptr(c, r));
+        record_done(c, r);
     }
 }
 
@@ -895,6 +940,7 @@ void enqueue_flips(umc_chain* c, double beta, uint64_t n, bool obs)
     for (uint64_t k = 0; k < n; ++k) {
         const uint64_t r = next_record(c);
         spin_flip(c, beta, obs ? record_ptr(c, r) : nullptr, size_ptr(c, r));
+        record_done(c, r);
     }
 }
 
@@ -904,9 +950,11 @@ void enqueue_hybrid(umc_chain* c, double beta, uint64_t n)
     if (!is_spin(c)) throw Error(UMC_ERR_UNSUPPORTED, "Wolff is defined for spin models only (driver.hpp:73-84)");
     for (uint64_t k = 0; k < n; ++k) {
         const uint64_t r = next_record(c);
-        if (fused_step(c, beta, true, true, record_ptr(c, r), size_ptr(c, r))) continue;
-        spin_flip(c, beta, nullptr, size_ptr(c, r));
-        spin_sweep(c, beta, record_ptr(c, r));
+        if (!fused_step(c, beta, true, true, record_ptr(c, r), size_ptr(c, r))) {
+            spin_flip(c, beta, nullptr, size_ptr(c, r));
+            spin_sweep(c, beta, record_ptr(c, r));
+        }
+        record_done(c, r);
     }
 }
 
@@ -1035,6 +1083,55 @@ int umc_chain_set_field(umc_chain* c, const void* host_field)
         // the caller's buffer is free once the copy has landed; the scatter
         // is stream-ordered before any later work on the chain
         cuda_check(cudaEventSynchronize(c->upload_done), "upload field");
+    });
+}
+
+int umc_chain_upload_async(umc_chain* c, const void* host_field)
+{
+    return guarded([&] {
+        if (!c || !host_field) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (!is_spin(c)) throw Error(UMC_ERR_UNSUPPORTED, "asynchronous upload is provided for spin models");
+        device_scope(c);
+        if (!c->up_stream) {
+            cuda_check(cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking), "upload stream");
+            for (int q = 0; q < 2; ++q) {
+                cuda_check(cudaEventCreateWithFlags(&c->up_copied[q], cudaEventDisableTiming), "upload event");
+                cuda_check(cudaEventCreateWithFlags(&c->up_consumed[q], cudaEventDisableTiming), "upload event");
+                c->up_staging[q].alloc(c->field_bytes, "upload staging");
+                cuda_check(cudaEventRecord(c->up_consumed[q], c->stream), "upload event");
+            }
+        }
+        const int q = c->up_next;
+        c->up_next ^= 1;
+        // the copy into buffer q waits until the layout pass that last read it has run
+        cuda_check(cudaStreamWaitEvent(c->up_stream, c->up_consumed[q], 0), "upload order");
+        cuda_check(cudaMemcpyAsync(c->up_staging[q].p, host_field, c->field_bytes, cudaMemcpyHostToDevice, c->up_stream),
+                   "upload field");
+        cuda_check(cudaEventRecord(c->up_copied[q], c->up_stream), "upload event");
+        cuda_check(cudaStreamWaitEvent(c->stream, c->up_copied[q], 0), "upload order");
+        const uint32_t g = grid_for(c, c->n);
+        {
+            LaunchScope ls(c, UMC_KERNEL_OTHER);
+            if (c->elem_bytes == 1)
+                scatter_field<int8_t><<<g, kBlock, 0, c->stream>>>(c->up_staging[q].as<int8_t>(), c->field.as<int8_t>(),
+                                                                   uint32_t(c->n), 1, placement(c));
+            else
+                scatter_field<float><<<g, kBlock, 0, c->stream>>>(c->up_staging[q].as<float>(), c->field.as<float>(),
+                                                                  uint32_t(c->n), c->comps, placement(c));
+            launch_check("scatter field");
+        }
+        cuda_check(cudaEventRecord(c->up_consumed[q], c->stream), "upload event");
+    });
+}
+
+int umc_chain_set_record_streaming(umc_chain* c, int enable)
+{
+    return guarded([&] {
+        if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
+        device_scope(c);
+        if (c->rec_pending) throw Error(UMC_ERR_STATE, "fetch pending records before switching record streaming");
+        c->stream_records = enable != 0;
+        c->streamed = 0;
     });
 }
 

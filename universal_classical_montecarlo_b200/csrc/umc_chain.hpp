@@ -81,6 +81,13 @@ struct umc_chain
     void* host_stage = nullptr;
     size_t host_stage_bytes = 0;
     cudaEvent_t upload_done = nullptr;  // set_field waits on the copy, not the scatter
+    bool stream_records = false;        // copy each record to host_stage as it is written
+    uint64_t streamed = 0;              // records [0, streamed) already in host_stage
+    // umc_chain_upload_async: copy stream, two staging buffers and their events
+    cudaStream_t up_stream = nullptr;
+    umc::DevBuf up_staging[2];
+    cudaEvent_t up_copied[2] = {nullptr, nullptr}, up_consumed[2] = {nullptr, nullptr};
+    int up_next = 0;
     uint64_t rec_pending = 0;
     bool rec_overflow = false;
     uint64_t sweeps = 0, flips = 0;
