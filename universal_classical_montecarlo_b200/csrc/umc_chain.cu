@@ -337,6 +337,10 @@ void spin_sweep(umc_chain* c, double beta, double* rec)
             a.T3 = tm[3];
             a.T4 = tm[4];
             a.J = c->J_int;
+            for (int b = 0; b < 4; ++b) {
+                a.m1[b] = 2u << (8 * b);
+                a.m2[b] = 0u - (4u << (8 * b));
+            }
             a.out = o;
             const uint32_t g = grid_for(c, c->n / 2 / 16);
             LaunchScope ls(c, UMC_KERNEL_METROPOLIS);

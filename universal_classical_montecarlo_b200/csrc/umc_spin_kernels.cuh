@@ -182,6 +182,10 @@ struct IsingFastArgs
     uint64_t kbase;
     uint32_t T3, T4;  // accept iff draw <= T for dE = 4J, 8J (T4 <= T3)
     int32_t J;
+    // 2^(8b+1) and -2^(8b+2) for byte b: kernel parameters rather than
+    // literals, so that the per-site accumulation stays three integer
+    // multiply-adds on the FMA pipe instead of shifts and adds on the ALU
+    uint32_t m1[4], m2[4];
     PassOut out;
 };
 
@@ -191,6 +195,18 @@ __device__ __forceinline__ uint32_t pcg_output_split(uint32_t lo, uint32_t hi)
 {
     const uint32_t xs = __funnelshift_r(lo, hi, 27) ^ __umulhi(hi, 1u << 19);
     return __funnelshift_r(xs, xs, __umulhi(hi, 32u));
+}
+
+// One Pcg32 step (rng.hpp:34, increment 1) on the state's 32-bit halves:
+// lo * A_lo + 1 as one wide multiply-add (the +1 rides in its addend), then
+// the high word from two multiply-adds and that product's carry word.
+__device__ __forceinline__ void pcg_step_split(uint32_t& lo, uint32_t& hi)
+{
+    constexpr uint32_t aL = uint32_t(kPcgMult), aH = uint32_t(kPcgMult >> 32);
+    uint64_t w;
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(w) : "r"(lo), "r"(aL), "l"(1ull));
+    hi = hi * aL + lo * aH + uint32_t(w >> 32);
+    lo = uint32_t(w);
 }
 
 // hi32(a * b + c) with one wide multiply-add.
@@ -227,7 +243,8 @@ __global__ void __launch_bounds__(kBlock) ising_fast_pass(IsingFastArgs a)
         const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
         const uint32_t uw[4] = {u4.x, u4.y, u4.z, u4.w};
         const uint32_t dw[4] = {d4.x, d4.y, d4.z, d4.w};
-        uint64_t st = first_state(id_seed(a.kbase, gbase + v));
+        const uint64_t st0 = first_state(id_seed(a.kbase, gbase + v));
+        uint32_t slo = uint32_t(st0), shi = uint32_t(st0 >> 32);
         uint32_t out[4], acc_f = 0, acc_dn = 0, acc_e = 0;
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
@@ -236,16 +253,19 @@ __global__ void __launch_bounds__(kBlock) ising_fast_pass(IsingFastArgs a)
             const uint32_t s = sw[w];
             // twice the number of neighbours whose spin differs from the site's
             const uint32_t A2 = ((mw[w] ^ s) & M2) + ((h2 ^ s) & M2) + ((uw[w] ^ s) & M2) + ((dw[w] ^ s) & M2);
-            // byte b: A2 + 2 ([r <= T3] + [r <= T4]) + 12, flip iff >= 16
-            uint32_t X = A2 + 0x0C0C0C0Cu;
+            // byte b: A2 + 16 - 2 ([r > T3] + [r > T4]), flip iff >= 16
+            uint32_t X = A2 + 0x10101010u;
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
-                const uint32_t r = pcg_output_split(uint32_t(st), uint32_t(st >> 32));
-                st = st * kPcgMult + 1ULL;
-                // hi32(r (2^32 - 1) + T) = r - [r > T], so 2 [r <= T] = 2 + 2 hi32 - 2 r
+                const uint32_t r = pcg_output_split(slo, shi);
+                pcg_step_split(slo, shi);
+                // hi32(r (2^32 - 1) + T) = r - [r > T]: byte b gains
+                // 2 (h3 + h4 - 2 r) = -2 ([r > T3] + [r > T4])
                 const uint32_t h3 = mad_wide_hi(r, 0xFFFFFFFFu, a.T3);
                 const uint32_t h4 = mad_wide_hi(r, 0xFFFFFFFFu, a.T4);
-                X += (4u + 2u * (h3 + h4) - 4u * r) << (8 * b);
+                X = h3 * a.m1[b] + X;
+                X = h4 * a.m1[b] + X;
+                X = r * a.m2[b] + X;
             }
             const uint32_t g = (X & 0x10101010u) >> 4;  // 1 per flipped site
             const uint32_t gm = g * 0xFFu;
