@@ -121,6 +121,11 @@ template <bool CLUSTER>
 __global__ void __launch_bounds__(1024) xy_batch_segment(SegArgs a)
 {
     __shared__ unsigned int accepted[kMaxCpc];
+    // per owned chain and sweep: key base, beta and field offset (computed once
+    // per CTA instead of once per site update)
+    __shared__ uint64_t kb_sh[kMaxCpc];
+    __shared__ float beta_sh[kMaxCpc];
+    __shared__ unsigned long long off_sh[kMaxCpc];
     const uint64_t sweep0 = a.ctr->sweep;
     const uint32_t H = a.H, half = a.half;
     uint32_t chain_lo, chain_n, row_lo, row_n, share = 0;
@@ -140,16 +145,44 @@ __global__ void __launch_bounds__(1024) xy_batch_segment(SegArgs a)
     __syncthreads();
     const uint32_t per_chain = row_n * H;  // sites of one colour per chain share
     const uint32_t work = chain_n * per_chain;
+    // H and per_chain are powers of two for the usual sides: shifts instead of
+    // integer divisions (uniform branch)
+    const bool pow2 = (H & (H - 1)) == 0 && (per_chain & (per_chain - 1)) == 0;
+    const uint32_t hs = __ffs(H) - 1, ps = __ffs(per_chain) - 1;
+    // every warp's items lie in one chain when a chain's share is a multiple
+    // of 32 items and the block a multiple of 32 threads
+    const bool warp_chain = (per_chain & 31u) == 0 && (blockDim.x & 31u) == 0;
     for (uint32_t s = 0; s < a.sweeps; ++s) {
+        for (uint32_t ci = threadIdx.x; ci < chain_n; ci += blockDim.x) {
+            const uint32_t chain = a.chains[chain_lo + ci];
+            kb_sh[ci] = key_base(key_seed(a.chain_seed[chain], sweep0 + s, tag_site(0)));
+            beta_sh[ci] = float(a.betas[(chain / a.R) * a.R + a.slot_of_chain[chain]]);
+            off_sh[ci] = a.off[chain];
+        }
+        __syncthreads();
         for (uint32_t colour = 0; colour < 2; ++colour) {
             for (uint32_t w = threadIdx.x; w < work; w += blockDim.x) {
-                const uint32_t ci = w / per_chain, r = w - ci * per_chain;
-                const uint32_t chain = a.chains[chain_lo + ci];
-                const uint32_t y = row_lo + r / H, i = r % H;
-                const float beta = float(a.betas[(chain / a.R) * a.R + a.slot_of_chain[chain]]);
-                const uint64_t kbase = key_base(key_seed(a.chain_seed[chain], sweep0 + s, tag_site(0)));
-                if (xy_update<CLUSTER>(a, a.theta + a.off[chain], colour, y, i, kbase, beta))
+                uint32_t ci, r, y, i;
+                if (pow2) {
+                    ci = w >> ps;
+                    r = w & (per_chain - 1);
+                    y = row_lo + (r >> hs);
+                    i = r & (H - 1);
+                } else {
+                    ci = w / per_chain;
+                    r = w - ci * per_chain;
+                    y = row_lo + r / H;
+                    i = r % H;
+                }
+                const bool acc = xy_update<CLUSTER>(a, a.theta + off_sh[ci], colour, y, i, kb_sh[ci], beta_sh[ci]);
+                if (warp_chain) {
+                    // the whole warp works on chain ci: one shared atomic per warp
+                    const unsigned act = __activemask();
+                    const unsigned bal = __ballot_sync(act, acc);
+                    if ((threadIdx.x & 31u) == uint32_t(__ffs(act) - 1) && bal) atomicAdd(&accepted[ci], __popc(bal));
+                } else if (acc) {
                     atomicAdd(&accepted[ci], 1u);
+                }
             }
             if constexpr (CLUSTER) cg::this_cluster().sync();
             else __syncthreads();
