@@ -18,6 +18,14 @@
 
 namespace umc::gpu {
 
+// dof/dof.hpp:9-13: a degree of freedom names its scalar type and how many of
+// them one site holds.
+template <class D>
+concept Dof = requires {
+    typename D::dtype;
+    { D::size } -> std::convertible_to<std::size_t>;
+};
+
 // Proposal contract of dof/proposal.hpp:8-12.
 template <typename Q, typename T, typename R>
 concept Proposal = requires(const Q& q, const T* cur, T* out, R& rng) {

@@ -10,6 +10,7 @@
 #include "detail.hpp"
 #include "dof.hpp"
 #include "driver.hpp"
+#include "generic.hpp"
 #include "lattice.hpp"
 #include "models.hpp"
 #include "rng.hpp"
@@ -19,22 +20,28 @@ using umc::gpu::Bond;
 using umc::gpu::Cell;
 using umc::gpu::CellComplex;
 using umc::gpu::CellComplexLike;
+using umc::gpu::CellModel;
+using umc::gpu::CellTerm;
 using umc::gpu::cubic_lattice;
+using umc::gpu::Dof;
 using umc::gpu::EnergyModel;
 using umc::gpu::FixedAxis;
 using umc::gpu::Flip;
 using umc::gpu::Heisenberg;
+using umc::gpu::HeisenbergTerm;
 using umc::gpu::Hits;
 using umc::gpu::hypercubic_plaquettes;
 using umc::gpu::Ising;
 using umc::gpu::IsingDof;
 using umc::gpu::IsingSpin;
+using umc::gpu::IsingTerm;
 using umc::gpu::LocalRotation;
 using umc::gpu::Metropolis;
 using umc::gpu::ModelLike;
 using umc::gpu::NoPayload;
 using umc::gpu::PairGraph;
 using umc::gpu::PairGraphLike;
+using umc::gpu::PairModel;
 using umc::gpu::Pcg32;
 using umc::gpu::plaquette;
 using umc::gpu::Proposal;
@@ -43,10 +50,12 @@ using umc::gpu::square_plaquettes;
 using umc::gpu::SUDof;
 using umc::gpu::SUGauge;
 using umc::gpu::SULink;
+using umc::gpu::SUPlaquetteTerm;
 using umc::gpu::SUShift;
 using umc::gpu::U1Dof;
 using umc::gpu::U1Gauge;
 using umc::gpu::U1Link;
+using umc::gpu::U1PlaquetteTerm;
 using umc::gpu::U1Shift;
 using umc::gpu::UniformSphereN;
 using umc::gpu::VectorDof;

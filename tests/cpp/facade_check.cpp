@@ -34,6 +34,17 @@ static_assert(Proposal<U1Shift, U1Link, Pcg32>);
 static_assert(Proposal<UniformSphereN<3>, double, Pcg32>);
 static_assert(PairGraphLike<PairGraph<>>);
 static_assert(CellComplexLike<CellComplex<4>>);
+// the reference's table-driven models with its built-in terms (model/pair.hpp,
+// model/cell.hpp, term/*.hpp)
+using PairIsing = PairModel<IsingDof, IsingTerm, PairGraph<>>;
+using PairHeis = PairModel<VectorDof<3>, HeisenbergTerm<3>, PairGraph<>>;
+using CellU1 = CellModel<U1Dof, U1PlaquetteTerm, CellComplex<4>>;
+using CellSU3 = CellModel<SUDof<3>, SUPlaquetteTerm<3>, CellComplex<4>>;
+static_assert(CellTerm<IsingTerm, IsingDof> && CellTerm<U1PlaquetteTerm, U1Dof>);
+static_assert(ModelLike<PairIsing> && WolffModel<PairIsing> && EnergyModel<PairIsing>);
+static_assert(ModelLike<PairHeis> && WolffModel<PairHeis>);
+static_assert(ModelLike<CellU1> && !WolffModel<CellU1>);
+static_assert(ModelLike<CellSU3>);
 
 template <class M>
 double total_energy(const M& m)
@@ -242,6 +253,80 @@ int main()
         std::printf("SU(3) 2^4 plaquette after 20 sweeps %.5f\n", P);
         CHECK(P > 0.3 && P < 1.0);
         CHECK(std::abs(P - metro.records()[19 * UMC_OBS_STRIDE + 1]) < 1e-5);
+    }
+
+    // ---- PairModel / CellModel: host dE by finite differences, and on the
+    // device the same chains as the example models they map to
+    {
+        PairIsing pm(square_lattice(16, 16), IsingTerm{1});
+        Ising em(square_lattice(16, 16), 1);
+        Pcg32 rng(31, 2);
+        for (std::size_t i = 0; i < pm.sites(); ++i) {
+            const IsingSpin s = rng.uni() < 0.5 ? IsingSpin(-1) : IsingSpin(1);
+            pm.update(i, &s);
+            em.update(i, &s);
+        }
+        const IsingSpin p = IsingSpin(-pm.data()[9]);
+        std::int32_t before = 0;
+        for (std::size_t i = 0; i < pm.sites(); ++i) before += pm.energy_at(i);
+        const std::int32_t dE = pm.energy_diff_at(9, &p);
+        CHECK(double(dE) == em.energy_diff_at(9, &p));
+        PairIsing q = pm;
+        q.update(9, &p);
+        std::int32_t after = 0;
+        for (std::size_t i = 0; i < q.sites(); ++i) after += q.energy_at(i);
+        CHECK(2 * dE == after - before);  // energy_at counts every bond from both ends
+        Metropolis a(pm, Flip{}, Pcg32(41, 0), 0.44);
+        Metropolis b(em, Flip{}, Pcg32(41, 0), 0.44);
+        a.run(30);
+        b.run(30);
+        for (std::size_t i = 0; i < pm.sites(); ++i) CHECK(pm.data()[i] == em.data()[i]);
+        Wolff wa(pm, FixedAxis{}, Pcg32(42, 0), 0.44);
+        Wolff wb(em, FixedAxis{}, Pcg32(42, 0), 0.44);
+        std::array<std::uint64_t, 20> sa{}, sb{};
+        wa.flips(20, sa.data());
+        wb.flips(20, sb.data());
+        CHECK(sa == sb);
+        for (std::size_t i = 0; i < pm.sites(); ++i) CHECK(pm.data()[i] == em.data()[i]);
+    }
+    {
+        CellU1 cm(square_plaquettes(8), U1PlaquetteTerm{2.0});
+        U1Gauge eg(square_plaquettes(8), 2.0);
+        Pcg32 rng(33, 1);
+        U1Shift shift{2.0};
+        for (std::size_t i = 0; i < cm.sites(); ++i) {
+            U1Link l;
+            shift.sample(cm.data() + i, rng, &l);
+            cm.update(i, &l);
+            eg.update(i, &l);
+        }
+        U1Link l;
+        shift.sample(cm.data() + 5, rng, &l);
+        const double dE = cm.energy_diff_at(5, &l), before = cm.total_energy();
+        CHECK(std::abs(dE - eg.energy_diff_at(5, &l)) < 1e-12);
+        CellU1 q = cm;
+        q.update(5, &l);
+        CHECK(std::abs(dE - (q.total_energy() - before)) < 1e-9);
+        Metropolis a(cm, U1Shift{0.7}, Pcg32(43, 0), 1.0);
+        Metropolis b(eg, U1Shift{0.7}, Pcg32(43, 0), 1.0);
+        a.run(40);
+        b.run(40);
+        for (std::size_t i = 0; i < cm.sites(); ++i) CHECK(cm.data()[i].theta == eg.data()[i].theta);
+    }
+    {
+        CellSU3 cm(hypercubic_plaquettes(2), SUPlaquetteTerm<3>{5.7});
+        SUGauge<3> eg(2, 5.7);
+        for (std::size_t i = 0; i < cm.sites(); ++i) {
+            const auto one = SULink<3>::identity();
+            cm.update(i, &one);  // CellModel starts at zero, as the reference's does
+        }
+        CHECK(std::abs(cm.total_energy()) < 1e-12);
+        Metropolis a(cm, SUShift<3>{0.2}, Pcg32(44, 0), 1.0);
+        Metropolis b(eg, SUShift<3>{0.2}, Pcg32(44, 0), 1.0);
+        a.run(5);
+        b.run(5);
+        for (std::size_t i = 0; i < cm.sites(); ++i)
+            for (std::size_t k = 0; k < 9; ++k) CHECK(cm.data()[i].m[k] == eg.data()[i].m[k]);
     }
 
     std::puts("ok");
