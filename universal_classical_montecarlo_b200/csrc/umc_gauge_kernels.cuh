@@ -212,14 +212,6 @@ __device__ __forceinline__ void su_exp_i(const Mat<N>& x, Mat<N>& e)
             }
         }
         const float c1 = 0.5f * (x2.re[0] + x2.re[4] + x2.re[8]);
-        if (c1 < 1e-8f) {  // exp(iX) = I + iX - X^2/2 + O(|X|^3)
-#pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                e.re[k] = (k % 4 == 0 ? 1.f : 0.f) - x.im[k] - 0.5f * x2.re[k];
-                e.im[k] = x.re[k] - 0.5f * x2.im[k];
-            }
-            return;
-        }
         // tr(X X^2) = 3 det X; both Hermitian, so the sum over i != j is twice
         // the real part over i < j
         float off = 0.f, tr3 = 0.f;
@@ -232,42 +224,78 @@ __device__ __forceinline__ void su_exp_i(const Mat<N>& x, Mat<N>& e)
         }
         tr3 = fmaf(2.f, off, tr3);
         const float c0 = tr3 * (1.f / 3.f);
-        const bool neg = c0 < 0.f;
-        // theta = acos(|c0| / c0_max), c0_max = 2 (c1 / 3)^(3/2)
-        const float c13 = c1 * (1.f / 3.f);
-        const float th = acosf(fminf(fabsf(c0) / (2.f * c13 * sqrtf(c13)), 1.f));
-        float s3, c3;
-        sincosf(th * (1.f / 3.f), &s3, &c3);
-        const float u = sqrtf(c1 * (1.f / 3.f)) * c3, w = sqrtf(c1) * s3;
-        const float w2 = w * w, u2 = u * u;
-        float su, cu, sw, cw;
-        sincosf(u, &su, &cu);
-        sincosf(w, &sw, &cw);
-        // sin 2u, cos 2u by the double-angle formulas
-        const float s2u = 2.f * su * cu, c2u = fmaf(cu, cu, -su * su);
-        const float xi = fabsf(w) < 0.05f ? 1.f - w2 * (1.f / 6.f) * (1.f - w2 * (1.f / 20.f) * (1.f - w2 * (1.f / 42.f)))
-                                          : sw / w;
-        // e^{-iu} = (cu, -su)
-        auto emiu = [&](float ar, float ai, float& rr, float& ri) {  // e^{-iu} (ar + i ai)
-            rr = cu * ar + su * ai;
-            ri = cu * ai - su * ar;
-        };
-        float h0r, h0i, h1r, h1i, h2r, h2i, tr, ti;
-        emiu(8.f * u2 * cw, 2.f * u * (3.f * u2 + w2) * xi, tr, ti);
-        h0r = (u2 - w2) * c2u + tr;
-        h0i = (u2 - w2) * s2u + ti;
-        emiu(2.f * u * cw, -(3.f * u2 - w2) * xi, tr, ti);
-        h1r = 2.f * u * c2u - tr;
-        h1i = 2.f * u * s2u - ti;
-        emiu(cw, 3.f * u * xi, tr, ti);
-        h2r = c2u - tr;
-        h2i = s2u - ti;
-        const float id = 1.f / (9.f * u2 - w2);
-        float f0r = h0r * id, f0i = h0i * id, f1r = h1r * id, f1i = h1i * id, f2r = h2r * id, f2i = h2i * id;
-        if (neg) {  // f_j(-c0) = (-1)^j conj f_j(c0)
-            f0i = -f0i;
-            f1r = -f1r;
-            f2i = -f2i;
+        float f0r, f0i, f1r, f1i, f2r, f2i;
+        if (c1 <= 0.75f) {
+            // |eigenvalues| <= sqrt(4 c1 / 3) <= 1: sum the series exp(iX) =
+            // sum_k i^k X^k / k! with X^k = a_k I + b_k X + d_k X^2, reduced by
+            // X^3 = c1 X + c0 I (Cayley-Hamilton): a' = c0 d, b' = a + c1 d,
+            // d' = b.  Twelve terms leave < 1/13! = 1.6e-10; no transcendentals.
+            constexpr double kInvFact[13] = {1.0, 1.0, 1.0 / 2, 1.0 / 6, 1.0 / 24, 1.0 / 120, 1.0 / 720, 1.0 / 5040,
+                                             1.0 / 40320, 1.0 / 362880, 1.0 / 3628800, 1.0 / 39916800,
+                                             1.0 / 479001600};
+            float a = 1.f, b = 0.f, d = 0.f;
+            f0r = 1.f;
+            f0i = f1r = f1i = f2r = f2i = 0.f;
+#pragma unroll
+            for (int k = 1; k <= 12; ++k) {
+                const float na = c0 * d, nb = fmaf(c1, d, a);
+                d = b;
+                a = na;
+                b = nb;
+                const float t = float(kInvFact[k]) * ((k & 2) ? -1.f : 1.f);  // i^k = +1, +i, -1, -i
+                if (k & 1) {
+                    f0i = fmaf(t, a, f0i);
+                    f1i = fmaf(t, b, f1i);
+                    f2i = fmaf(t, d, f2i);
+                } else {
+                    f0r = fmaf(t, a, f0r);
+                    f1r = fmaf(t, b, f1r);
+                    f2r = fmaf(t, d, f2r);
+                }
+            }
+        } else {
+            const bool neg = c0 < 0.f;
+            // theta = acos(|c0| / c0_max), c0_max = 2 (c1 / 3)^(3/2)
+            const float c13 = c1 * (1.f / 3.f);
+            const float th = acosf(fminf(fabsf(c0) / (2.f * c13 * sqrtf(c13)), 1.f));
+            float s3, c3;
+            sincosf(th * (1.f / 3.f), &s3, &c3);
+            const float u = sqrtf(c1 * (1.f / 3.f)) * c3, w = sqrtf(c1) * s3;
+            const float w2 = w * w, u2 = u * u;
+            float su, cu, sw, cw;
+            sincosf(u, &su, &cu);
+            sincosf(w, &sw, &cw);
+            // sin 2u, cos 2u by the double-angle formulas
+            const float s2u = 2.f * su * cu, c2u = fmaf(cu, cu, -su * su);
+            const float xi = fabsf(w) < 0.05f ? 1.f - w2 * (1.f / 6.f) * (1.f - w2 * (1.f / 20.f) * (1.f - w2 * (1.f / 42.f)))
+                                              : sw / w;
+            // e^{-iu} = (cu, -su)
+            auto emiu = [&](float ar, float ai, float& rr, float& ri) {  // e^{-iu} (ar + i ai)
+                rr = cu * ar + su * ai;
+                ri = cu * ai - su * ar;
+            };
+            float h0r, h0i, h1r, h1i, h2r, h2i, tr, ti;
+            emiu(8.f * u2 * cw, 2.f * u * (3.f * u2 + w2) * xi, tr, ti);
+            h0r = (u2 - w2) * c2u + tr;
+            h0i = (u2 - w2) * s2u + ti;
+            emiu(2.f * u * cw, -(3.f * u2 - w2) * xi, tr, ti);
+            h1r = 2.f * u * c2u - tr;
+            h1i = 2.f * u * s2u - ti;
+            emiu(cw, 3.f * u * xi, tr, ti);
+            h2r = c2u - tr;
+            h2i = s2u - ti;
+            const float id = 1.f / (9.f * u2 - w2);
+            f0r = h0r * id;
+            f0i = h0i * id;
+            f1r = h1r * id;
+            f1i = h1i * id;
+            f2r = h2r * id;
+            f2i = h2i * id;
+            if (neg) {  // f_j(-c0) = (-1)^j conj f_j(c0)
+                f0i = -f0i;
+                f1r = -f1r;
+                f2i = -f2i;
+            }
         }
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
