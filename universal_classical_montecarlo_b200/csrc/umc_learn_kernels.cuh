@@ -533,7 +533,8 @@ __device__ __forceinline__ void mixture_dir(const float o[16], MixtureDir& m)
 // with log q(t) = logsumexp_k(log w_k - log I0(kappa_k) + kappa_k cos(t - mu_k))
 // (the common log 2 pi cancels).  The per-component terms are FP32 -- their
 // error, about kappa 1e-7, is the size of the FP32 angle quantisation of the
-// proposal itself -- and log_p is formed in FP64.  Returns true if accepted.
+// proposal itself.  The accept test compares in FP32 with error bounds and
+// forms log_p in FP64 only inside them.  Returns true if accepted.
 __device__ __forceinline__ bool learned_update(const U1BatchArgs& a, float* th, uint32_t k, const float o[16],
                                                float Sr, float Si, uint64_t kbase)
 {
