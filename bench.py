@@ -49,7 +49,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", choices=["o3", "ising", "su3", "xybatch", "u1learned"], default="o3",
+    p.add_argument("--workload", choices=["o3", "ising", "su3", "xybatch", "u1batch", "u1learned"], default="o3",
                    help="o3: the headline configuration; ising / su3 / xybatch: secondary roofline runs; "
                         "u1learned: the learned-proposal study (effective samples/s)")
     p.add_argument("--no-learned", action="store_true", help="skip the learned-proposal summary of the o3 line")
@@ -149,6 +149,14 @@ def measured_peak_hbm():
             return float(json.load(f)["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         return 6650.0, "fallback"
+
+
+def measured_peak_bf16():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
 
 
 def profiled_traffic(kind: str, units: float):
@@ -624,7 +632,73 @@ class _BatchAsChain:
         self.timing = on
 
 
-WORKLOADS = {"o3": O3Hybrid, "ising": IsingSweep, "su3": SU3Sweep, "xybatch": XYBatch}
+class _U1AsChain:
+    """The few chain methods the timing loop uses, for a U(1) batch."""
+
+    def __init__(self, b):
+        self.b = b
+
+    def stream(self):
+        return self.b.stream()
+
+    def fetch(self, cap):
+        rec = self.b.fetch(min(cap, self.b.max_records))
+        return rec, __import__("numpy").zeros(len(rec))
+
+    def kernel_stats(self, reset=False):
+        _, k = self.b.counters()
+        out = {"learned": (k - getattr(self, "_base", 0), 0.0)}
+        if reset:
+            self._base = k
+        return out
+
+    def set_timing(self, on):
+        pass
+
+
+class U1LearnedSweep:
+    """The learned sampler alone: 444 2D U(1) 64x64 chains at beta 4, one
+    learned sweep per step (MLP 3-64-64-16 in BF16 on tcgen05, von Mises
+    mixture, MH), network weights from a fixed seed (untrained)."""
+
+    name = "u1batch"
+    unit = "link-updates/s"
+    dtype = "bf16/f32"
+    chains = 444
+
+    def __init__(self, umc, args, rank, local):
+        self.L = 64
+        self.b = umc.U1Batch(self.chains, self.L, 4.0, width=0.5, seed=1 + rank, device=local, max_records=4096)
+        self.b.run(200, records=False)
+        self.net = umc.ProposalNet(3 + rank, device=local)
+        self.n = self.chains * 2 * self.L * self.L
+        self.flush = True
+        self.ch = _U1AsChain(self.b)
+
+    def describe(self):
+        return (f"learned sampler: {self.chains} 2D U(1) {self.L}x{self.L} chains, beta 4, one learned sweep per step "
+                f"(MLP 3-64-64-16 BF16 tcgen05, 4-component von Mises mixture, MH); network from a fixed seed")
+
+    def enqueue(self, k):
+        self.b.enqueue(k, self.net)
+
+    def units(self, rec, sizes):
+        return len(rec) * self.n
+
+    def flops_per_launch(self, kind):
+        return 10624.0 * self.n  # network forward per link-update (tensor cores)
+
+    def bytes_per_launch(self, kind):
+        return 20.0 * self.n
+
+    def e2e(self, torch, K):
+        return None
+
+    def cpu(self, seconds):
+        return None
+
+
+WORKLOADS = {"o3": O3Hybrid, "ising": IsingSweep, "su3": SU3Sweep, "xybatch": XYBatch, "u1batch": U1LearnedSweep}
 
 
 def run_learned(args):
@@ -725,6 +799,8 @@ def main():
     # batch, one launch = the captured segment graph, timed by the step events)
     if wl.name == "xybatch":
         per_kind = {"batch": (K, total_ms)}
+    elif wl.name == "u1batch":
+        per_kind = {"learned": (K, total_ms)}
     else:
         per_kind = None
     ch.set_timing(True)
@@ -745,9 +821,19 @@ def main():
     kind, (nl, ms) = max(((k, v) for k, v in per_kind.items() if v[0] > 0 and k != "other"),
                          key=lambda kv: kv[1][1])
     avg_s = ms / nl / 1e3
-    achieved = wl.bytes_per_launch(kind) / avg_s / 1e9
-    peak, peak_src = measured_peak_hbm()
     traffic = profiled_traffic(f"{wl.name}:{kind}", 1.0)
+    if hasattr(wl, "flops_per_launch"):
+        achieved = wl.flops_per_launch(kind) / avg_s / 1e12
+        peak, peak_src = measured_peak_bf16()
+        roof = {"bound": "tensor", "unit": "TFLOP/s",
+                "peak_source": "of measured (MEASURED_PEAKS.json bf16_tflops)" if peak_src == "measured"
+                else "of fallback 1.59 PFLOP/s"}
+    else:
+        achieved = wl.bytes_per_launch(kind) / avg_s / 1e9
+        peak, peak_src = measured_peak_hbm()
+        roof = {"bound": "hbm", "unit": "GB/s",
+                "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
+                else "of fallback 6.65 TB/s"}
 
     # ---- end to end through the C ABI with host buffers
     e2e = None if args.no_e2e else wl.e2e(torch, min(K, 300))
@@ -797,9 +883,9 @@ def main():
                    "l2": ("flushed between timed steps (256 MiB write, outside the timed events)" if wl.flush
                           else "state larger than L2, no flush"),
                    "mean_cluster": float(sizes.mean()) if len(sizes) and wl.name == "o3" else None},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": kind, "avg_launch_us": avg_s * 1e6,
-                     "peak_source": "of measured (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "of fallback 6.65 TB/s"},
+        "roofline": {"bound": roof["bound"], "achieved": achieved, "peak": peak, "unit": roof["unit"],
+                     "frac": achieved / peak, "traffic": traffic, "kernel": kind, "avg_launch_us": avg_s * 1e6,
+                     "peak_source": roof["peak_source"]},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": gpu_launches,
