@@ -190,10 +190,44 @@ __device__ __forceinline__ void uf_find2(uint32_t* lab, uint32_t x0, uint32_t x1
     r1 = x1;
 }
 
+// The root of s (read only: every thread of the grid walks this same path)
+// together with two path-halving finds, all three load chains in lockstep.
+__device__ __forceinline__ void uf_find_with_root(uint32_t* lab, uint32_t s, uint32_t x0, uint32_t x1, uint32_t bound,
+                                                  unsigned* status, uint32_t& rs, uint32_t& r0, uint32_t& r1)
+{
+    volatile uint32_t* L = lab;
+    bool ds = false, d0 = false, d1 = false;
+    for (uint32_t it = 0; it < bound; ++it) {
+        const uint32_t ps = ds ? s : L[s];
+        const uint32_t p0 = d0 ? x0 : L[x0];
+        const uint32_t p1 = d1 ? x1 : L[x1];
+        ds = ds || ps == s;
+        d0 = d0 || p0 == x0;
+        d1 = d1 || p1 == x1;
+        if (ds && d0 && d1) {
+            rs = s;
+            r0 = x0;
+            r1 = x1;
+            return;
+        }
+        const uint32_t g0 = d0 ? x0 : L[p0];
+        const uint32_t g1 = d1 ? x1 : L[p1];
+        if (!d0 && g0 != p0) L[x0] = g0;
+        if (!d1 && g1 != p1) L[x1] = g1;
+        if (!ds) s = ps;
+        if (!d0) x0 = g0;
+        if (!d1) x1 = g1;
+    }
+    atomicOr(status, kDevErrUnionFind);
+    rs = s;
+    r0 = x0;
+    r1 = x1;
+}
+
 __device__ __forceinline__ void uf_union(uint32_t* lab, uint32_t a, uint32_t b, uint32_t bound, unsigned* status)
 {
-    a = uf_find(lab, a, bound, status);
-    b = uf_find(lab, b, bound, status);
+    // both finds walked together: their load chains overlap
+    uf_find2(lab, a, b, bound, status, a, b);
     for (uint32_t it = 0; it < (1u << 22); ++it) {
         if (a == b) return;
         if (uf_priority(a) > uf_priority(b)) {
@@ -204,8 +238,7 @@ __device__ __forceinline__ void uf_union(uint32_t* lab, uint32_t a, uint32_t b, 
         // link the lower-priority root under the higher-priority one
         const uint32_t old = atomicCAS(lab + a, a, b);
         if (old == a) return;
-        a = uf_find(lab, old, bound, status);
-        b = uf_find(lab, b, bound, status);
+        uf_find2(lab, old, b, bound, status, a, b);
     }
     atomicOr(status, kDevErrUnionFind);
 }

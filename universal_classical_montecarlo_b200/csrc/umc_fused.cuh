@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(TX * TY * TZ / SPT, 2 * SPT) hybrid_fused(Fuse
     static_assert(T % SPT == 0, "sites per thread must divide the tile");
     __shared__ uint32_t lab[T];
     __shared__ float r_sh[4];
-    __shared__ uint32_t root_sh;
+    __shared__ uint32_t seed_sh;
     __shared__ uint32_t xs_cnt, xs_base;
     const WolffTileArgs& w = a.w;
     unsigned* status = &w.ctl->status;
@@ -150,6 +150,13 @@ __global__ void __launch_bounds__(TX * TY * TZ / SPT, 2 * SPT) hybrid_fused(Fuse
             float r[N];
             sphere_sample<N>(gax, r);
             for (int c = 0; c < N; ++c) r_sh[c] = r[c];
+            // seed site: next draw of the axis stream, colour-major -> natural
+            const uint32_t ks = uint32_t(u_f64(gax.next()) * double(w.n));
+            const uint32_t c = ks >= w.half ? 1u : 0u, rank = ks - c * w.half;
+            uint32_t nat = 2 * rank;
+            const uint32_t x = nat % w.Lx, rr = nat / w.Lx, y = rr % w.Ly, z = rr / w.Ly;
+            if (((x + y + z) & 1u) != c) ++nat;
+            seed_sh = nat;
             if (blockIdx.x == 0) *w.size_slot = 0ull;
         }
         // ---- A: tiles
@@ -256,28 +263,23 @@ __global__ void __launch_bounds__(TX * TY * TZ / SPT, 2 * SPT) hybrid_fused(Fuse
 
         // ---- C: flip the seed's cluster (the list is consumed: reset it)
         if (gtid == 0) w.ctl->xcount = 0u;
-        if (tid == 0) {
-            // seed site: next draw of the axis stream, colour-major -> natural
-            const uint32_t ks = uint32_t(u_f64(gax.next()) * double(w.n));
-            const uint32_t c = ks >= w.half ? 1u : 0u, rank = ks - c * w.half;
-            uint32_t nat = 2 * rank;
-            const uint32_t x = nat % w.Lx, rr = nat / w.Lx, y = rr % w.Ly, z = rr / w.Ly;
-            if (((x + y + z) & 1u) != c) ++nat;
-            root_sh = uf_find(w.label, nat, w.n + 1, status);
-        }
-        __syncthreads();
         {
             float r[N];
 #pragma unroll
             for (int c = 0; c < N; ++c) r[c] = r_sh[c];
-            const uint32_t root = root_sh;
+            const uint32_t seed = seed_sh;
+            uint32_t root = 0xFFFFFFFFu;
             double cnt[1] = {0.0};
             float* f = static_cast<float*>(w.field);
-            // two sites per thread and iteration, their finds walked together
+            // two sites per thread and iteration, their finds walked together;
+            // in the first iteration every thread also walks the seed's path
+            // to its root (read only) in the same lockstep, so no thread waits
+            // for one thread's find of the seed
             for (uint32_t n0 = gtid; n0 < w.n; n0 += 2 * gsize) {
                 const uint32_t n1 = n0 + gsize;
                 uint32_t r0, r1;
-                uf_find2(w.label, n0, n1 < w.n ? n1 : n0, w.n + 1, status, r0, r1);
+                if (root == 0xFFFFFFFFu) uf_find_with_root(w.label, seed, n0, n1 < w.n ? n1 : n0, w.n + 1, status, root, r0, r1);
+                else uf_find2(w.label, n0, n1 < w.n ? n1 : n0, w.n + 1, status, r0, r1);
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
                     const uint32_t nat = u ? n1 : n0;
