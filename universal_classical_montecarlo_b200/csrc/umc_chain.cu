@@ -673,6 +673,7 @@ Stage host_stage(umc_chain* c)
     const size_t need = 16 + size_t(c->max_records) * (kObs * sizeof(double) + sizeof(unsigned long long));
     if (c->host_stage_bytes < need) {
         cuda_check(cudaStreamSynchronize(c->stream), "synchronise chain");
+        if (c->rec_stream) cuda_check(cudaStreamSynchronize(c->rec_stream), "synchronise record copies");
         if (c->host_stage) cudaFreeHost(c->host_stage);
         c->host_stage = nullptr;
         c->host_stage_bytes = 0;
@@ -691,10 +692,20 @@ void record_done(umc_chain* c, uint64_t r)
 {
     if (!c->stream_records || c->rec_overflow || r != c->streamed) return;
     const Stage h = host_stage(c);
+    if (!c->rec_stream) {
+        cuda_check(cudaStreamCreateWithFlags(&c->rec_stream, cudaStreamNonBlocking), "record stream");
+        for (auto& e : c->rec_ready) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "record event");
+    }
+    // the copies run on their own stream once the step has written slot r, so
+    // the next step's work on the chain's stream does not queue behind them
+    cudaEvent_t e = c->rec_ready[c->rec_next];
+    c->rec_next ^= 1;
+    cuda_check(cudaEventRecord(e, c->stream), "stream record");
+    cuda_check(cudaStreamWaitEvent(c->rec_stream, e, 0), "stream record");
     cuda_check(cudaMemcpyAsync(h.rec + r * kObs, c->records.as<double>() + r * kObs, kObs * sizeof(double),
-                               cudaMemcpyDeviceToHost, c->stream), "stream record");
+                               cudaMemcpyDeviceToHost, c->rec_stream), "stream record");
     cuda_check(cudaMemcpyAsync(h.sz + r, c->sizes.as<unsigned long long>() + r, sizeof(unsigned long long),
-                               cudaMemcpyDeviceToHost, c->stream), "stream record");
+                               cudaMemcpyDeviceToHost, c->rec_stream), "stream record");
     c->streamed = r + 1;
 }
 
@@ -720,6 +731,7 @@ void fetch(umc_chain* c, double* records, uint64_t* sizes, uint64_t capacity, ui
                    "fetch sizes");
     }
     cuda_check(cudaStreamSynchronize(c->stream), "synchronise chain");
+    if (c->rec_stream) cuda_check(cudaStreamSynchronize(c->rec_stream), "synchronise record copies");
     raise_status(c, *st);
     if (c->rec_overflow) {
         c->rec_overflow = false;
@@ -878,6 +890,8 @@ void destroy_chain(umc_chain* c)
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->up_stream) cudaStreamSynchronize(c->up_stream);
+    if (c->rec_stream) cudaStreamSynchronize(c->rec_stream);
     gauge_release(c);
     for (auto& t : c->timed) {
         cudaEventDestroy(t.a);
@@ -890,10 +904,10 @@ void destroy_chain(umc_chain* c)
         if (c->up_consumed[q]) cudaEventDestroy(c->up_consumed[q]);
         c->up_staging[q].free_();
     }
-    if (c->up_stream) {
-        cudaStreamSynchronize(c->up_stream);
-        cudaStreamDestroy(c->up_stream);
-    }
+    if (c->up_stream) cudaStreamDestroy(c->up_stream);
+    if (c->rec_stream) cudaStreamDestroy(c->rec_stream);
+    for (auto& e : c->rec_ready)
+        if (e) cudaEventDestroy(e);
     if (c->host_stage) cudaFreeHost(c->host_stage);
     c->host_stage = nullptr;
     for (DevBuf* b : {&c->field, &c->staging, &c->off, &c->adj, &c->slot, &c->position, &c->lab0, &c->lab1, &c->xlist, &c->cells,

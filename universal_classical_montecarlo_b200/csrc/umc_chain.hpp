@@ -83,6 +83,9 @@ struct umc_chain
     cudaEvent_t upload_done = nullptr;  // set_field waits on the copy, not the scatter
     bool stream_records = false;        // copy each record to host_stage as it is written
     uint64_t streamed = 0;              // records [0, streamed) already in host_stage
+    cudaStream_t rec_stream = nullptr;  // those copies, off the chain's stream
+    cudaEvent_t rec_ready[2] = {nullptr, nullptr};
+    int rec_next = 0;
     // umc_chain_upload_async: copy stream, two staging buffers and their events
     cudaStream_t up_stream = nullptr;
     umc::DevBuf up_staging[2];
