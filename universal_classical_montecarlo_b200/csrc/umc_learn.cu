@@ -51,6 +51,7 @@ struct umc_u1batch
     uint64_t max_records = 0, rec_pending = 0;
     bool rec_overflow = false;
     int plain_grid = 0, learned_grid = 0;
+    uint32_t groups = 0;  // tile groups of the learned kernel (learn::kGroupChoices)
     uint64_t launches = 0;
 };
 
@@ -157,9 +158,13 @@ void enqueue_sweeps(umc_u1batch* b, uint64_t n_sweeps, const umc_mlp* net, float
         a.n_sweeps = uint32_t(chunk);
         a.rec_slot0 = b->rec_pending;
         if (net) {
-            const learn::LearnSmem sp = learn::LearnSmem::plan(b->L, learn::kGroups);
-            learn::u1_learned_batch<<<std::min<int>(b->learned_grid, b->n_chains), learn::kTile * learn::kGroups,
-                                      sp.total, b->stream>>>(a);
+            const learn::LearnSmem sp = learn::LearnSmem::plan(b->L, b->groups);
+            const int grid = std::min<int>(b->learned_grid, b->n_chains);
+            switch (b->groups) {
+            case 8: learn::u1_learned_batch<8><<<grid, learn::kTile * 8, sp.total, b->stream>>>(a); break;
+            case 6: learn::u1_learned_batch<6><<<grid, learn::kTile * 6, sp.total, b->stream>>>(a); break;
+            default: learn::u1_learned_batch<4><<<grid, learn::kTile * 4, sp.total, b->stream>>>(a); break;
+            }
         } else {
             const size_t smem = size_t(2) * b->L * b->L * 4;
             learn::u1_plain_batch<<<std::min<int>(b->plain_grid, b->n_chains), 256, smem, b->stream>>>(a);
@@ -497,16 +502,25 @@ int umc_u1batch_create(const umc_u1batch_desc* d, umc_u1batch** out)
             b->records.alloc(b->max_records * b->n_chains * 4 * 8, "records");
             b->status.alloc(4, "status");
             cuda_check(cudaMemsetAsync(b->status.p, 0, 4, b->stream), "status");
-            const learn::LearnSmem sp = learn::LearnSmem::plan(b->L, learn::kGroups);
-            cuda_check(cudaFuncSetAttribute(learn::u1_learned_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            int(sp.total)),
+            // the most tile groups whose shared-memory plan fits one CTA
+            int smem_max = 0;
+            cuda_check(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device),
+                       "shared memory limit");
+            b->groups = 0;
+            for (uint32_t gch : learn::kGroupChoices)
+                if (!b->groups && learn::LearnSmem::plan(b->L, gch).total <= uint32_t(smem_max)) b->groups = gch;
+            if (!b->groups) throw Error(UMC_ERR_UNSUPPORTED, "chain too large for the learned sampler's shared memory");
+            const learn::LearnSmem sp = learn::LearnSmem::plan(b->L, b->groups);
+            const void* lk = b->groups == 8   ? reinterpret_cast<const void*>(learn::u1_learned_batch<8>)
+                             : b->groups == 6 ? reinterpret_cast<const void*>(learn::u1_learned_batch<6>)
+                                              : reinterpret_cast<const void*>(learn::u1_learned_batch<4>);
+            cuda_check(cudaFuncSetAttribute(lk, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sp.total)),
                        "learned smem");
             const size_t psm = per * 4;
             cuda_check(cudaFuncSetAttribute(learn::u1_plain_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             int(psm)),
                        "plain smem");
-            b->learned_grid = resident_grid(reinterpret_cast<const void*>(learn::u1_learned_batch),
-                                            learn::kTile * learn::kGroups, sp.total, b->device);
+            b->learned_grid = resident_grid(lk, int(learn::kTile * b->groups), sp.total, b->device);
             b->plain_grid = resident_grid(reinterpret_cast<const void*>(learn::u1_plain_batch), 256, psm, b->device);
             cuda_check(cudaStreamSynchronize(b->stream), "create");
         } catch (...) {

@@ -666,7 +666,10 @@ __global__ void __launch_bounds__(256) u1_plain_batch(U1BatchArgs a)
 // mbarriers and the TMEM address slot, then the chain's angles.  The total is
 // padded so that the CTAs one SM can hold never ask for more than 512 TMEM
 // columns between them.
-constexpr uint32_t kGroups = 6;  // tile groups of the learned sampler (768 threads, 6 x 64 TMEM columns)
+// Tile groups of the learned sampler: 8 (1024 threads, 8 x 64 = 512 TMEM
+// columns, two rounds of tiles per 2048-link colour class of a 64 x 64 chain)
+// when the shared-memory plan fits, else 6 or 4 for larger chains.
+constexpr uint32_t kGroupChoices[3] = {8, 6, 4};
 
 struct LearnSmem
 {
@@ -689,12 +692,13 @@ struct LearnSmem
 };
 
 // Learned Metropolis-Hastings sweeps.  One CTA holds one chain at a time in
-// shared memory; its kGroups tile groups share each colour class's tiles, and
+// shared memory; its G tile groups share each colour class's tiles, and
 // the class passes are separated by CTA-wide barriers.
-__global__ void __launch_bounds__(kTile * kGroups, 1) u1_learned_batch(U1BatchArgs a)
+template <uint32_t G>
+__global__ void __launch_bounds__(kTile * G, 1) u1_learned_batch(U1BatchArgs a)
 {
     extern __shared__ __align__(16) uint8_t smem[];
-    const LearnSmem sp = LearnSmem::plan(a.L, kGroups);
+    const LearnSmem sp = LearnSmem::plan(a.L, G);
     uint8_t* img = smem + sp.img;
     float* th = reinterpret_cast<float*>(smem + sp.field);
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + sp.bar);
@@ -704,8 +708,8 @@ __global__ void __launch_bounds__(kTile * kGroups, 1) u1_learned_batch(U1BatchAr
     for (uint32_t i = t; i < IMG_FWD_BYTES / 16; i += blockDim.x)
         reinterpret_cast<uint4*>(img)[i] = reinterpret_cast<const uint4*>(a.img)[i];
     if (t == 0)
-        for (uint32_t g = 0; g < kGroups; ++g) tc::mbar_init(mbar + g, 1);
-    if (t < 32) tc::tmem_alloc(tslot, alloc_cols(kFwdCols * kGroups));
+        for (uint32_t g = 0; g < G; ++g) tc::mbar_init(mbar + g, 1);
+    if (t < 32) tc::tmem_alloc(tslot, alloc_cols(kFwdCols * G));
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
@@ -724,7 +728,7 @@ __global__ void __launch_bounds__(kTile * kGroups, 1) u1_learned_batch(U1BatchAr
             const uint64_t kbase = key_base(key_seed(a.chain_seed[c], a.sweep0 + s, kTagLearned));
             double acc = 0.0;
             for (uint32_t cls = 0; cls < 4; ++cls) {
-                for (uint32_t tile = grp; tile < tiles; tile += kGroups) {
+                for (uint32_t tile = grp; tile < tiles; tile += G) {
                     const uint32_t q = tile * kTile + tl.row;
                     const bool valid = q < g.half;
                     float Sr = 1.0f, Si = 0.0f;
@@ -753,7 +757,7 @@ __global__ void __launch_bounds__(kTile * kGroups, 1) u1_learned_batch(U1BatchAr
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
-    if (t < 32) tc::tmem_dealloc(*tslot, alloc_cols(kFwdCols * kGroups));
+    if (t < 32) tc::tmem_dealloc(*tslot, alloc_cols(kFwdCols * G));
 }
 
 // ------------------------------------------------------------ forward (tests)
