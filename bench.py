@@ -246,7 +246,7 @@ class O3Hybrid:
         return len(rec) * self.n + float(sizes.sum())
 
     def bytes_per_launch(self, kind):
-        # algorithmic bytes (DESIGN.md): colour pass 36 B per site-update
+        # algorithmic bytes: colour pass 36 B per site-update
         # (read own + neighbour class, write own; 12 B per FP32 3-vector);
         # Wolff: bond pass reads each site and its + neighbours once (12 B +
         # 4 B label write + 1 B crossing mask), flip reads label + spin (16 B)
