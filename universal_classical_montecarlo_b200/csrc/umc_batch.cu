@@ -438,20 +438,25 @@ GroupCfg autotune(umc_batch* b, umc_batch::Group& g)
     GroupCfg best;
     float best_ms = 1e30f;
     for (const GroupCfg& cfg : candidates(g.L, uint32_t(g.chains.size()))) {
-        // warm once, then time two launches
+        // warm once, then the fastest of three timings of two launches each,
+        // so that one noisy timing does not pick the shape
         try {
             launch_segment(b, g, cfg, scratch.as<float>(), b->stream);
         } catch (const Error&) {
             cudaGetLastError();
             continue;
         }
-        cuda_check(cudaEventRecord(e0, b->stream), "event");
-        launch_segment(b, g, cfg, scratch.as<float>(), b->stream);
-        launch_segment(b, g, cfg, scratch.as<float>(), b->stream);
-        cuda_check(cudaEventRecord(e1, b->stream), "event");
-        cuda_check(cudaEventSynchronize(e1), "autotune");
-        float ms = 0;
-        cuda_check(cudaEventElapsedTime(&ms, e0, e1), "autotune");
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            cuda_check(cudaEventRecord(e0, b->stream), "event");
+            launch_segment(b, g, cfg, scratch.as<float>(), b->stream);
+            launch_segment(b, g, cfg, scratch.as<float>(), b->stream);
+            cuda_check(cudaEventRecord(e1, b->stream), "event");
+            cuda_check(cudaEventSynchronize(e1), "autotune");
+            float t = 0;
+            cuda_check(cudaEventElapsedTime(&t, e0, e1), "autotune");
+            ms = std::min(ms, t);
+        }
         if (ms < best_ms) {
             best_ms = ms;
             best = cfg;
