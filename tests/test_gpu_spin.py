@@ -388,7 +388,8 @@ def test_invalid_combinations_are_rejected(umc):
 
 @pytest.mark.parametrize("dims,N,prop", [((16, 16, 16), 3, "sphere"), ((32, 32, 1), 2, "rotation"),
                                          ((8, 8, 8), 4, "sphere"), ((6, 4, 2), 3, "rotation"),
-                                         ((64, 64, 64), 3, "sphere")])
+                                         ((64, 64, 64), 3, "sphere"), ((12, 10, 14), 3, "sphere"),
+                                         ((40, 18, 1), 2, "sphere"), ((24, 8, 2), 1, "sphere")])
 def test_fused_step_matches_multikernel(umc, dims, N, prop):
     """The one-kernel step (cooperative, grid barrier) and the five-kernel path
     produce the same field, cluster sizes and accept counts."""
