@@ -172,6 +172,18 @@ int umc_chain_get_field(umc_chain* c, void* host_field);
  * (umc_chain_sync, _fetch, _get_field, a *_run).  The reference sets a field
  * only through its model's update(i, .) (model.hpp:70-86). */
 int umc_chain_upload_async(umc_chain* c, const void* host_field);
+/* Chain checkpoints: a self-describing byte image of a chain -- an 88-byte
+ * header (magic "UMCCHK01", version, model, components, lattice size, seed,
+ * sweep and flip counters, coupling, proposal, width, hits, Wolff axis) and
+ * then the field in the reference's data() layout.  Restoring it into a chain
+ * of the same model, components, lattice size and coupling (for instance in a
+ * new process) sets the field, the key seed, the counters and the proposal,
+ * so the chain continues exactly as the checkpointed one would have.  The
+ * reference has no checkpoint format: its user copies data() by hand
+ * (model.hpp:70-86); this is the engine's own. */
+int umc_chain_checkpoint_bytes(const umc_chain* c, uint64_t* bytes);
+int umc_chain_checkpoint(umc_chain* c, void* buffer, uint64_t capacity);
+int umc_chain_restore(umc_chain* c, const void* buffer, uint64_t bytes);
 /* With streaming on, every record (and cluster size) is copied to pinned host
  * memory as soon as its step has run, on the chain's stream; umc_chain_fetch
  * then only waits.  This is how the reference's sample(n, observe) sees each

@@ -1,0 +1,71 @@
+"""Chain checkpoints (umc_chain_checkpoint / umc_chain_restore): a chain
+restored from an image taken mid-run -- into a fresh chain created with
+another seed, or through a file -- continues bit for bit as the original, for
+spin and gauge models; images of another model, size or coupling, and damaged
+images, are refused."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _make(umc, kind, seed):
+    if kind == "o3":
+        return umc.Chain(umc.MODEL_VECTOR, graph=umc.cubic_lattice(8, 8, 8), components=3, coupling=1.0,
+                         proposal=umc.PROPOSAL_SPHERE, wolff_axis=umc.AXIS_SPHERE, seed=seed)
+    if kind == "ising":
+        return umc.Chain(umc.MODEL_ISING, graph=umc.square_lattice(32, 32), coupling=1, proposal=umc.PROPOSAL_FLIP,
+                         wolff_axis=umc.AXIS_FIXED, seed=seed)
+    return umc.Chain(umc.MODEL_SU, cells=umc.hypercubic_plaquettes(4), components=2, coupling=2.3,
+                     proposal=umc.PROPOSAL_SUSHIFT, width=0.3, hits=2, seed=seed)
+
+
+def _advance(ch, kind, n):
+    if kind == "su2":
+        return ch.metropolis(1.0, n), None
+    sizes, rec = ch.hybrid(0.693 if kind == "o3" else 0.44, n)
+    return rec, sizes
+
+
+@pytest.mark.parametrize("kind", ["o3", "ising", "su2"])
+def test_restored_chain_continues_exactly(umc, kind, tmp_path):
+    a = _make(umc, kind, 11)
+    a.randomize(3)
+    _advance(a, kind, 6)
+    image = a.checkpoint()
+    a.save(tmp_path / "chain.ckpt")
+    ra, sa = _advance(a, kind, 8)
+    fa = a.get_field()
+    for via_file in (False, True):
+        b = _make(umc, kind, 999)  # another seed: the image carries the key seed
+        if via_file:
+            b.load(tmp_path / "chain.ckpt")
+        else:
+            b.restore(image)
+        assert b.counters() == (6, 6) if kind != "su2" else b.counters()[0] == 6
+        rb, sb = _advance(b, kind, 8)
+        np.testing.assert_array_equal(ra, rb)
+        if sa is not None:
+            np.testing.assert_array_equal(sa, sb)
+        np.testing.assert_array_equal(fa, b.get_field())
+
+
+def test_mismatched_or_damaged_images_are_refused(umc):
+    a = _make(umc, "o3", 1)
+    image = a.checkpoint()
+    other_size = umc.Chain(umc.MODEL_VECTOR, graph=umc.cubic_lattice(8, 8, 4), components=3, coupling=1.0,
+                           proposal=umc.PROPOSAL_SPHERE, wolff_axis=umc.AXIS_SPHERE, seed=1)
+    other_coupling = umc.Chain(umc.MODEL_VECTOR, graph=umc.cubic_lattice(8, 8, 8), components=3, coupling=0.5,
+                               proposal=umc.PROPOSAL_SPHERE, wolff_axis=umc.AXIS_SPHERE, seed=1)
+    ising = _make(umc, "ising", 1)
+    for ch in (other_size, other_coupling, ising):
+        with pytest.raises(ValueError):
+            ch.restore(image)
+    damaged = bytearray(image)
+    damaged[0] ^= 0xFF
+    with pytest.raises(ValueError):
+        a.restore(bytes(damaged))
+    with pytest.raises(ValueError):
+        a.restore(image[:-4])
+    # the refused restores left the chain as it was
+    np.testing.assert_array_equal(np.frombuffer(a.checkpoint(), np.uint8), np.frombuffer(image, np.uint8))

@@ -145,6 +145,9 @@ _decl("umc_chain_destroy", _int, _vp)
 _decl("umc_chain_set_field", _int, _vp, _vp)
 _decl("umc_chain_get_field", _int, _vp, _vp)
 _decl("umc_chain_upload_async", _int, _vp, _vp)
+_decl("umc_chain_checkpoint_bytes", _int, _vp, C.POINTER(_u64))
+_decl("umc_chain_checkpoint", _int, _vp, _vp, _u64)
+_decl("umc_chain_restore", _int, _vp, _vp, _u64)
 _decl("umc_chain_set_record_streaming", _int, _vp, _int)
 _decl("umc_chain_randomize", _int, _vp, _u64)
 _decl("umc_chain_set_proposal", _int, _vp, _i32, _f64, _u32)
@@ -466,6 +469,27 @@ class Chain:
             raise ValueError(f"field has {a.size} scalars, expected {self.n * self.comps}")
         check(lib.umc_chain_upload_async(self._h, _ptr(a)))
         self._inflight.append(a)
+
+    def checkpoint(self) -> bytes:
+        """umc_chain_checkpoint: header + field; restore() continues the chain
+        exactly, in this process or another."""
+        n = _u64(0)
+        check(lib.umc_chain_checkpoint_bytes(self._h, C.byref(n)))
+        buf = np.zeros(n.value, np.uint8)
+        check(lib.umc_chain_checkpoint(self._h, _ptr(buf), n.value))
+        return buf.tobytes()
+
+    def restore(self, image: bytes) -> None:
+        buf = np.frombuffer(image, np.uint8)
+        check(lib.umc_chain_restore(self._h, _ptr(buf), buf.size))
+
+    def save(self, path) -> None:
+        with open(path, "wb") as f:
+            f.write(self.checkpoint())
+
+    def load(self, path) -> None:
+        with open(path, "rb") as f:
+            self.restore(f.read())
 
     def set_record_streaming(self, enable: bool) -> None:
         check(lib.umc_chain_set_record_streaming(self._h, int(enable)))

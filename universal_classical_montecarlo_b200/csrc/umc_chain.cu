@@ -1104,6 +1104,94 @@ int umc_chain_set_field(umc_chain* c, const void* host_field)
     });
 }
 
+namespace {
+// Checkpoint image: this header, then the field in the reference's data()
+// layout.  Fixed-width fields, little-endian as the host writes them.
+struct CheckpointHeader
+{
+    char magic[8];  // "UMCCHK01"
+    uint32_t version;
+    int32_t model;
+    int32_t components;
+    uint32_t hits;
+    uint64_t n;
+    uint64_t field_bytes;
+    uint64_t seed, sweeps, flips;
+    double coupling, width;
+    int32_t proposal, wolff_axis;
+};
+static_assert(sizeof(CheckpointHeader) == 88, "checkpoint header layout");
+constexpr char kCheckpointMagic[8] = {'U', 'M', 'C', 'C', 'H', 'K', '0', '1'};
+
+uint64_t host_field_bytes(const umc_chain* c) { return c->n * c->comps * c->elem_bytes; }
+}  // namespace
+
+int umc_chain_checkpoint_bytes(const umc_chain* c, uint64_t* bytes)
+{
+    return guarded([&] {
+        if (!c || !bytes) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        *bytes = sizeof(CheckpointHeader) + host_field_bytes(c);
+    });
+}
+
+int umc_chain_checkpoint(umc_chain* c, void* buffer, uint64_t capacity)
+{
+    return guarded([&] {
+        if (!c || !buffer) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        const uint64_t fb = host_field_bytes(c);
+        if (capacity < sizeof(CheckpointHeader) + fb)
+            throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint buffer too small (see umc_chain_checkpoint_bytes)");
+        CheckpointHeader h{};
+        std::memcpy(h.magic, kCheckpointMagic, 8);
+        h.version = 1;
+        h.model = c->model;
+        h.components = c->N;
+        h.hits = c->desc.hits;
+        h.n = c->n;
+        h.field_bytes = fb;
+        h.seed = c->desc.seed;
+        h.sweeps = c->sweeps;
+        h.flips = c->flips;
+        h.coupling = c->desc.coupling;
+        h.width = c->desc.width;
+        h.proposal = c->desc.proposal;
+        h.wolff_axis = c->desc.wolff_axis;
+        uint8_t* out = static_cast<uint8_t*>(buffer);
+        const int st = umc_chain_get_field(c, out + sizeof h);
+        if (st != UMC_OK) throw Error(st, umc_last_error());
+        std::memcpy(out, &h, sizeof h);
+    });
+}
+
+int umc_chain_restore(umc_chain* c, const void* buffer, uint64_t bytes)
+{
+    return guarded([&] {
+        if (!c || !buffer) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (bytes < sizeof(CheckpointHeader)) throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint too short");
+        CheckpointHeader h;
+        std::memcpy(&h, buffer, sizeof h);
+        if (std::memcmp(h.magic, kCheckpointMagic, 8) != 0 || h.version != 1)
+            throw Error(UMC_ERR_INVALID_ARGUMENT, "not a chain checkpoint (magic or version)");
+        if (h.model != c->model || h.components != c->N || h.n != c->n)
+            throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint is of another model, component count or lattice size");
+        if (h.field_bytes != host_field_bytes(c) || bytes < sizeof h + h.field_bytes)
+            throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint field size does not match the chain");
+        if (h.coupling != c->desc.coupling)
+            throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint coupling differs from the chain's");
+        validate_proposal(c, h.proposal, h.width, h.hits);
+        validate_axis(c, h.wolff_axis);
+        const int st = umc_chain_set_field(c, static_cast<const uint8_t*>(buffer) + sizeof h);
+        if (st != UMC_OK) throw Error(st, umc_last_error());
+        c->desc.proposal = h.proposal;
+        c->desc.width = h.width;
+        c->desc.hits = h.hits;
+        c->desc.wolff_axis = h.wolff_axis;
+        c->desc.seed = h.seed;
+        c->sweeps = h.sweeps;
+        c->flips = h.flips;
+    });
+}
+
 int umc_chain_upload_async(umc_chain* c, const void* host_field)
 {
     return guarded([&] {
