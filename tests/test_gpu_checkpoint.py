@@ -69,3 +69,26 @@ def test_mismatched_or_damaged_images_are_refused(umc):
         a.restore(image[:-4])
     # the refused restores left the chain as it was
     np.testing.assert_array_equal(np.frombuffer(a.checkpoint(), np.uint8), np.frombuffer(image, np.uint8))
+
+
+def test_learned_batch_and_network_continue_exactly(umc, tmp_path):
+    """The C5 state -- the batch's angles and sweep counter, and the network --
+    saved mid-run and loaded into fresh objects continues the learned sweeps
+    bit for bit."""
+    a = umc.U1Batch(8, 16, 3.0, width=0.5, seed=4)
+    a.run(30, records=False)
+    net = umc.ProposalNet(5)
+    a.save(tmp_path / "batch.npz")
+    net.save(tmp_path / "net.npy")
+    ra = a.run(10, net)
+    b = umc.U1Batch(8, 16, 3.0, width=0.5, seed=4)
+    b.load(tmp_path / "batch.npz")
+    net2 = umc.ProposalNet(77)
+    net2.load(tmp_path / "net.npy")
+    rb = b.run(10, net2)
+    np.testing.assert_array_equal(ra, rb)
+    for c in range(8):
+        np.testing.assert_array_equal(a.get_field(c), b.get_field(c))
+    other = umc.U1Batch(8, 16, 3.0, width=0.5, seed=5)
+    with pytest.raises(ValueError):
+        other.load(tmp_path / "batch.npz")

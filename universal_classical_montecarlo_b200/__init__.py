@@ -756,6 +756,13 @@ class ProposalNet:
     def __del__(self):
         self.close()
 
+    def save(self, path) -> None:
+        """The network's parameters (.npy); load() sets them (and resets Adam)."""
+        np.save(path, self.get_params())
+
+    def load(self, path) -> None:
+        self.set_params(np.load(path))
+
     def set_params(self, p):
         a = np.ascontiguousarray(p, np.float32)
         if a.size != MLP_PARAMS:
@@ -869,6 +876,24 @@ class U1Batch:
         s, k = _u64(0), _u64(0)
         check(lib.umc_u1batch_counters(self._h, C.byref(s), C.byref(k)))
         return s.value, k.value
+
+    def save(self, path) -> None:
+        """Every chain's angles, the sweep counter and the chain seeds (.npz).
+        load() into a batch made with the same chains, L, beta, width and seed
+        continues it exactly."""
+        np.savez(path, theta=np.stack([self.get_field(c) for c in range(self.n_chains)]),
+                 sweeps=np.uint64(self.counters()[0]), seeds=self.seeds(),
+                 shape=np.array([self.n_chains, self.L], np.uint64), beta=np.float64(self.beta),
+                 width=np.float64(self.width))
+
+    def load(self, path) -> None:
+        z = np.load(path)
+        if (tuple(int(v) for v in z["shape"]) != (self.n_chains, self.L) or float(z["beta"]) != self.beta
+                or float(z["width"]) != self.width or not np.array_equal(z["seeds"], self.seeds())):
+            raise ValueError("checkpoint is of another batch (chains, L, beta, width or seed)")
+        for c in range(self.n_chains):
+            self.set_field(c, z["theta"][c])
+        self.set_counter(int(z["sweeps"]))
 
     def set_counter(self, sweeps):
         check(lib.umc_u1batch_set_counter(self._h, sweeps))
