@@ -301,6 +301,11 @@ int umc_batch_run(umc_batch* b, uint64_t n_segments, double* records);
 int umc_batch_counters(const umc_batch* b, uint64_t* sweeps, uint64_t* rounds, uint64_t* swaps_accepted);
 /* holder[l * replicas + k] = chain at slot k of ladder l. */
 int umc_batch_temperature_map(const umc_batch* b, uint32_t* holder);
+/* Sets the counters and the temperature map (holder as above, a permutation
+ * of each ladder's chains), so that a batch created with the same description
+ * and given the same fields continues a saved run exactly (engine extension;
+ * the reference has no batches). */
+int umc_batch_set_state(umc_batch* b, uint64_t sweeps, uint64_t rounds, uint64_t swaps_accepted, const uint32_t* holder);
 /* chain_seeds[c] keys chain c's site streams; ladder_seeds[l] its swaps. */
 int umc_batch_seeds(const umc_batch* b, uint64_t* chain_seeds, uint64_t* ladder_seeds);
 /* Launch shape the autotuner chose for the ladders of side L. */

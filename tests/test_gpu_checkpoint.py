@@ -92,3 +92,27 @@ def test_learned_batch_and_network_continue_exactly(umc, tmp_path):
     other = umc.U1Batch(8, 16, 3.0, width=0.5, seed=5)
     with pytest.raises(ValueError):
         other.load(tmp_path / "batch.npz")
+
+
+def test_replica_exchange_batch_continues_exactly(umc, tmp_path):
+    """Fields, counters and the temperature map saved after some exchange
+    rounds and loaded into a fresh batch continue the ladders exactly; a
+    holder that is not a permutation of a ladder's chains is refused."""
+    Ls = np.array([16, 32])
+    betas = np.stack([np.geomspace(0.8, 1.3, 4)] * 2)
+    a = umc.Batch(Ls, betas, width=1.0, sweeps_per_exchange=3, seed=9)
+    a.randomize(2)
+    a.run(5)
+    a.save(tmp_path / "ladders.npz")
+    ra = a.run(4)
+    b = umc.Batch(Ls, betas, width=1.0, sweeps_per_exchange=3, seed=9)
+    b.load(tmp_path / "ladders.npz")
+    rb = b.run(4)
+    np.testing.assert_array_equal(ra, rb)
+    np.testing.assert_array_equal(a.temperature_map(), b.temperature_map())
+    assert a.counters() == b.counters()
+    for c in range(a.n_chains):
+        np.testing.assert_array_equal(a.get_field(c), b.get_field(c))
+    bad = np.arange(8, dtype=np.uint32)[::-1].copy()  # swaps chains across ladders
+    with pytest.raises(ValueError):
+        umc.check(umc.lib.umc_batch_set_state(b._h, 0, 0, 0, bad.ctypes.data_as(umc._vp)))

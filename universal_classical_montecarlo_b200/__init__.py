@@ -145,6 +145,7 @@ _decl("umc_chain_destroy", _int, _vp)
 _decl("umc_chain_set_field", _int, _vp, _vp)
 _decl("umc_chain_get_field", _int, _vp, _vp)
 _decl("umc_chain_upload_async", _int, _vp, _vp)
+_decl("umc_batch_set_state", _int, _vp, _u64, _u64, _u64, _vp)
 _decl("umc_chain_checkpoint_bytes", _int, _vp, C.POINTER(_u64))
 _decl("umc_chain_checkpoint", _int, _vp, _vp, _u64)
 _decl("umc_chain_restore", _int, _vp, _vp, _u64)
@@ -665,6 +666,28 @@ class Batch:
         ls = np.zeros(self.n_ladders, np.uint64)
         check(lib.umc_batch_seeds(self._h, _ptr(cs), _ptr(ls)))
         return cs, ls
+
+    def save(self, path) -> None:
+        """Every chain's angles, the counters and the temperature map (.npz).
+        load() into a batch made with the same description continues it
+        exactly."""
+        s, r, w = self.counters()
+        cs, ls = self.seeds()
+        fields = {f"theta{c}": self.get_field(c) for c in range(self.n_chains)}
+        np.savez(path, counters=np.array([s, r, w], np.uint64), holder=self.temperature_map(), chain_seeds=cs,
+                 ladder_seeds=ls, L=self.L, betas=self.betas, **fields)
+
+    def load(self, path) -> None:
+        z = np.load(path)
+        cs, ls = self.seeds()
+        if (not np.array_equal(z["L"], self.L) or not np.array_equal(z["betas"], self.betas)
+                or not np.array_equal(z["chain_seeds"], cs) or not np.array_equal(z["ladder_seeds"], ls)):
+            raise ValueError("checkpoint is of another batch (sides, betas or seed)")
+        for c in range(self.n_chains):
+            self.set_field(c, z[f"theta{c}"])
+        s, r, w = (int(v) for v in z["counters"])
+        holder = np.ascontiguousarray(z["holder"], np.uint32).reshape(-1)
+        check(lib.umc_batch_set_state(self._h, s, r, w, _ptr(holder)))
 
     def config(self, L):
         a, b, c = _u32(0), _u32(0), _u32(0)

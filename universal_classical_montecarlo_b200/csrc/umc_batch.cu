@@ -813,6 +813,33 @@ int umc_batch_temperature_map(const umc_batch* b, uint32_t* holder)
     });
 }
 
+int umc_batch_set_state(umc_batch* b, uint64_t sweeps, uint64_t rounds, uint64_t swaps_accepted, const uint32_t* holder)
+{
+    return bguard([&] {
+        if (!b || !holder) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        batch_scope(b);
+        // holder must permute each ladder's own chains over its slots
+        std::vector<uint32_t> slot(b->n_chains, 0xFFFFFFFFu);
+        for (uint32_t l = 0; l < b->n_ladders; ++l)
+            for (uint32_t k = 0; k < b->R; ++k) {
+                const uint32_t c = holder[l * b->R + k];
+                if (c / b->R != l || c >= b->n_chains || slot[c] != 0xFFFFFFFFu)
+                    throw Error(UMC_ERR_INVALID_ARGUMENT, "holder is not a permutation of each ladder's chains");
+                slot[c] = k;
+            }
+        cuda_check(cudaStreamSynchronize(b->stream), "sync");
+        BatchCounters ctr{};
+        cuda_check(cudaMemcpy(&ctr, b->ctr.p, sizeof ctr, cudaMemcpyDeviceToHost), "counters");
+        ctr.sweep = sweeps;
+        ctr.round = rounds;
+        cuda_check(cudaMemcpy(b->ctr.p, &ctr, sizeof ctr, cudaMemcpyHostToDevice), "counters");
+        const unsigned long long sw = swaps_accepted;
+        cuda_check(cudaMemcpy(b->swaps.p, &sw, 8, cudaMemcpyHostToDevice), "swaps");
+        cuda_check(cudaMemcpy(b->holder_dev.p, holder, b->n_chains * 4, cudaMemcpyHostToDevice), "holders");
+        cuda_check(cudaMemcpy(b->slot_dev.p, slot.data(), b->n_chains * 4, cudaMemcpyHostToDevice), "slots");
+    });
+}
+
 int umc_batch_seeds(const umc_batch* b, uint64_t* chain_seeds, uint64_t* ladder_seeds)
 {
     return bguard([&] {
