@@ -49,8 +49,10 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", choices=["o3", "ising", "su3", "xybatch", "u1batch", "u1learned"], default="o3",
-                   help="o3: the headline configuration; ising / su3 / xybatch: secondary roofline runs; "
+    p.add_argument("--workload", choices=["o3", "ising", "su3", "xybatch", "u1batch", "u1learned", "userxy"],
+                   default="o3",
+                   help="o3: the headline configuration; ising / su3 / xybatch / userxy: secondary roofline runs "
+                        "(userxy: a user-written FP64 model through include/umc/device.cuh); "
                         "u1learned: the learned-proposal study (effective samples/s)")
     p.add_argument("--no-learned", action="store_true", help="skip the learned-proposal summary of the o3 line")
     return p.parse_args()
@@ -698,7 +700,145 @@ class U1LearnedSweep:
         return None
 
 
-WORKLOADS = {"o3": O3Hybrid, "ising": IsingSweep, "su3": SU3Sweep, "xybatch": XYBatch, "u1batch": U1LearnedSweep}
+# ------------------------------------------------ a user-written device model
+def _device_models_lib():
+    """examples/device_models/libumc_device_models.so (built when stale)."""
+    import ctypes as C
+
+    sys.path.insert(0, os.path.join(ROOT, "examples", "device_models"))
+    import build_device_models
+
+    lib = C.CDLL(build_device_models.build())
+    vp, d, u64 = C.c_void_p, C.c_double, C.c_uint64
+    lib.um_last_error.restype = C.c_char_p
+    lib.um_xy_session_create.argtypes = [vp, d, d, d, u64, C.POINTER(vp)]
+    lib.um_xy_session_destroy.argtypes = [vp]
+    lib.um_xy_session_stream.argtypes = [vp]
+    lib.um_xy_session_stream.restype = vp
+    lib.um_xy_session_set_field.argtypes = [vp, vp]
+    lib.um_xy_session_get_field.argtypes = [vp, vp]
+    lib.um_xy_session_enqueue.argtypes = [vp, u64]
+    lib.um_xy_session_set_timing.argtypes = [vp, C.c_int]
+    lib.um_xy_session_stats.argtypes = [vp, C.POINTER(u64), C.POINTER(d), C.c_int]
+    lib.um_xy_session_energy.argtypes = [vp, C.POINTER(d)]
+    lib.um_xy_session_counters.argtypes = [vp, C.POINTER(u64), C.POINTER(C.c_uint32)]
+    return lib
+
+
+class _SessionAsChain:
+    """The few chain methods the timing loop uses, for a device-model session."""
+
+    def __init__(self, wl):
+        self.wl = wl
+        self.pending = 0
+
+    def stream(self):
+        return self.wl.lib.um_xy_session_stream(self.wl.h)
+
+    def fetch(self, cap):
+        import numpy as np
+
+        self.kernel_stats(reset=False)  # waits for the stream, surfaces a device error
+        rec = np.zeros((self.pending, 1))
+        self.pending = 0
+        return rec, np.zeros(0, np.uint64)
+
+    def kernel_stats(self, reset=False):
+        import ctypes as C
+
+        n, ms = C.c_uint64(), C.c_double()
+        self.wl.call(self.wl.lib.um_xy_session_stats(self.wl.h, C.byref(n), C.byref(ms), int(reset)))
+        return {"metropolis_sweeps": (n.value, ms.value)}
+
+    def set_timing(self, on):
+        self.wl.call(self.wl.lib.um_xy_session_set_timing(self.wl.h, int(on)))
+
+
+class UserXY:
+    """A user-written model through include/umc/device.cuh: the XY model on
+    angles as PairModel<Angle, CosineTerm> with the AngleShift (U1Shift)
+    proposal, FP64, from examples/device_models/user_models.cu, on an L x L
+    square_lattice (CSR bond table), J=1, beta=1.1, width 1.0, random start;
+    step = one sweep = one cooperative launch of metropolis_sweeps.  The
+    reference runs the same model as PairModel<U1Dof, user term, PairGraph>
+    through its stock Metropolis driver."""
+
+    name = "userxy"
+    unit = "site-updates/s"
+    dtype = "f64"
+
+    def __init__(self, umc, args, rank, local):
+        import ctypes as C
+
+        import numpy as np
+
+        self.L = args.L if args.L != L_DEFAULT else 8192
+        self.n = self.L * self.L
+        self.lib = _device_models_lib()
+        self.g = umc.square_lattice(self.L, self.L)
+        h = C.c_void_p()
+        self.call(self.lib.um_xy_session_create(self.g._h, 1.0, 1.1, 1.0, 1 + rank, C.byref(h)))
+        self.h = h
+        self.theta = np.random.default_rng(5 + rank).uniform(-np.pi, np.pi, self.n)
+        self.call(self.lib.um_xy_session_set_field(self.h, self.theta.ctypes.data))
+        self.flush = self.n * 8 < (256 << 20)
+        self.ch = _SessionAsChain(self)
+
+    def call(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.um_last_error().decode())
+
+    def describe(self):
+        return (f"user-written XY PairModel (CosineTerm + AngleShift, FP64, examples/device_models) on "
+                f"{self.L}x{self.L} square_lattice, J=1, beta=1.1, width 1.0, random start; step = 1 Metropolis "
+                f"sweep (one launch of the generic device kernel over the 2 colour classes)")
+
+    def enqueue(self, k):
+        self.call(self.lib.um_xy_session_enqueue(self.h, k))
+        self.ch.pending += k
+
+    def units(self, rec, sizes):
+        return len(rec) * self.n
+
+    def bytes_per_launch(self, kind):
+        # per site-update: order 4 + offset 4 + 4 bonds 16 + field read as own
+        # and as a neighbour 16 + write 8 = 48 B
+        return 48.0 * self.n
+
+    def e2e(self, torch, K):
+        import ctypes as C
+
+        host = torch.from_numpy(self.theta.copy()).pin_memory()
+        e = C.c_double()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(K):
+            self.call(self.lib.um_xy_session_set_field(self.h, host.data_ptr()))
+            self.enqueue(1)
+            self.call(self.lib.um_xy_session_energy(self.h, C.byref(e)))
+        torch.cuda.synchronize()
+        self.ch.fetch(0)
+        blocks = min(1024, (self.n + 255) // 256)
+        return {"value": K * self.n / (time.perf_counter() - t0), "unit": self.unit,
+                "h2d_bytes_per_step": self.n * 8, "d2h_bytes_per_step": blocks * 8, "steps": K}
+
+    def cpu(self, seconds):
+        from oracle.oracle import Reference, have_reference
+
+        if not have_reference():
+            return None
+        r = Reference()
+        threads = cpu_threads()
+        su, sec = r.bench_xy(256, 1.1, 1.0, 1, 5, 1, 1)
+        sweeps = max(5, int(seconds * 5 / max(sec, 1e-4)))
+        su, sec = r.bench_xy(256, 1.1, 1.0, 1, sweeps, threads, 1)
+        return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                "sample": f"{sweeps} sweeps x {threads} independent 256x256 XY chains (reference PairModel<U1Dof, "
+                          f"user term> + U1Shift, stock driver), {sec:.1f} s"}
+
+
+WORKLOADS = {"o3": O3Hybrid, "ising": IsingSweep, "su3": SU3Sweep, "xybatch": XYBatch, "u1batch": U1LearnedSweep,
+             "userxy": UserXY}
 
 
 def run_learned(args):

@@ -1,0 +1,366 @@
+// User-written models driven on the GPU through umc/device.cuh, as a user of
+// the library would write them: three terms/models and two proposals with
+// __host__ __device__ members, none of them known to libumc_b200.
+//
+//   CosineTerm   -- pair term E = -J cos(ti - tj), the XY model on angles as a
+//                   PairModel (a user CellTerm of arity 2, term/cell.hpp:10-25);
+//   PlaquetteTerm-- U(1) plaquette beta (1 - cos(t0 + t1 - t2 - t3)), arity 4,
+//                   as a CellModel (term/plaquette.hpp:13-50);
+//   CubicHeisenberg -- a whole ModelLike (model.hpp:65-88) for the periodic
+//                   cubic O(3) model whose neighbours come from the site index,
+//                   with no bond table at all;
+//   AngleShift   -- U1Shift (dof/u1.hpp:35-50): remainder(t + w (2u - 1), 2 pi);
+//   Sphere3      -- UniformSphereN<3> (dof/vector.hpp:35-61).
+//
+// Exported with a C ABI for the Python tests and bench.py (ctypes): one-shot
+// runs (um_xy_pair, um_u1_cells, um_heisenberg_cubic) and a persistent XY
+// session (um_xy_session_*) whose launches bench.py times.
+#include <umc/device.cuh>
+
+#include <cmath>
+#include <cstdint>
+#include <string>
+
+namespace {
+
+using namespace umc::gpu::device;
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+struct Angle
+{
+    using dtype = double;
+    static constexpr std::size_t size = 1;
+};
+
+struct CosineTerm
+{
+    using dtype = double;
+    using energy_type = double;
+    static constexpr std::size_t arity = 2;
+    double J;
+
+    UMC_HD double energy(const double* const* l) const { return -J * cos(*l[0] - *l[1]); }
+    UMC_HD double delta(std::size_t which, const double* old, const double* nw, const double* const* l) const
+    {
+        const double fixed = *l[which == 0 ? 1 : 0];
+        return -J * (cos(*nw - fixed) - cos(*old - fixed));
+    }
+};
+
+struct PlaquetteTerm
+{
+    using dtype = double;
+    using energy_type = double;
+    static constexpr std::size_t arity = 4;
+    double beta;
+
+    UMC_HD static double plaq(const double* t) { return cos(t[0] + t[1] - t[2] - t[3]); }
+    UMC_HD double energy(const double* const* l) const
+    {
+        const double t[4] = {*l[0], *l[1], *l[2], *l[3]};
+        return beta * (1.0 - plaq(t));
+    }
+    UMC_HD double delta(std::size_t which, const double*, const double* nw, const double* const* l) const
+    {
+        double t[4] = {*l[0], *l[1], *l[2], *l[3]};
+        const double before = plaq(t);
+        t[which] = *nw;
+        return beta * (before - plaq(t));
+    }
+};
+
+struct AngleShift
+{
+    double width;
+
+    template <class R>
+    UMC_HD void sample(const double* cur, R& rng, double* out) const
+    {
+        const double shift = width * (2.0 * rng.uni() - 1.0);
+        out[0] = remainder(cur[0] + shift, 2.0 * kPi);
+    }
+    UMC_HD double log_ratio(const double*, const double*) const { return 0.0; }
+};
+
+struct Sphere3
+{
+    template <class R>
+    UMC_HD void sample(const double*, R& rng, double* out) const
+    {
+        const double z = 2.0 * rng.uni() - 1.0;
+        const double r = sqrt(1.0 - z * z);
+        const double phi = 2.0 * kPi * rng.uni();
+        out[0] = cos(phi) * r;
+        out[1] = sin(phi) * r;
+        out[2] = z;
+    }
+    UMC_HD double log_ratio(const double*, const double*) const { return 0.0; }
+};
+
+// Periodic Lx x Ly x Lz O(3) model, E = -J sum_<ij> S_i . S_j, site
+// (z Ly + y) Lx + x; bonds to +-x, +-y, +-z computed from the index.
+struct CubicHeisenberg
+{
+    using value_type = double;
+    static constexpr std::size_t size = 3;
+    double* s;
+    std::uint32_t Lx, Ly, Lz;
+    double J;
+
+    UMC_HD std::size_t sites() const { return std::size_t(Lx) * Ly * Lz; }
+    UMC_HD const double* data() const { return s; }
+    UMC_HD double* data() { return s; }
+    UMC_HD static double dot(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+    UMC_HD double energy_diff_at(std::size_t i, const double* p) const
+    {
+        const std::uint32_t x = std::uint32_t(i % Lx), y = std::uint32_t((i / Lx) % Ly),
+                            z = std::uint32_t(i / (std::size_t(Lx) * Ly));
+        const std::size_t nb[6] = {site((x + 1) % Lx, y, z), site((x + Lx - 1) % Lx, y, z),
+                                   site(x, (y + 1) % Ly, z), site(x, (y + Ly - 1) % Ly, z),
+                                   site(x, y, (z + 1) % Lz), site(x, y, (z + Lz - 1) % Lz)};
+        const double* cur = s + i * 3;
+        double d = 0.0;
+        for (int a = 0; a < 6; ++a) d += -J * (dot(p, s + nb[a] * 3) - dot(cur, s + nb[a] * 3));
+        return d;
+    }
+    UMC_HD double energy_at(std::size_t i) const
+    {
+        const std::uint32_t x = std::uint32_t(i % Lx), y = std::uint32_t((i / Lx) % Ly),
+                            z = std::uint32_t(i / (std::size_t(Lx) * Ly));
+        const double* cur = s + i * 3;
+        return -J * (dot(cur, s + site((x + 1) % Lx, y, z) * 3) + dot(cur, s + site(x, (y + 1) % Ly, z) * 3) +
+                     dot(cur, s + site(x, y, (z + 1) % Lz) * 3));
+    }
+    UMC_HD void update(std::size_t i, const double* p)
+    {
+        for (int k = 0; k < 3; ++k) s[i * 3 + k] = p[k];
+    }
+    UMC_HD std::size_t site(std::uint32_t x, std::uint32_t y, std::uint32_t z) const
+    {
+        return (std::size_t(z) * Ly + y) * Lx + x;
+    }
+};
+
+static_assert(ModelLike<CubicHeisenberg> && EnergyModel<CubicHeisenberg>);
+static_assert(CellTerm<CosineTerm, Angle> && CellTerm<PlaquetteTerm, Angle>);
+static_assert(Proposal<AngleShift, double> && Proposal<Sphere3, double>);
+
+thread_local std::string g_error;
+
+template <class F>
+int guarded(F&& f)
+{
+    try {
+        f();
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* um_last_error(void) { return g_error.c_str(); }
+
+// XY PairModel on a library pair graph: n_sweeps through sample(), recording
+// energy_at_sum / 2 after every sweep; theta (sites) in/out.
+int um_xy_pair(const umc_graph* g, double J, double beta, double width, std::uint64_t seed, std::uint64_t sweep0,
+               std::uint32_t n_sweeps, double* theta, double* energies, std::uint32_t* grid)
+{
+    return guarded([&] {
+        PairTables t(g);
+        Buffer<double> field(t.sites());
+        field.upload(theta);
+        auto model = t.model<Angle>(field.data(), CosineTerm{J});
+        Metropolis<decltype(model), AngleShift> mc(model, AngleShift{width}, t.classes(), seed, beta);
+        mc.set_sweeps(sweep0);
+        std::uint32_t k = 0;
+        mc.sample(n_sweeps, [&](const auto& m) { energies[k++] = 0.5 * m.energy_at_sum(); });
+        field.download(theta);
+        if (grid) *grid = mc.grid();
+    });
+}
+
+// U(1) CellModel on a library cell complex, n_sweeps in one launch; the total
+// energy sum_c beta (1 - P_c) afterwards.
+int um_u1_cells(const umc_cells* cc, double model_beta, double beta, double width, std::uint64_t seed,
+                std::uint64_t sweep0, std::uint32_t n_sweeps, double* theta, double* total_energy)
+{
+    return guarded([&] {
+        CellTables t(cc);
+        Buffer<double> field(t.sites());
+        field.upload(theta);
+        auto model = t.model<Angle>(field.data(), PlaquetteTerm{model_beta});
+        Metropolis<decltype(model), AngleShift> mc(model, AngleShift{width}, t.classes(), seed, beta);
+        mc.set_sweeps(sweep0);
+        mc.run(n_sweeps);
+        *total_energy = mc.total_energy();
+        field.download(theta);
+    });
+}
+
+// Table-free O(3) ModelLike on a periodic cubic lattice (even extents),
+// checkerboard classes; spins (sites x 3) in/out.
+int um_heisenberg_cubic(std::uint32_t Lx, std::uint32_t Ly, std::uint32_t Lz, double J, double beta,
+                        std::uint64_t seed, std::uint64_t sweep0, std::uint32_t n_sweeps, double* spins,
+                        double* energy)
+{
+    return guarded([&] {
+        const std::size_t n = std::size_t(Lx) * Ly * Lz;
+        std::vector<std::uint32_t> colour(n);
+        for (std::size_t i = 0; i < n; ++i) colour[i] = std::uint32_t((i % Lx + (i / Lx) % Ly + i / (std::size_t(Lx) * Ly)) & 1u);
+        ClassTable classes(Classes::from_colours(colour, 2));
+        Buffer<double> field(n * 3);
+        field.upload(spins);
+        CubicHeisenberg model{field.data(), Lx, Ly, Lz, J};
+        Metropolis<CubicHeisenberg, Sphere3> mc(model, Sphere3{}, classes, seed, beta);
+        mc.set_sweeps(sweep0);
+        mc.run(n_sweeps);
+        *energy = mc.energy_at_sum();
+        field.download(spins);
+    });
+}
+
+}  // extern "C"
+
+// ---- persistent XY session: tables, field and driver stay on the device
+namespace {
+struct XYSession
+{
+    static cudaStream_t make_stream()
+    {
+        cudaStream_t s = nullptr;
+        cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+        return s;
+    }
+    XYSession(const umc_graph* g, double J, double beta, double width, std::uint64_t seed)
+        : tables(g), field(tables.sites()), stream(make_stream()),
+          mc(tables.model<Angle>(field.data(), CosineTerm{J}), AngleShift{width}, tables.classes(), seed, beta, stream)
+    {}
+    ~XYSession()
+    {
+        for (auto& e : pending) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        cudaStreamDestroy(stream);
+    }
+    void fold()
+    {
+        cuda_check(cudaStreamSynchronize(stream), "sync");
+        for (auto& e : pending) {
+            float ms = 0.f;
+            cuda_check(cudaEventElapsedTime(&ms, e.first, e.second), "event");
+            timed_ms += ms;
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        pending.clear();
+    }
+
+    PairTables tables;
+    Buffer<double> field;
+    cudaStream_t stream;
+    Metropolis<PairModel<Angle, CosineTerm>, AngleShift> mc;
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    std::uint64_t launches = 0;
+    double timed_ms = 0.0;
+};
+}  // namespace
+
+extern "C" {
+
+int um_xy_session_create(const umc_graph* g, double J, double beta, double width, std::uint64_t seed, void** out)
+{
+    return guarded([&] { *out = new XYSession(g, J, beta, width, seed); });
+}
+
+void um_xy_session_destroy(void* h) { delete static_cast<XYSession*>(h); }
+
+void* um_xy_session_stream(void* h) { return static_cast<XYSession*>(h)->stream; }
+
+// Field from/to host memory (sites doubles), ordered on the session's stream.
+int um_xy_session_set_field(void* h, const double* theta)
+{
+    return guarded([&] {
+        auto* s = static_cast<XYSession*>(h);
+        s->field.upload_async(theta, s->stream);
+    });
+}
+int um_xy_session_get_field(void* h, double* theta)
+{
+    return guarded([&] {
+        auto* s = static_cast<XYSession*>(h);
+        s->field.download_async(theta, s->stream);
+        cuda_check(cudaStreamSynchronize(s->stream), "sync");
+    });
+}
+
+// n sweeps in one launch, not waited for; with timing on, CUDA events bracket it.
+int um_xy_session_enqueue(void* h, std::uint64_t sweeps)
+{
+    return guarded([&] {
+        auto* s = static_cast<XYSession*>(h);
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (s->timing) {
+            cuda_check(cudaEventCreate(&a), "event");
+            cuda_check(cudaEventCreate(&b), "event");
+            cuda_check(cudaEventRecord(a, s->stream), "event");
+        }
+        s->mc.enqueue(sweeps);
+        s->launches += (sweeps + (1u << 30) - 1) >> 30;
+        if (s->timing) {
+            cuda_check(cudaEventRecord(b, s->stream), "event");
+            s->pending.emplace_back(a, b);
+        }
+    });
+}
+
+int um_xy_session_set_timing(void* h, int on)
+{
+    return guarded([&] {
+        auto* s = static_cast<XYSession*>(h);
+        s->fold();
+        s->timing = on != 0;
+    });
+}
+
+// Waits for the stream; launches of metropolis_sweeps and their event time
+// (timed launches only) since the last reset; throws if a barrier wait ran out.
+int um_xy_session_stats(void* h, std::uint64_t* launches, double* ms, int reset)
+{
+    return guarded([&] {
+        auto* s = static_cast<XYSession*>(h);
+        s->fold();
+        s->mc.check();
+        *launches = s->launches;
+        *ms = s->timed_ms;
+        if (reset) {
+            s->launches = 0;
+            s->timed_ms = 0.0;
+        }
+    });
+}
+
+// Total energy (sum of energy_at / 2, FP64) of the current field.
+int um_xy_session_energy(void* h, double* e)
+{
+    return guarded([&] { *e = 0.5 * static_cast<XYSession*>(h)->mc.energy_at_sum(); });
+}
+
+int um_xy_session_counters(void* h, std::uint64_t* sweeps, std::uint32_t* grid)
+{
+    return guarded([&] {
+        auto* s = static_cast<XYSession*>(h);
+        *sweeps = s->mc.sweeps();
+        *grid = s->mc.grid();
+    });
+}
+
+}  // extern "C"

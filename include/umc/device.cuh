@@ -1,0 +1,707 @@
+// umc/device.cuh -- user-written models on the GPU.
+//
+// The reference's ModelLike concept (model.hpp:65-88) keeps a model a plain
+// struct "so the same definition can be copied to a device and driven by a
+// kernel".  This header is that kernel: a translation unit compiled by nvcc
+// includes it, writes its terms, proposals or whole models with __host__
+// __device__ members (UMC_HD), and drives them with device::Metropolis, the
+// single-site driver of driver.hpp:17-66 run over colour classes.  Tables
+// (PairGraph CSR, CellComplex cells and incidence, colourings) come from
+// libumc_b200.so; the update loop is instantiated for the user's types here.
+//
+//   * PairModel<D, Term>   -- model/pair.hpp:18-80 over a CSR bond table, for any
+//                             arity-2 CellTerm (term/cell.hpp:10-25);
+//   * CellModel<D, Term>   -- model/cell.hpp:16-99 over a cell table;
+//   * any other M          -- a user struct with value_type, size, sites(),
+//                             data(), energy_diff_at(loc, p) and update(loc, p)
+//                             (model.hpp:65-88), e.g. neighbours computed from
+//                             the site index instead of read from a table;
+//   * proposals            -- sample(cur, rng, out) and log_ratio(cur, out)
+//                             (dof/proposal.hpp:5-11); rng.uni() is Pcg32::uni
+//                             (rng.hpp:22-26).
+//
+// Update order and random numbers.  The reference sweeps sites 0..n-1 from one
+// sequential Pcg32.  Here a sweep visits the colour classes in order (no two
+// sites of a class interact, so a class updates in parallel) and site i draws
+// from its own counter-keyed stream Pcg32(id_seed(key_seed(seed, sweep,
+// tag_site(0)), k), 0), k = i's colour-major index.  The result equals the
+// reference driver run on the graph relabelled to colour-major order with
+// that keying, which is how the library's own chains are checked.
+//
+// One launch runs any number of sweeps: a cooperative persistent kernel whose
+// blocks meet at a grid barrier between classes.  The barrier's waits are
+// bounded; a wait that runs out sets a status bit, every block returns, and
+// the host call throws.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <umc_b200.h>
+#include <umc/keyed_pcg.cuh>
+
+#include <algorithm>
+#include <concepts>
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+namespace umc::gpu::device {
+
+// ------------------------------------------------------------------ errors
+
+inline void cuda_check(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+inline void umc_check(int status)
+{
+    if (status != UMC_OK) throw std::runtime_error("umc status " + std::to_string(status) + ": " + umc_last_error());
+}
+
+// ------------------------------------------------------------------ buffers
+
+// Device array of n T, freed on destruction; moved, never copied.
+template <class T>
+class Buffer
+{
+public:
+    Buffer() = default;
+    explicit Buffer(std::size_t n) : n_(n)
+    {
+        if (n) cuda_check(cudaMalloc(&p_, n * sizeof(T)), "cudaMalloc");
+    }
+    explicit Buffer(const std::vector<T>& host) : Buffer(host.size()) { upload(host.data()); }
+    ~Buffer()
+    {
+        if (p_) cudaFree(p_);
+    }
+    Buffer(const Buffer&) = delete;
+    Buffer& operator=(const Buffer&) = delete;
+    Buffer(Buffer&& o) noexcept : p_(std::exchange(o.p_, nullptr)), n_(std::exchange(o.n_, 0)) {}
+    Buffer& operator=(Buffer&& o) noexcept
+    {
+        if (this != &o) {
+            if (p_) cudaFree(p_);
+            p_ = std::exchange(o.p_, nullptr);
+            n_ = std::exchange(o.n_, 0);
+        }
+        return *this;
+    }
+
+    T* data() noexcept { return p_; }
+    const T* data() const noexcept { return p_; }
+    std::size_t size() const noexcept { return n_; }
+
+    void upload(const T* host) { cuda_check(cudaMemcpy(p_, host, n_ * sizeof(T), cudaMemcpyHostToDevice), "upload"); }
+    void download(T* host) const
+    {
+        cuda_check(cudaMemcpy(host, p_, n_ * sizeof(T), cudaMemcpyDeviceToHost), "download");
+    }
+    // Ordered on stream s; host must stay valid (pinned for overlap) until then.
+    void upload_async(const T* host, cudaStream_t s)
+    {
+        cuda_check(cudaMemcpyAsync(p_, host, n_ * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+    }
+    void download_async(T* host, cudaStream_t s) const
+    {
+        cuda_check(cudaMemcpyAsync(host, p_, n_ * sizeof(T), cudaMemcpyDeviceToHost, s), "download");
+    }
+    std::vector<T> to_host() const
+    {
+        std::vector<T> h(n_);
+        download(h.data());
+        return h;
+    }
+
+private:
+    T* p_ = nullptr;
+    std::size_t n_ = 0;
+};
+
+// ------------------------------------------------------------------ random numbers
+
+// The proposal's rng argument: one counter-keyed reference Pcg32.
+class Rng
+{
+public:
+    UMC_HD explicit Rng(KeyedPcg g) : g_(g) {}
+    // Pcg32::uni, rng.hpp:22-26: k * 2^-32, in [0, 1).
+    UMC_HD double uni() { return double(g_.next()) * 0x1.0p-32; }
+
+private:
+    KeyedPcg g_;
+};
+
+// ------------------------------------------------------------------ concepts
+
+// dof/dof.hpp:8-12
+template <class D>
+concept Dof = requires {
+    typename D::dtype;
+    { D::size } -> std::convertible_to<std::size_t>;
+};
+
+// term/cell.hpp:10-25; the members must be callable on the device.
+template <class Term, class D>
+concept CellTerm = Dof<D> && requires {
+    typename Term::dtype;
+    typename Term::energy_type;
+    { Term::arity } -> std::convertible_to<std::size_t>;
+    requires(Term::arity >= 1);
+    requires std::same_as<typename Term::dtype, typename D::dtype>;
+} && requires(const Term term, const typename D::dtype* const* links, const typename D::dtype* old,
+              const typename D::dtype* nw) {
+    { term.energy(links) } -> std::convertible_to<typename Term::energy_type>;
+    { term.delta(std::size_t{}, old, nw, links) } -> std::convertible_to<typename Term::energy_type>;
+};
+
+// model.hpp:65-88.  A model crosses to the device by value: it holds device
+// pointers, never owning containers.
+template <class M>
+concept ModelLike = std::is_trivially_copyable_v<M> &&
+                    requires(const M cm, M m, std::size_t loc, const typename M::value_type* p) {
+                        typename M::value_type;
+                        { M::size } -> std::convertible_to<std::size_t>;
+                        { cm.sites() } -> std::convertible_to<std::size_t>;
+                        { cm.data() } -> std::convertible_to<const typename M::value_type*>;
+                        { cm.energy_diff_at(loc, p) } -> std::convertible_to<double>;
+                        { m.update(loc, p) } -> std::same_as<void>;
+                    };
+
+// dof/proposal.hpp:5-11 with this header's Rng.
+template <class Q, class T>
+concept Proposal = std::is_trivially_copyable_v<Q> && requires(const Q& q, const T* cur, T* out, Rng& rng) {
+    { q.sample(cur, rng, out) };
+    { q.log_ratio(cur, out) } -> std::convertible_to<double>;
+};
+
+// model.hpp:93-96
+template <class M>
+concept EnergyModel = ModelLike<M> && requires(const M cm, std::size_t loc) {
+    { cm.energy_at(loc) } -> std::convertible_to<double>;
+};
+
+// model/cell.hpp:52-62: per-cell energies that sum to the total.
+template <class M>
+concept CellEnergyModel = ModelLike<M> && requires(const M cm, std::size_t c) {
+    { cm.cells() } -> std::convertible_to<std::size_t>;
+    { cm.cell_energy(c) } -> std::convertible_to<double>;
+};
+
+// ------------------------------------------------------------------ colour classes
+
+// Sites grouped by colour: order[begin[c] .. begin[c+1]) are the sites of
+// colour c, ascending.  The index k of a site in order is its colour-major
+// position, the id of its random stream.
+struct Classes
+{
+    std::vector<std::uint32_t> order;
+    std::vector<std::uint32_t> begin;
+
+    std::uint32_t count() const { return std::uint32_t(begin.size() - 1); }
+    std::uint32_t largest() const
+    {
+        std::uint32_t m = 0;
+        for (std::uint32_t c = 0; c + 1 < begin.size(); ++c) m = std::max(m, begin[c + 1] - begin[c]);
+        return m;
+    }
+
+    // From colour[i] in [0, n_colours): within a colour, ascending site index.
+    static Classes from_colours(const std::vector<std::uint32_t>& colour, std::uint32_t n_colours)
+    {
+        Classes k;
+        k.begin.assign(std::size_t(n_colours) + 1, 0);
+        for (const auto c : colour) {
+            if (c >= n_colours) throw std::invalid_argument("colour out of range");
+            ++k.begin[c + 1];
+        }
+        for (std::uint32_t c = 0; c < n_colours; ++c) k.begin[c + 1] += k.begin[c];
+        std::vector<std::uint32_t> next(k.begin.begin(), k.begin.end() - 1);
+        k.order.resize(colour.size());
+        for (std::uint32_t i = 0; i < colour.size(); ++i) k.order[next[colour[i]]++] = i;
+        return k;
+    }
+    // The library's colouring of a pair graph (umc_graph_colouring).
+    static Classes of(const umc_graph* g)
+    {
+        const std::uint64_t n = umc_graph_sites(g);
+        std::uint32_t nc = 0;
+        std::vector<std::uint32_t> colour(n), pos(n);
+        umc_check(umc_graph_colouring(g, &nc, colour.data(), pos.data()));
+        return from_positions(colour, pos, nc);
+    }
+    // The library's colouring of a cell complex's sites (umc_cells_colouring).
+    static Classes of(const umc_cells* cc)
+    {
+        const std::uint64_t n = umc_cells_sites(cc);
+        std::uint32_t nc = 0;
+        std::vector<std::uint32_t> colour(n), pos(n);
+        umc_check(umc_cells_colouring(cc, &nc, colour.data(), pos.data()));
+        return from_positions(colour, pos, nc);
+    }
+
+private:
+    static Classes from_positions(const std::vector<std::uint32_t>& colour, const std::vector<std::uint32_t>& pos,
+                                  std::uint32_t nc)
+    {
+        Classes k = from_colours(colour, nc);
+        for (std::uint32_t i = 0; i < pos.size(); ++i) k.order[pos[i]] = i;
+        return k;
+    }
+};
+
+// Classes on the device.  Must outlive the drivers that use it.
+class ClassTable
+{
+public:
+    explicit ClassTable(Classes k)
+        : host_(std::move(k)), order_(host_.order), begin_(host_.begin)
+    {
+        if (host_.begin.size() < 2 || host_.begin.back() != host_.order.size())
+            throw std::invalid_argument("class table: begin does not cover order");
+    }
+    const Classes& host() const noexcept { return host_; }
+    const std::uint32_t* order() const noexcept { return order_.data(); }
+    const std::uint32_t* begin() const noexcept { return begin_.data(); }
+
+private:
+    Classes host_;
+    Buffer<std::uint32_t> order_, begin_;
+};
+
+// ------------------------------------------------------------------ table models
+
+// PairModel (model/pair.hpp:18-80) as a device view: the field and the CSR
+// bond table live on the device; Term is any arity-2 CellTerm.
+template <class D, class Term>
+    requires CellTerm<Term, D> && (Term::arity == 2)
+struct PairModel
+{
+    using dtype = typename D::dtype;
+    using value_type = dtype;
+    using energy_type = typename Term::energy_type;
+    static constexpr std::size_t size = D::size;
+
+    dtype* field;
+    const std::uint32_t* offset;  // sites + 1
+    const std::uint32_t* bonds;   // offset[sites]
+    std::uint32_t n;
+    Term term;
+
+    UMC_HD std::size_t sites() const { return n; }
+    UMC_HD const dtype* data() const { return field; }
+    UMC_HD dtype* data() { return field; }
+    UMC_HD std::size_t degree(std::size_t i) const { return offset[i + 1] - offset[i]; }
+
+    // model/pair.hpp:38-49: bonds incident to i, each counted once.
+    UMC_HD energy_type energy_at(std::size_t i) const
+    {
+        energy_type e = 0;
+        const dtype* si = field + i * size;
+        for (std::uint32_t a = offset[i]; a < offset[i + 1]; ++a) {
+            const dtype* links[2] = {si, field + std::size_t(bonds[a]) * size};
+            e += term.energy(links);
+        }
+        return e;
+    }
+    // model/pair.hpp:52-63
+    UMC_HD energy_type energy_diff_at(std::size_t i, const dtype* p) const
+    {
+        energy_type d = 0;
+        const dtype* si = field + i * size;
+        for (std::uint32_t a = offset[i]; a < offset[i + 1]; ++a) {
+            const dtype* links[2] = {si, field + std::size_t(bonds[a]) * size};
+            d += term.delta(0, si, p, links);
+        }
+        return d;
+    }
+    UMC_HD void update(std::size_t i, const dtype* p)
+    {
+        for (std::size_t k = 0; k < size; ++k) field[i * size + k] = p[k];
+    }
+};
+
+// CellModel (model/cell.hpp:16-99) as a device view over a cell table and the
+// per-site incidence (cell, slot) lists.
+template <class D, class Term>
+    requires CellTerm<Term, D>
+struct CellModel
+{
+    using dtype = typename D::dtype;
+    using value_type = dtype;
+    using energy_type = typename Term::energy_type;
+    static constexpr std::size_t size = D::size;
+    static constexpr std::size_t arity = Term::arity;
+
+    dtype* field;
+    const std::uint32_t* cell_sites;   // n_cells * arity
+    const std::uint64_t* inc_offset;   // sites + 1
+    const std::uint32_t* inc_cell;
+    const std::uint8_t* inc_which;
+    std::uint32_t n, n_cells;
+    Term term;
+
+    UMC_HD std::size_t sites() const { return n; }
+    UMC_HD std::size_t cells() const { return n_cells; }
+    UMC_HD const dtype* data() const { return field; }
+    UMC_HD dtype* data() { return field; }
+
+    // model/cell.hpp:52-56
+    UMC_HD energy_type cell_energy(std::size_t c) const
+    {
+        const dtype* ls[arity];
+        for (std::size_t k = 0; k < arity; ++k) ls[k] = field + std::size_t(cell_sites[c * arity + k]) * size;
+        return term.energy(ls);
+    }
+    // model/cell.hpp:64-78
+    UMC_HD energy_type energy_diff_at(std::size_t i, const dtype* p) const
+    {
+        energy_type d = 0;
+        const dtype* old = field + i * size;
+        const dtype* ls[arity];
+        for (std::uint64_t a = inc_offset[i]; a < inc_offset[i + 1]; ++a) {
+            const std::uint32_t* cs = cell_sites + std::size_t(inc_cell[a]) * arity;
+            for (std::size_t k = 0; k < arity; ++k) ls[k] = field + std::size_t(cs[k]) * size;
+            d += term.delta(inc_which[a], old, p, ls);
+        }
+        return d;
+    }
+    // model/cell.hpp:80-83
+    UMC_HD void update(std::size_t i, const dtype* p)
+    {
+        for (std::size_t k = 0; k < size; ++k) field[i * size + k] = p[k];
+    }
+};
+
+// A pair graph's CSR and colour classes on the device.
+class PairTables
+{
+public:
+    explicit PairTables(const umc_graph* g) : classes_(Classes::of(g))
+    {
+        n_ = std::uint32_t(umc_graph_sites(g));
+        std::vector<std::uint32_t> off(std::size_t(n_) + 1), bonds(umc_graph_slots(g));
+        umc_check(umc_graph_csr(g, off.data(), bonds.data()));
+        offset_ = Buffer<std::uint32_t>(off);
+        bonds_ = Buffer<std::uint32_t>(bonds);
+    }
+    std::uint32_t sites() const noexcept { return n_; }
+    const ClassTable& classes() const noexcept { return classes_; }
+
+    // A PairModel view over field (sites * D::size device scalars).
+    template <class D, class Term>
+    PairModel<D, Term> model(typename D::dtype* field, Term term) const
+    {
+        return PairModel<D, Term>{field, offset_.data(), bonds_.data(), n_, term};
+    }
+
+private:
+    ClassTable classes_;
+    std::uint32_t n_ = 0;
+    Buffer<std::uint32_t> offset_, bonds_;
+};
+
+// A cell complex's cells, incidence and colour classes on the device.
+class CellTables
+{
+public:
+    explicit CellTables(const umc_cells* cc) : classes_(Classes::of(cc))
+    {
+        n_ = std::uint32_t(umc_cells_sites(cc));
+        n_cells_ = std::uint32_t(umc_cells_count(cc));
+        arity_ = umc_cells_arity(cc);
+        std::vector<std::uint32_t> cells(std::size_t(n_cells_) * arity_);
+        umc_check(umc_cells_table(cc, cells.data()));
+        std::vector<std::uint64_t> off(std::size_t(n_) + 1);
+        umc_check(umc_cells_incidence(cc, off.data(), nullptr, nullptr));
+        std::vector<std::uint32_t> inc_cell(off.back());
+        std::vector<std::uint8_t> inc_which(off.back());
+        umc_check(umc_cells_incidence(cc, off.data(), inc_cell.data(), inc_which.data()));
+        cells_ = Buffer<std::uint32_t>(cells);
+        inc_offset_ = Buffer<std::uint64_t>(off);
+        inc_cell_ = Buffer<std::uint32_t>(inc_cell);
+        inc_which_ = Buffer<std::uint8_t>(inc_which);
+    }
+    std::uint32_t sites() const noexcept { return n_; }
+    std::uint32_t cells() const noexcept { return n_cells_; }
+    const ClassTable& classes() const noexcept { return classes_; }
+
+    template <class D, class Term>
+    CellModel<D, Term> model(typename D::dtype* field, Term term) const
+    {
+        if (Term::arity != arity_) throw std::invalid_argument("term arity differs from the cell table's");
+        return CellModel<D, Term>{field, cells_.data(), inc_offset_.data(), inc_cell_.data(), inc_which_.data(),
+                                  n_, n_cells_, term};
+    }
+
+private:
+    ClassTable classes_;
+    std::uint32_t n_ = 0, n_cells_ = 0, arity_ = 0;
+    Buffer<std::uint32_t> cells_;
+    Buffer<std::uint64_t> inc_offset_;
+    Buffer<std::uint32_t> inc_cell_;
+    Buffer<std::uint8_t> inc_which_;
+};
+
+// ------------------------------------------------------------------ kernels
+
+namespace detail {
+
+constexpr int kThreads = 256;
+constexpr unsigned kSpinLimit = 1u << 24;  // about a second of 64 ns sleeps
+
+struct Control
+{
+    unsigned count;       // blocks arrived at the current barrier
+    unsigned generation;  // barriers completed
+    unsigned status;      // bit 0: a barrier wait ran out
+    unsigned pad;
+};
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid barrier of a cooperative launch.  Returns false in every thread of
+// every block once any block's wait has run out.
+__device__ __forceinline__ bool grid_sync(Control* ctl)
+{
+    int fail = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = ld_acquire(&ctl->generation);
+        __threadfence();
+        if (atomicAdd(&ctl->count, 1u) == gridDim.x - 1) {
+            atomicExch(&ctl->count, 0u);
+            st_release(&ctl->generation, gen + 1);
+        } else {
+            unsigned spins = 0;
+            while (ld_acquire(&ctl->generation) == gen) {
+                if (ld_acquire(&ctl->status) != 0u || ++spins > kSpinLimit) {
+                    atomicOr(&ctl->status, 1u);
+                    fail = 1;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    return __syncthreads_or(fail) == 0;
+}
+
+// n_sweeps Metropolis sweeps (driver.hpp:29-43) over the colour classes.
+template <class M, class Q>
+__global__ void __launch_bounds__(kThreads) metropolis_sweeps(M m, Q q, const std::uint32_t* __restrict__ order,
+                                                              const std::uint32_t* __restrict__ begin,
+                                                              std::uint32_t n_classes, double beta, std::uint64_t seed,
+                                                              std::uint64_t sweep0, std::uint32_t n_sweeps,
+                                                              Control* ctl)
+{
+    using T = typename M::value_type;
+    const std::uint32_t stride = gridDim.x * blockDim.x;
+    const std::uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    for (std::uint32_t s = 0; s < n_sweeps; ++s) {
+        const std::uint64_t kbase = key_base(key_seed(seed, sweep0 + s, tag_site(0)));
+        for (std::uint32_t c = 0; c < n_classes; ++c) {
+            const std::uint32_t end = begin[c + 1];
+            for (std::uint32_t k = begin[c] + t; k < end; k += stride) {
+                const std::uint32_t i = order[k];
+                Rng rng(KeyedPcg::open(kbase, k));
+                T cand[M::size];
+                const T* cur = m.data() + std::size_t(i) * M::size;
+                q.sample(cur, rng, cand);
+                const double dE = m.energy_diff_at(i, cand);
+                const double log_p = -beta * dE + q.log_ratio(cur, cand);
+                if (log_p >= 0.0 || log(rng.uni()) < log_p) m.update(i, cand);
+            }
+            if ((s + 1 < n_sweeps || c + 1 < n_classes) && !grid_sync(ctl)) return;
+        }
+    }
+}
+
+// Per-block FP64 sums of f(m, x) over x < count; the host adds the blocks'
+// partials in block order.
+template <class M, class F>
+__global__ void __launch_bounds__(kThreads) block_sums(M m, std::uint64_t count, F f, double* partial)
+{
+    __shared__ double sh[kThreads];
+    double v = 0.0;
+    for (std::uint64_t x = blockIdx.x * std::uint64_t(blockDim.x) + threadIdx.x; x < count;
+         x += std::uint64_t(gridDim.x) * blockDim.x)
+        v += double(f(m, x));
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = kThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+struct CellEnergyOf
+{
+    template <class M>
+    __device__ double operator()(const M& m, std::uint64_t c) const
+    {
+        return double(m.cell_energy(c));
+    }
+};
+struct EnergyAtOf
+{
+    template <class M>
+    __device__ double operator()(const M& m, std::uint64_t i) const
+    {
+        return double(m.energy_at(i));
+    }
+};
+
+}  // namespace detail
+
+// ------------------------------------------------------------------ driver
+
+// Metropolis (driver.hpp:17-66) for a device model M and proposal Q.  The
+// reference's rng argument becomes a seed: every sweep keys its own streams
+// from (seed, sweep counter), so a chain continues exactly after
+// set_sweeps() and runs the same on any grid size.
+template <ModelLike M, class Q>
+    requires Proposal<Q, typename M::value_type>
+class Metropolis
+{
+public:
+    Metropolis(M model, Q proposal, const ClassTable& classes, std::uint64_t seed, double beta,
+               cudaStream_t stream = nullptr)
+        : model_(model), proposal_(proposal), classes_(classes), seed_(seed), beta_(beta), stream_(stream),
+          ctl_(1)
+    {
+        if (classes.host().order.size() != model.sites())
+            throw std::invalid_argument("colour classes do not cover the model's sites");
+        int dev = 0, sms = 0, per_sm = 0;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, detail::metropolis_sweeps<M, Q>,
+                                                                  detail::kThreads, 0),
+                   "occupancy");
+        if (per_sm < 1) throw std::runtime_error("Metropolis kernel does not fit on an SM");
+        const std::uint32_t need = (classes.host().largest() + detail::kThreads - 1) / detail::kThreads;
+        grid_ = std::max<std::uint32_t>(1, std::min<std::uint32_t>(need, std::uint32_t(per_sm) * sms));
+    }
+
+    // One pass over every site (driver.hpp:29-43).
+    void sweep() { run(1); }
+
+    // n passes (driver.hpp:46-50) in one launch; returns when they are done.
+    void run(std::size_t sweeps)
+    {
+        enqueue(sweeps);
+        cuda_check(cudaStreamSynchronize(stream_), "Metropolis::run");
+        check();
+    }
+
+    // Runs n sweeps, calling observe(*this) after each (driver.hpp:55-62).
+    template <class F>
+    void sample(std::size_t sweeps, F&& observe)
+    {
+        for (std::size_t k = 0; k < sweeps; ++k) {
+            run(1);
+            observe(std::as_const(*this));
+        }
+    }
+
+    // The launch alone, ordered on the stream; check() after a sync.
+    void enqueue(std::size_t sweeps)
+    {
+        while (sweeps > 0) {
+            const std::uint32_t chunk = std::uint32_t(std::min<std::size_t>(sweeps, 1u << 30));
+            cuda_check(cudaMemsetAsync(ctl_.data(), 0, sizeof(detail::Control), stream_), "reset barrier");
+            M m = model_;
+            Q q = proposal_;
+            const std::uint32_t* order = classes_.order();
+            const std::uint32_t* begin = classes_.begin();
+            std::uint32_t nc = classes_.host().count();
+            double beta = beta_;
+            std::uint64_t seed = seed_, sweep0 = sweeps_;
+            std::uint32_t n = chunk;
+            detail::Control* ctl = ctl_.data();
+            void* args[] = {&m, &q, &order, &begin, &nc, &beta, &seed, &sweep0, &n, &ctl};
+            cuda_check(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&detail::metropolis_sweeps<M, Q>),
+                                                   dim3(grid_), dim3(detail::kThreads), args, 0, stream_),
+                       "Metropolis launch");
+            sweeps_ += chunk;
+            sweeps -= chunk;
+        }
+    }
+
+    // Throws if a barrier wait of an earlier launch ran out.
+    void check() const
+    {
+        detail::Control h{};
+        cuda_check(cudaMemcpyAsync(&h, ctl_.data(), sizeof h, cudaMemcpyDeviceToHost, stream_), "read status");
+        cuda_check(cudaStreamSynchronize(stream_), "read status");
+        if (h.status != 0u) throw std::runtime_error("Metropolis: a grid barrier wait ran out");
+    }
+
+    // Sum over cells of cell_energy (model/cell.hpp:58-62), FP64.
+    double total_energy() const
+        requires CellEnergyModel<M>
+    {
+        return sum(model_.cells(), detail::CellEnergyOf{});
+    }
+    // Sum over sites of energy_at (model.hpp:93-96), FP64; for a pair model
+    // every bond appears twice.
+    double energy_at_sum() const
+        requires EnergyModel<M>
+    {
+        return sum(model_.sites(), detail::EnergyAtOf{});
+    }
+
+    const M& model() const noexcept { return model_; }
+    std::uint64_t sweeps() const noexcept { return sweeps_; }
+    void set_sweeps(std::uint64_t s) noexcept { sweeps_ = s; }
+    double beta() const noexcept { return beta_; }
+    void set_beta(double b) noexcept { beta_ = b; }
+    std::uint32_t grid() const noexcept { return grid_; }
+
+private:
+    template <class F>
+    double sum(std::uint64_t count, F f) const
+    {
+        const std::uint32_t blocks =
+            std::uint32_t(std::max<std::uint64_t>(1, std::min<std::uint64_t>(1024, (count + 255) / 256)));
+        Buffer<double> partial(blocks);
+        detail::block_sums<M, F><<<blocks, detail::kThreads, 0, stream_>>>(model_, count, f, partial.data());
+        cuda_check(cudaGetLastError(), "energy launch");
+        std::vector<double> h(blocks);
+        cuda_check(cudaMemcpyAsync(h.data(), partial.data(), blocks * sizeof(double), cudaMemcpyDeviceToHost,
+                                   stream_),
+                   "energy read");
+        cuda_check(cudaStreamSynchronize(stream_), "energy read");
+        double e = 0.0;
+        for (const double v : h) e += v;
+        return e;
+    }
+
+    M model_;
+    Q proposal_;
+    const ClassTable& classes_;
+    std::uint64_t seed_;
+    double beta_;
+    cudaStream_t stream_;
+    Buffer<detail::Control> ctl_;
+    std::uint32_t grid_ = 1;
+    std::uint64_t sweeps_ = 0;
+};
+
+}  // namespace umc::gpu::device

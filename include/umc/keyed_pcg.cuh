@@ -1,4 +1,4 @@
-// umc_rng.cuh -- counter-keyed PCG32, identical on host and device.
+// umc/keyed_pcg.cuh -- counter-keyed PCG32, identical on host and device.
 //
 // The reference draws every random number from one sequential Pcg32
 // (rng.hpp:8-44), and how many it draws depends on the data (the accept draw is

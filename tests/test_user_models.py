@@ -1,0 +1,172 @@
+"""User-written models on the GPU (include/umc/device.cuh).
+
+examples/device_models/user_models.cu defines, the way a user would, an XY pair term, a
+U(1) plaquette term, a table-free cubic O(3) ModelLike and two proposals, all
+in FP64 with __host__ __device__ members, and drives them with
+umc::gpu::device::Metropolis.  On the GPU every sweep is compared with the
+oracle's reference-semantics driver on the colour-major relabelled tables
+(same keyed streams): the field agrees to 1e-9 except at decisions that sat
+within 1e-9 of their threshold and the sites those decisions touch, and the
+energies from energy_at / cell_energy agree with the oracle's observables.
+"""
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), "examples", "device_models"))
+sys.path.insert(0, HERE)
+
+from helpers import checker_position, cubic_edges, random_unit_vectors, relabel_edges  # noqa: E402
+
+TOL = 1e-9
+MARGIN = 1e-9
+_vp, _d, _u64, _u32 = C.c_void_p, C.c_double, C.c_uint64, C.c_uint32
+_dp = C.POINTER(C.c_double)
+
+
+@pytest.fixture(scope="module")
+def lib(umc):
+    import build_device_models
+
+    path = build_device_models.build()
+    L = C.CDLL(path)
+    L.um_last_error.restype = C.c_char_p
+    L.um_xy_pair.argtypes = [_vp, _d, _d, _d, _u64, _u64, _u32, _dp, _dp, C.POINTER(_u32)]
+    L.um_u1_cells.argtypes = [_vp, _d, _d, _d, _u64, _u64, _u32, _dp, _dp]
+    L.um_heisenberg_cubic.argtypes = [_u32, _u32, _u32, _d, _d, _u64, _u64, _u32, _dp, _dp]
+    return L
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _call(lib, rc):
+    assert rc == 0, lib.um_last_error().decode()
+
+
+def xy_run(lib, g, theta, beta, width, seed, sweep0, n):
+    th = np.array(theta, np.float64, copy=True)
+    en = np.zeros(n)
+    grid = _u32(0)
+    _call(lib, lib.um_xy_pair(g._h, 1.0, beta, width, seed, sweep0, n, _p(th), _p(en), C.byref(grid)))
+    return th, en, grid.value
+
+
+def _neighbours(off, bonds, sites):
+    out = set()
+    for i in sites:
+        out.update(bonds[off[i]:off[i + 1]].tolist())
+    return out
+
+
+def test_user_library_exports_and_fails_loudly_without_gpu(umc, lib):
+    for name in ("um_xy_pair", "um_u1_cells", "um_heisenberg_cubic", "um_last_error"):
+        assert hasattr(lib, name)
+    if umc.device_count() > 0:
+        pytest.skip("a GPU is present")
+    g = umc.square_lattice(8, 8)
+    th = np.zeros(64)
+    en = np.zeros(1)
+    rc = lib.um_xy_pair(g._h, 1.0, 1.0, 1.0, 1, 0, 1, _p(th), _p(en), None)
+    assert rc != 0 and lib.um_last_error()  # a CUDA error, no CPU fallback
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L,sweeps", [(64, 3), (1024, 2)])
+def test_user_xy_pair_model_per_sweep(umc, oracle, lib, L, sweeps):
+    g = umc.square_lattice(L, L)
+    n = L * L
+    _, _, pos = g.colouring()
+    off_o, bonds_o = oracle_csr(oracle, umc, g, pos)
+    off_s, bonds_s = g.csr()
+    th = np.random.default_rng(L).uniform(-np.pi, np.pi, n)
+    for sweep in range(sweeps):
+        cm = np.empty(n)
+        cm[pos] = th
+        t_o, obs_o, margin = oracle.xy_metropolis(off_o, bonds_o, 1.0, 1.1, 1.0, 4, sweep, 1, cm)
+        th, en, grid = xy_run(lib, g, th, 1.1, 1.0, 4, sweep, 1)
+        if L == 1024:
+            assert grid * 256 < n // 2  # the grid-stride loop wraps within a class
+        d = np.abs(np.angle(np.exp(1j * (th - t_o[pos]))))
+        near = np.nonzero(np.abs(margin[pos]) < MARGIN)[0]
+        bad = set(np.nonzero(d > TOL)[0].tolist())
+        assert bad <= set(near.tolist()) | _neighbours(off_s, bonds_s, near), sorted(bad)[:10]
+        assert abs(en[0] - obs_o[0, 0]) < 1e-9 * n
+
+
+def oracle_csr(oracle, umc, g, pos):
+    off, bonds = g.csr()
+    ei = np.repeat(np.arange(len(off) - 1, dtype=np.uint32), np.diff(off))
+    keep = ei < bonds  # every undirected bond once, in CSR order of its lower endpoint
+    ri, rj = relabel_edges(ei[keep], bonds[keep], pos)
+    st, o, b, _ = oracle.pair_graph(len(off) - 1, ri, rj)
+    assert st == 0
+    return o, b
+
+
+@pytest.mark.gpu
+def test_user_xy_runs_continue_exactly(umc, lib):
+    """n sweeps in one launch equal the same sweeps split across launches
+    (the counter keys the streams), and sample() records the energy after
+    every sweep."""
+    g = umc.square_lattice(128, 128)
+    th0 = np.random.default_rng(2).uniform(-np.pi, np.pi, 128 * 128)
+    a, ea, _ = xy_run(lib, g, th0, 0.9, 1.3, 8, 0, 5)
+    b1, eb1, _ = xy_run(lib, g, th0, 0.9, 1.3, 8, 0, 2)
+    b2, eb2, _ = xy_run(lib, g, b1, 0.9, 1.3, 8, 2, 3)
+    np.testing.assert_array_equal(a, b2)
+    np.testing.assert_array_equal(ea, np.concatenate([eb1, eb2]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,L,beta,width,sweeps", [("2d", 8, 2.0, 0.5, 4), ("4d", 4, 1.1, 0.7, 3),
+                                                      ("4d", 6, 0.9, 1.0, 2)])
+def test_user_u1_cell_model(umc, oracle, lib, kind, L, beta, width, sweeps):
+    cc = umc.square_plaquettes(L) if kind == "2d" else umc.hypercubic_plaquettes(L)
+    n = cc.sites()
+    _, _, pos = cc.colouring()
+    cells = cc.table()
+    rcells = pos[cells]
+    inc = oracle.cell_incidence(n, rcells)[1:]
+    th0 = np.random.default_rng(L).uniform(-np.pi, np.pi, n)
+    # all sweeps in one launch against the oracle's sweeps in link order
+    th = th0.copy()
+    E = _d(0.0)
+    _call(lib, lib.um_u1_cells(cc._h, beta, 1.0, width, 3, 0, sweeps, _p(th), C.byref(E)))
+    cm = np.empty(n)
+    cm[pos] = th0
+    t_o, obs_o, margin = oracle.u1_metropolis(rcells, inc, beta, 1.0, width, 1, 3, 0, sweeps, cm)
+    d = np.abs(np.angle(np.exp(1j * (th - t_o[pos]))))
+    assert d.max() < TOL, d.max()
+    assert abs(E.value - obs_o[-1, 0]) < 1e-9 * max(1.0, abs(obs_o[-1, 0]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,beta", [((8, 8, 8), 0.693), ((16, 16, 4), 0.5), ((64, 64, 64), 0.693)])
+def test_user_table_free_heisenberg(umc, oracle, lib, dims, beta):
+    Lx, Ly, Lz = dims
+    n = Lx * Ly * Lz
+    pos = checker_position(Lx, Ly, Lz)
+    ei, ej = cubic_edges(Lx, Ly, Lz)
+    st, off, bonds, _ = oracle.pair_graph(n, *relabel_edges(ei, ej, pos))
+    assert st == 0
+    s = random_unit_vectors(n, 3, 5)
+    sweeps = 2 if n > 100000 else 3
+    for sweep in range(sweeps):
+        cm = np.empty((n, 3))
+        cm[pos] = s
+        v_o, obs_o, margin = oracle.vector_metropolis(3, off, bonds, 1.0, beta, 0, 0.0, 6, sweep, 1, cm)
+        flat = np.ascontiguousarray(s.reshape(-1))
+        E = _d(0.0)
+        _call(lib, lib.um_heisenberg_cubic(Lx, Ly, Lz, 1.0, beta, 6, sweep, 1, _p(flat), C.byref(E)))
+        s = flat.reshape(n, 3)
+        d = np.abs(s - v_o[pos]).max(axis=1)
+        near = np.nonzero(np.abs(margin[pos]) < MARGIN)[0]
+        bad = np.nonzero(d > TOL)[0]
+        assert len(bad) <= 7 * len(near), (len(bad), len(near))
+        assert abs(E.value - obs_o[0, 0]) < 1e-9 * n

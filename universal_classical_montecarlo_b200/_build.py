@@ -36,7 +36,8 @@ def _sources():
 
 
 def _deps():
-    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(INCLUDE, "umc_b200.h")]
+    shared = [os.path.join(INCLUDE, "umc", f) for f in os.listdir(os.path.join(INCLUDE, "umc")) if f.endswith(".cuh")]
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(INCLUDE, "umc_b200.h")] + shared
 
 
 def _stale(obj: str, src: str) -> bool:

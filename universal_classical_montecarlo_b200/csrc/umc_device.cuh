@@ -14,7 +14,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "umc_rng.cuh"
+#include <umc/keyed_pcg.cuh>
 
 namespace umc {
 

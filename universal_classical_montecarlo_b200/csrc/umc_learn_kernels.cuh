@@ -33,7 +33,7 @@
 #include <cstdint>
 
 #include "umc_device.cuh"
-#include "umc_rng.cuh"
+#include <umc/keyed_pcg.cuh>
 #include "umc_tc.cuh"
 
 namespace umc {
