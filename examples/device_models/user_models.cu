@@ -175,13 +175,13 @@ int um_xy_pair(const umc_graph* g, double J, double beta, double width, std::uin
     return guarded([&] {
         PairTables t(g);
         Buffer<double> field(t.sites());
-        field.upload(theta);
+        t.upload(field, theta, 1);
         auto model = t.model<Angle>(field.data(), CosineTerm{J});
         Metropolis<decltype(model), AngleShift> mc(model, AngleShift{width}, t.classes(), seed, beta);
         mc.set_sweeps(sweep0);
         std::uint32_t k = 0;
         mc.sample(n_sweeps, [&](const auto& m) { energies[k++] = 0.5 * m.energy_at_sum(); });
-        field.download(theta);
+        t.download(field, theta, 1);
         if (grid) *grid = mc.grid();
     });
 }
@@ -194,13 +194,13 @@ int um_u1_cells(const umc_cells* cc, double model_beta, double beta, double widt
     return guarded([&] {
         CellTables t(cc);
         Buffer<double> field(t.sites());
-        field.upload(theta);
+        t.upload(field, theta, 1);
         auto model = t.model<Angle>(field.data(), PlaquetteTerm{model_beta});
         Metropolis<decltype(model), AngleShift> mc(model, AngleShift{width}, t.classes(), seed, beta);
         mc.set_sweeps(sweep0);
         mc.run(n_sweeps);
         *total_energy = mc.total_energy();
-        field.download(theta);
+        t.download(field, theta, 1);
     });
 }
 
@@ -285,20 +285,20 @@ void um_xy_session_destroy(void* h) { delete static_cast<XYSession*>(h); }
 
 void* um_xy_session_stream(void* h) { return static_cast<XYSession*>(h)->stream; }
 
-// Field from/to host memory (sites doubles), ordered on the session's stream.
+// Field from/to host memory (sites doubles, site order), ordered on the
+// session's stream; set_field returns before the copy completes.
 int um_xy_session_set_field(void* h, const double* theta)
 {
     return guarded([&] {
         auto* s = static_cast<XYSession*>(h);
-        s->field.upload_async(theta, s->stream);
+        s->tables.upload(s->field, theta, 1, s->stream);
     });
 }
 int um_xy_session_get_field(void* h, double* theta)
 {
     return guarded([&] {
         auto* s = static_cast<XYSession*>(h);
-        s->field.download_async(theta, s->stream);
-        cuda_check(cudaStreamSynchronize(s->stream), "sync");
+        s->tables.download(s->field, theta, 1, s->stream);
     });
 }
 

@@ -28,6 +28,12 @@
 // reference driver run on the graph relabelled to colour-major order with
 // that keying, which is how the library's own chains are checked.
 //
+// Layout.  PairTables and CellTables number sites colour-major on the device
+// (a class is a contiguous range; table rows and field entries of a class are
+// read with unit stride) and move fields to and from the host in the
+// reference's site order, permuting on the device.  A model that numbers its
+// own sites (any other M) keeps its numbering; its classes list the sites.
+//
 // One launch runs any number of sweeps: a cooperative persistent kernel whose
 // blocks meet at a grid barrier between classes.  The barrier's waits are
 // bounded; a wait that runs out sets a status bit, every block returns, and
@@ -195,14 +201,16 @@ concept CellEnergyModel = ModelLike<M> && requires(const M cm, std::size_t c) {
 // ------------------------------------------------------------------ colour classes
 
 // Sites grouped by colour: order[begin[c] .. begin[c+1]) are the sites of
-// colour c, ascending.  The index k of a site in order is its colour-major
-// position, the id of its random stream.
+// colour c.  The index k of a site in order is its colour-major position, the
+// id of its random stream.  An empty order is the identity: the model numbers
+// its sites colour-major already (the table models below do).
 struct Classes
 {
     std::vector<std::uint32_t> order;
     std::vector<std::uint32_t> begin;
 
     std::uint32_t count() const { return std::uint32_t(begin.size() - 1); }
+    std::uint64_t sites() const { return begin.back(); }
     std::uint32_t largest() const
     {
         std::uint32_t m = 0;
@@ -225,31 +233,11 @@ struct Classes
         for (std::uint32_t i = 0; i < colour.size(); ++i) k.order[next[colour[i]]++] = i;
         return k;
     }
-    // The library's colouring of a pair graph (umc_graph_colouring).
-    static Classes of(const umc_graph* g)
+    // Contiguous classes [begin[c], begin[c+1]) of a colour-major numbering.
+    static Classes identity(std::vector<std::uint32_t> begin)
     {
-        const std::uint64_t n = umc_graph_sites(g);
-        std::uint32_t nc = 0;
-        std::vector<std::uint32_t> colour(n), pos(n);
-        umc_check(umc_graph_colouring(g, &nc, colour.data(), pos.data()));
-        return from_positions(colour, pos, nc);
-    }
-    // The library's colouring of a cell complex's sites (umc_cells_colouring).
-    static Classes of(const umc_cells* cc)
-    {
-        const std::uint64_t n = umc_cells_sites(cc);
-        std::uint32_t nc = 0;
-        std::vector<std::uint32_t> colour(n), pos(n);
-        umc_check(umc_cells_colouring(cc, &nc, colour.data(), pos.data()));
-        return from_positions(colour, pos, nc);
-    }
-
-private:
-    static Classes from_positions(const std::vector<std::uint32_t>& colour, const std::vector<std::uint32_t>& pos,
-                                  std::uint32_t nc)
-    {
-        Classes k = from_colours(colour, nc);
-        for (std::uint32_t i = 0; i < pos.size(); ++i) k.order[pos[i]] = i;
+        Classes k;
+        k.begin = std::move(begin);
         return k;
     }
 };
@@ -258,19 +246,159 @@ private:
 class ClassTable
 {
 public:
-    explicit ClassTable(Classes k)
-        : host_(std::move(k)), order_(host_.order), begin_(host_.begin)
+    explicit ClassTable(Classes k) : host_(std::move(k))
     {
-        if (host_.begin.size() < 2 || host_.begin.back() != host_.order.size())
+        const auto& b = host_.begin;
+        if (b.size() < 2 || b.front() != 0 || !std::is_sorted(b.begin(), b.end()))
+            throw std::invalid_argument("class table: begin must rise from 0");
+        if (!host_.order.empty() && host_.order.size() != b.back())
             throw std::invalid_argument("class table: begin does not cover order");
+        begin_ = Buffer<std::uint32_t>(b);
+        if (!host_.order.empty()) order_ = Buffer<std::uint32_t>(host_.order);
     }
     const Classes& host() const noexcept { return host_; }
-    const std::uint32_t* order() const noexcept { return order_.data(); }
+    // nullptr for the identity order
+    const std::uint32_t* order() const noexcept { return host_.order.empty() ? nullptr : order_.data(); }
     const std::uint32_t* begin() const noexcept { return begin_.data(); }
 
 private:
     Classes host_;
     Buffer<std::uint32_t> order_, begin_;
+};
+
+// ------------------------------------------------------------------ colour-major numbering
+
+namespace detail {
+
+constexpr int kThreads = 256;
+
+// dst[k] = src[order[k]] (device numbering from site order), per_site scalars
+// per site; scatter_sites is the inverse.
+template <class T>
+__global__ void __launch_bounds__(kThreads) gather_sites(T* __restrict__ dst, const T* __restrict__ src,
+                                                         const std::uint32_t* __restrict__ order, std::uint64_t n,
+                                                         std::uint32_t per_site)
+{
+    for (std::uint64_t x = blockIdx.x * std::uint64_t(blockDim.x) + threadIdx.x; x < n * per_site;
+         x += std::uint64_t(gridDim.x) * blockDim.x)
+        dst[x] = src[std::uint64_t(order[x / per_site]) * per_site + x % per_site];
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) scatter_sites(T* __restrict__ dst, const T* __restrict__ src,
+                                                          const std::uint32_t* __restrict__ order, std::uint64_t n,
+                                                          std::uint32_t per_site)
+{
+    for (std::uint64_t x = blockIdx.x * std::uint64_t(blockDim.x) + threadIdx.x; x < n * per_site;
+         x += std::uint64_t(gridDim.x) * blockDim.x)
+        dst[std::uint64_t(order[x / per_site]) * per_site + x % per_site] = src[x];
+}
+
+inline unsigned permute_grid(std::uint64_t count)
+{
+    return unsigned(std::max<std::uint64_t>(1, std::min<std::uint64_t>(148 * 16, (count + kThreads - 1) / kThreads)));
+}
+
+// The library's colouring of a table: colour and colour-major position of
+// every site (umc_graph_colouring / umc_cells_colouring).
+struct Colouring
+{
+    std::vector<std::uint32_t> colour, position;
+    std::uint32_t count = 0;
+
+    std::vector<std::uint32_t> order() const
+    {
+        std::vector<std::uint32_t> o(position.size());
+        for (std::uint32_t i = 0; i < position.size(); ++i) o[position[i]] = i;
+        return o;
+    }
+    std::vector<std::uint32_t> begin() const
+    {
+        std::vector<std::uint32_t> b(std::size_t(count) + 1, 0);
+        for (const auto c : colour) ++b[c + 1];
+        for (std::uint32_t c = 0; c < count; ++c) b[c + 1] += b[c];
+        return b;
+    }
+};
+
+inline Colouring colouring_of(const umc_graph* g)
+{
+    Colouring c;
+    c.colour.resize(umc_graph_sites(g));
+    c.position.resize(c.colour.size());
+    umc_check(umc_graph_colouring(g, &c.count, c.colour.data(), c.position.data()));
+    return c;
+}
+
+inline Colouring colouring_of(const umc_cells* cc)
+{
+    Colouring c;
+    c.colour.resize(umc_cells_sites(cc));
+    c.position.resize(c.colour.size());
+    umc_check(umc_cells_colouring(cc, &c.count, c.colour.data(), c.position.data()));
+    return c;
+}
+
+}  // namespace detail
+
+// The device numbering of the table models.  Site i of the library's table
+// is device site position[i] (colour-major), so a colour class is one
+// contiguous range and its sites, their table rows and their field entries
+// are read with unit stride.  Fields cross to and from the host in the
+// reference's site order (data() of model/pair.hpp and model/cell.hpp) and
+// are permuted on the device.
+class ColourMajor
+{
+public:
+    explicit ColourMajor(const detail::Colouring& c)
+        : position_(c.position), order_(c.order()), begin_(c.begin()), order_dev_(order_)
+    {}
+
+    std::uint32_t sites() const noexcept { return std::uint32_t(position_.size()); }
+    const std::vector<std::uint32_t>& position() const noexcept { return position_; }
+    const std::vector<std::uint32_t>& order() const noexcept { return order_; }
+    const std::vector<std::uint32_t>& class_begin() const noexcept { return begin_; }
+
+    // field (sites * per_site, device numbering) <- host (site order).  Ordered
+    // on stream s; a pinned host buffer must stay valid until s passes the copy.
+    // Transfers through one object share a staging buffer: issue them on one
+    // stream.
+    template <class T>
+    void upload(Buffer<T>& field, const T* host, std::size_t per_site, cudaStream_t s = nullptr) const
+    {
+        const std::uint64_t count = std::uint64_t(sites()) * per_site;
+        if (field.size() != count) throw std::invalid_argument("upload: field size differs from sites * per_site");
+        T* stage = staging<T>(count);
+        cuda_check(cudaMemcpyAsync(stage, host, count * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+        detail::gather_sites<T><<<detail::permute_grid(count), detail::kThreads, 0, s>>>(
+            field.data(), stage, order_dev_.data(), sites(), std::uint32_t(per_site));
+        cuda_check(cudaGetLastError(), "upload permute");
+    }
+    // host (site order) <- field; returns when the host copy is complete.
+    template <class T>
+    void download(const Buffer<T>& field, T* host, std::size_t per_site, cudaStream_t s = nullptr) const
+    {
+        const std::uint64_t count = std::uint64_t(sites()) * per_site;
+        if (field.size() != count) throw std::invalid_argument("download: field size differs from sites * per_site");
+        T* stage = staging<T>(count);
+        detail::scatter_sites<T><<<detail::permute_grid(count), detail::kThreads, 0, s>>>(
+            stage, field.data(), order_dev_.data(), sites(), std::uint32_t(per_site));
+        cuda_check(cudaGetLastError(), "download permute");
+        cuda_check(cudaMemcpyAsync(host, stage, count * sizeof(T), cudaMemcpyDeviceToHost, s), "download");
+        cuda_check(cudaStreamSynchronize(s), "download");
+    }
+
+private:
+    template <class T>
+    T* staging(std::uint64_t count) const
+    {
+        if (stage_.size() < count * sizeof(T)) stage_ = Buffer<unsigned char>(count * sizeof(T));
+        return reinterpret_cast<T*>(stage_.data());
+    }
+
+    std::vector<std::uint32_t> position_, order_, begin_;
+    Buffer<std::uint32_t> order_dev_;
+    mutable Buffer<unsigned char> stage_;
 };
 
 // ------------------------------------------------------------------ table models
@@ -377,56 +505,51 @@ struct CellModel
     }
 };
 
-// A pair graph's CSR and colour classes on the device.
-class PairTables
+// A pair graph's CSR in the colour-major device numbering: row k holds the
+// bonds of site order[k], each as the neighbour's device index.
+class PairTables : public ColourMajor
 {
 public:
-    explicit PairTables(const umc_graph* g) : classes_(Classes::of(g))
-    {
-        n_ = std::uint32_t(umc_graph_sites(g));
-        std::vector<std::uint32_t> off(std::size_t(n_) + 1), bonds(umc_graph_slots(g));
-        umc_check(umc_graph_csr(g, off.data(), bonds.data()));
-        offset_ = Buffer<std::uint32_t>(off);
-        bonds_ = Buffer<std::uint32_t>(bonds);
-    }
-    std::uint32_t sites() const noexcept { return n_; }
+    explicit PairTables(const umc_graph* g) : PairTables(g, detail::colouring_of(g)) {}
+
     const ClassTable& classes() const noexcept { return classes_; }
 
-    // A PairModel view over field (sites * D::size device scalars).
+    // A PairModel view over field (sites * D::size device scalars, device numbering).
     template <class D, class Term>
     PairModel<D, Term> model(typename D::dtype* field, Term term) const
     {
-        return PairModel<D, Term>{field, offset_.data(), bonds_.data(), n_, term};
+        return PairModel<D, Term>{field, offset_.data(), bonds_.data(), sites(), term};
     }
 
 private:
+    PairTables(const umc_graph* g, const detail::Colouring& c)
+        : ColourMajor(c), classes_(Classes::identity(class_begin()))
+    {
+        const std::uint32_t n = sites();
+        std::vector<std::uint32_t> off(std::size_t(n) + 1), bonds(umc_graph_slots(g));
+        umc_check(umc_graph_csr(g, off.data(), bonds.data()));
+        std::vector<std::uint32_t> doff(std::size_t(n) + 1, 0), dbonds(bonds.size());
+        for (std::uint32_t k = 0; k < n; ++k) {
+            const std::uint32_t i = order()[k];
+            std::uint32_t w = doff[k];
+            for (std::uint32_t a = off[i]; a < off[i + 1]; ++a) dbonds[w++] = position()[bonds[a]];
+            doff[k + 1] = w;
+        }
+        offset_ = Buffer<std::uint32_t>(doff);
+        bonds_ = Buffer<std::uint32_t>(dbonds);
+    }
+
     ClassTable classes_;
-    std::uint32_t n_ = 0;
     Buffer<std::uint32_t> offset_, bonds_;
 };
 
-// A cell complex's cells, incidence and colour classes on the device.
-class CellTables
+// A cell complex in the colour-major device numbering: cell c lists its
+// sites' device indices; incidence row k is that of site order[k].
+class CellTables : public ColourMajor
 {
 public:
-    explicit CellTables(const umc_cells* cc) : classes_(Classes::of(cc))
-    {
-        n_ = std::uint32_t(umc_cells_sites(cc));
-        n_cells_ = std::uint32_t(umc_cells_count(cc));
-        arity_ = umc_cells_arity(cc);
-        std::vector<std::uint32_t> cells(std::size_t(n_cells_) * arity_);
-        umc_check(umc_cells_table(cc, cells.data()));
-        std::vector<std::uint64_t> off(std::size_t(n_) + 1);
-        umc_check(umc_cells_incidence(cc, off.data(), nullptr, nullptr));
-        std::vector<std::uint32_t> inc_cell(off.back());
-        std::vector<std::uint8_t> inc_which(off.back());
-        umc_check(umc_cells_incidence(cc, off.data(), inc_cell.data(), inc_which.data()));
-        cells_ = Buffer<std::uint32_t>(cells);
-        inc_offset_ = Buffer<std::uint64_t>(off);
-        inc_cell_ = Buffer<std::uint32_t>(inc_cell);
-        inc_which_ = Buffer<std::uint8_t>(inc_which);
-    }
-    std::uint32_t sites() const noexcept { return n_; }
+    explicit CellTables(const umc_cells* cc) : CellTables(cc, detail::colouring_of(cc)) {}
+
     std::uint32_t cells() const noexcept { return n_cells_; }
     const ClassTable& classes() const noexcept { return classes_; }
 
@@ -435,12 +558,44 @@ public:
     {
         if (Term::arity != arity_) throw std::invalid_argument("term arity differs from the cell table's");
         return CellModel<D, Term>{field, cells_.data(), inc_offset_.data(), inc_cell_.data(), inc_which_.data(),
-                                  n_, n_cells_, term};
+                                  sites(), n_cells_, term};
     }
 
 private:
+    CellTables(const umc_cells* cc, const detail::Colouring& c)
+        : ColourMajor(c), classes_(Classes::identity(class_begin()))
+    {
+        const std::uint32_t n = sites();
+        n_cells_ = std::uint32_t(umc_cells_count(cc));
+        arity_ = umc_cells_arity(cc);
+        std::vector<std::uint32_t> cells(std::size_t(n_cells_) * arity_);
+        umc_check(umc_cells_table(cc, cells.data()));
+        for (auto& s : cells) s = position()[s];
+        std::vector<std::uint64_t> off(std::size_t(n) + 1);
+        umc_check(umc_cells_incidence(cc, off.data(), nullptr, nullptr));
+        std::vector<std::uint32_t> inc_cell(off.back());
+        std::vector<std::uint8_t> inc_which(off.back());
+        umc_check(umc_cells_incidence(cc, off.data(), inc_cell.data(), inc_which.data()));
+        std::vector<std::uint64_t> doff(std::size_t(n) + 1, 0);
+        std::vector<std::uint32_t> dcell(inc_cell.size());
+        std::vector<std::uint8_t> dwhich(inc_which.size());
+        for (std::uint32_t k = 0; k < n; ++k) {
+            const std::uint32_t i = order()[k];
+            std::uint64_t w = doff[k];
+            for (std::uint64_t a = off[i]; a < off[i + 1]; ++a, ++w) {
+                dcell[w] = inc_cell[a];
+                dwhich[w] = inc_which[a];
+            }
+            doff[k + 1] = w;
+        }
+        cells_ = Buffer<std::uint32_t>(cells);
+        inc_offset_ = Buffer<std::uint64_t>(doff);
+        inc_cell_ = Buffer<std::uint32_t>(dcell);
+        inc_which_ = Buffer<std::uint8_t>(dwhich);
+    }
+
     ClassTable classes_;
-    std::uint32_t n_ = 0, n_cells_ = 0, arity_ = 0;
+    std::uint32_t n_cells_ = 0, arity_ = 0;
     Buffer<std::uint32_t> cells_;
     Buffer<std::uint64_t> inc_offset_;
     Buffer<std::uint32_t> inc_cell_;
@@ -451,7 +606,6 @@ private:
 
 namespace detail {
 
-constexpr int kThreads = 256;
 constexpr unsigned kSpinLimit = 1u << 24;  // about a second of 64 ns sleeps
 
 struct Control
@@ -518,7 +672,7 @@ __global__ void __launch_bounds__(kThreads) metropolis_sweeps(M m, Q q, const st
         for (std::uint32_t c = 0; c < n_classes; ++c) {
             const std::uint32_t end = begin[c + 1];
             for (std::uint32_t k = begin[c] + t; k < end; k += stride) {
-                const std::uint32_t i = order[k];
+                const std::uint32_t i = order ? order[k] : k;
                 Rng rng(KeyedPcg::open(kbase, k));
                 T cand[M::size];
                 const T* cur = m.data() + std::size_t(i) * M::size;
@@ -586,7 +740,7 @@ public:
         : model_(model), proposal_(proposal), classes_(classes), seed_(seed), beta_(beta), stream_(stream),
           ctl_(1)
     {
-        if (classes.host().order.size() != model.sites())
+        if (classes.host().sites() != model.sites())
             throw std::invalid_argument("colour classes do not cover the model's sites");
         int dev = 0, sms = 0, per_sm = 0;
         cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
