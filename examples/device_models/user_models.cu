@@ -6,6 +6,8 @@
 //                   PairModel (a user CellTerm of arity 2, term/cell.hpp:10-25);
 //   PlaquetteTerm-- U(1) plaquette beta (1 - cos(t0 + t1 - t2 - t3)), arity 4,
 //                   as a CellModel (term/plaquette.hpp:13-50);
+//   DotTerm<N>   -- the Heisenberg pair term -J s_i . s_j, driven by Wolff
+//                   (a PairModel is a WolffModel, driver.hpp:69-83);
 //   CubicHeisenberg -- a whole ModelLike (model.hpp:65-88) for the periodic
 //                   cubic O(3) model whose neighbours come from the site index,
 //                   with no bond table at all;
@@ -13,7 +15,7 @@
 //   Sphere3      -- UniformSphereN<3> (dof/vector.hpp:35-61).
 //
 // Exported with a C ABI for the Python tests and bench.py (ctypes): one-shot
-// runs (um_xy_pair, um_u1_cells, um_heisenberg_cubic) and a persistent XY
+// runs (um_xy_pair, um_u1_cells, um_heisenberg_cubic, um_o3_wolff) and a persistent XY
 // session (um_xy_session_*) whose launches bench.py times.
 #include <umc/device.cuh>
 
@@ -31,6 +33,36 @@ struct Angle
 {
     using dtype = double;
     static constexpr std::size_t size = 1;
+};
+
+template <std::size_t N>
+struct Vec
+{
+    using dtype = double;
+    static constexpr std::size_t size = N;
+};
+
+// E = -J s_i . s_j with HeisenbergTerm's arithmetic (term/heisenberg.hpp:11-35).
+template <std::size_t N>
+struct DotTerm
+{
+    using dtype = double;
+    using energy_type = double;
+    static constexpr std::size_t arity = 2;
+    double J;
+
+    UMC_HD static double dot(const double* a, const double* b)
+    {
+        double s = 0.0;
+        for (std::size_t k = 0; k < N; ++k) s += a[k] * b[k];
+        return s;
+    }
+    UMC_HD double energy(const double* const* l) const { return -J * dot(l[0], l[1]); }
+    UMC_HD double delta(std::size_t which, const double* old, const double* nw, const double* const* l) const
+    {
+        const double* fixed = l[which == 0 ? 1 : 0];
+        return -J * (dot(nw, fixed) - dot(old, fixed));
+    }
 };
 
 struct CosineTerm
@@ -144,6 +176,7 @@ struct CubicHeisenberg
 };
 
 static_assert(ModelLike<CubicHeisenberg> && EnergyModel<CubicHeisenberg>);
+static_assert(WolffModel<PairModel<Vec<3>, DotTerm<3>>>);
 static_assert(CellTerm<CosineTerm, Angle> && CellTerm<PlaquetteTerm, Angle>);
 static_assert(Proposal<AngleShift, double> && Proposal<Sphere3, double>);
 
@@ -223,6 +256,30 @@ int um_heisenberg_cubic(std::uint32_t Lx, std::uint32_t Ly, std::uint32_t Lz, do
         mc.run(n_sweeps);
         *energy = mc.energy_at_sum();
         field.download(spins);
+    });
+}
+
+// O(3) Wolff on a library pair graph with the user's DotTerm<3> and Sphere3
+// axis.  sweeps == 0: n flips, their sizes to `sizes`; sweeps == 1: n Wolff
+// sweeps (flips until the flipped sites add up to the lattice).  spins
+// (sites x 3, site order) in/out.
+int um_o3_wolff(const umc_graph* g, double J, double beta, std::uint64_t seed, std::uint64_t flip0, std::uint32_t n,
+                int sweeps, double* spins, std::uint64_t* sizes, std::uint64_t* flips_done, double* mean_size)
+{
+    return guarded([&] {
+        PairTables t(g);
+        Buffer<double> field(std::size_t(t.sites()) * 3);
+        t.upload(field, spins, 3);
+        auto model = t.model<Vec<3>>(field.data(), DotTerm<3>{J});
+        Wolff<decltype(model), Sphere3> w(model, Sphere3{}, seed, beta);
+        w.set_flips(flip0);
+        if (sweeps)
+            w.run(n);
+        else
+            w.flips(n, sizes);
+        *flips_done = w.flips_done() - flip0;
+        *mean_size = w.mean_cluster_size();
+        t.download(field, spins, 3);
     });
 }
 

@@ -5,7 +5,8 @@
 // kernel".  This header is that kernel: a translation unit compiled by nvcc
 // includes it, writes its terms, proposals or whole models with __host__
 // __device__ members (UMC_HD), and drives them with device::Metropolis, the
-// single-site driver of driver.hpp:17-66 run over colour classes.  Tables
+// single-site driver of driver.hpp:17-66 run over colour classes, and with
+// device::Wolff (driver.hpp:85-210) when they are WolffModels.  Tables
 // (PairGraph CSR, CellComplex cells and incidence, colourings) come from
 // libumc_b200.so; the update loop is instantiated for the user's types here.
 //
@@ -196,6 +197,21 @@ template <class M>
 concept CellEnergyModel = ModelLike<M> && requires(const M cm, std::size_t c) {
     { cm.cells() } -> std::convertible_to<std::size_t>;
     { cm.cell_energy(c) } -> std::convertible_to<double>;
+};
+
+// driver.hpp:69-83, plus bond_id(i, a): the key of the a-th bond of i's row.
+// The device tests each bond once, from its lower endpoint, with a draw keyed
+// by that id, so the ids of the bonds i tests (those with j > i) must be
+// distinct.  bond_type has a member j, the neighbour.
+template <class M>
+concept WolffModel = ModelLike<M> && requires(const M cm, std::size_t loc, const typename M::value_type* p,
+                                              const typename M::bond_type& b, std::size_t a) {
+    typename M::bond_type;
+    { cm.degree(loc) } -> std::convertible_to<std::size_t>;
+    { cm.bonds(loc) } -> std::convertible_to<const typename M::bond_type*>;
+    { cm.energy_diff_bond(loc, b, p) } -> std::convertible_to<double>;
+    { cm.bond_id(loc, a) } -> std::convertible_to<std::uint32_t>;
+    { b.j } -> std::convertible_to<std::size_t>;
 };
 
 // ------------------------------------------------------------------ colour classes
@@ -403,6 +419,13 @@ private:
 
 // ------------------------------------------------------------------ table models
 
+// One entry of a bond row: PairGraph's Bond<NoPayload> (lattice/pair_graph.hpp)
+// on the device, the neighbour's device index.
+struct Bond
+{
+    std::uint32_t j;
+};
+
 // PairModel (model/pair.hpp:18-80) as a device view: the field and the CSR
 // bond table live on the device; Term is any arity-2 CellTerm.
 template <class D, class Term>
@@ -412,11 +435,12 @@ struct PairModel
     using dtype = typename D::dtype;
     using value_type = dtype;
     using energy_type = typename Term::energy_type;
+    using bond_type = Bond;
     static constexpr std::size_t size = D::size;
 
     dtype* field;
     const std::uint32_t* offset;  // sites + 1
-    const std::uint32_t* bonds;   // offset[sites]
+    const Bond* row;              // offset[sites]
     std::uint32_t n;
     Term term;
 
@@ -424,6 +448,9 @@ struct PairModel
     UMC_HD const dtype* data() const { return field; }
     UMC_HD dtype* data() { return field; }
     UMC_HD std::size_t degree(std::size_t i) const { return offset[i + 1] - offset[i]; }
+    UMC_HD const Bond* bonds(std::size_t i) const { return row + offset[i]; }
+    // Key of the a-th bond of i's row: its CSR slot.
+    UMC_HD std::uint32_t bond_id(std::size_t i, std::size_t a) const { return offset[i] + std::uint32_t(a); }
 
     // model/pair.hpp:38-49: bonds incident to i, each counted once.
     UMC_HD energy_type energy_at(std::size_t i) const
@@ -431,7 +458,7 @@ struct PairModel
         energy_type e = 0;
         const dtype* si = field + i * size;
         for (std::uint32_t a = offset[i]; a < offset[i + 1]; ++a) {
-            const dtype* links[2] = {si, field + std::size_t(bonds[a]) * size};
+            const dtype* links[2] = {si, field + std::size_t(row[a].j) * size};
             e += term.energy(links);
         }
         return e;
@@ -442,10 +469,17 @@ struct PairModel
         energy_type d = 0;
         const dtype* si = field + i * size;
         for (std::uint32_t a = offset[i]; a < offset[i + 1]; ++a) {
-            const dtype* links[2] = {si, field + std::size_t(bonds[a]) * size};
+            const dtype* links[2] = {si, field + std::size_t(row[a].j) * size};
             d += term.delta(0, si, p, links);
         }
         return d;
+    }
+    // model/pair.hpp:66-72: the bond's energy change when b.j takes p, i fixed.
+    UMC_HD energy_type energy_diff_bond(std::size_t i, const Bond& b, const dtype* p) const
+    {
+        const dtype* sj = field + std::size_t(b.j) * size;
+        const dtype* links[2] = {sj, field + i * size};
+        return term.delta(0, sj, p, links);
     }
     UMC_HD void update(std::size_t i, const dtype* p)
     {
@@ -518,7 +552,7 @@ public:
     template <class D, class Term>
     PairModel<D, Term> model(typename D::dtype* field, Term term) const
     {
-        return PairModel<D, Term>{field, offset_.data(), bonds_.data(), sites(), term};
+        return PairModel<D, Term>{field, offset_.data(), reinterpret_cast<const Bond*>(bonds_.data()), sites(), term};
     }
 
 private:
@@ -722,6 +756,161 @@ struct EnergyAtOf
     }
 };
 
+// FP64 sum of f(m, x) over x < count: per-block partials, added on the host
+// in block order (deterministic for a given count).
+template <class M, class F>
+double device_sum(const M& m, std::uint64_t count, F f, cudaStream_t s)
+{
+    const std::uint32_t blocks =
+        std::uint32_t(std::max<std::uint64_t>(1, std::min<std::uint64_t>(1024, (count + kThreads - 1) / kThreads)));
+    Buffer<double> partial(blocks);
+    block_sums<M, F><<<blocks, kThreads, 0, s>>>(m, count, f, partial.data());
+    cuda_check(cudaGetLastError(), "sum launch");
+    std::vector<double> h(blocks);
+    cuda_check(cudaMemcpyAsync(h.data(), partial.data(), blocks * sizeof(double), cudaMemcpyDeviceToHost, s),
+               "sum read");
+    cuda_check(cudaStreamSynchronize(s), "sum read");
+    double e = 0.0;
+    for (const double v : h) e += v;
+    return e;
+}
+
+// Blocks of a cooperative launch of kernel: all resident at once, no more
+// than `need`.
+inline std::uint32_t cooperative_grid(const void* kernel, std::uint64_t need)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0), "occupancy");
+    if (per_sm < 1) throw std::runtime_error("kernel does not fit on an SM");
+    return std::uint32_t(std::max<std::uint64_t>(1, std::min<std::uint64_t>(need, std::uint64_t(per_sm) * sms)));
+}
+
+// ---- Wolff: bond activation, union-find labelling, flip of the seed's cluster
+
+constexpr unsigned kUfLimit = 1u << 26;  // steps of one find or union before giving up
+
+struct WolffControl
+{
+    Control bar;
+    unsigned long long touched;  // sites flipped by this launch
+    unsigned done;               // flips completed by this launch
+    unsigned uf_status;          // bit 1: a find or union ran past kUfLimit
+};
+
+__device__ __forceinline__ std::uint32_t uf_load(const std::uint32_t* p) { return *(const volatile std::uint32_t*)p; }
+
+// Root of x with path halving.  Links only point to smaller indices, so every
+// step moves down and the walk ends within x steps.
+__device__ __forceinline__ std::uint32_t uf_root(std::uint32_t* parent, std::uint32_t x, unsigned* status)
+{
+    for (unsigned it = 0; it < kUfLimit; ++it) {
+        const std::uint32_t p = uf_load(parent + x);
+        if (p == x) return x;
+        const std::uint32_t gp = uf_load(parent + p);
+        if (gp != p) *(volatile std::uint32_t*)(parent + x) = gp;
+        x = gp;
+    }
+    atomicOr(status, 2u);
+    return x;
+}
+
+// Joins the sets of a and b: the larger root is linked under the smaller.
+__device__ __forceinline__ void uf_unite(std::uint32_t* parent, std::uint32_t a, std::uint32_t b, unsigned* status)
+{
+    for (unsigned it = 0; it < kUfLimit; ++it) {
+        a = uf_root(parent, a, status);
+        b = uf_root(parent, b, status);
+        if (a == b) return;
+        if (a > b) {
+            const std::uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(parent + b, b, a) == b) return;
+    }
+    atomicOr(status, 2u);
+}
+
+// out = s - 2 (s . r) r, in T arithmetic as Wolff::flip does (driver.hpp:127-130).
+template <class T, std::size_t D>
+__device__ __forceinline__ void reflect(const T* s, const T* r, T* out)
+{
+    T dot = 0;
+    for (std::size_t k = 0; k < D; ++k) dot += s[k] * r[k];
+    for (std::size_t k = 0; k < D; ++k) out[k] = s[k] - T(2) * dot * r[k];
+}
+
+// Wolff::flip (driver.hpp:104-162) for flips flip0, flip0 + 1, ...: stops
+// after max_flips, or once the flipped sites reach `target` when target > 0.
+// Per flip: the axis and seed site from the key (seed, flip, kTagAxis); every
+// bond (i, j > i) active with probability 1 - exp(-beta dE), dE =
+// energy_diff_bond(i, b, reflected s_j), its uniform keyed (seed, flip,
+// kTagBond, bond_id); the seed's component of the active bonds reflected.
+// With a reflection-invariant pair energy the bond test is the same from
+// either end, so this is the reference's cluster for those draws.
+template <class M, class A>
+__global__ void __launch_bounds__(kThreads) wolff_flips(M m, A axis, double beta, std::uint64_t seed,
+                                                        std::uint64_t flip0, std::uint32_t max_flips,
+                                                        std::uint64_t target, std::uint32_t* parent,
+                                                        unsigned long long* sizes, WolffControl* ctl)
+{
+    using T = typename M::value_type;
+    constexpr std::size_t D = M::size;
+    __shared__ unsigned long long block_count;
+    const std::uint32_t n = std::uint32_t(m.sites());
+    const std::uint32_t stride = gridDim.x * blockDim.x;
+    const std::uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long touched = 0;
+    for (std::uint32_t f = 0; f < max_flips; ++f) {
+        const std::uint64_t counter = flip0 + f;
+        Rng g(KeyedPcg::open_key(seed, counter, kTagAxis, 0));
+        T r[D];
+        axis.sample(static_cast<const T*>(nullptr), g, r);
+        const std::uint32_t seed_site = std::uint32_t(g.uni() * double(n));
+        for (std::uint32_t i = t; i < n; i += stride) parent[i] = i;
+        if (threadIdx.x == 0) block_count = 0;
+        if (!grid_sync(&ctl->bar)) return;
+
+        const std::uint64_t kbond = key_base(key_seed(seed, counter, kTagBond));
+        for (std::uint32_t i = t; i < n; i += stride) {
+            const auto* row = m.bonds(i);
+            const std::size_t deg = m.degree(i);
+            for (std::size_t a = 0; a < deg; ++a) {
+                const std::uint32_t j = std::uint32_t(row[a].j);
+                if (j <= i) continue;
+                T nb[D];
+                reflect<T, D>(m.data() + std::size_t(j) * D, r, nb);
+                const double dE = m.energy_diff_bond(i, row[a], nb);
+                Rng u(KeyedPcg::open(kbond, m.bond_id(i, a)));
+                if (u.uni() < 1.0 - exp(-beta * dE)) uf_unite(parent, i, j, &ctl->uf_status);
+            }
+        }
+        if (!grid_sync(&ctl->bar)) return;
+
+        const std::uint32_t root = uf_root(parent, seed_site, &ctl->uf_status);
+        unsigned long long mine = 0;
+        for (std::uint32_t i = t; i < n; i += stride) {
+            if (uf_root(parent, i, &ctl->uf_status) != root) continue;
+            T prop[D];
+            reflect<T, D>(m.data() + std::size_t(i) * D, r, prop);
+            m.update(i, prop);
+            ++mine;
+        }
+        if (mine) atomicAdd(&block_count, mine);
+        __syncthreads();
+        if (threadIdx.x == 0 && block_count) atomicAdd(sizes + f, block_count);
+        if (!grid_sync(&ctl->bar)) return;
+        touched += __ldcg(sizes + f);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            ctl->done = f + 1;
+            ctl->touched = touched;
+        }
+        if (target > 0 && touched >= target) return;
+    }
+}
+
 }  // namespace detail
 
 // ------------------------------------------------------------------ driver
@@ -742,15 +931,8 @@ public:
     {
         if (classes.host().sites() != model.sites())
             throw std::invalid_argument("colour classes do not cover the model's sites");
-        int dev = 0, sms = 0, per_sm = 0;
-        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, detail::metropolis_sweeps<M, Q>,
-                                                                  detail::kThreads, 0),
-                   "occupancy");
-        if (per_sm < 1) throw std::runtime_error("Metropolis kernel does not fit on an SM");
-        const std::uint32_t need = (classes.host().largest() + detail::kThreads - 1) / detail::kThreads;
-        grid_ = std::max<std::uint32_t>(1, std::min<std::uint32_t>(need, std::uint32_t(per_sm) * sms));
+        grid_ = detail::cooperative_grid(reinterpret_cast<const void*>(&detail::metropolis_sweeps<M, Q>),
+                                         (classes.host().largest() + detail::kThreads - 1) / detail::kThreads);
     }
 
     // One pass over every site (driver.hpp:29-43).
@@ -811,14 +993,14 @@ public:
     double total_energy() const
         requires CellEnergyModel<M>
     {
-        return sum(model_.cells(), detail::CellEnergyOf{});
+        return detail::device_sum(model_, model_.cells(), detail::CellEnergyOf{}, stream_);
     }
     // Sum over sites of energy_at (model.hpp:93-96), FP64; for a pair model
     // every bond appears twice.
     double energy_at_sum() const
         requires EnergyModel<M>
     {
-        return sum(model_.sites(), detail::EnergyAtOf{});
+        return detail::device_sum(model_, model_.sites(), detail::EnergyAtOf{}, stream_);
     }
 
     const M& model() const noexcept { return model_; }
@@ -829,24 +1011,6 @@ public:
     std::uint32_t grid() const noexcept { return grid_; }
 
 private:
-    template <class F>
-    double sum(std::uint64_t count, F f) const
-    {
-        const std::uint32_t blocks =
-            std::uint32_t(std::max<std::uint64_t>(1, std::min<std::uint64_t>(1024, (count + 255) / 256)));
-        Buffer<double> partial(blocks);
-        detail::block_sums<M, F><<<blocks, detail::kThreads, 0, stream_>>>(model_, count, f, partial.data());
-        cuda_check(cudaGetLastError(), "energy launch");
-        std::vector<double> h(blocks);
-        cuda_check(cudaMemcpyAsync(h.data(), partial.data(), blocks * sizeof(double), cudaMemcpyDeviceToHost,
-                                   stream_),
-                   "energy read");
-        cuda_check(cudaStreamSynchronize(stream_), "energy read");
-        double e = 0.0;
-        for (const double v : h) e += v;
-        return e;
-    }
-
     M model_;
     Q proposal_;
     const ClassTable& classes_;
@@ -856,6 +1020,143 @@ private:
     Buffer<detail::Control> ctl_;
     std::uint32_t grid_ = 1;
     std::uint64_t sweeps_ = 0;
+};
+
+// Wolff (driver.hpp:85-210) for a device WolffModel M and axis proposal A.
+// Flip f keys its draws by (seed, f), so set_flips() continues a chain
+// exactly.  The device needs no stack: every bond is tested at once, a
+// union-find labels the active bonds' components, and the seed's component is
+// reflected, in one cooperative launch for many flips.
+template <WolffModel M, class A>
+    requires Proposal<A, typename M::value_type>
+class Wolff
+{
+public:
+    Wolff(M model, A axis, std::uint64_t seed, double beta, cudaStream_t stream = nullptr)
+        : model_(model), axis_(axis), seed_(seed), beta_(beta), stream_(stream), parent_(model.sites()),
+          sizes_(kCapacity), ctl_(1)
+    {
+        if (model.sites() == 0 || model.sites() >= (std::uint64_t(1) << 32))
+            throw std::invalid_argument("Wolff: the model needs 1 to 2^32 - 1 sites");
+        grid_ = detail::cooperative_grid(kernel(), (model.sites() + detail::kThreads - 1) / detail::kThreads);
+    }
+
+    // One cluster flip; returns how many sites it flipped (driver.hpp:104-162).
+    std::size_t flip()
+    {
+        std::uint64_t size = 0;
+        launch(1, 0, &size);
+        return std::size_t(size);
+    }
+
+    // n flips in launches of up to 65,536; sizes (n entries) may be null.
+    void flips(std::size_t n, std::uint64_t* sizes = nullptr)
+    {
+        while (n > 0) {
+            const std::uint32_t chunk = std::uint32_t(std::min<std::size_t>(n, kCapacity));
+            launch(chunk, 0, sizes);
+            if (sizes) sizes += chunk;
+            n -= chunk;
+        }
+    }
+
+    // Flips until the flipped sites add up to the lattice (driver.hpp:163-173).
+    void sweep()
+    {
+        std::uint64_t need = model_.sites();
+        while (need > 0) {
+            const std::uint64_t got = launch(kCapacity, need, nullptr);
+            need = got >= need ? 0 : need - got;
+        }
+    }
+
+    // n sweeps (driver.hpp:175-180).
+    void run(std::size_t sweeps)
+    {
+        for (std::size_t k = 0; k < sweeps; ++k) sweep();
+    }
+
+    // Flips n clusters, calling observe(*this) after each (driver.hpp:182-190).
+    template <class F>
+    void sample(std::size_t flips, F&& observe)
+    {
+        for (std::size_t k = 0; k < flips; ++k) {
+            flip();
+            observe(std::as_const(*this));
+        }
+    }
+
+    // Mean cluster size over every flip so far (driver.hpp:193-197).
+    double mean_cluster_size() const { return flips_ == 0 ? 0.0 : size_sum_ / double(flips_); }
+
+    double total_energy() const
+        requires CellEnergyModel<M>
+    {
+        return detail::device_sum(model_, model_.cells(), detail::CellEnergyOf{}, stream_);
+    }
+    double energy_at_sum() const
+        requires EnergyModel<M>
+    {
+        return detail::device_sum(model_, model_.sites(), detail::EnergyAtOf{}, stream_);
+    }
+
+    const M& model() const noexcept { return model_; }
+    std::uint64_t flips_done() const noexcept { return flips_; }
+    void set_flips(std::uint64_t f) noexcept { flips_ = f; }
+    double beta() const noexcept { return beta_; }
+    void set_beta(double b) noexcept { beta_ = b; }
+    std::uint32_t grid() const noexcept { return grid_; }
+
+private:
+    static constexpr std::uint32_t kCapacity = 1u << 16;
+    static const void* kernel() { return reinterpret_cast<const void*>(&detail::wolff_flips<M, A>); }
+
+    // Up to max_flips flips (fewer once target sites are flipped, target > 0);
+    // returns the sites flipped and writes one size per flip to sizes_out.
+    std::uint64_t launch(std::uint32_t max_flips, std::uint64_t target, std::uint64_t* sizes_out)
+    {
+        cuda_check(cudaMemsetAsync(ctl_.data(), 0, sizeof(detail::WolffControl), stream_), "reset control");
+        cuda_check(cudaMemsetAsync(sizes_.data(), 0, max_flips * sizeof(unsigned long long), stream_), "reset sizes");
+        M m = model_;
+        A a = axis_;
+        double beta = beta_;
+        std::uint64_t seed = seed_, flip0 = flips_;
+        std::uint32_t nf = max_flips;
+        std::uint64_t tgt = target;
+        std::uint32_t* parent = parent_.data();
+        unsigned long long* sizes = sizes_.data();
+        detail::WolffControl* ctl = ctl_.data();
+        void* args[] = {&m, &a, &beta, &seed, &flip0, &nf, &tgt, &parent, &sizes, &ctl};
+        cuda_check(cudaLaunchCooperativeKernel(kernel(), dim3(grid_), dim3(detail::kThreads), args, 0, stream_),
+                   "Wolff launch");
+        detail::WolffControl h{};
+        cuda_check(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, stream_), "read control");
+        cuda_check(cudaStreamSynchronize(stream_), "Wolff");
+        if (h.bar.status != 0u) throw std::runtime_error("Wolff: a grid barrier wait ran out");
+        if (h.uf_status != 0u) throw std::runtime_error("Wolff: a union-find walk ran past its limit");
+        std::vector<unsigned long long> sz(h.done);
+        if (h.done)
+            cuda_check(cudaMemcpy(sz.data(), sizes, h.done * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+                       "read sizes");
+        for (std::uint32_t k = 0; k < h.done; ++k) {
+            size_sum_ += double(sz[k]);
+            if (sizes_out) sizes_out[k] = sz[k];
+        }
+        flips_ += h.done;
+        return h.touched;
+    }
+
+    M model_;
+    A axis_;
+    std::uint64_t seed_;
+    double beta_;
+    cudaStream_t stream_;
+    Buffer<std::uint32_t> parent_;
+    Buffer<unsigned long long> sizes_;
+    Buffer<detail::WolffControl> ctl_;
+    std::uint32_t grid_ = 1;
+    std::uint64_t flips_ = 0;
+    double size_sum_ = 0.0;
 };
 
 }  // namespace umc::gpu::device

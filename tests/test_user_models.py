@@ -170,3 +170,89 @@ def test_user_table_free_heisenberg(umc, oracle, lib, dims, beta):
         bad = np.nonzero(d > TOL)[0]
         assert len(bad) <= 7 * len(near), (len(bad), len(near))
         assert abs(E.value - obs_o[0, 0]) < 1e-9 * n
+
+
+def device_csr(g):
+    """The CSR of PairTables: row k holds the bonds of the site at colour-major
+    position k, as positions; and for every slot the key of its bond (the slot
+    of the bond in the row of its lower endpoint)."""
+    off, bonds = g.csr()
+    _, _, pos = g.colouring()
+    order = np.argsort(pos)
+    deg = np.diff(off)[order]
+    doff = np.concatenate([[0], np.cumsum(deg)]).astype(np.uint32)
+    dbonds = np.concatenate([pos[bonds[off[i]:off[i + 1]]] for i in order]).astype(np.uint32)
+    rows = np.repeat(np.arange(len(order)), deg)
+    key = np.arange(len(dbonds), dtype=np.uint32)
+    for a in np.nonzero(rows > dbonds)[0]:
+        i, j = rows[a], dbonds[a]
+        back = doff[j] + np.nonzero(dbonds[doff[j]:doff[j + 1]] == i)[0]
+        assert len(back) == 1
+        key[a] = back[0]
+    return pos, doff, dbonds, key
+
+
+def o3_wolff(lib, g, spins, beta, seed, flip0, n, sweeps=0):
+    flat = np.ascontiguousarray(np.asarray(spins, np.float64).reshape(-1)).copy()
+    sizes = np.zeros(max(n, 1), np.uint64)
+    done = _u64(0)
+    mean = _d(0.0)
+    _call(lib, lib.um_o3_wolff(g._h, 1.0, beta, seed, flip0, n, sweeps, _p(flat),
+                               sizes.ctypes.data_as(C.POINTER(_u64)), C.byref(done), C.byref(mean)))
+    return flat.reshape(-1, 3), sizes[:n], done.value, mean.value
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L,beta,flips", [(8, 0.693, 12), (16, 0.693, 6), (12, 0.4, 10), (32, 0.75, 3)])
+def test_user_wolff_flips(umc, oracle, lib, L, beta, flips):
+    """Wolff<PairModel<Vec<3>, DotTerm<3>>, Sphere3>: every flip's cluster size
+    equals the oracle's (driver.hpp:104-162 with the same keyed draws) and the
+    field agrees to 1e-9, unless a bond test sat within 1e-9 of its threshold."""
+    lib.um_o3_wolff.argtypes = [_vp, _d, _d, _u64, _u64, _u32, C.c_int, _dp, C.POINTER(_u64), C.POINTER(_u64),
+                                C.POINTER(_d)]
+    g = umc.cubic_lattice(L, L, L)
+    n = L ** 3
+    pos, doff, dbonds, key = device_csr(g)
+    s = random_unit_vectors(n, 3, L)
+    for f in range(flips):
+        cm = np.empty((n, 3))
+        cm[pos] = s
+        v_o, sz_o, _, margin = oracle.vector_wolff(3, doff, dbonds, key, 1.0, beta, 21, f, 1, cm)
+        s, sz, done, _ = o3_wolff(lib, g, s, beta, 21, f, 1)
+        assert done == 1
+        if margin[0] < MARGIN:
+            continue
+        assert sz[0] == sz_o[0], (f, sz, sz_o)
+        assert np.abs(s - v_o[pos]).max() < TOL
+    # several flips in one launch continue the same sequence
+    a, sa, _, _ = o3_wolff(lib, g, s, beta, 21, 100, 5)
+    b1, sb1, _, _ = o3_wolff(lib, g, s, beta, 21, 100, 2)
+    b2, sb2, _, _ = o3_wolff(lib, g, b1, beta, 21, 102, 3)
+    np.testing.assert_array_equal(a, b2)
+    np.testing.assert_array_equal(sa, np.concatenate([sb1, sb2]))
+
+
+@pytest.mark.gpu
+def test_user_wolff_sweep_flips_until_the_lattice_is_covered(umc, oracle, lib):
+    """Wolff::sweep (driver.hpp:163-173): flips until the flipped sites add up
+    to the lattice; the number of flips and the field equal the oracle's."""
+    lib.um_o3_wolff.argtypes = [_vp, _d, _d, _u64, _u64, _u32, C.c_int, _dp, C.POINTER(_u64), C.POINTER(_u64),
+                                C.POINTER(_d)]
+    L, beta = 10, 0.6
+    g = umc.cubic_lattice(L, L, L)
+    n = L ** 3
+    pos, doff, dbonds, key = device_csr(g)
+    s0 = random_unit_vectors(n, 3, 3)
+    s, _, done, mean = o3_wolff(lib, g, s0, beta, 5, 0, 1, sweeps=1)
+    cm = np.empty((n, 3))
+    cm[pos] = s0
+    touched, f, sizes = 0, 0, []
+    while touched < n:
+        cm, sz, _, margin = oracle.vector_wolff(3, doff, dbonds, key, 1.0, beta, 5, f, 1, cm)
+        assert margin[0] >= MARGIN
+        touched += int(sz[0])
+        sizes.append(int(sz[0]))
+        f += 1
+    assert done == f
+    assert abs(mean - np.mean(sizes)) < 1e-9
+    assert np.abs(s - cm[pos]).max() < TOL
