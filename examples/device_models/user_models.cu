@@ -8,6 +8,8 @@
 //                   as a CellModel (term/plaquette.hpp:13-50);
 //   DotTerm<N>   -- the Heisenberg pair term -J s_i . s_j, driven by Wolff
 //                   (a PairModel is a WolffModel, driver.hpp:69-83);
+//   IsingBondTerm + UpAxis -- the Ising pair term in int32 with FixedAxis,
+//                   driven by Wolff;
 //   CubicHeisenberg -- a whole ModelLike (model.hpp:65-88) for the periodic
 //                   cubic O(3) model whose neighbours come from the site index,
 //                   with no bond table at all;
@@ -15,7 +17,8 @@
 //   Sphere3      -- UniformSphereN<3> (dof/vector.hpp:35-61).
 //
 // Exported with a C ABI for the Python tests and bench.py (ctypes): one-shot
-// runs (um_xy_pair, um_u1_cells, um_heisenberg_cubic, um_o3_wolff) and a persistent XY
+// runs (um_xy_pair, um_u1_cells, um_heisenberg_cubic, um_o3_wolff,
+// um_ising_wolff) and a persistent XY
 // session (um_xy_session_*) whose launches bench.py times.
 #include <umc/device.cuh>
 
@@ -33,6 +36,39 @@ struct Angle
 {
     using dtype = double;
     static constexpr std::size_t size = 1;
+};
+
+struct Spin
+{
+    using dtype = std::int8_t;
+    static constexpr std::size_t size = 1;
+};
+
+// IsingTerm's arithmetic (term/ising.hpp:12-34): E = -J s_i s_j in int32.
+struct IsingBondTerm
+{
+    using dtype = std::int8_t;
+    using energy_type = std::int32_t;
+    static constexpr std::size_t arity = 2;
+    std::int32_t J;
+
+    UMC_HD std::int32_t energy(const std::int8_t* const* l) const { return -J * (std::int32_t(*l[0]) * *l[1]); }
+    UMC_HD std::int32_t delta(std::size_t which, const std::int8_t* old, const std::int8_t* nw,
+                              const std::int8_t* const* l) const
+    {
+        const std::int8_t* fixed = l[which == 0 ? 1 : 0];
+        return -J * (std::int32_t(*nw) * *fixed - std::int32_t(*old) * *fixed);
+    }
+};
+
+// FixedAxis (dof/ising.hpp:41-49): the axis 1, no draw.
+struct UpAxis
+{
+    template <class R>
+    UMC_HD void sample(const std::int8_t*, R&, std::int8_t* out) const
+    {
+        out[0] = 1;
+    }
 };
 
 template <std::size_t N>
@@ -176,7 +212,8 @@ struct CubicHeisenberg
 };
 
 static_assert(ModelLike<CubicHeisenberg> && EnergyModel<CubicHeisenberg>);
-static_assert(WolffModel<PairModel<Vec<3>, DotTerm<3>>>);
+static_assert(WolffModel<PairModel<Vec<3>, DotTerm<3>>> && WolffModel<PairModel<Spin, IsingBondTerm>>);
+static_assert(Axis<UpAxis, std::int8_t> && Axis<Sphere3, double>);
 static_assert(CellTerm<CosineTerm, Angle> && CellTerm<PlaquetteTerm, Angle>);
 static_assert(Proposal<AngleShift, double> && Proposal<Sphere3, double>);
 
@@ -280,6 +317,23 @@ int um_o3_wolff(const umc_graph* g, double J, double beta, std::uint64_t seed, s
         *flips_done = w.flips_done() - flip0;
         *mean_size = w.mean_cluster_size();
         t.download(field, spins, 3);
+    });
+}
+
+// Ising Wolff (IsingBondTerm, UpAxis) on a library pair graph: n flips, their
+// sizes to `sizes`; spins (sites, site order) in/out.
+int um_ising_wolff(const umc_graph* g, std::int32_t J, double beta, std::uint64_t seed, std::uint64_t flip0,
+                   std::uint32_t n, std::int8_t* spins, std::uint64_t* sizes)
+{
+    return guarded([&] {
+        PairTables t(g);
+        Buffer<std::int8_t> field(t.sites());
+        t.upload(field, spins, 1);
+        auto model = t.model<Spin>(field.data(), IsingBondTerm{J});
+        Wolff<decltype(model), UpAxis> w(model, UpAxis{}, seed, beta);
+        w.set_flips(flip0);
+        w.flips(n, sizes);
+        t.download(field, spins, 1);
     });
 }
 

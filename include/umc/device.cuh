@@ -186,6 +186,13 @@ concept Proposal = std::is_trivially_copyable_v<Q> && requires(const Q& q, const
     { q.log_ratio(cur, out) } -> std::convertible_to<double>;
 };
 
+// Wolff's axis argument (driver.hpp:108-109): only sample(cur, rng, out) is
+// used, with cur == nullptr; FixedAxis (dof/ising.hpp:41-49) has nothing else.
+template <class A, class T>
+concept Axis = std::is_trivially_copyable_v<A> && requires(const A& a, const T* cur, T* out, Rng& rng) {
+    { a.sample(cur, rng, out) };
+};
+
 // model.hpp:93-96
 template <class M>
 concept EnergyModel = ModelLike<M> && requires(const M cm, std::size_t loc) {
@@ -1028,7 +1035,7 @@ private:
 // union-find labels the active bonds' components, and the seed's component is
 // reflected, in one cooperative launch for many flips.
 template <WolffModel M, class A>
-    requires Proposal<A, typename M::value_type>
+    requires Axis<A, typename M::value_type>
 class Wolff
 {
 public:
