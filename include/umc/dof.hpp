@@ -16,6 +16,8 @@
 #include <cstdint>
 #include <numbers>
 
+#include "detail.hpp"
+
 namespace umc::gpu {
 
 // dof/dof.hpp:9-13: a degree of freedom names its scalar type and how many of
@@ -45,18 +47,18 @@ struct IsingDof
 struct Flip
 {
     template <class R>
-    void sample(const IsingSpin* cur, R&, IsingSpin* out) const noexcept
+    UMC_FACADE_HD void sample(const IsingSpin* cur, R&, IsingSpin* out) const noexcept
     {
         *out = IsingSpin(-*cur);
     }
-    double log_ratio(const IsingSpin*, const IsingSpin*) const noexcept { return 0.0; }
+    UMC_FACADE_HD double log_ratio(const IsingSpin*, const IsingSpin*) const noexcept { return 0.0; }
 };
 
 // Wolff reflection axis r = +1 (the only reflection of an Ising spin).
 struct FixedAxis
 {
     template <class C, class R>
-    void sample(C, R&, IsingSpin* out) const noexcept
+    UMC_FACADE_HD void sample(C, R&, IsingSpin* out) const noexcept
     {
         *out = 1;
     }
@@ -77,15 +79,15 @@ template <std::size_t N, class T = double>
 struct UniformSphereN
 {
     template <class C, class R>
-    void sample(C, R& rng, T* out) const
+    UMC_FACADE_HD void sample(C, R& rng, T* out) const
     {
         fill<N>(rng, out);
     }
-    double log_ratio(const T*, const T*) const noexcept { return 0.0; }
+    UMC_FACADE_HD double log_ratio(const T*, const T*) const noexcept { return 0.0; }
 
 private:
     template <std::size_t M, class R>
-    static void fill(R& rng, T* out)
+    UMC_FACADE_HD static void fill(R& rng, T* out)
     {
         if constexpr (M == 1) {
             out[0] = rng.uni() < 0.5 ? T(-1) : T(1);
@@ -124,7 +126,7 @@ struct U1Dof
     static constexpr std::size_t size = 1;
 };
 
-inline double plaquette(double t0, double t1, double t2, double t3) noexcept
+UMC_FACADE_HD inline double plaquette(double t0, double t1, double t2, double t3) noexcept
 {
     return std::cos(t0 + t1 - t2 - t3);
 }
@@ -135,11 +137,11 @@ struct U1Shift
     double width = 0.5;
 
     template <class R>
-    void sample(const U1Link* cur, R& rng, U1Link* out) const
+    UMC_FACADE_HD void sample(const U1Link* cur, R& rng, U1Link* out) const
     {
         out->theta = std::remainder(cur->theta + width * (2.0 * rng.uni() - 1.0), 2.0 * std::numbers::pi);
     }
-    double log_ratio(const U1Link*, const U1Link*) const noexcept { return 0.0; }
+    UMC_FACADE_HD double log_ratio(const U1Link*, const U1Link*) const noexcept { return 0.0; }
 };
 
 // ---- SU(N) ---------------------------------------------------------------------

@@ -1,5 +1,7 @@
 // umc/driver.hpp -- Metropolis<M,Q,R> and Wolff<M,A,R> with the reference's
 // constructors and members (driver.hpp:17-68, :92-210), running on the GPU.
+// A PairModel/CellModel with a user-written term, in a file compiled by nvcc,
+// runs through umc/device.cuh instead of an engine chain.
 //
 // A driver owns one device chain (umc_chain) built from the model, its
 // proposal or axis, and the key of its Pcg32.  run() and the Wolff flips go to
@@ -11,12 +13,14 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <type_traits>
 #include <utility>
 #include <vector>
 
 #include "detail.hpp"
 #include "dof.hpp"
+#include "generic.hpp"
 #include "models.hpp"
 #include "rng.hpp"
 
@@ -93,6 +97,13 @@ std::uint64_t key_of(const R& rng)
     return rng.key();
 }
 
+// Drivers of umc/device.cuh for models with a user-written term; defined in
+// umc/device_facade.cuh, which umc/umc.hpp includes in nvcc builds.
+template <class M, class Q>
+std::unique_ptr<UserRunner> make_user_metropolis(M& model, const Q& proposal, std::uint64_t key, double beta);
+template <class M, class A>
+std::unique_ptr<UserRunner> make_user_wolff(M& model, const A& axis, std::uint64_t key, double beta);
+
 }  // namespace detail
 
 template <class M, class Q, class R>
@@ -102,26 +113,45 @@ public:
     Metropolis(M& model, Q proposal, R rng, double beta)
         : model_(model), proposal_(std::move(proposal)), rng_(std::move(rng)), beta_(beta)
     {
-        umc_chain_desc d = model_.chain_desc();
-        detail::ProposalKind<Q>::set(d, proposal_);
-        d.seed = detail::key_of(rng_);
-        chain_ = detail::make_chain(d);
+        if constexpr (detail::UserTermModel<M>) {
+            user_ = detail::make_user_metropolis(model_, proposal_, detail::key_of(rng_), beta_);
+        } else {
+            umc_chain_desc d = model_.chain_desc();
+            detail::ProposalKind<Q>::set(d, proposal_);
+            d.seed = detail::key_of(rng_);
+            chain_ = detail::make_chain(d);
+        }
     }
     Metropolis(const Metropolis&) = delete;
     Metropolis& operator=(const Metropolis&) = delete;
-    ~Metropolis() { model_.detach(chain_.get()); }
+    ~Metropolis()
+    {
+        if constexpr (detail::UserTermModel<M>)
+            model_.detach(static_cast<detail::DeviceCopy*>(user_.get()));
+        else
+            model_.detach(chain_.get());
+    }
 
     // One pass over every site.
     void sweep() { run(1); }
 
-    // n sweeps (one call into the engine).
+    // n sweeps (one call into the engine).  A user-written term runs in one
+    // launch of umc/device.cuh's Metropolis; records() stays empty then.
     void run(std::size_t sweeps)
     {
         if (!sweeps) return;
-        model_.attach(chain_.get());
-        records_.assign(sweeps * UMC_OBS_STRIDE, 0.0);
-        detail::check(umc_metropolis_run(chain_.get(), beta_, sweeps, records_.data()));
-        model_.mark_device(chain_.get());
+        if constexpr (detail::UserTermModel<M>) {
+            auto* copy = static_cast<detail::DeviceCopy*>(user_.get());
+            model_.attach(copy);
+            records_.clear();
+            user_->run(sweeps, nullptr);
+            model_.mark_device(copy);
+        } else {
+            model_.attach(chain_.get());
+            records_.assign(sweeps * UMC_OBS_STRIDE, 0.0);
+            detail::check(umc_metropolis_run(chain_.get(), beta_, sweeps, records_.data()));
+            model_.mark_device(chain_.get());
+        }
     }
 
     // n sweeps, observe(model) after each.
@@ -144,6 +174,7 @@ private:
     R rng_;
     double beta_;
     detail::ChainPtr chain_;
+    std::unique_ptr<detail::UserRunner> user_;
     std::vector<double> records_;
 };
 
@@ -154,15 +185,25 @@ public:
     Wolff(M& model, A axis, R rng, double beta) : model_(model), axis_(std::move(axis)), rng_(std::move(rng)), beta_(beta)
     {
         static_assert(WolffModel<M>, "Wolff needs a pair model (degree, bonds, energy_diff_bond)");
-        umc_chain_desc d = model_.chain_desc();
-        d.proposal = std::is_same_v<A, FixedAxis> ? UMC_PROPOSAL_FLIP : UMC_PROPOSAL_SPHERE;
-        d.wolff_axis = detail::AxisKind<A>::value;
-        d.seed = detail::key_of(rng_);
-        chain_ = detail::make_chain(d);
+        if constexpr (detail::UserTermModel<M>) {
+            user_ = detail::make_user_wolff(model_, axis_, detail::key_of(rng_), beta_);
+        } else {
+            umc_chain_desc d = model_.chain_desc();
+            d.proposal = std::is_same_v<A, FixedAxis> ? UMC_PROPOSAL_FLIP : UMC_PROPOSAL_SPHERE;
+            d.wolff_axis = detail::AxisKind<A>::value;
+            d.seed = detail::key_of(rng_);
+            chain_ = detail::make_chain(d);
+        }
     }
     Wolff(const Wolff&) = delete;
     Wolff& operator=(const Wolff&) = delete;
-    ~Wolff() { model_.detach(chain_.get()); }
+    ~Wolff()
+    {
+        if constexpr (detail::UserTermModel<M>)
+            model_.detach(static_cast<detail::DeviceCopy*>(user_.get()));
+        else
+            model_.detach(chain_.get());
+    }
 
     // One cluster flip; returns how many sites it flipped.
     std::size_t flip()
@@ -201,9 +242,16 @@ public:
     {
         if (!n) return;
         std::vector<std::uint64_t> s(n);
-        model_.attach(chain_.get());
-        detail::check(umc_wolff_run(chain_.get(), beta_, n, s.data(), nullptr));
-        model_.mark_device(chain_.get());
+        if constexpr (detail::UserTermModel<M>) {
+            auto* copy = static_cast<detail::DeviceCopy*>(user_.get());
+            model_.attach(copy);
+            user_->run(n, s.data());
+            model_.mark_device(copy);
+        } else {
+            model_.attach(chain_.get());
+            detail::check(umc_wolff_run(chain_.get(), beta_, n, s.data(), nullptr));
+            model_.mark_device(chain_.get());
+        }
         for (std::size_t k = 0; k < n; ++k) {
             size_sum_ += double(s[k]);
             if (sizes) sizes[k] = s[k];
@@ -220,6 +268,7 @@ private:
     R rng_;
     double beta_;
     detail::ChainPtr chain_;
+    std::unique_ptr<detail::UserRunner> user_;
     std::size_t n_flips_ = 0;
     double size_sum_ = 0.0;
 };

@@ -9,9 +9,12 @@
 // energy_diff_bond) follow the reference's arithmetic.  A driver runs these
 // models on the device kernels of the matching example model: IsingTerm ->
 // Ising, HeisenbergTerm<N> -> VectorSpin<N>, U1PlaquetteTerm -> U(1) links,
-// SUPlaquetteTerm<N> -> SU(N) links.  A term the engine has no kernel for is a
-// compile-time error (the device cannot run arbitrary host code, and there is
-// no CPU fallback).  As in the reference, every component starts at zero.
+// SUPlaquetteTerm<N> -> SU(N) links.  Any other term is a user-written one:
+// in a file compiled by nvcc, whose term members are __host__ __device__,
+// the drivers run it through umc/device.cuh (the generic device Metropolis
+// and Wolff); under g++ it is a compile-time error, since g++ cannot build
+// device code and there is no CPU fallback.  As in the reference, every
+// component starts at zero.
 #pragma once
 
 #include <array>
@@ -154,11 +157,27 @@ struct SUPlaquetteTerm
 namespace detail {
 // Which device model runs a (degree of freedom, term) pair, and the host
 // scalars of one site in the reference's data() layout.
+// No built-in device model: a user-written term.  Under nvcc it runs through
+// umc/device.cuh with the field in the dtype itself; g++ builds refuse it.
 template <class D, class Term>
 struct DeviceTerm
 {
     static constexpr bool ok = false;
+    using HS = typename D::dtype;
+    using DevT = typename D::dtype;
+    static constexpr std::size_t scalars = D::size;
 };
+
+#if defined(__CUDACC__)
+inline constexpr bool kUserTermsOnDevice = true;
+#else
+inline constexpr bool kUserTermsOnDevice = false;
+#endif
+
+// A PairModel or CellModel whose term has no built-in device model.
+template <class M>
+concept UserTermModel = requires { typename M::term_type; typename M::dof_type; } &&
+                        !DeviceTerm<typename M::dof_type, typename M::term_type>::ok;
 template <>
 struct DeviceTerm<IsingDof, IsingTerm>
 {
@@ -210,7 +229,9 @@ template <class D, class Term, class G>
 class PairModel : public detail::TermField<D, Term>
 {
     using DT = detail::DeviceTerm<D, Term>;
-    static_assert(DT::ok, "the device engine provides IsingTerm and HeisenbergTerm<N> pair terms");
+    static_assert(DT::ok || detail::kUserTermsOnDevice,
+                  "a user-written pair term runs on the device when this file is compiled by nvcc "
+                  "(umc/device.cuh); g++ builds run IsingTerm and HeisenbergTerm<N>");
     static_assert(std::is_same_v<G, PairGraph<>>, "the device engine takes the unweighted PairGraph<>");
 
 public:
@@ -219,6 +240,8 @@ public:
     using energy_type = typename Term::energy_type;
     static constexpr std::size_t size = D::size;
     using bond_type = typename G::bond_type;
+    using dof_type = D;
+    using term_type = Term;
 
     PairModel(G graph, Term term) : graph_(std::move(graph)), term_(std::move(term))
     {
@@ -234,6 +257,7 @@ public:
     std::size_t degree(std::size_t i) const noexcept { return graph_.degree(i); }
     const bond_type* bonds(std::size_t i) const noexcept { return graph_.bonds(i); }
     const Term& term() const noexcept { return term_; }
+    const G& graph() const noexcept { return graph_; }
 
     energy_type energy_at(std::size_t i) const
     {
@@ -288,8 +312,11 @@ template <class D, class Term, class List>
 class CellModel : public detail::TermField<D, Term>
 {
     using DT = detail::DeviceTerm<D, Term>;
-    static_assert(DT::ok, "the device engine provides U1PlaquetteTerm and SUPlaquetteTerm<N> cell terms");
-    static_assert(std::is_same_v<List, CellComplex<4>>, "the device engine takes CellComplex<4> plaquette lists");
+    static_assert(DT::ok || detail::kUserTermsOnDevice,
+                  "a user-written cell term runs on the device when this file is compiled by nvcc "
+                  "(umc/device.cuh); g++ builds run U1PlaquetteTerm and SUPlaquetteTerm<N>");
+    static_assert(std::is_same_v<List, CellComplex<List::arity>>, "the device engine takes CellComplex<A> lists");
+    static_assert(!DT::ok || List::arity == 4, "the built-in cell terms are plaquettes of CellComplex<4>");
 
 public:
     using dtype = typename D::dtype;
@@ -297,6 +324,8 @@ public:
     using energy_type = typename Term::energy_type;
     static constexpr std::size_t size = D::size;
     static constexpr std::size_t arity = List::arity;
+    using dof_type = D;
+    using term_type = Term;
 
     CellModel(List list, Term term) : list_(std::move(list)), term_(std::move(term))
     {
@@ -311,6 +340,7 @@ public:
         return reinterpret_cast<const dtype*>(this->host_.data());
     }
     const Term& term() const noexcept { return term_; }
+    const List& list() const noexcept { return list_; }
     std::span<const std::uint32_t, arity> cell_sites(std::size_t c) const { return list_.cell(c); }
 
     energy_type cell_energy(std::size_t c) const

@@ -15,6 +15,10 @@
 #include "models.hpp"
 #include "rng.hpp"
 
+#if defined(__CUDACC__)
+#include "device_facade.cuh"  // user-written terms on the device (nvcc builds)
+#endif
+
 #ifndef UMC_NO_GLOBAL_NAMES
 using umc::gpu::Bond;
 using umc::gpu::Cell;

@@ -1,0 +1,160 @@
+// A reference-style program whose models use terms written by the user,
+// built with nvcc so that the facade's drivers run those terms on the device
+// (umc/device_facade.cuh).  Apart from the __host__ __device__ markers on the
+// terms, it is what a user of the reference writes: PairModel / CellModel
+// over square_lattice / hypercubic_plaquettes, Metropolis and Wolff with the
+// reference's proposals and axes, Pcg32 for the keys, data() to read back.
+//
+// Writes to argv[1], in order: the XY start and end angles, the Ising start
+// and end spins and the 12 cluster sizes, the U(1) start and end angles.
+#include <umc/umc.hpp>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <numbers>
+#include <vector>
+
+// E = -J cos(t_i - t_j) on U1Link angles: the XY model as a user pair term.
+struct XYAngleTerm
+{
+    using dtype = U1Link;
+    using energy_type = double;
+    static constexpr std::size_t arity = 2;
+    double J = 1.0;
+
+    __host__ __device__ energy_type energy(const dtype* const* l) const { return -J * cos(l[0]->theta - l[1]->theta); }
+    __host__ __device__ energy_type delta(std::size_t which, const dtype* old, const dtype* nw,
+                                          const dtype* const* l) const
+    {
+        const dtype* fixed = l[which == 0 ? 1 : 0];
+        return -J * (cos(nw->theta - fixed->theta) - cos(old->theta - fixed->theta));
+    }
+};
+
+// E = -J s_i s_j on int8 spins, in int32 (IsingTerm's arithmetic, rewritten by the user).
+struct MyIsingTerm
+{
+    using dtype = IsingSpin;
+    using energy_type = std::int32_t;
+    static constexpr std::size_t arity = 2;
+    std::int32_t J = 1;
+
+    __host__ __device__ energy_type energy(const dtype* const* l) const { return -J * (std::int32_t(*l[0]) * *l[1]); }
+    __host__ __device__ energy_type delta(std::size_t which, const dtype* old, const dtype* nw,
+                                          const dtype* const* l) const
+    {
+        const dtype* fixed = l[which == 0 ? 1 : 0];
+        return -J * (std::int32_t(*nw) * *fixed - std::int32_t(*old) * *fixed);
+    }
+};
+
+// S_p = beta (1 - cos(t0 + t1 - t2 - t3)) as a user cell term of arity 4.
+struct MyPlaquetteTerm
+{
+    using dtype = U1Link;
+    using energy_type = double;
+    static constexpr std::size_t arity = 4;
+    double beta = 1.0;
+
+    __host__ __device__ static double angle_cos(const double* t) { return cos(t[0] + t[1] - t[2] - t[3]); }
+    __host__ __device__ energy_type energy(const dtype* const* l) const
+    {
+        const double t[4] = {l[0]->theta, l[1]->theta, l[2]->theta, l[3]->theta};
+        return beta * (1.0 - angle_cos(t));
+    }
+    __host__ __device__ energy_type delta(std::size_t which, const dtype*, const dtype* nw,
+                                          const dtype* const* l) const
+    {
+        double t[4] = {l[0]->theta, l[1]->theta, l[2]->theta, l[3]->theta};
+        const double before = angle_cos(t);
+        t[which] = nw->theta;
+        return beta * (before - angle_cos(t));
+    }
+};
+
+static_assert(CellTerm<XYAngleTerm, U1Dof> && CellTerm<MyIsingTerm, IsingDof> && CellTerm<MyPlaquetteTerm, U1Dof>);
+
+template <class T>
+static void put(std::FILE* f, const T* p, std::size_t n)
+{
+    if (std::fwrite(p, sizeof(T), n, f) != n) throw std::runtime_error("write failed");
+}
+
+template <class M>
+static std::vector<double> angles(const M& m)
+{
+    std::vector<double> t(m.sites());
+    for (std::size_t i = 0; i < m.sites(); ++i) t[i] = m.data()[i].theta;
+    return t;
+}
+
+int main(int argc, char** argv)
+{
+    if (argc < 2) return 2;
+    std::FILE* out = std::fopen(argv[1], "wb");
+    if (!out) return 2;
+    try {
+        // XY: PairModel<U1Dof, user term, PairGraph<>> with U1Shift, 3 sweeps then 2 observed sweeps
+        PairModel<U1Dof, XYAngleTerm, PairGraph<>> xy(square_lattice(32, 32), XYAngleTerm{1.0});
+        Pcg32 init(5, 3);
+        for (std::size_t i = 0; i < xy.sites(); ++i) {
+            const U1Link l{2.0 * std::numbers::pi * init.uni() - std::numbers::pi};
+            xy.update(i, &l);
+        }
+        const auto xy0 = angles(xy);
+        {
+            Metropolis metro(xy, U1Shift{1.0}, Pcg32(4, 0), 1.1);
+            metro.run(3);
+            double e = 0.0;
+            metro.sample(2, [&](const auto& m) {
+                for (std::size_t i = 0; i < m.sites(); ++i) e += 0.5 * m.energy_at(i);
+            });
+            std::printf("XY user term: E per site after 5 sweeps %.6f\n", e / 2.0 / double(xy.sites()));
+        }
+        const auto xy1 = angles(xy);
+        put(out, xy0.data(), xy0.size());
+        put(out, xy1.data(), xy1.size());
+
+        // Ising: PairModel<IsingDof, user term, PairGraph<>>, Wolff with FixedAxis, 12 flips
+        PairModel<IsingDof, MyIsingTerm, PairGraph<>> ising(square_lattice(24, 24), MyIsingTerm{1});
+        for (std::size_t i = 0; i < ising.sites(); ++i) {
+            const IsingSpin s = init.uni() < 0.5 ? IsingSpin(1) : IsingSpin(-1);
+            ising.update(i, &s);
+        }
+        std::vector<IsingSpin> s0(ising.data(), ising.data() + ising.sites());
+        std::vector<std::uint64_t> sizes(12);
+        {
+            Wolff wolf(ising, FixedAxis{}, Pcg32(13, 0), 0.44);
+            wolf.flips(12, sizes.data());
+            std::printf("Ising user term: mean cluster %.2f\n", wolf.mean_cluster_size());
+        }
+        std::vector<IsingSpin> s1(ising.data(), ising.data() + ising.sites());
+        put(out, s0.data(), s0.size());
+        put(out, s1.data(), s1.size());
+        put(out, sizes.data(), sizes.size());
+
+        // U(1): CellModel<U1Dof, user cell term, CellComplex<4>> on the 4^4 plaquettes, 2 sweeps
+        CellModel<U1Dof, MyPlaquetteTerm, CellComplex<4>> u1(hypercubic_plaquettes(4), MyPlaquetteTerm{1.3});
+        for (std::size_t i = 0; i < u1.sites(); ++i) {
+            const U1Link l{2.0 * std::numbers::pi * init.uni() - std::numbers::pi};
+            u1.update(i, &l);
+        }
+        const auto u0 = angles(u1);
+        {
+            Metropolis metro(u1, U1Shift{0.7}, Pcg32(9, 0), 1.0);
+            metro.run(2);
+        }
+        const auto u1a = angles(u1);
+        std::printf("U(1) user cell term: S = %.6f\n", u1.total_energy());
+        put(out, u0.data(), u0.size());
+        put(out, u1a.data(), u1a.size());
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "error: %s\n", e.what());
+        std::fclose(out);
+        return 1;
+    }
+    std::fclose(out);
+    std::printf("ok\n");
+    return 0;
+}

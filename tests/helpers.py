@@ -109,3 +109,23 @@ def mlp_init(seed: int, scale: float = 1.0):
     W3 = rng.standard_normal((64, 16)) * np.sqrt(1 / 64) * scale
     b3 = rng.standard_normal(16) * 0.1
     return np.concatenate([W1.ravel(), b1, W2.ravel(), b2, W3.ravel(), b3]).astype(np.float32).astype(np.float64)
+
+
+def device_csr(g):
+    """The CSR of PairTables: row k holds the bonds of the site at colour-major
+    position k, as positions; and for every slot the key of its bond (the slot
+    of the bond in the row of its lower endpoint)."""
+    off, bonds = g.csr()
+    _, _, pos = g.colouring()
+    order = np.argsort(pos)
+    deg = np.diff(off)[order]
+    doff = np.concatenate([[0], np.cumsum(deg)]).astype(np.uint32)
+    dbonds = np.concatenate([pos[bonds[off[i]:off[i + 1]]] for i in order]).astype(np.uint32)
+    rows = np.repeat(np.arange(len(order)), deg)
+    key = np.arange(len(dbonds), dtype=np.uint32)
+    for a in np.nonzero(rows > dbonds)[0]:
+        i, j = rows[a], dbonds[a]
+        back = doff[j] + np.nonzero(dbonds[doff[j]:doff[j + 1]] == i)[0]
+        assert len(back) == 1
+        key[a] = back[0]
+    return pos, doff, dbonds, key

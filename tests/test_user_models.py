@@ -20,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(os.path.dirname(HERE), "examples", "device_models"))
 sys.path.insert(0, HERE)
 
-from helpers import checker_position, cubic_edges, random_unit_vectors, relabel_edges  # noqa: E402
+from helpers import checker_position, cubic_edges, device_csr, random_unit_vectors, relabel_edges  # noqa: E402
 
 TOL = 1e-9
 MARGIN = 1e-9
@@ -170,26 +170,6 @@ def test_user_table_free_heisenberg(umc, oracle, lib, dims, beta):
         bad = np.nonzero(d > TOL)[0]
         assert len(bad) <= 7 * len(near), (len(bad), len(near))
         assert abs(E.value - obs_o[0, 0]) < 1e-9 * n
-
-
-def device_csr(g):
-    """The CSR of PairTables: row k holds the bonds of the site at colour-major
-    position k, as positions; and for every slot the key of its bond (the slot
-    of the bond in the row of its lower endpoint)."""
-    off, bonds = g.csr()
-    _, _, pos = g.colouring()
-    order = np.argsort(pos)
-    deg = np.diff(off)[order]
-    doff = np.concatenate([[0], np.cumsum(deg)]).astype(np.uint32)
-    dbonds = np.concatenate([pos[bonds[off[i]:off[i + 1]]] for i in order]).astype(np.uint32)
-    rows = np.repeat(np.arange(len(order)), deg)
-    key = np.arange(len(dbonds), dtype=np.uint32)
-    for a in np.nonzero(rows > dbonds)[0]:
-        i, j = rows[a], dbonds[a]
-        back = doff[j] + np.nonzero(dbonds[doff[j]:doff[j + 1]] == i)[0]
-        assert len(back) == 1
-        key[a] = back[0]
-    return pos, doff, dbonds, key
 
 
 def o3_wolff(lib, g, spins, beta, seed, flip0, n, sweeps=0):
