@@ -18,7 +18,7 @@
 //
 // Exported with a C ABI for the Python tests and bench.py (ctypes): one-shot
 // runs (um_xy_pair, um_u1_cells, um_heisenberg_cubic, um_o3_wolff,
-// um_ising_wolff) and a persistent XY
+// um_ising_wolff, um_lattice_o3) and a persistent XY
 // session (um_xy_session_*) whose launches bench.py times.
 #include <umc/device.cuh>
 
@@ -214,6 +214,7 @@ struct CubicHeisenberg
 static_assert(ModelLike<CubicHeisenberg> && EnergyModel<CubicHeisenberg>);
 static_assert(WolffModel<PairModel<Vec<3>, DotTerm<3>>> && WolffModel<PairModel<Spin, IsingBondTerm>>);
 static_assert(Axis<UpAxis, std::int8_t> && Axis<Sphere3, double>);
+static_assert(WolffModel<LatticePairModel<Vec<3>, DotTerm<3>>> && EnergyModel<LatticePairModel<Vec<3>, DotTerm<3>>>);
 static_assert(CellTerm<CosineTerm, Angle> && CellTerm<PlaquetteTerm, Angle>);
 static_assert(Proposal<AngleShift, double> && Proposal<Sphere3, double>);
 
@@ -334,6 +335,31 @@ int um_ising_wolff(const umc_graph* g, std::int32_t J, double beta, std::uint64_
         w.set_flips(flip0);
         w.flips(n, sizes);
         t.download(field, spins, 1);
+    });
+}
+
+// O(3) with the user's DotTerm<3> on a table-free RegularLattice (Lx even,
+// Ly and Lz even or 1): wolff == 0, n Metropolis sweeps with Sphere3 from
+// sweep `first`; wolff == 1, n Wolff flips with the Sphere3 axis from flip
+// `first`, sizes to `sizes`.  spins (sites x 3, site order) in/out.
+int um_lattice_o3(std::uint32_t Lx, std::uint32_t Ly, std::uint32_t Lz, double J, double beta, std::uint64_t seed,
+                  std::uint64_t first, std::uint32_t n, int wolff, double* spins, std::uint64_t* sizes)
+{
+    return guarded([&] {
+        LatticeTables t(RegularLattice{Lx, Ly, Lz});
+        Buffer<double> field(std::size_t(t.sites()) * 3);
+        t.upload(field, spins, 3);
+        auto model = t.model<Vec<3>>(field.data(), DotTerm<3>{J});
+        if (wolff) {
+            Wolff<decltype(model), Sphere3> w(model, Sphere3{}, seed, beta);
+            w.set_flips(first);
+            w.flips(n, sizes);
+        } else {
+            Metropolis<decltype(model), Sphere3> mc(model, Sphere3{}, t.classes(), seed, beta);
+            mc.set_sweeps(first);
+            mc.run(n);
+        }
+        t.download(field, spins, 3);
     });
 }
 

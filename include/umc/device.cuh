@@ -210,16 +210,24 @@ concept CellEnergyModel = ModelLike<M> && requires(const M cm, std::size_t c) {
 // The device tests each bond once, from its lower endpoint, with a draw keyed
 // by that id, so the ids of the bonds i tests (those with j > i) must be
 // distinct.  bond_type has a member j, the neighbour.
+//
+// A model without bond storage (a lattice that computes its neighbours) gives
+// bond(i, a) by value instead of the row pointer bonds(i).
 template <class M>
-concept WolffModel = ModelLike<M> && requires(const M cm, std::size_t loc, const typename M::value_type* p,
-                                              const typename M::bond_type& b, std::size_t a) {
-    typename M::bond_type;
-    { cm.degree(loc) } -> std::convertible_to<std::size_t>;
-    { cm.bonds(loc) } -> std::convertible_to<const typename M::bond_type*>;
-    { cm.energy_diff_bond(loc, b, p) } -> std::convertible_to<double>;
-    { cm.bond_id(loc, a) } -> std::convertible_to<std::uint32_t>;
-    { b.j } -> std::convertible_to<std::size_t>;
-};
+concept WolffModel =
+    ModelLike<M> &&
+    requires(const M cm, std::size_t loc, const typename M::value_type* p, const typename M::bond_type& b,
+             std::size_t a) {
+        typename M::bond_type;
+        { cm.degree(loc) } -> std::convertible_to<std::size_t>;
+        { cm.energy_diff_bond(loc, b, p) } -> std::convertible_to<double>;
+        { cm.bond_id(loc, a) } -> std::convertible_to<std::uint32_t>;
+        { b.j } -> std::convertible_to<std::size_t>;
+    } &&
+    (requires(const M cm, std::size_t loc) { { cm.bonds(loc) } -> std::convertible_to<const typename M::bond_type*>; } ||
+     requires(const M cm, std::size_t loc, std::size_t a) {
+         { cm.bond(loc, a) } -> std::convertible_to<typename M::bond_type>;
+     });
 
 // ------------------------------------------------------------------ colour classes
 
@@ -643,6 +651,163 @@ private:
     Buffer<std::uint8_t> inc_which_;
 };
 
+// ------------------------------------------------------------------ tables without storage
+
+// A periodic Lx x Ly x Lz lattice whose bonds are computed, not stored
+// (square_lattice's and cubic_lattice's sites and bonds; Lz = 1 in 2D).
+// Lx is even and Ly, Lz are even or 1, so the checkerboard is a proper
+// 2-colouring and sites 2r, 2r + 1 share a row;
+// device site k is the colour-major position ((x+y+z)&1) n/2 + s/2 of
+// reference site s = (z Ly + y) Lx + x.  Bonds of k, in the order +x, -x,
+// +y, -y, +z, -z over the extents above 1, are the neighbours' device sites.
+struct RegularLattice
+{
+    std::uint32_t Lx, Ly, Lz;
+
+    UMC_HD std::uint32_t sites() const { return Lx * Ly * Lz; }
+    UMC_HD std::uint32_t degree() const { return 2u * ((Lx > 1) + (Ly > 1) + (Lz > 1)); }
+    UMC_HD std::uint32_t index_of(std::uint32_t x, std::uint32_t y, std::uint32_t z) const
+    {
+        const std::uint32_t s = (z * Ly + y) * Lx + x;
+        return ((x + y + z) & 1u) * (sites() / 2) + s / 2;
+    }
+    // Coordinates of device site k.
+    UMC_HD void coords(std::uint32_t k, std::uint32_t& x, std::uint32_t& y, std::uint32_t& z) const
+    {
+        const std::uint32_t half = sites() / 2;
+        const std::uint32_t c = k >= half ? 1u : 0u;
+        const std::uint32_t s0 = 2u * (k - c * half);  // the even site of the pair; same row as s0 + 1
+        y = (s0 / Lx) % Ly;
+        z = s0 / (Lx * Ly);
+        x = s0 % Lx + ((c + y + z + s0 % Lx) & 1u);
+    }
+    UMC_HD std::uint32_t neighbour(std::uint32_t k, std::uint32_t a) const
+    {
+        std::uint32_t x, y, z;
+        coords(k, x, y, z);
+        std::uint32_t d = a >> 1;
+        const bool minus = a & 1u;
+        if (d >= 1 && Ly == 1) ++d;
+        if (d == 0) x = minus ? (x + Lx - 1) % Lx : (x + 1) % Lx;
+        else if (d == 1) y = minus ? (y + Ly - 1) % Ly : (y + 1) % Ly;
+        else z = minus ? (z + Lz - 1) % Lz : (z + 1) % Lz;
+        return index_of(x, y, z);
+    }
+};
+
+namespace detail {
+inline Colouring checkerboard(const RegularLattice& l)
+{
+    if (l.Lx < 2 || l.Lx % 2 || l.Ly < 1 || l.Lz < 1 || (l.Ly > 1 && l.Ly % 2) || (l.Lz > 1 && l.Lz % 2))
+        throw std::invalid_argument("RegularLattice: Lx must be even, Ly and Lz even or 1");
+    if (std::uint64_t(l.Lx) * l.Ly * l.Lz * l.degree() >= (std::uint64_t(1) << 32))
+        throw std::invalid_argument("RegularLattice: sites x degree must stay below 2^32");
+    Colouring c;
+    c.count = 2;
+    c.colour.resize(l.sites());
+    c.position.resize(l.sites());
+    for (std::uint32_t z = 0, s = 0; z < l.Lz; ++z)
+        for (std::uint32_t y = 0; y < l.Ly; ++y)
+            for (std::uint32_t x = 0; x < l.Lx; ++x, ++s) {
+                c.colour[s] = (x + y + z) & 1u;
+                c.position[s] = l.index_of(x, y, z);
+            }
+    return c;
+}
+}  // namespace detail
+
+// PairModel over a RegularLattice: neighbours computed from the device index,
+// no CSR bytes read.  A ModelLike, EnergyModel and WolffModel (bond(i, a) by
+// value; bond_id(i, a) = i * degree + a).
+template <class D, class Term>
+    requires CellTerm<Term, D> && (Term::arity == 2)
+struct LatticePairModel
+{
+    using dtype = typename D::dtype;
+    using value_type = dtype;
+    using energy_type = typename Term::energy_type;
+    using bond_type = Bond;
+    static constexpr std::size_t size = D::size;
+
+    dtype* field;
+    RegularLattice lattice;
+    Term term;
+
+    UMC_HD std::size_t sites() const { return lattice.sites(); }
+    UMC_HD const dtype* data() const { return field; }
+    UMC_HD dtype* data() { return field; }
+    UMC_HD std::size_t degree(std::size_t) const { return lattice.degree(); }
+    UMC_HD Bond bond(std::size_t i, std::size_t a) const
+    {
+        return Bond{lattice.neighbour(std::uint32_t(i), std::uint32_t(a))};
+    }
+    UMC_HD std::uint32_t bond_id(std::size_t i, std::size_t a) const
+    {
+        return std::uint32_t(i) * lattice.degree() + std::uint32_t(a);
+    }
+
+    // model/pair.hpp:38-49
+    UMC_HD energy_type energy_at(std::size_t i) const
+    {
+        energy_type e = 0;
+        const dtype* si = field + i * size;
+        for (std::uint32_t a = 0; a < lattice.degree(); ++a) {
+            const dtype* links[2] = {si, field + std::size_t(lattice.neighbour(std::uint32_t(i), a)) * size};
+            e += term.energy(links);
+        }
+        return e;
+    }
+    // model/pair.hpp:52-63
+    UMC_HD energy_type energy_diff_at(std::size_t i, const dtype* p) const
+    {
+        energy_type d = 0;
+        const dtype* si = field + i * size;
+        for (std::uint32_t a = 0; a < lattice.degree(); ++a) {
+            const dtype* links[2] = {si, field + std::size_t(lattice.neighbour(std::uint32_t(i), a)) * size};
+            d += term.delta(0, si, p, links);
+        }
+        return d;
+    }
+    // model/pair.hpp:66-72
+    UMC_HD energy_type energy_diff_bond(std::size_t i, const Bond& b, const dtype* p) const
+    {
+        const dtype* sj = field + std::size_t(b.j) * size;
+        const dtype* links[2] = {sj, field + i * size};
+        return term.delta(0, sj, p, links);
+    }
+    UMC_HD void update(std::size_t i, const dtype* p)
+    {
+        for (std::size_t k = 0; k < size; ++k) field[i * size + k] = p[k];
+    }
+};
+
+// The two colour classes of a RegularLattice and the site-order transfers;
+// nothing about its bonds is stored.
+class LatticeTables : public ColourMajor
+{
+public:
+    explicit LatticeTables(RegularLattice l)
+        : LatticeTables(l, detail::checkerboard(l))
+    {}
+
+    const RegularLattice& lattice() const noexcept { return lattice_; }
+    const ClassTable& classes() const noexcept { return classes_; }
+
+    template <class D, class Term>
+    LatticePairModel<D, Term> model(typename D::dtype* field, Term term) const
+    {
+        return LatticePairModel<D, Term>{field, lattice_, term};
+    }
+
+private:
+    LatticeTables(RegularLattice l, const detail::Colouring& c)
+        : ColourMajor(c), lattice_(l), classes_(Classes::identity(class_begin()))
+    {}
+
+    RegularLattice lattice_;
+    ClassTable classes_;
+};
+
 // ------------------------------------------------------------------ kernels
 
 namespace detail {
@@ -840,6 +1005,17 @@ __device__ __forceinline__ void uf_unite(std::uint32_t* parent, std::uint32_t a,
     atomicOr(status, 2u);
 }
 
+// The a-th bond of i: from the row pointer, or by value from a model that
+// computes its bonds.
+template <class M>
+__device__ __forceinline__ typename M::bond_type bond_of(const M& m, std::uint32_t i, std::size_t a)
+{
+    if constexpr (requires { m.bond(std::size_t(i), a); })
+        return m.bond(i, a);
+    else
+        return m.bonds(i)[a];
+}
+
 // out = s - 2 (s . r) r, in T arithmetic as Wolff::flip does (driver.hpp:127-130).
 template <class T, std::size_t D>
 __device__ __forceinline__ void reflect(const T* s, const T* r, T* out)
@@ -882,14 +1058,14 @@ __global__ void __launch_bounds__(kThreads) wolff_flips(M m, A axis, double beta
 
         const std::uint64_t kbond = key_base(key_seed(seed, counter, kTagBond));
         for (std::uint32_t i = t; i < n; i += stride) {
-            const auto* row = m.bonds(i);
             const std::size_t deg = m.degree(i);
             for (std::size_t a = 0; a < deg; ++a) {
-                const std::uint32_t j = std::uint32_t(row[a].j);
+                const auto b = bond_of(m, i, a);
+                const std::uint32_t j = std::uint32_t(b.j);
                 if (j <= i) continue;
                 T nb[D];
                 reflect<T, D>(m.data() + std::size_t(j) * D, r, nb);
-                const double dE = m.energy_diff_bond(i, row[a], nb);
+                const double dE = m.energy_diff_bond(i, b, nb);
                 Rng u(KeyedPcg::open(kbond, m.bond_id(i, a)));
                 if (u.uni() < 1.0 - exp(-beta * dE)) uf_unite(parent, i, j, &ctl->uf_status);
             }

@@ -257,3 +257,67 @@ def test_user_ising_wolff_is_bit_exact(umc, oracle, lib, L, beta):
     s_o, sz_o, _, _ = oracle.ising_wolff(doff, dbonds, key, 1, beta, 13, 7, 20, cm)
     np.testing.assert_array_equal(sizes, sz_o)
     np.testing.assert_array_equal(s, s_o[pos])
+
+
+def lattice_csr(Lx, Ly, Lz):
+    """RegularLattice's device numbering (colour-major checkerboard) and its
+    bond rows in the order +x, -x, +y, -y, +z, -z over the extents above 1,
+    with the Wolff keys k * degree + a from each bond's lower endpoint."""
+    n = Lx * Ly * Lz
+    s = np.arange(n)
+    x, y, z = s % Lx, (s // Lx) % Ly, s // (Lx * Ly)
+    pos = (((x + y + z) & 1) * (n // 2) + s // 2).astype(np.uint32)
+    steps = [(1, 0, 0), (-1, 0, 0)]
+    if Ly > 1:
+        steps += [(0, 1, 0), (0, -1, 0)]
+    if Lz > 1:
+        steps += [(0, 0, 1), (0, 0, -1)]
+    deg = len(steps)
+    rows = np.empty((n, deg), np.uint32)
+    for a, (dx, dy, dz) in enumerate(steps):
+        t = (((z + dz) % Lz) * Ly + (y + dy) % Ly) * Lx + (x + dx) % Lx
+        rows[pos, a] = pos[t]
+    off = (np.arange(n + 1) * deg).astype(np.uint32)
+    bonds = rows.reshape(-1)
+    key = np.arange(n * deg, dtype=np.uint32)
+    for k in range(n):
+        for a in range(deg):
+            j = rows[k, a]
+            if j < k:
+                back = np.nonzero(rows[j] == k)[0]
+                assert len(back) == 1
+                key[k * deg + a] = j * deg + back[0]
+    return pos, off, bonds, key
+
+
+def lattice_o3(lib, dims, spins, beta, seed, first, n, wolff):
+    lib.um_lattice_o3.argtypes = [_u32, _u32, _u32, _d, _d, _u64, _u64, _u32, C.c_int, _dp, _vp]
+    flat = np.ascontiguousarray(np.asarray(spins, np.float64).reshape(-1)).copy()
+    sizes = np.zeros(max(n, 1), np.uint64)
+    _call(lib, lib.um_lattice_o3(*dims, 1.0, beta, seed, first, n, wolff, _p(flat), sizes.ctypes.data))
+    return flat.reshape(-1, 3), sizes[:n]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(8, 8, 8), (16, 6, 1), (12, 4, 10)])
+def test_user_term_on_table_free_lattice(umc, oracle, lib, dims):
+    """LatticePairModel<Vec<3>, DotTerm<3>> over RegularLattice (no CSR on the
+    device): Metropolis sweeps and Wolff flips equal the oracle on the same
+    numbering and bond keys."""
+    n = int(np.prod(dims))
+    pos, off, bonds, key = lattice_csr(*dims)
+    s = random_unit_vectors(n, 3, 8)
+    for sweep in range(3):
+        cm = np.empty((n, 3))
+        cm[pos] = s
+        v_o, _, margin = oracle.vector_metropolis(3, off, bonds, 1.0, 0.7, 0, 0.0, 17, sweep, 1, cm)
+        s, _ = lattice_o3(lib, dims, s, 0.7, 17, sweep, 1, 0)
+        d = np.abs(s - v_o[pos]).max(axis=1)
+        assert (d > TOL).sum() <= 7 * (np.abs(margin) < MARGIN).sum()
+    cm = np.empty((n, 3))
+    cm[pos] = s
+    v_o, sz_o, _, margin = oracle.vector_wolff(3, off, bonds, key, 1.0, 0.7, 23, 0, 6, cm)
+    s2, sz = lattice_o3(lib, dims, s, 0.7, 23, 0, 6, 1)
+    if margin.min() >= MARGIN:
+        np.testing.assert_array_equal(sz, sz_o)
+        assert np.abs(s2 - v_o[pos]).max() < TOL
