@@ -49,10 +49,11 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", choices=["o3", "ising", "su3", "xybatch", "u1batch", "u1learned", "userxy"],
+    p.add_argument("--workload", choices=["o3", "ising", "su3", "xybatch", "u1batch", "u1learned", "userxy",
+                                          "usero3", "usero3csr"],
                    default="o3",
-                   help="o3: the headline configuration; ising / su3 / xybatch / userxy: secondary roofline runs "
-                        "(userxy: a user-written FP64 model through include/umc/device.cuh); "
+                   help="o3: the headline configuration; ising / su3 / xybatch / userxy / usero3 / usero3csr: "
+                        "secondary roofline runs (user*: user-written models through include/umc/device.cuh); "
                         "u1learned: the learned-proposal study (effective samples/s)")
     p.add_argument("--no-learned", action="store_true", help="skip the learned-proposal summary of the o3 line")
     return p.parse_args()
@@ -700,7 +701,7 @@ class U1LearnedSweep:
         return None
 
 
-# ------------------------------------------------ a user-written device model
+# ------------------------------------------------ user-written device models
 def _device_models_lib():
     """examples/device_models/libumc_device_models.so (built when stale)."""
     import ctypes as C
@@ -709,19 +710,19 @@ def _device_models_lib():
     import build_device_models
 
     lib = C.CDLL(build_device_models.build())
-    vp, d, u64 = C.c_void_p, C.c_double, C.c_uint64
+    vp, d, u32, u64 = C.c_void_p, C.c_double, C.c_uint32, C.c_uint64
     lib.um_last_error.restype = C.c_char_p
-    lib.um_xy_session_create.argtypes = [vp, d, d, d, u64, C.POINTER(vp)]
-    lib.um_xy_session_destroy.argtypes = [vp]
-    lib.um_xy_session_stream.argtypes = [vp]
-    lib.um_xy_session_stream.restype = vp
-    lib.um_xy_session_set_field.argtypes = [vp, vp]
-    lib.um_xy_session_get_field.argtypes = [vp, vp]
-    lib.um_xy_session_enqueue.argtypes = [vp, u64]
-    lib.um_xy_session_set_timing.argtypes = [vp, C.c_int]
-    lib.um_xy_session_stats.argtypes = [vp, C.POINTER(u64), C.POINTER(d), C.c_int]
-    lib.um_xy_session_energy.argtypes = [vp, C.POINTER(d)]
-    lib.um_xy_session_counters.argtypes = [vp, C.POINTER(u64), C.POINTER(C.c_uint32)]
+    lib.um_session_create.argtypes = [C.c_int, vp, u32, u32, u32, d, d, d, u64, C.POINTER(vp)]
+    lib.um_session_destroy.argtypes = [vp]
+    lib.um_session_stream.argtypes = [vp]
+    lib.um_session_stream.restype = vp
+    lib.um_session_set_field.argtypes = [vp, vp]
+    lib.um_session_get_field.argtypes = [vp, vp]
+    lib.um_session_enqueue.argtypes = [vp, u64]
+    lib.um_session_set_timing.argtypes = [vp, C.c_int]
+    lib.um_session_stats.argtypes = [vp, C.POINTER(u64), C.POINTER(d), C.c_int]
+    lib.um_session_energy.argtypes = [vp, C.POINTER(d)]
+    lib.um_session_counters.argtypes = [vp, C.POINTER(u64), C.POINTER(u32)]
     return lib
 
 
@@ -733,7 +734,7 @@ class _SessionAsChain:
         self.pending = 0
 
     def stream(self):
-        return self.wl.lib.um_xy_session_stream(self.wl.h)
+        return self.wl.lib.um_session_stream(self.wl.h)
 
     def fetch(self, cap):
         import numpy as np
@@ -747,80 +748,89 @@ class _SessionAsChain:
         import ctypes as C
 
         n, ms = C.c_uint64(), C.c_double()
-        self.wl.call(self.wl.lib.um_xy_session_stats(self.wl.h, C.byref(n), C.byref(ms), int(reset)))
+        self.wl.call(self.wl.lib.um_session_stats(self.wl.h, C.byref(n), C.byref(ms), int(reset)))
         return {"metropolis_sweeps": (n.value, ms.value)}
 
     def set_timing(self, on):
-        self.wl.call(self.wl.lib.um_xy_session_set_timing(self.wl.h, int(on)))
+        self.wl.call(self.wl.lib.um_session_set_timing(self.wl.h, int(on)))
 
 
-class UserXY:
-    """A user-written model through include/umc/device.cuh: the XY model on
-    angles as PairModel<Angle, CosineTerm> with the AngleShift (U1Shift)
-    proposal, FP64, from examples/device_models/user_models.cu, on an L x L
-    square_lattice (CSR bond table), J=1, beta=1.1, width 1.0, random start;
-    step = one sweep = one cooperative launch of metropolis_sweeps.  The
-    reference runs the same model as PairModel<U1Dof, user term, PairGraph>
-    through its stock Metropolis driver."""
+class _UserSession:
+    """A session of examples/device_models/user_models.cu: tables, field and
+    the generic device Metropolis of include/umc/device.cuh for one user
+    model; step = one sweep = one cooperative launch of metropolis_sweeps."""
 
-    name = "userxy"
     unit = "site-updates/s"
-    dtype = "f64"
 
-    def __init__(self, umc, args, rank, local):
+    def _open(self, umc, kind, graph, dims, J, beta, width, seed, field):
         import ctypes as C
 
-        import numpy as np
-
-        self.L = args.L if args.L != L_DEFAULT else 8192
-        self.n = self.L * self.L
         self.lib = _device_models_lib()
-        self.g = umc.square_lattice(self.L, self.L)
         h = C.c_void_p()
-        self.call(self.lib.um_xy_session_create(self.g._h, 1.0, 1.1, 1.0, 1 + rank, C.byref(h)))
+        self.call(self.lib.um_session_create(kind, graph, *dims, J, beta, width, seed, C.byref(h)))
         self.h = h
-        self.theta = np.random.default_rng(5 + rank).uniform(-np.pi, np.pi, self.n)
-        self.call(self.lib.um_xy_session_set_field(self.h, self.theta.ctypes.data))
-        self.flush = self.n * 8 < (256 << 20)
+        self.field = field
+        self.call(self.lib.um_session_set_field(self.h, self.field.ctypes.data))
         self.ch = _SessionAsChain(self)
 
     def call(self, rc):
         if rc != 0:
             raise RuntimeError(self.lib.um_last_error().decode())
 
-    def describe(self):
-        return (f"user-written XY PairModel (CosineTerm + AngleShift, FP64, examples/device_models) on "
-                f"{self.L}x{self.L} square_lattice, J=1, beta=1.1, width 1.0, random start; step = 1 Metropolis "
-                f"sweep (one launch of the generic device kernel over the 2 colour classes)")
-
     def enqueue(self, k):
-        self.call(self.lib.um_xy_session_enqueue(self.h, k))
+        self.call(self.lib.um_session_enqueue(self.h, k))
         self.ch.pending += k
 
     def units(self, rec, sizes):
         return len(rec) * self.n
 
-    def bytes_per_launch(self, kind):
-        # per site-update: order 4 + offset 4 + 4 bonds 16 + field read as own
-        # and as a neighbour 16 + write 8 = 48 B
-        return 48.0 * self.n
-
     def e2e(self, torch, K):
         import ctypes as C
 
-        host = torch.from_numpy(self.theta.copy()).pin_memory()
+        host = torch.from_numpy(self.field.copy()).pin_memory()
         e = C.c_double()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(K):
-            self.call(self.lib.um_xy_session_set_field(self.h, host.data_ptr()))
+            self.call(self.lib.um_session_set_field(self.h, host.data_ptr()))
             self.enqueue(1)
-            self.call(self.lib.um_xy_session_energy(self.h, C.byref(e)))
+            self.call(self.lib.um_session_energy(self.h, C.byref(e)))
         torch.cuda.synchronize()
         self.ch.fetch(0)
         blocks = min(1024, (self.n + 255) // 256)
         return {"value": K * self.n / (time.perf_counter() - t0), "unit": self.unit,
-                "h2d_bytes_per_step": self.n * 8, "d2h_bytes_per_step": blocks * 8, "steps": K}
+                "h2d_bytes_per_step": self.field.nbytes, "d2h_bytes_per_step": blocks * 8, "steps": K}
+
+
+class UserXY(_UserSession):
+    """The XY model on angles as PairModel<Angle, CosineTerm> with the
+    AngleShift (U1Shift) proposal, FP64, from examples/device_models, on an
+    L x L square_lattice (CSR bond table), J=1, beta=1.1, width 1.0, random
+    start.  The reference runs the same model as PairModel<U1Dof, user term,
+    PairGraph> through its stock Metropolis driver."""
+
+    name = "userxy"
+    dtype = "f64"
+
+    def __init__(self, umc, args, rank, local):
+        import numpy as np
+
+        self.L = args.L if args.L != L_DEFAULT else 8192
+        self.n = self.L * self.L
+        self.g = umc.square_lattice(self.L, self.L)
+        theta = np.random.default_rng(5 + rank).uniform(-np.pi, np.pi, self.n)
+        self._open(umc, 0, self.g._h, (0, 0, 0), 1.0, 1.1, 1.0, 1 + rank, theta)
+        self.flush = self.n * 8 < (256 << 20)
+
+    def describe(self):
+        return (f"user-written XY PairModel (CosineTerm + AngleShift, FP64, examples/device_models) on "
+                f"{self.L}x{self.L} square_lattice, J=1, beta=1.1, width 1.0, random start; step = 1 Metropolis "
+                f"sweep (one launch of the generic device kernel over the 2 colour classes)")
+
+    def bytes_per_launch(self, kind):
+        # per site-update: order 4 + offset 4 + 4 bonds 16 + field read as own
+        # and as a neighbour 16 + write 8 = 48 B
+        return 48.0 * self.n
 
     def cpu(self, seconds):
         from oracle.oracle import Reference, have_reference
@@ -837,8 +847,50 @@ class UserXY:
                           f"user term> + U1Shift, stock driver), {sec:.1f} s"}
 
 
+class UserO3(_UserSession):
+    """A user-written FP32 Heisenberg pair term (DotTerm<float, 3> with an
+    FP32 UniformSphereN<3>) on an L^3 periodic cubic lattice, J=1, beta=0.693,
+    random unit start.  usero3: the table-free RegularLattice (neighbours
+    computed, nothing about bonds read); usero3csr: the same model on the
+    lattice's CSR tables (PairTables)."""
+
+    dtype = "f32"
+
+    def __init__(self, umc, args, rank, local, tables=False):
+        import numpy as np
+
+        self.tables = tables
+        self.name = "usero3csr" if tables else "usero3"
+        self.L = args.L if args.L != L_DEFAULT else 256
+        self.n = self.L ** 3
+        v = np.random.default_rng(9 + rank).normal(size=(self.n, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        self._open(umc, 2 if tables else 1, None, (self.L, self.L, self.L), 1.0, 0.693, 0.0, 1 + rank,
+                   np.ascontiguousarray(v, np.float32).reshape(-1))
+        self.flush = self.n * 12 < (256 << 20)
+
+    def describe(self):
+        where = "PairTables (the lattice's CSR)" if self.tables else "RegularLattice (no bond tables)"
+        return (f"user-written FP32 Heisenberg PairModel (DotTerm<float,3> + FP32 UniformSphereN<3>, "
+                f"examples/device_models) on {self.L}^3 periodic cubic, {where}, J=1, beta=0.693, random start; "
+                f"step = 1 Metropolis sweep (one launch of the generic device kernel)")
+
+    def bytes_per_launch(self, kind):
+        # 36 B per site-update (own 12 read, 12 as a neighbour, 12 write); the
+        # tables add offset 4 + six bonds 24
+        return (64.0 if self.tables else 36.0) * self.n
+
+    def cpu(self, seconds):
+        return None
+
+
+class UserO3Csr(UserO3):
+    def __init__(self, umc, args, rank, local):
+        super().__init__(umc, args, rank, local, tables=True)
+
+
 WORKLOADS = {"o3": O3Hybrid, "ising": IsingSweep, "su3": SU3Sweep, "xybatch": XYBatch, "u1batch": U1LearnedSweep,
-             "userxy": UserXY}
+             "userxy": UserXY, "usero3": UserO3, "usero3csr": UserO3Csr}
 
 
 def run_learned(args):

@@ -18,8 +18,8 @@
 //
 // Exported with a C ABI for the Python tests and bench.py (ctypes): one-shot
 // runs (um_xy_pair, um_u1_cells, um_heisenberg_cubic, um_o3_wolff,
-// um_ising_wolff, um_lattice_o3) and a persistent XY
-// session (um_xy_session_*) whose launches bench.py times.
+// um_ising_wolff, um_lattice_o3) and persistent sessions (um_session_*) whose
+// launches bench.py times.
 #include <umc/device.cuh>
 
 #include <cmath>
@@ -365,9 +365,61 @@ int um_lattice_o3(std::uint32_t Lx, std::uint32_t Ly, std::uint32_t Lz, double J
 
 }  // extern "C"
 
-// ---- persistent XY session: tables, field and driver stay on the device
+// ---- persistent sessions: tables, field and driver stay on the device; the
+// launches bench.py times.  Kinds:
+//   0  XY (CosineTerm + AngleShift, FP64) on a library pair graph's tables;
+//   1  O(3) (DotTerm<3, float> + SphereF, FP32) on a table-free RegularLattice;
+//   2  the same O(3) model on the lattice's CSR tables (PairTables).
 namespace {
-struct XYSession
+
+template <class T, std::size_t N>
+struct VecT
+{
+    using dtype = T;
+    static constexpr std::size_t size = N;
+};
+
+// E = -J s_i . s_j in the spins' own precision.
+template <class T, std::size_t N>
+struct DotTermT
+{
+    using dtype = T;
+    using energy_type = T;
+    static constexpr std::size_t arity = 2;
+    T J;
+
+    UMC_HD static T dot(const T* a, const T* b)
+    {
+        T s = 0;
+        for (std::size_t k = 0; k < N; ++k) s += a[k] * b[k];
+        return s;
+    }
+    UMC_HD T energy(const T* const* l) const { return -J * dot(l[0], l[1]); }
+    UMC_HD T delta(std::size_t which, const T* old, const T* nw, const T* const* l) const
+    {
+        const T* fixed = l[which == 0 ? 1 : 0];
+        return -J * (dot(nw, fixed) - dot(old, fixed));
+    }
+};
+
+// UniformSphereN<3> in FP32: height z = 2u - 1, angle 2 pi u.
+struct SphereF
+{
+    template <class R>
+    UMC_HD void sample(const float*, R& rng, float* out) const
+    {
+        const float z = float(2.0 * rng.uni() - 1.0);
+        const float r = sqrtf(fmaxf(0.f, 1.f - z * z));
+        float sn, cs;
+        sincospif(float(2.0 * rng.uni()), &sn, &cs);
+        out[0] = cs * r;
+        out[1] = sn * r;
+        out[2] = z;
+    }
+    UMC_HD float log_ratio(const float*, const float*) const { return 0.f; }
+};
+
+struct SessionBase
 {
     static cudaStream_t make_stream()
     {
@@ -375,11 +427,8 @@ struct XYSession
         cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
         return s;
     }
-    XYSession(const umc_graph* g, double J, double beta, double width, std::uint64_t seed)
-        : tables(g), field(tables.sites()), stream(make_stream()),
-          mc(tables.model<Angle>(field.data(), CosineTerm{J}), AngleShift{width}, tables.classes(), seed, beta, stream)
-    {}
-    ~XYSession()
+    SessionBase() : stream(make_stream()) {}
+    virtual ~SessionBase()
     {
         for (auto& e : pending) {
             cudaEventDestroy(e.first);
@@ -387,6 +436,14 @@ struct XYSession
         }
         cudaStreamDestroy(stream);
     }
+    virtual void set_field(const void* host) = 0;
+    virtual void get_field(void* host) = 0;
+    virtual void launch(std::uint64_t sweeps) = 0;
+    virtual void check() = 0;
+    virtual double energy() = 0;
+    virtual std::uint64_t sweeps() const = 0;
+    virtual std::uint32_t grid() const = 0;
+
     void fold()
     {
         cuda_check(cudaStreamSynchronize(stream), "sync");
@@ -400,57 +457,102 @@ struct XYSession
         pending.clear();
     }
 
-    PairTables tables;
-    Buffer<double> field;
     cudaStream_t stream;
-    Metropolis<PairModel<Angle, CosineTerm>, AngleShift> mc;
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
     std::uint64_t launches = 0;
     double timed_ms = 0.0;
 };
+
+// Tables + field + Metropolis; `scalars` field values per site.
+template <class Tables, class D, class Term, class Q>
+struct Session final : SessionBase
+{
+    using T = typename D::dtype;
+    template <class Src>
+    Session(const Src& src, Term term, Q q, double beta, std::uint64_t seed)
+        : tables(src), field(std::size_t(tables.sites()) * D::size),
+          mc(tables.template model<D>(field.data(), term), q, tables.classes(), seed, beta, stream)
+    {}
+    void set_field(const void* host) override { tables.upload(field, static_cast<const T*>(host), D::size, stream); }
+    void get_field(void* host) override { tables.download(field, static_cast<T*>(host), D::size, stream); }
+    void launch(std::uint64_t sweeps) override { mc.enqueue(sweeps); }
+    void check() override { mc.check(); }
+    double energy() override { return 0.5 * mc.energy_at_sum(); }
+    std::uint64_t sweeps() const override { return mc.sweeps(); }
+    std::uint32_t grid() const override { return mc.grid(); }
+
+    Tables tables;
+    Buffer<T> field;
+    Metropolis<decltype(std::declval<Tables&>().template model<D>(nullptr, std::declval<Term>())), Q> mc;
+};
+
+using XYSession = Session<PairTables, Angle, CosineTerm, AngleShift>;
+using O3LatticeSession = Session<LatticeTables, VecT<float, 3>, DotTermT<float, 3>, SphereF>;
+using O3TableSession = Session<PairTables, VecT<float, 3>, DotTermT<float, 3>, SphereF>;
+
+// The lattice's own CSR as a library graph, for the table variant.
+struct LatticeGraph
+{
+    umc_graph* g = nullptr;
+    LatticeGraph(std::uint32_t Lx, std::uint32_t Ly, std::uint32_t Lz)
+    {
+        umc_check(Lz > 1 ? umc_graph_cubic(Lx, Ly, Lz, &g) : umc_graph_square(Lx, Ly, &g));
+    }
+    ~LatticeGraph() { umc_graph_destroy(g); }
+};
+
 }  // namespace
 
 extern "C" {
 
-int um_xy_session_create(const umc_graph* g, double J, double beta, double width, std::uint64_t seed, void** out)
+// kind 0: graph, J, beta, width (dims unused); kinds 1, 2: dims Lx, Ly, Lz, J, beta.
+int um_session_create(int kind, const umc_graph* g, std::uint32_t Lx, std::uint32_t Ly, std::uint32_t Lz, double J,
+                      double beta, double width, std::uint64_t seed, void** out)
 {
-    return guarded([&] { *out = new XYSession(g, J, beta, width, seed); });
+    return guarded([&] {
+        if (kind == 0) {
+            *out = static_cast<SessionBase*>(new XYSession(g, CosineTerm{J}, AngleShift{width}, beta, seed));
+        } else if (kind == 1) {
+            *out = static_cast<SessionBase*>(
+                new O3LatticeSession(RegularLattice{Lx, Ly, Lz}, DotTermT<float, 3>{float(J)}, SphereF{}, beta, seed));
+        } else if (kind == 2) {
+            LatticeGraph lg(Lx, Ly, Lz);
+            *out = static_cast<SessionBase*>(
+                new O3TableSession(lg.g, DotTermT<float, 3>{float(J)}, SphereF{}, beta, seed));
+        } else {
+            throw std::invalid_argument("unknown session kind");
+        }
+    });
 }
 
-void um_xy_session_destroy(void* h) { delete static_cast<XYSession*>(h); }
+void um_session_destroy(void* h) { delete static_cast<SessionBase*>(h); }
 
-void* um_xy_session_stream(void* h) { return static_cast<XYSession*>(h)->stream; }
+void* um_session_stream(void* h) { return static_cast<SessionBase*>(h)->stream; }
 
-// Field from/to host memory (sites doubles, site order), ordered on the
+// Field from/to host memory (site order, the model's dtype), ordered on the
 // session's stream; set_field returns before the copy completes.
-int um_xy_session_set_field(void* h, const double* theta)
+int um_session_set_field(void* h, const void* host)
 {
-    return guarded([&] {
-        auto* s = static_cast<XYSession*>(h);
-        s->tables.upload(s->field, theta, 1, s->stream);
-    });
+    return guarded([&] { static_cast<SessionBase*>(h)->set_field(host); });
 }
-int um_xy_session_get_field(void* h, double* theta)
+int um_session_get_field(void* h, void* host)
 {
-    return guarded([&] {
-        auto* s = static_cast<XYSession*>(h);
-        s->tables.download(s->field, theta, 1, s->stream);
-    });
+    return guarded([&] { static_cast<SessionBase*>(h)->get_field(host); });
 }
 
 // n sweeps in one launch, not waited for; with timing on, CUDA events bracket it.
-int um_xy_session_enqueue(void* h, std::uint64_t sweeps)
+int um_session_enqueue(void* h, std::uint64_t sweeps)
 {
     return guarded([&] {
-        auto* s = static_cast<XYSession*>(h);
+        auto* s = static_cast<SessionBase*>(h);
         cudaEvent_t a = nullptr, b = nullptr;
         if (s->timing) {
             cuda_check(cudaEventCreate(&a), "event");
             cuda_check(cudaEventCreate(&b), "event");
             cuda_check(cudaEventRecord(a, s->stream), "event");
         }
-        s->mc.enqueue(sweeps);
+        s->launch(sweeps);
         s->launches += (sweeps + (1u << 30) - 1) >> 30;
         if (s->timing) {
             cuda_check(cudaEventRecord(b, s->stream), "event");
@@ -459,10 +561,10 @@ int um_xy_session_enqueue(void* h, std::uint64_t sweeps)
     });
 }
 
-int um_xy_session_set_timing(void* h, int on)
+int um_session_set_timing(void* h, int on)
 {
     return guarded([&] {
-        auto* s = static_cast<XYSession*>(h);
+        auto* s = static_cast<SessionBase*>(h);
         s->fold();
         s->timing = on != 0;
     });
@@ -470,12 +572,12 @@ int um_xy_session_set_timing(void* h, int on)
 
 // Waits for the stream; launches of metropolis_sweeps and their event time
 // (timed launches only) since the last reset; throws if a barrier wait ran out.
-int um_xy_session_stats(void* h, std::uint64_t* launches, double* ms, int reset)
+int um_session_stats(void* h, std::uint64_t* launches, double* ms, int reset)
 {
     return guarded([&] {
-        auto* s = static_cast<XYSession*>(h);
+        auto* s = static_cast<SessionBase*>(h);
         s->fold();
-        s->mc.check();
+        s->check();
         *launches = s->launches;
         *ms = s->timed_ms;
         if (reset) {
@@ -486,17 +588,17 @@ int um_xy_session_stats(void* h, std::uint64_t* launches, double* ms, int reset)
 }
 
 // Total energy (sum of energy_at / 2, FP64) of the current field.
-int um_xy_session_energy(void* h, double* e)
+int um_session_energy(void* h, double* e)
 {
-    return guarded([&] { *e = 0.5 * static_cast<XYSession*>(h)->mc.energy_at_sum(); });
+    return guarded([&] { *e = static_cast<SessionBase*>(h)->energy(); });
 }
 
-int um_xy_session_counters(void* h, std::uint64_t* sweeps, std::uint32_t* grid)
+int um_session_counters(void* h, std::uint64_t* sweeps, std::uint32_t* grid)
 {
     return guarded([&] {
-        auto* s = static_cast<XYSession*>(h);
-        *sweeps = s->mc.sweeps();
-        *grid = s->mc.grid();
+        auto* s = static_cast<SessionBase*>(h);
+        *sweeps = s->sweeps();
+        *grid = s->grid();
     });
 }
 

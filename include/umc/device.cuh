@@ -653,15 +653,48 @@ private:
 
 // ------------------------------------------------------------------ tables without storage
 
+// n / d for 32-bit n and a fixed d >= 1 without a divide: the high 64 bits of
+// n * ceil(2^64 / d).  The rounding error is below 2^-32 <= 1/d, so the
+// quotient is exact for every 32-bit n.
+struct FastDiv
+{
+    std::uint32_t d = 1;
+    std::uint64_t m = 0;
+
+    FastDiv() = default;
+    explicit FastDiv(std::uint32_t divisor) : d(divisor)
+    {
+        if (d == 0) throw std::invalid_argument("FastDiv: divisor 0");
+        // ceil(2^64 / d) = floor((2^64 - 1) / d) + 1 for every d >= 2
+        m = d == 1 ? 0 : ~std::uint64_t(0) / d + 1;
+    }
+    UMC_HD std::uint32_t div(std::uint32_t n) const
+    {
+        if (d == 1) return n;
+#if defined(__CUDA_ARCH__)
+        return std::uint32_t(__umul64hi(std::uint64_t(n), m));
+#else
+        return std::uint32_t((unsigned __int128)n * m >> 64);
+#endif
+    }
+};
+
 // A periodic Lx x Ly x Lz lattice whose bonds are computed, not stored
 // (square_lattice's and cubic_lattice's sites and bonds; Lz = 1 in 2D).
 // Lx is even and Ly, Lz are even or 1, so the checkerboard is a proper
-// 2-colouring and sites 2r, 2r + 1 share a row;
-// device site k is the colour-major position ((x+y+z)&1) n/2 + s/2 of
-// reference site s = (z Ly + y) Lx + x.  Bonds of k, in the order +x, -x,
-// +y, -y, +z, -z over the extents above 1, are the neighbours' device sites.
-struct RegularLattice
+// 2-colouring and sites 2r, 2r + 1 share a row; device site k is the
+// colour-major position ((x+y+z)&1) n/2 + s/2 of reference site
+// s = (z Ly + y) Lx + x.  The bonds of k, in the order +x, -x, +y, -y, +z, -z
+// over the extents above 1, are the neighbours' device sites.
+class RegularLattice
 {
+public:
+    static constexpr std::uint32_t kMaxDegree = 6;
+
+    RegularLattice(std::uint32_t lx, std::uint32_t ly, std::uint32_t lz)
+        : Lx(lx), Ly(ly), Lz(lz), div_x(lx ? lx : 1), div_y(ly ? ly : 1)
+    {}
+
     std::uint32_t Lx, Ly, Lz;
 
     UMC_HD std::uint32_t sites() const { return Lx * Ly * Lz; }
@@ -677,22 +710,49 @@ struct RegularLattice
         const std::uint32_t half = sites() / 2;
         const std::uint32_t c = k >= half ? 1u : 0u;
         const std::uint32_t s0 = 2u * (k - c * half);  // the even site of the pair; same row as s0 + 1
-        y = (s0 / Lx) % Ly;
-        z = s0 / (Lx * Ly);
-        x = s0 % Lx + ((c + y + z + s0 % Lx) & 1u);
+        const std::uint32_t row = div_x.div(s0);
+        z = div_y.div(row);
+        y = row - z * Ly;
+        const std::uint32_t x0 = s0 - row * Lx;
+        x = x0 + ((c + y + z) & 1u);
+    }
+    // All degree() neighbours of device site k, in bond order.  Site k is
+    // s = 2r + b (rank r in its colour c); every neighbour has the other
+    // colour, and s +- 1, s +- Lx, s +- Lx Ly have ranks r + b or r + b - 1,
+    // r +- Lx/2, r +- Lx Ly/2 (Lx even), shifted by one period at a wrap.
+    // Unsigned wrap-around in the intermediate sums is harmless: every result
+    // is a valid rank.
+    UMC_HD void neighbours(std::uint32_t k, std::uint32_t* nb) const
+    {
+        const std::uint32_t half = sites() / 2, hx = Lx / 2, ha = Lx * Ly / 2;
+        const std::uint32_t c = k >= half ? 1u : 0u;
+        const std::uint32_t r = k - c * half;
+        const std::uint32_t row = div_x.div(2u * r);
+        const std::uint32_t z = div_y.div(row), y = row - z * Ly;
+        const std::uint32_t b = (c + y + z) & 1u;
+        const std::uint32_t x = 2u * r - row * Lx + b;
+        const std::uint32_t o = (1u - c) * half;
+        std::uint32_t a = 0;
+        nb[a++] = o + (x + 1 == Lx ? r + 1 - hx : r + b);
+        nb[a++] = o + (x == 0 ? r + hx - 1 : r + b - 1);
+        if (Ly > 1) {
+            nb[a++] = o + (y + 1 == Ly ? r + hx - ha : r + hx);
+            nb[a++] = o + (y == 0 ? r - hx + ha : r - hx);
+        }
+        if (Lz > 1) {
+            nb[a++] = o + (z + 1 == Lz ? r + ha - half : r + ha);
+            nb[a++] = o + (z == 0 ? r - ha + half : r - ha);
+        }
     }
     UMC_HD std::uint32_t neighbour(std::uint32_t k, std::uint32_t a) const
     {
-        std::uint32_t x, y, z;
-        coords(k, x, y, z);
-        std::uint32_t d = a >> 1;
-        const bool minus = a & 1u;
-        if (d >= 1 && Ly == 1) ++d;
-        if (d == 0) x = minus ? (x + Lx - 1) % Lx : (x + 1) % Lx;
-        else if (d == 1) y = minus ? (y + Ly - 1) % Ly : (y + 1) % Ly;
-        else z = minus ? (z + Lz - 1) % Lz : (z + 1) % Lz;
-        return index_of(x, y, z);
+        std::uint32_t nb[kMaxDegree];
+        neighbours(k, nb);
+        return nb[a];
     }
+
+private:
+    FastDiv div_x, div_y;
 };
 
 namespace detail {
@@ -749,10 +809,12 @@ struct LatticePairModel
     // model/pair.hpp:38-49
     UMC_HD energy_type energy_at(std::size_t i) const
     {
+        std::uint32_t nb[RegularLattice::kMaxDegree];
+        lattice.neighbours(std::uint32_t(i), nb);
         energy_type e = 0;
         const dtype* si = field + i * size;
         for (std::uint32_t a = 0; a < lattice.degree(); ++a) {
-            const dtype* links[2] = {si, field + std::size_t(lattice.neighbour(std::uint32_t(i), a)) * size};
+            const dtype* links[2] = {si, field + std::size_t(nb[a]) * size};
             e += term.energy(links);
         }
         return e;
@@ -760,10 +822,12 @@ struct LatticePairModel
     // model/pair.hpp:52-63
     UMC_HD energy_type energy_diff_at(std::size_t i, const dtype* p) const
     {
+        std::uint32_t nb[RegularLattice::kMaxDegree];
+        lattice.neighbours(std::uint32_t(i), nb);
         energy_type d = 0;
         const dtype* si = field + i * size;
         for (std::uint32_t a = 0; a < lattice.degree(); ++a) {
-            const dtype* links[2] = {si, field + std::size_t(lattice.neighbour(std::uint32_t(i), a)) * size};
+            const dtype* links[2] = {si, field + std::size_t(nb[a]) * size};
             d += term.delta(0, si, p, links);
         }
         return d;
@@ -862,6 +926,21 @@ __device__ __forceinline__ bool grid_sync(Control* ctl)
     return __syncthreads_or(fail) == 0;
 }
 
+// log(u) < log_p, decided as the FP64 test decides it.  logf(float(u)) is
+// within 2^-24 + 2^-23 |log u| of log(u): rounding u to float moves log u by
+// at most 2^-24, and logf is accurate to 1 ulp.  The FP32 answer is taken
+// when it clears log_p by 2^-21 (1 + |logf|), at least four times that error;
+// otherwise the FP64 log decides.
+__device__ __forceinline__ bool log_below(double u, double log_p)
+{
+    const float lf = logf(float(u));
+    const double gap = double(lf) - log_p;
+    const double bound = 0x1.0p-21 * (1.0 + fabs(double(lf)));
+    if (gap > bound) return false;
+    if (gap < -bound) return true;
+    return log(u) < log_p;
+}
+
 // n_sweeps Metropolis sweeps (driver.hpp:29-43) over the colour classes.
 template <class M, class Q>
 __global__ void __launch_bounds__(kThreads) metropolis_sweeps(M m, Q q, const std::uint32_t* __restrict__ order,
@@ -885,7 +964,7 @@ __global__ void __launch_bounds__(kThreads) metropolis_sweeps(M m, Q q, const st
                 q.sample(cur, rng, cand);
                 const double dE = m.energy_diff_at(i, cand);
                 const double log_p = -beta * dE + q.log_ratio(cur, cand);
-                if (log_p >= 0.0 || log(rng.uni()) < log_p) m.update(i, cand);
+                if (log_p >= 0.0 || log_below(rng.uni(), log_p)) m.update(i, cand);
             }
             if ((s + 1 < n_sweeps || c + 1 < n_classes) && !grid_sync(ctl)) return;
         }

@@ -321,3 +321,45 @@ def test_user_term_on_table_free_lattice(umc, oracle, lib, dims):
     if margin.min() >= MARGIN:
         np.testing.assert_array_equal(sz, sz_o)
         assert np.abs(s2 - v_o[pos]).max() < TOL
+
+
+@pytest.mark.gpu
+def test_fp32_user_term_same_on_lattice_and_tables(umc, lib):
+    """The FP32 O(3) user model of the bench runs the same chain on the
+    table-free RegularLattice and on PairTables (same numbering and keys;
+    only the neighbours' summation order differs), and its energy is finite
+    and below the random start's."""
+    vp = C.c_void_p
+    lib.um_session_create.argtypes = [C.c_int, vp, _u32, _u32, _u32, _d, _d, _d, _u64, C.POINTER(vp)]
+    lib.um_session_destroy.argtypes = [vp]
+    lib.um_session_set_field.argtypes = [vp, vp]
+    lib.um_session_get_field.argtypes = [vp, vp]
+    lib.um_session_enqueue.argtypes = [vp, _u64]
+    lib.um_session_stats.argtypes = [vp, C.POINTER(_u64), C.POINTER(_d), C.c_int]
+    lib.um_session_energy.argtypes = [vp, C.POINTER(_d)]
+    L, n = 16, 16 ** 3
+    v0 = np.ascontiguousarray(random_unit_vectors(n, 3, 4), np.float32).reshape(-1)
+    out, energies = [], []
+    for kind in (1, 2):
+        h = vp()
+        _call(lib, lib.um_session_create(kind, None, L, L, L, 1.0, 0.693, 0.0, 3, C.byref(h)))
+        try:
+            _call(lib, lib.um_session_set_field(h, v0.ctypes.data))
+            e0 = _d()
+            _call(lib, lib.um_session_energy(h, C.byref(e0)))
+            _call(lib, lib.um_session_enqueue(h, 5))
+            cnt, ms = _u64(), _d()
+            _call(lib, lib.um_session_stats(h, C.byref(cnt), C.byref(ms), 1))
+            f = np.empty_like(v0)
+            _call(lib, lib.um_session_get_field(h, f.ctypes.data))
+            e = _d()
+            _call(lib, lib.um_session_energy(h, C.byref(e)))
+        finally:
+            lib.um_session_destroy(h)
+        out.append(f.reshape(n, 3))
+        energies.append((e0.value, e.value))
+    d = np.abs(out[0] - out[1]).max(axis=1)
+    assert (d > 1e-4).sum() <= 20, (d > 1e-4).sum()
+    for e0, e in energies:
+        assert np.isfinite(e) and e < e0
+    assert abs(np.linalg.norm(out[0], axis=1) - 1).max() < 1e-5
