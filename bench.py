@@ -881,7 +881,18 @@ class UserO3(_UserSession):
         return (64.0 if self.tables else 36.0) * self.n
 
     def cpu(self, seconds):
-        return None
+        from oracle.oracle import Reference, have_reference
+
+        if not have_reference():
+            return None
+        r = Reference()
+        threads = cpu_threads()
+        su, sec = r.bench_pair_o3(32, 0.693, 1, 3, 1, 1)
+        sweeps = max(3, int(seconds * 3 / max(sec, 1e-4)))
+        su, sec = r.bench_pair_o3(32, 0.693, 1, sweeps, threads, 1)
+        return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                "sample": f"{sweeps} sweeps x {threads} independent 32^3 chains (reference PairModel<VectorDof<3>, "
+                          f"HeisenbergTerm<3>> + UniformSphereN<3>, stock driver, FP64), {sec:.1f} s"}
 
 
 class UserO3Csr(UserO3):

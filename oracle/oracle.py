@@ -430,6 +430,7 @@ class Reference:
         self._stock_su3 = L.fn("stock_su3_chain", _int, _u64, _f64, _f64, _u64, _u32, _u64, _u64, _vp)
         self._bench_ising = L.fn("bench_ising", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._bench_xy = L.fn("bench_xy", _int, _u64, _f64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
+        self._bench_pair_o3 = L.fn("bench_pair_o3", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
 
     def pcg32_draws(self, seed, stream, n):
         out = np.zeros(n, np.uint32)
@@ -625,6 +626,19 @@ def _bench_xy(self, L, beta, width, warmup, sweeps, threads, seed=1):
 
 
 Reference.bench_xy = _bench_xy
+
+
+def _bench_pair_o3(self, L, beta, warmup, sweeps, threads, seed=1):
+    """Reference PairModel<VectorDof<3>, HeisenbergTerm<3>> Metropolis on L^3:
+    (site-updates, seconds of the slowest thread)."""
+    su = C.c_double()
+    sec = C.c_double()
+    st = self._bench_pair_o3(L, beta, warmup, sweeps, threads, seed, C.byref(su), C.byref(sec))
+    assert st == 0, st
+    return su.value, sec.value
+
+
+Reference.bench_pair_o3 = _bench_pair_o3
 
 
 def have_reference() -> bool:

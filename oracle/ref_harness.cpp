@@ -49,6 +49,7 @@
 #include <model/cell.hpp>
 #include <model/pair.hpp>
 #include <rng.hpp>
+#include <term/heisenberg.hpp>
 #include <term/plaquette.hpp>
 #include <term/sun_plaquette.hpp>
 
@@ -968,6 +969,55 @@ extern "C" int ref_bench_xy(std::uint64_t L, double beta, double width, std::uin
         double worst = 0.0;
         for (double x : secs) worst = x > worst ? x : worst;
         *site_updates = double(threads) * double(L * L) * double(sweeps);
+        *seconds = worst;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+// Times the reference's generic table-driven O(3) model: PairModel<VectorDof<3>,
+// HeisenbergTerm<3>, PairGraph<>> (model/pair.hpp, term/heisenberg.hpp) on the
+// periodic L^3 cubic edge list, Metropolis with UniformSphereN<3> and a plain
+// Pcg32, one chain per thread, uniform random start.
+extern "C" int ref_bench_pair_o3(std::uint64_t L, double beta, std::uint64_t warmup, std::uint64_t sweeps,
+                                 std::uint32_t threads, std::uint64_t seed, double* site_updates, double* seconds)
+{
+    try {
+        using PM = PairModel<VectorDof<3>, HeisenbergTerm<3>, PairGraph<>>;
+        std::vector<PairGraph<>::Edge> edges;
+        edges.reserve(3 * L * L * L);
+        for (std::uint64_t z = 0; z < L; ++z)
+            for (std::uint64_t y = 0; y < L; ++y)
+                for (std::uint64_t x = 0; x < L; ++x) {
+                    const auto i = static_cast<std::uint32_t>((z * L + y) * L + x);
+                    edges.push_back({i, static_cast<std::uint32_t>((z * L + y) * L + (x + 1) % L), {}});
+                    edges.push_back({i, static_cast<std::uint32_t>((z * L + (y + 1) % L) * L + x), {}});
+                    edges.push_back({i, static_cast<std::uint32_t>((((z + 1) % L) * L + y) * L + x), {}});
+                }
+        const std::size_t n = L * L * L;
+        std::vector<double> secs(threads, 0.0);
+        std::vector<std::thread> pool;
+        for (std::uint32_t t = 0; t < threads; ++t)
+            pool.emplace_back([&, t] {
+                PM model(PairGraph<>(n, edges), HeisenbergTerm<3>{1.0});
+                Pcg32 init(seed + t, 7);
+                double v[3];
+                for (std::size_t i = 0; i < n; ++i) {
+                    UniformSphereN<3>{}.sample(nullptr, init, v);
+                    model.update(i, v);
+                }
+                Metropolis<PM, UniformSphereN<3>, Pcg32> mc(model, UniformSphereN<3>{}, Pcg32(seed + t, 1), beta);
+                mc.run(warmup);
+                const auto t0 = std::chrono::steady_clock::now();
+                mc.run(sweeps);
+                const auto t1 = std::chrono::steady_clock::now();
+                secs[t] = std::chrono::duration<double>(t1 - t0).count();
+            });
+        for (auto& th : pool) th.join();
+        double worst = 0.0;
+        for (double x : secs) worst = x > worst ? x : worst;
+        *site_updates = double(threads) * double(n) * double(sweeps);
         *seconds = worst;
         return 0;
     } catch (...) {
