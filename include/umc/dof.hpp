@@ -14,6 +14,7 @@
 #include <concepts>
 #include <cstddef>
 #include <cstdint>
+#include <limits>
 #include <numbers>
 
 #include "detail.hpp"
@@ -105,12 +106,51 @@ private:
     }
 };
 
-// Rotation by an angle in [-delta, delta] in a random 2-plane (device only).
+// Rotation by an angle in [-delta, delta] in a uniform random oriented
+// 2-plane (dof/vector.hpp:62-122): u on the sphere, a second sphere point made
+// orthogonal to u and normalised (redrawn while |v - (v.u) u|^2 <= 64 eps),
+// then the rotation of cur in the (u, v) plane.  The engine's chains run it in
+// their own kernels; sample() serves user-written terms (nvcc builds) and
+// host code.  The redraw is capped at 64 tries, a limit that a draw reaches
+// with probability below 1e-800.
 template <std::size_t N, class T = double>
 struct LocalRotation
 {
+    static_assert(N >= 2, "LocalRotation needs at least two components");
     T delta = T(0.5);
-    double log_ratio(const T*, const T*) const noexcept { return 0.0; }
+
+    template <class R>
+    UMC_FACADE_HD void sample(const T* cur, R& rng, T* out) const
+    {
+        T u[N] = {}, v[N] = {};
+        UniformSphereN<N, T>{}.sample(nullptr, rng, u);
+        const T eps = T(64) * std::numeric_limits<T>::epsilon();
+        for (int tries = 0; tries < 64; ++tries) {
+            UniformSphereN<N, T>{}.sample(nullptr, rng, v);
+            T proj = 0;
+            for (std::size_t k = 0; k < N; ++k) proj += v[k] * u[k];
+            T r2 = 0;
+            for (std::size_t k = 0; k < N; ++k) {
+                v[k] -= proj * u[k];
+                r2 += v[k] * v[k];
+            }
+            if (r2 > eps) {
+                const T inv = T(1) / std::sqrt(r2);
+                for (std::size_t k = 0; k < N; ++k) v[k] *= inv;
+                break;
+            }
+        }
+        const T th = delta * (T(2) * static_cast<T>(rng.uni()) - T(1));
+        const T c = std::cos(th);
+        const T s = std::sin(th);
+        T cu = 0, cv = 0;
+        for (std::size_t k = 0; k < N; ++k) {
+            cu += u[k] * cur[k];
+            cv += v[k] * cur[k];
+        }
+        for (std::size_t k = 0; k < N; ++k) out[k] = cur[k] + (c - T(1)) * (cu * u[k] + cv * v[k]) + s * (cu * v[k] - cv * u[k]);
+    }
+    UMC_FACADE_HD double log_ratio(const T*, const T*) const noexcept { return 0.0; }
 };
 
 // ---- U(1) --------------------------------------------------------------------

@@ -6,7 +6,8 @@
 // reference's proposals and axes, Pcg32 for the keys, data() to read back.
 //
 // Writes to argv[1], in order: the XY start and end angles, the Ising start
-// and end spins and the 12 cluster sizes, the U(1) start and end angles.
+// and end spins and the 12 cluster sizes, the U(1) start and end angles, the
+// O(3) start and end spins.
 #include <umc/umc.hpp>
 
 #include <cmath>
@@ -73,7 +74,29 @@ struct MyPlaquetteTerm
     }
 };
 
-static_assert(CellTerm<XYAngleTerm, U1Dof> && CellTerm<MyIsingTerm, IsingDof> && CellTerm<MyPlaquetteTerm, U1Dof>);
+// E = -J s_i . s_j on VectorDof<3>, as a user would write HeisenbergTerm.
+struct MyHeisenbergTerm
+{
+    using dtype = double;
+    using energy_type = double;
+    static constexpr std::size_t arity = 2;
+    double J = 1.0;
+
+    __host__ __device__ static double dot3(const double* a, const double* b)
+    {
+        return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+    }
+    __host__ __device__ energy_type energy(const dtype* const* l) const { return -J * dot3(l[0], l[1]); }
+    __host__ __device__ energy_type delta(std::size_t which, const dtype* old, const dtype* nw,
+                                          const dtype* const* l) const
+    {
+        const dtype* fixed = l[which == 0 ? 1 : 0];
+        return -J * (dot3(nw, fixed) - dot3(old, fixed));
+    }
+};
+
+static_assert(CellTerm<XYAngleTerm, U1Dof> && CellTerm<MyIsingTerm, IsingDof> && CellTerm<MyPlaquetteTerm, U1Dof> &&
+              CellTerm<MyHeisenbergTerm, VectorDof<3>>);
 
 template <class T>
 static void put(std::FILE* f, const T* p, std::size_t n)
@@ -149,6 +172,22 @@ int main(int argc, char** argv)
         std::printf("U(1) user cell term: S = %.6f\n", u1.total_energy());
         put(out, u0.data(), u0.size());
         put(out, u1a.data(), u1a.size());
+
+        // O(3): PairModel<VectorDof<3>, user term, PairGraph<>> on 8^3 with LocalRotation, 2 sweeps
+        PairModel<VectorDof<3>, MyHeisenbergTerm, PairGraph<>> o3(cubic_lattice(8, 8, 8), MyHeisenbergTerm{1.0});
+        for (std::size_t i = 0; i < o3.sites(); ++i) {
+            double v[3];
+            UniformSphereN<3>{}.sample(nullptr, init, v);
+            o3.update(i, v);
+        }
+        const std::vector<double> v0(o3.data(), o3.data() + 3 * o3.sites());
+        {
+            Metropolis metro(o3, LocalRotation<3>{0.6}, Pcg32(21, 0), 0.693);
+            metro.run(2);
+        }
+        const std::vector<double> v1(o3.data(), o3.data() + 3 * o3.sites());
+        put(out, v0.data(), v0.size());
+        put(out, v1.data(), v1.size());
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());
         std::fclose(out);

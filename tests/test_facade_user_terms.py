@@ -4,7 +4,8 @@ device through umc/device_facade.cuh.  The program compiles here; without a
 GPU it fails loudly; on the GPU its fields equal the oracle's:
 - XY angles, 5 sweeps, to 1e-9;
 - Ising under Wolff, spins and cluster sizes bit for bit;
-- U(1) plaquettes, 2 sweeps, to 1e-9.
+- U(1) plaquettes, 2 sweeps, to 1e-9;
+- O(3) with LocalRotation, 2 sweeps, to 1e-9.
 The oracle runs on the colour-major device numbering with the same keys."""
 import os
 import shutil
@@ -87,9 +88,20 @@ def test_user_term_program_matches_the_oracle(program, umc, oracle, tmp_path):
     rcells = pos[cc.table()]
     inc = oracle.cell_incidence(n, rcells)[1:]
     u0, u1 = take(np.float64, n), take(np.float64, n)
-    assert at == len(raw)
     cm = np.empty(n)
     cm[pos] = u0
     t_o, _, _ = oracle.u1_metropolis(rcells, inc, 1.3, 1.0, 0.7, 1, 9, 0, 2, cm)
     d = np.abs(np.angle(np.exp(1j * (u1 - t_o[pos]))))
     assert d.max() < 1e-9, d.max()
+
+    # O(3) with the user's Heisenberg term and LocalRotation(0.6), 2 sweeps, keys 21
+    g = umc.cubic_lattice(8, 8, 8)
+    n = 512
+    pos, doff, dbonds, key = device_csr(g)
+    v0, v1 = take(np.float64, 3 * n).reshape(n, 3), take(np.float64, 3 * n).reshape(n, 3)
+    assert at == len(raw)
+    cm = np.empty((n, 3))
+    cm[pos] = v0
+    v_o, _, margin = oracle.vector_metropolis(3, doff, dbonds, 1.0, 0.693, 1, 0.6, 21, 0, 2, cm)
+    assert np.abs(v1 - v_o[pos]).max() < 1e-9
+    assert abs(np.linalg.norm(v1, axis=1) - 1).max() < 1e-12
