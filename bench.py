@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--workload", choices=["o3", "ising", "su3", "xybatch", "u1batch", "u1learned", "userxy",
-                                          "usero3", "usero3csr"],
+                                          "usero3", "usero3csr", "userwolff"],
                    default="o3",
                    help="o3: the headline configuration; ising / su3 / xybatch / userxy / usero3 / usero3csr: "
                         "secondary roofline runs (user*: user-written models through include/umc/device.cuh); "
@@ -723,6 +723,7 @@ def _device_models_lib():
     lib.um_session_stats.argtypes = [vp, C.POINTER(u64), C.POINTER(d), C.c_int]
     lib.um_session_energy.argtypes = [vp, C.POINTER(d)]
     lib.um_session_counters.argtypes = [vp, C.POINTER(u64), C.POINTER(u32)]
+    lib.um_session_take_sizes.argtypes = [vp, vp, u64, C.POINTER(u64)]
     return lib
 
 
@@ -737,19 +738,24 @@ class _SessionAsChain:
         return self.wl.lib.um_session_stream(self.wl.h)
 
     def fetch(self, cap):
+        import ctypes as C
+
         import numpy as np
 
         self.kernel_stats(reset=False)  # waits for the stream, surfaces a device error
         rec = np.zeros((self.pending, 1))
+        sizes = np.zeros(self.pending, np.uint64)
+        got = C.c_uint64()
+        self.wl.call(self.wl.lib.um_session_take_sizes(self.wl.h, sizes.ctypes.data, len(sizes), C.byref(got)))
         self.pending = 0
-        return rec, np.zeros(0, np.uint64)
+        return rec, sizes[:min(got.value, len(sizes))]
 
     def kernel_stats(self, reset=False):
         import ctypes as C
 
         n, ms = C.c_uint64(), C.c_double()
         self.wl.call(self.wl.lib.um_session_stats(self.wl.h, C.byref(n), C.byref(ms), int(reset)))
-        return {"metropolis_sweeps": (n.value, ms.value)}
+        return {getattr(self.wl, "kernel_name", "metropolis_sweeps"): (n.value, ms.value)}
 
     def set_timing(self, on):
         self.wl.call(self.wl.lib.um_session_set_timing(self.wl.h, int(on)))
@@ -900,8 +906,84 @@ class UserO3Csr(UserO3):
         super().__init__(umc, args, rank, local, tables=True)
 
 
+class UserIsingWolff(_UserSession):
+    """A user-written Ising pair term in int32 on int8 spins (IsingBondTerm)
+    with a fixed axis, driven by the generic device Wolff of
+    include/umc/device.cuh on an L x L square_lattice's tables, J=1,
+    beta=0.44, cold start; step = one cluster flip (bond activation,
+    union-find labelling and the seed cluster's flip in one cooperative
+    launch).  Units: flipped sites.  The reference runs
+    Wolff<Ising, FixedAxis> through its stock driver."""
+
+    name = "userwolff"
+    dtype = "i8"
+
+    def __init__(self, umc, args, rank, local):
+        import numpy as np
+
+        self.L = args.L if args.L != L_DEFAULT else 2048
+        self.n = self.L * self.L
+        self.g = umc.square_lattice(self.L, self.L)
+        s = np.ones(self.n, np.int8)  # cold start, as Ising's constructor (example/ising.hpp:24)
+        self._open(umc, 3, self.g._h, (0, 0, 0), 1.0, 0.44, 0.0, 1 + rank, s)
+        self.kernel_name = "wolff_flips"
+        self.flush = True  # field, parent array and tables (about 100 MB at 2048^2) fit in L2
+        self.mean_cluster = 0.0
+
+    def describe(self):
+        return (f"user-written Ising PairModel (IsingBondTerm int32 on int8, UpAxis = FixedAxis, "
+                f"examples/device_models) on {self.L}x{self.L} square_lattice tables, J=1, beta=0.44, cold "
+                f"start; step = 1 Wolff flip of the generic device kernel; units = flipped sites")
+
+    def units(self, rec, sizes):
+        if len(sizes):
+            self.mean_cluster = float(sizes.mean())
+        return float(sizes.sum())
+
+    def bytes_per_launch(self, kind):
+        # per site and flip: parent init 4 + offset 4 + four bonds 16 + own and
+        # neighbour spins 2 + parent read in the flip 4 = 30 B; per cluster
+        # site the spin's read and write, 2 B
+        return 30.0 * self.n + 2.0 * self.mean_cluster
+
+    def e2e(self, torch, K):
+        import ctypes as C
+
+        # the chain's current (equilibrated) field, uploaded before every flip:
+        # each step is one flip from the same state, like the timed steps
+        host = torch.empty(self.n, dtype=torch.int8, pin_memory=True)
+        self.call(self.lib.um_session_get_field(self.h, host.data_ptr()))
+        self.ch.fetch(0)
+        e = C.c_double()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(K):
+            self.call(self.lib.um_session_set_field(self.h, host.data_ptr()))
+            self.enqueue(1)
+            self.call(self.lib.um_session_energy(self.h, C.byref(e)))
+        torch.cuda.synchronize()
+        _, sizes = self.ch.fetch(0)
+        return {"value": float(sizes.sum()) / (time.perf_counter() - t0), "unit": self.unit,
+                "h2d_bytes_per_step": self.field.nbytes, "d2h_bytes_per_step": 8 + min(1024, (self.n + 255) // 256) * 8,
+                "steps": K}
+
+    def cpu(self, seconds):
+        from oracle.oracle import Reference, have_reference
+
+        if not have_reference():
+            return None
+        r = Reference()
+        threads = cpu_threads()
+        su, sec = r.bench_ising_wolff(256, 0.44, 50, 50, 1, 1)
+        flips = max(50, int(seconds * 50 / max(sec, 1e-4)))
+        su, sec = r.bench_ising_wolff(256, 0.44, 200, flips, threads, 1)
+        return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                "sample": f"{flips} flips x {threads} independent 256x256 Ising chains (reference Wolff<Ising, "
+                          f"FixedAxis>, stock driver, 200 warm-up flips), {sec:.1f} s"}
+
+
 WORKLOADS = {"o3": O3Hybrid, "ising": IsingSweep, "su3": SU3Sweep, "xybatch": XYBatch, "u1batch": U1LearnedSweep,
-             "userxy": UserXY, "usero3": UserO3, "usero3csr": UserO3Csr}
+             "userxy": UserXY, "usero3": UserO3, "usero3csr": UserO3Csr, "userwolff": UserIsingWolff}
 
 
 def run_learned(args):
@@ -1085,7 +1167,7 @@ def main():
         "config": {"workload": wl.describe(), "L": wl.L, "parallelism": f"replicas x{ws}" if ws > 1 else "1 chain",
                    "l2": ("flushed between timed steps (256 MiB write, outside the timed events)" if wl.flush
                           else "state larger than L2, no flush"),
-                   "mean_cluster": float(sizes.mean()) if len(sizes) and wl.name == "o3" else None},
+                   "mean_cluster": float(sizes.mean()) if len(sizes) and wl.name in ("o3", "userwolff") else None},
         "roofline": {"bound": roof["bound"], "achieved": achieved, "peak": peak, "unit": roof["unit"],
                      "frac": achieved / peak, "traffic": traffic, "kernel": kind, "avg_launch_us": avg_s * 1e6,
                      "peak_source": roof["peak_source"]},

@@ -309,7 +309,7 @@ int um_o3_wolff(const umc_graph* g, double J, double beta, std::uint64_t seed, s
         Buffer<double> field(std::size_t(t.sites()) * 3);
         t.upload(field, spins, 3);
         auto model = t.model<Vec<3>>(field.data(), DotTerm<3>{J});
-        Wolff<decltype(model), Sphere3> w(model, Sphere3{}, seed, beta);
+        Wolff<decltype(model), Sphere3> w(model, Sphere3{}, t, seed, beta);
         w.set_flips(flip0);
         if (sweeps)
             w.run(n);
@@ -322,16 +322,18 @@ int um_o3_wolff(const umc_graph* g, double J, double beta, std::uint64_t seed, s
 }
 
 // Ising Wolff (IsingBondTerm, UpAxis) on a library pair graph: n flips, their
-// sizes to `sizes`; spins (sites, site order) in/out.
+// sizes to `sizes`; spins (sites, site order) in/out.  tiled: the driver gets
+// the tables (shared-memory tile labelling) or not (global union-find only).
 int um_ising_wolff(const umc_graph* g, std::int32_t J, double beta, std::uint64_t seed, std::uint64_t flip0,
-                   std::uint32_t n, std::int8_t* spins, std::uint64_t* sizes)
+                   std::uint32_t n, std::int8_t* spins, std::uint64_t* sizes, int tiled)
 {
     return guarded([&] {
         PairTables t(g);
         Buffer<std::int8_t> field(t.sites());
         t.upload(field, spins, 1);
         auto model = t.model<Spin>(field.data(), IsingBondTerm{J});
-        Wolff<decltype(model), UpAxis> w(model, UpAxis{}, seed, beta);
+        using W = Wolff<decltype(model), UpAxis>;
+        W w = tiled ? W(model, UpAxis{}, t, seed, beta) : W(model, UpAxis{}, seed, beta);
         w.set_flips(flip0);
         w.flips(n, sizes);
         t.download(field, spins, 1);
@@ -351,7 +353,7 @@ int um_lattice_o3(std::uint32_t Lx, std::uint32_t Ly, std::uint32_t Lz, double J
         t.upload(field, spins, 3);
         auto model = t.model<Vec<3>>(field.data(), DotTerm<3>{J});
         if (wolff) {
-            Wolff<decltype(model), Sphere3> w(model, Sphere3{}, seed, beta);
+            Wolff<decltype(model), Sphere3> w(model, Sphere3{}, t, seed, beta);
             w.set_flips(first);
             w.flips(n, sizes);
         } else {
@@ -369,7 +371,8 @@ int um_lattice_o3(std::uint32_t Lx, std::uint32_t Ly, std::uint32_t Lz, double J
 // launches bench.py times.  Kinds:
 //   0  XY (CosineTerm + AngleShift, FP64) on a library pair graph's tables;
 //   1  O(3) (DotTerm<3, float> + SphereF, FP32) on a table-free RegularLattice;
-//   2  the same O(3) model on the lattice's CSR tables (PairTables).
+//   2  the same O(3) model on the lattice's CSR tables (PairTables);
+//   3  Ising Wolff (IsingBondTerm + UpAxis) on a library pair graph's tables.
 namespace {
 
 template <class T, std::size_t N>
@@ -443,6 +446,8 @@ struct SessionBase
     virtual double energy() = 0;
     virtual std::uint64_t sweeps() const = 0;
     virtual std::uint32_t grid() const = 0;
+    // Sites each step updated since the last call (Wolff: cluster sizes).
+    virtual std::vector<std::uint64_t> take_sizes() { return {}; }
 
     void fold()
     {
@@ -487,6 +492,34 @@ struct Session final : SessionBase
     Metropolis<decltype(std::declval<Tables&>().template model<D>(nullptr, std::declval<Term>())), Q> mc;
 };
 
+// Ising Wolff (IsingBondTerm + UpAxis) on a library pair graph's tables; a
+// launch is n flips, and their sizes are kept for take_sizes().
+struct IsingWolffSession final : SessionBase
+{
+    IsingWolffSession(const umc_graph* g, std::int32_t J, double beta, std::uint64_t seed)
+        : tables(g), field(tables.sites()),
+          w(tables.model<Spin>(field.data(), IsingBondTerm{J}), UpAxis{}, tables, seed, beta, stream)
+    {}
+    void set_field(const void* host) override { tables.upload(field, static_cast<const std::int8_t*>(host), 1, stream); }
+    void get_field(void* host) override { tables.download(field, static_cast<std::int8_t*>(host), 1, stream); }
+    void launch(std::uint64_t n) override
+    {
+        const std::size_t at = sizes.size();
+        sizes.resize(at + n);
+        w.flips(n, sizes.data() + at);
+    }
+    void check() override {}
+    double energy() override { return 0.5 * w.energy_at_sum(); }
+    std::uint64_t sweeps() const override { return w.flips_done(); }
+    std::uint32_t grid() const override { return w.grid(); }
+    std::vector<std::uint64_t> take_sizes() override { return std::exchange(sizes, {}); }
+
+    PairTables tables;
+    Buffer<std::int8_t> field;
+    Wolff<PairModel<Spin, IsingBondTerm>, UpAxis> w;
+    std::vector<std::uint64_t> sizes;
+};
+
 using XYSession = Session<PairTables, Angle, CosineTerm, AngleShift>;
 using O3LatticeSession = Session<LatticeTables, VecT<float, 3>, DotTermT<float, 3>, SphereF>;
 using O3TableSession = Session<PairTables, VecT<float, 3>, DotTermT<float, 3>, SphereF>;
@@ -506,7 +539,8 @@ struct LatticeGraph
 
 extern "C" {
 
-// kind 0: graph, J, beta, width (dims unused); kinds 1, 2: dims Lx, Ly, Lz, J, beta.
+// kind 0: graph, J, beta, width (dims unused); kinds 1, 2: dims Lx, Ly, Lz, J,
+// beta; kind 3: graph, J (an integer), beta.
 int um_session_create(int kind, const umc_graph* g, std::uint32_t Lx, std::uint32_t Ly, std::uint32_t Lz, double J,
                       double beta, double width, std::uint64_t seed, void** out)
 {
@@ -520,6 +554,8 @@ int um_session_create(int kind, const umc_graph* g, std::uint32_t Lx, std::uint3
             LatticeGraph lg(Lx, Ly, Lz);
             *out = static_cast<SessionBase*>(
                 new O3TableSession(lg.g, DotTermT<float, 3>{float(J)}, SphereF{}, beta, seed));
+        } else if (kind == 3) {
+            *out = static_cast<SessionBase*>(new IsingWolffSession(g, std::int32_t(J), beta, seed));
         } else {
             throw std::invalid_argument("unknown session kind");
         }
@@ -591,6 +627,17 @@ int um_session_stats(void* h, std::uint64_t* launches, double* ms, int reset)
 int um_session_energy(void* h, double* e)
 {
     return guarded([&] { *e = static_cast<SessionBase*>(h)->energy(); });
+}
+
+// Sizes of the Wolff flips since the last call (at most cap; *n = how many
+// there were); nothing for Metropolis sessions.
+int um_session_take_sizes(void* h, std::uint64_t* out, std::uint64_t cap, std::uint64_t* n)
+{
+    return guarded([&] {
+        const auto s = static_cast<SessionBase*>(h)->take_sizes();
+        *n = s.size();
+        for (std::size_t k = 0; k < s.size() && k < cap; ++k) out[k] = s[k];
+    });
 }
 
 int um_session_counters(void* h, std::uint64_t* sweeps, std::uint32_t* grid)

@@ -382,13 +382,17 @@ class ColourMajor
 {
 public:
     explicit ColourMajor(const detail::Colouring& c)
-        : position_(c.position), order_(c.order()), begin_(c.begin()), order_dev_(order_)
+        : position_(c.position), order_(c.order()), begin_(c.begin()), order_dev_(order_), position_dev_(position_)
     {}
 
     std::uint32_t sites() const noexcept { return std::uint32_t(position_.size()); }
     const std::vector<std::uint32_t>& position() const noexcept { return position_; }
     const std::vector<std::uint32_t>& order() const noexcept { return order_; }
     const std::vector<std::uint32_t>& class_begin() const noexcept { return begin_; }
+    // On the device: the reference site of each device site, and the device
+    // site of each reference site (Wolff's site-order tiles use both).
+    const std::uint32_t* device_order() const noexcept { return order_dev_.data(); }
+    const std::uint32_t* device_position() const noexcept { return position_dev_.data(); }
 
     // field (sites * per_site, device numbering) <- host (site order).  Ordered
     // on stream s; a pinned host buffer must stay valid until s passes the copy.
@@ -428,7 +432,7 @@ private:
     }
 
     std::vector<std::uint32_t> position_, order_, begin_;
-    Buffer<std::uint32_t> order_dev_;
+    Buffer<std::uint32_t> order_dev_, position_dev_;
     mutable Buffer<unsigned char> stage_;
 };
 
@@ -562,6 +566,8 @@ public:
     explicit PairTables(const umc_graph* g) : PairTables(g, detail::colouring_of(g)) {}
 
     const ClassTable& classes() const noexcept { return classes_; }
+    // Bond slots of the CSR (each bond appears in both endpoints' rows).
+    std::uint64_t bond_slots() const noexcept { return bonds_.size(); }
 
     // A PairModel view over field (sites * D::size device scalars, device numbering).
     template <class D, class Term>
@@ -856,6 +862,7 @@ public:
 
     const RegularLattice& lattice() const noexcept { return lattice_; }
     const ClassTable& classes() const noexcept { return classes_; }
+    std::uint64_t bond_slots() const noexcept { return std::uint64_t(lattice_.sites()) * lattice_.degree(); }
 
     template <class D, class Term>
     LatticePairModel<D, Term> model(typename D::dtype* field, Term term) const
@@ -1047,13 +1054,22 @@ struct WolffControl
     Control bar;
     unsigned long long touched;  // sites flipped by this launch
     unsigned done;               // flips completed by this launch
-    unsigned uf_status;          // bit 1: a find or union ran past kUfLimit
+    unsigned uf_status;          // bit 1: a find or union ran past kUfLimit; bit 2: crossing list full
+    unsigned long long xcount;   // active bonds between tiles in this flip (tiled kernel)
 };
 
 __device__ __forceinline__ std::uint32_t uf_load(const std::uint32_t* p) { return *(const volatile std::uint32_t*)p; }
 
-// Root of x with path halving.  Links only point to smaller indices, so every
-// step moves down and the walk ends within x steps.
+// Linking order of the union-find: a root is linked under a root of higher
+// priority, the priority of site x being stream_id(x) (a bijection of 32-bit
+// words, so the order is strict).  Random priorities keep the trees shallow
+// and spread the roots, and so the CAS traffic, over memory; linking by index
+// piled the unions of a large cluster onto a few low-index roots.
+__device__ __forceinline__ bool uf_below(std::uint32_t a, std::uint32_t b) { return stream_id(a) < stream_id(b); }
+
+// Root of x with path halving.  The links form a forest (a union links a root
+// under another root; the tiled kernel also points sites at their tile's
+// root), so a walk ends within n steps; kUfLimit guards it all the same.
 __device__ __forceinline__ std::uint32_t uf_root(std::uint32_t* parent, std::uint32_t x, unsigned* status)
 {
     for (unsigned it = 0; it < kUfLimit; ++it) {
@@ -1067,14 +1083,14 @@ __device__ __forceinline__ std::uint32_t uf_root(std::uint32_t* parent, std::uin
     return x;
 }
 
-// Joins the sets of a and b: the larger root is linked under the smaller.
+// Joins the sets of a and b: the root of lower priority is linked under the other.
 __device__ __forceinline__ void uf_unite(std::uint32_t* parent, std::uint32_t a, std::uint32_t b, unsigned* status)
 {
     for (unsigned it = 0; it < kUfLimit; ++it) {
         a = uf_root(parent, a, status);
         b = uf_root(parent, b, status);
         if (a == b) return;
-        if (a > b) {
+        if (uf_below(a, b)) {
             const std::uint32_t t = a;
             a = b;
             b = t;
@@ -1093,6 +1109,20 @@ __device__ __forceinline__ typename M::bond_type bond_of(const M& m, std::uint32
         return m.bond(i, a);
     else
         return m.bonds(i)[a];
+}
+
+// u < 1 - exp(-x) for x > 0, decided as the FP64 test decides it.
+// 1 - expf(-float(x)) is within 2^-22 of 1 - exp(-x): rounding x to float
+// moves exp(-x) by at most x e^-x 2^-24 < 2^-24, and expf's 2-ulp error is at
+// most 2^-23 for a result below 1.  The FP32 answer is taken when it clears u
+// by 2^-19, eight times that; otherwise FP64 decides.
+__device__ __forceinline__ bool activates(double u, double x)
+{
+    const double p32 = 1.0 - double(expf(-float(x)));
+    const double gap = u - p32;
+    if (gap > 0x1.0p-19) return false;
+    if (gap < -0x1.0p-19) return true;
+    return u < 1.0 - exp(-x);
 }
 
 // out = s - 2 (s . r) r, in T arithmetic as Wolff::flip does (driver.hpp:127-130).
@@ -1116,7 +1146,9 @@ template <class M, class A>
 __global__ void __launch_bounds__(kThreads) wolff_flips(M m, A axis, double beta, std::uint64_t seed,
                                                         std::uint64_t flip0, std::uint32_t max_flips,
                                                         std::uint64_t target, std::uint32_t* parent,
-                                                        unsigned long long* sizes, WolffControl* ctl)
+                                                        unsigned long long* sizes, WolffControl* ctl,
+                                                        const std::uint32_t*, const std::uint32_t*, uint2*,
+                                                        unsigned long long)  // the tiled kernel's; unused
 {
     using T = typename M::value_type;
     constexpr std::size_t D = M::size;
@@ -1145,13 +1177,18 @@ __global__ void __launch_bounds__(kThreads) wolff_flips(M m, A axis, double beta
                 T nb[D];
                 reflect<T, D>(m.data() + std::size_t(j) * D, r, nb);
                 const double dE = m.energy_diff_bond(i, b, nb);
+                if (!(beta * dE > 0.0)) continue;  // p = 1 - exp(-beta dE) <= 0: never active
                 Rng u(KeyedPcg::open(kbond, m.bond_id(i, a)));
-                if (u.uni() < 1.0 - exp(-beta * dE)) uf_unite(parent, i, j, &ctl->uf_status);
+                if (activates(u.uni(), beta * dE)) uf_unite(parent, i, j, &ctl->uf_status);
             }
         }
         if (!grid_sync(&ctl->bar)) return;
 
-        const std::uint32_t root = uf_root(parent, seed_site, &ctl->uf_status);
+        // the seed's root, found once per block (the trees are fixed in this phase)
+        __shared__ std::uint32_t root_sh;
+        if (threadIdx.x == 0) root_sh = uf_root(parent, seed_site, &ctl->uf_status);
+        __syncthreads();
+        const std::uint32_t root = root_sh;
         unsigned long long mine = 0;
         for (std::uint32_t i = t; i < n; i += stride) {
             if (uf_root(parent, i, &ctl->uf_status) != root) continue;
@@ -1163,6 +1200,152 @@ __global__ void __launch_bounds__(kThreads) wolff_flips(M m, A axis, double beta
         if (mine) atomicAdd(&block_count, mine);
         __syncthreads();
         if (threadIdx.x == 0 && block_count) atomicAdd(sizes + f, block_count);
+        if (!grid_sync(&ctl->bar)) return;
+        touched += __ldcg(sizes + f);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            ctl->done = f + 1;
+            ctl->touched = touched;
+        }
+        if (target > 0 && touched >= target) return;
+    }
+}
+
+// Whether the a-th bond of i (j > i) is active in this flip: the same test,
+// draw and key as wolff_flips.
+template <class M, class T, std::size_t D>
+__device__ __forceinline__ bool bond_active(const M& m, std::uint32_t i, std::size_t a,
+                                            const typename M::bond_type& b, const T* r, double beta,
+                                            std::uint64_t kbond)
+{
+    T nb[D];
+    reflect<T, D>(m.data() + std::size_t(b.j) * D, r, nb);
+    const double dE = m.energy_diff_bond(i, b, nb);
+    if (!(beta * dE > 0.0)) return false;
+    Rng u(KeyedPcg::open(kbond, m.bond_id(i, a)));
+    return activates(u.uni(), beta * dE);
+}
+
+// Reference sites per shared-memory tile (16-bit local labels, 8 KB).  Larger
+// tiles cut the crossing bonds but leave blocks without a tile: 16,384 ran a
+// 2048^2 flip in 0.68 ms against 0.41 ms here.
+constexpr std::uint32_t kWolffTile = 4096;
+
+// Local root of t in a tile's shared-memory forest (links point to smaller t).
+__device__ __forceinline__ std::uint32_t tile_root(unsigned short* lab, std::uint32_t t)
+{
+    for (std::uint32_t it = 0; it < kWolffTile; ++it) {
+        const std::uint32_t p = *(volatile unsigned short*)(lab + t);
+        if (p == t) return t;
+        const std::uint32_t gp = *(volatile unsigned short*)(lab + p);
+        if (gp != p) *(volatile unsigned short*)(lab + t) = (unsigned short)gp;
+        t = gp;
+    }
+    return t;  // unreachable: each step moves to a smaller index
+}
+
+__device__ __forceinline__ void tile_unite(unsigned short* lab, std::uint32_t a, std::uint32_t b)
+{
+    for (std::uint32_t it = 0; it < 4 * kWolffTile; ++it) {
+        a = tile_root(lab, a);
+        b = tile_root(lab, b);
+        if (a == b) return;
+        if (a > b) {
+            const std::uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(lab + b, (unsigned short)b, (unsigned short)a) == b) return;
+    }
+}
+
+// wolff_flips with the labelling done in two levels.  Each block takes tiles
+// of kWolffTile consecutive reference sites (site_of / dev_of translate to and
+// from the device numbering): the active bonds inside a tile are united in
+// shared memory, every site's global parent is set to its tile root, and the
+// active bonds between tiles go to a list that a second phase unites in
+// global memory.  Same bonds, draws and keys as wolff_flips, so the same
+// clusters; far fewer global unions and shallow global trees.
+template <class M, class A>
+__global__ void __launch_bounds__(kThreads) wolff_flips_tiled(M m, A axis, double beta, std::uint64_t seed,
+                                                              std::uint64_t flip0, std::uint32_t max_flips,
+                                                              std::uint64_t target, std::uint32_t* parent,
+                                                              unsigned long long* sizes, WolffControl* ctl,
+                                                              const std::uint32_t* __restrict__ site_of,
+                                                              const std::uint32_t* __restrict__ dev_of,
+                                                              uint2* xlist, unsigned long long xcap)
+{
+    using T = typename M::value_type;
+    constexpr std::size_t D = M::size;
+    __shared__ unsigned short lab[kWolffTile];
+    __shared__ unsigned long long block_count;
+    __shared__ std::uint32_t root_sh;
+    const std::uint32_t n = std::uint32_t(m.sites());
+    const std::uint32_t tiles = (n + kWolffTile - 1) / kWolffTile;
+    unsigned long long touched = 0;
+    for (std::uint32_t f = 0; f < max_flips; ++f) {
+        const std::uint64_t counter = flip0 + f;
+        Rng g(KeyedPcg::open_key(seed, counter, kTagAxis, 0));
+        T r[D];
+        axis.sample(static_cast<const T*>(nullptr), g, r);
+        const std::uint32_t seed_site = std::uint32_t(g.uni() * double(n));
+        const std::uint64_t kbond = key_base(key_seed(seed, counter, kTagBond));
+        if (threadIdx.x == 0) block_count = 0;
+
+        // tiles: local unions in shared memory, crossing bonds to the list
+        for (std::uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+            const std::uint32_t s0 = tile * kWolffTile;
+            const std::uint32_t len = min(kWolffTile, n - s0);
+            for (std::uint32_t t = threadIdx.x; t < len; t += blockDim.x) lab[t] = (unsigned short)t;
+            __syncthreads();
+            for (std::uint32_t t = threadIdx.x; t < len; t += blockDim.x) {
+                const std::uint32_t i = dev_of[s0 + t];
+                const std::size_t deg = m.degree(i);
+                for (std::size_t a = 0; a < deg; ++a) {
+                    const auto b = bond_of(m, i, a);
+                    const std::uint32_t j = std::uint32_t(b.j);
+                    if (j <= i || !bond_active<M, T, D>(m, i, a, b, r, beta, kbond)) continue;
+                    const std::uint32_t sj = site_of[j];
+                    if (sj - s0 < len) {
+                        tile_unite(lab, t, sj - s0);
+                    } else {
+                        const unsigned long long at = atomicAdd(&ctl->xcount, 1ull);
+                        if (at < xcap) xlist[at] = make_uint2(i, j);
+                        else atomicOr(&ctl->uf_status, 4u);
+                    }
+                }
+            }
+            __syncthreads();
+            for (std::uint32_t t = threadIdx.x; t < len; t += blockDim.x)
+                parent[dev_of[s0 + t]] = dev_of[s0 + tile_root(lab, t)];
+            __syncthreads();
+        }
+        if (!grid_sync(&ctl->bar)) return;
+
+        // crossing bonds: global unions
+        const unsigned long long xn = min(__ldcg(&ctl->xcount), xcap);
+        for (unsigned long long e = blockIdx.x * std::uint64_t(blockDim.x) + threadIdx.x; e < xn;
+             e += std::uint64_t(gridDim.x) * blockDim.x) {
+            const uint2 bj = xlist[e];
+            uf_unite(parent, bj.x, bj.y, &ctl->uf_status);
+        }
+        if (!grid_sync(&ctl->bar)) return;
+
+        // the seed's cluster, as in wolff_flips
+        if (threadIdx.x == 0) root_sh = uf_root(parent, seed_site, &ctl->uf_status);
+        __syncthreads();
+        const std::uint32_t root = root_sh;
+        unsigned long long mine = 0;
+        for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+            if (uf_root(parent, i, &ctl->uf_status) != root) continue;
+            T prop[D];
+            reflect<T, D>(m.data() + std::size_t(i) * D, r, prop);
+            m.update(i, prop);
+            ++mine;
+        }
+        if (mine) atomicAdd(&block_count, mine);
+        __syncthreads();
+        if (threadIdx.x == 0 && block_count) atomicAdd(sizes + f, block_count);
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->xcount = 0;  // read by no one until the next flip's list
         if (!grid_sync(&ctl->bar)) return;
         touched += __ldcg(sizes + f);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1302,6 +1485,24 @@ public:
             throw std::invalid_argument("Wolff: the model needs 1 to 2^32 - 1 sites");
         grid_ = detail::cooperative_grid(kernel(), (model.sites() + detail::kThreads - 1) / detail::kThreads);
     }
+    // With the tables the model was made from (PairTables, LatticeTables):
+    // the labelling runs in shared-memory tiles of consecutive reference
+    // sites first (wolff_flips_tiled), with the same clusters.
+    template <class Tables>
+        requires requires(const Tables& t) {
+            { t.device_order() } -> std::convertible_to<const std::uint32_t*>;
+            { t.device_position() } -> std::convertible_to<const std::uint32_t*>;
+            { t.bond_slots() } -> std::convertible_to<std::uint64_t>;
+        }
+    Wolff(M model, A axis, const Tables& layout, std::uint64_t seed, double beta, cudaStream_t stream = nullptr)
+        : Wolff(model, axis, seed, beta, stream)
+    {
+        if (layout.sites() != model.sites()) throw std::invalid_argument("Wolff: tables of another size");
+        site_of_ = layout.device_order();
+        dev_of_ = layout.device_position();
+        xlist_ = Buffer<uint2>(std::max<std::uint64_t>(1, layout.bond_slots()));
+        grid_ = detail::cooperative_grid(kernel(), (model.sites() + detail::kThreads - 1) / detail::kThreads);
+    }
 
     // One cluster flip; returns how many sites it flipped (driver.hpp:104-162).
     std::size_t flip()
@@ -1371,7 +1572,11 @@ public:
 
 private:
     static constexpr std::uint32_t kCapacity = 1u << 16;
-    static const void* kernel() { return reinterpret_cast<const void*>(&detail::wolff_flips<M, A>); }
+    const void* kernel() const
+    {
+        return site_of_ ? reinterpret_cast<const void*>(&detail::wolff_flips_tiled<M, A>)
+                        : reinterpret_cast<const void*>(&detail::wolff_flips<M, A>);
+    }
 
     // Up to max_flips flips (fewer once target sites are flipped, target > 0);
     // returns the sites flipped and writes one size per flip to sizes_out.
@@ -1388,13 +1593,18 @@ private:
         std::uint32_t* parent = parent_.data();
         unsigned long long* sizes = sizes_.data();
         detail::WolffControl* ctl = ctl_.data();
-        void* args[] = {&m, &a, &beta, &seed, &flip0, &nf, &tgt, &parent, &sizes, &ctl};
+        const std::uint32_t* site_of = site_of_;
+        const std::uint32_t* dev_of = dev_of_;
+        uint2* xlist = xlist_.data();
+        unsigned long long xcap = xlist_.size();
+        void* args[] = {&m, &a, &beta, &seed, &flip0, &nf, &tgt, &parent, &sizes, &ctl, &site_of, &dev_of, &xlist, &xcap};
         cuda_check(cudaLaunchCooperativeKernel(kernel(), dim3(grid_), dim3(detail::kThreads), args, 0, stream_),
                    "Wolff launch");
         detail::WolffControl h{};
         cuda_check(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, stream_), "read control");
         cuda_check(cudaStreamSynchronize(stream_), "Wolff");
         if (h.bar.status != 0u) throw std::runtime_error("Wolff: a grid barrier wait ran out");
+        if (h.uf_status & 4u) throw std::runtime_error("Wolff: the crossing-bond list overflowed");
         if (h.uf_status != 0u) throw std::runtime_error("Wolff: a union-find walk ran past its limit");
         std::vector<unsigned long long> sz(h.done);
         if (h.done)
@@ -1416,6 +1626,9 @@ private:
     Buffer<std::uint32_t> parent_;
     Buffer<unsigned long long> sizes_;
     Buffer<detail::WolffControl> ctl_;
+    const std::uint32_t* site_of_ = nullptr;  // tiled labelling (with tables)
+    const std::uint32_t* dev_of_ = nullptr;
+    Buffer<uint2> xlist_;
     std::uint32_t grid_ = 1;
     std::uint64_t flips_ = 0;
     double size_sum_ = 0.0;

@@ -79,7 +79,8 @@ template <class M, class A>
 class UserWolff final : public UserField<M>
 {
 public:
-    UserWolff(const M& m, const A& a, std::uint64_t key, double beta) : UserField<M>(m), w_(this->view(m), a, key, beta)
+    UserWolff(const M& m, const A& a, std::uint64_t key, double beta)
+        : UserField<M>(m), w_(this->view(m), a, this->tables_, key, beta)
     {}
     void run(std::size_t n, std::uint64_t* sizes) override { w_.flips(n, sizes); }
 

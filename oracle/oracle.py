@@ -431,6 +431,7 @@ class Reference:
         self._bench_ising = L.fn("bench_ising", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._bench_xy = L.fn("bench_xy", _int, _u64, _f64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._bench_pair_o3 = L.fn("bench_pair_o3", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
+        self._bench_ising_wolff = L.fn("bench_ising_wolff", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
 
     def pcg32_draws(self, seed, stream, n):
         out = np.zeros(n, np.uint32)
@@ -639,6 +640,19 @@ def _bench_pair_o3(self, L, beta, warmup, sweeps, threads, seed=1):
 
 
 Reference.bench_pair_o3 = _bench_pair_o3
+
+
+def _bench_ising_wolff(self, L, beta, warmup, flips, threads, seed=1):
+    """Reference Ising Wolff (FixedAxis) on L x L: (flipped sites of the timed
+    flips over all threads, seconds of the slowest thread)."""
+    su = C.c_double()
+    sec = C.c_double()
+    st = self._bench_ising_wolff(L, beta, warmup, flips, threads, seed, C.byref(su), C.byref(sec))
+    assert st == 0, st
+    return su.value, sec.value
+
+
+Reference.bench_ising_wolff = _bench_ising_wolff
 
 
 def have_reference() -> bool:

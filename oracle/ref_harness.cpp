@@ -940,6 +940,41 @@ extern "C" int ref_bench_ising(std::uint64_t L, double beta, std::uint64_t warmu
     }
 }
 
+// Times the reference's stock Ising Wolff: Ising on an L x L square_lattice
+// (cold start, then `warmup` flips) with FixedAxis and a plain Pcg32, one
+// chain per thread; site_updates = the flipped sites of the timed flips.
+extern "C" int ref_bench_ising_wolff(std::uint64_t L, double beta, std::uint64_t warmup, std::uint64_t flips,
+                                     std::uint32_t threads, std::uint64_t seed, double* site_updates, double* seconds)
+{
+    try {
+        std::vector<double> secs(threads, 0.0), sites(threads, 0.0);
+        std::vector<std::thread> pool;
+        for (std::uint32_t t = 0; t < threads; ++t)
+            pool.emplace_back([&, t] {
+                Ising model(square_lattice(L, L), 1);
+                Wolff<Ising, FixedAxis, Pcg32> w(model, FixedAxis{}, Pcg32(seed + t, 2), beta);
+                for (std::uint64_t f = 0; f < warmup; ++f) (void)w.flip();
+                double u = 0.0;
+                const auto t0 = std::chrono::steady_clock::now();
+                for (std::uint64_t f = 0; f < flips; ++f) u += double(w.flip());
+                const auto t1 = std::chrono::steady_clock::now();
+                secs[t] = std::chrono::duration<double>(t1 - t0).count();
+                sites[t] = u;
+            });
+        for (auto& th : pool) th.join();
+        double worst = 0.0, total = 0.0;
+        for (std::uint32_t t = 0; t < threads; ++t) {
+            worst = secs[t] > worst ? secs[t] : worst;
+            total += sites[t];
+        }
+        *site_updates = total;
+        *seconds = worst;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
 // Times the reference's stock XY model on angles: PairModel<U1Dof, -J cos> on an
 // L x L square_lattice with U1Shift{width} and a plain Pcg32, one chain per
 // thread, uniform random start.

@@ -239,19 +239,21 @@ def test_user_wolff_sweep_flips_until_the_lattice_is_covered(umc, oracle, lib):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("L,beta", [(16, 0.44), (64, 0.3), (48, 0.6)])
-def test_user_ising_wolff_is_bit_exact(umc, oracle, lib, L, beta):
+@pytest.mark.parametrize("L,beta,tiled", [(16, 0.44, 0), (64, 0.3, 0), (48, 0.6, 0), (16, 0.44, 1), (64, 0.3, 1),
+                                          (48, 0.6, 1), (200, 0.44, 1), (100, 0.5, 0)])
+def test_user_ising_wolff_is_bit_exact(umc, oracle, lib, L, beta, tiled):
     """Wolff<PairModel<Spin, IsingBondTerm>, UpAxis> (int8 spins, int32 energy,
     FixedAxis): 20 flips in one launch equal the oracle's spins and cluster
-    sizes bit for bit."""
-    lib.um_ising_wolff.argtypes = [_vp, C.c_int32, _d, _u64, _u64, _u32, _vp, _vp]
+    sizes bit for bit, with the global union-find alone (tiled 0) and with the
+    shared-memory tiles first (tiled 1; 200^2 spans ten tiles)."""
+    lib.um_ising_wolff.argtypes = [_vp, C.c_int32, _d, _u64, _u64, _u32, _vp, _vp, C.c_int]
     g = umc.square_lattice(L, L)
     n = L * L
     pos, doff, dbonds, key = device_csr(g)
     s0 = np.where(np.random.default_rng(L).random(n) < 0.5, 1, -1).astype(np.int8)
     s = s0.copy()
     sizes = np.zeros(20, np.uint64)
-    _call(lib, lib.um_ising_wolff(g._h, 1, beta, 13, 7, 20, s.ctypes.data, sizes.ctypes.data))
+    _call(lib, lib.um_ising_wolff(g._h, 1, beta, 13, 7, 20, s.ctypes.data, sizes.ctypes.data, tiled))
     cm = np.empty(n, np.int8)
     cm[pos] = s0
     s_o, sz_o, _, _ = oracle.ising_wolff(doff, dbonds, key, 1, beta, 13, 7, 20, cm)
