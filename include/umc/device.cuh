@@ -1369,6 +1369,8 @@ template <ModelLike M, class Q>
 class Metropolis
 {
 public:
+    // The driver keeps a reference to classes: a temporary is refused.
+    Metropolis(M, Q, ClassTable&&, std::uint64_t, double, cudaStream_t = nullptr) = delete;
     Metropolis(M model, Q proposal, const ClassTable& classes, std::uint64_t seed, double beta,
                cudaStream_t stream = nullptr)
         : model_(model), proposal_(proposal), classes_(classes), seed_(seed), beta_(beta), stream_(stream),
@@ -1487,7 +1489,12 @@ public:
     }
     // With the tables the model was made from (PairTables, LatticeTables):
     // the labelling runs in shared-memory tiles of consecutive reference
-    // sites first (wolff_flips_tiled), with the same clusters.
+    // sites first (wolff_flips_tiled), with the same clusters.  The driver
+    // keeps pointers into the tables, which must outlive it (a temporary is
+    // refused).
+    template <class Tables>
+        requires(!std::is_lvalue_reference_v<Tables>)
+    Wolff(M, A, Tables&&, std::uint64_t, double, cudaStream_t = nullptr) = delete;
     template <class Tables>
         requires requires(const Tables& t) {
             { t.device_order() } -> std::convertible_to<const std::uint32_t*>;
