@@ -28,3 +28,22 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert "workload" in d["config"] and d["config"]["L"] == 16
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("workload,L", [("userxy", 256), ("usero3", 32), ("usero3csr", 32), ("userwolff", 128)])
+def test_user_model_bench_lines_keep_the_contract(workload, L):
+    """The user-model workloads (generic device kernels of include/umc/device.cuh)
+    print one JSON line with the contract's fields, a roofline of their own
+    kernel and a positive end-to-end figure."""
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--workload", workload, "--L", str(L),
+                        "--steps", "5", "--warmup", "3", "--no-cpu-baseline"], capture_output=True, text=True,
+                       timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.strip().startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["value"] > 0 and d["steps"] == 5 and d["warmup"] == 3 and d["unit"] == "site-updates/s"
+    assert d["roofline"]["kernel"] in ("metropolis_sweeps", "wolff_flips") and d["roofline"]["achieved"] > 0
+    assert d["gpu_launches"] >= 5 and d["e2e"]["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] > 0
+    assert d["config"]["L"] == L and "clocks" in d
