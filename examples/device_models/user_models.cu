@@ -17,8 +17,8 @@
 //   Sphere3      -- UniformSphereN<3> (dof/vector.hpp:35-61).
 //
 // Exported with a C ABI for the Python tests and bench.py (ctypes): one-shot
-// runs (um_xy_pair, um_u1_cells, um_heisenberg_cubic, um_o3_wolff,
-// um_ising_wolff, um_lattice_o3) and persistent sessions (um_session_*) whose
+// runs (um_xy_pair, um_xy_record, um_u1_cells, um_heisenberg_cubic,
+// um_o3_wolff, um_ising_wolff, um_lattice_o3) and persistent sessions (um_session_*) whose
 // launches bench.py times.
 #include <umc/device.cuh>
 
@@ -254,6 +254,24 @@ int um_xy_pair(const umc_graph* g, double J, double beta, double width, std::uin
         mc.sample(n_sweeps, [&](const auto& m) { energies[k++] = 0.5 * m.energy_at_sum(); });
         t.download(field, theta, 1);
         if (grid) *grid = mc.grid();
+    });
+}
+
+// XY as um_xy_pair, but the energies come from one launch that observes on
+// the device (Metropolis::record_energy; energy_at summed, so 2E per sweep).
+int um_xy_record(const umc_graph* g, double J, double beta, double width, std::uint64_t seed, std::uint64_t sweep0,
+                 std::uint32_t n_sweeps, double* theta, double* energies)
+{
+    return guarded([&] {
+        PairTables t(g);
+        Buffer<double> field(t.sites());
+        t.upload(field, theta, 1);
+        auto model = t.model<Angle>(field.data(), CosineTerm{J});
+        Metropolis<decltype(model), AngleShift> mc(model, AngleShift{width}, t.classes(), seed, beta);
+        mc.set_sweeps(sweep0);
+        mc.record_energy(n_sweeps, energies);
+        for (std::uint32_t k = 0; k < n_sweeps; ++k) energies[k] *= 0.5;
+        t.download(field, theta, 1);
     });
 }
 

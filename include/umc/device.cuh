@@ -948,15 +948,39 @@ __device__ __forceinline__ bool log_below(double u, double log_p)
     return log(u) < log_p;
 }
 
+// No per-sweep observable.
+struct NoObservable
+{};
+
+// Sum over the block of v; the result is valid in thread 0.
+__device__ __forceinline__ double block_total(double v)
+{
+    __shared__ double sh[kThreads];
+    __syncthreads();
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int w = kThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    return sh[0];
+}
+
 // n_sweeps Metropolis sweeps (driver.hpp:29-43) over the colour classes.
-template <class M, class Q>
+// With an observable O, record after sweep s the FP64 sum of obs(m, x) over
+// x < obs_count into records[s]: per-block partials, then block 0 adds them in
+// block order (deterministic for a given grid).  This is sample(n, observe)
+// (driver.hpp:54-61) with the observation on the device, inside the launch.
+template <class M, class Q, class O = NoObservable>
 __global__ void __launch_bounds__(kThreads) metropolis_sweeps(M m, Q q, const std::uint32_t* __restrict__ order,
                                                               const std::uint32_t* __restrict__ begin,
                                                               std::uint32_t n_classes, double beta, std::uint64_t seed,
                                                               std::uint64_t sweep0, std::uint32_t n_sweeps,
-                                                              Control* ctl)
+                                                              Control* ctl, O obs = {}, std::uint64_t obs_count = 0,
+                                                              double* partial = nullptr, double* records = nullptr)
 {
     using T = typename M::value_type;
+    constexpr bool kObserve = !std::is_same_v<O, NoObservable>;
     const std::uint32_t stride = gridDim.x * blockDim.x;
     const std::uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     for (std::uint32_t s = 0; s < n_sweeps; ++s) {
@@ -973,7 +997,19 @@ __global__ void __launch_bounds__(kThreads) metropolis_sweeps(M m, Q q, const st
                 const double log_p = -beta * dE + q.log_ratio(cur, cand);
                 if (log_p >= 0.0 || log_below(rng.uni(), log_p)) m.update(i, cand);
             }
-            if ((s + 1 < n_sweeps || c + 1 < n_classes) && !grid_sync(ctl)) return;
+            if ((kObserve || s + 1 < n_sweeps || c + 1 < n_classes) && !grid_sync(ctl)) return;
+        }
+        if constexpr (kObserve) {
+            double v = 0.0;
+            for (std::uint64_t x = t; x < obs_count; x += stride) v += double(obs(m, x));
+            const double b = block_total(v);
+            if (threadIdx.x == 0) partial[blockIdx.x] = b;
+            if (!grid_sync(ctl)) return;
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                double e = 0.0;
+                for (std::uint32_t k = 0; k < gridDim.x; ++k) e += __ldcg(partial + k);
+                records[s] = e;
+            }
         }
     }
 }
@@ -1418,7 +1454,13 @@ public:
             std::uint64_t seed = seed_, sweep0 = sweeps_;
             std::uint32_t n = chunk;
             detail::Control* ctl = ctl_.data();
-            void* args[] = {&m, &q, &order, &begin, &nc, &beta, &seed, &sweep0, &n, &ctl};
+            detail::NoObservable obs;
+            std::uint64_t obs_count = 0;
+            double* partial = nullptr;
+            double* records = nullptr;
+            // every kernel parameter, the unused observable ones included
+            void* args[] = {&m, &q, &order, &begin, &nc, &beta, &seed, &sweep0, &n, &ctl, &obs, &obs_count, &partial,
+                            &records};
             cuda_check(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&detail::metropolis_sweeps<M, Q>),
                                                    dim3(grid_), dim3(detail::kThreads), args, 0, stream_),
                        "Metropolis launch");
@@ -1434,6 +1476,52 @@ public:
         cuda_check(cudaMemcpyAsync(&h, ctl_.data(), sizeof h, cudaMemcpyDeviceToHost, stream_), "read status");
         cuda_check(cudaStreamSynchronize(stream_), "read status");
         if (h.status != 0u) throw std::runtime_error("Metropolis: a grid barrier wait ran out");
+    }
+
+    // n sweeps in one launch, observing on the device: after sweep s,
+    // records[s] (host, n entries) = FP64 sum of obs(model, x) over x < count.
+    // obs is a device functor double(const M&, std::uint64_t).  The
+    // observation is driver.hpp:54-61's observe hook without a host round
+    // trip per sweep.
+    template <class O>
+    void record(std::size_t sweeps, O obs, std::uint64_t count, double* records)
+    {
+        if (sweeps == 0) return;
+        if (sweeps >= (std::size_t(1) << 30)) throw std::invalid_argument("record: at most 2^30 sweeps per call");
+        const void* k = reinterpret_cast<const void*>(&detail::metropolis_sweeps<M, Q, O>);
+        const std::uint32_t grid =
+            detail::cooperative_grid(k, (classes_.host().largest() + detail::kThreads - 1) / detail::kThreads);
+        Buffer<double> partial(grid), rec(sweeps);
+        cuda_check(cudaMemsetAsync(ctl_.data(), 0, sizeof(detail::Control), stream_), "reset barrier");
+        M m = model_;
+        Q q = proposal_;
+        const std::uint32_t* order = classes_.order();
+        const std::uint32_t* begin = classes_.begin();
+        std::uint32_t nc = classes_.host().count();
+        double beta = beta_;
+        std::uint64_t seed = seed_, sweep0 = sweeps_;
+        std::uint32_t n = std::uint32_t(sweeps);
+        detail::Control* ctl = ctl_.data();
+        std::uint64_t cnt = count;
+        double* part = partial.data();
+        double* out = rec.data();
+        void* args[] = {&m, &q, &order, &begin, &nc, &beta, &seed, &sweep0, &n, &ctl, &obs, &cnt, &part, &out};
+        cuda_check(cudaLaunchCooperativeKernel(k, dim3(grid), dim3(detail::kThreads), args, 0, stream_),
+                   "Metropolis launch");
+        sweeps_ += sweeps;
+        cuda_check(cudaMemcpyAsync(records, out, sweeps * sizeof(double), cudaMemcpyDeviceToHost, stream_), "records");
+        cuda_check(cudaStreamSynchronize(stream_), "Metropolis::record");
+        check();
+    }
+    // The energy after each of n sweeps: sum of energy_at (EnergyModel; a
+    // pair model counts every bond twice) or of cell_energy (CellEnergyModel).
+    void record_energy(std::size_t sweeps, double* records)
+        requires EnergyModel<M> || CellEnergyModel<M>
+    {
+        if constexpr (CellEnergyModel<M>)
+            record(sweeps, detail::CellEnergyOf{}, model_.cells(), records);
+        else
+            record(sweeps, detail::EnergyAtOf{}, model_.sites(), records);
     }
 
     // Sum over cells of cell_energy (model/cell.hpp:58-62), FP64.

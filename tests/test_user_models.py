@@ -365,3 +365,21 @@ def test_fp32_user_term_same_on_lattice_and_tables(umc, lib):
     for e0, e in energies:
         assert np.isfinite(e) and e < e0
     assert abs(np.linalg.norm(out[0], axis=1) - 1).max() < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L", [64, 512])
+def test_user_xy_energies_recorded_in_the_launch(umc, lib, L):
+    """Metropolis::record_energy runs the sweeps in one launch and sums
+    energy_at on the device after each: the same chain as sample() with a
+    host observe after every sweep, and the same energies up to the
+    summation order."""
+    lib.um_xy_record.argtypes = [_vp, _d, _d, _d, _u64, _u64, _u32, _dp, _dp]
+    g = umc.square_lattice(L, L)
+    th0 = np.random.default_rng(L + 1).uniform(-np.pi, np.pi, L * L)
+    a, ea, _ = xy_run(lib, g, th0, 1.1, 1.0, 12, 3, 6)
+    b = th0.copy()
+    eb = np.zeros(6)
+    _call(lib, lib.um_xy_record(g._h, 1.0, 1.1, 1.0, 12, 3, 6, _p(b), _p(eb)))
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_allclose(eb, ea, rtol=1e-12, atol=1e-9)
