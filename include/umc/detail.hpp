@@ -76,6 +76,9 @@ struct UserRunner : DeviceCopy
 {
     virtual ~UserRunner() = default;
     virtual void run(std::size_t n, std::uint64_t* sizes) = 0;
+    // n Metropolis sweeps with the total energy after each (observed on the
+    // device); a Wolff runner has none.
+    virtual void run_energy(std::size_t n, double* energy) = 0;
 };
 
 // A model's field on the host as scalars HS in the reference's data() layout,

@@ -70,6 +70,14 @@ public:
         : UserField<M>(m), mc_(this->view(m), q, this->tables_.classes(), key, beta)
     {}
     void run(std::size_t n, std::uint64_t*) override { mc_.run(n); }
+    // E after each sweep: half the sum of energy_at for a pair model (every
+    // bond counted at both ends), the sum of cell_energy for a cell model.
+    void run_energy(std::size_t n, double* energy) override
+    {
+        mc_.record_energy(n, energy);
+        if constexpr (!device::CellEnergyModel<typename UserDevice<M>::View>)
+            for (std::size_t k = 0; k < n; ++k) energy[k] *= 0.5;
+    }
 
 private:
     device::Metropolis<typename UserDevice<M>::View, Q> mc_;
@@ -83,6 +91,7 @@ public:
         : UserField<M>(m), w_(this->view(m), a, this->tables_, key, beta)
     {}
     void run(std::size_t n, std::uint64_t* sizes) override { w_.flips(n, sizes); }
+    void run_energy(std::size_t, double*) override { throw std::logic_error("Wolff records no energies"); }
 
 private:
     device::Wolff<typename UserDevice<M>::View, A> w_;

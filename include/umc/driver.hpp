@@ -13,6 +13,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <limits>
 #include <memory>
 #include <type_traits>
 #include <utility>
@@ -136,16 +137,20 @@ public:
     void sweep() { run(1); }
 
     // n sweeps (one call into the engine).  A user-written term runs in one
-    // launch of umc/device.cuh's Metropolis; records() stays empty then.
+    // launch of umc/device.cuh's Metropolis, which records the energy after
+    // every sweep (records() slot 0; the other slots are NaN).
     void run(std::size_t sweeps)
     {
         if (!sweeps) return;
         if constexpr (detail::UserTermModel<M>) {
             auto* copy = static_cast<detail::DeviceCopy*>(user_.get());
             model_.attach(copy);
-            records_.clear();
-            user_->run(sweeps, nullptr);
+            std::vector<double> e(sweeps);
+            user_->run_energy(sweeps, e.data());
             model_.mark_device(copy);
+            // the energy only: a user term defines no magnetisation or plaquette
+            records_.assign(sweeps * UMC_OBS_STRIDE, std::numeric_limits<double>::quiet_NaN());
+            for (std::size_t k = 0; k < sweeps; ++k) records_[k * UMC_OBS_STRIDE] = e[k];
         } else {
             model_.attach(chain_.get());
             records_.assign(sweeps * UMC_OBS_STRIDE, 0.0);

@@ -131,7 +131,12 @@ int main(int argc, char** argv)
             metro.run(3);
             double e = 0.0;
             metro.sample(2, [&](const auto& m) {
-                for (std::size_t i = 0; i < m.sites(); ++i) e += 0.5 * m.energy_at(i);
+                double ek = 0.0;
+                for (std::size_t i = 0; i < m.sites(); ++i) ek += 0.5 * m.energy_at(i);
+                // the device-recorded energy of this sweep equals the host sum
+                const double rec = metro.records()[0];
+                if (std::fabs(rec - ek) > 1e-9 * double(m.sites())) throw std::runtime_error("record differs");
+                e += ek;
             });
             std::printf("XY user term: E per site after 5 sweeps %.6f\n", e / 2.0 / double(xy.sites()));
         }
