@@ -17,8 +17,8 @@
 //   Sphere3      -- UniformSphereN<3> (dof/vector.hpp:35-61).
 //
 // Exported with a C ABI for the Python tests and bench.py (ctypes): one-shot
-// runs (um_xy_pair, um_xy_record, um_u1_cells, um_heisenberg_cubic,
-// um_o3_wolff, um_ising_wolff, um_lattice_o3) and persistent sessions (um_session_*) whose
+// runs (um_xy_pair, um_xy_record, um_u1_cells, um_plaquette_u1,
+// um_heisenberg_cubic, um_o3_wolff, um_ising_wolff, um_lattice_o3) and persistent sessions (um_session_*) whose
 // launches bench.py times.
 #include <umc/device.cuh>
 
@@ -215,6 +215,7 @@ static_assert(ModelLike<CubicHeisenberg> && EnergyModel<CubicHeisenberg>);
 static_assert(WolffModel<PairModel<Vec<3>, DotTerm<3>>> && WolffModel<PairModel<Spin, IsingBondTerm>>);
 static_assert(Axis<UpAxis, std::int8_t> && Axis<Sphere3, double>);
 static_assert(WolffModel<LatticePairModel<Vec<3>, DotTerm<3>>> && EnergyModel<LatticePairModel<Vec<3>, DotTerm<3>>>);
+static_assert(ModelLike<LatticeCellModel<Angle, PlaquetteTerm>> && CellEnergyModel<LatticeCellModel<Angle, PlaquetteTerm>>);
 static_assert(CellTerm<CosineTerm, Angle> && CellTerm<PlaquetteTerm, Angle>);
 static_assert(Proposal<AngleShift, double> && Proposal<Sphere3, double>);
 
@@ -282,6 +283,26 @@ int um_u1_cells(const umc_cells* cc, double model_beta, double beta, double widt
 {
     return guarded([&] {
         CellTables t(cc);
+        Buffer<double> field(t.sites());
+        t.upload(field, theta, 1);
+        auto model = t.model<Angle>(field.data(), PlaquetteTerm{model_beta});
+        Metropolis<decltype(model), AngleShift> mc(model, AngleShift{width}, t.classes(), seed, beta);
+        mc.set_sweeps(sweep0);
+        mc.run(n_sweeps);
+        *total_energy = mc.total_energy();
+        t.download(field, theta, 1);
+    });
+}
+
+// U(1) with the user's PlaquetteTerm on a table-free PlaquetteLattice (L even;
+// dim 2 = square_plaquettes, 4 = hypercubic_plaquettes), n_sweeps in one
+// launch; the total energy afterwards.
+int um_plaquette_u1(std::uint32_t L, std::uint32_t dim, double model_beta, double beta, double width,
+                    std::uint64_t seed, std::uint64_t sweep0, std::uint32_t n_sweeps, double* theta,
+                    double* total_energy)
+{
+    return guarded([&] {
+        PlaquetteTables t(L, dim);
         Buffer<double> field(t.sites());
         t.upload(field, theta, 1);
         auto model = t.model<Angle>(field.data(), PlaquetteTerm{model_beta});

@@ -879,6 +879,205 @@ private:
     ClassTable classes_;
 };
 
+// A periodic L^dim plaquette complex whose cells and incidence are computed,
+// not stored: hypercubic_plaquettes (dim 4, lattice/hypercubic.hpp:15-64:
+// link mu L^4 + ((t L + z) L + y) L + x, direction 0 along t) and the library's
+// 2D square_plaquettes (dim 2: link mu L^2 + y L + x, direction 0 along x).
+// Plaquette (a < b) at site c is [U_a(c), U_b(c + a), U_a(c + b), U_b(c)], in
+// the reference's cell order (pairs (a, b) ascending, then sites).  L is even,
+// so the device numbering is the library's closed-form link colouring:
+// class 2 mu + parity(site), position class V/2 + site/2, and every unit step
+// flips a site's parity.
+class PlaquetteLattice
+{
+public:
+    static constexpr std::uint32_t kMaxDim = 4;
+
+    PlaquetteLattice(std::uint32_t l, std::uint32_t d) : L(l), dim(d), div_l(l ? l : 1)
+    {
+        V = 1;
+        for (std::uint32_t k = 0; k < dim; ++k) V *= L;
+    }
+
+    std::uint32_t L, dim, V;
+
+    UMC_HD std::uint32_t sites() const { return dim * V; }
+    UMC_HD std::uint32_t cells() const { return V * dim * (dim - 1) / 2; }
+    // Base-L digit (0 = fastest) that direction mu moves, and its stride.
+    UMC_HD std::uint32_t digit_of(std::uint32_t mu) const { return dim == 2 ? mu : dim - 1 - mu; }
+    UMC_HD std::uint32_t stride_of(std::uint32_t mu) const
+    {
+        std::uint32_t st = 1;
+        for (std::uint32_t k = 0; k < digit_of(mu); ++k) st *= L;
+        return st;
+    }
+    UMC_HD void digits(std::uint32_t s, std::uint32_t* dg) const
+    {
+        for (std::uint32_t k = 0; k < dim; ++k) {
+            const std::uint32_t q = div_l.div(s);
+            dg[k] = s - q * L;
+            s = q;
+        }
+    }
+    UMC_HD std::uint32_t parity(std::uint32_t s) const
+    {
+        std::uint32_t dg[kMaxDim], p = 0;
+        digits(s, dg);
+        for (std::uint32_t k = 0; k < dim; ++k) p += dg[k];
+        return p & 1u;
+    }
+    // Device index of link (mu, site s) whose site parity is par.
+    UMC_HD std::uint32_t link(std::uint32_t mu, std::uint32_t s, std::uint32_t par) const
+    {
+        return (2u * mu + par) * (V / 2) + s / 2;
+    }
+    // Site s moved by one step (+1 or -1) along direction mu; dg are s's digits.
+    UMC_HD std::uint32_t step(std::uint32_t s, const std::uint32_t* dg, std::uint32_t mu, bool up) const
+    {
+        const std::uint32_t st = stride_of(mu), x = dg[digit_of(mu)];
+        if (up) return x + 1 == L ? s - (L - 1) * st : s + st;
+        return x == 0 ? s + (L - 1) * st : s - st;
+    }
+    // Direction and site of device link k.
+    UMC_HD void decode(std::uint32_t k, std::uint32_t& mu, std::uint32_t& s, std::uint32_t& par) const
+    {
+        const std::uint32_t half = V / 2, cls = k / half;
+        mu = cls >> 1;
+        par = cls & 1u;
+        const std::uint32_t s0 = 2u * (k - cls * half);  // s0 and s0 + 1 differ in the fastest digit only
+        s = s0 + ((par + parity(s0)) & 1u);
+    }
+
+private:
+    FastDiv div_l;
+};
+
+namespace detail {
+inline Colouring plaquette_colouring(const PlaquetteLattice& l)
+{
+    if (!(l.dim == 2 || l.dim == 4) || l.L < 2 || l.L % 2)
+        throw std::invalid_argument("PlaquetteLattice: dim 2 or 4 and an even L");
+    if (std::uint64_t(l.V) * l.dim >= (std::uint64_t(1) << 32))
+        throw std::invalid_argument("PlaquetteLattice: links must stay below 2^32");
+    Colouring c;
+    c.count = 2 * l.dim;
+    c.colour.resize(l.sites());
+    c.position.resize(l.sites());
+    for (std::uint32_t mu = 0; mu < l.dim; ++mu)
+        for (std::uint32_t s = 0; s < l.V; ++s) {
+            const std::uint32_t par = l.parity(s);
+            c.colour[mu * l.V + s] = 2 * mu + par;
+            c.position[mu * l.V + s] = l.link(mu, s, par);
+        }
+    return c;
+}
+}  // namespace detail
+
+// CellModel over a PlaquetteLattice: cells and incidence computed from the
+// device index, no tables read.  A ModelLike and CellEnergyModel.
+template <class D, class Term>
+    requires CellTerm<Term, D> && (Term::arity == 4)
+struct LatticeCellModel
+{
+    using dtype = typename D::dtype;
+    using value_type = dtype;
+    using energy_type = typename Term::energy_type;
+    static constexpr std::size_t size = D::size;
+    static constexpr std::size_t arity = 4;
+
+    dtype* field;
+    PlaquetteLattice lattice;
+    Term term;
+
+    UMC_HD std::size_t sites() const { return lattice.sites(); }
+    UMC_HD std::size_t cells() const { return lattice.cells(); }
+    UMC_HD const dtype* data() const { return field; }
+    UMC_HD dtype* data() { return field; }
+    UMC_HD const dtype* at(std::uint32_t k) const { return field + std::size_t(k) * size; }
+
+    // model/cell.hpp:52-56; cell c = pair index * V + site, pairs (a < b) ascending.
+    UMC_HD energy_type cell_energy(std::size_t c) const
+    {
+        const PlaquetteLattice& l = lattice;
+        std::uint32_t pi = std::uint32_t(c / l.V), a = 0, b = 1;
+        for (std::uint32_t q = 0; q < pi; ++q)
+            if (++b == l.dim) b = ++a + 1;
+        const std::uint32_t x = std::uint32_t(c - std::size_t(pi) * l.V);
+        std::uint32_t dg[PlaquetteLattice::kMaxDim];
+        l.digits(x, dg);
+        const std::uint32_t par = l.parity(x);
+        const dtype* ls[4] = {at(l.link(a, x, par)), at(l.link(b, l.step(x, dg, a, true), par ^ 1u)),
+                              at(l.link(a, l.step(x, dg, b, true), par ^ 1u)), at(l.link(b, x, par))};
+        return term.energy(ls);
+    }
+    // model/cell.hpp:64-78 over the 2 (dim - 1) plaquettes that hold link k.
+    UMC_HD energy_type energy_diff_at(std::size_t k, const dtype* p) const
+    {
+        const PlaquetteLattice& l = lattice;
+        std::uint32_t mu, x, par;
+        l.decode(std::uint32_t(k), mu, x, par);
+        std::uint32_t dg[PlaquetteLattice::kMaxDim];
+        l.digits(x, dg);
+        const dtype* old = at(std::uint32_t(k));
+        energy_type d = 0;
+        for (std::uint32_t nu = 0; nu < l.dim; ++nu) {
+            if (nu == mu) continue;
+            const std::uint32_t xm = l.step(x, dg, nu, false);  // x - nu
+            std::uint32_t dm[PlaquetteLattice::kMaxDim];
+            l.digits(xm, dm);
+            if (mu < nu) {
+                // (mu, nu) at x, slot 0; at x - nu, slot 2
+                const dtype* c1[4] = {old, at(l.link(nu, l.step(x, dg, mu, true), par ^ 1u)),
+                                      at(l.link(mu, l.step(x, dg, nu, true), par ^ 1u)), at(l.link(nu, x, par))};
+                d += term.delta(0, old, p, c1);
+                const dtype* c2[4] = {at(l.link(mu, xm, par ^ 1u)), at(l.link(nu, l.step(xm, dm, mu, true), par)), old,
+                                      at(l.link(nu, xm, par ^ 1u))};
+                d += term.delta(2, old, p, c2);
+            } else {
+                // (nu, mu) at x - nu, slot 1; at x, slot 3
+                const dtype* c3[4] = {at(l.link(nu, xm, par ^ 1u)), old, at(l.link(nu, l.step(xm, dm, mu, true), par)),
+                                      at(l.link(mu, xm, par ^ 1u))};
+                d += term.delta(1, old, p, c3);
+                const dtype* c4[4] = {at(l.link(nu, x, par)), at(l.link(mu, l.step(x, dg, nu, true), par ^ 1u)),
+                                      at(l.link(nu, l.step(x, dg, mu, true), par ^ 1u)), old};
+                d += term.delta(3, old, p, c4);
+            }
+        }
+        return d;
+    }
+    UMC_HD void update(std::size_t i, const dtype* p)
+    {
+        for (std::size_t k = 0; k < size; ++k) field[i * size + k] = p[k];
+    }
+};
+
+// The 2 dim colour classes of a PlaquetteLattice and the transfers in the
+// reference's link order; nothing about its cells is stored.
+class PlaquetteTables : public ColourMajor
+{
+public:
+    PlaquetteTables(std::uint32_t L, std::uint32_t dim) : PlaquetteTables(PlaquetteLattice(L, dim)) {}
+    explicit PlaquetteTables(PlaquetteLattice l) : PlaquetteTables(l, detail::plaquette_colouring(l)) {}
+
+    const PlaquetteLattice& lattice() const noexcept { return lattice_; }
+    const ClassTable& classes() const noexcept { return classes_; }
+    std::uint32_t cells() const noexcept { return lattice_.cells(); }
+
+    template <class D, class Term>
+    LatticeCellModel<D, Term> model(typename D::dtype* field, Term term) const
+    {
+        return LatticeCellModel<D, Term>{field, lattice_, term};
+    }
+
+private:
+    PlaquetteTables(PlaquetteLattice l, const detail::Colouring& c)
+        : ColourMajor(c), lattice_(l), classes_(Classes::identity(class_begin()))
+    {}
+
+    PlaquetteLattice lattice_;
+    ClassTable classes_;
+};
+
 // ------------------------------------------------------------------ kernels
 
 namespace detail {

@@ -1,12 +1,17 @@
 // Host-side checks of include/umc/device.cuh that need no GPU: the fast
 // division, RegularLattice's numbering and neighbours against a direct
-// construction, the checkerboard colouring, Classes::from_colours, and the
-// Rng against a sequential reference Pcg32 seeded the keyed way.  Prints "ok".
+// construction, the checkerboard colouring, Classes::from_colours, the Rng
+// against a sequential reference Pcg32 seeded the keyed way, and
+// PlaquetteLattice's numbering, cells and incidence against the library's
+// plaquette complexes.  Prints "ok".
 #include <umc/device.cuh>
 
+#include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstdlib>
 #include <random>
+#include <utility>
 #include <vector>
 
 using namespace umc::gpu::device;
@@ -141,6 +146,103 @@ static void check_rng()
             }
 }
 
+// A cell term that records which links a model hands it (host only).
+struct Angle1
+{
+    using dtype = double;
+    static constexpr std::size_t size = 1;
+};
+static std::vector<std::pair<std::array<std::uint32_t, 4>, std::size_t>> g_seen;
+static const double* g_base = nullptr;
+struct RecordingTerm
+{
+    using dtype = double;
+    using energy_type = double;
+    static constexpr std::size_t arity = 4;
+    __host__ __device__ double energy(const double* const*) const { return 0.0; }
+    __host__ double delta(std::size_t which, const double*, const double*, const double* const* l) const
+    {
+        std::array<std::uint32_t, 4> c{};
+        for (int k = 0; k < 4; ++k) c[k] = std::uint32_t(l[k] - g_base);
+        g_seen.emplace_back(c, which);
+        return 0.0;
+    }
+};
+
+// Records the links cell_energy hands to energy (host only).
+struct CellRecorder
+{
+    using dtype = double;
+    using energy_type = double;
+    static constexpr std::size_t arity = 4;
+    __host__ __device__ double delta(std::size_t, const double*, const double*, const double* const*) const
+    {
+        return 0.0;
+    }
+    __host__ double energy(const double* const* ls) const
+    {
+        std::array<std::uint32_t, 4> cl{};
+        for (int k = 0; k < 4; ++k) cl[k] = std::uint32_t(ls[k] - g_base);
+        g_seen.emplace_back(cl, 0);
+        return 0.0;
+    }
+};
+
+// PlaquetteLattice against the library's plaquette complex: the numbering is
+// the library's link colouring, and every link's computed (cell, slot) list is
+// the library's incidence of that link, relabelled.
+static void check_plaquettes(std::uint32_t L, std::uint32_t dim)
+{
+    umc_cells* cc = nullptr;
+    umc_check(dim == 4 ? umc_cells_hypercubic(L, &cc) : umc_cells_square_plaquettes(L, &cc));
+    const std::uint32_t n = std::uint32_t(umc_cells_sites(cc)), nc = std::uint32_t(umc_cells_count(cc));
+    std::vector<std::uint32_t> colour(n), pos(n), cells(std::size_t(nc) * 4);
+    std::uint32_t ncol = 0;
+    umc_check(umc_cells_colouring(cc, &ncol, colour.data(), pos.data()));
+    umc_check(umc_cells_table(cc, cells.data()));
+    std::vector<std::uint64_t> off(n + 1);
+    umc_check(umc_cells_incidence(cc, off.data(), nullptr, nullptr));
+    std::vector<std::uint32_t> inc_cell(off.back());
+    std::vector<std::uint8_t> inc_which(off.back());
+    umc_check(umc_cells_incidence(cc, off.data(), inc_cell.data(), inc_which.data()));
+    umc_cells_destroy(cc);
+
+    const PlaquetteLattice l(L, dim);
+    const auto c = detail::plaquette_colouring(l);
+    CHECK(l.sites() == n && l.cells() == nc && c.count == ncol);
+    for (std::uint32_t i = 0; i < n; ++i) CHECK(c.position[i] == pos[i]);
+    std::vector<double> field(n, 0.0);
+    g_base = field.data();
+    const LatticeCellModel<Angle1, RecordingTerm> m{field.data(), l, RecordingTerm{}};
+    for (std::uint32_t i = 0; i < n; ++i) {
+        const std::uint32_t k = pos[i];
+        std::uint32_t mu, x, par;
+        l.decode(k, mu, x, par);
+        CHECK(mu * l.V + x == i);
+        g_seen.clear();
+        const double p = 0.0;
+        (void)m.energy_diff_at(k, &p);
+        std::vector<std::pair<std::array<std::uint32_t, 4>, std::size_t>> want;
+        for (std::uint64_t a = off[i]; a < off[i + 1]; ++a) {
+            std::array<std::uint32_t, 4> cl{};
+            for (int q = 0; q < 4; ++q) cl[q] = pos[cells[std::size_t(inc_cell[a]) * 4 + q]];
+            want.emplace_back(cl, inc_which[a]);
+        }
+        std::sort(want.begin(), want.end());
+        std::sort(g_seen.begin(), g_seen.end());
+        CHECK(want == g_seen);
+    }
+    for (std::uint32_t q = 0; q < nc; ++q) {
+        // cell_energy's links, read the same way
+        g_seen.clear();
+        const LatticeCellModel<Angle1, CellRecorder> mc{field.data(), l, CellRecorder{}};
+        (void)mc.cell_energy(q);
+        std::array<std::uint32_t, 4> want{};
+        for (int k = 0; k < 4; ++k) want[k] = pos[cells[std::size_t(q) * 4 + k]];
+        CHECK(g_seen.size() == 1 && g_seen[0].first == want);
+    }
+}
+
 int main()
 {
     check_fast_div();
@@ -150,6 +252,10 @@ int main()
     check_lattice_refusals();
     check_classes();
     check_rng();
+    check_plaquettes(4, 4);
+    check_plaquettes(6, 4);
+    check_plaquettes(8, 2);
+    check_plaquettes(2, 2);
     std::printf("ok\n");
     return 0;
 }

@@ -20,7 +20,7 @@ def test_device_header_host_arithmetic(tmp_path, umc):
         pytest.skip("nvcc not available")
     out = str(tmp_path / "device_host_check")
     cmd = [NVCC, "-std=c++20", "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "--expt-relaxed-constexpr",
-           "-diag-suppress", "177", f"-I{os.path.join(ROOT, 'include')}", SRC, f"-L{PKG}", "-lumc_b200",
+           "-diag-suppress", "177,20011", f"-I{os.path.join(ROOT, 'include')}", SRC, f"-L{PKG}", "-lumc_b200",
            "-Xlinker", f"-rpath,{PKG}", "-o", out]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

@@ -383,3 +383,29 @@ def test_user_xy_energies_recorded_in_the_launch(umc, lib, L):
     _call(lib, lib.um_xy_record(g._h, 1.0, 1.1, 1.0, 12, 3, 6, _p(b), _p(eb)))
     np.testing.assert_array_equal(a, b)
     np.testing.assert_allclose(eb, ea, rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,L,beta,width,sweeps", [("2d", 8, 2.0, 0.5, 3), ("4d", 4, 1.1, 0.7, 2),
+                                                      ("4d", 6, 0.9, 1.0, 2), ("2d", 64, 1.5, 1.0, 2)])
+def test_user_u1_on_table_free_plaquettes(umc, oracle, lib, kind, L, beta, width, sweeps):
+    """LatticeCellModel over PlaquetteLattice (cells and incidence computed
+    from the link index): the same chain as the oracle on the library's
+    plaquette complex, relabelled by the library's link colouring."""
+    lib.um_plaquette_u1.argtypes = [_u32, _u32, _d, _d, _d, _u64, _u64, _u32, _dp, _dp]
+    dim = 2 if kind == "2d" else 4
+    cc = umc.square_plaquettes(L) if kind == "2d" else umc.hypercubic_plaquettes(L)
+    n = cc.sites()
+    _, _, pos = cc.colouring()
+    rcells = pos[cc.table()]
+    inc = oracle.cell_incidence(n, rcells)[1:]
+    th0 = np.random.default_rng(L + dim).uniform(-np.pi, np.pi, n)
+    th = th0.copy()
+    E = _d(0.0)
+    _call(lib, lib.um_plaquette_u1(L, dim, beta, 1.0, width, 5, 0, sweeps, _p(th), C.byref(E)))
+    cm = np.empty(n)
+    cm[pos] = th0
+    t_o, obs_o, _ = oracle.u1_metropolis(rcells, inc, beta, 1.0, width, 1, 5, 0, sweeps, cm)
+    d = np.abs(np.angle(np.exp(1j * (th - t_o[pos]))))
+    assert d.max() < TOL, d.max()
+    assert abs(E.value - obs_o[-1, 0]) < 1e-9 * max(1.0, abs(obs_o[-1, 0]))
