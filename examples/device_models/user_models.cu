@@ -239,6 +239,12 @@ extern "C" {
 
 const char* um_last_error(void) { return g_error.c_str(); }
 
+// 1 when device.cuh's grid barrier gives up on a block that never arrives.
+int um_barrier_selftest(int* timed_out)
+{
+    return guarded([&] { *timed_out = barrier_timeout_selftest() ? 1 : 0; });
+}
+
 // XY PairModel on a library pair graph: n_sweeps through sample(), recording
 // energy_at_sum / 2 after every sweep; theta (sites) in/out.
 int um_xy_pair(const umc_graph* g, double J, double beta, double width, std::uint64_t seed, std::uint64_t sweep0,

@@ -1147,6 +1147,20 @@ __device__ __forceinline__ bool log_below(double u, double log_p)
     return log(u) < log_p;
 }
 
+// The failure path of grid_sync: block 0 waits at a barrier that block 1
+// never reaches, so its bounded wait runs out, sets the status bit and
+// returns false.  status[0] = the status word, status[1] = what grid_sync
+// returned in block 0.
+__global__ void barrier_timeout_probe(Control* ctl, unsigned* status)
+{
+    if (blockIdx.x != 0) return;  // block 1 leaves without arriving
+    const bool ok = grid_sync(ctl);
+    if (threadIdx.x == 0) {
+        status[0] = ld_acquire(&ctl->status);
+        status[1] = ok ? 1u : 0u;
+    }
+}
+
 // No per-sweep observable.
 struct NoObservable
 {};
@@ -1594,6 +1608,23 @@ __global__ void __launch_bounds__(kThreads) wolff_flips_tiled(M m, A axis, doubl
 }  // namespace detail
 
 // ------------------------------------------------------------------ driver
+
+// Runs the barrier's failure path once (a second or two): true when the wait
+// ran out, set the status bit that the drivers turn into an exception, and
+// returned instead of hanging.
+inline bool barrier_timeout_selftest()
+{
+    Buffer<detail::Control> ctl(1);
+    Buffer<unsigned> status(2);
+    cuda_check(cudaMemset(ctl.data(), 0, sizeof(detail::Control)), "reset");
+    cuda_check(cudaMemset(status.data(), 0, 2 * sizeof(unsigned)), "reset");
+    detail::barrier_timeout_probe<<<2, detail::kThreads>>>(ctl.data(), status.data());
+    cuda_check(cudaGetLastError(), "probe launch");
+    cuda_check(cudaDeviceSynchronize(), "probe");
+    unsigned h[2] = {0, 0};
+    cuda_check(cudaMemcpy(h, status.data(), sizeof h, cudaMemcpyDeviceToHost), "probe status");
+    return (h[0] & 1u) != 0u && h[1] == 0u;
+}
 
 // Metropolis (driver.hpp:17-66) for a device model M and proposal Q.  The
 // reference's rng argument becomes a seed: every sweep keys its own streams

@@ -409,3 +409,14 @@ def test_user_u1_on_table_free_plaquettes(umc, oracle, lib, kind, L, beta, width
     d = np.abs(np.angle(np.exp(1j * (th - t_o[pos]))))
     assert d.max() < TOL, d.max()
     assert abs(E.value - obs_o[-1, 0]) < 1e-9 * max(1.0, abs(obs_o[-1, 0]))
+
+
+@pytest.mark.gpu
+def test_device_header_barrier_wait_is_bounded(lib):
+    """A block waiting at device.cuh's grid barrier for a block that never
+    arrives gives up after its bounded wait, sets the status bit and returns
+    (the kernel ends; nothing hangs)."""
+    lib.um_barrier_selftest.argtypes = [C.POINTER(C.c_int)]
+    out = C.c_int(0)
+    _call(lib, lib.um_barrier_selftest(C.byref(out)))
+    assert out.value == 1
