@@ -1264,13 +1264,14 @@ struct EnergyAtOf
 };
 
 // FP64 sum of f(m, x) over x < count: per-block partials, added on the host
-// in block order (deterministic for a given count).
+// in block order (deterministic for a given count).  partial is the caller's
+// reusable buffer (grown here), so a sum allocates nothing after the first.
 template <class M, class F>
-double device_sum(const M& m, std::uint64_t count, F f, cudaStream_t s)
+double device_sum(const M& m, std::uint64_t count, F f, cudaStream_t s, Buffer<double>& partial)
 {
     const std::uint32_t blocks =
         std::uint32_t(std::max<std::uint64_t>(1, std::min<std::uint64_t>(1024, (count + kThreads - 1) / kThreads)));
-    Buffer<double> partial(blocks);
+    if (partial.size() < blocks) partial = Buffer<double>(1024);
     block_sums<M, F><<<blocks, kThreads, 0, s>>>(m, count, f, partial.data());
     cuda_check(cudaGetLastError(), "sum launch");
     std::vector<double> h(blocks);
@@ -1721,7 +1722,8 @@ public:
         const void* k = reinterpret_cast<const void*>(&detail::metropolis_sweeps<M, Q, O>);
         const std::uint32_t grid =
             detail::cooperative_grid(k, (classes_.host().largest() + detail::kThreads - 1) / detail::kThreads);
-        Buffer<double> partial(grid), rec(sweeps);
+        if (rec_partial_.size() < grid) rec_partial_ = Buffer<double>(grid);
+        if (rec_out_.size() < sweeps) rec_out_ = Buffer<double>(std::max<std::size_t>(sweeps, 64));
         cuda_check(cudaMemsetAsync(ctl_.data(), 0, sizeof(detail::Control), stream_), "reset barrier");
         M m = model_;
         Q q = proposal_;
@@ -1733,8 +1735,8 @@ public:
         std::uint32_t n = std::uint32_t(sweeps);
         detail::Control* ctl = ctl_.data();
         std::uint64_t cnt = count;
-        double* part = partial.data();
-        double* out = rec.data();
+        double* part = rec_partial_.data();
+        double* out = rec_out_.data();
         void* args[] = {&m, &q, &order, &begin, &nc, &beta, &seed, &sweep0, &n, &ctl, &obs, &cnt, &part, &out};
         cuda_check(cudaLaunchCooperativeKernel(k, dim3(grid), dim3(detail::kThreads), args, 0, stream_),
                    "Metropolis launch");
@@ -1758,14 +1760,14 @@ public:
     double total_energy() const
         requires CellEnergyModel<M>
     {
-        return detail::device_sum(model_, model_.cells(), detail::CellEnergyOf{}, stream_);
+        return detail::device_sum(model_, model_.cells(), detail::CellEnergyOf{}, stream_, sum_partial_);
     }
     // Sum over sites of energy_at (model.hpp:93-96), FP64; for a pair model
     // every bond appears twice.
     double energy_at_sum() const
         requires EnergyModel<M>
     {
-        return detail::device_sum(model_, model_.sites(), detail::EnergyAtOf{}, stream_);
+        return detail::device_sum(model_, model_.sites(), detail::EnergyAtOf{}, stream_, sum_partial_);
     }
 
     const M& model() const noexcept { return model_; }
@@ -1783,6 +1785,8 @@ private:
     double beta_;
     cudaStream_t stream_;
     Buffer<detail::Control> ctl_;
+    mutable Buffer<double> sum_partial_;  // energy sums' block partials, reused
+    Buffer<double> rec_partial_, rec_out_;  // record()'s partials and records, reused
     std::uint32_t grid_ = 1;
     std::uint64_t sweeps_ = 0;
 };
@@ -1880,12 +1884,12 @@ public:
     double total_energy() const
         requires CellEnergyModel<M>
     {
-        return detail::device_sum(model_, model_.cells(), detail::CellEnergyOf{}, stream_);
+        return detail::device_sum(model_, model_.cells(), detail::CellEnergyOf{}, stream_, sum_partial_);
     }
     double energy_at_sum() const
         requires EnergyModel<M>
     {
-        return detail::device_sum(model_, model_.sites(), detail::EnergyAtOf{}, stream_);
+        return detail::device_sum(model_, model_.sites(), detail::EnergyAtOf{}, stream_, sum_partial_);
     }
 
     const M& model() const noexcept { return model_; }
@@ -1954,6 +1958,7 @@ private:
     const std::uint32_t* site_of_ = nullptr;  // tiled labelling (with tables)
     const std::uint32_t* dev_of_ = nullptr;
     Buffer<uint2> xlist_;
+    mutable Buffer<double> sum_partial_;  // energy sums' block partials, reused
     std::uint32_t grid_ = 1;
     std::uint64_t flips_ = 0;
     double size_sum_ = 0.0;
