@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--workload", choices=["o3", "ising", "su3", "xybatch", "u1batch", "u1learned", "userxy",
-                                          "usero3", "usero3csr", "userwolff"],
+                                          "usero3", "usero3csr", "userwolff", "useru1", "useru1tables"],
                    default="o3",
                    help="o3: the headline configuration; ising / su3 / xybatch / userxy / usero3 / usero3csr: "
                         "secondary roofline runs (user*: user-written models through include/umc/device.cuh); "
@@ -982,8 +982,62 @@ class UserIsingWolff(_UserSession):
                           f"FixedAxis>, stock driver, 200 warm-up flips), {sec:.1f} s"}
 
 
+class UserU1(_UserSession):
+    """A user-written U(1) plaquette cell term (PlaquetteTerm, FP64: beta (1 -
+    cos(t0 + t1 - t2 - t3))) with AngleShift 0.7 on L^4 hypercubic plaquettes,
+    model beta 1.1, random start; step = one sweep (8 colour classes, one
+    launch of the generic device kernel).  useru1: the table-free
+    PlaquetteLattice (a link's plaquettes computed); useru1tables: the same
+    on the library's cell and incidence tables (CellTables)."""
+
+    unit = "link-updates/s"
+    dtype = "f64"
+
+    def __init__(self, umc, args, rank, local, tables=False):
+        import numpy as np
+
+        self.tables = tables
+        self.name = "useru1tables" if tables else "useru1"
+        self.L = args.L if args.L != L_DEFAULT else 48
+        self.n = 4 * self.L ** 4
+        theta = np.random.default_rng(21 + rank).uniform(-np.pi, np.pi, self.n)
+        self._open(umc, 4 if tables else 5, None, (self.L, 0, 0), 1.1, 1.0, 0.7, 1 + rank, theta)
+        self.flush = self.n * 8 < (256 << 20)
+
+    def describe(self):
+        where = "hypercubic_plaquettes tables (CellTables)" if self.tables else "PlaquetteLattice (no tables)"
+        return (f"user-written U(1) plaquette term (FP64, examples/device_models) on {self.L}^4, {where}, model "
+                f"beta 1.1, AngleShift 0.7, random start; step = 1 Metropolis sweep (one launch)")
+
+    def bytes_per_launch(self, kind):
+        # per (direction, parity) pass: read 4.5 V links and write V/2 (8 B
+        # each) for V/2 link-updates = 80 B per link-update; the tables add
+        # the offset 8, six (cell, slot) entries 30 and six cells' links 96
+        return (214.0 if self.tables else 80.0) * self.n
+
+    def cpu(self, seconds):
+        from oracle.oracle import Reference, have_reference
+
+        if not have_reference():
+            return None
+        r = Reference()
+        threads = cpu_threads()
+        su, sec = r.bench_u1_cells(8, 1.1, 1.0, 0.7, 1, 2, 1, 1)
+        sweeps = max(2, int(seconds * 2 / max(sec, 1e-4)))
+        su, sec = r.bench_u1_cells(8, 1.1, 1.0, 0.7, 1, sweeps, threads, 1)
+        return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                "sample": f"{sweeps} sweeps x {threads} independent 8^4 chains (reference CellModel<U1Dof, "
+                          f"U1PlaquetteTerm, CellComplex<4>> + U1Shift, stock driver, FP64), {sec:.1f} s"}
+
+
+class UserU1Tables(UserU1):
+    def __init__(self, umc, args, rank, local):
+        super().__init__(umc, args, rank, local, tables=True)
+
+
 WORKLOADS = {"o3": O3Hybrid, "ising": IsingSweep, "su3": SU3Sweep, "xybatch": XYBatch, "u1batch": U1LearnedSweep,
-             "userxy": UserXY, "usero3": UserO3, "usero3csr": UserO3Csr, "userwolff": UserIsingWolff}
+             "userxy": UserXY, "usero3": UserO3, "usero3csr": UserO3Csr, "userwolff": UserIsingWolff,
+             "useru1": UserU1, "useru1tables": UserU1Tables}
 
 
 def run_learned(args):

@@ -417,7 +417,9 @@ int um_lattice_o3(std::uint32_t Lx, std::uint32_t Ly, std::uint32_t Lz, double J
 //   0  XY (CosineTerm + AngleShift, FP64) on a library pair graph's tables;
 //   1  O(3) (DotTerm<3, float> + SphereF, FP32) on a table-free RegularLattice;
 //   2  the same O(3) model on the lattice's CSR tables (PairTables);
-//   3  Ising Wolff (IsingBondTerm + UpAxis) on a library pair graph's tables.
+//   3  Ising Wolff (IsingBondTerm + UpAxis) on a library pair graph's tables;
+//   4  U(1) (PlaquetteTerm + AngleShift, FP64) on hypercubic_plaquettes(L) tables;
+//   5  the same on the table-free PlaquetteLattice(L, 4).
 namespace {
 
 template <class T, std::size_t N>
@@ -528,7 +530,13 @@ struct Session final : SessionBase
     void get_field(void* host) override { tables.download(field, static_cast<T*>(host), D::size, stream); }
     void launch(std::uint64_t sweeps) override { mc.enqueue(sweeps); }
     void check() override { mc.check(); }
-    double energy() override { return 0.5 * mc.energy_at_sum(); }
+    double energy() override
+    {
+        if constexpr (requires { mc.total_energy(); })
+            return mc.total_energy();  // a cell model: the sum over cells
+        else
+            return 0.5 * mc.energy_at_sum();  // a pair model: every bond at both ends
+    }
     std::uint64_t sweeps() const override { return mc.sweeps(); }
     std::uint32_t grid() const override { return mc.grid(); }
 
@@ -566,6 +574,8 @@ struct IsingWolffSession final : SessionBase
 };
 
 using XYSession = Session<PairTables, Angle, CosineTerm, AngleShift>;
+using U1CellSession = Session<CellTables, Angle, PlaquetteTerm, AngleShift>;
+using U1PlaquetteSession = Session<PlaquetteTables, Angle, PlaquetteTerm, AngleShift>;
 using O3LatticeSession = Session<LatticeTables, VecT<float, 3>, DotTermT<float, 3>, SphereF>;
 using O3TableSession = Session<PairTables, VecT<float, 3>, DotTermT<float, 3>, SphereF>;
 
@@ -601,6 +611,20 @@ int um_session_create(int kind, const umc_graph* g, std::uint32_t Lx, std::uint3
                 new O3TableSession(lg.g, DotTermT<float, 3>{float(J)}, SphereF{}, beta, seed));
         } else if (kind == 3) {
             *out = static_cast<SessionBase*>(new IsingWolffSession(g, std::int32_t(J), beta, seed));
+        } else if (kind == 4 || kind == 5) {
+            // U(1) plaquettes on L^4 (Lx = L): J is the model's beta, width the shift
+            umc_cells* cc = nullptr;
+            umc_check(umc_cells_hypercubic(Lx, &cc));
+            struct Free
+            {
+                umc_cells* c;
+                ~Free() { umc_cells_destroy(c); }
+            } guard{cc};
+            if (kind == 4)
+                *out = static_cast<SessionBase*>(new U1CellSession(cc, PlaquetteTerm{J}, AngleShift{width}, beta, seed));
+            else
+                *out = static_cast<SessionBase*>(
+                    new U1PlaquetteSession(PlaquetteLattice(Lx, 4), PlaquetteTerm{J}, AngleShift{width}, beta, seed));
         } else {
             throw std::invalid_argument("unknown session kind");
         }

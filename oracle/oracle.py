@@ -432,6 +432,7 @@ class Reference:
         self._bench_xy = L.fn("bench_xy", _int, _u64, _f64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._bench_pair_o3 = L.fn("bench_pair_o3", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._bench_ising_wolff = L.fn("bench_ising_wolff", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
+        self._bench_u1_cells = L.fn("bench_u1_cells", _int, _u64, _f64, _f64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
 
     def pcg32_draws(self, seed, stream, n):
         out = np.zeros(n, np.uint32)
@@ -653,6 +654,19 @@ def _bench_ising_wolff(self, L, beta, warmup, flips, threads, seed=1):
 
 
 Reference.bench_ising_wolff = _bench_ising_wolff
+
+
+def _bench_u1_cells(self, L, model_beta, beta, width, warmup, sweeps, threads, seed=1):
+    """Reference CellModel<U1Dof, U1PlaquetteTerm, CellComplex<4>> Metropolis on
+    L^4: (link-updates, seconds of the slowest thread)."""
+    su = C.c_double()
+    sec = C.c_double()
+    st = self._bench_u1_cells(L, model_beta, beta, width, warmup, sweeps, threads, seed, C.byref(su), C.byref(sec))
+    assert st == 0, st
+    return su.value, sec.value
+
+
+Reference.bench_u1_cells = _bench_u1_cells
 
 
 def have_reference() -> bool:

@@ -975,6 +975,46 @@ extern "C" int ref_bench_ising_wolff(std::uint64_t L, double beta, std::uint64_t
     }
 }
 
+// Times the reference's generic cell model: CellModel<U1Dof, U1PlaquetteTerm,
+// CellComplex<4>> (model/cell.hpp, term/plaquette.hpp) on hypercubic_plaquettes(L)
+// with U1Shift{width} and a plain Pcg32, one chain per thread, uniform random
+// start; site_updates = links x sweeps x threads.
+extern "C" int ref_bench_u1_cells(std::uint64_t L, double model_beta, double beta, double width, std::uint64_t warmup,
+                                  std::uint64_t sweeps, std::uint32_t threads, std::uint64_t seed,
+                                  double* site_updates, double* seconds)
+{
+    try {
+        using CM = CellModel<U1Dof, U1PlaquetteTerm, CellComplex<4>>;
+        std::vector<double> secs(threads, 0.0);
+        std::vector<std::thread> pool;
+        std::size_t links = 0;
+        for (std::uint32_t t = 0; t < threads; ++t)
+            pool.emplace_back([&, t] {
+                CM model(hypercubic_plaquettes(L), U1PlaquetteTerm{model_beta});
+                Pcg32 init(seed + t, 9);
+                for (std::size_t i = 0; i < model.sites(); ++i) {
+                    const U1Link l{6.283185307179586 * init.uni() - 3.141592653589793};
+                    model.update(i, &l);
+                }
+                if (t == 0) links = model.sites();
+                Metropolis<CM, U1Shift, Pcg32> mc(model, U1Shift{width}, Pcg32(seed + t, 1), beta);
+                mc.run(warmup);
+                const auto t0 = std::chrono::steady_clock::now();
+                mc.run(sweeps);
+                const auto t1 = std::chrono::steady_clock::now();
+                secs[t] = std::chrono::duration<double>(t1 - t0).count();
+            });
+        for (auto& th : pool) th.join();
+        double worst = 0.0;
+        for (double x : secs) worst = x > worst ? x : worst;
+        *site_updates = double(threads) * double(links) * double(sweeps);
+        *seconds = worst;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
 // Times the reference's stock XY model on angles: PairModel<U1Dof, -J cos> on an
 // L x L square_lattice with U1Shift{width} and a plain Pcg32, one chain per
 // thread, uniform random start.
