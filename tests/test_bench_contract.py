@@ -31,7 +31,8 @@ def test_reference_arm_prints_one_contract_line():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("workload,L", [("userxy", 256), ("usero3", 32), ("usero3csr", 32), ("userwolff", 128)])
+@pytest.mark.parametrize("workload,L", [("userxy", 256), ("usero3", 32), ("usero3csr", 32), ("userwolff", 128),
+                                        ("useru1", 8), ("useru1tables", 8)])
 def test_user_model_bench_lines_keep_the_contract(workload, L):
     """The user-model workloads (generic device kernels of include/umc/device.cuh)
     print one JSON line with the contract's fields, a roofline of their own
@@ -43,7 +44,7 @@ def test_user_model_bench_lines_keep_the_contract(workload, L):
     lines = [ln for ln in r.stdout.splitlines() if ln.strip().startswith("{")]
     assert len(lines) == 1, r.stdout
     d = json.loads(lines[0])
-    assert d["value"] > 0 and d["steps"] == 5 and d["warmup"] == 3 and d["unit"] == "site-updates/s"
+    assert d["value"] > 0 and d["steps"] == 5 and d["warmup"] == 3 and d["unit"] in ("site-updates/s", "link-updates/s")
     assert d["roofline"]["kernel"] in ("metropolis_sweeps", "wolff_flips") and d["roofline"]["achieved"] > 0
     assert d["gpu_launches"] >= 5 and d["e2e"]["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] > 0
     assert d["config"]["L"] == L and "clocks" in d
