@@ -14,10 +14,14 @@
 //                   cubic O(3) model whose neighbours come from the site index,
 //                   with no bond table at all;
 //   AngleShift   -- U1Shift (dof/u1.hpp:35-50): remainder(t + w (2u - 1), 2 pi);
-//   Sphere3      -- UniformSphereN<3> (dof/vector.hpp:35-61).
+//   Sphere3      -- UniformSphereN<3> (dof/vector.hpp:35-61);
+//   SU2PlaquetteTerm + SU2Step -- a gauge group the library has no kernel for
+//                   in this form: SU(2) links as unit quaternions (a user link
+//                   type), the Wilson plaquette term and a symmetric left
+//                   multiplication proposal.
 //
 // Exported with a C ABI for the Python tests and bench.py (ctypes): one-shot
-// runs (um_xy_pair, um_xy_record, um_u1_cells, um_plaquette_u1,
+// runs (um_xy_pair, um_xy_record, um_u1_cells, um_plaquette_u1, um_su2_2d,
 // um_heisenberg_cubic, um_o3_wolff, um_ising_wolff, um_lattice_o3) and persistent sessions (um_session_*) whose
 // launches bench.py times.
 #include <umc/device.cuh>
@@ -138,6 +142,75 @@ struct PlaquetteTerm
     }
 };
 
+// SU(2) links as unit quaternions: U = a0 + i (a1 s1 + a2 s2 + a3 s3), s_k
+// the Pauli matrices, so (1/2) Tr U = a0, U^dagger = (a0, -a), and
+// U V = (a0 b0 - a.b, a0 b + b0 a - a x b).
+struct Quat
+{
+    double a[4];
+};
+struct SU2Dof
+{
+    using dtype = Quat;
+    static constexpr std::size_t size = 1;
+};
+UMC_HD Quat qmul(const Quat& x, const Quat& y)
+{
+    const double* a = x.a;
+    const double* b = y.a;
+    return Quat{{a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3],
+                 a[0] * b[1] + b[0] * a[1] - (a[2] * b[3] - a[3] * b[2]),
+                 a[0] * b[2] + b[0] * a[2] - (a[3] * b[1] - a[1] * b[3]),
+                 a[0] * b[3] + b[0] * a[3] - (a[1] * b[2] - a[2] * b[1])}};
+}
+UMC_HD Quat qdag(const Quat& x) { return Quat{{x.a[0], -x.a[1], -x.a[2], -x.a[3]}}; }
+
+// Wilson plaquette term beta (1 - (1/2) Tr U0 U1 U2^dagger U3^dagger) for SU(2),
+// a user cell term of arity 4 with a user link type.
+struct SU2PlaquetteTerm
+{
+    using dtype = Quat;
+    using energy_type = double;
+    static constexpr std::size_t arity = 4;
+    double beta;
+
+    UMC_HD static double half_trace(const Quat& u0, const Quat& u1, const Quat& u2, const Quat& u3)
+    {
+        return qmul(qmul(u0, u1), qmul(qdag(u3), qdag(u2))).a[0];  // U0 U1 (U3 U2)^dagger
+    }
+    UMC_HD double energy(const Quat* const* l) const { return beta * (1.0 - half_trace(*l[0], *l[1], *l[2], *l[3])); }
+    UMC_HD double delta(std::size_t which, const Quat*, const Quat* nw, const Quat* const* l) const
+    {
+        Quat u[4] = {*l[0], *l[1], *l[2], *l[3]};
+        const double before = half_trace(u[0], u[1], u[2], u[3]);
+        u[which] = *nw;
+        return beta * (before - half_trace(u[0], u[1], u[2], u[3]));
+    }
+};
+
+// U -> R U with R = (cos t, sin t n), t uniform in [-w, w], n uniform on the
+// sphere: R and R^dagger are equally likely, so the proposal is symmetric.
+struct SU2Step
+{
+    double width;
+
+    template <class R>
+    UMC_HD void sample(const Quat* cur, R& rng, Quat* out) const
+    {
+        const double t = width * (2.0 * rng.uni() - 1.0);
+        const double z = 2.0 * rng.uni() - 1.0;
+        const double rr = sqrt(fmax(0.0, 1.0 - z * z));
+        const double phi = 2.0 * kPi * rng.uni();
+        const double st = sin(t);
+        const Quat rot{{cos(t), st * rr * cos(phi), st * rr * sin(phi), st * z}};
+        Quat u = qmul(rot, *cur);
+        const double inv = 1.0 / sqrt(u.a[0] * u.a[0] + u.a[1] * u.a[1] + u.a[2] * u.a[2] + u.a[3] * u.a[3]);
+        for (double& c : u.a) c *= inv;  // keep |U| = 1 against rounding drift
+        *out = u;
+    }
+    UMC_HD double log_ratio(const Quat*, const Quat*) const { return 0.0; }
+};
+
 struct AngleShift
 {
     double width;
@@ -216,6 +289,7 @@ static_assert(WolffModel<PairModel<Vec<3>, DotTerm<3>>> && WolffModel<PairModel<
 static_assert(Axis<UpAxis, std::int8_t> && Axis<Sphere3, double>);
 static_assert(WolffModel<LatticePairModel<Vec<3>, DotTerm<3>>> && EnergyModel<LatticePairModel<Vec<3>, DotTerm<3>>>);
 static_assert(ModelLike<LatticeCellModel<Angle, PlaquetteTerm>> && CellEnergyModel<LatticeCellModel<Angle, PlaquetteTerm>>);
+static_assert(CellTerm<SU2PlaquetteTerm, SU2Dof> && Proposal<SU2Step, Quat>);
 static_assert(CellTerm<CosineTerm, Angle> && CellTerm<PlaquetteTerm, Angle>);
 static_assert(Proposal<AngleShift, double> && Proposal<Sphere3, double>);
 
@@ -317,6 +391,25 @@ int um_plaquette_u1(std::uint32_t L, std::uint32_t dim, double model_beta, doubl
         mc.run(n_sweeps);
         *total_energy = mc.total_energy();
         t.download(field, theta, 1);
+    });
+}
+
+// 2D SU(2) with the user's quaternion links on the table-free L x L
+// plaquettes, cold start: `warmup` sweeps, then n_sweeps recorded in one
+// launch; plaq[s] = the mean (1/2) Tr U_p after sweep s.
+int um_su2_2d(std::uint32_t L, double beta, double width, std::uint64_t seed, std::uint32_t warmup,
+              std::uint32_t n_sweeps, double* plaq)
+{
+    return guarded([&] {
+        PlaquetteTables t(L, 2);
+        Buffer<Quat> field(t.sites());
+        const std::vector<Quat> cold(t.sites(), Quat{{1.0, 0.0, 0.0, 0.0}});
+        t.upload(field, cold.data(), 1);
+        auto model = t.model<SU2Dof>(field.data(), SU2PlaquetteTerm{beta});
+        Metropolis<decltype(model), SU2Step> mc(model, SU2Step{width}, t.classes(), seed, 1.0);
+        mc.run(warmup);
+        mc.record_energy(n_sweeps, plaq);
+        for (std::uint32_t k = 0; k < n_sweeps; ++k) plaq[k] = 1.0 - plaq[k] / (beta * double(t.cells()));
     });
 }
 

@@ -420,3 +420,23 @@ def test_device_header_barrier_wait_is_bounded(lib):
     out = C.c_int(0)
     _call(lib, lib.um_barrier_selftest(C.byref(out)))
     assert out.value == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("beta", [2.0, 4.0])
+def test_user_su2_quaternion_gauge_model_matches_the_exact_2d_plaquette(lib, beta):
+    """A gauge group given entirely by the user (SU(2) as unit quaternions, a
+    Wilson plaquette term and a symmetric left-multiplication proposal) on the
+    table-free 16 x 16 plaquettes: the mean plaquette recorded in the launch
+    equals 2D lattice gauge theory's exact <(1/2) Tr U_p> = I_2(beta) / I_1(beta)
+    within five binned standard errors."""
+    from scipy.special import iv
+
+    lib.um_su2_2d.argtypes = [_u32, _d, _d, _u64, _u32, _u32, _dp]
+    n = 6000
+    plaq = np.zeros(n)
+    _call(lib, lib.um_su2_2d(16, beta, 1.0, 17, 500, n, _p(plaq)))
+    exact = iv(2, beta) / iv(1, beta)
+    bins = plaq[: n - n % 50].reshape(-1, 50).mean(axis=1)
+    err = bins.std(ddof=1) / np.sqrt(len(bins))
+    assert abs(plaq.mean() - exact) < 5 * err + 1e-4, (plaq.mean(), exact, err)
