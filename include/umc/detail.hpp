@@ -79,6 +79,9 @@ struct UserRunner : DeviceCopy
     // n Metropolis sweeps with the total energy after each (observed on the
     // device); a Wolff runner has none.
     virtual void run_energy(std::size_t n, double* energy) = 0;
+    // One Wolff sweep (flips until the flipped sites reach the lattice) in as
+    // few launches as possible; adds its flips and flipped sites.
+    virtual void wolff_sweep(std::size_t& flips, double& sites) = 0;
 };
 
 // A model's field on the host as scalars HS in the reference's data() layout,

@@ -1853,14 +1853,17 @@ public:
         }
     }
 
-    // Flips until the flipped sites add up to the lattice (driver.hpp:163-173).
-    void sweep()
+    // Flips until the flipped sites add up to the lattice (driver.hpp:163-173);
+    // returns the sites flipped.
+    std::uint64_t sweep()
     {
-        std::uint64_t need = model_.sites();
+        std::uint64_t need = model_.sites(), total = 0;
         while (need > 0) {
             const std::uint64_t got = launch(kCapacity, need, nullptr);
+            total += got;
             need = got >= need ? 0 : need - got;
         }
+        return total;
     }
 
     // n sweeps (driver.hpp:175-180).

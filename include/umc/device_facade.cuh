@@ -70,6 +70,7 @@ public:
         : UserField<M>(m), mc_(this->view(m), q, this->tables_.classes(), key, beta)
     {}
     void run(std::size_t n, std::uint64_t*) override { mc_.run(n); }
+    void wolff_sweep(std::size_t&, double&) override { throw std::logic_error("a Metropolis runner has no Wolff sweep"); }
     // E after each sweep: half the sum of energy_at for a pair model (every
     // bond counted at both ends), the sum of cell_energy for a cell model.
     void run_energy(std::size_t n, double* energy) override
@@ -92,6 +93,12 @@ public:
     {}
     void run(std::size_t n, std::uint64_t* sizes) override { w_.flips(n, sizes); }
     void run_energy(std::size_t, double*) override { throw std::logic_error("Wolff records no energies"); }
+    void wolff_sweep(std::size_t& flips, double& sites) override
+    {
+        const std::uint64_t f0 = w_.flips_done();
+        sites += double(w_.sweep());
+        flips += std::size_t(w_.flips_done() - f0);
+    }
 
 private:
     device::Wolff<typename UserDevice<M>::View, A> w_;

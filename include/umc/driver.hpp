@@ -218,13 +218,25 @@ public:
         return std::size_t(size);
     }
 
-    // Flips until the flipped sites add up to one lattice.
+    // Flips until the flipped sites add up to one lattice.  A user-written
+    // term does this in the device Wolff's own launch, which stops there.
     void sweep()
     {
-        std::size_t touched = 0;
-        do {
-            touched += flip();
-        } while (touched < model_.sites());
+        if constexpr (detail::UserTermModel<M>) {
+            auto* copy = static_cast<detail::DeviceCopy*>(user_.get());
+            model_.attach(copy);
+            std::size_t f = 0;
+            double s = 0.0;
+            user_->wolff_sweep(f, s);
+            model_.mark_device(copy);
+            n_flips_ += f;
+            size_sum_ += s;
+        } else {
+            std::size_t touched = 0;
+            do {
+                touched += flip();
+            } while (touched < model_.sites());
+        }
     }
 
     void run(std::size_t sweeps)

@@ -5,9 +5,10 @@
 // over square_lattice / hypercubic_plaquettes, Metropolis and Wolff with the
 // reference's proposals and axes, Pcg32 for the keys, data() to read back.
 //
-// Writes to argv[1], in order: the XY start and end angles, the Ising start
-// and end spins and the 12 cluster sizes, the U(1) start and end angles, the
-// O(3) start and end spins.
+// Writes to argv[1], in order: the XY start and end angles; the Ising start
+// spins, the spins after 12 flips, their cluster sizes, the spins after one
+// more Wolff sweep and the mean cluster size; the U(1) start and end angles;
+// the O(3) start and end spins.
 #include <umc/umc.hpp>
 
 #include <cmath>
@@ -152,15 +153,22 @@ int main(int argc, char** argv)
         }
         std::vector<IsingSpin> s0(ising.data(), ising.data() + ising.sites());
         std::vector<std::uint64_t> sizes(12);
+        std::vector<IsingSpin> s1;
+        double mean_after_sweep = 0.0;
         {
             Wolff wolf(ising, FixedAxis{}, Pcg32(13, 0), 0.44);
             wolf.flips(12, sizes.data());
             std::printf("Ising user term: mean cluster %.2f\n", wolf.mean_cluster_size());
+            s1.assign(ising.data(), ising.data() + ising.sites());
+            wolf.sweep();  // flips 12, 13, ... until the flipped sites cover the lattice
+            mean_after_sweep = wolf.mean_cluster_size();
         }
-        std::vector<IsingSpin> s1(ising.data(), ising.data() + ising.sites());
+        std::vector<IsingSpin> s2(ising.data(), ising.data() + ising.sites());
         put(out, s0.data(), s0.size());
         put(out, s1.data(), s1.size());
         put(out, sizes.data(), sizes.size());
+        put(out, s2.data(), s2.size());
+        put(out, &mean_after_sweep, 1);
 
         // U(1): CellModel<U1Dof, user cell term, CellComplex<4>> on the 4^4 plaquettes, 2 sweeps
         CellModel<U1Dof, MyPlaquetteTerm, CellComplex<4>> u1(hypercubic_plaquettes(4), MyPlaquetteTerm{1.3});

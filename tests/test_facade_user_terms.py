@@ -3,7 +3,7 @@ built with nvcc: the facade's Metropolis and Wolff run the user's terms on the
 device through umc/device_facade.cuh.  The program compiles here; without a
 GPU it fails loudly; on the GPU its fields equal the oracle's:
 - XY angles, 5 sweeps, to 1e-9;
-- Ising under Wolff, spins and cluster sizes bit for bit;
+- Ising under Wolff, spins and cluster sizes bit for bit, flips and a sweep;
 - U(1) plaquettes, 2 sweeps, to 1e-9;
 - O(3) with LocalRotation, 2 sweeps, to 1e-9.
 The oracle runs on the colour-major device numbering with the same keys."""
@@ -75,11 +75,21 @@ def test_user_term_program_matches_the_oracle(program, umc, oracle, tmp_path):
     n = 24 * 24
     pos, doff, dbonds, key = device_csr(g)
     s0, s1, sizes = take(np.int8, n), take(np.int8, n), take(np.uint64, 12)
+    s2, mean_after = take(np.int8, n), take(np.float64, 1)[0]
     cm = np.empty(n, np.int8)
     cm[pos] = s0
     s_o, sz_o, _, _ = oracle.ising_wolff(doff, dbonds, key, 1, 0.44, 13, 0, 12, cm)
     np.testing.assert_array_equal(sizes, sz_o)
     np.testing.assert_array_equal(s1, s_o[pos])
+    # Wolff::sweep: flips 12, 13, ... until the flipped sites reach the lattice
+    all_sizes, touched, f, cur = list(sz_o), 0, 12, s_o
+    while touched < n:
+        cur, sz, _, _ = oracle.ising_wolff(doff, dbonds, key, 1, 0.44, 13, f, 1, cur)
+        touched += int(sz[0])
+        all_sizes.append(int(sz[0]))
+        f += 1
+    np.testing.assert_array_equal(s2, cur[pos])
+    assert abs(mean_after - np.mean(all_sizes)) < 1e-9
 
     # U(1): 2 sweeps on the 4^4 plaquettes, keys 9
     cc = umc.hypercubic_plaquettes(4)
