@@ -125,7 +125,8 @@ def device_csr(g):
     key = np.arange(len(dbonds), dtype=np.uint32)
     for a in np.nonzero(rows > dbonds)[0]:
         i, j = rows[a], dbonds[a]
+        # a duplicated bond: the m-th copy in i's row pairs with the m-th in j's
+        m = int(np.count_nonzero(dbonds[doff[i]:a] == j))
         back = doff[j] + np.nonzero(dbonds[doff[j]:doff[j + 1]] == i)[0]
-        assert len(back) == 1
-        key[a] = back[0]
+        key[a] = back[m]
     return pos, doff, dbonds, key

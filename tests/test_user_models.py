@@ -440,3 +440,31 @@ def test_user_su2_quaternion_gauge_model_matches_the_exact_2d_plaquette(lib, bet
     bins = plaq[: n - n % 50].reshape(-1, 50).mean(axis=1)
     err = bins.std(ddof=1) / np.sqrt(len(bins))
     assert abs(plaq.mean() - exact) < 5 * err + 1e-4, (plaq.mean(), exact, err)
+
+
+@pytest.mark.gpu
+def test_user_xy_on_a_random_graph(umc, oracle, lib):
+    """The generic kernel on an irregular, non-bipartite PairGraph (random
+    edges, duplicates kept): the library's greedy colouring gives more than
+    two classes, and every sweep still equals the oracle's on the relabelled
+    graph."""
+    rng = np.random.default_rng(31)
+    n = 600
+    ei = rng.integers(0, n, 2000)
+    ej = (ei + rng.integers(1, n, 2000)) % n  # no self-loops
+    g = umc.PairGraph(n, np.stack([ei, ej], axis=1).astype(np.uint32))
+    ncol, _, pos = g.colouring()
+    assert ncol > 2
+    _, doff, dbonds, _ = device_csr(g)
+    off_s, bonds_s = g.csr()
+    th = rng.uniform(-np.pi, np.pi, n)
+    for sweep in range(3):
+        cm = np.empty(n)
+        cm[pos] = th
+        t_o, obs_o, margin = oracle.xy_metropolis(doff, dbonds, 1.0, 0.8, 1.2, 9, sweep, 1, cm)
+        th, en, _ = xy_run(lib, g, th, 0.8, 1.2, 9, sweep, 1)
+        d = np.abs(np.angle(np.exp(1j * (th - t_o[pos]))))
+        near = np.nonzero(np.abs(margin[pos]) < MARGIN)[0]
+        bad = set(np.nonzero(d > TOL)[0].tolist())
+        assert bad <= set(near.tolist()) | _neighbours(off_s, bonds_s, near), sorted(bad)[:10]
+        assert abs(en[0] - obs_o[0, 0]) < 1e-9 * n
