@@ -468,3 +468,28 @@ def test_user_xy_on_a_random_graph(umc, oracle, lib):
         bad = set(np.nonzero(d > TOL)[0].tolist())
         assert bad <= set(near.tolist()) | _neighbours(off_s, bonds_s, near), sorted(bad)[:10]
         assert abs(en[0] - obs_o[0, 0]) < 1e-9 * n
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tiled", [0, 1])
+def test_user_ising_wolff_on_a_random_graph(umc, oracle, lib, tiled):
+    """The device Wolff on an irregular graph with duplicate edges (a bond
+    listed twice is tested twice, as the reference's rows hold it twice), with
+    and without the shared-memory tiles: spins and cluster sizes bit for bit
+    against the oracle over 15 flips."""
+    lib.um_ising_wolff.argtypes = [_vp, C.c_int32, _d, _u64, _u64, _u32, _vp, _vp, C.c_int]
+    rng = np.random.default_rng(44)
+    n = 9000  # three tiles of 4,096 reference sites
+    ei = rng.integers(0, n, 20000)
+    ej = (ei + rng.integers(1, 40, 20000)) % n  # mostly local bonds, some repeated
+    g = umc.PairGraph(n, np.stack([ei, ej], axis=1).astype(np.uint32))
+    pos, doff, dbonds, key = device_csr(g)
+    s0 = np.where(rng.random(n) < 0.5, 1, -1).astype(np.int8)
+    s = s0.copy()
+    sizes = np.zeros(15, np.uint64)
+    _call(lib, lib.um_ising_wolff(g._h, 1, 0.35, 3, 0, 15, s.ctypes.data, sizes.ctypes.data, tiled))
+    cm = np.empty(n, np.int8)
+    cm[pos] = s0
+    s_o, sz_o, _, _ = oracle.ising_wolff(doff, dbonds, key, 1, 0.35, 3, 0, 15, cm)
+    np.testing.assert_array_equal(sizes, sz_o)
+    np.testing.assert_array_equal(s, s_o[pos])
