@@ -493,3 +493,50 @@ def test_user_ising_wolff_on_a_random_graph(umc, oracle, lib, tiled):
     s_o, sz_o, _, _ = oracle.ising_wolff(doff, dbonds, key, 1, 0.35, 3, 0, 15, cm)
     np.testing.assert_array_equal(sizes, sz_o)
     np.testing.assert_array_equal(s, s_o[pos])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", [1, 2])
+def test_fp32_user_o3_term_per_sweep(umc, oracle, lib, kind):
+    """The bench's FP32 user model (DotTermT<float, 3>, FP32 sphere proposal;
+    kind 1 on the table-free lattice, kind 2 on CSR tables) against the FP64
+    oracle, one sweep at a time from the same state: spins agree to 1e-5
+    except at decisions within 1e-3 of their threshold and the sites next to
+    them, as for the engine's FP32 chains."""
+    vp = C.c_void_p
+    lib.um_session_create.argtypes = [C.c_int, vp, _u32, _u32, _u32, _d, _d, _d, _u64, C.POINTER(vp)]
+    lib.um_session_destroy.argtypes = [vp]
+    lib.um_session_set_field.argtypes = [vp, vp]
+    lib.um_session_get_field.argtypes = [vp, vp]
+    lib.um_session_enqueue.argtypes = [vp, _u64]
+    lib.um_session_stats.argtypes = [vp, C.POINTER(_u64), C.POINTER(_d), C.c_int]
+    L, n = 8, 512
+    pos, off, bonds, _ = lattice_csr(L, L, L)
+    rows = {int(k): set(bonds[off[k]:off[k + 1]].tolist()) for k in range(n)}
+    h = vp()
+    _call(lib, lib.um_session_create(kind, None, L, L, L, 1.0, 0.693, 0.0, 7, C.byref(h)))
+    try:
+        s = np.ascontiguousarray(random_unit_vectors(n, 3, 12), np.float32)
+        bad_total = 0
+        for sweep in range(3):
+            _call(lib, lib.um_session_set_field(h, s.ctypes.data))
+            _call(lib, lib.um_session_enqueue(h, 1))
+            cnt, ms = _u64(), _d()
+            _call(lib, lib.um_session_stats(h, C.byref(cnt), C.byref(ms), 1))
+            out = np.empty_like(s)
+            _call(lib, lib.um_session_get_field(h, out.ctypes.data))
+            cm = np.empty((n, 3))
+            cm[pos] = s.astype(np.float64)
+            v_o, _, margin = oracle.vector_metropolis(3, off, bonds, 1.0, 0.693, 0, 0.0, 7, sweep, 1, cm)
+            d = np.abs(out.astype(np.float64) - v_o[pos]).max(axis=1)
+            near = set(pos[np.nonzero(np.abs(margin[pos]) < 1e-3)[0]].tolist())  # device indices
+            allowed = set(near)
+            for k in near:
+                allowed |= rows[k]
+            bad = set(pos[np.nonzero(d > 1e-5)[0]].tolist())
+            assert bad <= allowed, sorted(bad - allowed)[:10]
+            bad_total += len(bad)
+            s = out
+        assert bad_total <= 20
+    finally:
+        lib.um_session_destroy(h)
