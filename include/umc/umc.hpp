@@ -4,7 +4,7 @@
 // UMC_NO_GLOBAL_NAMES is defined the names are also brought into the global
 // namespace, as the reference declares them, so reference-style programs
 // compile after swapping their includes for this one.  Link with
-// libumc_b200.so (see INTEGRATION.md of the repository).
+// libumc_b200.so.
 #pragma once
 
 #include "detail.hpp"

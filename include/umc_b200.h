@@ -20,7 +20,7 @@
  * the same messages available from umc_last_error() (thread-local).
  *
  * Random numbers: every update opens its own reference-semantics Pcg32 keyed by
- * (seed, counter, tag, id) -- see the package's csrc/umc_rng.cuh -- so a chain
+ * (seed, counter, tag, id) -- see include/umc/keyed_pcg.cuh -- so a chain
  * is a pure function of (field, seed, counters) and can be replayed by the
  * reference driver on the CPU.
  */
@@ -172,13 +172,17 @@ int umc_chain_get_field(umc_chain* c, void* host_field);
  * (umc_chain_sync, _fetch, _get_field, a *_run).  The reference sets a field
  * only through its model's update(i, .) (model.hpp:70-86). */
 int umc_chain_upload_async(umc_chain* c, const void* host_field);
-/* Chain checkpoints: a self-describing byte image of a chain -- an 88-byte
- * header (magic "UMCCHK01", version, model, components, lattice size, seed,
- * sweep and flip counters, coupling, proposal, width, hits, Wolff axis) and
- * then the field in the reference's data() layout.  Restoring it into a chain
- * of the same model, components, lattice size and coupling (for instance in a
- * new process) sets the field, the key seed, the counters and the proposal,
- * so the chain continues exactly as the checkpointed one would have.  The
+/* Chain checkpoints: a self-describing byte image of a chain -- a 104-byte
+ * header (magic "UMCCHK01", version 2, model, components, lattice size, seed,
+ * sweep and flip counters, coupling, proposal, width, hits, Wolff axis, and
+ * the Wolff flips done with the sum of their cluster sizes) and then the field
+ * in the reference's data() layout.  Restoring it into a chain of the same
+ * model, components, lattice size and coupling (for instance in a new process)
+ * sets the field, the key seed, the counters, the proposal and the Wolff
+ * statistics, so the chain continues exactly as the checkpointed one would
+ * have, mean_cluster_size included.  Version-1 images (an 88-byte header
+ * without the Wolff statistics) are still accepted; their restore resets
+ * mean_cluster_size to start from the restored flip.  The
  * reference has no checkpoint format: its user copies data() by hand
  * (model.hpp:70-86); this is the engine's own. */
 int umc_chain_checkpoint_bytes(const umc_chain* c, uint64_t* bytes);
@@ -331,11 +335,16 @@ void* umc_batch_stream(const umc_batch* b);
  * Its scratch (union-find labels and a status word) is a file-scope device
  * array sized for at most 1,048,576 sites; larger graphs return
  * UMC_ERR_UNSUPPORTED.  Every GPU that loads the library holds that array
- * (about 8 MiB) until the process exits.  The first call on a device resolves
- * the array's address (cudaGetSymbolAddress) with that device current, so make
- * it before any stream capture.  All calls share the array: each call resets
- * what must start from a known value, and calls that overlap on the GPU race.
- * The call synchronises `stream` and returns the cluster size. */
+ * (about 8 MiB) until the process exits.  Each call resolves the array's
+ * address (cudaGetSymbolAddress) on the current device.  All calls share the
+ * array: each call resets what must start from a known value, and calls that
+ * overlap on the GPU race.  Before flipping, a device check verifies the CSR
+ * (offset[0] = 0, non-decreasing offsets, neighbour ids < n_sites and no
+ * self-loops, each bond stored equally often at both ends) and refuses a graph
+ * that fails with UMC_ERR_INVALID_ARGUMENT, launching no flip; offset must
+ * hold n_sites + 1 entries and bonds/slot_edge offset[n_sites].  The call is
+ * synchronous (it synchronises `stream` twice and returns the cluster size), so
+ * it must never be made while `stream` is being captured. */
 int umc_wolff_flip_noalloc(int32_t model, int32_t components, void* field, uint64_t n_sites,
                            const uint32_t* offset, const uint32_t* bonds, const uint32_t* slot_edge,
                            double coupling, double beta, uint64_t seed, uint64_t flip,

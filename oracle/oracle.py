@@ -50,11 +50,18 @@ _f64 = C.c_double
 _int = C.c_int
 
 
-def build(reference_root: str | None = "/root/reference") -> None:
-    """Builds the oracle (and the reference harness where the tree exists)."""
+def build(reference_root: str | None = None) -> None:
+    """Builds the oracle, and the reference harness where the reference tree
+    exists: at ``reference_root``, else at $UMC_REFERENCE_ROOT, else wherever
+    oracle/Makefile's REF default points (the Makefile skips the harness when
+    no tree is there)."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if reference_root and os.path.isfile(os.path.join(reference_root, "driver.hpp")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={reference_root}"], check=True)
+    root = reference_root or os.environ.get("UMC_REFERENCE_ROOT")
+    if root:
+        if os.path.isfile(os.path.join(root, "driver.hpp")):
+            subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={root}"], check=True)
+    else:
+        subprocess.run(["make", "-s", "-C", HERE, "ref-if-present"], check=True)
 
 
 def _ptr(a):

@@ -36,6 +36,7 @@ def test_restored_chain_continues_exactly(umc, kind, tmp_path):
     a.save(tmp_path / "chain.ckpt")
     ra, sa = _advance(a, kind, 8)
     fa = a.get_field()
+    stats_a = a.wolff_stats()
     for via_file in (False, True):
         b = _make(umc, kind, 999)  # another seed: the image carries the key seed
         if via_file:
@@ -48,6 +49,29 @@ def test_restored_chain_continues_exactly(umc, kind, tmp_path):
         if sa is not None:
             np.testing.assert_array_equal(sa, sb)
         np.testing.assert_array_equal(fa, b.get_field())
+        # the image carries the Wolff statistics behind mean_cluster_size
+        assert b.wolff_stats() == stats_a
+
+
+def test_version1_image_is_accepted_and_restarts_the_wolff_statistics(umc):
+    """An image in the earlier 88-byte-header layout (no Wolff statistics)
+    still restores the field, seed and counters; mean_cluster_size then counts
+    only the flips made after the restore."""
+    a = _make(umc, "o3", 11)
+    a.randomize(3)
+    _advance(a, "o3", 6)
+    v2 = bytearray(a.checkpoint())
+    assert int.from_bytes(v2[8:12], "little") == 2
+    v1 = bytearray(v2[:88] + v2[104:])
+    v1[8:12] = (1).to_bytes(4, "little")
+    ra, sa = _advance(a, "o3", 5)
+    b = _make(umc, "o3", 999)
+    b.restore(bytes(v1))
+    assert b.counters() == (6, 6) and b.wolff_stats() == (0, 0.0)
+    rb, sb = _advance(b, "o3", 5)
+    np.testing.assert_array_equal(ra, rb)
+    np.testing.assert_array_equal(sa, sb)
+    assert b.wolff_stats() == (5, float(np.sum(sb)))
 
 
 def test_mismatched_or_damaged_images_are_refused(umc):

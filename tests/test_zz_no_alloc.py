@@ -96,3 +96,44 @@ def test_noalloc_rejects_graphs_above_its_scratch(umc, oracle):
                      csr[2].data_ptr(), 1.0, 0.4, 1, 0, C.byref(size), torch.cuda.current_stream().cuda_stream)
     assert rc == umc.ERR_UNSUPPORTED
     assert "1,048,576" in umc.lib.umc_last_error().decode()
+
+
+def test_noalloc_refuses_a_bad_csr_and_stays_usable(umc, oracle):
+    """A neighbour id beyond the graph, a self-loop and a bond stored at one
+    end only are refused by the device check before any flip kernel runs;
+    the field is untouched and the next valid call flips as the chain does."""
+    torch = pytest.importorskip("torch")
+    L, beta, seed = 8, 0.44, 3
+    g = umc.square_lattice(L, L)
+    n = L * L
+    pos, csr = _device_csr(torch, oracle, g, *square_edges(L, L))
+    off = csr[0].cpu().numpy().view(np.uint32)
+    bonds = csr[1].cpu().numpy().view(np.uint32)
+    field = torch.ones(n, dtype=torch.int8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def call(b):
+        size = C.c_uint64(0)
+        dev = torch.from_numpy(b.view(np.int32)).cuda()
+        rc = _entry(umc)(umc.MODEL_ISING, 1, field.data_ptr(), n, csr[0].data_ptr(), dev.data_ptr(),
+                         csr[2].data_ptr(), 1.0, beta, seed, 0, C.byref(size), stream)
+        return rc, umc.lib.umc_last_error().decode()
+
+    out_of_range = bonds.copy()
+    out_of_range[5] = n + 7  # in-bounds slot, id beyond the graph
+    self_loop = bonds.copy()
+    self_loop[off[9]] = 9
+    one_sided = bonds.copy()
+    i, j = 10, int(bonds[off[10]])
+    one_sided[off[10]] = int(bonds[off[10] + 1])  # row 10 loses its bond to j, j keeps its bond to 10
+    for bad, words in ((out_of_range, "neighbour id"), (self_loop, "self-loop"), (one_sided, "not symmetric")):
+        rc, msg = call(bad)
+        assert rc == umc.ERR_INVALID_ARGUMENT and words in msg, (rc, msg)
+        assert bool((field == 1).all()), "a refused call changed the field"
+    rc, msg = call(bonds.copy())
+    assert rc == umc.OK, msg
+    ch = umc.Chain(umc.MODEL_ISING, graph=g, coupling=1, proposal=umc.PROPOSAL_FLIP, wolff_axis=umc.AXIS_FIXED,
+                   seed=seed)
+    ch.set_field(np.ones(n, np.int8))
+    ch.wolff(beta, 1, records=False)
+    np.testing.assert_array_equal(field.cpu().numpy()[pos], ch.get_field())

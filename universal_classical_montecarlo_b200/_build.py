@@ -23,7 +23,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++20", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", f"-I{INCLUDE}"]
-CXX_FLAGS = ["-std=c++20", "-O2", "-fPIC", "-Wall", "-Wextra", f"-I{INCLUDE}", f"-I{CUDA_HOME}/include"]
+CXX_FLAGS = ["-std=c++23", "-O2", "-fPIC", "-Wall", "-Wextra", f"-I{INCLUDE}", f"-I{CUDA_HOME}/include"]
 
 CU_SOURCES = ["umc_chain.cu", "umc_gauge.cu", "umc_batch.cu", "umc_learn.cu", "umc_noalloc.cu"]
 CXX_SOURCES = ["umc_tables.cpp", "umc_stats.cpp"]
@@ -37,7 +37,9 @@ def _sources():
 
 def _deps():
     shared = [os.path.join(INCLUDE, "umc", f) for f in os.listdir(os.path.join(INCLUDE, "umc")) if f.endswith(".cuh")]
-    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(INCLUDE, "umc_b200.h")] + shared
+    # this file too: a change of flags rebuilds
+    return ([os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(INCLUDE, "umc_b200.h")] + shared
+            + [os.path.abspath(__file__)])
 
 
 def _stale(obj: str, src: str) -> bool:

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <limits>
 #include <new>
@@ -1107,6 +1108,8 @@ int umc_chain_set_field(umc_chain* c, const void* host_field)
 namespace {
 // Checkpoint image: this header, then the field in the reference's data()
 // layout.  Fixed-width fields, little-endian as the host writes them.
+// Version 1 ended after wolff_axis (88 bytes); version 2 appends the Wolff
+// statistics behind mean_cluster_size (flips done and the sum of their sizes).
 struct CheckpointHeader
 {
     char magic[8];  // "UMCCHK01"
@@ -1119,8 +1122,13 @@ struct CheckpointHeader
     uint64_t seed, sweeps, flips;
     double coupling, width;
     int32_t proposal, wolff_axis;
+    uint64_t wolff_flips_done;  // version 2
+    double wolff_size_sum;      // version 2
 };
-static_assert(sizeof(CheckpointHeader) == 88, "checkpoint header layout");
+constexpr size_t kCheckpointHeaderV1 = 88;
+static_assert(offsetof(CheckpointHeader, wolff_flips_done) == kCheckpointHeaderV1, "checkpoint v1 layout");
+static_assert(sizeof(CheckpointHeader) == 104, "checkpoint header layout");
+constexpr uint32_t kCheckpointVersion = 2;
 constexpr char kCheckpointMagic[8] = {'U', 'M', 'C', 'C', 'H', 'K', '0', '1'};
 
 uint64_t host_field_bytes(const umc_chain* c) { return c->n * c->comps * c->elem_bytes; }
@@ -1143,7 +1151,7 @@ int umc_chain_checkpoint(umc_chain* c, void* buffer, uint64_t capacity)
             throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint buffer too small (see umc_chain_checkpoint_bytes)");
         CheckpointHeader h{};
         std::memcpy(h.magic, kCheckpointMagic, 8);
-        h.version = 1;
+        h.version = kCheckpointVersion;
         h.model = c->model;
         h.components = c->N;
         h.hits = c->desc.hits;
@@ -1156,6 +1164,8 @@ int umc_chain_checkpoint(umc_chain* c, void* buffer, uint64_t capacity)
         h.width = c->desc.width;
         h.proposal = c->desc.proposal;
         h.wolff_axis = c->desc.wolff_axis;
+        h.wolff_flips_done = c->wolff_flips_done;
+        h.wolff_size_sum = c->wolff_size_sum;
         uint8_t* out = static_cast<uint8_t*>(buffer);
         const int st = umc_chain_get_field(c, out + sizeof h);
         if (st != UMC_OK) throw Error(st, umc_last_error());
@@ -1167,21 +1177,27 @@ int umc_chain_restore(umc_chain* c, const void* buffer, uint64_t bytes)
 {
     return guarded([&] {
         if (!c || !buffer) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
-        if (bytes < sizeof(CheckpointHeader)) throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint too short");
-        CheckpointHeader h;
-        std::memcpy(&h, buffer, sizeof h);
-        if (std::memcmp(h.magic, kCheckpointMagic, 8) != 0 || h.version != 1)
+        if (bytes < kCheckpointHeaderV1) throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint too short");
+        CheckpointHeader h{};
+        std::memcpy(&h, buffer, kCheckpointHeaderV1);
+        if (std::memcmp(h.magic, kCheckpointMagic, 8) != 0 || (h.version != 1 && h.version != 2))
             throw Error(UMC_ERR_INVALID_ARGUMENT, "not a chain checkpoint (magic or version)");
+        // a version-1 image has no Wolff statistics: mean_cluster_size restarts from zero
+        const size_t hb = h.version == 1 ? kCheckpointHeaderV1 : sizeof h;
+        if (bytes < hb) throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint too short");
+        std::memcpy(&h, buffer, hb);
         if (h.model != c->model || h.components != c->N || h.n != c->n)
             throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint is of another model, component count or lattice size");
-        if (h.field_bytes != host_field_bytes(c) || bytes < sizeof h + h.field_bytes)
+        if (h.field_bytes != host_field_bytes(c) || bytes < hb + h.field_bytes)
             throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint field size does not match the chain");
         if (h.coupling != c->desc.coupling)
             throw Error(UMC_ERR_INVALID_ARGUMENT, "checkpoint coupling differs from the chain's");
         validate_proposal(c, h.proposal, h.width, h.hits);
         validate_axis(c, h.wolff_axis);
-        const int st = umc_chain_set_field(c, static_cast<const uint8_t*>(buffer) + sizeof h);
+        const int st = umc_chain_set_field(c, static_cast<const uint8_t*>(buffer) + hb);
         if (st != UMC_OK) throw Error(st, umc_last_error());
+        c->wolff_flips_done = h.wolff_flips_done;
+        c->wolff_size_sum = h.wolff_size_sum;
         c->desc.proposal = h.proposal;
         c->desc.width = h.width;
         c->desc.hits = h.hits;

@@ -16,9 +16,20 @@
 //  * all calls on a device share it and it keeps the last call's contents --
 //    each call re-initialises the parts that must start from a known value, and
 //    calls that overlap on the GPU (two streams, or two host threads) race;
-//  * the first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (with that device current) and caches it; make that
-//    first call before any stream capture.
+//  * every call looks up the array's device address with cudaGetSymbolAddress
+//    on the current device (cheap once the module is loaded, and never stale
+//    after a device reset re-creates the context);
+//  * the call is synchronous: it checks the graph and reads the cluster size
+//    back with stream synchronisations, so it must never be made while its
+//    stream is being captured into a CUDA graph.
+//
+// Before the flip a check kernel verifies the caller's CSR over n sites:
+// offset[0] = 0, non-decreasing offsets, every neighbour id below n and not
+// the site itself, and every bond stored from both ends the same number of
+// times.  A graph that fails is refused with UMC_ERR_INVALID_ARGUMENT and the
+// flip kernels are not launched, so a bad id never reaches the labels.  The
+// check reads offset[0..n] and bonds[offset[0]..offset[n]); those arrays must
+// have that many entries.
 //
 // The kernels are the chain's own Wolff kernels (bond activation + union-find,
 // then the cluster flip), so a call reproduces umc_wolff_run on the same field,
@@ -27,7 +38,6 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 
 #include "umc_chain.hpp"
 #include "umc_spin_kernels.cuh"
@@ -42,29 +52,67 @@ struct NoAllocScratch
     uint32_t labels[2][kNoAllocMaxSites];
     DevCtl ctl;
     unsigned long long size;
+    uint32_t csr_fault;  // bits set by noalloc_check_csr
 };
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-NoAllocScratch* g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device (looked up once).
-NoAllocScratch* scratch_for(int device)
+// Device address of the scratch array on the current device.  Resolved on
+// every call: a cached address would outlive a cudaDeviceReset that reloads
+// the module.
+NoAllocScratch* scratch_on_current_device()
 {
-    if (device < 0 || device >= kMaxDevices) throw Error(UMC_ERR_UNSUPPORTED, "device ordinal above 63");
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            throw Error(UMC_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-        }
-        g_scratch_ptr[device] = static_cast<NoAllocScratch*>(p);
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        throw Error(UMC_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
     }
-    return g_scratch_ptr[device];
+    return static_cast<NoAllocScratch*>(p);
+}
+
+constexpr uint32_t kCsrOffsets = 1u;    // offset[0] != 0 or a decreasing offset
+constexpr uint32_t kCsrNeighbour = 2u;  // a neighbour id >= n, or a self-loop
+constexpr uint32_t kCsrAsymmetric = 4u; // bond i-j stored a different number of times at i and at j
+
+// Checks the caller's CSR before any kernel indexes labels with it.  One
+// thread per site; a bond's multiplicity is counted at its first slot in row i
+// against row j.
+__global__ void noalloc_check_csr(const uint32_t* off, const uint32_t* adj, uint32_t n, uint32_t* fault)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t bad = 0;
+        const uint32_t a0 = off[i], a1 = off[i + 1];
+        if (i == 0 && a0 != 0) bad |= kCsrOffsets;
+        if (a0 > a1) {
+            atomicOr(fault, bad | kCsrOffsets);
+            continue;
+        }
+        for (uint32_t q = a0; q < a1; ++q) {
+            const uint32_t j = adj[q];
+            if (j >= n || j == i) {
+                bad |= kCsrNeighbour;
+                continue;
+            }
+            bool first = true;
+            uint32_t here = 1;
+            for (uint32_t p = a0; p < a1; ++p) {
+                if (p == q || adj[p] != j) continue;
+                if (p < q) {
+                    first = false;
+                    break;
+                }
+                ++here;
+            }
+            if (!first) continue;
+            const uint32_t b0 = off[j], b1 = off[j + 1];
+            if (b0 > b1) continue;  // reported by site j's own thread
+            uint32_t there = 0;
+            for (uint32_t p = b0; p < b1; ++p) there += adj[p] == i ? 1u : 0u;
+            if (there != here) bad |= kCsrAsymmetric;
+        }
+        if (bad) atomicOr(fault, bad);
+    }
 }
 
 __global__ void noalloc_reset(NoAllocScratch* s, uint32_t n)
@@ -113,12 +161,27 @@ extern "C" int umc_wolff_flip_noalloc(int32_t model, int32_t components, void* f
         }
         int device = 0;
         cuda_check(cudaGetDevice(&device), "cudaGetDevice");
-        NoAllocScratch* s = scratch_for(device);
+        NoAllocScratch* s = scratch_on_current_device();
         int sms = 0;
         cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
         const uint64_t blocks = (n_sites + kBlock - 1) / kBlock;
         const uint32_t grid = uint32_t(blocks < uint64_t(sms) * 8 ? blocks : uint64_t(sms) * 8);
         cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+        // the graph is checked before any kernel indexes the labels with it
+        uint32_t fault = 0;
+        cuda_check(cudaMemsetAsync(&s->csr_fault, 0, sizeof fault, st), "clear CSR check");
+        noalloc_check_csr<<<grid, kBlock, 0, st>>>(offset, bonds, uint32_t(n_sites), &s->csr_fault);
+        cuda_check(cudaGetLastError(), "CSR check");
+        cuda_check(cudaMemcpyAsync(&fault, &s->csr_fault, sizeof fault, cudaMemcpyDeviceToHost, st), "read CSR check");
+        cuda_check(cudaStreamSynchronize(st), "CSR check");
+        if (fault & kCsrOffsets)
+            throw Error(UMC_ERR_INVALID_ARGUMENT, "umc_wolff_flip_noalloc: offsets must start at 0 and never decrease");
+        if (fault & kCsrNeighbour)
+            throw Error(UMC_ERR_INVALID_ARGUMENT, "umc_wolff_flip_noalloc: a neighbour id is >= n_sites or a self-loop");
+        if (fault & kCsrAsymmetric)
+            throw Error(UMC_ERR_INVALID_ARGUMENT,
+                        "umc_wolff_flip_noalloc: the CSR is not symmetric (a bond is not stored equally at both ends)");
 
         WolffArgs a{};
         a.field = field;
