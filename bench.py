@@ -36,6 +36,9 @@ sys.path.insert(0, ROOT)
 METRIC = "effective samples/s per B200 (learned+batched vs plain GPU); site-updates/s"
 L_DEFAULT = 64
 BETA = 0.693
+# untimed hybrid steps from the random start before either arm is timed: at
+# 64^3 and beta 0.693 the energy per site settles within about 500 steps
+THERM_STEPS = 1000
 PROFILES = os.path.join(ROOT, "profiles")
 
 
@@ -185,14 +188,22 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def reference_o3(L, warmup, steps, threads):
-    from oracle.oracle import Reference, have_reference
+def timing_reference():
+    """(Reference, build) of the timed CPU baselines (oracle.timing_reference:
+    the -O3 x86-64-v3 build of the reference harness where the host runs it),
+    or (None, None)."""
+    from oracle.oracle import timing_reference as tr
 
-    if not have_reference():
+    got = tr()
+    return got if got is not None else (None, None)
+
+
+def reference_o3(L, warmup, steps, threads):
+    r, build = timing_reference()
+    if r is None:
         return None
-    r = Reference()
     su, sec = r.bench_o3(L, BETA, warmup, steps, threads, 1)
-    return su, sec
+    return su, sec, build
 
 
 def run_reference(args):
@@ -200,23 +211,29 @@ def run_reference(args):
     if rank != 0:
         return
     threads = cpu_threads()
-    # a step of the stock CPU path is ~35 ms per thread at 64^3: bound the sample
+    # a step of the stock CPU path is ~15-35 ms per thread at 64^3: bound the
+    # sample; every chain first thermalises as the GPU arm's chain does
     steps = max(1, min(args.steps, 200))
     warm = max(0, min(args.warmup, 3))
-    res = reference_o3(args.L, warm, steps, threads)
+    res = reference_o3(args.L, THERM_STEPS + warm, steps, threads)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libumc_ref.so was not built"}))
         return
-    su, sec = res
+    su, sec, build = res
     value = su / sec
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": args.gpus,
         "steps": steps, "warmup": warm, "ms_per_step": 1e3 * sec / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": workload(args.L), "L": args.L, "beta": BETA, "chains": threads,
-                   "note": "the reference's stock driver (driver.hpp) on the host cores, one independent chain per thread"},
+                   "note": "the reference's stock driver (driver.hpp) on the host cores, one independent chain per "
+                           f"thread, built {build}",
+                   "thermalisation": f"{THERM_STEPS} untimed steps per chain from its random start, then the "
+                                     f"{warm} warm-up steps"},
         "cpu_baseline": {"value": value, "unit": "site-updates/s", "cores": threads, "kind": "reference",
-                         "sample": f"{steps} steps x {threads} chains of {args.L}^3 after {warm} warm-up steps"},
+                         "build": build,
+                         "sample": f"{steps} steps x {threads} chains of {args.L}^3 after {THERM_STEPS + warm} "
+                                   f"untimed steps"},
         "e2e": {"value": value, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -238,6 +255,14 @@ class O3Hybrid:
                             wolff_axis=umc.AXIS_SPHERE, seed=1 + rank, device=local, max_records=8192)
         self.ch.randomize(1000 + rank)
         self.flush = True
+
+    def thermalise(self):
+        """THERM_STEPS untimed steps from the random start, so the timed steps
+        see the configuration's equilibrium clusters; returns their mean size
+        over the last 200 steps."""
+        self.ch.enqueue_hybrid(BETA, THERM_STEPS)
+        _, sizes = self.ch.fetch(8192)
+        return float(sizes[-200:].mean())
 
     def describe(self):
         return workload(self.L)
@@ -294,10 +319,11 @@ class O3Hybrid:
             return None
         threads = cpu_threads()
         steps = max(2, int(seconds / max(est[1], 1e-4)))
-        su, sec = reference_o3(self.L, 1, steps, threads)
+        su, sec, build = reference_o3(self.L, THERM_STEPS, steps, threads)
         return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                         "build": build,
                 "sample": f"{steps} steps x {threads} independent {self.L}^3 chains (reference stock driver, "
-                          f"plain Pcg32), {sec:.1f} s"}
+                          f"plain Pcg32) after {THERM_STEPS} untimed steps each, {sec:.1f} s"}
 
 
 class IsingSweep:
@@ -344,14 +370,13 @@ class IsingSweep:
                 "d2h_bytes_per_step": 64, "steps": K}
 
     def cpu(self, seconds):
-        from oracle.oracle import Reference, have_reference
-
-        if not have_reference():
+        r, build = timing_reference()
+        if r is None:
             return None
-        r = Reference()
         threads = cpu_threads()
         su, sec = r.bench_ising(64, 0.44, 10, 2000, threads, 1)
         return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                         "build": build,
                 "sample": f"2000 sweeps x {threads} independent 64x64 chains (reference stock driver)"}
 
 
@@ -400,7 +425,22 @@ class SU3Sweep:
                 "h2d_bytes_per_step": self.n * 72, "d2h_bytes_per_step": 64, "steps": K}
 
     def cpu(self, seconds):
-        return None
+        """The reference's SUGauge<3> with SUShift 0.2 and 10 hits per link
+        (multi-hit through a window adapter), one chain per thread, timed on a
+        window of each thread's lattice: a full 24^4 sweep of 10 hits takes
+        about a minute per core, so the rate of a bounded window is reported."""
+        r, build = timing_reference()
+        if r is None:
+            return None
+        threads = cpu_threads()
+        su, sec = r.bench_su3(self.L, 5.7, 0.2, 10, 2000, 1, 1, 1)
+        window = max(2000, min(self.n, int(2000 * seconds / max(sec, 1e-4))))
+        su, sec = r.bench_su3(self.L, 5.7, 0.2, 10, window, 1, threads, 1)
+        return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                         "build": build,
+                "sample": f"{threads} independent {self.L}^4 chains (reference SUGauge<3>, SUShift 0.2, 10 hits per "
+                          f"link, cold start), each timed on one pass over a window of {window} of its "
+                          f"{self.n} links ({sec:.1f} s); the rate of a full sweep is extrapolated from it"}
 
 
 class XYBatch:
@@ -458,16 +498,15 @@ class XYBatch:
                 "h2d_bytes_per_step": self.n * 4, "d2h_bytes_per_step": self.b.n_chains * 64, "steps": K}
 
     def cpu(self, seconds):
-        from oracle.oracle import Reference, have_reference
-
-        if not have_reference():
+        r, build = timing_reference()
+        if r is None:
             return None
-        r = Reference()
         threads = cpu_threads()
         su, sec = r.bench_xy(64, 1.0, 1.0, 2, 50, 1, 1)
         sweeps = max(10, int(seconds * 50 / max(sec, 1e-4)))
         su, sec = r.bench_xy(64, 1.0, 1.0, 2, sweeps, threads, 1)
         return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                         "build": build,
                 "sample": f"{sweeps} sweeps x {threads} independent 64x64 XY chains (reference PairModel + "
                           f"U1Shift, stock driver), {sec:.1f} s"}
 
@@ -839,16 +878,15 @@ class UserXY(_UserSession):
         return 48.0 * self.n
 
     def cpu(self, seconds):
-        from oracle.oracle import Reference, have_reference
-
-        if not have_reference():
+        r, build = timing_reference()
+        if r is None:
             return None
-        r = Reference()
         threads = cpu_threads()
         su, sec = r.bench_xy(256, 1.1, 1.0, 1, 5, 1, 1)
         sweeps = max(5, int(seconds * 5 / max(sec, 1e-4)))
         su, sec = r.bench_xy(256, 1.1, 1.0, 1, sweeps, threads, 1)
         return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                         "build": build,
                 "sample": f"{sweeps} sweeps x {threads} independent 256x256 XY chains (reference PairModel<U1Dof, "
                           f"user term> + U1Shift, stock driver), {sec:.1f} s"}
 
@@ -887,16 +925,15 @@ class UserO3(_UserSession):
         return (64.0 if self.tables else 36.0) * self.n
 
     def cpu(self, seconds):
-        from oracle.oracle import Reference, have_reference
-
-        if not have_reference():
+        r, build = timing_reference()
+        if r is None:
             return None
-        r = Reference()
         threads = cpu_threads()
         su, sec = r.bench_pair_o3(32, 0.693, 1, 3, 1, 1)
         sweeps = max(3, int(seconds * 3 / max(sec, 1e-4)))
         su, sec = r.bench_pair_o3(32, 0.693, 1, sweeps, threads, 1)
         return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                         "build": build,
                 "sample": f"{sweeps} sweeps x {threads} independent 32^3 chains (reference PairModel<VectorDof<3>, "
                           f"HeisenbergTerm<3>> + UniformSphereN<3>, stock driver, FP64), {sec:.1f} s"}
 
@@ -968,16 +1005,15 @@ class UserIsingWolff(_UserSession):
                 "steps": K}
 
     def cpu(self, seconds):
-        from oracle.oracle import Reference, have_reference
-
-        if not have_reference():
+        r, build = timing_reference()
+        if r is None:
             return None
-        r = Reference()
         threads = cpu_threads()
         su, sec = r.bench_ising_wolff(256, 0.44, 50, 50, 1, 1)
         flips = max(50, int(seconds * 50 / max(sec, 1e-4)))
         su, sec = r.bench_ising_wolff(256, 0.44, 200, flips, threads, 1)
         return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                         "build": build,
                 "sample": f"{flips} flips x {threads} independent 256x256 Ising chains (reference Wolff<Ising, "
                           f"FixedAxis>, stock driver, 200 warm-up flips), {sec:.1f} s"}
 
@@ -1016,16 +1052,15 @@ class UserU1(_UserSession):
         return (214.0 if self.tables else 80.0) * self.n
 
     def cpu(self, seconds):
-        from oracle.oracle import Reference, have_reference
-
-        if not have_reference():
+        r, build = timing_reference()
+        if r is None:
             return None
-        r = Reference()
         threads = cpu_threads()
         su, sec = r.bench_u1_cells(8, 1.1, 1.0, 0.7, 1, 2, 1, 1)
         sweeps = max(2, int(seconds * 2 / max(sec, 1e-4)))
         su, sec = r.bench_u1_cells(8, 1.1, 1.0, 0.7, 1, sweeps, threads, 1)
         return {"value": su / sec, "unit": self.unit, "cores": threads, "kind": "reference",
+                         "build": build,
                 "sample": f"{sweeps} sweeps x {threads} independent 8^4 chains (reference CellModel<U1Dof, "
                           f"U1PlaquetteTerm, CellComplex<4>> + U1Shift, stock driver, FP64), {sec:.1f} s"}
 
@@ -1087,6 +1122,7 @@ def main():
     import universal_classical_montecarlo_b200 as umc
 
     wl = WORKLOADS[args.workload](umc, args, rank, local)
+    therm_cluster = wl.thermalise() if hasattr(wl, "thermalise") else None
     ch = wl.ch
     stream = torch.cuda.ExternalStream(ch.stream(), device=torch.device("cuda", local))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if wl.flush else None
@@ -1140,6 +1176,9 @@ def main():
         per_kind = {"batch": (K, total_ms)}
     elif wl.name == "u1batch":
         per_kind = {"learned": (K, total_ms)}
+    elif len([k for k, v in launches.items() if v[0]]) == 1 and gpu_launches == K:
+        # one launch per step: the step events time the kernel itself
+        per_kind = {next(k for k, v in launches.items() if v[0]): (K, total_ms)}
     else:
         per_kind = None
     ch.set_timing(True)
@@ -1221,7 +1260,10 @@ def main():
         "config": {"workload": wl.describe(), "L": wl.L, "parallelism": f"replicas x{ws}" if ws > 1 else "1 chain",
                    "l2": ("flushed between timed steps (256 MiB write, outside the timed events)" if wl.flush
                           else "state larger than L2, no flush"),
-                   "mean_cluster": float(sizes.mean()) if len(sizes) and wl.name in ("o3", "userwolff") else None},
+                   "mean_cluster": float(sizes.mean()) if len(sizes) and wl.name in ("o3", "userwolff") else None,
+                   "thermalisation": (None if therm_cluster is None else
+                                      f"{THERM_STEPS} untimed steps from the random start (mean cluster of the "
+                                      f"last 200: {therm_cluster:.1f})")},
         "roofline": {"bound": roof["bound"], "achieved": achieved, "peak": peak, "unit": roof["unit"],
                      "frac": achieved / peak, "traffic": traffic, "kernel": kind, "avg_launch_us": avg_s * 1e6,
                      "peak_source": roof["peak_source"]},

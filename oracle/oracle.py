@@ -23,6 +23,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libumc_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libumc_ref.so")
+# the same harness built -O3 -march=x86-64-v3, for the timed CPU baselines
+REF_FAST_SO = os.path.join(HERE, "_ref", "libumc_ref_fast.so")
+_X86_64_V3 = {"avx", "avx2", "bmi1", "bmi2", "fma", "f16c", "lzcnt", "movbe", "xsave"}
 
 TAG_BOND = 1
 TAG_AXIS = 2
@@ -434,12 +437,14 @@ class Reference:
         self._su_shift = L.fn("su_shift", None, _u32, _f64, _u64, _u64, _u32, _u32, _vp, _vp)
         self._bench_o3 = L.fn("bench_o3", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._stock_o3 = L.fn("stock_o3_chain", _int, _u64, _f64, _u64, _u64, _u64, _vp)
+        self._stock_o3_multi = L.fn("stock_o3_chains", _int, _u64, _f64, _u64, _u32, _vp, _u64, _u64, _vp)
         self._stock_su3 = L.fn("stock_su3_chain", _int, _u64, _f64, _f64, _u64, _u32, _u64, _u64, _vp)
         self._bench_ising = L.fn("bench_ising", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._bench_xy = L.fn("bench_xy", _int, _u64, _f64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._bench_pair_o3 = L.fn("bench_pair_o3", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._bench_ising_wolff = L.fn("bench_ising_wolff", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
         self._bench_u1_cells = L.fn("bench_u1_cells", _int, _u64, _f64, _f64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
+        self._bench_su3 = L.fn("bench_su3", _int, _u64, _f64, _f64, _u32, _u64, _u64, _u32, _u64, _vp, _vp)
 
     def pcg32_draws(self, seed, stream, n):
         out = np.zeros(n, np.uint32)
@@ -600,6 +605,21 @@ class Reference:
         assert st == 0, st
         return obs
 
+    def stock_o3_chains(self, L, beta, seed, chains, warmup, steps, init=None):
+        """Independent reference O(3) L^3 chains, one per thread (seed + c),
+        chain c from init[c] (chains x n x 3, the natural site order) or its
+        own random start: (chains, steps, 4) of per-step [E, Mx, My, Mz] after
+        `warmup`."""
+        obs = np.zeros((chains, steps, 4))
+        ini = None
+        if init is not None:
+            ini = np.ascontiguousarray(init, np.float64)
+            assert ini.shape == (chains, L**3, 3), ini.shape
+            ini = ini.reshape(-1)
+        st = self._stock_o3_multi(L, beta, seed, chains, _ptr(ini), warmup, steps, _ptr(obs))
+        assert st == 0, st
+        return obs
+
     def stock_su3_chain(self, L, beta, width, seed, chains, warmup, sweeps):
         """The reference's own SU(3) L^4 chains (SUGauge<3>, SUShift, 1 hit,
         plain Pcg32 seeded seed + c), one per thread: (chains, sweeps) mean
@@ -676,5 +696,41 @@ def _bench_u1_cells(self, L, model_beta, beta, width, warmup, sweeps, threads, s
 Reference.bench_u1_cells = _bench_u1_cells
 
 
+def _bench_su3(self, L, model_beta, width, hits, window, sweeps, threads, seed=1):
+    """ref_bench_su3: the reference's stock SU(3) multi-hit Metropolis timed on
+    a window of links per thread; returns (link-updates, seconds)."""
+    su, sec = _f64(0), _f64(0)
+    st = self._bench_su3(L, model_beta, width, hits, window, sweeps, threads, seed, C.byref(su), C.byref(sec))
+    assert st == 0, st
+    return su.value, sec.value
+
+
+Reference.bench_su3 = _bench_su3
+
+
 def have_reference() -> bool:
     return os.path.isfile(REF_SO)
+
+
+def _host_has_x86_64_v3() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    # lzcnt is listed as abm on some kernels
+                    return _X86_64_V3 <= (flags | ({"lzcnt"} if "abm" in flags else set()))
+    except OSError:
+        pass
+    return False
+
+
+def timing_reference():
+    """(Reference, build) for the timed CPU baselines: the -O3 x86-64-v3 build
+    of the harness when it exists and the host runs that instruction set, else
+    the portable -O2 parity build.  None when neither was built."""
+    if os.path.isfile(REF_FAST_SO) and _host_has_x86_64_v3():
+        return Reference(REF_FAST_SO), "g++ -O3 -march=x86-64-v3"
+    if os.path.isfile(REF_SO):
+        return Reference(REF_SO), "g++ -O2 (portable parity build)"
+    return None

@@ -23,6 +23,7 @@
 // prefix, plus ref_bench_* entry points that time the reference's own stock
 // path (plain Pcg32, no adapters) for the CPU baseline.
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -875,6 +876,149 @@ extern "C" int ref_stock_o3_chain(std::uint64_t L, double beta, std::uint64_t se
             if (s >= warmup) vector_obs<3>(model, obs + (s - warmup) * 4);
         }
         return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+namespace {
+// A window of `links` links of a model, each visited K times in a row, for
+// timing the reference's stock multi-hit Metropolis on a bounded sample:
+// pseudo-site i is hit i % K of link i / K; data() points at a dummy buffer
+// so the driver's pointer arithmetic stays inside an allocation.
+template <class M>
+struct HitWindow
+{
+    using value_type = typename M::value_type;
+    static constexpr std::size_t size = M::size;
+
+    M* m;
+    std::size_t K, links;
+    std::vector<value_type> dummy;
+
+    std::size_t sites() const { return links * K; }
+    const value_type* data() const { return dummy.data(); }
+    double energy_diff_at(std::size_t i, const value_type* p) const { return m->energy_diff_at(i / K, p); }
+    void update(std::size_t i, const value_type* p) { m->update(i / K, p); }
+};
+
+// The stock proposal on a HitWindow: proposes from the model's current link
+// (not the dummy pointer) with the driver's plain Pcg32.
+template <class Q, class M>
+struct StockHit
+{
+    Q inner;
+    const HitWindow<M>* w;
+
+    template <class R, class T>
+    void sample(const T* cur, R& rng, T* out) const
+    {
+        const std::size_t i = static_cast<std::size_t>(cur - w->dummy.data()) / M::size;
+        inner.sample(w->m->data() + (i / w->K) * M::size, rng, out);
+    }
+    template <class T>
+    double log_ratio(const T* a, const T* b) const { return inner.log_ratio(a, b); }
+};
+}  // namespace
+
+// Times the reference's stock SU(3) path: SUGauge<3> (example/sun_gauge.hpp)
+// on hypercubic_plaquettes(L) with model beta and a cold start, Metropolis
+// with SUShift<3>{width}, driver beta 1 and a plain Pcg32, `hits` proposals per
+// link in a row; one chain per thread, each sweeping a window of the first
+// `window` links (the reference's link order) `sweeps` times after one
+// untimed window sweep.  site_updates = threads x window x hits x sweeps.
+extern "C" int ref_bench_su3(std::uint64_t L, double model_beta, double width, std::uint32_t hits, std::uint64_t window,
+                             std::uint64_t sweeps, std::uint32_t threads, std::uint64_t seed, double* site_updates,
+                             double* seconds)
+{
+    try {
+        std::vector<double> secs(threads, 0.0);
+        std::vector<std::thread> pool;
+        std::atomic<int> failed{0};
+        std::size_t used = 0;
+        for (std::uint32_t t = 0; t < threads; ++t)
+            pool.emplace_back([&, t] {
+                try {
+                    SUGauge<3> model(L, model_beta);
+                    const std::size_t w = std::min<std::size_t>(window, model.sites());
+                    if (t == 0) used = w;
+                    HitWindow<SUGauge<3>> hw{&model, hits, w, std::vector<SULink<3>>(w * hits)};
+                    using Q = StockHit<SUShift<3>, SUGauge<3>>;
+                    Metropolis<HitWindow<SUGauge<3>>, Q, Pcg32> mc(hw, Q{SUShift<3>{width}, &hw}, Pcg32(seed + t, 1), 1.0);
+                    mc.sweep();
+                    const auto t0 = std::chrono::steady_clock::now();
+                    mc.run(sweeps);
+                    const auto t1 = std::chrono::steady_clock::now();
+                    secs[t] = std::chrono::duration<double>(t1 - t0).count();
+                } catch (...) {
+                    failed = 1;
+                }
+            });
+        for (auto& th : pool) th.join();
+        if (failed) return -1;
+        double worst = 0.0;
+        for (double x : secs) worst = x > worst ? x : worst;
+        *site_updates = double(threads) * double(used) * double(hits) * double(sweeps);
+        *seconds = worst;
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+// Independent copies of the reference's stock O(3) chain (set-up of
+// ref_stock_o3_chain), one per thread: chain c starts from init + c n 3 (n x 3
+// doubles per chain, the site order of the user edge list; NULL = the uniform
+// random start of seed + c), runs `warmup` steps with plain Pcg32 streams seeded
+// seed + c, then records [E, Mx, My, Mz] of every step into
+// obs[(c * steps + k) * 4].  A start taken from another chain's equilibrium
+// lets the reference's chains skip their own thermalisation.
+extern "C" int ref_stock_o3_chains(std::uint64_t L, double beta, std::uint64_t seed, std::uint32_t chains,
+                                   const double* init, std::uint64_t warmup, std::uint64_t steps, double* obs)
+{
+    try {
+        std::vector<PairGraph<>::Edge> edges;
+        edges.reserve(3 * L * L * L);
+        for (std::uint64_t z = 0; z < L; ++z)
+            for (std::uint64_t y = 0; y < L; ++y)
+                for (std::uint64_t x = 0; x < L; ++x) {
+                    const auto i = static_cast<std::uint32_t>((z * L + y) * L + x);
+                    edges.push_back({i, static_cast<std::uint32_t>((z * L + y) * L + (x + 1) % L), {}});
+                    edges.push_back({i, static_cast<std::uint32_t>((z * L + (y + 1) % L) * L + x), {}});
+                    edges.push_back({i, static_cast<std::uint32_t>((((z + 1) % L) * L + y) * L + x), {}});
+                }
+        const std::size_t n = L * L * L;
+        std::vector<std::thread> pool;
+        std::atomic<int> failed{0};
+        for (std::uint32_t c = 0; c < chains; ++c)
+            pool.emplace_back([&, c] {
+                try {
+                    VectorSpin<3> model(PairGraph<>(n, edges), 1.0);
+                    Pcg32 init_rng(seed + c, 7);
+                    double v[3];
+                    for (std::size_t i = 0; i < n; ++i) {
+                        if (init) {
+                            model.update(i, init + (std::uint64_t(c) * n + i) * 3);
+                        } else {
+                            UniformSphereN<3>{}.sample(nullptr, init_rng, v);
+                            model.update(i, v);
+                        }
+                    }
+                    Metropolis<VectorSpin<3>, UniformSphereN<3>, Pcg32> mc(model, UniformSphereN<3>{}, Pcg32(seed + c, 1),
+                                                                         beta);
+                    Wolff<VectorSpin<3>, UniformSphereN<3>, Pcg32> w(model, UniformSphereN<3>{}, Pcg32(seed + c, 2), beta);
+                    double* out = obs + std::uint64_t(c) * steps * 4;
+                    for (std::uint64_t s = 0; s < warmup + steps; ++s) {
+                        (void)w.flip();
+                        mc.sweep();
+                        if (s >= warmup) vector_obs<3>(model, out + (s - warmup) * 4);
+                    }
+                } catch (...) {
+                    failed = 1;
+                }
+            });
+        for (auto& th : pool) th.join();
+        return failed ? -1 : 0;
     } catch (...) {
         return status_of(std::current_exception());
     }

@@ -13,7 +13,10 @@ from helpers import checker_position, relabel_edges, square_edges
 pytestmark = pytest.mark.gpu
 
 TOL = 4e-5     # radians after one segment (10 sweeps)
-MARGIN = 1e-3
+# the kernel decides as the FP64 test does on its FP32 angles; only the FP32
+# rounding of the proposed angle (about 2.4e-7, moving log_p by < 1.5e-6 at
+# beta <= 1.3) separates its decisions from the oracle's
+MARGIN = 2e-5
 
 
 def _geometric(lo, hi, R):

@@ -5,6 +5,12 @@ oracle (CellModel + U1PlaquetteTerm / SUPlaquetteTerm arithmetic, multi-hit in
 link order) and the engine (staple per link, FP32, SU(N) reunitarised).  Links
 must agree within TOL except where the oracle's accept decision sat within
 MARGIN of its threshold (and the links that share a cell with those).
+
+The engine decides as the FP64 test does on its FP32 links (FP32 first, FP64
+inside the FP32 error band), so MARGIN only covers the FP32 rounding of the
+proposal: the U(1) shift moves the new angle by about 2.4e-7 (log_p by
+beta deg 2.4e-7 < 1e-5 here), the SU(N) candidate U exp(iX) by about 1e-6 per
+entry (log_p by up to (beta/N) N^2 deg 1e-6, about 1e-4 at beta 2).
 """
 import numpy as np
 import pytest
@@ -12,7 +18,8 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-5
-MARGIN = 1e-3
+MARGIN_U1 = 2e-5
+MARGIN_SU = 2e-4
 
 
 def _setup(umc, oracle, cc):
@@ -62,7 +69,7 @@ def test_u1_per_sweep(umc, oracle, kind, L, beta, width, hits):
         got = ch.get_field().astype(np.float64)
         d = np.abs(np.angle(np.exp(1j * (got - t_o[pos]))))
         bad = np.nonzero(d > TOL)[0]
-        near = np.nonzero(np.abs(margin[pos]) < MARGIN)[0]
+        near = np.nonzero(np.abs(margin[pos]) < MARGIN_U1)[0]
         assert set(bad.tolist()) <= _cell_neighbours(cells_site, near) | set(near.tolist()), (bad, d[bad])
         mism += len(bad)
         P_true = oracle.u1_mean_plaquette(cells_site, got)
@@ -73,8 +80,10 @@ def test_u1_per_sweep(umc, oracle, kind, L, beta, width, hits):
     assert mism <= max(2, n // 50)
 
 
-@pytest.mark.parametrize("N,L,hits", [(3, 2, 2), (2, 4, 1), (3, 3, 1)])
+@pytest.mark.parametrize("N,L,hits", [(3, 2, 2), (2, 4, 1), (3, 3, 1), (3, 3, 10), (2, 2, 10)])
 def test_su_per_sweep(umc, oracle, N, L, hits):
+    """hits = 10 is the SU(3) configuration's multi-hit count: ten proposals
+    per link in a row, each from its own keyed stream."""
     cc = umc.hypercubic_plaquettes(L)
     n = cc.sites()
     pos, rcells, inc = _setup(umc, oracle, cc)
@@ -93,7 +102,7 @@ def test_su_per_sweep(umc, oracle, N, L, hits):
         got = _su_field(ch, N)
         d = np.abs(got - u_o[pos]).reshape(n, -1).max(axis=1)
         bad = np.nonzero(d > TOL)[0]
-        near = np.nonzero(np.abs(margin[pos]) < MARGIN)[0]
+        near = np.nonzero(np.abs(margin[pos]) < MARGIN_SU)[0]
         assert set(bad.tolist()) <= _cell_neighbours(cells_site, near) | set(near.tolist()), (bad, d[bad])
         mism += len(bad)
         P_true = oracle.su_mean_plaquette(N, cells_site, got)

@@ -18,6 +18,11 @@ from test_oracle_learn import torus_plaquette
 
 pytestmark = pytest.mark.gpu
 
+# the plain batched sweep decides as the FP64 test does on its FP32 angles, so
+# only the FP32 rounding of the proposed angle (log_p moves by < 1e-5 at
+# beta <= 5) separates it from the oracle; the learned MH step keeps its FP32
+# energy difference and the wider margin
+MARGIN_PLAIN = 2e-5
 MARGIN = 1e-3
 
 
@@ -95,7 +100,7 @@ def test_plain_sweep_matches_single_chain_oracle(umc, oracle, L, beta):
             t_o, obs, margin = oracle.u1_metropolis(cells, inc, beta, 1.0, 0.5, 1, int(seeds[c]), sweep, 1, cm)
             got = np.empty(2 * L * L)
             got[pos] = b.get_field(c)
-            near = np.abs(margin) < MARGIN
+            near = np.abs(margin) < MARGIN_PLAIN
             d = np.abs(np.remainder(got - t_o + np.pi, 2 * np.pi) - np.pi)
             bad = (d > 1e-4) & ~near
             total += got.size

@@ -10,15 +10,26 @@ deterministic).
 
 - O(3) 8^3, beta = 0.693, one Wolff flip + one sweep per step: E per site,
   |m| and chi = n (<m^2> - <|m|>^2);
+- O(3) 64^3, beta = 0.693 (the O(3) configuration itself): the same three
+  observables, the reference's chains started from equilibrium configurations
+  the GPU chain passed through (their own warm-up then forgets the start);
 - SU(3) 4^4, beta = 5.7, SUShift 0.2: mean plaquette (10 hits per link on the
   GPU, the reference's single hit: the same equilibrium distribution).
+
+Every observable must agree within two standard errors (Z_MAX = 2), the
+criterion of the parity target.  That is a per-observable test: for a correct
+sampler each z is a half-normal variate, so each comparison fails by chance
+with probability 4.6 %, and at least one of the seven compared here with
+1 - 0.954^7 = 28 %.  A family-wise 5 % test would need z < 2.69 (Bonferroni,
+7 comparisons); the z values are printed so a reader can apply either.  The
+seeds are fixed, so the outcome is deterministic.
 """
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
-Z_MAX = 3.0
+Z_MAX = 2.0
 
 
 def _mean_err(umc, x, n_bins=40):
@@ -69,6 +80,63 @@ def test_o3_hybrid_chain_matches_reference_chain(umc, ref):
     zs["chi"] = (_z(ca, eca, cb, ecb), ca, cb)
     print("O(3) 8^3 z, gpu, reference:", zs)
     for name, (z, a, b) in zs.items():
+        assert z < Z_MAX, (name, z, a, b)
+
+
+def _pooled_chi(m, n):
+    """chi = n (<m^2> - <m>^2) pooled over chains (rows of m), with a
+    jackknife error over the chains."""
+    m = np.asarray(m, np.float64)
+    s1, s2, cnt = m.sum(axis=1), (m * m).sum(axis=1), m.shape[1]
+    tot = m.size
+
+    def chi(a1, a2, c):
+        return n * (a2 / c - (a1 / c) ** 2)
+
+    full = chi(s1.sum(), s2.sum(), tot)
+    k = m.shape[0]
+    jk = np.array([chi(s1.sum() - s1[i], s2.sum() - s2[i], tot - cnt) for i in range(k)])
+    return full, np.sqrt((k - 1) / k * ((jk - jk.mean()) ** 2).sum())
+
+
+def test_o3_64_configuration_matches_reference_chains(umc, ref):
+    """The O(3) configuration: 64^3, beta = 0.693, one Wolff flip (random
+    axis) and one UniformSphereN sweep per step.  The GPU chain thermalises for
+    2000 steps from its random start (E per site settles within about 500),
+    then runs 20000 steps; every 1250 steps it leaves a snapshot.  Sixteen
+    reference chains (stock driver, plain Pcg32, FP64), one per host thread,
+    start from those snapshots, run 500 steps of their own and record 1500.
+    The reference's error is the scatter of its sixteen chain means
+    (jackknife over chains for chi); the GPU's is binned (Sokal window for the
+    means)."""
+    L, beta = 64, 0.693
+    n = L**3
+    ch = umc.Chain(umc.MODEL_VECTOR, graph=umc.cubic_lattice(L, L, L), components=3, coupling=1.0,
+                   proposal=umc.PROPOSAL_SPHERE, wolff_axis=umc.AXIS_SPHERE, seed=41)
+    ch.randomize(6)
+    ch.hybrid(beta, 2000)
+    recs, snaps = [], []
+    for _ in range(16):
+        snaps.append(ch.get_field().astype(np.float64).reshape(n, 3))
+        recs.append(ch.hybrid(beta, 1250)[1])
+    rec = np.concatenate(recs)
+    g_e = rec[:, 0] / n
+    g_m = np.linalg.norm(rec[:, 1:4], axis=1) / n
+    obs = ref.stock_o3_chains(L, beta, 900, len(snaps), 500, 1500, init=np.stack(snaps))
+    r_e = obs[:, :, 0] / n
+    r_m = np.linalg.norm(obs[:, :, 1:4], axis=2) / n
+
+    zs = {}
+    for name, a, b in (("E/site", g_e, r_e), ("|m|", g_m, r_m)):
+        tau = umc.tau_int(a)[0]
+        ma, ea = a.mean(), a.std() * np.sqrt(2 * tau / a.size)
+        cm = b.mean(axis=1)
+        mb, eb = cm.mean(), cm.std(ddof=1) / np.sqrt(cm.size)
+        zs[name] = (_z(ma, ea, mb, eb), ma, mb, ea, eb)
+    (ca, eca), (cb, ecb) = _chi_err(g_m, n, n_bins=16), _pooled_chi(r_m, n)
+    zs["chi"] = (_z(ca, eca, cb, ecb), ca, cb, eca, ecb)
+    print("O(3) 64^3 z, gpu, reference, errors:", zs)
+    for name, (z, a, b, _, _) in zs.items():
         assert z < Z_MAX, (name, z, a, b)
 
 

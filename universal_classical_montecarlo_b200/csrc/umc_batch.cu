@@ -73,6 +73,8 @@ struct SegArgs
     const unsigned long long* chain_seed;
     float J, width;
     double* part;  // per chain, kMaxShares shares: [E, Mx, My, accepted]
+    double J64;    // the coupling of the FP64 decisions
+    float err_per_beta;  // xy_metropolis_err(1, J, 4): the bound scales with beta
 };
 
 template <bool CG>
@@ -82,11 +84,24 @@ __device__ __forceinline__ float ldf(const float* p)
     else return *p;
 }
 
+// -beta dE of an XY site with four neighbour angles going from t to p:
+// -J sum_j (cos(p - t_j) - cos(t - t_j)), in FP64 on the FP32 angles.  Out of
+// line: it runs only for decisions the FP32 test cannot call.
+__device__ __noinline__ double xy4_log_ratio64(double J64, double beta64, float t, float p, float n0, float n1, float n2,
+                                               float n3)
+{
+    const float nb[4] = {n0, n1, n2, n3};
+    double d = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) d += -J64 * (cos(double(p) - double(nb[q])) - cos(double(t) - double(nb[q])));
+    return -beta64 * d;
+}
+
 // One XY site update (the body of xy_pass in umc_spin_kernels.cuh) on chain
 // data `th`; neighbours through L1 inside one CTA, through L2 in a cluster.
 template <bool CLUSTER>
 __device__ __forceinline__ bool xy_update(const SegArgs& a, float* th, uint32_t colour, uint32_t y, uint32_t i,
-                                          uint64_t kbase, float beta)
+                                          uint64_t kbase, float beta, double beta64)
 {
     const uint32_t L = a.L, H = a.H;
     const uint32_t p = (y + colour) & 1u;
@@ -112,19 +127,25 @@ __device__ __forceinline__ bool xy_update(const SegArgs& a, float* th, uint32_t 
     __sincosf(t, &so, &co);
     __sincosf(prop, &sp, &cp);
     const float dE = -a.J * ((cp - co) * C + (sp - so) * S);
-    if (!metropolis_accept(g, -beta * dE)) return false;
+    const bool ok = metropolis_accept(g, -beta * dE, beta * a.err_per_beta, [&] {
+        return xy4_log_ratio64(a.J64, beta64, t, prop, nb[0], nb[1], nb[2], nb[3]);
+    });
+    if (!ok) return false;
     own[y * H + i] = prop;
     return true;
 }
 
+// The cluster form stays at 32 registers (two CTAs per SM); the FP64
+// decision is out of line and spills inside itself.
 template <bool CLUSTER>
-__global__ void __launch_bounds__(1024) xy_batch_segment(SegArgs a)
+__global__ void __launch_bounds__(1024, CLUSTER ? 2 : 1) xy_batch_segment(SegArgs a)
 {
     __shared__ unsigned int accepted[kMaxCpc];
     // per owned chain and sweep: key base, beta and field offset (computed once
     // per CTA instead of once per site update)
     __shared__ uint64_t kb_sh[kMaxCpc];
     __shared__ float beta_sh[kMaxCpc];
+    __shared__ double beta64_sh[kMaxCpc];
     __shared__ unsigned long long off_sh[kMaxCpc];
     const uint64_t sweep0 = a.ctr->sweep;
     const uint32_t H = a.H, half = a.half;
@@ -156,7 +177,8 @@ __global__ void __launch_bounds__(1024) xy_batch_segment(SegArgs a)
         for (uint32_t ci = threadIdx.x; ci < chain_n; ci += blockDim.x) {
             const uint32_t chain = a.chains[chain_lo + ci];
             kb_sh[ci] = key_base(key_seed(a.chain_seed[chain], sweep0 + s, tag_site(0)));
-            beta_sh[ci] = float(a.betas[(chain / a.R) * a.R + a.slot_of_chain[chain]]);
+            beta64_sh[ci] = a.betas[(chain / a.R) * a.R + a.slot_of_chain[chain]];
+            beta_sh[ci] = float(beta64_sh[ci]);
             off_sh[ci] = a.off[chain];
         }
         __syncthreads();
@@ -174,7 +196,8 @@ __global__ void __launch_bounds__(1024) xy_batch_segment(SegArgs a)
                     y = row_lo + r / H;
                     i = r % H;
                 }
-                const bool acc = xy_update<CLUSTER>(a, a.theta + off_sh[ci], colour, y, i, kb_sh[ci], beta_sh[ci]);
+                const bool acc =
+                    xy_update<CLUSTER>(a, a.theta + off_sh[ci], colour, y, i, kb_sh[ci], beta_sh[ci], beta64_sh[ci]);
                 if (warp_chain) {
                     // the whole warp works on chain ci: one shared atomic per warp
                     const unsigned act = __activemask();
@@ -369,6 +392,8 @@ SegArgs seg_args(umc_batch* b, umc_batch::Group& g, float* theta)
     a.chain_seed = b->seeds_dev.as<unsigned long long>();
     a.J = float(b->desc.coupling);
     a.width = float(b->desc.width);
+    a.J64 = b->desc.coupling;
+    a.err_per_beta = xy_metropolis_err(1.0, b->desc.coupling, 4);
     a.part = b->part.as<double>();
     return a;
 }

@@ -260,10 +260,12 @@ void spin_pass(umc_chain* c, uint32_t p, double beta, uint64_t kbase, const Pass
         IsingArgs a{c->field.as<int8_t>(), first, count, kbase, c->tm1.as<uint32_t>(), c->max_degree, c->J_int, o};
         launch_ising_generic(c, a, t);
     } else if (c->model == UMC_MODEL_VECTOR) {
-        VecArgs a{c->field.as<float>(), uint32_t(c->n), first, count, kbase, c->J, float(beta), float(c->desc.width), o};
+        VecArgs a{c->field.as<float>(), uint32_t(c->n), first, count, kbase, c->J, float(beta), float(c->desc.width), o,
+                  c->desc.coupling, beta, vector_metropolis_err(beta, c->desc.coupling, c->N, c->max_degree)};
         launch_vector_n(c, a, t);
     } else {
-        XYArgs a{c->field.as<float>(), first, count, kbase, c->J, float(beta), float(c->desc.width), o};
+        XYArgs a{c->field.as<float>(), first, count, kbase, c->J, float(beta), float(c->desc.width), o,
+                 c->desc.coupling, beta, xy_metropolis_err(beta, c->desc.coupling, c->max_degree)};
         LaunchScope ls(c, UMC_KERNEL_METROPOLIS);
         xy_pass<Topo><<<grid_for(c, count), kBlock, 0, c->stream>>>(a, t);
     }
@@ -429,6 +431,9 @@ void stencil_flip(umc_chain* c, double beta, unsigned long long* size_slot)
     t.flip = c->flips;
     t.J = c->J;
     t.beta = float(beta);
+    t.J64 = c->desc.coupling;
+    t.beta64 = beta;
+    t.err = vector_wolff_err(beta, c->desc.coupling, c->N);
     if (c->model == UMC_MODEL_ISING) {
         if (!c->cw_valid || c->cw_beta != beta) {
             ising_wolff_thresholds(c->J_int, beta, c->cw);
@@ -539,6 +544,9 @@ bool fused_step(umc_chain* c, double beta, bool wolff, bool sweep, double* rec, 
     t.flip = c->flips;
     t.J = c->J;
     t.beta = float(beta);
+    t.J64 = c->desc.coupling;
+    t.beta64 = beta;
+    t.err = vector_wolff_err(beta, c->desc.coupling, c->N);
     t.ctl = c->ctl.as<DevCtl>();
     t.size_slot = size_slot;
     a.bar = &c->ctl.as<DevCtl>()->bar;
@@ -553,6 +561,8 @@ bool fused_step(umc_chain* c, double beta, bool wolff, bool sweep, double* rec, 
     }
     a.sweep_kbase = key_base(key_seed(c->desc.seed, c->sweeps, tag_site(0)));
     a.beta_metro = float(beta);
+    a.beta_metro64 = beta;
+    a.err_metro = vector_metropolis_err(beta, c->desc.coupling, c->N, c->max_degree);
     a.proposal = c->desc.proposal == UMC_PROPOSAL_ROTATION ? kPropRotation : kPropSphere;
     a.delta = float(c->desc.width);
     a.out = PassOut{c->ctl.as<DevCtl>(), c->partials.as<double>(), sweep ? rec : nullptr, nullptr, kMaxPasses - 2, 1, 1};
@@ -600,6 +610,9 @@ void spin_flip(umc_chain* c, double beta, double* rec, unsigned long long* size_
     a.flip = c->flips;
     a.J = c->J;
     a.beta = float(beta);
+    a.J64 = c->desc.coupling;
+    a.beta64 = beta;
+    a.err = vector_wolff_err(beta, c->desc.coupling, c->N);
     if (c->model == UMC_MODEL_ISING) {
         if (!c->cw_valid || c->cw_beta != beta) {
             ising_wolff_thresholds(c->J_int, beta, c->cw);

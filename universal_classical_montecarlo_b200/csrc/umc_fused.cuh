@@ -83,6 +83,8 @@ struct FusedArgs
     PassOut out;        // record of the sweep (pass index: dedicated slot)
     uint32_t* xlist;    // activated tile-crossing bonds, site * 4 + direction
     uint32_t xcap;      // its capacity (>= every + bond that can leave a tile)
+    double beta_metro64;  // beta of the FP64 accept decisions
+    float err_metro;      // vector_metropolis_err
 };
 
 template <int N>
@@ -108,7 +110,21 @@ __device__ __forceinline__ void fused_site(const FusedArgs& a, const StencilTopo
     bool acc_ok = false;
     if (ok) {
         const float dE = -a.w.J * (vdot<N>(cand, h) - vdot<N>(s, h));
-        acc_ok = metropolis_accept(g, -a.beta_metro * dE);
+        acc_ok = metropolis_accept(g, -a.beta_metro * dE, a.err_metro, [&] {
+            // the reference's sum over bonds, in FP64 on the FP32 state
+            double d = 0.0;
+            t.neighbours(k, [&](uint32_t j, bool) {
+                double pj = 0.0, oj = 0.0;
+#pragma unroll
+                for (int c = 0; c < N; ++c) {
+                    const double v = __ldcg(f + c * n + j);
+                    pj += double(cand[c]) * v;
+                    oj += double(s[c]) * v;
+                }
+                d += -a.w.J64 * (pj - oj);
+            });
+            return -a.beta_metro64 * d;
+        });
     }
     if (acc_ok) {
 #pragma unroll
@@ -187,7 +203,6 @@ __global__ void __launch_bounds__(TX * TY * TZ / SPT, 2 * SPT) hybrid_fused(Fuse
                 nat[u] = (z * w.Ly + y) * w.Lx + x;
                 float si[N];
                 load_spin<N>(w.field, w.n, colour_major(nat[u], x, y, z, w.half), si);
-                const float ri = vdot<N>(si, r);
                 uint32_t rank = 0;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
@@ -203,7 +218,7 @@ __global__ void __launch_bounds__(TX * TY * TZ / SPT, 2 * SPT) hybrid_fused(Fuse
                     load_spin<N>(w.field, w.n, colour_major(nj, xj, yj, zj, w.half), sj);
                     const uint32_t k = first_draw(kb, nat[u] * w.ndir + rank);
                     ++rank;
-                    if (!wolff_bond_active<N>(w.J, w.beta, w.cw, ri, vdot<N>(sj, r), 0, 0, k)) continue;
+                    if (!vector_bond_active<N>(w.J, w.beta, w.J64, w.beta64, w.err, si, sj, r, k)) continue;
                     if (xj / TX == bx && yj / TY == by && zj / TZ == bz) {
                         tjs[u][d] = ((zj - bz * TZ) * TY + (yj - by * TY)) * TX + (xj - bx * TX);
                         inner[u] |= 1u << d;

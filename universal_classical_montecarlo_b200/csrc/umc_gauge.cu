@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -58,6 +59,9 @@ void gauge_configure(umc_chain* c)
     c->h_inc_cell.resize(cc->c_inc_cell.size());
     for (size_t e = 0; e < cc->c_inc_cell.size(); ++e) c->h_inc_cell[e] = (cc->c_inc_cell[e] << 2) | cc->c_inc_which[e];
     if (!c->h_inc_off.empty() && c->h_inc_off.back() > 0xFFFFFFFFull) throw Error(UMC_ERR_OVERFLOW, "incidence count exceeds uint32");
+    c->max_incident = 0;
+    for (size_t k = 0; k + 1 < c->h_inc_off.size(); ++k)
+        c->max_incident = std::max<uint32_t>(c->max_incident, uint32_t(c->h_inc_off[k + 1] - c->h_inc_off[k]));
     c->J = float(c->desc.coupling);
     c->elem_bytes = 4;
     c->stencil = false;
@@ -158,6 +162,10 @@ void gauge_sweep(umc_chain* c, double beta, double* record)
     a.model_beta = c->J;
     a.driver_beta = float(beta);
     a.width = float(c->desc.width);
+    a.model_beta64 = c->desc.coupling;
+    a.driver_beta64 = beta;
+    a.err = c->N == 1 ? u1_metropolis_err(beta, c->desc.coupling, c->max_incident)
+                      : su_metropolis_err(beta, c->desc.coupling, c->N, c->max_incident);
     const int np = int(c->n_colours) + 1;
     for (uint32_t p = 0; p < c->n_colours; ++p) {
         a.first = uint32_t(c->class_start[p]);

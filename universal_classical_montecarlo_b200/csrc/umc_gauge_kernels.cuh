@@ -416,6 +416,8 @@ struct GaugeArgs
     uint32_t hits;
     float model_beta, driver_beta, width;
     PassOut out;
+    double model_beta64, driver_beta64;  // the couplings of the FP64 decisions
+    float err;                           // u1_metropolis_err / su_metropolis_err
 };
 
 // Key base of hit h of this sweep (the same for every link): the first
@@ -434,7 +436,34 @@ __device__ __forceinline__ uint64_t hit_key(const uint64_t* keys, const GaugeArg
     return h < kHitKeys ? keys[h] : key_base(key_seed(a.seed, a.sweep, tag_site(h)));
 }
 
-static __global__ void __launch_bounds__(kBlock) u1_pass(GaugeArgs a)
+// model_beta sum over link k's cells of cos(theta_p) - cos(theta_p') for the
+// link going from angle t to p, in FP64 on the FP32 angles; the plaquette angle
+// theta0 + theta1 - theta2 - theta3 (dof/u1.hpp:18-21) is +-(theta_k + phi)
+// with phi the sum of the cell's other three links.  Out of line and on plain
+// pointers: it runs only for decisions the FP32 test cannot call.
+__device__ __noinline__ double u1_delta64(const float* f, const uint32_t* inc_off, const uint32_t* inc,
+                                          const uint4* cells, uint32_t k, float t, float p, double model_beta)
+{
+    double d = 0.0;
+    for (uint32_t e = inc_off[k]; e < inc_off[k + 1]; ++e) {
+        const uint32_t w = inc[e];
+        const uint4 c = cells[w >> 2];
+        const double t0 = f[c.x], t1 = f[c.y], t2 = f[c.z], t3 = f[c.w];
+        double phi;
+        switch (w & 3u) {
+        case 0: phi = t1 - t2 - t3; break;
+        case 1: phi = t0 - t2 - t3; break;
+        case 2: phi = t3 - t0 - t1; break;
+        default: phi = t2 - t0 - t1; break;
+        }
+        d += model_beta * (cos(double(t) + phi) - cos(double(p) + phi));
+    }
+    return d;
+}
+
+// (kBlock, 5): at most 48 registers; the out-of-line FP64 decision spills
+// inside itself instead of widening the kernel.
+static __global__ void __launch_bounds__(kBlock, 5) u1_pass(GaugeArgs a)
 {
     __shared__ uint64_t keys[kHitKeys];
     hit_keys_init(keys, a);
@@ -469,7 +498,10 @@ static __global__ void __launch_bounds__(kBlock) u1_pass(GaugeArgs a)
             sincosf(p, &sp, &cp);
             // beta * sum_p (cos theta_p - cos theta_p')
             const float dE = a.model_beta * ((co - cp) * Sr - (so - sp) * Si);
-            if (metropolis_accept(g, -a.driver_beta * dE)) {
+            const bool ok = metropolis_accept(g, -a.driver_beta * dE, a.err, [&] {
+                return -a.driver_beta64 * u1_delta64(a.f, a.inc_off, a.inc, a.cells, k, th, p, a.model_beta64);
+            });
+            if (ok) {
                 th = p;
                 co = cp;
                 so = sp;
@@ -480,6 +512,99 @@ static __global__ void __launch_bounds__(kBlock) u1_pass(GaugeArgs a)
         acc[7] += double(accepted);
     }
     finish_pass<kObs>(acc, a.out);
+}
+
+// FP64 complex N x N matrices for the rare FP64 accept decisions.
+template <int N>
+struct MatD
+{
+    double re[N * N];
+    double im[N * N];
+};
+
+template <int N>
+__device__ __forceinline__ void matd_load(MatD<N>& m, const float* f, uint32_t n, uint32_t k)
+{
+#pragma unroll
+    for (int q = 0; q < N * N; ++q) {
+        m.re[q] = f[(2 * q) * n + k];
+        m.im[q] = f[(2 * q + 1) * n + k];
+    }
+}
+
+template <int N, bool DA, bool DB>
+__device__ __forceinline__ void matd_mul(const MatD<N>& a, const MatD<N>& b, MatD<N>& r)
+{
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            double sr = 0.0, si = 0.0;
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                const int ia = DA ? k * N + i : i * N + k;
+                const int ib = DB ? j * N + k : k * N + j;
+                const double ar = a.re[ia], ai = DA ? -a.im[ia] : a.im[ia];
+                const double br = b.re[ib], bi = DB ? -b.im[ib] : b.im[ib];
+                sr += ar * br - ai * bi;
+                si += ar * bi + ai * br;
+            }
+            r.re[i * N + j] = sr;
+            r.im[i * N + j] = si;
+        }
+}
+
+// Sum over link k's cells of ReTr(U_p) with the plaquette U0 U1 U2^dag U3^dag
+// (dof/sun.hpp:78-84) and link k taken as stored at f[., k], in FP64 on the
+// FP32 links, through each cell's staple.  Out of line and on plain pointers:
+// it runs only for decisions the FP32 test cannot call.
+template <int N>
+__device__ __noinline__ double su_trace64(const float* f, uint32_t n, const uint32_t* inc_off, const uint32_t* inc,
+                                          const uint4* cells, uint32_t k)
+{
+    MatD<N> u;
+    matd_load(u, f, n, k);
+    double tr = 0.0;
+    for (uint32_t e = inc_off[k]; e < inc_off[k + 1]; ++e) {
+        const uint32_t w = inc[e];
+        const uint4 c = cells[w >> 2];
+        MatD<N> x, y, t, b;
+        switch (w & 3u) {
+        case 0:  // B = U1 U2^dag U3^dag
+            matd_load(x, f, n, c.y);
+            matd_load(y, f, n, c.z);
+            matd_mul<N, false, true>(x, y, t);
+            matd_load(x, f, n, c.w);
+            matd_mul<N, false, true>(t, x, b);
+            break;
+        case 1:  // B = U2^dag U3^dag U0
+            matd_load(x, f, n, c.z);
+            matd_load(y, f, n, c.w);
+            matd_mul<N, true, true>(x, y, t);
+            matd_load(x, f, n, c.x);
+            matd_mul<N, false, false>(t, x, b);
+            break;
+        case 2:  // B = U1^dag U0^dag U3
+            matd_load(x, f, n, c.y);
+            matd_load(y, f, n, c.x);
+            matd_mul<N, true, true>(x, y, t);
+            matd_load(x, f, n, c.w);
+            matd_mul<N, false, false>(t, x, b);
+            break;
+        default:  // B = U2 U1^dag U0^dag
+            matd_load(x, f, n, c.z);
+            matd_load(y, f, n, c.y);
+            matd_mul<N, false, true>(x, y, t);
+            matd_load(x, f, n, c.x);
+            matd_mul<N, false, true>(t, x, b);
+            break;
+        }
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int q = 0; q < N; ++q) tr += u.re[i * N + q] * b.re[q * N + i] - u.im[i * N + q] * b.im[q * N + i];
+    }
+    return tr;
 }
 
 template <int N>
@@ -538,7 +663,17 @@ __global__ void __launch_bounds__(kBlock, 3) su_pass(GaugeArgs a)
             su_shift<N>(g, a.width, U, V);
             const float tr_new = re_tr_mul<N>(V, A);
             const float dE = coef * (tr_old - tr_new);
-            if (metropolis_accept(g, -a.driver_beta * dE)) {
+            const bool ok = metropolis_accept(g, -a.driver_beta * dE, a.err, [&] {
+                // link k is read by no other thread of this colour class: it
+                // holds U, then V, while the FP64 traces read it
+                mat_store(U, a.f, a.n, k);
+                const double t_old = su_trace64<N>(a.f, a.n, a.inc_off, a.inc, a.cells, k);
+                mat_store(V, a.f, a.n, k);
+                const double t_new = su_trace64<N>(a.f, a.n, a.inc_off, a.inc, a.cells, k);
+                mat_store(U, a.f, a.n, k);
+                return -a.driver_beta64 * (a.model_beta64 / double(N)) * (t_old - t_new);
+            });
+            if (ok) {
                 U = V;
                 tr_old = tr_new;
                 ++accepted;

@@ -143,6 +143,9 @@ void enqueue_sweeps(umc_u1batch* b, uint64_t n_sweeps, const umc_mlp* net, float
     a.chain_seed = b->seeds.as<unsigned long long>();
     a.model_beta = float(b->desc.beta);
     a.driver_beta = 1.0f;
+    a.model_beta64 = b->desc.beta;
+    a.driver_beta64 = 1.0;
+    a.err = u1_metropolis_err(1.0, b->desc.beta, 2);
     a.width = float(b->desc.width);
     a.img = net ? net->img.as<uint8_t>() : nullptr;
     a.records = b->records.as<double>();

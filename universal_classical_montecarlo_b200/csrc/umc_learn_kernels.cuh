@@ -451,6 +451,28 @@ __device__ __forceinline__ void staple2(const float* th, const Lat2& g, uint32_t
     Si = sA + sB;
 }
 
+// model_beta sum over the link's two cells of cos(theta_p) - cos(theta_p') for
+// the link going from t to p, in FP64 on the FP32 angles (the cells of staple2).
+__device__ __noinline__ double u1_delta2_64(const float* th, const Lat2& g, uint32_t cls, uint32_t q, float t, float p,
+                                            double model_beta)
+{
+    const uint32_t mu = cls >> 1, par = cls & 1u;
+    const uint32_t y = q / g.Lh, j = q - y * g.Lh;
+    const uint32_t x = 2u * j + ((y + par) & 1u);
+    const uint32_t L = g.L;
+    const uint32_t xp = x + 1 == L ? 0u : x + 1, xm = x == 0 ? L - 1 : x - 1;
+    const uint32_t yp = y + 1 == L ? 0u : y + 1, ym = y == 0 ? L - 1 : y - 1;
+    double phA, phB;
+    if (mu == 0) {
+        phA = double(th[g.idx(1, xp, y)]) - double(th[g.idx(0, x, yp)]) - double(th[g.idx(1, x, y)]);
+        phB = double(th[g.idx(1, x, ym)]) - double(th[g.idx(0, x, ym)]) - double(th[g.idx(1, xp, ym)]);
+    } else {
+        phA = double(th[g.idx(0, xm, y)]) - double(th[g.idx(0, xm, yp)]) - double(th[g.idx(1, xm, y)]);
+        phB = double(th[g.idx(0, x, yp)]) - double(th[g.idx(0, x, y)]) - double(th[g.idx(1, xp, y)]);
+    }
+    return model_beta * ((cos(double(t) + phA) - cos(double(p) + phA)) + (cos(double(t) + phB) - cos(double(p) + phB)));
+}
+
 struct U1BatchArgs
 {
     float* theta;                         // n_chains x 2 L^2
@@ -465,6 +487,8 @@ struct U1BatchArgs
     unsigned long long rec_capacity;      // slots (sweeps) in the record buffer
     float* dump;                          // learned: outputs of chain 0, first sweep (2 L^2 x 16)
     unsigned int* status;
+    double model_beta64, driver_beta64;   // plain: the couplings of the FP64 decisions
+    float err;                            // plain: u1_metropolis_err(driver_beta, model_beta, 2)
 };
 
 // Per-sweep observables of the chain in shared memory (all threads call it).
@@ -646,7 +670,10 @@ __global__ void __launch_bounds__(256) u1_plain_batch(U1BatchArgs a)
                     float sp, cp;
                     sincosf(p, &sp, &cp);
                     const float dE = a.model_beta * ((co - cp) * Sr - (so - sp) * Si);
-                    if (metropolis_accept(r, -a.driver_beta * dE)) {
+                    const bool ok = metropolis_accept(r, -a.driver_beta * dE, a.err, [&] {
+                        return -a.driver_beta64 * u1_delta2_64(th, g, cls, q, t, p, a.model_beta64);
+                    });
+                    if (ok) {
                         th[k] = p;
                         acc += 1.0;
                     }

@@ -195,6 +195,9 @@ extern "C" int umc_wolff_flip_noalloc(int32_t model, int32_t components, void* f
         a.flip = flip;
         a.J = float(coupling);
         a.beta = float(beta);
+        a.J64 = coupling;
+        a.beta64 = beta;
+        a.err = vector_wolff_err(beta, coupling, mk == 0 ? 1 : mk);
         if (mk == 0) ising_wolff_thresholds(int32_t(coupling), beta, a.cw);
         a.ctl = &s->ctl;
         a.size_slot = &s->size;

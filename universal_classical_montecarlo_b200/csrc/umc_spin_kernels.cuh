@@ -15,6 +15,8 @@
 // std::log, so Ising chains are bit-exact with the reference driver.
 #pragma once
 
+#include <cmath>
+
 #include "umc_device.cuh"
 
 namespace umc {
@@ -414,12 +416,102 @@ __device__ __forceinline__ float u1_shift(KeyedPcg& g, float width, float cur)
     return remainderf(cur + width * sym_f32(g.next()), 6.283185307179586f);
 }
 
-// Accept test of driver.hpp:39-40 in FP32: the uniform is drawn only when needed,
-// exactly like the reference (the keyed stream makes the skipped draw harmless).
-__device__ __forceinline__ bool metropolis_accept(KeyedPcg& g, float log_p)
+// ------------------------------------ accept and activation decisions in FP64
+
+// N floats by value (arguments of the out-of-line FP64 decisions).
+template <int N>
+struct SpinVal
 {
-    if (log_p >= 0.0f) return true;
-    return u_f32(g.next()) < __expf(log_p);  // log(u) < log_p, monotone-equivalent
+    float v[N];
+};
+
+
+// Metropolis accept (driver.hpp:39-40): log_p >= 0 || log(u) < log_p, with the
+// uniform drawn only when needed, as the reference draws it (the keyed stream
+// makes a skipped draw harmless).  lp is the kernel's FP32 log-ratio and err
+// bounds its distance from lp64(), the same log-ratio recomputed in FP64 from
+// the same FP32 state.  The FP32 test compares u_f32(k) (within 2^-24 of u,
+// relatively) with __expf(lp) (within (2 + 1.173 |lp|) ulps of exp(lp)); with
+// the rounding of the band edge it misplaces log u - log_p by at most
+// err + 2^-23 (3 + 1.2 |lp|).  Outside twice that band the FP32 answer is the
+// FP64 one; inside it lp64() and the FP64 log decide.  So every decision is
+// the reference's FP64 test applied to the kernel's FP32 values.
+template <class F64>
+__device__ __forceinline__ bool metropolis_accept(KeyedPcg& g, float lp, float err, F64&& lp64)
+{
+    const float tol = 2.0f * (err + 0x1.0p-23f * (3.0f + 1.2f * fabsf(lp)));
+    if (lp >= tol) return true;
+    const uint32_t k = g.next();
+    if (lp <= -tol) {
+        const float u = u_f32(k), e = __expf(lp);
+        if (u < e * (1.0f - tol)) return true;
+        if (u > e * (1.0f + tol)) return false;
+    }
+    const double l = lp64();
+    return l >= 0.0 || log(u_f64(k)) < l;
+}
+
+// Wolff bond activation (driver.hpp:151): u < 1 - exp(-x), x = beta dE.  x is
+// the kernel's FP32 value and err bounds its distance from x64(), the same
+// quantity in FP64 from the same FP32 state.  For x >= 0, 1 - __expf(-x) is
+// within err + 2^-23 (3 + 1.2 x) of 1 - exp(-x64) (exp(-x) <= 1 turns the
+// relative error of __expf into an absolute one), and u_f32(k) within 2^-25
+// of u.  Outside twice that band the FP32 comparison decides; inside it x64()
+// and FP64 do.  A negative x never activates: 1 - exp(-x) < 0 <= u.
+template <class F64>
+__device__ __forceinline__ bool wolff_activates(uint32_t k, float x, float err, F64&& x64)
+{
+    const float tol = 2.0f * (err + 0x1.0p-23f * (3.0f + 1.2f * fabsf(x)));
+    if (x <= -tol) return false;
+    if (x >= tol) {
+        const float p = 1.0f - __expf(-x), u = u_f32(k);
+        if (u < p - tol) return true;
+        if (u > p + tol) return false;
+    }
+    return u_f64(k) < 1.0 - exp(-x64());
+}
+
+// Error bounds (in units of log_p, resp. x) of the FP32 forms below, for the
+// host to pass with each launch.  u = 2^-24; spins are unit vectors, so every
+// component and every neighbour term is at most 1 in magnitude.
+//  * VectorSpin<N> Metropolis over deg neighbours: h_c sums deg terms
+//    ((deg - 1) deg u), each dot takes N fused products (N sqrt(N) deg u),
+//    their difference, J, beta and the FP32 beta add 3 u |lp| <= 6 u beta |J|
+//    sqrt(N) deg:  beta |J| u sqrt(N) deg (2 (N + deg - 1) + 8).
+//  * Wolff on VectorSpin<N>: x = 2 beta J (r.s_i)(r.s_j), each dot within N u,
+//    three products and the FP32 beta: beta |J| u (4 N + 8).
+inline float vector_metropolis_err(double beta, double J, int N, uint32_t deg)
+{
+    return float(std::fabs(beta * J) * 0x1.0p-24 * std::sqrt(double(N)) * double(deg) * (2.0 * (N + deg - 1.0) + 8.0));
+}
+inline float vector_wolff_err(double beta, double J, int N)
+{
+    return float(std::fabs(beta * J) * 0x1.0p-24 * (4.0 * N + 8.0));
+}
+// XY on angles over deg neighbours with __sincosf (each value within 2^-18 of
+// the exact one, generously, for angles within a few pi of zero):
+// beta |J| deg 2^-18 10.
+inline float xy_metropolis_err(double beta, double J, uint32_t deg)
+{
+    return float(std::fabs(beta * J) * double(deg) * 0x1.0p-18 * 10.0);
+}
+// The gauge passes (umc_gauge_kernels.cuh, and the plain batched U(1) chains),
+// deg = cells per link:
+//  * U(1): a cell's staple angle sums three FP32 angles of at most 2 pi
+//    (38 u), sincosf adds 2 u, deg of them make Sr and Si; with the old and
+//    new cos/sin and the products: driver_beta model_beta u deg (4 (40 + deg) + 24).
+//  * SU(N): every entry of a product of two (near-)unitary FP32 matrices is
+//    within 4 N u; a staple sums deg products of three; ReTr(U A) adds N^2
+//    products; tr_old and tr_new both: driver_beta (model_beta / N) u
+//    (4 N^2 deg + 2 N deg (8 N + deg) + 16).
+inline float u1_metropolis_err(double driver_beta, double model_beta, uint32_t deg)
+{
+    return float(std::fabs(driver_beta * model_beta) * 0x1.0p-24 * double(deg) * (4.0 * (40.0 + deg) + 24.0));
+}
+inline float su_metropolis_err(double driver_beta, double model_beta, int N, uint32_t deg)
+{
+    const double n = N, d = deg;
+    return float(std::fabs(driver_beta * model_beta / n) * 0x1.0p-24 * (4.0 * n * n * d + 2.0 * n * d * (8.0 * n + d) + 16.0));
 }
 
 // ------------------------------------------------------ VectorSpin<N> pass
@@ -434,10 +526,34 @@ struct VecArgs
     uint64_t kbase;
     float J, beta, delta;
     PassOut out;
+    double J64, beta64;  // the coupling and beta of the FP64 decisions
+    float err;           // vector_metropolis_err
 };
 
+// -beta dE of site k taking cand (energy_diff_at, example/vector_spin.hpp:50-60:
+// sum over bonds of -J (cand.s_j - s.s_j)) in FP64 on the FP32 state.  Out of
+// line: it runs only for decisions the FP32 test cannot call.
+template <int N, class Topo>
+__device__ __noinline__ double vector_log_ratio64(const VecArgs& a, Topo t, uint32_t k, SpinVal<N> cand, SpinVal<N> s)
+{
+    double d = 0.0;
+    t.neighbours(k, [&](uint32_t j, bool) {
+        double pj = 0.0, oj = 0.0;
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+            const double v = a.f[c * a.n + j];
+            pj += double(cand.v[c]) * v;
+            oj += double(s.v[c]) * v;
+        }
+        d += -a.J64 * (pj - oj);
+    });
+    return -a.beta64 * d;
+}
+
+// (kBlock, 4): at most 64 registers, the occupancy of the FP32 path; the
+// out-of-line FP64 decision spills inside itself instead of widening it.
 template <int N, int PROP, class Topo>
-__global__ void __launch_bounds__(kBlock) vector_pass(VecArgs a, Topo t)
+__global__ void __launch_bounds__(kBlock, 4) vector_pass(VecArgs a, Topo t)
 {
     double acc[kObs] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < a.count; q += gridDim.x * blockDim.x) {
@@ -466,7 +582,15 @@ __global__ void __launch_bounds__(kBlock) vector_pass(VecArgs a, Topo t)
         if (ok) {
             // energy_diff_at, example/vector_spin.hpp:50-60: -J (p.h - s.h)
             const float dE = -a.J * (vdot<N>(cand, h) - vdot<N>(s, h));
-            acc_ok = metropolis_accept(g, -a.beta * dE);
+            acc_ok = metropolis_accept(g, -a.beta * dE, a.err, [&] {
+                SpinVal<N> cv, sv;
+#pragma unroll
+                for (int c = 0; c < N; ++c) {
+                    cv.v[c] = cand[c];
+                    sv.v[c] = s[c];
+                }
+                return vector_log_ratio64<N>(a, t, k, cv, sv);
+            });
         }
         if (acc_ok) {
 #pragma unroll
@@ -494,10 +618,28 @@ struct XYArgs
     uint64_t kbase;
     float J, beta, width;
     PassOut out;
+    double J64, beta64;  // the coupling and beta of the FP64 decisions
+    float err;           // xy_metropolis_err
 };
 
+// -beta dE of angle site k going from t0 to p: -J sum_j (cos(p - t_j) -
+// cos(t0 - t_j)) (PairModel with the XY term, model/pair.hpp:53-64), in FP64 on
+// the FP32 angles.  Out of line: it runs only for decisions the FP32 test
+// cannot call.
 template <class Topo>
-__global__ void __launch_bounds__(kBlock) xy_pass(XYArgs a, Topo t)
+__device__ __noinline__ double xy_log_ratio64(const XYArgs& a, Topo t, uint32_t k, float t0, float p)
+{
+    double d = 0.0;
+    t.neighbours(k, [&](uint32_t j, bool) {
+        const double tj = a.th[j];
+        d += -a.J64 * (cos(double(p) - tj) - cos(double(t0) - tj));
+    });
+    return -a.beta64 * d;
+}
+
+// (kBlock, 5): at most 48 registers (see vector_pass).
+template <class Topo>
+__global__ void __launch_bounds__(kBlock, 5) xy_pass(XYArgs a, Topo t)
 {
     double acc[kObs] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < a.count; q += gridDim.x * blockDim.x) {
@@ -518,7 +660,7 @@ __global__ void __launch_bounds__(kBlock) xy_pass(XYArgs a, Topo t)
         __sincosf(th, &so, &co);
         __sincosf(p, &sp, &cp);
         const float dE = -a.J * ((cp - co) * C + (sp - so) * S);
-        const bool ok = metropolis_accept(g, -a.beta * dE);
+        const bool ok = metropolis_accept(g, -a.beta * dE, a.err, [&] { return xy_log_ratio64(a, t, k, th, p); });
         if (ok) {
             a.th[k] = p;
             th = p;
@@ -603,23 +745,57 @@ struct WolffArgs
     unsigned long long cw[2];  // Ising: activate iff draw < cw[s_i s_j > 0]
     DevCtl* ctl;
     unsigned long long* size_slot;
+    double J64, beta64;  // VectorSpin: the coupling and beta of the FP64 decisions
+    float err;           // VectorSpin: vector_wolff_err
 };
 
 // Activation of one bond (driver.hpp:150-151): uni() < 1 - exp(-beta dE).
 // The reference's energy_diff_bond, -J (nb.s_i - s_j.s_i) with the reflected
 // nb = s_j - 2 (s_j.r) r, equals 2 J (r.s_i)(r.s_j); that symmetric form is
-// used so the decision does not depend on which end reaches the bond first.
-// Ising compares the draw with integer thresholds (exact); ri, rj unused.
-template <int MODEL>
-__device__ __forceinline__ bool wolff_bond_active(float J, float beta, const unsigned long long* cw, float ri, float rj,
-                                                  int si, int sj, uint32_t k)
+// used in FP32 so the decision does not depend on which end reaches the bond
+// first.  Near the threshold the reference's own form decides in FP64
+// (wolff_activates), on the FP32 spins and axis, and is symmetric to within
+// 1e-16.  Ising compares the draw with integer thresholds (exact).
+__device__ __forceinline__ bool ising_bond_active(const unsigned long long* cw, int si, int sj, uint32_t k)
 {
-    if constexpr (MODEL == 0) {
-        return uint64_t(k) < cw[si * sj > 0 ? 1 : 0];
-    } else {
-        const float dE = 2.0f * J * (ri * rj);
-        return u_f32(k) < 1.0f - __expf(-beta * dE);
+    return uint64_t(k) < cw[si * sj > 0 ? 1 : 0];
+}
+
+// beta dE of bond (i, j) with s_j reflected: energy_diff_bond
+// (example/vector_spin.hpp:62-68) with nb = s_j - 2 (s_j.r) r (driver.hpp:
+// 142-146), in FP64 on the FP32 spins and axis.  Out of line: it runs only for
+// decisions the FP32 test cannot call.
+template <int N>
+__device__ __noinline__ double vector_bond_x64(SpinVal<N> si, SpinVal<N> sj, SpinVal<N> r, double J64, double beta64)
+{
+    double d = 0.0;
+#pragma unroll
+    for (int c = 0; c < N; ++c) d += double(sj.v[c]) * double(r.v[c]);
+    double pn = 0.0, po = 0.0;
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+        const double nb = double(sj.v[c]) - 2.0 * d * double(r.v[c]);
+        pn += nb * double(si.v[c]);
+        po += double(sj.v[c]) * double(si.v[c]);
     }
+    return beta64 * (-J64 * (pn - po));
+}
+
+template <int N>
+__device__ __forceinline__ bool vector_bond_active(float J, float beta, double J64, double beta64, float err,
+                                                   const float* si, const float* sj, const float* r, uint32_t k)
+{
+    const float x = beta * (2.0f * J * (vdot<N>(si, r) * vdot<N>(sj, r)));
+    return wolff_activates(k, x, err, [&] {
+        SpinVal<N> a, b, c;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            a.v[q] = si[q];
+            b.v[q] = sj[q];
+            c.v[q] = r[q];
+        }
+        return vector_bond_x64<N>(a, b, c, J64, beta64);
+    });
 }
 
 // Axis and seed site of one flip (driver.hpp:110-115), from the axis key.
@@ -632,8 +808,9 @@ __device__ __forceinline__ uint32_t wolff_axis(const WolffArgs& a, float* r)
     return uint32_t(u_f64(g.next()) * double(a.n));  // same double product as the reference
 }
 
+// (kBlock, 8): at most 32 registers (see vector_pass).
 template <int MODEL>
-__global__ void __launch_bounds__(kBlock) wolff_union(WolffArgs a)
+__global__ void __launch_bounds__(kBlock, 8) wolff_union(WolffArgs a)
 {
     constexpr int N = MODEL == 0 ? 1 : MODEL;
     __shared__ float r_sh[4];
@@ -657,14 +834,13 @@ __global__ void __launch_bounds__(kBlock) wolff_union(WolffArgs a)
                 const uint32_t j = a.adj[q];
                 if (j <= i) continue;
                 const uint32_t k = first_draw(kb, a.slot[q]);
-                if (wolff_bond_active<0>(a.J, a.beta, a.cw, 0.f, 0.f, si, s[j], k)) uf_union(a.lab, i, j, a.n + 1, &a.ctl->status);
+                if (ising_bond_active(a.cw, si, s[j], k)) uf_union(a.lab, i, j, a.n + 1, &a.ctl->status);
             }
         } else {
             const float* f = static_cast<const float*>(a.field);
             float si[N];
 #pragma unroll
             for (int c = 0; c < N; ++c) si[c] = f[c * a.n + i];
-            const float ri = vdot<N>(si, r);
             for (uint32_t q = a0; q < a1; ++q) {
                 const uint32_t j = a.adj[q];
                 if (j <= i) continue;
@@ -672,7 +848,7 @@ __global__ void __launch_bounds__(kBlock) wolff_union(WolffArgs a)
 #pragma unroll
                 for (int c = 0; c < N; ++c) t[c] = f[c * a.n + j];
                 const uint32_t k = first_draw(kb, a.slot[q]);
-                if (wolff_bond_active<MODEL>(a.J, a.beta, a.cw, ri, vdot<N>(t, r), 0, 0, k))
+                if (vector_bond_active<N>(a.J, a.beta, a.J64, a.beta64, a.err, si, t, r, k))
                     uf_union(a.lab, i, j, a.n + 1, &a.ctl->status);
             }
         }

@@ -35,6 +35,8 @@ struct WolffTileArgs
     unsigned long long cw[2];
     DevCtl* ctl;
     unsigned long long* size_slot;
+    double J64, beta64;  // VectorSpin: the coupling and beta of the FP64 decisions
+    float err;           // VectorSpin: vector_wolff_err
 };
 
 __device__ __forceinline__ uint32_t colour_major(uint32_t nat, uint32_t x, uint32_t y, uint32_t z, uint32_t half)
@@ -85,8 +87,10 @@ __device__ __forceinline__ void smem_union(uint32_t* lab, uint32_t a, uint32_t b
     atomicOr(status, kDevErrUnionFind);
 }
 
+// (512 threads, 4 blocks): at most 32 registers; the out-of-line FP64
+// activation test spills inside itself instead of widening the kernel.
 template <int MODEL, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX * TY * TZ) wolff_tile_local(WolffTileArgs a)
+__global__ void __launch_bounds__(TX * TY * TZ, 65536 / (32 * TX * TY * TZ)) wolff_tile_local(WolffTileArgs a)
 {
     constexpr int N = MODEL == 0 ? 1 : MODEL;
     constexpr int T = TX * TY * TZ;
@@ -118,7 +122,6 @@ __global__ void __launch_bounds__(TX * TY * TZ) wolff_tile_local(WolffTileArgs a
         nat = (z * a.Ly + y) * a.Lx + x;
         float si[N];
         load_spin<MODEL>(a.field, a.n, colour_major(nat, x, y, z, a.half), si);
-        const float ri = MODEL == 0 ? 0.f : vdot<N>(si, r);
         uint32_t rank = 0;
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -133,8 +136,10 @@ __global__ void __launch_bounds__(TX * TY * TZ) wolff_tile_local(WolffTileArgs a
             load_spin<MODEL>(a.field, a.n, colour_major(nj, xj, yj, zj, a.half), sj);
             const uint32_t k = first_draw(kb, nat * a.ndir + rank);
             ++rank;
-            const float rj = MODEL == 0 ? 0.f : vdot<N>(sj, r);
-            if (!wolff_bond_active<MODEL>(a.J, a.beta, a.cw, ri, rj, int(si[0]), int(sj[0]), k)) continue;
+            bool on;
+            if constexpr (MODEL == 0) on = ising_bond_active(a.cw, int(si[0]), int(sj[0]), k);
+            else on = vector_bond_active<N>(a.J, a.beta, a.J64, a.beta64, a.err, si, sj, r, k);
+            if (!on) continue;
             const bool same = xj / TX == bx && yj / TY == by && zj / TZ == bz;
             if (same) {
                 const uint32_t tj = ((zj - bz * TZ) * TY + (yj - by * TY)) * TX + (xj - bx * TX);
