@@ -10,6 +10,9 @@
 //                   (a PairModel is a WolffModel, driver.hpp:69-83);
 //   IsingBondTerm + UpAxis -- the Ising pair term in int32 with FixedAxis,
 //                   driven by Wolff;
+//   WeightedIsing -- the reference graph test's IsingGraph: double spins and
+//                   a coupling carried by every bond (PairGraph<double>),
+//                   under Metropolis (FlipDouble) and Wolff (UnitAxis);
 //   CubicHeisenberg -- a whole ModelLike (model.hpp:65-88) for the periodic
 //                   cubic O(3) model whose neighbours come from the site index,
 //                   with no bond table at all;
@@ -22,7 +25,8 @@
 //
 // Exported with a C ABI for the Python tests and bench.py (ctypes): one-shot
 // runs (um_xy_pair, um_xy_record, um_u1_cells, um_plaquette_u1, um_su2_2d,
-// um_heisenberg_cubic, um_o3_wolff, um_ising_wolff, um_lattice_o3) and persistent sessions (um_session_*) whose
+// um_heisenberg_cubic, um_o3_wolff, um_ising_wolff, um_weighted_ising, um_lattice_o3) and persistent
+// sessions (um_session_*) whose
 // launches bench.py times.
 #include <umc/device.cuh>
 
@@ -72,6 +76,69 @@ struct UpAxis
     UMC_HD void sample(const std::int8_t*, R&, std::int8_t* out) const
     {
         out[0] = 1;
+    }
+};
+
+// The weighted Ising model of the reference's graph test (test/graph_check.cpp:
+// 34-83, IsingGraph): double spins, E = -sum over bonds of c s_i s_j with the
+// coupling c carried by each bond of a PairGraph<double>.  A whole ModelLike
+// and WolffModel over the weighted device rows (BondTables<double>::rows()):
+// random-bond and weighted Ising models drop in this way.
+struct WeightedIsing
+{
+    using value_type = double;
+    static constexpr std::size_t size = 1;
+    using bond_type = BondOf<double>;
+
+    double* spin;
+    PairRows<double> graph;
+
+    UMC_HD std::size_t sites() const { return graph.sites(); }
+    UMC_HD const double* data() const { return spin; }
+    UMC_HD double* data() { return spin; }
+    UMC_HD std::size_t degree(std::size_t i) const { return graph.degree(i); }
+    UMC_HD const bond_type* bonds(std::size_t i) const { return graph.bonds(i); }
+    UMC_HD std::uint32_t bond_id(std::size_t i, std::size_t a) const { return graph.bond_id(i, a); }
+
+    UMC_HD double energy_at(std::size_t i) const
+    {
+        double e = 0.0;
+        const bond_type* bs = graph.bonds(i);
+        for (std::size_t a = 0; a < graph.degree(i); ++a) e += -bs[a].c * spin[i] * spin[bs[a].j];
+        return e;
+    }
+    UMC_HD double energy_diff_at(std::size_t i, const double* p) const
+    {
+        double d = 0.0;
+        const bond_type* bs = graph.bonds(i);
+        for (std::size_t a = 0; a < graph.degree(i); ++a) d += -bs[a].c * (*p - spin[i]) * spin[bs[a].j];
+        return d;
+    }
+    UMC_HD double energy_diff_bond(std::size_t i, const bond_type& b, const double* p) const
+    {
+        return -b.c * (*p - spin[b.j]) * spin[i];
+    }
+    UMC_HD void update(std::size_t i, const double* p) { spin[i] = *p; }
+};
+
+// The graph test's own Flip on double spins (test/graph_check.cpp:15-24) and
+// its fixed reflection axis r = 1 (:27-32).
+struct FlipDouble
+{
+    template <class R>
+    UMC_HD void sample(const double* cur, R&, double* out) const
+    {
+        *out = *cur > 0.0 ? -1.0 : 1.0;
+    }
+    UMC_HD double log_ratio(const double*, const double*) const { return 0.0; }
+};
+
+struct UnitAxis
+{
+    template <class R>
+    UMC_HD void sample(const double*, R&, double* out) const
+    {
+        out[0] = 1.0;
     }
 };
 
@@ -474,6 +541,44 @@ int um_ising_wolff(const umc_graph* g, std::int32_t J, double beta, std::uint64_
         W w = tiled ? W(model, UpAxis{}, t, seed, beta) : W(model, UpAxis{}, seed, beta);
         w.set_flips(flip0);
         w.flips(n, sizes);
+        t.download(field, spins, 1);
+    });
+}
+
+// The weighted Ising model (WeightedIsing, FlipDouble, UnitAxis) on a library
+// pair graph built with a double payload per bond (the coupling): wolff == 0,
+// n Metropolis sweeps from sweep `first`, energies[k] = E after sweep k (may be
+// NULL); wolff == 1, n Wolff flips from flip `first`, their sizes to `sizes`
+// and E after each to `energies` (either may be NULL).  tiled: the Wolff
+// driver gets the tables (shared-memory tile labelling).  spins (sites, site
+// order) in/out.
+int um_weighted_ising(const umc_graph* g, double beta, std::uint64_t seed, std::uint64_t first, std::uint32_t n,
+                      int wolff, int tiled, double* spins, double* energies, std::uint64_t* sizes)
+{
+    return guarded([&] {
+        BondTables<double> t(g);
+        Buffer<double> field(t.sites());
+        t.upload(field, spins, 1);
+        WeightedIsing model{field.data(), t.rows()};
+        if (wolff) {
+            using W = Wolff<WeightedIsing, UnitAxis>;
+            W w = tiled ? W(model, UnitAxis{}, t, seed, beta) : W(model, UnitAxis{}, seed, beta);
+            w.set_flips(first);
+            for (std::uint32_t k = 0; k < n; ++k) {
+                std::uint64_t sz = 0;
+                w.flips(1, &sz);
+                if (sizes) sizes[k] = sz;
+                if (energies) energies[k] = 0.5 * w.energy_at_sum();
+            }
+        } else {
+            Metropolis<WeightedIsing, FlipDouble> mc(model, FlipDouble{}, t.classes(), seed, beta);
+            mc.set_sweeps(first);
+            std::uint32_t k = 0;
+            mc.sample(n, [&](const auto& m) {
+                if (energies) energies[k] = 0.5 * m.energy_at_sum();
+                ++k;
+            });
+        }
         t.download(field, spins, 1);
     });
 }

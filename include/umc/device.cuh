@@ -598,6 +598,76 @@ private:
     Buffer<std::uint32_t> offset_, bonds_;
 };
 
+// One entry of a bond row with a payload: PairGraph's Bond<P> (lattice/
+// pair_graph.hpp:16-22) on the device, the neighbour's device index and the
+// bond's payload c (a coupling, for instance).
+template <class P>
+struct BondOf
+{
+    std::uint32_t j;
+    P c;
+};
+
+// A PairGraphLike view of a weighted graph on the device (lattice/
+// pair_graph.hpp:86-116): sites(), degree(i), bonds(i) over rows of BondOf<P>
+// in the colour-major device numbering, and bond_id(i, a), the key of the
+// a-th bond of i's row (its CSR slot).  Trivially copyable: a user model
+// holds one as a member, as the reference's models hold their PairGraph.
+template <class P>
+struct PairRows
+{
+    using bond_type = BondOf<P>;
+    const std::uint32_t* offset;  // sites + 1
+    const BondOf<P>* row;         // offset[sites]
+    std::uint32_t n;
+
+    UMC_HD std::size_t sites() const { return n; }
+    UMC_HD std::size_t degree(std::size_t i) const { return offset[i + 1] - offset[i]; }
+    UMC_HD const BondOf<P>* bonds(std::size_t i) const { return row + offset[i]; }
+    UMC_HD std::uint32_t bond_id(std::size_t i, std::size_t a) const { return offset[i] + std::uint32_t(a); }
+};
+
+// PairTables plus each slot's payload: the CSR of a PairGraph<P> built with a
+// payload (umc_graph_create_payload, or the facade's PairGraph<P>) in the
+// colour-major device numbering, slot for slot the rows of PairTables, each
+// bond carrying the payload the reference copies into it from its Edge.
+// rows() is the device view a weighted user model reads; the rest (classes,
+// upload/download, the Wolff tiles) is PairTables'.
+template <class P>
+class BondTables : public PairTables
+{
+    static_assert(std::is_trivially_copyable_v<P>, "a bond payload must be trivially copyable");
+
+public:
+    explicit BondTables(const umc_graph* g) : PairTables(g)
+    {
+        if (umc_graph_payload_bytes(g) != sizeof(P))
+            throw std::invalid_argument("BondTables<P>: the graph's payload size differs from sizeof(P)");
+        const std::uint32_t n = sites();
+        const std::size_t m = umc_graph_slots(g);
+        std::vector<std::uint32_t> off(std::size_t(n) + 1), bonds(m);
+        umc_check(umc_graph_csr(g, off.data(), bonds.data()));
+        std::vector<P> pay(m);
+        if (m) umc_check(umc_graph_payloads(g, pay.data()));
+        std::vector<std::uint32_t> doff(std::size_t(n) + 1, 0);
+        std::vector<BondOf<P>> rows(m);
+        for (std::uint32_t k = 0; k < n; ++k) {
+            const std::uint32_t i = order()[k];
+            std::uint32_t w = doff[k];
+            for (std::uint32_t a = off[i]; a < off[i + 1]; ++a, ++w) rows[w] = BondOf<P>{position()[bonds[a]], pay[a]};
+            doff[k + 1] = w;
+        }
+        woffset_ = Buffer<std::uint32_t>(doff);
+        wrows_ = Buffer<BondOf<P>>(rows);
+    }
+
+    PairRows<P> rows() const noexcept { return PairRows<P>{woffset_.data(), wrows_.data(), sites()}; }
+
+private:
+    Buffer<std::uint32_t> woffset_;
+    Buffer<BondOf<P>> wrows_;
+};
+
 // A cell complex in the colour-major device numbering: cell c lists its
 // sites' device indices; incidence row k is that of site order[k].
 class CellTables : public ColourMajor

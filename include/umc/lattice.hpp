@@ -9,6 +9,7 @@
 #include <concepts>
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <memory>
 #include <span>
 #include <stdexcept>
@@ -29,10 +30,16 @@ struct Bond
     [[no_unique_address]] P c;
 };
 
+// P is the per-bond payload (lattice/pair_graph.hpp:13-22): NoPayload, or a
+// trivially copyable record of at most UMC_MAX_PAYLOAD_BYTES bytes (a coupling,
+// a vector of couplings, ...) that the engine keeps beside the CSR and hands
+// to device code (umc/device.cuh BondTables<P>).
 template <class P = NoPayload>
 class PairGraph
 {
-    static_assert(std::is_same_v<P, NoPayload>, "the device engine supports unweighted graphs (NoPayload)");
+    static_assert(std::is_same_v<P, NoPayload> ||
+                      (std::is_trivially_copyable_v<P> && sizeof(P) <= UMC_MAX_PAYLOAD_BYTES),
+                  "a bond payload must be trivially copyable and at most UMC_MAX_PAYLOAD_BYTES bytes");
 
 public:
     using bond_type = Bond<P>;
@@ -46,7 +53,8 @@ public:
 
     PairGraph() = default;
 
-    // Same rules and exceptions as the reference constructor.
+    // Same rules and exceptions as the reference constructor; c is copied into
+    // both directed entries when symmetric.
     PairGraph(std::size_t n, std::span<const Edge> edges, bool symmetric = true)
     {
         std::vector<std::uint32_t> ei(edges.size()), ej(edges.size());
@@ -55,7 +63,14 @@ public:
             ej[k] = edges[k].j;
         }
         umc_graph* g = nullptr;
-        detail::check(umc_graph_create(n, ei.data(), ej.data(), edges.size(), symmetric ? 1 : 0, &g));
+        if constexpr (std::is_same_v<P, NoPayload>) {
+            detail::check(umc_graph_create(n, ei.data(), ej.data(), edges.size(), symmetric ? 1 : 0, &g));
+        } else {
+            std::vector<unsigned char> blob(edges.size() * sizeof(P));
+            for (std::size_t k = 0; k < edges.size(); ++k) std::memcpy(blob.data() + k * sizeof(P), &edges[k].c, sizeof(P));
+            detail::check(umc_graph_create_payload(n, ei.data(), ej.data(), edges.size(), symmetric ? 1 : 0,
+                                                   blob.data(), std::uint32_t(sizeof(P)), &g));
+        }
         adopt(g);
     }
 
@@ -85,6 +100,12 @@ private:
         detail::check(umc_graph_csr(g, offset_.data(), b.data()));
         bonds_.resize(m);
         for (std::size_t k = 0; k < m; ++k) bonds_[k] = bond_type{b[k], {}};
+        if constexpr (!std::is_same_v<P, NoPayload>) {
+            if (umc_graph_payload_bytes(g) != sizeof(P)) throw std::invalid_argument("PairGraph: payload size differs");
+            std::vector<unsigned char> blob(m * sizeof(P));
+            if (m) detail::check(umc_graph_payloads(g, blob.data()));
+            for (std::size_t k = 0; k < m; ++k) std::memcpy(&bonds_[k].c, blob.data() + k * sizeof(P), sizeof(P));
+        }
     }
 
     std::shared_ptr<umc_graph> g_;

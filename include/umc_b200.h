@@ -63,6 +63,26 @@ typedef struct umc_graph umc_graph;
  * endpoints >= n rejected (OUT_OF_RANGE), n or 2E beyond uint32 (OVERFLOW). */
 int umc_graph_create(uint64_t n_sites, const uint32_t* edge_i, const uint32_t* edge_j,
                      uint64_t n_edges, int symmetric, umc_graph** out);
+/* PairGraph<P>(n, edges, symmetric) with a per-bond payload -- lattice/
+ * pair_graph.hpp:13-83 (Bond<P>::c, Edge::c): edge e's payload is the
+ * payload_bytes record at payload + e * payload_bytes (a trivially copyable P,
+ * 1 to UMC_MAX_PAYLOAD_BYTES bytes), copied into both directed slots as the
+ * reference copies Edge::c.  Same checks and errors as umc_graph_create.  The
+ * built-in models take NoPayload graphs only (as the reference's Ising and
+ * VectorSpin take PairGraph<>); weighted models are user models over the
+ * device tables (umc/device.cuh BondTables<P>). */
+#define UMC_MAX_PAYLOAD_BYTES 256
+int umc_graph_create_payload(uint64_t n_sites, const uint32_t* edge_i, const uint32_t* edge_j,
+                             uint64_t n_edges, int symmetric, const void* payload, uint32_t payload_bytes,
+                             umc_graph** out);
+/* Bytes per payload record; 0 for a NoPayload graph. */
+uint32_t umc_graph_payload_bytes(const umc_graph* g);
+/* Bond<P>::c of every CSR slot (lattice/pair_graph.hpp:98-102), in the slot
+ * order of umc_graph_csr: slots x payload_bytes bytes. */
+int umc_graph_payloads(const umc_graph* g, void* out);
+/* The input edge of every CSR slot (slots entries): the reference fills rows
+ * in edge order, so this maps bonds(i)[a] back to its Edge. */
+int umc_graph_slot_edges(const umc_graph* g, uint32_t* out);
 /* square_lattice(Lx, Ly) -- lattice/square.hpp:15-38. */
 int umc_graph_square(uint64_t Lx, uint64_t Ly, umc_graph** out);
 /* Periodic Lx*Ly*Lz cubic lattice with square_lattice's conventions (site

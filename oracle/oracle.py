@@ -114,6 +114,10 @@ class Oracle:
                                _f64, _u64, _u64, _u64, _vp, _vp, _vp)
         self._vec_wolff = L.fn("vector_wolff", None, _u32, _u64, _vp, _vp, _vp, _f64, _f64, _u64,
                                _u64, _u64, _vp, _vp, _vp, _vp)
+        self._wising_metro = L.fn("weighted_ising_metropolis", None, _u64, _vp, _vp, _vp, _f64, _u64, _u64, _u64,
+                                  _vp, _vp, _vp)
+        self._wising_wolff = L.fn("weighted_ising_wolff", None, _u64, _vp, _vp, _vp, _vp, _f64, _u64, _u64, _u64,
+                                  _vp, _vp, _vp)
         self._xy_metro = L.fn("xy_metropolis", None, _u64, _vp, _vp, _f64, _f64, _f64, _u64, _u64,
                               _u64, _vp, _vp, _vp)
         self._u1_metro = L.fn("u1_metropolis", None, _u64, _vp, _u64, _vp, _vp, _vp, _f64, _f64,
@@ -242,6 +246,28 @@ class Oracle:
         self._ising_wolff(len(s), _ptr(offset), _ptr(bonds), _ptr(slot_edge), J, beta, seed, flip0,
                           n_flips, _ptr(s), _ptr(sizes), _ptr(E), _ptr(M))
         return s, sizes, E, M
+
+    # ---- weighted Ising (test/graph_check.cpp's IsingGraph on PairGraph<double>)
+    def weighted_ising_metropolis(self, offset, bonds, c, beta, seed, sweep0, n_sweeps, spins):
+        """c: the coupling of every CSR slot.  Returns spins, E per sweep and
+        the last sweep's accept margins log(u) - log_p."""
+        s = np.array(spins, np.float64, copy=True)
+        c = np.ascontiguousarray(c, np.float64)
+        E = np.zeros(n_sweeps)
+        margin = np.zeros(len(s))
+        self._wising_metro(len(s), _ptr(offset), _ptr(bonds), _ptr(c), beta, seed, sweep0, n_sweeps, _ptr(s),
+                           _ptr(E), _ptr(margin))
+        return s, E, margin
+
+    def weighted_ising_wolff(self, offset, bonds, key, c, beta, seed, flip0, n_flips, spins):
+        s = np.array(spins, np.float64, copy=True)
+        c = np.ascontiguousarray(c, np.float64)
+        key = np.ascontiguousarray(key, np.uint32)
+        sizes = np.zeros(n_flips, np.uint64)
+        E = np.zeros(n_flips)
+        self._wising_wolff(len(s), _ptr(offset), _ptr(bonds), _ptr(key), _ptr(c), beta, seed, flip0, n_flips,
+                           _ptr(s), _ptr(sizes), _ptr(E))
+        return s, sizes, E
 
     # ---- VectorSpin
     def vector_metropolis(self, N, offset, bonds, J, beta, proposal, delta, seed, sweep0, n_sweeps, spins):
@@ -436,6 +462,10 @@ class Reference:
         self._su_expm = L.fn("su_expm", None, _u32, _vp, _vp)
         self._su_shift = L.fn("su_shift", None, _u32, _f64, _u64, _u64, _u32, _u32, _vp, _vp)
         self._bench_o3 = L.fn("bench_o3", _int, _u64, _f64, _u64, _u64, _u32, _u64, _vp, _vp)
+        self._wising_metro = L.fn("weighted_ising_metropolis", _int, _u64, _vp, _vp, _vp, _u64, _f64, _u64, _u64,
+                                  _u64, _vp, _vp)
+        self._wising_wolff = L.fn("weighted_ising_wolff", _int, _u64, _vp, _vp, _vp, _u64, _vp, _f64, _u64, _u64,
+                                  _u64, _vp, _vp, _vp)
         self._stock_o3 = L.fn("stock_o3_chain", _int, _u64, _f64, _u64, _u64, _u64, _vp)
         self._stock_o3_multi = L.fn("stock_o3_chains", _int, _u64, _f64, _u64, _u32, _vp, _u64, _u64, _vp)
         self._stock_su3 = L.fn("stock_su3_chain", _int, _u64, _f64, _f64, _u64, _u32, _u64, _u64, _vp)
@@ -596,6 +626,33 @@ class Reference:
         out = np.zeros((N, N), np.complex128)
         self._su_shift(N, width, seed, counter, tag, id_, _ptr(cur), _ptr(out))
         return out
+
+    def weighted_ising_metropolis(self, n, ei, ej, c, beta, seed, sweep0, n_sweeps, spins):
+        """The reference Metropolis on the weighted Ising model of
+        test/graph_check.cpp (c: per-edge couplings): spins and E per sweep."""
+        ei = np.ascontiguousarray(ei, np.uint32)
+        ej = np.ascontiguousarray(ej, np.uint32)
+        c = np.ascontiguousarray(c, np.float64)
+        s = np.array(spins, np.float64, copy=True)
+        E = np.zeros(n_sweeps)
+        st = self._wising_metro(n, _ptr(ei), _ptr(ej), _ptr(c), len(ei), beta, seed, sweep0, n_sweeps, _ptr(s),
+                                _ptr(E))
+        assert st == 0, st
+        return s, E
+
+    def weighted_ising_wolff(self, n, ei, ej, c, key, beta, seed, flip0, n_flips, spins):
+        """The reference Wolff on the weighted Ising model; key: per CSR slot."""
+        ei = np.ascontiguousarray(ei, np.uint32)
+        ej = np.ascontiguousarray(ej, np.uint32)
+        c = np.ascontiguousarray(c, np.float64)
+        key = np.ascontiguousarray(key, np.uint32)
+        s = np.array(spins, np.float64, copy=True)
+        sizes = np.zeros(n_flips, np.uint64)
+        E = np.zeros(n_flips)
+        st = self._wising_wolff(n, _ptr(ei), _ptr(ej), _ptr(c), len(ei), _ptr(key), beta, seed, flip0, n_flips,
+                                _ptr(s), _ptr(sizes), _ptr(E))
+        assert st == 0, st
+        return s, sizes, E
 
     def stock_o3_chain(self, L, beta, seed, warmup, steps):
         """The reference's own O(3) L^3 chain (plain Pcg32; 1 Wolff flip + 1

@@ -461,6 +461,133 @@ extern "C" int ref_ising_wolff(std::uint64_t n, const std::uint32_t* ei, const s
     }
 }
 
+// ----------------------------------------------------- weighted Ising (payload)
+namespace {
+// The model of the reference's graph test (test/graph_check.cpp:34-83): double
+// spins, E = -sum over bonds of c s_i s_j, c carried by PairGraph<double>'s
+// bonds; a ModelLike and WolffModel against the reference's own concepts and
+// graph type, so the reference drivers run it unchanged.
+class WeightedIsing
+{
+public:
+    using value_type = double;
+    static constexpr std::size_t size = 1;
+    using bond_type = PairGraph<double>::bond_type;
+
+    explicit WeightedIsing(PairGraph<double> g) : graph_(std::move(g)), spin_(graph_.sites(), 1.0) {}
+
+    std::size_t sites() const noexcept { return graph_.sites(); }
+    const double* data() const noexcept { return spin_.data(); }
+    std::size_t degree(std::size_t i) const noexcept { return graph_.degree(i); }
+    const bond_type* bonds(std::size_t i) const noexcept { return graph_.bonds(i); }
+    double energy_at(std::size_t i) const noexcept
+    {
+        double e = 0.0;
+        const bond_type* bs = graph_.bonds(i);
+        for (std::size_t a = 0; a < graph_.degree(i); ++a) e += -bs[a].c * spin_[i] * spin_[bs[a].j];
+        return e;
+    }
+    double energy_diff_at(std::size_t i, const double* p) const noexcept
+    {
+        double d = 0.0;
+        const bond_type* bs = graph_.bonds(i);
+        for (std::size_t a = 0; a < graph_.degree(i); ++a) d += -bs[a].c * (*p - spin_[i]) * spin_[bs[a].j];
+        return d;
+    }
+    double energy_diff_bond(std::size_t i, const bond_type& b, const double* p) const noexcept
+    {
+        return -b.c * (*p - spin_[b.j]) * spin_[i];
+    }
+    void update(std::size_t i, const double* p) noexcept { spin_[i] = *p; }
+
+private:
+    PairGraph<double> graph_;
+    std::vector<double> spin_;
+};
+static_assert(ModelLike<WeightedIsing>);
+static_assert(WolffModel<WeightedIsing>);
+
+// The graph test's Flip on double spins and its axis r = 1 (test/graph_check.cpp:15-32).
+struct FlipDouble
+{
+    template <class R>
+    void sample(const double* cur, R&, double* out) const { *out = *cur > 0.0 ? -1.0 : 1.0; }
+    double log_ratio(const double*, const double*) const { return 0.0; }
+};
+struct AxisDouble
+{
+    template <class R>
+    void sample(const double*, R&, double* out) const { out[0] = 1.0; }
+};
+
+WeightedIsing weighted_model(std::uint64_t n, const std::uint32_t* ei, const std::uint32_t* ej, const double* c,
+                             std::uint64_t m, const double* spins)
+{
+    std::vector<PairGraph<double>::Edge> edges(m);
+    for (std::uint64_t e = 0; e < m; ++e) edges[e] = {ei[e], ej[e], c[e]};
+    WeightedIsing model(PairGraph<double>(n, edges));
+    for (std::size_t i = 0; i < n; ++i) model.update(i, spins + i);
+    return model;
+}
+}  // namespace
+
+// The reference's Metropolis over the weighted Ising model with per-site keyed
+// streams (site i: stream id i, the accept draw its first output); c[e] is
+// edge e's coupling.  E_out: 0.5 sum_i energy_at(i) after every sweep.
+extern "C" int ref_weighted_ising_metropolis(std::uint64_t n, const std::uint32_t* ei, const std::uint32_t* ej,
+                                             const double* c, std::uint64_t m, double beta, std::uint64_t seed,
+                                             std::uint64_t sweep0, std::uint64_t n_sweeps, double* spins,
+                                             double* E_out)
+{
+    try {
+        WeightedIsing model = weighted_model(n, ei, ej, c, m, spins);
+        KeyState ks;
+        ks.seed = seed;
+        ks.counter = sweep0;
+        using Q = Keyed<FlipDouble, double>;
+        Metropolis<WeightedIsing, Q, KeyedRng> mc(model, Q{FlipDouble{}, &ks, model.data(), 1, tag_site(0)},
+                                                  KeyedRng{&ks}, beta);
+        std::uint64_t k = 0;
+        mc.sample(n_sweeps, [&](const WeightedIsing& mdl) {
+            if (E_out) E_out[k] = half_energy_sum(mdl);
+            ++k;
+            ++ks.counter;
+        });
+        std::memcpy(spins, model.data(), n * sizeof(double));
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
+// The reference's Wolff over the weighted Ising model, the bond in CSR slot a
+// drawing from key[a], the axis and seed site from the flip's axis key.
+extern "C" int ref_weighted_ising_wolff(std::uint64_t n, const std::uint32_t* ei, const std::uint32_t* ej,
+                                        const double* c, std::uint64_t m, const std::uint32_t* key, double beta,
+                                        std::uint64_t seed, std::uint64_t flip0, std::uint64_t n_flips, double* spins,
+                                        std::uint64_t* sizes, double* E_out)
+{
+    try {
+        WeightedIsing model = weighted_model(n, ei, ej, c, m, spins);
+        KeyState ks;
+        ks.seed = seed;
+        ks.counter = flip0;
+        KeyedWolff<WeightedIsing> km{&model, &ks, key};
+        Wolff<KeyedWolff<WeightedIsing>, KeyedAxis<AxisDouble>, KeyedRng> w(
+            km, KeyedAxis<AxisDouble>{AxisDouble{}, &ks}, KeyedRng{&ks}, beta);
+        for (std::uint64_t f = 0; f < n_flips; ++f) {
+            const std::size_t sz = w.flip();
+            if (sizes) sizes[f] = sz;
+            if (E_out) E_out[f] = half_energy_sum(model);
+            ++ks.counter;
+        }
+        std::memcpy(spins, model.data(), n * sizeof(double));
+        return 0;
+    } catch (...) {
+        return status_of(std::current_exception());
+    }
+}
+
 // ------------------------------------------------------------------ VectorSpin
 namespace {
 template <std::size_t N>

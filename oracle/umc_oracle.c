@@ -386,6 +386,103 @@ void orc_ising_wolff(uint64_t n, const uint32_t* offset, const uint32_t* bonds,
     free(stack);
 }
 
+/* ------------------------------------------------- weighted Ising (bond payload)
+ * The reference graph test's IsingGraph (test/graph_check.cpp:34-83): double
+ * spins, coupling c[a] carried by CSR slot a (PairGraph<double>'s Bond::c).  */
+
+static double wising_energy_at(const uint32_t* offset, const uint32_t* bonds, const double* c, const double* s,
+                               uint64_t i)
+{
+    double e = 0.0; /* IsingGraph::energy_at, test/graph_check.cpp:47-54 */
+    for (uint32_t a = offset[i]; a < offset[i + 1]; ++a) e += -c[a] * s[i] * s[bonds[a]];
+    return e;
+}
+
+static double wising_half_energy(uint64_t n, const uint32_t* offset, const uint32_t* bonds, const double* c,
+                                 const double* s)
+{
+    double e = 0.0;
+    for (uint64_t i = 0; i < n; ++i) e += wising_energy_at(offset, bonds, c, s, i);
+    return 0.5 * e;
+}
+
+/* Metropolis::sweep (driver.hpp:29-43) over IsingGraph with the test's Flip
+ * (test/graph_check.cpp:15-24): site i opens its own keyed stream (id i), the
+ * accept test takes its first output. */
+void orc_weighted_ising_metropolis(uint64_t n, const uint32_t* offset, const uint32_t* bonds, const double* c,
+                                   double beta, uint64_t seed, uint64_t sweep0, uint64_t n_sweeps, double* s,
+                                   double* E_out, double* margin_out)
+{
+    for (uint64_t k = 0; k < n_sweeps; ++k) {
+        const uint64_t counter = sweep0 + k;
+        for (uint64_t i = 0; i < n; ++i) {
+            orc_pcg32 g;
+            orc_key_open(&g, seed, counter, ORC_TAG_SITE(0), (uint32_t)i);
+            const double p = s[i] > 0.0 ? -1.0 : 1.0;
+            double d = 0.0; /* IsingGraph::energy_diff_at, test/graph_check.cpp:58-65 */
+            for (uint32_t a = offset[i]; a < offset[i + 1]; ++a) d += -c[a] * (p - s[i]) * s[bonds[a]];
+            const double log_p = -beta * d + 0.0;
+            int accept;
+            double margin = INFINITY;
+            if (log_p >= 0.0) accept = 1;
+            else {
+                const double lu = log(orc_pcg32_uni(&g));
+                margin = lu - log_p;
+                accept = lu < log_p;
+            }
+            if (margin_out && k + 1 == n_sweeps) margin_out[i] = margin;
+            if (accept) s[i] = p;
+        }
+        if (E_out) E_out[k] = wising_half_energy(n, offset, bonds, c, s);
+    }
+}
+
+/* Wolff::flip (driver.hpp:104-162) over IsingGraph with the fixed axis r = 1
+ * (test/graph_check.cpp:27-32) and IsingGraph::energy_diff_bond (:67-70); the
+ * uniform of the bond in slot a is keyed by key[a]. */
+void orc_weighted_ising_wolff(uint64_t n, const uint32_t* offset, const uint32_t* bonds, const uint32_t* key,
+                              const double* c, double beta, uint64_t seed, uint64_t flip0, uint64_t n_flips,
+                              double* s, uint64_t* sizes, double* E_out)
+{
+    char* in_cluster = (char*)malloc(n ? n : 1);
+    uint64_t* stack = (uint64_t*)malloc((n ? n : 1) * sizeof(uint64_t));
+    for (uint64_t f = 0; f < n_flips; ++f) {
+        const uint64_t counter = flip0 + f;
+        orc_pcg32 g;
+        orc_key_open(&g, seed, counter, ORC_TAG_AXIS, 0);
+        const double r = 1.0;
+        memset(in_cluster, 0, n);
+        const uint64_t seed_site = (uint64_t)(orc_pcg32_uni(&g) * (double)n);
+        in_cluster[seed_site] = 1;
+        stack[0] = seed_site;
+        uint64_t top = 1, cluster = 0;
+        while (top > 0) {
+            const uint64_t i = stack[--top];
+            ++cluster;
+            const double si = s[i];
+            const double prop = si - 2.0 * (si * r) * r;
+            for (uint32_t a = offset[i]; a < offset[i + 1]; ++a) {
+                const uint32_t j = bonds[a];
+                if (in_cluster[j]) continue;
+                const double t = s[j];
+                const double nb = t - 2.0 * (t * r) * r;
+                const double dE = -c[a] * (nb - s[j]) * si;
+                orc_pcg32 gb;
+                orc_key_open(&gb, seed, counter, ORC_TAG_BOND, key[a]);
+                if (orc_pcg32_uni(&gb) < 1.0 - exp(-beta * dE)) {
+                    in_cluster[j] = 1;
+                    stack[top++] = j;
+                }
+            }
+            s[i] = prop;
+        }
+        if (sizes) sizes[f] = cluster;
+        if (E_out) E_out[f] = wising_half_energy(n, offset, bonds, c, s);
+    }
+    free(in_cluster);
+    free(stack);
+}
+
 /* ------------------------------------------------------------------ VectorSpin */
 
 static const double ORC_PI = 3.141592653589793238462643383279502884;

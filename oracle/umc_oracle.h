@@ -107,6 +107,19 @@ void orc_ising_wolff(uint64_t n, const uint32_t* offset, const uint32_t* bonds,
                      uint64_t flip0, uint64_t n_flips, int8_t* spins, uint64_t* sizes,
                      double* E_out, double* M_out);
 
+/* ---- weighted Ising: the reference graph test's IsingGraph (test/graph_check.cpp:
+ * 34-83) on a PairGraph<double>, c[a] the coupling of CSR slot a ---------------------
+ * spins: doubles in {-1,+1}, updated in place.  Metropolis with the test's Flip:
+ * site i's accept draw is the first output of its keyed stream (id i); margin_out
+ * (may be NULL) as in orc_vector_metropolis.  Wolff with r = 1: the bond in slot a
+ * draws from key[a].  E_out (may be NULL): 0.5 * sum_i energy_at(i) per sweep/flip. */
+void orc_weighted_ising_metropolis(uint64_t n, const uint32_t* offset, const uint32_t* bonds, const double* c,
+                                   double beta, uint64_t seed, uint64_t sweep0, uint64_t n_sweeps, double* spins,
+                                   double* E_out, double* margin_out);
+void orc_weighted_ising_wolff(uint64_t n, const uint32_t* offset, const uint32_t* bonds, const uint32_t* key,
+                              const double* c, double beta, uint64_t seed, uint64_t flip0, uint64_t n_flips,
+                              double* spins, uint64_t* sizes, double* E_out);
+
 /* ---- VectorSpin<N> (example/vector_spin.hpp) -------------------------------------
  * spins: n*N doubles.  proposal: 0 = UniformSphereN<N>, 1 = LocalRotation<N>{delta}.
  * obs_out (may be NULL): per sweep/flip, [E, M_0 .. M_{N-1}]  (stride N+1).

@@ -8,6 +8,7 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <string>
 #include <cstdlib>
 #include <stdexcept>
 #include <tuple>
@@ -33,6 +34,8 @@ static_assert(Proposal<Flip, IsingSpin, Pcg32>);
 static_assert(Proposal<U1Shift, U1Link, Pcg32>);
 static_assert(Proposal<UniformSphereN<3>, double, Pcg32>);
 static_assert(PairGraphLike<PairGraph<>>);
+static_assert(PairGraphLike<PairGraph<double>>);
+static_assert(sizeof(Bond<NoPayload>) == 4);
 static_assert(CellComplexLike<CellComplex<4>>);
 // the reference's table-driven models with its built-in terms (model/pair.hpp,
 // model/cell.hpp, term/*.hpp)
@@ -91,8 +94,52 @@ double torus_plaquette(double beta, int n_plaq)
     return num / den;
 }
 
-int main()
+// PairGraph<double>: the reference graph test's weighted 16 x 16 lattice
+// (test/graph_check.cpp:86-127) with random couplings; each row carries its
+// edges' couplings, so the row energy equals the edge sum.
+void check_weighted_graph()
 {
+    constexpr std::uint32_t L = 16, N = L * L;
+    std::vector<PairGraph<double>::Edge> edges;
+    Pcg32 rng(77, 3);
+    for (std::uint32_t y = 0; y < L; ++y)
+        for (std::uint32_t x = 0; x < L; ++x) {
+            edges.push_back({y * L + x, y * L + (x + 1) % L, 2.0 * rng.uni() - 1.0});
+            edges.push_back({y * L + x, ((y + 1) % L) * L + x, 2.0 * rng.uni() - 1.0});
+        }
+    const PairGraph<double> g(N, edges);
+    CHECK(g.sites() == N);
+    std::vector<double> s(N);
+    for (auto& v : s) v = rng.uni() < 0.5 ? -1.0 : 1.0;
+    double row = 0.0, edge = 0.0;
+    for (std::size_t i = 0; i < N; ++i) {
+        CHECK(g.degree(i) == 4);
+        for (std::size_t a = 0; a < g.degree(i); ++a) row += -g.bonds(i)[a].c * s[i] * s[g.bonds(i)[a].j];
+    }
+    for (const auto& e : edges) edge += -e.c * s[e.i] * s[e.j];
+    CHECK(std::abs(0.5 * row - edge) < 1e-9);
+    // the first edge's coupling sits in row 0 (slot 0) and in row 1
+    CHECK(g.bonds(0)[0].j == 1 && g.bonds(0)[0].c == edges[0].c);
+    bool found = false;
+    for (std::size_t a = 0; a < g.degree(1); ++a) found |= g.bonds(1)[a].j == 0 && g.bonds(1)[a].c == edges[0].c;
+    CHECK(found);
+    // a copy shares the table; a directed graph keeps one entry per edge
+    const PairGraph<double> copy = g;
+    CHECK(copy.bonds(5)[2].c == g.bonds(5)[2].c);
+    const std::array<PairGraph<double>::Edge, 1> one{PairGraph<double>::Edge{0, 1, 0.25}};
+    const PairGraph<double> directed(2, one, false);
+    CHECK(directed.degree(0) == 1 && directed.degree(1) == 0 && directed.bonds(0)[0].c == 0.25);
+}
+
+int main(int argc, char** argv)
+{
+    // ---- host-side tables (no GPU needed)
+    check_weighted_graph();
+    if (argc > 1 && std::string(argv[1]) == "tables") {
+        std::puts("facade_check tables: ok");
+        return 0;
+    }
+
     // ---- tables
     const auto graph = square_lattice(4, 4);
     CHECK(graph.sites() == 16);

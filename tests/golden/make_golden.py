@@ -27,6 +27,7 @@ from helpers import (  # noqa: E402
     random_unit_vectors,
     relabel_cells,
     relabel_edges,
+    slot_edges,
     square_edges,
     square_plaquette_cells,
 )
@@ -69,6 +70,23 @@ def main():
     g["ising8_s0r"] = s0r
     s, E, M = r.ising_metropolis(L * L, ei, ej, -1, 0.7, 11, 5, 20, s0r)
     g["ising8_afm_spins"], g["ising8_afm_E"], g["ising8_afm_M"] = s, E, M
+
+    # ---- weighted Ising (test/graph_check.cpp's IsingGraph on PairGraph<double>):
+    # 40 sites, 100 random edges (duplicates kept), couplings +-1 times a weight,
+    # random start; the Wolff bond in slot a keyed by its edge index
+    rng = np.random.default_rng(31)
+    e = rng.integers(0, 40, (120, 2))
+    e = e[e[:, 0] != e[:, 1]][:100].astype(np.uint32)
+    c = rng.choice([-1.0, 1.0], len(e)) * rng.uniform(0.5, 1.5, len(e))
+    g["wising_ei"], g["wising_ej"], g["wising_c"] = e[:, 0].copy(), e[:, 1].copy(), c
+    s0 = np.where(rng.random(40) < 0.5, -1.0, 1.0)
+    g["wising_s0"] = s0
+    s, E = r.weighted_ising_metropolis(40, e[:, 0], e[:, 1], c, 0.6, 13, 0, 20, s0)
+    g["wising_metro_s"], g["wising_metro_E"] = s, E
+    st, off, bonds = r.pair_graph(40, e[:, 0], e[:, 1])
+    slot = slot_edges(off, e[:, 0], e[:, 1])
+    s, sizes, E = r.weighted_ising_wolff(40, e[:, 0], e[:, 1], c, slot, 0.6, 14, 0, 50, s0)
+    g["wising_wolff_s"], g["wising_wolff_sizes"], g["wising_wolff_E"] = s, sizes, E
 
     # ---- VectorSpin<3> on a 4^3 cubic lattice
     L = 4

@@ -130,3 +130,17 @@ def device_csr(g):
         back = doff[j] + np.nonzero(dbonds[doff[j]:doff[j + 1]] == i)[0]
         key[a] = back[m]
     return pos, doff, dbonds, key
+
+
+def slot_edges(off, ei, ej, symmetric=True):
+    """The input edge of every CSR slot, replaying PairGraph's scatter
+    (lattice/pair_graph.hpp:77-81): rows filled in edge order."""
+    pos = np.array(off[:-1], np.int64)
+    slot = np.zeros(int(off[-1]), np.uint32)
+    for e, (i, j) in enumerate(zip(ei, ej)):
+        slot[pos[i]] = e
+        pos[i] += 1
+        if symmetric:
+            slot[pos[j]] = e
+            pos[j] += 1
+    return slot

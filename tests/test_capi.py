@@ -170,3 +170,55 @@ def test_ising_thresholds_pin_the_reference_accept_rule():
                 hi = mid
         assert math.log(lo * 2.0**-32) < log_p
         assert not math.log((lo + 1) * 2.0**-32) < log_p
+
+
+# ------------------------------------------------------ bond payloads (PairGraph<P>)
+def test_payload_graph_copies_edge_payloads_into_both_slots(umc):
+    """PairGraph<double>(n, edges): every slot carries its edge's payload
+    (lattice/pair_graph.hpp:77-81), duplicates and the directed form included;
+    the CSR itself is the NoPayload graph's."""
+    from helpers import slot_edges
+
+    rng = np.random.default_rng(9)
+    e = rng.integers(0, 30, (80, 2))
+    e = e[e[:, 0] != e[:, 1]].astype(np.uint32)
+    e = np.concatenate([e, e[:3]])  # duplicated edges stay duplicated
+    c = rng.normal(size=len(e))
+    for symmetric in (True, False):
+        g = umc.PairGraph(30, e, symmetric=symmetric, payload=c)
+        g0 = umc.PairGraph(30, e, symmetric=symmetric)
+        off, bonds = g.csr()
+        off0, bonds0 = g0.csr()
+        np.testing.assert_array_equal(off, off0)
+        np.testing.assert_array_equal(bonds, bonds0)
+        slot = slot_edges(off, e[:, 0], e[:, 1], symmetric)
+        np.testing.assert_array_equal(g.slot_edges(), slot)
+        np.testing.assert_array_equal(g.payloads(), c[slot])
+    # a record of several values per edge (a structured payload)
+    rec = rng.normal(size=(len(e), 3)).astype(np.float32)
+    g = umc.PairGraph(30, e, payload=rec)
+    np.testing.assert_array_equal(g.payloads(), rec[slot_edges(g.csr()[0], e[:, 0], e[:, 1])])
+    assert umc.lib.umc_graph_payload_bytes(g._h) == 12
+    assert umc.lib.umc_graph_payload_bytes(umc.PairGraph(30, e)._h) == 0
+
+
+def test_payload_graph_errors(umc):
+    e = np.array([[0, 1], [1, 2]], np.uint32)
+    ei, ej = np.ascontiguousarray(e[:, 0]), np.ascontiguousarray(e[:, 1])
+    h = umc._vp()
+    pay = np.zeros(2 * 300, np.uint8)
+    for nbytes in (0, 257):
+        rc = umc.lib.umc_graph_create_payload(3, ei.ctypes.data, ej.ctypes.data, 2, 1, pay.ctypes.data, nbytes,
+                                              ctypes.byref(h))
+        assert rc == umc.ERR_INVALID_ARGUMENT
+    rc = umc.lib.umc_graph_create_payload(3, ei.ctypes.data, ej.ctypes.data, 2, 1, None, 8, ctypes.byref(h))
+    assert rc == umc.ERR_INVALID_ARGUMENT
+    # the reference's construction rules still apply
+    with pytest.raises(ValueError):
+        umc.PairGraph(3, [[0, 0]], payload=np.ones(1))
+    with pytest.raises(IndexError):
+        umc.PairGraph(3, [[0, 5]], payload=np.ones(1))
+    with pytest.raises(ValueError):
+        umc.PairGraph(3, e, payload=np.ones(3))  # one record per edge
+    with pytest.raises(ValueError):
+        umc.PairGraph(3, e).payloads()

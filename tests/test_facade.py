@@ -32,6 +32,14 @@ def test_facade_compiles(facade_binary):
     assert os.path.isfile(facade_binary)
 
 
+def test_facade_host_tables(facade_binary):
+    """The host-side tables, PairGraph<double> with bond payloads included,
+    behave as the reference's (tests/cpp/facade_check.cpp, `tables` mode)."""
+    r = subprocess.run([facade_binary, "tables"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "tables: ok" in r.stdout
+
+
 def test_facade_without_a_gpu_fails_loudly(facade_binary, umc):
     if umc.device_count() > 0:
         pytest.skip("a GPU is present")

@@ -305,3 +305,68 @@ def test_u1_2d_live_against_reference(oracle, ref):
     b, ob = ref.u1_metropolis(cells, 3.0, 1.0, 0.5, 3, 9, 4, 5, th0)
     np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(oa, ob)
+
+
+# --------------------------------------------- weighted Ising (bond payloads)
+def _wising_setup(golden):
+    ei, ej, c = golden["wising_ei"], golden["wising_ej"], golden["wising_c"]
+    return ei, ej, c
+
+
+def _slot_couplings(oracle, n, ei, ej, c):
+    """CSR of PairGraph<double>(n, edges) and the coupling of every slot (the
+    reference copies Edge::c into both directed entries)."""
+    from helpers import slot_edges
+
+    st, off, bonds, _ = oracle.pair_graph(n, ei, ej)
+    assert st == 0
+    slot = slot_edges(off, ei, ej)
+    return off, bonds, slot, c[slot]
+
+
+def test_weighted_ising_matches_reference_vectors(oracle, golden):
+    """test/graph_check.cpp's IsingGraph (PairGraph<double> couplings, random
+    +-J times a weight, duplicate edges) under Metropolis and Wolff."""
+    ei, ej, c = _wising_setup(golden)
+    off, bonds, slot, cs = _slot_couplings(oracle, 40, ei, ej, c)
+    s, E, _ = oracle.weighted_ising_metropolis(off, bonds, cs, 0.6, 13, 0, 20, golden["wising_s0"])
+    np.testing.assert_array_equal(s, golden["wising_metro_s"])
+    np.testing.assert_allclose(E, golden["wising_metro_E"], rtol=1e-12)
+    s, sizes, E = oracle.weighted_ising_wolff(off, bonds, slot, cs, 0.6, 14, 0, 50, golden["wising_s0"])
+    np.testing.assert_array_equal(sizes, golden["wising_wolff_sizes"])
+    np.testing.assert_array_equal(s, golden["wising_wolff_s"])
+    np.testing.assert_allclose(E, golden["wising_wolff_E"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_weighted_ising_matches_reference_live(oracle, ref, seed):
+    rng = np.random.default_rng(100 + seed)
+    n = 64
+    e = rng.integers(0, n, (200, 2))
+    e = e[e[:, 0] != e[:, 1]].astype(np.uint32)
+    c = rng.choice([-1.0, 1.0], len(e)) * rng.uniform(0.2, 2.0, len(e))
+    off, bonds, slot, cs = _slot_couplings(oracle, n, e[:, 0], e[:, 1], c)
+    s0 = np.where(rng.random(n) < 0.5, -1.0, 1.0)
+    s_r, E_r = ref.weighted_ising_metropolis(n, e[:, 0], e[:, 1], c, 0.45, seed, 3, 15, s0)
+    s_o, E_o, _ = oracle.weighted_ising_metropolis(off, bonds, cs, 0.45, seed, 3, 15, s0)
+    np.testing.assert_array_equal(s_o, s_r)
+    np.testing.assert_allclose(E_o, E_r, rtol=1e-12)
+    s_r, z_r, E_r = ref.weighted_ising_wolff(n, e[:, 0], e[:, 1], c, slot, 0.45, seed, 2, 30, s0)
+    s_o, z_o, E_o = oracle.weighted_ising_wolff(off, bonds, slot, cs, 0.45, seed, 2, 30, s0)
+    np.testing.assert_array_equal(z_o, z_r)
+    np.testing.assert_array_equal(s_o, s_r)
+
+
+def test_weighted_ising_uniform_couplings_equal_the_ising_model(oracle):
+    """With every coupling 1 the weighted Wolff is the plain Ising Wolff
+    (example/ising.hpp, J = 1) on the same keys."""
+    L = 8
+    ei, ej = square_edges(L, L)
+    st, off, bonds, slot = oracle.pair_graph(L * L, ei, ej)
+    s0 = np.where(np.random.default_rng(4).random(L * L) < 0.5, -1, 1).astype(np.int8)
+    s_i, z_i, E_i, _ = oracle.ising_wolff(off, bonds, slot, 1, 0.44, 5, 0, 40, s0)
+    s_w, z_w, E_w = oracle.weighted_ising_wolff(off, bonds, slot, np.ones(len(bonds)), 0.44, 5, 0, 40,
+                                                s0.astype(np.float64))
+    np.testing.assert_array_equal(z_w, z_i)
+    np.testing.assert_array_equal(s_w, s_i.astype(np.float64))
+    np.testing.assert_array_equal(E_w, E_i)

@@ -20,7 +20,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(os.path.dirname(HERE), "examples", "device_models"))
 sys.path.insert(0, HERE)
 
-from helpers import checker_position, cubic_edges, device_csr, random_unit_vectors, relabel_edges  # noqa: E402
+from helpers import (checker_position, cubic_edges, device_csr, random_unit_vectors, relabel_edges,  # noqa: E402
+                     square_edges)
 
 TOL = 1e-9
 MARGIN = 1e-9
@@ -540,3 +541,85 @@ def test_fp32_user_o3_term_per_sweep(umc, oracle, lib, kind):
         assert bad_total <= 20
     finally:
         lib.um_session_destroy(h)
+
+
+# --------------------------------------- weighted models: PairGraph<double> payloads
+def _device_payloads(g):
+    """The bond payloads in the device rows' slot order (BondTables): rows in
+    colour-major order, each row's slots in the reference row order."""
+    off, _ = g.csr()
+    _, _, pos = g.colouring()
+    pay = g.payloads()
+    return np.concatenate([pay[off[i]:off[i + 1]] for i in np.argsort(pos)])
+
+
+def _weighted_graph(umc, kind):
+    rng = np.random.default_rng(77)
+    if kind == "random":
+        n = 300
+        e = rng.integers(0, n, (900, 2))
+        e = e[e[:, 0] != e[:, 1]].astype(np.uint32)
+        e = np.concatenate([e, e[:20]])  # duplicated bonds stay duplicated
+    else:  # the reference graph test's 16 x 16 periodic lattice, random couplings
+        n = 256
+        e = np.stack(square_edges(16, 16), axis=1)
+    c = rng.choice([-1.0, 1.0], len(e)) * rng.uniform(0.5, 1.5, len(e))
+    return umc.PairGraph(n, e, payload=c), n
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["random", "square"])
+def test_user_weighted_ising_metropolis_is_bit_exact(umc, oracle, lib, kind):
+    """test/graph_check.cpp's IsingGraph as a user ModelLike on the device: double
+    spins and the coupling carried by each bond of a PairGraph<double>
+    (BondTables<double>::rows()), random +-J couplings.  30 sweeps equal the
+    oracle's bit for bit (every decision is the FP64 test's), energies to 1e-12."""
+    lib.um_weighted_ising.argtypes = [_vp, _d, _u64, _u64, _u32, C.c_int, C.c_int, _vp, _vp, _vp]
+    g, n = _weighted_graph(umc, kind)
+    pos, doff, dbonds, key = device_csr(g)
+    cs = _device_payloads(g)
+    s0 = np.where(np.random.default_rng(5).random(n) < 0.5, 1.0, -1.0)
+    s = s0.copy()
+    en = np.zeros(30)
+    _call(lib, lib.um_weighted_ising(g._h, 0.45, 21, 4, 30, 0, 0, s.ctypes.data, en.ctypes.data, None))
+    cm = np.empty(n)
+    cm[pos] = s0
+    s_o, E_o, margin = oracle.weighted_ising_metropolis(doff, dbonds, cs, 0.45, 21, 4, 30, cm)
+    np.testing.assert_array_equal(s, s_o[pos])
+    np.testing.assert_allclose(en, E_o, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["random", "square"])
+@pytest.mark.parametrize("tiled", [0, 1])
+def test_user_weighted_ising_wolff_is_bit_exact(umc, oracle, lib, kind, tiled):
+    """The same model under the device Wolff with the fixed axis: 25 flips, one
+    launch each, equal the oracle's spins and cluster sizes bit for bit, with
+    and without the shared-memory tiles; the bond tests read each bond's own
+    coupling (energy_diff_bond = -c (p - s_j) s_i)."""
+    lib.um_weighted_ising.argtypes = [_vp, _d, _u64, _u64, _u32, C.c_int, C.c_int, _vp, _vp, _vp]
+    g, n = _weighted_graph(umc, kind)
+    pos, doff, dbonds, key = device_csr(g)
+    cs = _device_payloads(g)
+    s0 = np.where(np.random.default_rng(6).random(n) < 0.5, 1.0, -1.0)
+    s = s0.copy()
+    sizes = np.zeros(25, np.uint64)
+    en = np.zeros(25)
+    _call(lib, lib.um_weighted_ising(g._h, 0.6, 33, 2, 25, 1, tiled, s.ctypes.data, en.ctypes.data,
+                                     sizes.ctypes.data))
+    cm = np.empty(n)
+    cm[pos] = s0
+    s_o, z_o, E_o = oracle.weighted_ising_wolff(doff, dbonds, key, cs, 0.6, 33, 2, 25, cm)
+    np.testing.assert_array_equal(sizes, z_o)
+    np.testing.assert_array_equal(s, s_o[pos])
+    np.testing.assert_allclose(en, E_o, rtol=1e-12, atol=1e-12)
+    assert sizes.max() > 1  # clusters grew
+
+
+@pytest.mark.gpu
+def test_builtin_models_refuse_weighted_graphs(umc):
+    """As the reference's Ising and VectorSpin take PairGraph<> (no payload),
+    the engine's built-in models refuse a graph with bond payloads."""
+    g, _ = _weighted_graph(umc, "square")
+    with pytest.raises(Exception, match="payload"):
+        umc.Chain(umc.MODEL_ISING, graph=g, coupling=1, proposal=umc.PROPOSAL_FLIP, seed=1)

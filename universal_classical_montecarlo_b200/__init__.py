@@ -129,6 +129,10 @@ _decl("umc_graph_destroy", None, _vp)
 _decl("umc_graph_sites", _u64, _vp)
 _decl("umc_graph_slots", _u64, _vp)
 _decl("umc_graph_csr", _int, _vp, _vp, _vp)
+_decl("umc_graph_create_payload", _int, _u64, _vp, _vp, _u64, _int, _vp, _u32, C.POINTER(_vp))
+_decl("umc_graph_payload_bytes", _u32, _vp)
+_decl("umc_graph_payloads", _int, _vp, _vp)
+_decl("umc_graph_slot_edges", _int, _vp, _vp)
 _decl("umc_graph_colouring", _int, _vp, _vp, _vp, _vp)
 _decl("umc_cells_create", _int, _u64, _u32, _vp, _u64, C.POINTER(_vp))
 _decl("umc_cells_hypercubic", _int, _u64, C.POINTER(_vp))
@@ -275,11 +279,16 @@ def binning_error(series, bin: int):
 
 # ===================================================================== tables
 class PairGraph:
-    """PairGraph(n, edges, symmetric) -- lattice/pair_graph.hpp:49-83."""
+    """PairGraph(n, edges, symmetric) -- lattice/pair_graph.hpp:49-83.
 
-    def __init__(self, n_sites: int = 0, edges=None, symmetric: bool = True, _handle=None):
+    payload: optional per-edge records (PairGraph<P>'s Edge::c), a numpy array
+    with one row (or element) per edge, e.g. float64 couplings or a structured
+    dtype; each is copied into both directed slots as the reference copies c."""
+
+    def __init__(self, n_sites: int = 0, edges=None, symmetric: bool = True, payload=None, _handle=None):
         if _handle is not None:
             self._h = _handle
+            self.payload_dtype = None
             return
         e = np.zeros((0, 2), np.uint32) if edges is None else np.asarray(edges)
         e = np.ascontiguousarray(e.reshape(-1, 2))
@@ -288,8 +297,34 @@ class PairGraph:
         ei = np.ascontiguousarray(e[:, 0], np.uint32)
         ej = np.ascontiguousarray(e[:, 1], np.uint32)
         h = _vp()
-        check(lib.umc_graph_create(n_sites, _ptr(ei), _ptr(ej), len(ei), int(symmetric), C.byref(h)))
+        self.payload_dtype = None
+        if payload is None:
+            check(lib.umc_graph_create(n_sites, _ptr(ei), _ptr(ej), len(ei), int(symmetric), C.byref(h)))
+        else:
+            pay = np.ascontiguousarray(payload)
+            if len(pay) != len(ei):
+                raise ValueError("PairGraph: one payload record per edge")
+            rec = pay.reshape(len(ei), -1) if pay.ndim > 1 else pay.reshape(len(ei))
+            nbytes = rec.itemsize * (rec.shape[1] if rec.ndim > 1 else 1)
+            self.payload_dtype = (pay.dtype, pay.shape[1:])
+            check(lib.umc_graph_create_payload(n_sites, _ptr(ei), _ptr(ej), len(ei), int(symmetric), _ptr(rec),
+                                               nbytes, C.byref(h)))
         self._h = h
+
+    def payloads(self):
+        """Bond<P>::c of every CSR slot, in umc_graph_csr's slot order."""
+        if self.payload_dtype is None:
+            raise ValueError("graph has no payload")
+        dt, shape = self.payload_dtype
+        out = np.zeros((int(lib.umc_graph_slots(self._h)),) + tuple(shape), dt)
+        check(lib.umc_graph_payloads(self._h, _ptr(out)))
+        return out
+
+    def slot_edges(self):
+        """The input edge of every CSR slot."""
+        out = np.zeros(int(lib.umc_graph_slots(self._h)), np.uint32)
+        check(lib.umc_graph_slot_edges(self._h, _ptr(out)))
+        return out
 
     def __del__(self):
         h = getattr(self, "_h", None)

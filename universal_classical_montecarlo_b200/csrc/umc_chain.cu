@@ -823,6 +823,10 @@ void create_chain(const umc_chain_desc* d, umc_chain* c)
     if (is_spin(c)) {
         const umc_graph* g = d->graph;
         if (!g) throw Error(UMC_ERR_INVALID_ARGUMENT, "spin models need a graph");
+        if (g->payload_bytes)
+            throw Error(UMC_ERR_UNSUPPORTED,
+                        "the built-in spin models take a graph without bond payloads, as the reference's Ising and "
+                        "VectorSpin take PairGraph<>; a weighted model is a user model (umc/device.cuh BondTables)");
         c->n = g->n;
         c->symmetric = g->symmetric;
         c->n_colours = g->col.n_colours;

@@ -11,6 +11,7 @@
 #include "umc_tables.hpp"
 
 #include <algorithm>
+#include <memory>
 #include <cstring>
 #include <limits>
 #include <new>
@@ -489,6 +490,47 @@ int umc_graph_create(uint64_t n_sites, const uint32_t* edge_i, const uint32_t* e
     return guarded([&] {
         if (!out) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "null output handle");
         *out = umc::make_graph(n_sites, edge_i, edge_j, n_edges, symmetric != 0, umc::Lattice::Generic, nullptr);
+    });
+}
+
+int umc_graph_create_payload(uint64_t n_sites, const uint32_t* edge_i, const uint32_t* edge_j, uint64_t n_edges,
+                             int symmetric, const void* payload, uint32_t payload_bytes, umc_graph** out)
+{
+    return guarded([&] {
+        if (!out) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "null output handle");
+        if (payload_bytes == 0 || payload_bytes > UMC_MAX_PAYLOAD_BYTES)
+            throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "PairGraph: payload size must be 1 to 256 bytes");
+        if (n_edges && !payload) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "PairGraph: null payload array");
+        std::unique_ptr<umc_graph> g(
+            umc::make_graph(n_sites, edge_i, edge_j, n_edges, symmetric != 0, umc::Lattice::Generic, nullptr));
+        const auto* p = static_cast<const uint8_t*>(payload);
+        g->payload_bytes = payload_bytes;
+        g->payload.assign(p, p + n_edges * payload_bytes);
+        *out = g.release();
+    });
+}
+
+uint32_t umc_graph_payload_bytes(const umc_graph* g) { return g ? g->payload_bytes : 0u; }
+
+int umc_graph_payloads(const umc_graph* g, void* out)
+{
+    return guarded([&] {
+        if (!g) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "null graph");
+        if (!g->payload_bytes) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "graph has no payload (NoPayload)");
+        if (!out) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "null output");
+        auto* o = static_cast<uint8_t*>(out);
+        const size_t b = g->payload_bytes;
+        for (size_t a = 0; a < g->slot_edge.size(); ++a)
+            std::memcpy(o + a * b, g->payload.data() + size_t(g->slot_edge[a]) * b, b);
+    });
+}
+
+int umc_graph_slot_edges(const umc_graph* g, uint32_t* out)
+{
+    return guarded([&] {
+        if (!g || !out) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        umc::materialize(g);
+        std::copy(g->slot_edge.begin(), g->slot_edge.end(), out);
     });
 }
 

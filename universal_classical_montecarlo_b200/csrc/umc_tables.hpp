@@ -51,6 +51,11 @@ struct umc_graph
     // (edge list, CSR, colouring arrays); n, degree and the colour classes are
     // known in closed form
     bool materialized = true;
+    // PairGraph<P>'s per-bond payload (lattice/pair_graph.hpp:36-41): one
+    // payload_bytes record per input edge, copied into both directed slots
+    // (slot a carries payload[slot_edge[a]]); payload_bytes 0 = NoPayload
+    uint32_t payload_bytes = 0;
+    std::vector<uint8_t> payload;
 };
 
 // CellComplex<A> (lattice/cell_complex.hpp:21-87) plus the colour-major copy.
