@@ -493,6 +493,26 @@ int umc_tau_int_multi(const double* x, uint64_t series, uint64_t length, double 
  * consecutive values (at least two bins). */
 int umc_binning_error(const double* x, uint64_t n, uint64_t bin, double* mean, double* err);
 
+/* Observable streams: a per-sweep or per-flip FP64 series on disk for offline
+ * autocorrelation analysis (no reference counterpart: the reference's observe
+ * callbacks keep nothing, driver.hpp:54-61).  The file is a 56-byte header
+ * (magic "UMCOBS01", version 1, columns, records, seed, first counter, model,
+ * beta), columns x 32-byte NUL-padded names, then records x columns doubles,
+ * little-endian.  The record count is rewritten after every append, so a run
+ * cut short still reads back every counted record.  Not thread-safe per
+ * handle. */
+typedef struct umc_obs_stream umc_obs_stream;
+int umc_obs_stream_create(const char* path, uint32_t columns, const char* const* names, uint64_t seed,
+                          uint64_t first, int32_t model, double beta, umc_obs_stream** out);
+/* Appends n records (n x columns doubles, row-major). */
+int umc_obs_stream_append(umc_obs_stream* s, const double* records, uint64_t n);
+int umc_obs_stream_close(umc_obs_stream* s);
+/* Header of a stream file; names (columns x 32 bytes) may be NULL, as may any output. */
+int umc_obs_stream_info(const char* path, uint32_t* columns, uint64_t* records, uint64_t* seed, uint64_t* first,
+                        int32_t* model, double* beta, char* names);
+/* Records [first_record, first_record + n) into out (n x columns). */
+int umc_obs_stream_read(const char* path, uint64_t first_record, uint64_t n, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -83,3 +83,35 @@ def test_tau_multi_pools_chains(umc):
     tf, _, _ = umc.tau_int_multi(xf)
     assert tf == pytest.approx(t, rel=1e-9)
     assert umc.tau_int_multi(np.ones((3, 10)))[0] == 0.5
+
+
+def test_observable_stream_round_trip_and_offline_tau(umc, tmp_path):
+    """umc_obs_stream_*: records appended in chunks read back exactly, with
+    the header's names, seed, first counter, model and beta; tau_int of the
+    stored series equals tau_int of the series in memory; a partial read and
+    reads beyond the stream behave."""
+    rng = np.random.default_rng(4)
+    phi, n = 0.8, 6000
+    x = np.zeros(n)
+    for t in range(1, n):
+        x[t] = phi * x[t - 1] + rng.normal()
+    rec = np.stack([x, x**2, np.arange(n, dtype=np.float64)], axis=1)
+    path = tmp_path / "obs.umc"
+    with umc.ObsStream(path, ["E", "E2", "sweep"], seed=17, first=1000, model=umc.MODEL_VECTOR, beta=0.693) as s:
+        for k in range(0, n, 1024):
+            s.append(rec[k:k + 1024])
+        meta, mid = umc.read_obs_stream(path)  # readable while still open
+        assert meta["records"] == n
+    meta, got = umc.read_obs_stream(path)
+    np.testing.assert_array_equal(got, rec)
+    assert meta == {"names": ["E", "E2", "sweep"], "records": n, "seed": 17, "first": 1000,
+                    "model": umc.MODEL_VECTOR, "beta": 0.693}
+    assert umc.tau_int(got[:, 0]) == umc.tau_int(x)
+    _, part = umc.read_obs_stream(path, first=10, n=5)
+    np.testing.assert_array_equal(part, rec[10:15])
+    with pytest.raises(IndexError):
+        umc.read_obs_stream(path, first=n - 2, n=5)
+    bad = tmp_path / "bad.umc"
+    bad.write_bytes(b"not a stream at all, definitely not" * 3)
+    with pytest.raises(ValueError):
+        umc.read_obs_stream(bad)

@@ -277,6 +277,69 @@ def binning_error(series, bin: int):
     return m.value, e.value
 
 
+_decl("umc_obs_stream_create", _int, C.c_char_p, _u32, _vp, _u64, _u64, _i32, _f64, C.POINTER(_vp))
+_decl("umc_obs_stream_append", _int, _vp, _vp, _u64)
+_decl("umc_obs_stream_close", _int, _vp)
+_decl("umc_obs_stream_info", _int, C.c_char_p, C.POINTER(_u32), C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64),
+      C.POINTER(_i32), C.POINTER(_f64), _vp)
+_decl("umc_obs_stream_read", _int, C.c_char_p, _u64, _u64, _vp)
+
+
+class ObsStream:
+    """umc_obs_stream_*: a per-sweep (or per-flip) FP64 observable series
+    written to disk as it is produced, for offline tau_int of long runs.
+
+        with ObsStream(path, ["E", "Mx", "My", "Mz"], seed=1, first=0) as s:
+            s.append(chain.metropolis(beta, 1000)[:, :4])
+        meta, data = read_obs_stream(path)
+    """
+
+    def __init__(self, path, names, seed: int = 0, first: int = 0, model: int = 0, beta: float = 0.0):
+        self.columns = len(names)
+        arr = (C.c_char_p * self.columns)(*[n.encode() for n in names])
+        h = _vp()
+        check(lib.umc_obs_stream_create(os.fspath(path).encode(), self.columns, C.cast(arr, _vp), seed, first, model,
+                                        beta, C.byref(h)))
+        self._h = h
+
+    def append(self, records) -> None:
+        r = np.ascontiguousarray(records, np.float64).reshape(-1, self.columns)
+        check(lib.umc_obs_stream_append(self._h, _ptr(r), r.shape[0]))
+
+    def close(self) -> None:
+        if self._h:
+            h, self._h = self._h, None
+            check(lib.umc_obs_stream_close(h))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.umc_obs_stream_close(self._h)
+            self._h = None
+
+
+def read_obs_stream(path, first: int = 0, n: int | None = None):
+    """(meta, records): the stream's header fields and records [first, first + n)."""
+    p = os.fspath(path).encode()
+    cols, recs, seed, f0, beta, model = _u32(), _u64(), _u64(), _u64(), _f64(), _i32()
+    check(lib.umc_obs_stream_info(p, C.byref(cols), C.byref(recs), C.byref(seed), C.byref(f0), C.byref(model),
+                                  C.byref(beta), None))
+    names = C.create_string_buffer(32 * cols.value)
+    check(lib.umc_obs_stream_info(p, None, None, None, None, None, None, names))
+    count = recs.value - first if n is None else n
+    out = np.zeros((count, cols.value))
+    check(lib.umc_obs_stream_read(p, first, count, _ptr(out)))
+    raw = names.raw
+    meta = {"names": [raw[32 * c:32 * (c + 1)].split(b"\0", 1)[0].decode() for c in range(cols.value)],
+            "records": recs.value, "seed": seed.value, "first": f0.value, "model": model.value, "beta": beta.value}
+    return meta, out
+
+
 # ===================================================================== tables
 class PairGraph:
     """PairGraph(n, edges, symmetric) -- lattice/pair_graph.hpp:49-83.

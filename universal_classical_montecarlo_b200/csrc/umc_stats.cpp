@@ -134,3 +134,160 @@ int umc_binning_error(const double* x, uint64_t n, uint64_t bin, double* mean, d
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------- observable streams
+// A per-sweep (or per-flip) series of FP64 observables on disk, for offline
+// autocorrelation analysis (umc_tau_int) of runs longer than memory.  Layout,
+// little-endian as the host writes it:
+//   char magic[8] "UMCOBS01"; uint32 version (1); uint32 columns;
+//   uint64 records; uint64 seed; uint64 first (counter of record 0);
+//   int32 model; uint32 reserved; double beta;          -- 56 bytes
+//   char names[columns][32] (NUL-padded column names);
+//   double data[records][columns].
+// `records` is rewritten after every append, so a stream cut short by a crash
+// still reads back every record its header counts.
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+namespace {
+constexpr char kObsMagic[8] = {'U', 'M', 'C', 'O', 'B', 'S', '0', '1'};
+constexpr uint32_t kObsName = 32;
+
+struct ObsHeader
+{
+    char magic[8];
+    uint32_t version, columns;
+    uint64_t records, seed, first;
+    int32_t model;
+    uint32_t reserved;
+    double beta;
+};
+static_assert(sizeof(ObsHeader) == 56, "observable stream header layout");
+
+ObsHeader read_header(std::FILE* f, const char* path)
+{
+    ObsHeader h{};
+    if (std::fread(&h, sizeof h, 1, f) != 1 || std::memcmp(h.magic, kObsMagic, 8) != 0 || h.version != 1 ||
+        h.columns == 0)
+        throw umc::Error(UMC_ERR_INVALID_ARGUMENT, std::string("not an observable stream: ") + path);
+    return h;
+}
+}  // namespace
+
+struct umc_obs_stream
+{
+    std::FILE* f = nullptr;
+    ObsHeader h{};
+};
+
+extern "C" {
+
+int umc_obs_stream_create(const char* path, uint32_t columns, const char* const* names, uint64_t seed,
+                          uint64_t first, int32_t model, double beta, umc_obs_stream** out)
+{
+    return umc::sguard([&] {
+        if (!path || !out) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (columns == 0 || columns > 4096) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "1 to 4096 columns");
+        auto* s = new umc_obs_stream;
+        s->f = std::fopen(path, "w+b");
+        if (!s->f) {
+            delete s;
+            throw umc::Error(UMC_ERR_INVALID_ARGUMENT, std::string("cannot create ") + path);
+        }
+        std::memcpy(s->h.magic, kObsMagic, 8);
+        s->h.version = 1;
+        s->h.columns = columns;
+        s->h.seed = seed;
+        s->h.first = first;
+        s->h.model = model;
+        s->h.beta = beta;
+        std::vector<char> nm(size_t(columns) * kObsName, 0);
+        for (uint32_t c = 0; names && c < columns; ++c)
+            if (names[c]) std::strncpy(nm.data() + size_t(c) * kObsName, names[c], kObsName - 1);
+        const bool ok = std::fwrite(&s->h, sizeof s->h, 1, s->f) == 1 && std::fwrite(nm.data(), 1, nm.size(), s->f) == nm.size();
+        if (!ok || std::fflush(s->f) != 0) {
+            std::fclose(s->f);
+            delete s;
+            throw umc::Error(UMC_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
+        }
+        *out = s;
+    });
+}
+
+int umc_obs_stream_append(umc_obs_stream* s, const double* records, uint64_t n)
+{
+    return umc::sguard([&] {
+        if (!s || (n && !records)) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (n == 0) return;
+        const long data = long(sizeof(ObsHeader) + size_t(s->h.columns) * kObsName);
+        const uint64_t vals = n * s->h.columns;
+        if (std::fseek(s->f, data + long(s->h.records * s->h.columns * sizeof(double)), SEEK_SET) != 0 ||
+            std::fwrite(records, sizeof(double), vals, s->f) != vals)
+            throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "observable stream: write failed");
+        s->h.records += n;
+        if (std::fflush(s->f) != 0 || std::fseek(s->f, 0, SEEK_SET) != 0 || std::fwrite(&s->h, sizeof s->h, 1, s->f) != 1 ||
+            std::fflush(s->f) != 0)
+            throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "observable stream: header update failed");
+    });
+}
+
+int umc_obs_stream_close(umc_obs_stream* s)
+{
+    return umc::sguard([&] {
+        if (!s) return;
+        const int rc = std::fclose(s->f);
+        delete s;
+        if (rc != 0) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "observable stream: close failed");
+    });
+}
+
+int umc_obs_stream_info(const char* path, uint32_t* columns, uint64_t* records, uint64_t* seed, uint64_t* first,
+                        int32_t* model, double* beta, char* names)
+{
+    return umc::sguard([&] {
+        if (!path) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "null path");
+        std::FILE* f = std::fopen(path, "rb");
+        if (!f) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path);
+        try {
+            const ObsHeader h = read_header(f, path);
+            if (columns) *columns = h.columns;
+            if (records) *records = h.records;
+            if (seed) *seed = h.seed;
+            if (first) *first = h.first;
+            if (model) *model = h.model;
+            if (beta) *beta = h.beta;
+            if (names && std::fread(names, 1, size_t(h.columns) * kObsName, f) != size_t(h.columns) * kObsName)
+                throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "observable stream: truncated names");
+        } catch (...) {
+            std::fclose(f);
+            throw;
+        }
+        std::fclose(f);
+    });
+}
+
+int umc_obs_stream_read(const char* path, uint64_t first_record, uint64_t n, double* out)
+{
+    return umc::sguard([&] {
+        if (!path || (n && !out)) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        std::FILE* f = std::fopen(path, "rb");
+        if (!f) throw umc::Error(UMC_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path);
+        try {
+            const ObsHeader h = read_header(f, path);
+            if (first_record > h.records || n > h.records - first_record)
+                throw umc::Error(UMC_ERR_OUT_OF_RANGE, "observable stream: records beyond the stream");
+            const long at = long(sizeof h + size_t(h.columns) * kObsName + first_record * h.columns * sizeof(double));
+            const uint64_t vals = n * h.columns;
+            if (std::fseek(f, at, SEEK_SET) != 0 || std::fread(out, sizeof(double), vals, f) != vals)
+                throw umc::Error(UMC_ERR_INVALID_ARGUMENT, "observable stream: truncated data");
+        } catch (...) {
+            std::fclose(f);
+            throw;
+        }
+        std::fclose(f);
+    });
+}
+
+}  // extern "C"
