@@ -5,10 +5,14 @@ Every chain is checked segment by segment against the single-chain oracle
 square lattice, keyed by the chain's seed) and the exchange round against the
 oracle's swap rule, both from identical states.
 """
+import os
+
 import numpy as np
 import pytest
 
 from helpers import checker_position, relabel_edges, square_edges
+
+HERE = os.path.dirname(os.path.abspath(__file__))
 
 pytestmark = pytest.mark.gpu
 
@@ -106,3 +110,34 @@ def test_batch_energy_per_site_orders_with_beta(umc):
     e = rec[:, :, :, 0].mean(axis=0) / (32 * 32)
     assert (np.diff(e, axis=1) < 0.02).all()
     assert e[0, 0] > e[0, -1]
+
+
+def test_autotuner_file_cache(tmp_path):
+    """With UMC_TUNE_CACHE set, a batch's tuned launch shapes are appended to
+    that file keyed by (GPU, kernel, L, chains, sweeps per exchange), and a
+    later process takes them from the file instead of timing candidates: an
+    entry edited by hand is what the next batch uses."""
+    import subprocess
+    import sys
+
+    root = os.path.dirname(HERE)
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "import numpy as np, universal_classical_montecarlo_b200 as umc\n"
+            "b = umc.Batch([16, 32], np.stack([np.geomspace(0.8, 1.3, 4)] * 2), width=1.0, sweeps_per_exchange=3)\n"
+            "print(*[b.config(L)[k] for L in (16, 32) for k in ('chains_per_cta', 'ctas_per_chain', 'block')])\n"
+            ) % root
+    path = tmp_path / "tune.txt"
+    env = dict(os.environ, UMC_TUNE_CACHE=str(path))
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = path.read_text().split()
+    assert len(lines) == 8 and "/L16/" in path.read_text() and "/L32/" in path.read_text()
+    first = [int(v) for v in r.stdout.split()]
+    # hand-edit the L = 16 entry: one chain per CTA, 64 threads
+    text = "\n".join(ln if "/L16/" not in ln else ln.split()[0] + " 1 1 64" for ln in path.read_text().splitlines())
+    path.write_text(text + "\n")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    second = [int(v) for v in r.stdout.split()]
+    assert second[:3] == [1, 1, 64] and second[3:] == first[3:]
+    assert len(path.read_text().split()) == 8  # nothing re-tuned, nothing appended

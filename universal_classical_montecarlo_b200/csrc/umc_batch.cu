@@ -28,6 +28,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -36,6 +38,7 @@
 
 #include "umc_chain.hpp"
 #include "umc_spin_kernels.cuh"
+#include "umc_nvtx.hpp"
 
 namespace cg = cooperative_groups;
 
@@ -330,6 +333,41 @@ struct GroupCfg
 
 std::mutex g_tune_mutex;
 std::map<std::string, GroupCfg> g_tune_cache;
+bool g_tune_file_loaded = false;
+
+// The autotuner's file cache: when UMC_TUNE_CACHE names a file, its lines
+// "<key> <chains per CTA> <CTAs per chain> <block>" are read once per
+// process and every new tuning result is appended, so later processes on the
+// same kind of GPU skip the timing runs.  The key holds the GPU name, the
+// model and kernel, the lattice side, the chain count and the sweeps per
+// exchange.  Call with g_tune_mutex held.
+const char* tune_file() { return std::getenv("UMC_TUNE_CACHE"); }
+
+void load_tune_file()
+{
+    if (g_tune_file_loaded) return;
+    g_tune_file_loaded = true;
+    const char* path = tune_file();
+    if (!path || !*path) return;
+    std::FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    char key[512];
+    unsigned cpc, cpk, block;
+    while (std::fscanf(f, "%511s %u %u %u", key, &cpc, &cpk, &block) == 4)
+        if (cpc >= 1 && cpc <= kMaxCpc && cpk >= 1 && cpk <= kMaxShares && block >= 32 && block <= 1024 && block % 32 == 0)
+            g_tune_cache[key] = GroupCfg{cpc, cpk, block};
+    std::fclose(f);
+}
+
+void store_tune_file(const std::string& key, const GroupCfg& c)
+{
+    const char* path = tune_file();
+    if (!path || !*path) return;
+    if (std::FILE* f = std::fopen(path, "a")) {
+        std::fprintf(f, "%s %u %u %u\n", key.c_str(), c.cpc, c.cpk, c.block);
+        std::fclose(f);
+    }
+}
 
 }  // namespace
 }  // namespace umc
@@ -447,10 +485,14 @@ GroupCfg autotune(umc_batch* b, umc_batch::Group& g)
 {
     cudaDeviceProp prop{};
     cuda_check(cudaGetDeviceProperties(&prop, b->device), "device properties");
-    const std::string key = std::string(prop.name) + "/L" + std::to_string(g.L) + "/n" + std::to_string(g.chains.size()) +
+    std::string gpu = prop.name;
+    for (char& ch : gpu)
+        if (ch == ' ') ch = '_';
+    const std::string key = gpu + "/xy_batch_segment/L" + std::to_string(g.L) + "/n" + std::to_string(g.chains.size()) +
                             "/s" + std::to_string(b->sweeps_per_exchange);
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
+        load_tune_file();
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) return it->second;
     }
@@ -492,7 +534,7 @@ GroupCfg autotune(umc_batch* b, umc_batch::Group& g)
     scratch.free_();
     b->launches = 0;
     std::lock_guard<std::mutex> lock(g_tune_mutex);
-    g_tune_cache[key] = best;
+    if (g_tune_cache.emplace(key, best).second) store_tune_file(key, best);
     return best;
 }
 
@@ -758,6 +800,7 @@ int umc_batch_get_field(umc_batch* b, uint32_t chain, float* theta)
 int umc_batch_enqueue(umc_batch* b, uint64_t n_segments)
 {
     return bguard([&] {
+        NvtxRange range("umc_batch_enqueue");
         if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
         batch_scope(b);
         for (uint64_t s = 0; s < n_segments; ++s) cuda_check(cudaGraphLaunch(b->graph, b->stream), "segment graph");
@@ -793,6 +836,7 @@ int umc_batch_fetch(umc_batch* b, double* records, uint64_t capacity, uint64_t* 
 int umc_batch_run(umc_batch* b, uint64_t n_segments, double* records)
 {
     return bguard([&] {
+        NvtxRange range("umc_batch_run");
         if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
         uint64_t done = 0;
         {

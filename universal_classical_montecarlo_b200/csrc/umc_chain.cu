@@ -21,6 +21,7 @@
 #include "umc_gauge.hpp"
 #include "umc_spin_kernels.cuh"
 #include "umc_fused.cuh"
+#include "umc_nvtx.hpp"
 #include "umc_wolff_tiled.cuh"
 
 namespace umc {
@@ -96,6 +97,7 @@ void ising_wolff_thresholds(int32_t J, double beta, unsigned long long cw[2])
 
 LaunchScope::LaunchScope(umc_chain* chain, int k) : c(chain), kind(k)
 {
+    nvtxRangePushA(kernel_kind_name(k));
     c->launches[k]++;
     if (!c->timing) return;
     if (c->event_pool.size() < 2) {
@@ -112,6 +114,7 @@ LaunchScope::LaunchScope(umc_chain* chain, int k) : c(chain), kind(k)
 
 LaunchScope::~LaunchScope()
 {
+    nvtxRangePop();
     if (!a) return;
     cudaEvent_t b = c->event_pool.back();
     c->event_pool.pop_back();
@@ -1400,6 +1403,7 @@ int umc_chain_observe(umc_chain* c, double* record)
 int umc_metropolis_run(umc_chain* c, double beta, uint64_t n_sweeps, double* records)
 {
     return guarded([&] {
+        NvtxRange range("umc_metropolis_run");
         if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
         device_scope(c);
         run_chunked(c, n_sweeps, records, nullptr, false, [&](uint64_t m) { enqueue_sweeps(c, beta, m); });
@@ -1409,6 +1413,7 @@ int umc_metropolis_run(umc_chain* c, double beta, uint64_t n_sweeps, double* rec
 int umc_wolff_run(umc_chain* c, double beta, uint64_t n_flips, uint64_t* sizes, double* records)
 {
     return guarded([&] {
+        NvtxRange range("umc_wolff_run");
         if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
         device_scope(c);
         run_chunked(c, n_flips, records, sizes, true, [&](uint64_t m) { enqueue_flips(c, beta, m, records != nullptr); });
@@ -1418,6 +1423,7 @@ int umc_wolff_run(umc_chain* c, double beta, uint64_t n_flips, uint64_t* sizes, 
 int umc_hybrid_run(umc_chain* c, double beta, uint64_t n_steps, uint64_t* sizes, double* records)
 {
     return guarded([&] {
+        NvtxRange range("umc_hybrid_run");
         if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
         device_scope(c);
         run_chunked(c, n_steps, records, sizes, true, [&](uint64_t m) { enqueue_hybrid(c, beta, m); });
@@ -1427,6 +1433,7 @@ int umc_hybrid_run(umc_chain* c, double beta, uint64_t n_steps, uint64_t* sizes,
 int umc_metropolis_enqueue(umc_chain* c, double beta, uint64_t n_sweeps)
 {
     return guarded([&] {
+        NvtxRange range("umc_metropolis_enqueue");
         if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
         device_scope(c);
         enqueue_sweeps(c, beta, n_sweeps);
@@ -1436,6 +1443,7 @@ int umc_metropolis_enqueue(umc_chain* c, double beta, uint64_t n_sweeps)
 int umc_wolff_enqueue(umc_chain* c, double beta, uint64_t n_flips)
 {
     return guarded([&] {
+        NvtxRange range("umc_wolff_enqueue");
         if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
         device_scope(c);
         enqueue_flips(c, beta, n_flips, true);
@@ -1445,6 +1453,7 @@ int umc_wolff_enqueue(umc_chain* c, double beta, uint64_t n_flips)
 int umc_hybrid_enqueue(umc_chain* c, double beta, uint64_t n_steps)
 {
     return guarded([&] {
+        NvtxRange range("umc_hybrid_enqueue");
         if (!c) throw Error(UMC_ERR_INVALID_ARGUMENT, "null chain");
         device_scope(c);
         enqueue_hybrid(c, beta, n_steps);

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <vector>
 
+#include "umc_nvtx.hpp"
 #include "umc_chain.hpp"
 #include "umc_spin_kernels.cuh"
 #include "umc_learn_kernels.cuh"
@@ -440,6 +441,7 @@ int umc_mlp_clear_configs(umc_mlp* n)
 int umc_mlp_train(umc_mlp* n, uint64_t steps, uint32_t batch, double lr, double* losses)
 {
     return lguard([&] {
+        NvtxRange range("umc_mlp_train");
         if (!n) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
         if (!n->n_configs) throw Error(UMC_ERR_STATE, "no training configurations");
         if (batch == 0 || batch > (1u << 24)) throw Error(UMC_ERR_INVALID_ARGUMENT, "batch out of range");
@@ -600,6 +602,7 @@ int umc_u1batch_get_field(umc_u1batch* b, uint32_t chain, float* theta)
 int umc_u1batch_enqueue(umc_u1batch* b, uint64_t n_sweeps, const umc_mlp* net)
 {
     return lguard([&] {
+        NvtxRange range("umc_u1batch_enqueue");
         if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
         scope(b->device);
         enqueue_sweeps(b, n_sweeps, net, nullptr);
@@ -626,6 +629,7 @@ int umc_u1batch_fetch(umc_u1batch* b, double* records, uint64_t max_sweeps, uint
 int umc_u1batch_run(umc_u1batch* b, uint64_t n_sweeps, const umc_mlp* net, double* records)
 {
     return lguard([&] {
+        NvtxRange range("umc_u1batch_run");
         if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
         if (records && n_sweeps > b->max_records) throw Error(UMC_ERR_INVALID_ARGUMENT, "more sweeps than record slots");
         scope(b->device);
