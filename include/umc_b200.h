@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define UMC_ABI_VERSION 1
+#define UMC_ABI_VERSION 2
 
 typedef enum umc_status {
     UMC_OK = 0,
@@ -302,7 +302,16 @@ typedef struct umc_batch_desc {
     int32_t device;
     void* stream;                 /* NULL: the batch owns one                    */
     uint64_t max_records;         /* segments kept on the device (0: 1024)       */
+    uint32_t first_ladder;        /* global index of ladder 0 (sharding, below)   */
 } umc_batch_desc;
+
+/* Sharding a batch over ranks (one process per GPU): the ladders are
+ * independent units, so rank r of W creates a batch of its contiguous range of
+ * ladders [l0, l1) with first_ladder = l0 and the same seed; ladder l and the
+ * chains in it draw from the keys of global ladder l0 + l (chain seeds from
+ * global chain index, ladder seeds from global ladder index), so the union of
+ * the ranks' batches runs exactly the chains and exchanges of one unsharded
+ * batch.  No data-path collective is needed; records are gathered at the end. */
 
 typedef struct umc_batch umc_batch;
 
@@ -396,6 +405,8 @@ typedef struct umc_u1batch_desc {
     int32_t device;
     void* stream;          /* cudaStream_t, NULL = own stream */
     uint64_t max_records;  /* record slots (sweeps) between fetches; 0 = 1024 */
+    uint32_t first_chain;  /* global index of chain 0: chain c draws as global chain first_chain + c
+                              (sharding over ranks, as first_ladder of umc_batch_desc) */
 } umc_u1batch_desc;
 
 /* Record per sweep and chain: [S, mean plaquette, topological charge

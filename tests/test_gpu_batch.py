@@ -141,3 +141,58 @@ def test_autotuner_file_cache(tmp_path):
     second = [int(v) for v in r.stdout.split()]
     assert second[:3] == [1, 1, 64] and second[3:] == first[3:]
     assert len(path.read_text().split()) == 8  # nothing re-tuned, nothing appended
+
+
+def test_sharded_batch_equals_the_whole_batch(umc):
+    """The ladders shard over ranks with no exchange between shards: the two
+    shards of a 2-rank split (run here one after the other on one GPU, no
+    kernel waiting on another) reproduce the unsharded batch -- the same
+    chain and ladder keys, fields bit for bit, the same temperature maps and
+    records (energies to FP64 summation order)."""
+    Ls = np.array([16, 32, 16, 8, 32])
+    R = 4
+    betas = np.stack([_geometric(0.8, 1.3, R)] * len(Ls))
+    whole = umc.Batch(Ls, betas, width=1.0, sweeps_per_exchange=3, seed=21)
+    whole.randomize(8)
+    rec_w = whole.run(4)
+    parts, recs = [], []
+    for rank in range(2):
+        b = umc.Batch.shard(Ls, betas, rank, 2, width=1.0, sweeps_per_exchange=3, seed=21)
+        b.randomize(8)
+        recs.append(b.run(4))
+        parts.append(b)
+    lo1 = parts[1].ladder_range[0]
+    assert parts[0].ladder_range == (0, lo1) and parts[1].ladder_range == (lo1, len(Ls))
+    cs_w, ls_w = whole.seeds()
+    cs = np.concatenate([p.seeds()[0] for p in parts])
+    ls = np.concatenate([p.seeds()[1] for p in parts])
+    np.testing.assert_array_equal(cs, cs_w)
+    np.testing.assert_array_equal(ls, ls_w)
+    recs[1][..., 3] += lo1 * R  # a shard's records name its chains by local index
+    rec = np.concatenate(recs, axis=1)
+    np.testing.assert_array_equal(rec[..., 3], rec_w[..., 3])  # which chain held each slot
+    np.testing.assert_allclose(rec, rec_w, rtol=1e-12, atol=1e-9)
+    tmap = np.concatenate([p.temperature_map() + p.ladder_range[0] * R for p in parts])
+    np.testing.assert_array_equal(tmap, whole.temperature_map())
+    for c in range(whole.n_chains):
+        p = parts[0] if c < lo1 * R else parts[1]
+        np.testing.assert_array_equal(p.get_field(c - p.ladder_range[0] * R), whole.get_field(c))
+
+
+def test_sharded_u1batch_equals_the_whole_batch(umc):
+    whole = umc.U1Batch(7, 8, 2.0, width=0.5, seed=3)
+    whole.randomize(4)
+    rec_w = whole.run(5)
+    recs, parts = [], []
+    for rank in range(3):
+        b = umc.U1Batch.shard(7, 8, 2.0, rank, 3, width=0.5, seed=3)
+        b.randomize(4)
+        recs.append(b.run(5))
+        parts.append(b)
+    np.testing.assert_array_equal(np.concatenate([p.seeds() for p in parts]), whole.seeds())
+    np.testing.assert_allclose(np.concatenate(recs, axis=1), rec_w, rtol=1e-12, atol=1e-12)
+    c = 0
+    for p in parts:
+        for k in range(p.n_chains):
+            np.testing.assert_array_equal(p.get_field(k), whole.get_field(c))
+            c += 1

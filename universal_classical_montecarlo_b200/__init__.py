@@ -188,6 +188,7 @@ class BatchDesc(C.Structure):
         ("device", _i32),
         ("stream", _vp),
         ("max_records", _u64),
+        ("first_ladder", _u32),
     ]
 
 
@@ -684,11 +685,46 @@ class Chain:
         return f.value, s.value
 
 
+def shard_range(n_units: int, rank: int, world: int):
+    """The contiguous range [lo, hi) of n_units independent units (ladders,
+    chains) that rank `rank` of `world` owns: sizes differ by at most one,
+    lower ranks take the larger shares."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    q, r = divmod(n_units, world)
+    lo = rank * q + min(rank, r)
+    return lo, lo + q + (1 if rank < r else 0)
+
+
+def gather_shards(local, group=None):
+    """All ranks' arrays (e.g. the records of their shards, ladders or chains
+    along axis 1) concatenated in rank order along axis 1, on every rank,
+    through torch.distributed (gloo on CPU, NCCL on GPUs)."""
+    import torch.distributed as dist
+
+    parts = [None] * dist.get_world_size(group)
+    dist.all_gather_object(parts, np.asarray(local), group=group)
+    return np.concatenate(parts, axis=1)
+
+
 class Batch:
-    """Independent XY chains in replica-exchange ladders (umc_batch_*)."""
+    """Independent XY chains in replica-exchange ladders (umc_batch_*).
+
+    first_ladder: global index of this batch's first ladder, for a shard of a
+    larger batch (Batch.shard); its chains then run exactly as in the
+    unsharded batch."""
+
+    @classmethod
+    def shard(cls, L, betas, rank, world, **kw):
+        """The batch of rank `rank` of `world`: its contiguous range of the
+        ladders (shard_range), keyed as in the whole batch."""
+        lo, hi = shard_range(len(L), rank, world)
+        b = cls(np.asarray(L)[lo:hi], np.asarray(betas)[lo:hi], first_ladder=lo, **kw)
+        b.ladder_range = (lo, hi)
+        return b
 
     def __init__(self, L, betas, *, coupling=1.0, width=1.0, sweeps_per_exchange=10, seed=1, device=0,
-                 max_records=1024):
+                 max_records=1024, first_ladder=0):
         L = np.ascontiguousarray(L, np.uint32)
         betas = np.ascontiguousarray(betas, np.float64)
         if betas.ndim != 2 or betas.shape[0] != len(L):
@@ -700,6 +736,7 @@ class Batch:
         d.coupling, d.width = coupling, width
         d.sweeps_per_exchange = sweeps_per_exchange
         d.seed, d.device, d.stream, d.max_records = seed, device, None, max_records
+        d.first_ladder = first_ladder
         h = _vp()
         check(lib.umc_batch_create(C.byref(d), C.byref(h)))
         self._h = h
@@ -812,6 +849,7 @@ class U1BatchDesc(C.Structure):
         ("device", _i32),
         ("stream", _vp),
         ("max_records", _u64),
+        ("first_chain", _u32),
     ]
 
 
@@ -940,10 +978,20 @@ class U1Batch:
     Metropolis-Hastings with a ProposalNet.  Records per sweep and chain:
     [S, mean plaquette, Q, accepted]."""
 
-    def __init__(self, n_chains, L, beta, *, width=0.5, seed=1, device=0, max_records=1024):
+    @classmethod
+    def shard(cls, n_chains, L, beta, rank, world, **kw):
+        """Rank `rank` of `world`'s contiguous range of n_chains chains
+        (shard_range), keyed as in the whole batch."""
+        lo, hi = shard_range(n_chains, rank, world)
+        b = cls(hi - lo, L, beta, first_chain=lo, **kw)
+        b.chain_range = (lo, hi)
+        return b
+
+    def __init__(self, n_chains, L, beta, *, width=0.5, seed=1, device=0, max_records=1024, first_chain=0):
         d = U1BatchDesc()
         d.n_chains, d.L, d.beta, d.width = n_chains, L, beta, width
         d.seed, d.device, d.stream, d.max_records = seed, device, None, max_records
+        d.first_chain = first_chain
         h = _vp()
         check(lib.umc_u1batch_create(C.byref(d), C.byref(h)))
         self._h = h

@@ -596,13 +596,15 @@ void create_batch(const umc_batch_desc* d, umc_batch* b)
     for (uint32_t l = 0; l < b->n_ladders; ++l) {
         const uint64_t L = d->L[l];
         if (L < 2 || L % 2 || L > 4096) throw Error(UMC_ERR_INVALID_ARGUMENT, "ladder side L must be even, in [2, 4096]");
-        b->ladder_seed[l] = mix64(d->seed + 0xD1B54A32D192ED03ULL * (l + 1));
+        // keys of the global ladder first_ladder + l and its global chains
+        const uint64_t gl = uint64_t(d->first_ladder) + l;
+        b->ladder_seed[l] = mix64(d->seed + 0xD1B54A32D192ED03ULL * (gl + 1));
         for (uint32_t k = 0; k < b->R; ++k) {
             const uint32_t c = l * b->R + k;
             b->L[c] = uint32_t(L);
             b->off[c] = acc;
             acc += L * L;
-            b->chain_seed[c] = mix64(d->seed + kGolden * (c + 1ull));
+            b->chain_seed[c] = mix64(d->seed + kGolden * (gl * b->R + k + 1ull));
             by_L[uint32_t(L)].push_back(c);
         }
     }
@@ -754,7 +756,8 @@ int umc_batch_randomize(umc_batch* b, uint64_t seed)
         batch_scope(b);
         // per-chain init keys derive from the run seed and the chain index
         std::vector<unsigned long long> s(b->n_chains);
-        for (uint32_t c = 0; c < b->n_chains; ++c) s[c] = mix64(seed + kGolden * (c + 1ull));
+        const uint64_t g0 = uint64_t(b->desc.first_ladder) * b->R;  // global index of chain 0
+        for (uint32_t c = 0; c < b->n_chains; ++c) s[c] = mix64(seed + kGolden * (g0 + c + 1ull));
         DevBuf sd;
         sd.alloc(s.size() * 8, "init seeds");
         cuda_check(cudaMemcpy(sd.p, s.data(), s.size() * 8, cudaMemcpyHostToDevice), "init seeds");

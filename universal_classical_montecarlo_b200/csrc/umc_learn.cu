@@ -498,7 +498,8 @@ int umc_u1batch_create(const umc_u1batch_desc* d, umc_u1batch** out)
             b->theta.alloc(per * b->n_chains * 4, "angles");
             cuda_check(cudaMemsetAsync(b->theta.p, 0, per * b->n_chains * 4, b->stream), "cold start");
             b->chain_seed.resize(b->n_chains);
-            for (uint32_t c = 0; c < b->n_chains; ++c) b->chain_seed[c] = mix64(d->seed + kGolden * (c + 1ull));
+            for (uint32_t c = 0; c < b->n_chains; ++c)
+                b->chain_seed[c] = mix64(d->seed + kGolden * (uint64_t(d->first_chain) + c + 1ull));
             b->seeds.alloc(b->n_chains * 8, "seeds");
             cuda_check(cudaMemcpyAsync(b->seeds.p, b->chain_seed.data(), b->n_chains * 8, cudaMemcpyHostToDevice,
                                        b->stream),
@@ -558,7 +559,8 @@ int umc_u1batch_randomize(umc_u1batch* b, uint64_t seed)
         const uint32_t nl = 2 * b->L * b->L;
         std::vector<float> h(size_t(nl) * b->n_chains);
         for (uint32_t c = 0; c < b->n_chains; ++c) {
-            const uint64_t kb = key_base(key_seed(mix64(seed + kGolden * (c + 1ull)), 0, kTagInit));
+            const uint64_t kb =
+                key_base(key_seed(mix64(seed + kGolden * (uint64_t(b->desc.first_chain) + c + 1ull)), 0, kTagInit));
             for (uint32_t i = 0; i < nl; ++i) {
                 KeyedPcg g = KeyedPcg::open(kb, i);
                 h[size_t(c) * nl + colour_index(b->L, i)] = 3.14159265358979f * sym_f32(g.next());
