@@ -348,6 +348,47 @@ int umc_batch_sites(const umc_batch* b, uint64_t* total_sites, uint64_t* kernel_
 /* The stream the batch's segments run on (cudaStream_t). */
 void* umc_batch_stream(const umc_batch* b);
 
+/* ==================================================== one lattice over ranks */
+
+/* Slab domain decomposition of the regular-lattice Metropolis sweep, for a
+ * lattice larger than one GPU (no reference counterpart: the reference runs
+ * one chain in one process, driver.hpp:17-68).  The lattice Lx x Ly x Lz
+ * (Lz = 1 in 2D; Lx, Ly even, Lz 1 or even) is cut along z in 3D, along y in
+ * 2D, into planes; a rank holds planes [first_plane, first_plane + planes)
+ * plus a halo plane on each side in a caller-owned device array (natural
+ * order, x fastest; Ising int8, VectorSpin<N> one float array per component
+ * with stride umc_slab_local_sites).  umc_slab_pass runs one checkerboard
+ * colour over the owned planes; the caller refreshes both halos from the
+ * neighbouring ranks after each pass (the planes at local index 1 and
+ * `planes` are the ones they need).  Sites draw from the keys of their global
+ * colour-major index and sum neighbours in the single-GPU kernels' order, so
+ * the ranks together run exactly the single-GPU chain (Ising bit for bit).
+ * Wolff across slabs (a cross-rank union-find) is not provided. */
+typedef struct umc_slab_desc {
+    int32_t model;        /* UMC_MODEL_ISING (Flip) or UMC_MODEL_VECTOR       */
+    int32_t components;   /* VectorSpin<N>: 1..4                              */
+    uint32_t Lx, Ly, Lz;  /* the whole lattice                                */
+    uint32_t first_plane; /* this rank's first plane along z (3D) or y (2D)   */
+    uint32_t planes;      /* its plane count (>= 1)                           */
+    double coupling;      /* J (integer for Ising)                            */
+    int32_t proposal;     /* UMC_PROPOSAL_FLIP / _SPHERE / _ROTATION          */
+    double width;         /* LocalRotation delta                              */
+    uint64_t seed;        /* the chain's key seed (the same on every rank)    */
+    int32_t device;
+} umc_slab_desc;
+typedef struct umc_slab umc_slab;
+int umc_slab_create(const umc_slab_desc* desc, umc_slab** out);
+int umc_slab_destroy(umc_slab* s);
+/* (planes + 2) x plane sites: halo, owned planes, halo. */
+uint64_t umc_slab_local_sites(const umc_slab* s);
+/* Colour pass `colour` (0 then 1 make sweep `sweep`) of the owned sites of
+ * `field` (device pointer) on `stream` (cudaStream_t, NULL = default). */
+int umc_slab_pass(umc_slab* s, void* field, double beta, uint64_t sweep, uint32_t colour, void* stream);
+/* This rank's part of the last completed sweep's record: [E (bonds whose
+ * colour-1 end it owns), M_0..M_{N-1}, 0.., accepted]; the ranks' parts add up
+ * to the single-GPU record.  Synchronises `stream`. */
+int umc_slab_record(umc_slab* s, double* out, void* stream);
+
 /* ================================================= allocation-free Wolff flip */
 
 /* No counterpart in the reference: an extra entry point for callers that cannot

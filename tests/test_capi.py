@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol(umc):
 
 
 def test_abi_version(umc):
-    assert umc.lib.umc_abi_version() == 1
+    assert umc.lib.umc_abi_version() == 2
 
 
 @pytest.mark.parametrize("Lx,Ly", [(1, 1), (1, 4), (2, 2), (4, 4), (3, 5), (8, 6)])
@@ -222,3 +222,30 @@ def test_payload_graph_errors(umc):
         umc.PairGraph(3, e, payload=np.ones(3))  # one record per edge
     with pytest.raises(ValueError):
         umc.PairGraph(3, e).payloads()
+
+
+def test_slab_descriptions_are_checked(umc):
+    """umc_slab_create refuses what the decomposition cannot run, before any
+    device work: odd or unit extents, planes outside the lattice, other
+    models and proposals."""
+    def create(**kw):
+        d = umc.SlabDesc()
+        d.model, d.components, d.Lx, d.Ly, d.Lz = umc.MODEL_ISING, 1, 8, 8, 1
+        d.first_plane, d.planes, d.coupling, d.proposal, d.seed = 0, 4, 1.0, umc.PROPOSAL_FLIP, 1
+        for k, v in kw.items():
+            setattr(d, k, v)
+        h = umc._vp()
+        rc = umc.lib.umc_slab_create(ctypes.byref(d), ctypes.byref(h))
+        if rc == umc.OK:
+            umc.lib.umc_slab_destroy(h)
+        return rc
+
+    assert create(Lx=7) == umc.ERR_INVALID_ARGUMENT
+    assert create(Ly=1) == umc.ERR_INVALID_ARGUMENT
+    assert create(Lz=3) == umc.ERR_INVALID_ARGUMENT
+    assert create(first_plane=6, planes=3) == umc.ERR_OUT_OF_RANGE
+    assert create(planes=0) == umc.ERR_OUT_OF_RANGE
+    assert create(coupling=0.5) == umc.ERR_INVALID_ARGUMENT
+    assert create(model=umc.MODEL_U1) == umc.ERR_UNSUPPORTED
+    assert create(model=umc.MODEL_VECTOR, components=3, proposal=umc.PROPOSAL_FLIP) == umc.ERR_UNSUPPORTED
+    assert create(model=umc.MODEL_VECTOR, components=5, proposal=umc.PROPOSAL_SPHERE) == umc.ERR_UNSUPPORTED

@@ -707,6 +707,163 @@ def gather_shards(local, group=None):
     return np.concatenate(parts, axis=1)
 
 
+class SlabDesc(C.Structure):
+    _fields_ = [
+        ("model", _i32),
+        ("components", _i32),
+        ("Lx", _u32),
+        ("Ly", _u32),
+        ("Lz", _u32),
+        ("first_plane", _u32),
+        ("planes", _u32),
+        ("coupling", _f64),
+        ("proposal", _i32),
+        ("width", _f64),
+        ("seed", _u64),
+        ("device", _i32),
+    ]
+
+
+_decl("umc_slab_create", _int, C.POINTER(SlabDesc), C.POINTER(_vp))
+_decl("umc_slab_destroy", _int, _vp)
+_decl("umc_slab_local_sites", _u64, _vp)
+_decl("umc_slab_pass", _int, _vp, _vp, _f64, _u64, _u32, _vp)
+_decl("umc_slab_record", _int, _vp, _vp, _vp)
+
+
+class SlabChain:
+    """One periodic Lx x Ly x Lz lattice (Lz = 1 in 2D) split into slabs over
+    the ranks of a torch.distributed group, one process per GPU (umc_slab_*):
+    this rank's planes along z (3D) or y (2D) plus a halo plane on each side
+    live in a torch tensor on its GPU; each colour pass is followed by an
+    exchange of the boundary planes with the two neighbouring ranks
+    (batch_isend_irecv: NCCL device to device, gloo through host copies).
+    Without a process group (world 1) the halos are the slab's own periodic
+    planes.  The ranks together run exactly the single-GPU Chain of the same
+    seed (keys of global site indices); records are summed over the ranks."""
+
+    def __init__(self, model, dims, *, rank=0, world=1, group=None, components=1, coupling=1.0,
+                 proposal=None, width=0.0, seed=1, device=0):
+        import torch
+
+        self.torch = torch
+        Lx, Ly, Lz = (tuple(dims) + (1,))[:3]
+        self.dims = (Lx, Ly, Lz)
+        self.rank, self.world, self.group = rank, world, group
+        total = Lz if Lz > 1 else Ly
+        lo, hi = shard_range(total, rank, world)
+        self.planes_range = (lo, hi)
+        self.planes = hi - lo
+        self.P = Lx * Ly if Lz > 1 else Lx
+        self.model = model
+        self.N = components if model == MODEL_VECTOR else 1
+        if proposal is None:
+            proposal = PROPOSAL_FLIP if model == MODEL_ISING else PROPOSAL_SPHERE
+        d = SlabDesc()
+        d.model, d.components, d.Lx, d.Ly, d.Lz = model, self.N, Lx, Ly, Lz
+        d.first_plane, d.planes, d.coupling, d.proposal, d.width = lo, self.planes, coupling, proposal, width
+        d.seed, d.device = seed, device
+        h = _vp()
+        check(lib.umc_slab_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.nloc = int(lib.umc_slab_local_sites(h))
+        self.device = torch.device("cuda", device)
+        dt = torch.int8 if model == MODEL_ISING else torch.float32
+        self.field = torch.zeros(self.N * self.nloc, dtype=dt, device=self.device)
+        self.stream = torch.cuda.current_stream(self.device)
+        self.sweeps = 0
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h and lib is not None:
+            lib.umc_slab_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _local_planes(self):
+        total = self.dims[2] if self.dims[2] > 1 else self.dims[1]
+        lo, hi = self.planes_range
+        return [(p % total) for p in range(lo - 1, hi + 1)]
+
+    def set_field(self, full):
+        """full: the whole lattice in natural site order ((z Ly + y) Lx + x),
+        shape (sites,) or (sites, N); every rank passes the same array."""
+        a = np.asarray(full).reshape(-1, self.N)
+        planes = self._local_planes()
+        loc = np.concatenate([a[p * self.P:(p + 1) * self.P] for p in planes])  # (nloc, N)
+        soa = np.ascontiguousarray(loc.T).reshape(-1).astype(np.int8 if self.model == MODEL_ISING else np.float32)
+        self.field.copy_(self.torch.from_numpy(soa).to(self.device))
+
+    def get_field(self):
+        """This rank's planes in natural order: (planes * plane sites, N)."""
+        loc = self.field.cpu().numpy().reshape(self.N, self.nloc).T
+        return loc[self.P:(self.planes + 1) * self.P].copy()
+
+    def gather_field(self):
+        """The whole lattice (natural order), on every rank."""
+        if self.world == 1:
+            return self.get_field()
+        import torch.distributed as dist
+
+        parts = [None] * self.world
+        dist.all_gather_object(parts, self.get_field(), group=self.group)
+        return np.concatenate(parts)
+
+    def _plane(self, k):
+        v = self.field.view(self.N, self.nloc)
+        return v[:, k * self.P:(k + 1) * self.P]
+
+    def _exchange(self):
+        """Both halos from the neighbouring ranks' boundary planes."""
+        if self.world == 1:
+            self._plane(0).copy_(self._plane(self.planes))
+            self._plane(self.planes + 1).copy_(self._plane(1))
+            return
+        import torch.distributed as dist
+
+        prev, nxt = (self.rank - 1) % self.world, (self.rank + 1) % self.world
+        cpu = dist.get_backend(self.group) == "gloo"
+        mv = (lambda t: t.cpu()) if cpu else (lambda t: t.contiguous())
+        last, first = mv(self._plane(self.planes)), mv(self._plane(1))
+        lower = self.torch.empty_like(last)
+        upper = self.torch.empty_like(first)
+        # the same order on every rank: sends to next then prev, receives from
+        # prev then next (tags for gloo; NCCL matches each pair's messages in order)
+        ops = [dist.P2POp(dist.isend, last, nxt, self.group, 0), dist.P2POp(dist.isend, first, prev, self.group, 1),
+               dist.P2POp(dist.irecv, lower, prev, self.group, 0), dist.P2POp(dist.irecv, upper, nxt, self.group, 1)]
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+        self._plane(0).copy_(lower.to(self.device))
+        self._plane(self.planes + 1).copy_(upper.to(self.device))
+
+    def sweep(self, beta):
+        """One Metropolis sweep of the whole lattice; returns its record
+        summed over the ranks ([E, M_0..M_{N-1}, .., accepted])."""
+        s = self.stream.cuda_stream
+        for colour in (0, 1):
+            check(lib.umc_slab_pass(self._h, C.c_void_p(self.field.data_ptr()), beta, self.sweeps, colour, s))
+            self._exchange()
+        self.sweeps += 1
+        rec = np.zeros(OBS_STRIDE)
+        check(lib.umc_slab_record(self._h, _ptr(rec), s))
+        if self.world > 1:
+            import torch.distributed as dist
+
+            t = self.torch.from_numpy(rec.copy())
+            if dist.get_backend(self.group) != "gloo":
+                t = t.to(self.device)
+            dist.all_reduce(t, group=self.group)
+            rec = t.cpu().numpy()
+        return rec
+
+    def metropolis(self, beta, n):
+        """n sweeps; their records (n x OBS_STRIDE)."""
+        self._exchange()
+        return np.stack([self.sweep(beta) for _ in range(n)])
+
+
 class Batch:
     """Independent XY chains in replica-exchange ladders (umc_batch_*).
 

@@ -1,0 +1,375 @@
+// umc_slab.cu -- one lattice over several GPUs: slab domain decomposition of
+// the regular-lattice Metropolis sweep (one process per GPU).
+//
+// The lattice Lx x Ly x Lz (Lz = 1 in 2D) is cut along its slowest axis of
+// extent above 1 (z in 3D, y in 2D) into contiguous planes; a rank holds its
+// planes [first, first + planes) plus one halo plane on each side, in natural
+// order (x fastest), one array per component (component c of local site q at
+// field[c * local_sites + q]).  A colour pass updates the rank's sites of one
+// checkerboard colour; their neighbours of the other colour lie in the slab
+// or its halos, which the caller refreshes from the neighbouring ranks between
+// passes (the boundary planes only: torch.distributed send/recv over NCCL, or
+// any copy).  Every site draws from the keyed stream of its GLOBAL colour-major
+// index, and sums its neighbours in the order of the single-GPU stencil
+// kernels (umc_spin_kernels.cuh StencilTopo), so the union of the ranks'
+// updates is the single-GPU chain: bit for bit for Ising (integer thresholds),
+// and to the same FP32 arithmetic for VectorSpin<N>.
+//
+// The reference has no decomposition (one chain per driver object,
+// driver.hpp:17-68); the per-site rule is its Metropolis::sweep body
+// (driver.hpp:34-42) with Ising::energy_diff_at (example/ising.hpp:46-56) or
+// VectorSpin::energy_diff_at (example/vector_spin.hpp:50-60).
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "umc_chain.hpp"
+#include "umc_nvtx.hpp"
+#include "umc_spin_kernels.cuh"
+
+namespace umc {
+namespace {
+
+struct SlabArgs
+{
+    void* field;
+    uint32_t Lx, Ly, Lz;
+    uint32_t along_z;  // 1: planes are z planes (3D); 0: rows y (2D)
+    uint32_t first, planes;
+    uint32_t P;        // sites per plane
+    uint32_t nloc;     // (planes + 2) * P
+    uint32_t half;     // global sites / 2
+    uint32_t colour;
+    uint64_t kbase;
+    float J, beta, delta;
+    double J64, beta64;
+    float err;
+    const uint32_t* tm1;  // Ising: accept iff draw <= tm1[s h + D]
+    int32_t D, Jint;
+    PassOut out;
+};
+
+// Owned site q of the pass's colour -> its local index, its global
+// colour-major index, and its neighbours' local indices in StencilTopo's
+// order: the two same-row neighbours (x+1, x-1 when the site sits on an even
+// x of its row's colour pattern, else x-1, x+1), then y-1, y+1, then z-1, z+1,
+// each pair only where that extent exceeds 1.
+struct SlabSite
+{
+    uint32_t li, k, deg;
+    uint32_t nb[6];
+};
+
+__device__ __forceinline__ SlabSite slab_site(const SlabArgs& a, uint32_t q)
+{
+    const uint32_t H = a.Lx / 2;
+    const uint32_t per_plane = a.P / 2;
+    const uint32_t pl = q / per_plane, r = q - pl * per_plane;
+    uint32_t x, y, z;
+    if (a.along_z) {
+        y = r / H;
+        const uint32_t i = r - y * H;
+        z = a.first + pl;
+        x = 2 * i + ((y + z + a.colour) & 1u);
+    } else {
+        y = a.first + pl;
+        z = 0;
+        x = 2 * r + ((y + a.colour) & 1u);
+    }
+    SlabSite s;
+    const uint32_t lp = pl + 1;  // local plane (0 and planes + 1 are the halos)
+    const uint32_t inplane = a.along_z ? y * a.Lx : 0u;
+    s.li = lp * a.P + inplane + x;
+    const uint32_t g = (z * a.Ly + y) * a.Lx + x;
+    s.k = a.colour * a.half + g / 2;
+    const uint32_t xp = x + 1 == a.Lx ? 0u : x + 1, xm = x == 0 ? a.Lx - 1 : x - 1;
+    const uint32_t row = lp * a.P + inplane;
+    const bool even = ((x & 1u) == 0u);
+    s.nb[0] = row + (even ? xp : xm);
+    s.nb[1] = row + (even ? xm : xp);
+    s.deg = 2;
+    if (a.Ly > 1) {
+        if (a.along_z) {
+            const uint32_t ym = y == 0 ? a.Ly - 1 : y - 1, yp = y + 1 == a.Ly ? 0u : y + 1;
+            s.nb[s.deg++] = lp * a.P + ym * a.Lx + x;
+            s.nb[s.deg++] = lp * a.P + yp * a.Lx + x;
+        } else {
+            s.nb[s.deg++] = (lp - 1) * a.P + x;
+            s.nb[s.deg++] = (lp + 1) * a.P + x;
+        }
+    }
+    if (a.along_z && a.Lz > 1) {
+        s.nb[s.deg++] = (lp - 1) * a.P + y * a.Lx + x;
+        s.nb[s.deg++] = (lp + 1) * a.P + y * a.Lx + x;
+    }
+    return s;
+}
+
+template <int N>
+__device__ __noinline__ double slab_log_ratio64(const SlabArgs& a, SlabSite st, SpinVal<N> cand, SpinVal<N> s)
+{
+    const float* f = static_cast<const float*>(a.field);
+    double d = 0.0;
+    for (uint32_t m = 0; m < st.deg; ++m) {
+        double pj = 0.0, oj = 0.0;
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+            const double v = f[c * a.nloc + st.nb[m]];
+            pj += double(cand.v[c]) * v;
+            oj += double(s.v[c]) * v;
+        }
+        d += -a.J64 * (pj - oj);
+    }
+    return -a.beta64 * d;
+}
+
+template <int N, int PROP>
+__global__ void __launch_bounds__(kBlock, 4) slab_vector_pass(SlabArgs a)
+{
+    double acc[kObs] = {0, 0, 0, 0, 0, 0, 0, 0};
+    float* f = static_cast<float*>(a.field);
+    const uint32_t count = a.planes * (a.P / 2);
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+        const SlabSite st = slab_site(a, q);
+        float s[N], h[N];
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+            s[c] = f[c * a.nloc + st.li];
+            h[c] = 0.0f;
+        }
+        for (uint32_t m = 0; m < st.deg; ++m)
+#pragma unroll
+            for (int c = 0; c < N; ++c) h[c] += f[c * a.nloc + st.nb[m]];
+        KeyedPcg g = KeyedPcg::open(a.kbase, st.k);
+        float cand[N];
+        bool ok = true;
+        if constexpr (PROP == kPropSphere) sphere_sample<N>(g, cand);
+        else ok = local_rotation<N>(g, a.delta, s, cand);
+        bool acc_ok = false;
+        if (ok) {
+            const float dE = -a.J * (vdot<N>(cand, h) - vdot<N>(s, h));
+            acc_ok = metropolis_accept(g, -a.beta * dE, a.err, [&] {
+                SpinVal<N> cv, sv;
+#pragma unroll
+                for (int c = 0; c < N; ++c) {
+                    cv.v[c] = cand[c];
+                    sv.v[c] = s[c];
+                }
+                return slab_log_ratio64<N>(a, st, cv, sv);
+            });
+        }
+        if (acc_ok) {
+#pragma unroll
+            for (int c = 0; c < N; ++c) {
+                s[c] = cand[c];
+                f[c * a.nloc + st.li] = cand[c];
+            }
+        }
+        // every bond joins the two colours: count it in the colour-1 pass
+        if (a.colour == 1u) acc[0] += double(-a.J * vdot<N>(s, h));
+#pragma unroll
+        for (int c = 0; c < N; ++c) acc[1 + c] += double(s[c]);
+        acc[7] += acc_ok ? 1.0 : 0.0;
+    }
+    finish_pass<kObs>(acc, a.out);
+}
+
+__global__ void __launch_bounds__(kBlock) slab_ising_pass(SlabArgs a)
+{
+    int64_t e_acc = 0, m_acc = 0, n_acc = 0;
+    int8_t* sp = static_cast<int8_t*>(a.field);
+    const uint32_t count = a.planes * (a.P / 2);
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x) {
+        const SlabSite st = slab_site(a, q);
+        int32_t h = 0;
+        for (uint32_t m = 0; m < st.deg; ++m) h += sp[st.nb[m]];
+        const int32_t s = sp[st.li];
+        // one draw per site: output k % 16 of the stream of id k / 16, the
+        // engine's Ising keying; integer thresholds make the decision exact
+        const uint32_t r = group_draw(a.kbase, st.k);
+        const bool flip = r <= a.tm1[s * h + a.D];
+        const int32_t ns = flip ? -s : s;
+        if (flip) sp[st.li] = int8_t(ns);
+        if (a.colour == 1u) e_acc += ns * h;
+        m_acc += ns;
+        n_acc += flip;
+    }
+    double v[kObs] = {double(-int64_t(a.Jint) * e_acc), double(m_acc), 0, 0, 0, 0, 0, double(n_acc)};
+    finish_pass<kObs>(v, a.out);
+}
+
+}  // namespace
+}  // namespace umc
+
+using namespace umc;
+
+struct umc_slab
+{
+    umc_slab_desc desc{};
+    uint32_t P = 0, nloc = 0, half = 0, along_z = 0, deg = 0;
+    int device = 0;
+    uint32_t grid = 0;
+    DevBuf ctl, partials, record, tm1;
+    std::vector<uint32_t> h_tm1;
+    double tm1_beta = std::nan("");
+    int32_t J_int = 0;
+};
+
+namespace {
+
+template <class F>
+int slab_guard(F&& f)
+{
+    try {
+        set_last_error("");
+        f();
+        return UMC_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return UMC_ERR_INVALID_ARGUMENT;
+    }
+}
+
+template <int N>
+void launch_vector(const umc_slab* s, const SlabArgs& a, cudaStream_t st)
+{
+    if (s->desc.proposal == UMC_PROPOSAL_ROTATION) slab_vector_pass<N, kPropRotation><<<s->grid, kBlock, 0, st>>>(a);
+    else slab_vector_pass<N, kPropSphere><<<s->grid, kBlock, 0, st>>>(a);
+}
+
+}  // namespace
+
+extern "C" {
+
+int umc_slab_create(const umc_slab_desc* d, umc_slab** out)
+{
+    return slab_guard([&] {
+        if (!d || !out) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        const uint64_t Lx = d->Lx, Ly = d->Ly, Lz = d->Lz;
+        if (Lx < 2 || Lx % 2 || Ly < 2 || Ly % 2 || (Lz != 1 && Lz % 2))
+            throw Error(UMC_ERR_INVALID_ARGUMENT, "slabs need Lx and Ly even and at least 2, Lz 1 or even");
+        if (Lx * Ly * Lz > 0xFFFFFFFFull) throw Error(UMC_ERR_OVERFLOW, "lattice exceeds uint32 sites");
+        const uint64_t planes_total = Lz > 1 ? Lz : Ly;
+        if (d->planes == 0 || uint64_t(d->first_plane) + d->planes > planes_total)
+            throw Error(UMC_ERR_OUT_OF_RANGE, "slab planes outside the lattice");
+        if (d->model == UMC_MODEL_ISING) {
+            if (d->coupling != std::floor(d->coupling) || std::fabs(d->coupling) > 1e6)
+                throw Error(UMC_ERR_INVALID_ARGUMENT, "Ising coupling J must be an integer");
+            if (d->proposal != UMC_PROPOSAL_FLIP) throw Error(UMC_ERR_UNSUPPORTED, "Ising slabs use the Flip proposal");
+        } else if (d->model == UMC_MODEL_VECTOR) {
+            if (d->components < 1 || d->components > 4) throw Error(UMC_ERR_UNSUPPORTED, "VectorSpin<N>: N must be 1..4");
+            if (d->proposal != UMC_PROPOSAL_SPHERE && d->proposal != UMC_PROPOSAL_ROTATION)
+                throw Error(UMC_ERR_UNSUPPORTED, "VectorSpin slabs use UniformSphereN or LocalRotation");
+        } else {
+            throw Error(UMC_ERR_UNSUPPORTED, "slabs are provided for Ising and VectorSpin on square and cubic lattices");
+        }
+        auto s = std::make_unique<umc_slab>();
+        s->desc = *d;
+        s->along_z = Lz > 1 ? 1u : 0u;
+        s->P = uint32_t(s->along_z ? Lx * Ly : Lx);
+        const uint64_t nloc = (uint64_t(d->planes) + 2) * s->P;
+        if (nloc > 0xFFFFFFFFull / 4) throw Error(UMC_ERR_OVERFLOW, "slab too large");
+        s->nloc = uint32_t(nloc);
+        s->half = uint32_t(Lx * Ly * Lz / 2);
+        s->deg = 2 + (Ly > 1 ? 2 : 0) + (Lz > 1 ? 2 : 0);
+        s->device = d->device;
+        s->J_int = int32_t(d->coupling);
+        cuda_check(cudaSetDevice(d->device), "cudaSetDevice");
+        int sms = 0;
+        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device), "SM count");
+        const uint64_t work = (uint64_t(d->planes) * s->P / 2 + kBlock - 1) / kBlock;
+        s->grid = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(work, uint64_t(sms) * 8)));
+        s->ctl.alloc(sizeof(DevCtl), "slab control");
+        cuda_check(cudaMemset(s->ctl.p, 0, sizeof(DevCtl)), "slab control");
+        s->partials.alloc(size_t(s->grid) * kObs * sizeof(double), "slab partials");
+        s->record.alloc(kObs * sizeof(double), "slab record");
+        cuda_check(cudaMemset(s->record.p, 0, kObs * sizeof(double)), "slab record");
+        *out = s.release();
+    });
+}
+
+int umc_slab_destroy(umc_slab* s)
+{
+    return slab_guard([&] { delete s; });
+}
+
+uint64_t umc_slab_local_sites(const umc_slab* s) { return s ? s->nloc : 0; }
+
+int umc_slab_pass(umc_slab* s, void* field, double beta, uint64_t sweep, uint32_t colour, void* stream)
+{
+    return slab_guard([&] {
+        NvtxRange range("umc_slab_pass");
+        if (!s || !field) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (colour > 1) throw Error(UMC_ERR_INVALID_ARGUMENT, "colour is 0 or 1");
+        if (!std::isfinite(beta)) throw Error(UMC_ERR_INVALID_ARGUMENT, "beta must be finite");
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        const umc_slab_desc& d = s->desc;
+        SlabArgs a{};
+        a.field = field;
+        a.Lx = d.Lx;
+        a.Ly = d.Ly;
+        a.Lz = d.Lz;
+        a.along_z = s->along_z;
+        a.first = d.first_plane;
+        a.planes = d.planes;
+        a.P = s->P;
+        a.nloc = s->nloc;
+        a.half = s->half;
+        a.colour = colour;
+        a.kbase = key_base(key_seed(d.seed, sweep, tag_site(0)));
+        a.J = float(d.coupling);
+        a.beta = float(beta);
+        a.delta = float(d.width);
+        a.J64 = d.coupling;
+        a.beta64 = beta;
+        a.out = PassOut{s->ctl.as<DevCtl>(), s->partials.as<double>(), s->record.as<double>(), nullptr, int(colour),
+                        2, colour == 1 ? 1 : 0};
+        if (d.model == UMC_MODEL_ISING) {
+            if (!(s->tm1_beta == beta)) {
+                s->h_tm1 = ising_metropolis_thresholds(s->J_int, beta, s->deg);
+                if (!s->tm1.p) s->tm1.alloc(s->h_tm1.size() * 4, "slab thresholds");
+                cuda_check(cudaMemcpyAsync(s->tm1.p, s->h_tm1.data(), s->h_tm1.size() * 4, cudaMemcpyHostToDevice, st),
+                           "slab thresholds");
+                cuda_check(cudaStreamSynchronize(st), "slab thresholds");
+                s->tm1_beta = beta;
+            }
+            a.tm1 = s->tm1.as<uint32_t>();
+            a.D = int32_t(s->deg);
+            a.Jint = s->J_int;
+            slab_ising_pass<<<s->grid, kBlock, 0, st>>>(a);
+        } else {
+            a.err = vector_metropolis_err(beta, d.coupling, d.components, s->deg);
+            switch (d.components) {
+            case 1: launch_vector<1>(s, a, st); break;
+            case 2: launch_vector<2>(s, a, st); break;
+            case 3: launch_vector<3>(s, a, st); break;
+            default: launch_vector<4>(s, a, st); break;
+            }
+        }
+        cuda_check(cudaGetLastError(), "slab pass");
+    });
+}
+
+int umc_slab_record(umc_slab* s, double* out, void* stream)
+{
+    return slab_guard([&] {
+        if (!s || !out) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        cuda_check(cudaMemcpyAsync(out, s->record.p, kObs * sizeof(double), cudaMemcpyDeviceToHost, st), "slab record");
+        cuda_check(cudaStreamSynchronize(st), "slab record");
+        unsigned status = 0;
+        cuda_check(cudaMemcpy(&status, &s->ctl.as<DevCtl>()->status, sizeof status, cudaMemcpyDeviceToHost),
+                   "slab status");
+        if (status) throw Error(UMC_ERR_DEVICE_TIMEOUT, "slab pass reported a device error");
+    });
+}
+
+}  // extern "C"
