@@ -196,3 +196,30 @@ def test_sharded_u1batch_equals_the_whole_batch(umc):
         for k in range(p.n_chains):
             np.testing.assert_array_equal(p.get_field(k), whole.get_field(c))
             c += 1
+
+
+def test_persistent_segment_equals_grouped_segments(umc):
+    """The one-kernel segment (default: resident clusters taking work items,
+    a 256^2 chain swept by a cluster of four CTAs, small chains packed, the
+    exchanges run by whichever CTA completes a ladder) and the per-group
+    kernels run the same chains and exchanges: fields bit for bit, temperature
+    maps and records equal (energies to FP64 summation order)."""
+    Ls = np.array([256, 16, 64, 32, 256, 128, 16])
+    R = 4
+    betas = np.stack([_geometric(0.8, 1.3, R)] * len(Ls))
+    a = umc.Batch(Ls, betas, width=1.0, sweeps_per_exchange=4, seed=5)
+    b = umc.Batch(Ls, betas, width=1.0, sweeps_per_exchange=4, seed=5)
+    b.set_persistent(False)
+    info = a.persistent_info()
+    assert info["enabled"] and info["big_items"] == 2 * R and info["grid"] % 4 == 0
+    assert not b.persistent_info()["enabled"]
+    for x in (a, b):
+        x.randomize(6)
+    ra, rb = a.run(5), b.run(5)
+    np.testing.assert_array_equal(ra[..., 3], rb[..., 3])
+    np.testing.assert_allclose(ra, rb, rtol=1e-12, atol=1e-9)
+    np.testing.assert_array_equal(a.temperature_map(), b.temperature_map())
+    assert a.counters() == b.counters()
+    for c in range(a.n_chains):
+        np.testing.assert_array_equal(a.get_field(c), b.get_field(c))
+    assert a.sites()[1] == 5  # one kernel per segment

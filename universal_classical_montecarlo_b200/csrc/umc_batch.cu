@@ -138,34 +138,30 @@ __device__ __forceinline__ bool xy_update(const SegArgs& a, float* th, uint32_t 
     return true;
 }
 
-// The cluster form stays at 32 registers (two CTAs per SM); the FP64
-// decision is out of line and spills inside itself.
-template <bool CLUSTER>
-__global__ void __launch_bounds__(1024, CLUSTER ? 2 : 1) xy_batch_segment(SegArgs a)
+// Per-CTA staging of the chains a CTA updates: per owned chain and sweep the
+// key base, beta and field offset (computed once per CTA instead of once per
+// site update), and its accepted-update count.
+struct SegShared
 {
-    __shared__ unsigned int accepted[kMaxCpc];
-    // per owned chain and sweep: key base, beta and field offset (computed once
-    // per CTA instead of once per site update)
-    __shared__ uint64_t kb_sh[kMaxCpc];
-    __shared__ float beta_sh[kMaxCpc];
-    __shared__ double beta64_sh[kMaxCpc];
-    __shared__ unsigned long long off_sh[kMaxCpc];
+    unsigned int accepted[kMaxCpc];
+    uint64_t kb[kMaxCpc];
+    float beta[kMaxCpc];
+    double beta64[kMaxCpc];
+    unsigned long long off[kMaxCpc];
+};
+
+// a.sweeps sweeps of chain_n chains (ids chains[0..chain_n)) of side a.L, rows
+// [row_lo, row_lo + row_n) of each (all of them unless a cluster shares the
+// chains), then their observables into a.part (share `share`).  CLUSTER: the
+// CTAs of a thread-block cluster share the chains and meet at the cluster
+// barrier between colour passes; else one CTA and __syncthreads.
+template <bool CLUSTER>
+__device__ __forceinline__ void run_share(const SegArgs& a, SegShared& sh, const uint32_t* chains, uint32_t chain_n,
+                                          uint32_t row_lo, uint32_t row_n, uint32_t share)
+{
     const uint64_t sweep0 = a.ctr->sweep;
     const uint32_t H = a.H, half = a.half;
-    uint32_t chain_lo, chain_n, row_lo, row_n, share = 0;
-    if (CLUSTER) {
-        chain_lo = blockIdx.x / a.cpk;
-        chain_n = 1;
-        share = blockIdx.x % a.cpk;
-        row_n = a.L / a.cpk;
-        row_lo = share * row_n;
-    } else {
-        chain_lo = blockIdx.x * a.cpc;
-        chain_n = min(a.cpc, a.n_chains - chain_lo);
-        row_lo = 0;
-        row_n = a.L;
-    }
-    if (threadIdx.x < kMaxCpc) accepted[threadIdx.x] = 0u;
+    if (threadIdx.x < kMaxCpc) sh.accepted[threadIdx.x] = 0u;
     __syncthreads();
     const uint32_t per_chain = row_n * H;  // sites of one colour per chain share
     const uint32_t work = chain_n * per_chain;
@@ -178,11 +174,11 @@ __global__ void __launch_bounds__(1024, CLUSTER ? 2 : 1) xy_batch_segment(SegArg
     const bool warp_chain = (per_chain & 31u) == 0 && (blockDim.x & 31u) == 0;
     for (uint32_t s = 0; s < a.sweeps; ++s) {
         for (uint32_t ci = threadIdx.x; ci < chain_n; ci += blockDim.x) {
-            const uint32_t chain = a.chains[chain_lo + ci];
-            kb_sh[ci] = key_base(key_seed(a.chain_seed[chain], sweep0 + s, tag_site(0)));
-            beta64_sh[ci] = a.betas[(chain / a.R) * a.R + a.slot_of_chain[chain]];
-            beta_sh[ci] = float(beta64_sh[ci]);
-            off_sh[ci] = a.off[chain];
+            const uint32_t chain = chains[ci];
+            sh.kb[ci] = key_base(key_seed(a.chain_seed[chain], sweep0 + s, tag_site(0)));
+            sh.beta64[ci] = a.betas[(chain / a.R) * a.R + a.slot_of_chain[chain]];
+            sh.beta[ci] = float(sh.beta64[ci]);
+            sh.off[ci] = a.off[chain];
         }
         __syncthreads();
         for (uint32_t colour = 0; colour < 2; ++colour) {
@@ -200,14 +196,14 @@ __global__ void __launch_bounds__(1024, CLUSTER ? 2 : 1) xy_batch_segment(SegArg
                     i = r % H;
                 }
                 const bool acc =
-                    xy_update<CLUSTER>(a, a.theta + off_sh[ci], colour, y, i, kb_sh[ci], beta_sh[ci], beta64_sh[ci]);
+                    xy_update<CLUSTER>(a, a.theta + sh.off[ci], colour, y, i, sh.kb[ci], sh.beta[ci], sh.beta64[ci]);
                 if (warp_chain) {
                     // the whole warp works on chain ci: one shared atomic per warp
                     const unsigned act = __activemask();
                     const unsigned bal = __ballot_sync(act, acc);
-                    if ((threadIdx.x & 31u) == uint32_t(__ffs(act) - 1) && bal) atomicAdd(&accepted[ci], __popc(bal));
+                    if ((threadIdx.x & 31u) == uint32_t(__ffs(act) - 1) && bal) atomicAdd(&sh.accepted[ci], __popc(bal));
                 } else if (acc) {
-                    atomicAdd(&accepted[ci], 1u);
+                    atomicAdd(&sh.accepted[ci], 1u);
                 }
             }
             if constexpr (CLUSTER) cg::this_cluster().sync();
@@ -216,7 +212,7 @@ __global__ void __launch_bounds__(1024, CLUSTER ? 2 : 1) xy_batch_segment(SegArg
     }
     // observables of this CTA's share, per chain, in FP64 (fixed-order sums)
     for (uint32_t ci = 0; ci < chain_n; ++ci) {
-        const uint32_t chain = a.chains[chain_lo + ci];
+        const uint32_t chain = chains[ci];
         const float* th = a.theta + a.off[chain];
         double v[3] = {0, 0, 0};
         for (uint32_t r = threadIdx.x; r < per_chain; r += blockDim.x) {
@@ -243,14 +239,98 @@ __global__ void __launch_bounds__(1024, CLUSTER ? 2 : 1) xy_batch_segment(SegArg
             out[0] = v[0];
             out[1] = v[1];
             out[2] = v[2];
-            out[3] = double(accepted[ci]);
+            out[3] = double(sh.accepted[ci]);
         }
     }
 }
 
-// One exchange round per ladder (one thread per ladder), after writing the
-// segment's record [E, Mx, My, chain, beta, swap accepted, accepted updates, 0]
-// for every temperature slot.
+// The cluster form stays at 32 registers (two CTAs per SM); the FP64
+// decision is out of line and spills inside itself.
+template <bool CLUSTER>
+__global__ void __launch_bounds__(1024, CLUSTER ? 2 : 1) xy_batch_segment(SegArgs a)
+{
+    __shared__ SegShared sh;
+    uint32_t chain_lo, chain_n, row_lo, row_n, share = 0;
+    if (CLUSTER) {
+        chain_lo = blockIdx.x / a.cpk;
+        chain_n = 1;
+        share = blockIdx.x % a.cpk;
+        row_n = a.L / a.cpk;
+        row_lo = share * row_n;
+    } else {
+        chain_lo = blockIdx.x * a.cpc;
+        chain_n = min(a.cpc, a.n_chains - chain_lo);
+        row_lo = 0;
+        row_n = a.L;
+    }
+    run_share<CLUSTER>(a, sh, a.chains + chain_lo, chain_n, row_lo, row_n, share);
+}
+
+// Ladder l's record of the segment [E, Mx, My, chain, beta, swap accepted,
+// accepted updates, 0] for every temperature slot, then its exchange round:
+// slots (k, k+1), k of the round's parity, swap their chains iff
+// (beta_k - beta_{k+1})(E_k - E_{k+1}) >= 0 or log(u) < that product.  One
+// thread; part holds each chain's share partials (read through L2: another
+// CTA may have written them in this launch).
+__device__ void exchange_ladder(uint32_t l, uint32_t R, unsigned long long round, unsigned long long rec, bool keep,
+                                uint32_t n_ladders, const uint32_t* cpk_of_chain, const double* part,
+                                const double* betas, uint32_t* holder, uint32_t* slot_of_chain,
+                                const unsigned long long* ladder_seed, double* records, unsigned long long* swaps)
+{
+    double E[kMaxRungs];
+    for (uint32_t q = 0; q < R; ++q) {
+        const uint32_t c = l * R + q, k = cpk_of_chain[c];
+        double e = 0.0;
+        for (uint32_t r = 0; r < k; ++r) e += __ldcg(part + (uint64_t(c) * kMaxShares + r) * 4);
+        E[q] = e;
+    }
+    for (uint32_t k = 0; k < R && keep; ++k) {
+        const uint32_t c = holder[l * R + k], nk = cpk_of_chain[c];
+        double mx = 0.0, my = 0.0, acc = 0.0;
+        for (uint32_t r = 0; r < nk; ++r) {
+            mx += __ldcg(part + (uint64_t(c) * kMaxShares + r) * 4 + 1);
+            my += __ldcg(part + (uint64_t(c) * kMaxShares + r) * 4 + 2);
+            acc += __ldcg(part + (uint64_t(c) * kMaxShares + r) * 4 + 3);
+        }
+        double* out = records + ((rec * n_ladders + l) * R + k) * kObs;
+        out[0] = E[c - l * R];
+        out[1] = mx;
+        out[2] = my;
+        out[3] = double(c);
+        out[4] = betas[l * R + k];
+        out[5] = 0.0;
+        out[6] = acc;
+        out[7] = 0.0;
+    }
+    const uint32_t parity = uint32_t(round & 1ull);
+    const uint64_t kb = key_base(key_seed(ladder_seed[l], round, kTagSwap));
+    for (uint32_t k = parity; k + 1 < R; k += 2) {
+        const uint32_t a = holder[l * R + k], b = holder[l * R + k + 1];
+        const double delta = (betas[l * R + k] - betas[l * R + k + 1]) * (E[a - l * R] - E[b - l * R]);
+        const bool acc = delta >= 0.0 || log(u_f64(first_draw(kb, k))) < delta;
+        if (keep) records[((rec * n_ladders + l) * R + k) * kObs + 5] = acc ? 1.0 : 0.0;
+        if (acc) {
+            holder[l * R + k] = b;
+            holder[l * R + k + 1] = a;
+            slot_of_chain[a] = k + 1;
+            slot_of_chain[b] = k;
+            atomicAdd(swaps, 1ull);
+        }
+    }
+}
+
+// The segment's bookkeeping once every ladder has exchanged: counters advance
+// (or the record ring reports overflow).
+__device__ __forceinline__ void close_segment(BatchCounters* ctr, unsigned long long round, unsigned long long rec,
+                                              bool keep, uint32_t sweeps)
+{
+    ctr->round = round + 1;
+    ctr->sweep += sweeps;
+    if (keep) ctr->rec = rec + 1;
+    else ctr->status |= kBatchErrRecords;
+}
+
+// One exchange round per ladder (one thread per ladder).
 __global__ void xy_batch_swap(BatchCounters* ctr, uint32_t n_ladders, uint32_t R, const uint32_t* cpk_of_chain,
                               const double* part, const double* betas, uint32_t* holder, uint32_t* slot_of_chain,
                               const unsigned long long* ladder_seed, double* records, unsigned long long* swaps,
@@ -260,54 +340,100 @@ __global__ void xy_batch_swap(BatchCounters* ctr, uint32_t n_ladders, uint32_t R
     const unsigned long long rec = ctr->rec;
     const bool keep = rec < ctr->capacity;
     __syncthreads();
-    for (uint32_t l = threadIdx.x; l < n_ladders; l += blockDim.x) {
-        double E[kMaxRungs];
-        for (uint32_t q = 0; q < R; ++q) {
-            const uint32_t c = l * R + q, k = cpk_of_chain[c];
-            double e = 0.0;
-            for (uint32_t r = 0; r < k; ++r) e += part[(uint64_t(c) * kMaxShares + r) * 4];
-            E[q] = e;
-        }
-        for (uint32_t k = 0; k < R && keep; ++k) {
-            const uint32_t c = holder[l * R + k], nk = cpk_of_chain[c];
-            double mx = 0.0, my = 0.0, acc = 0.0;
-            for (uint32_t r = 0; r < nk; ++r) {
-                mx += part[(uint64_t(c) * kMaxShares + r) * 4 + 1];
-                my += part[(uint64_t(c) * kMaxShares + r) * 4 + 2];
-                acc += part[(uint64_t(c) * kMaxShares + r) * 4 + 3];
-            }
-            double* out = records + ((rec * n_ladders + l) * R + k) * kObs;
-            out[0] = E[c - l * R];
-            out[1] = mx;
-            out[2] = my;
-            out[3] = double(c);
-            out[4] = betas[l * R + k];
-            out[5] = 0.0;
-            out[6] = acc;
-            out[7] = 0.0;
-        }
-        const uint32_t parity = uint32_t(round & 1ull);
-        const uint64_t kb = key_base(key_seed(ladder_seed[l], round, kTagSwap));
-        for (uint32_t k = parity; k + 1 < R; k += 2) {
-            const uint32_t a = holder[l * R + k], b = holder[l * R + k + 1];
-            const double delta = (betas[l * R + k] - betas[l * R + k + 1]) * (E[a - l * R] - E[b - l * R]);
-            const bool acc = delta >= 0.0 || log(u_f64(first_draw(kb, k))) < delta;
-            if (keep) records[((rec * n_ladders + l) * R + k) * kObs + 5] = acc ? 1.0 : 0.0;
-            if (acc) {
-                holder[l * R + k] = b;
-                holder[l * R + k + 1] = a;
-                slot_of_chain[a] = k + 1;
-                slot_of_chain[b] = k;
-                atomicAdd(swaps, 1ull);
-            }
-        }
-    }
+    for (uint32_t l = threadIdx.x; l < n_ladders; l += blockDim.x)
+        exchange_ladder(l, R, round, rec, keep, n_ladders, cpk_of_chain, part, betas, holder, slot_of_chain,
+                        ladder_seed, records, swaps);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        ctr->round = round + 1;
-        ctr->sweep += sweeps;
-        if (keep) ctr->rec = rec + 1;
-        else ctr->status |= kBatchErrRecords;
+    if (threadIdx.x == 0) close_segment(ctr, round, rec, keep, sweeps);
+}
+
+// ---------------------------------------------------- one persistent kernel
+// The whole segment -- every chain's sweeps and every ladder's exchange -- in
+// one launch of resident CTAs grouped in clusters of kPersistCluster.  Work
+// items, largest first: a "big" chain is swept by a whole cluster (one row
+// band per CTA, the cluster barrier between colour passes); smaller chains are
+// packed into CTA items of up to kPersistSites sites per colour.  CTAs take
+// items from two atomic counters (big, then small), so the long items start
+// first and the short ones fill the gaps.  The CTA that completes the last
+// share of a ladder runs its exchange; the one that completes the last ladder
+// advances the counters.  No CTA ever waits for another: the scheduler is
+// atomics only, and the cluster barrier joins CTAs that are co-scheduled.
+constexpr uint32_t kPersistCluster = 4;
+constexpr uint32_t kPersistSites = 8192;   // sites per colour of a CTA item
+constexpr uint32_t kPersistBlock = 1024;
+
+struct PersistArgs
+{
+    SegArgs seg;                // fields common to all items (seg.L/H/half set per item)
+    const uint4* items;         // {first index into chains, chains, L, shares}
+    const uint32_t* chains;     // chain ids in item order
+    uint32_t n_big, n_items;
+    unsigned* sched;            // [0] next big item, [1] next small item, [2] ladders exchanged
+    unsigned* ladder_done;      // per ladder: chain shares completed
+    const uint32_t* cpk_of_chain;
+    uint32_t n_ladders;
+    double* records;
+    uint32_t* holder;
+    const unsigned long long* ladder_seed;
+    unsigned long long* swaps;
+};
+
+// Counts the item's chain shares as done; the CTA that completes a ladder
+// exchanges it, and the one that completes the last ladder closes the segment.
+__device__ void complete_item(const PersistArgs& p, const uint32_t* chains, uint32_t chain_n, uint32_t shares)
+{
+    if (threadIdx.x != 0) return;
+    __threadfence();  // this CTA's partials before the counts that publish them
+    const SegArgs& a = p.seg;
+    for (uint32_t ci = 0; ci < chain_n; ++ci) {
+        const uint32_t l = chains[ci] / a.R;
+        if (atomicAdd(&p.ladder_done[l], 1u) + 1u != a.R * shares) continue;
+        __threadfence();
+        const unsigned long long round = a.ctr->round, rec = a.ctr->rec;
+        const bool keep = rec < a.ctr->capacity;
+        exchange_ladder(l, a.R, round, rec, keep, p.n_ladders, p.cpk_of_chain, a.part, a.betas, p.holder,
+                        const_cast<uint32_t*>(a.slot_of_chain), p.ladder_seed, p.records, p.swaps);
+        __threadfence();
+        if (atomicAdd(&p.sched[2], 1u) + 1u == p.n_ladders)
+            close_segment(const_cast<BatchCounters*>(a.ctr), round, rec, keep, a.sweeps);
+    }
+}
+
+__global__ void __launch_bounds__(kPersistBlock, 1) xy_batch_persistent(PersistArgs p)
+{
+    __shared__ SegShared sh;
+    __shared__ uint32_t item_sh;
+    cg::cluster_group cl = cg::this_cluster();
+    // big chains: the whole cluster, one band of rows per CTA
+    for (;;) {
+        if (cl.block_rank() == 0 && threadIdx.x == 0) item_sh = atomicAdd(&p.sched[0], 1u);
+        cl.sync();
+        const uint32_t it = *cl.map_shared_rank(&item_sh, 0);
+        cl.sync();
+        if (it >= p.n_big) break;
+        const uint4 w = p.items[it];
+        SegArgs a = p.seg;
+        a.L = w.z;
+        a.H = w.z / 2;
+        a.half = w.z * w.z / 2;
+        const uint32_t rows = w.z / kPersistCluster, share = cl.block_rank();
+        run_share<true>(a, sh, p.chains + w.x, 1, share * rows, rows, share);
+        complete_item(p, p.chains + w.x, 1, kPersistCluster);
+    }
+    // packed smaller chains, one CTA each
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) item_sh = atomicAdd(&p.sched[1], 1u);
+        __syncthreads();
+        const uint32_t it = p.n_big + item_sh;
+        if (it >= p.n_items) break;
+        const uint4 w = p.items[it];
+        SegArgs a = p.seg;
+        a.L = w.z;
+        a.H = w.z / 2;
+        a.half = w.z * w.z / 2;
+        run_share<false>(a, sh, p.chains + w.x, w.y, 0, w.z, 0);
+        complete_item(p, p.chains + w.x, w.y, 1);
     }
 }
 
@@ -403,6 +529,12 @@ struct umc_batch
     uint32_t sweeps_per_exchange = 10;
     cudaGraphExec_t graph = nullptr;
     uint64_t launches = 0;
+    // the one-kernel segment (xy_batch_persistent): its items, per-chain
+    // share counts and scheduler counters; on by default
+    bool persistent = true;
+    uint32_t p_big = 0, p_items = 0, p_grid = 0;
+    std::vector<uint32_t> p_cpk;
+    umc::DevBuf p_items_dev, p_chains_dev, p_cpk_dev, p_sched;
 };
 
 namespace umc {
@@ -538,6 +670,109 @@ GroupCfg autotune(umc_batch* b, umc_batch::Group& g)
     return best;
 }
 
+// Work items of the one-kernel segment, largest first: a chain whose colour
+// class holds at least 2 kPersistSites sites and whose rows split into
+// kPersistCluster bands of at least 2 rows is swept by a whole cluster; the
+// others are packed, chains of one side together, into CTA items of up to
+// kPersistSites sites per colour.
+void build_persistent(umc_batch* b)
+{
+    std::vector<uint32_t> order(b->n_chains);
+    for (uint32_t c = 0; c < b->n_chains; ++c) order[c] = c;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return b->L[x] > b->L[y]; });
+    std::vector<uint4> items;
+    std::vector<uint32_t> chains;
+    b->p_cpk.assign(b->n_chains, 1);
+    uint32_t n_big = 0;
+    size_t q = 0;
+    while (q < order.size() && [&] {
+        const uint32_t L = b->L[order[q]];
+        return uint64_t(L) * L / 2 >= 2ull * kPersistSites && L % (2 * kPersistCluster) == 0;
+    }()) {
+        const uint32_t c = order[q++];
+        items.push_back(make_uint4(uint32_t(chains.size()), 1u, b->L[c], kPersistCluster));
+        chains.push_back(c);
+        b->p_cpk[c] = kPersistCluster;
+        ++n_big;
+    }
+    while (q < order.size()) {
+        const uint32_t L = b->L[order[q]];
+        const uint32_t per = L * L / 2;
+        const uint32_t cpc = std::max<uint32_t>(1, std::min<uint32_t>(kMaxCpc, kPersistSites / per));
+        const uint32_t first = uint32_t(chains.size());
+        uint32_t n = 0;
+        while (q < order.size() && n < cpc && b->L[order[q]] == L) {
+            chains.push_back(order[q++]);
+            ++n;
+        }
+        items.push_back(make_uint4(first, n, L, 1u));
+    }
+    b->p_big = n_big;
+    b->p_items = uint32_t(items.size());
+    b->p_items_dev.alloc(items.size() * sizeof(uint4), "persistent items");
+    cuda_check(cudaMemcpy(b->p_items_dev.p, items.data(), items.size() * sizeof(uint4), cudaMemcpyHostToDevice), "items");
+    b->p_chains_dev.alloc(chains.size() * 4, "persistent chains");
+    cuda_check(cudaMemcpy(b->p_chains_dev.p, chains.data(), chains.size() * 4, cudaMemcpyHostToDevice), "chains");
+    b->p_cpk_dev.alloc(b->n_chains * 4, "persistent shares");
+    cuda_check(cudaMemcpy(b->p_cpk_dev.p, b->p_cpk.data(), b->n_chains * 4, cudaMemcpyHostToDevice), "shares");
+    b->p_sched.alloc((3 + size_t(b->n_ladders)) * 4, "persistent scheduler");
+    // resident clusters: the kernel never waits across clusters, so this only
+    // sizes the grid to what runs at once
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(kPersistCluster);
+    lc.blockDim = dim3(kPersistBlock);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kPersistCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, xy_batch_persistent, &lc) != cudaSuccess || clusters <= 0) {
+        cudaGetLastError();
+        int sms = 0;
+        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "SM count");
+        clusters = std::max(1, sms / int(kPersistCluster));
+    }
+    b->p_grid = uint32_t(clusters) * kPersistCluster;
+}
+
+void launch_persistent(umc_batch* b, cudaStream_t st)
+{
+    cuda_check(cudaMemsetAsync(b->p_sched.p, 0, b->p_sched.bytes, st), "reset scheduler");
+    PersistArgs p{};
+    umc_batch::Group g0;  // seg_args takes the per-group fields from a group; the kernel sets L per item
+    g0.L = 2;
+    p.seg = seg_args(b, g0, b->theta.as<float>());
+    p.seg.chains = nullptr;
+    p.seg.n_chains = 0;
+    p.items = b->p_items_dev.as<uint4>();
+    p.chains = b->p_chains_dev.as<uint32_t>();
+    p.n_big = b->p_big;
+    p.n_items = b->p_items;
+    p.sched = b->p_sched.as<unsigned>();
+    p.ladder_done = b->p_sched.as<unsigned>() + 3;
+    p.cpk_of_chain = b->p_cpk_dev.as<uint32_t>();
+    p.n_ladders = b->n_ladders;
+    p.records = b->records.as<double>();
+    p.holder = b->holder_dev.as<uint32_t>();
+    p.ladder_seed = b->lseeds_dev.as<unsigned long long>();
+    p.swaps = b->swaps.as<unsigned long long>();
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(b->p_grid);
+    lc.blockDim = dim3(kPersistBlock);
+    lc.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kPersistCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    cuda_check(cudaLaunchKernelEx(&lc, xy_batch_persistent, p), "persistent batch segment");
+}
+
 void build_graph(umc_batch* b)
 {
     if (b->graph) {
@@ -546,6 +781,13 @@ void build_graph(umc_batch* b)
     }
     cudaGraph_t graph;
     cuda_check(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    if (b->persistent) {
+        launch_persistent(b, b->stream);
+        cuda_check(cudaStreamEndCapture(b->stream, &graph), "end capture");
+        cuda_check(cudaGraphInstantiate(&b->graph, graph, 0), "instantiate graph");
+        cudaGraphDestroy(graph);
+        return;
+    }
     cuda_check(cudaEventRecord(b->fork, b->stream), "fork");
     for (auto& g : b->groups) {
         cuda_check(cudaStreamWaitEvent(g.stream, b->fork, 0), "fork wait");
@@ -661,6 +903,7 @@ void create_batch(const umc_batch_desc* d, umc_batch* b)
     up(b->cpk_dev, b->cpk_of_chain.data(), b->cpk_of_chain.size() * 4, "cpk");
     cuda_check(cudaMemset(b->ctr.p, 0, sizeof(BatchCounters)), "counters");
     cuda_check(cudaMemcpy(&b->ctr.as<BatchCounters>()->capacity, &b->max_records, 8, cudaMemcpyHostToDevice), "capacity");
+    build_persistent(b);
     build_graph(b);
 }
 
@@ -807,7 +1050,7 @@ int umc_batch_enqueue(umc_batch* b, uint64_t n_segments)
         if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
         batch_scope(b);
         for (uint64_t s = 0; s < n_segments; ++s) cuda_check(cudaGraphLaunch(b->graph, b->stream), "segment graph");
-        b->launches += n_segments * (b->groups.size() + 1);
+        b->launches += n_segments * (b->persistent ? 1 : b->groups.size() + 1);
     });
 }
 
@@ -933,6 +1176,28 @@ int umc_batch_config(const umc_batch* b, uint32_t L, uint32_t* chains_per_cta, u
                 return;
             }
         throw Error(UMC_ERR_OUT_OF_RANGE, "no ladder with that side");
+    });
+}
+
+int umc_batch_set_persistent(umc_batch* b, int enable)
+{
+    return bguard([&] {
+        if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
+        batch_scope(b);
+        cuda_check(cudaStreamSynchronize(b->stream), "sync");
+        b->persistent = enable != 0;
+        build_graph(b);
+    });
+}
+
+int umc_batch_persistent_info(const umc_batch* b, int* enabled, uint32_t* grid, uint32_t* big_items, uint32_t* items)
+{
+    return bguard([&] {
+        if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
+        if (enabled) *enabled = b->persistent ? 1 : 0;
+        if (grid) *grid = b->p_grid;
+        if (big_items) *big_items = b->p_big;
+        if (items) *items = b->p_items;
     });
 }
 
