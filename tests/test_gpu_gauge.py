@@ -6,11 +6,12 @@ link order) and the engine (staple per link, FP32, SU(N) reunitarised).  Links
 must agree within TOL except where the oracle's accept decision sat within
 MARGIN of its threshold (and the links that share a cell with those).
 
-The engine decides as the FP64 test does on its FP32 links (FP32 first, FP64
-inside the FP32 error band), so MARGIN only covers the FP32 rounding of the
-proposal: the U(1) shift moves the new angle by about 2.4e-7 (log_p by
-beta deg 2.4e-7 < 1e-5 here), the SU(N) candidate U exp(iX) by about 1e-6 per
-entry (log_p by up to (beta/N) N^2 deg 1e-6, about 1e-4 at beta 2).
+For U(1) the engine decides as the FP64 test does on its FP32 links (FP32
+first, FP64 inside the FP32 error band), so MARGIN_U1 only covers the FP32
+rounding of the proposal: the shift moves the new angle by about 2.4e-7
+(log_p by beta deg 2.4e-7 < 1e-5 here).  SU(N) decides in FP32: its staple
+arithmetic and its candidate U exp(iX) (about 1e-6 per entry) each move log_p
+by up to about (beta/N) N^2 deg 1e-6, 1e-4 at beta 2.
 """
 import numpy as np
 import pytest

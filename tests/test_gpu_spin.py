@@ -267,16 +267,22 @@ def _vector_energy(g, s):
     return 0.5 * e
 
 
-def test_vector_wolff_per_flip(umc, oracle):
-    L = 8
+@pytest.mark.parametrize("L", [8, 16, 24])
+def test_vector_wolff_per_flip(umc, oracle, L):
+    """One O(3) Wolff flip at a time from an identical state, on one 8^3 tile
+    and on 8 and 27 tiles (the tile-crossing bonds of the fused kernel)."""
     g = umc.cubic_lattice(L, L, L)
     n = L**3
     ei, ej = cubic_edges(L, L, L)
     pos, off, bonds, slot = _vector_setup(umc, oracle, g, ei, ej)
     ch = umc.Chain(umc.MODEL_VECTOR, graph=g, components=3, coupling=1.0, proposal=umc.PROPOSAL_SPHERE,
                    wolff_axis=umc.AXIS_SPHERE, seed=9)
-    ch.set_field(random_unit_vectors(n, 3, 4).astype(np.float32))
-    checked = 0
+    v0 = random_unit_vectors(n, 3, 4)
+    if L > 8:  # a partly ordered start: clusters span many tiles
+        v0 = v0 * 0.8 + np.array([0.0, 0.0, 1.0])
+        v0 /= np.linalg.norm(v0, axis=1, keepdims=True)
+    ch.set_field(v0.astype(np.float32))
+    checked, big = 0, 0
     for f in range(40):
         state = ch.get_field().reshape(n, 3)
         cm = np.empty((n, 3))
@@ -287,9 +293,11 @@ def test_vector_wolff_per_flip(umc, oracle):
         if margin[0] < MARGIN:
             continue  # an activation decision sat on its threshold: resync
         checked += 1
+        big += int(z_o[0] > 512)
         assert sizes[0] == z_o[0]
         np.testing.assert_allclose(got, v_o[pos], rtol=0, atol=TOL)
     assert checked >= 30
+    assert L == 8 or big >= 5  # clusters beyond one tile were compared
 
 
 def test_xy_angle_per_sweep(umc, oracle):

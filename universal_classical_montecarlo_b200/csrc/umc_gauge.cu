@@ -164,8 +164,7 @@ void gauge_sweep(umc_chain* c, double beta, double* record)
     a.width = float(c->desc.width);
     a.model_beta64 = c->desc.coupling;
     a.driver_beta64 = beta;
-    a.err = c->N == 1 ? u1_metropolis_err(beta, c->desc.coupling, c->max_incident)
-                      : su_metropolis_err(beta, c->desc.coupling, c->N, c->max_incident);
+    a.err = c->N == 1 ? u1_metropolis_err(beta, c->desc.coupling, c->max_incident) : 0.0f;  // SU(N): FP32 test
     const int np = int(c->n_colours) + 1;
     for (uint32_t p = 0; p < c->n_colours; ++p) {
         a.first = uint32_t(c->class_start[p]);

@@ -495,23 +495,14 @@ inline float xy_metropolis_err(double beta, double J, uint32_t deg)
 {
     return float(std::fabs(beta * J) * double(deg) * 0x1.0p-18 * 10.0);
 }
-// The gauge passes (umc_gauge_kernels.cuh, and the plain batched U(1) chains),
-// deg = cells per link:
-//  * U(1): a cell's staple angle sums three FP32 angles of at most 2 pi
-//    (38 u), sincosf adds 2 u, deg of them make Sr and Si; with the old and
-//    new cos/sin and the products: driver_beta model_beta u deg (4 (40 + deg) + 24).
-//  * SU(N): every entry of a product of two (near-)unitary FP32 matrices is
-//    within 4 N u; a staple sums deg products of three; ReTr(U A) adds N^2
-//    products; tr_old and tr_new both: driver_beta (model_beta / N) u
-//    (4 N^2 deg + 2 N deg (8 N + deg) + 16).
+// The U(1) gauge passes (umc_gauge_kernels.cuh, and the plain batched U(1)
+// chains), deg = cells per link: a cell's staple angle sums three FP32 angles
+// of at most 2 pi (38 u), sincosf adds 2 u, deg of them make Sr and Si; with
+// the old and new cos/sin and the products: driver_beta model_beta u deg
+// (4 (40 + deg) + 24).
 inline float u1_metropolis_err(double driver_beta, double model_beta, uint32_t deg)
 {
     return float(std::fabs(driver_beta * model_beta) * 0x1.0p-24 * double(deg) * (4.0 * (40.0 + deg) + 24.0));
-}
-inline float su_metropolis_err(double driver_beta, double model_beta, int N, uint32_t deg)
-{
-    const double n = N, d = deg;
-    return float(std::fabs(driver_beta * model_beta / n) * 0x1.0p-24 * (4.0 * n * n * d + 2.0 * n * d * (8.0 * n + d) + 16.0));
 }
 
 // ------------------------------------------------------ VectorSpin<N> pass
