@@ -582,6 +582,58 @@ def torus_plaquette(beta, n_plaq):
     return float(np.exp(lse(a) - lse(b)))
 
 
+def torus_plaquette_sectors(beta, n_plaq, charges, weights=None):
+    """Exact <cos theta_p> of 2D U(1) on a periodic torus of n_plaq plaquettes
+    within each topological sector Q of `charges` (Q = sum_p wrap(theta_p) /
+    2 pi).  With the plaquette angles independent apart from sum_p theta_p =
+    2 pi Q, Z_Q = int dk cos(2 pi k Q) c(k)^n_plaq with c(k) = (1/pi) int_0^pi
+    e^{beta cos t} cos(k t) dt, and <P>_Q = int cos(2 pi k Q) c^(n-1) c' /
+    int cos(2 pi k Q) c^n, c' = dc/dbeta; summed over Q with weights Z_Q this
+    is torus_plaquette (Poisson summation turns the k integral into the sum
+    over representations).  Local updates at large beta rarely change Q, so a
+    chain's plaquette is compared with the sector values of the charges it
+    visited.  Quadrature: Gauss-Legendre in t, trapezoid in k.  weights, if a
+    dict, receives Z_Q / Z_0 for each Q."""
+    import numpy as np
+
+    t, w = np.polynomial.legendre.leggauss(400)
+    t = 0.5 * np.pi * (t + 1.0)
+    w = 0.5 * np.pi * w
+    width = 12.0 * np.sqrt(max(beta, 1.0) / n_plaq)  # c^n decays as exp(-n k^2 / (2 beta))
+    k = np.linspace(0.0, min(width, 4.0), 4001)
+    e = np.exp(beta * (np.cos(t) - 1.0))                     # scaled by e^-beta
+    ck = (np.cos(np.outer(k, t)) * e) @ w / np.pi
+    dk = (np.cos(np.outer(k, t)) * (np.cos(t) * e)) @ w / np.pi
+    if (ck <= 0).any():
+        raise ValueError("c(k) changes sign inside the k range")
+    lc = np.log(ck)
+    base = n_plaq * lc[0]
+    out = {}
+    for Q in charges:
+        cq = np.cos(2.0 * np.pi * k * Q)
+        zn = np.trapezoid(cq * np.exp(n_plaq * lc - base), k)
+        zd = np.trapezoid(cq * np.exp((n_plaq - 1) * lc - base) * dk, k)
+        out[int(Q)] = float(zd / zn)
+        if weights is not None:
+            weights[int(Q)] = float(zn)
+    if weights is not None and 0 in weights:
+        z0 = weights[0]
+        for q in weights:
+            weights[q] /= z0
+    return out
+
+
+def sector_matched_plaquette(beta, n_plaq, charges):
+    """The exact plaquette a sampler should show given the charges it visited:
+    the mean over records of <P>_Q(record)."""
+    import numpy as np
+
+    q = np.rint(np.asarray(charges)).astype(int).ravel()
+    vals, counts = np.unique(q, return_counts=True)
+    table = torus_plaquette_sectors(beta, n_plaq, vals)
+    return float(sum(table[int(v)] * c for v, c in zip(vals, counts)) / counts.sum())
+
+
 def learned_study(umc, torch, betas=LEARN_BETAS, L=64, chains=444, n_configs=20000, train_steps=1500,
                   batch=16384, lr=3e-3, therm=20000, meas=4000, seed=1):
     """Effective independent samples per second of the plaquette P and the
@@ -646,6 +698,13 @@ def learned_study(umc, torch, betas=LEARN_BETAS, L=64, chains=444, n_configs=200
                 row["exact_plaquette"] = exact
                 row["z_vs_exact"] = {"plain": float((mp.mean() - exact) / (mp.std(ddof=1) / np.sqrt(chains))),
                                      "learned": float((ml.mean() - exact) / (ml.std(ddof=1) / np.sqrt(chains)))}
+                # the known answer for the sectors each sampler visited (at
+                # large beta local updates keep a chain near its charge)
+                sp = sector_matched_plaquette(beta, L * L, rec_p[:, :, 2])
+                sl = sector_matched_plaquette(beta, L * L, rec_l[:, :, 2])
+                row["sector_matched_plaquette"] = {"plain": sp, "learned": sl}
+                row["z_vs_sector_exact"] = {"plain": float((mp.mean() - sp) / (mp.std(ddof=1) / np.sqrt(chains))),
+                                            "learned": float((ml.mean() - sl) / (ml.std(ddof=1) / np.sqrt(chains)))}
             row[name] = {"tau_int": {"plain": tp, "plain_err": ep, "learned": tl, "learned_err": el},
                          "tau_converged": {"plain": wp < meas // 2, "learned": wl < meas // 2},
                          "effective_samples_per_s": eff,
@@ -1255,6 +1314,7 @@ def main():
                                     "tau_int": {o: row[o]["tau_int"] for o in ("plaquette", "Q")},
                                     "tau_converged": {o: row[o]["tau_converged"] for o in ("plaquette", "Q")},
                                     "z_vs_exact_plaquette": row["z_vs_exact"],
+                                    "z_vs_sector_matched_plaquette": row["z_vs_sector_exact"],
                                     "acceptance": row["acceptance"]}
                                 for b, row in study.items()}}
 

@@ -208,3 +208,22 @@ def test_plain_keyed_chain_samples_the_exact_distribution(oracle, umc):
     m, err = umc.binning_error(obs[:, 1], 5000)
     exact = torus_plaquette(beta, L * L)
     assert abs(m - exact) < 4 * err, (m, err, exact)
+
+
+def test_sector_plaquettes_recombine_to_the_torus_value():
+    """bench.py's exact plaquette per topological sector: weighted by Z_Q
+    the sector values give back the all-sector torus plaquette (character
+    expansion), and the sectors differ as expected (|Q| > 0 costs action)."""
+    import importlib.util
+    import os
+
+    spec = importlib.util.spec_from_file_location(
+        "bench", os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    for beta, V in [(2.0, 16), (4.0, 64), (8.0, 4096)]:
+        w = {}
+        tab = bench.torus_plaquette_sectors(beta, V, range(-15, 16), weights=w)
+        mix = sum(w[q] * tab[q] for q in tab) / sum(w.values())
+        assert abs(mix - bench.torus_plaquette(beta, V)) < 1e-9, (beta, V, mix)
+        assert tab[0] > tab[1] > tab[2] and abs(tab[1] - tab[-1]) < 1e-12
