@@ -223,7 +223,7 @@ def test_sector_plaquettes_recombine_to_the_torus_value():
     spec.loader.exec_module(bench)
     for beta, V in [(2.0, 16), (4.0, 64), (8.0, 4096)]:
         w = {}
-        tab = bench.torus_plaquette_sectors(beta, V, range(-15, 16), weights=w)
+        tab = bench.torus_plaquette_sectors(beta, V, range(-40, 41), weights=w)
         mix = sum(w[q] * tab[q] for q in tab) / sum(w.values())
         assert abs(mix - bench.torus_plaquette(beta, V)) < 1e-9, (beta, V, mix)
         assert tab[0] > tab[1] > tab[2] and abs(tab[1] - tab[-1]) < 1e-12
