@@ -481,7 +481,8 @@ class XYBatch:
         return (f"512 XY chains in 32 replica-exchange ladders of 16, L per ladder {counts} (ladders per L), "
                 f"FP32 angles, J=1, betas geometric on [0.8, 1.3], U1Shift 1.0, swaps every 10 sweeps; "
                 f"step = 10 sweeps of every chain + one exchange round, one persistent kernel per step "
-                f"({info['grid']} CTAs in clusters of 4, {info['big_items']} cluster-swept chains, "
+                f"({info['grid']} CTAs of 1024 threads in clusters of {info['cluster']}, {info['ctas_per_sm']} per SM, "
+                f"{info['big_items']} cluster-swept chains, "
                 f"{info['items']} work items)")
 
     def enqueue(self, k):

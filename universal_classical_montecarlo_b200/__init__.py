@@ -194,7 +194,8 @@ class BatchDesc(C.Structure):
 
 _decl("umc_batch_create", _int, C.POINTER(BatchDesc), C.POINTER(_vp))
 _decl("umc_batch_set_persistent", _int, _vp, _int)
-_decl("umc_batch_persistent_info", _int, _vp, C.POINTER(_int), C.POINTER(_u32), C.POINTER(_u32), C.POINTER(_u32))
+_decl("umc_batch_persistent_info", _int, _vp, C.POINTER(_int), C.POINTER(_u32), C.POINTER(_u32), C.POINTER(_u32),
+      C.POINTER(_u32), C.POINTER(_u32))
 _decl("umc_batch_destroy", _int, _vp)
 _decl("umc_batch_randomize", _int, _vp, _u64)
 _decl("umc_batch_set_field", _int, _vp, _u32, _vp)
@@ -999,9 +1000,11 @@ class Batch:
         check(lib.umc_batch_set_persistent(self._h, int(enable)))
 
     def persistent_info(self):
-        e, g, nb, ni = _int(0), _u32(0), _u32(0), _u32(0)
-        check(lib.umc_batch_persistent_info(self._h, C.byref(e), C.byref(g), C.byref(nb), C.byref(ni)))
-        return {"enabled": bool(e.value), "grid": g.value, "big_items": nb.value, "items": ni.value}
+        e, g, nb, ni, kc, mb = _int(0), _u32(0), _u32(0), _u32(0), _u32(0), _u32(0)
+        check(lib.umc_batch_persistent_info(self._h, C.byref(e), C.byref(g), C.byref(nb), C.byref(ni), C.byref(kc),
+                                            C.byref(mb)))
+        return {"enabled": bool(e.value), "grid": g.value, "big_items": nb.value, "items": ni.value,
+                "cluster": kc.value, "ctas_per_sm": mb.value}
 
     def stream(self) -> int:
         return lib.umc_batch_stream(self._h) or 0

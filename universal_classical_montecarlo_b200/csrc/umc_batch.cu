@@ -349,7 +349,7 @@ __global__ void xy_batch_swap(BatchCounters* ctr, uint32_t n_ladders, uint32_t R
 
 // ---------------------------------------------------- one persistent kernel
 // The whole segment -- every chain's sweeps and every ladder's exchange -- in
-// one launch of resident CTAs grouped in clusters of kPersistCluster.  Work
+// one launch of resident CTAs grouped in clusters of KC (4 or 8).  Work
 // items, largest first: a "big" chain is swept by a whole cluster (one row
 // band per CTA, the cluster barrier between colour passes); smaller chains are
 // packed into CTA items of up to kPersistSites sites per colour.  CTAs take
@@ -358,7 +358,8 @@ __global__ void xy_batch_swap(BatchCounters* ctr, uint32_t n_ladders, uint32_t R
 // share of a ladder runs its exchange; the one that completes the last ladder
 // advances the counters.  No CTA ever waits for another: the scheduler is
 // atomics only, and the cluster barrier joins CTAs that are co-scheduled.
-constexpr uint32_t kPersistCluster = 4;
+// cluster sizes the autotuner chooses between (a big chain's bands)
+constexpr uint32_t kPersistClusters[2] = {4, 8};
 constexpr uint32_t kPersistSites = 8192;   // sites per colour of a CTA item
 constexpr uint32_t kPersistBlock = 1024;
 
@@ -399,7 +400,10 @@ __device__ void complete_item(const PersistArgs& p, const uint32_t* chains, uint
     }
 }
 
-__global__ void __launch_bounds__(kPersistBlock, 1) xy_batch_persistent(PersistArgs p)
+// KC: the cluster size; MINB: resident CTAs per SM the registers are capped
+// for (1: 64 registers; 2: 32, with a few spills).
+template <uint32_t KC, int MINB>
+__global__ void __launch_bounds__(kPersistBlock, MINB) xy_batch_persistent(PersistArgs p)
 {
     __shared__ SegShared sh;
     __shared__ uint32_t item_sh;
@@ -416,9 +420,9 @@ __global__ void __launch_bounds__(kPersistBlock, 1) xy_batch_persistent(PersistA
         a.L = w.z;
         a.H = w.z / 2;
         a.half = w.z * w.z / 2;
-        const uint32_t rows = w.z / kPersistCluster, share = cl.block_rank();
+        const uint32_t rows = w.z / KC, share = cl.block_rank();
         run_share<true>(a, sh, p.chains + w.x, 1, share * rows, rows, share);
-        complete_item(p, p.chains + w.x, 1, kPersistCluster);
+        complete_item(p, p.chains + w.x, 1, KC);
     }
     // packed smaller chains, one CTA each
     for (;;) {
@@ -532,7 +536,7 @@ struct umc_batch
     // the one-kernel segment (xy_batch_persistent): its items, per-chain
     // share counts and scheduler counters; on by default
     bool persistent = true;
-    uint32_t p_big = 0, p_items = 0, p_grid = 0;
+    uint32_t p_kc = 4, p_minb = 1, p_big = 0, p_items = 0, p_grid = 0;
     std::vector<uint32_t> p_cpk;
     umc::DevBuf p_items_dev, p_chains_dev, p_cpk_dev, p_sched;
 };
@@ -671,11 +675,11 @@ GroupCfg autotune(umc_batch* b, umc_batch::Group& g)
 }
 
 // Work items of the one-kernel segment, largest first: a chain whose colour
-// class holds at least 2 kPersistSites sites and whose rows split into
-// kPersistCluster bands of at least 2 rows is swept by a whole cluster; the
-// others are packed, chains of one side together, into CTA items of up to
-// kPersistSites sites per colour.
-void build_persistent(umc_batch* b)
+// class holds at least 2 kPersistSites sites and whose rows split into KC
+// bands of at least 2 rows is swept by a whole cluster; the others are
+// packed, chains of one side together, into CTA items of up to kPersistSites
+// sites per colour.
+void build_persistent(umc_batch* b, uint32_t kc)
 {
     std::vector<uint32_t> order(b->n_chains);
     for (uint32_t c = 0; c < b->n_chains; ++c) order[c] = c;
@@ -687,12 +691,12 @@ void build_persistent(umc_batch* b)
     size_t q = 0;
     while (q < order.size() && [&] {
         const uint32_t L = b->L[order[q]];
-        return uint64_t(L) * L / 2 >= 2ull * kPersistSites && L % (2 * kPersistCluster) == 0;
+        return uint64_t(L) * L / 2 >= 2ull * kPersistSites && L % (2 * kc) == 0;
     }()) {
         const uint32_t c = order[q++];
-        items.push_back(make_uint4(uint32_t(chains.size()), 1u, b->L[c], kPersistCluster));
+        items.push_back(make_uint4(uint32_t(chains.size()), 1u, b->L[c], kc));
         chains.push_back(c);
-        b->p_cpk[c] = kPersistCluster;
+        b->p_cpk[c] = kc;
         ++n_big;
     }
     while (q < order.size()) {
@@ -707,6 +711,7 @@ void build_persistent(umc_batch* b)
         }
         items.push_back(make_uint4(first, n, L, 1u));
     }
+    b->p_kc = kc;
     b->p_big = n_big;
     b->p_items = uint32_t(items.size());
     b->p_items_dev.alloc(items.size() * sizeof(uint4), "persistent items");
@@ -716,30 +721,52 @@ void build_persistent(umc_batch* b)
     b->p_cpk_dev.alloc(b->n_chains * 4, "persistent shares");
     cuda_check(cudaMemcpy(b->p_cpk_dev.p, b->p_cpk.data(), b->n_chains * 4, cudaMemcpyHostToDevice), "shares");
     b->p_sched.alloc((3 + size_t(b->n_ladders)) * 4, "persistent scheduler");
-    // resident clusters: the kernel never waits across clusters, so this only
-    // sizes the grid to what runs at once
+    b->p_grid = 0;
+}
+
+// The four kernel variants by (cluster size, CTAs per SM).
+const void* persistent_kernel(uint32_t kc, uint32_t minb)
+{
+    if (kc == 8) return minb == 2 ? reinterpret_cast<const void*>(&xy_batch_persistent<8, 2>)
+                                  : reinterpret_cast<const void*>(&xy_batch_persistent<8, 1>);
+    return minb == 2 ? reinterpret_cast<const void*>(&xy_batch_persistent<4, 2>)
+                     : reinterpret_cast<const void*>(&xy_batch_persistent<4, 1>);
+}
+
+cudaLaunchConfig_t persistent_config(uint32_t kc, uint32_t grid, cudaStream_t st, cudaLaunchAttribute* attr)
+{
     cudaLaunchConfig_t lc{};
-    lc.gridDim = dim3(kPersistCluster);
+    lc.gridDim = dim3(grid);
     lc.blockDim = dim3(kPersistBlock);
-    cudaLaunchAttribute attr[1];
+    lc.stream = st;
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kPersistCluster;
+    attr[0].val.clusterDim.x = kc;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     lc.attrs = attr;
     lc.numAttrs = 1;
+    return lc;
+}
+
+// Resident clusters: the kernel never waits across clusters, so this only
+// sizes the grid to what runs at once.
+uint32_t persistent_grid(umc_batch* b, uint32_t kc, uint32_t minb)
+{
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t lc = persistent_config(kc, kc, nullptr, attr);
     int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, xy_batch_persistent, &lc) != cudaSuccess || clusters <= 0) {
+    if (cudaOccupancyMaxActiveClusters(&clusters, persistent_kernel(kc, minb), &lc) != cudaSuccess || clusters <= 0) {
         cudaGetLastError();
         int sms = 0;
         cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "SM count");
-        clusters = std::max(1, sms / int(kPersistCluster));
+        clusters = std::max(1, sms / int(kc));
     }
-    b->p_grid = uint32_t(clusters) * kPersistCluster;
+    return uint32_t(clusters) * kc;
 }
 
 void launch_persistent(umc_batch* b, cudaStream_t st)
 {
+    if (!b->p_grid) b->p_grid = persistent_grid(b, b->p_kc, b->p_minb);
     cuda_check(cudaMemsetAsync(b->p_sched.p, 0, b->p_sched.bytes, st), "reset scheduler");
     PersistArgs p{};
     umc_batch::Group g0;  // seg_args takes the per-group fields from a group; the kernel sets L per item
@@ -759,18 +786,90 @@ void launch_persistent(umc_batch* b, cudaStream_t st)
     p.holder = b->holder_dev.as<uint32_t>();
     p.ladder_seed = b->lseeds_dev.as<unsigned long long>();
     p.swaps = b->swaps.as<unsigned long long>();
-    cudaLaunchConfig_t lc{};
-    lc.gridDim = dim3(b->p_grid);
-    lc.blockDim = dim3(kPersistBlock);
-    lc.stream = st;
     cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kPersistCluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    lc.attrs = attr;
-    lc.numAttrs = 1;
-    cuda_check(cudaLaunchKernelEx(&lc, xy_batch_persistent, p), "persistent batch segment");
+    cudaLaunchConfig_t lc = persistent_config(b->p_kc, b->p_grid, st, attr);
+    cudaError_t e;
+    if (b->p_kc == 8) e = b->p_minb == 2 ? cudaLaunchKernelEx(&lc, xy_batch_persistent<8, 2>, p)
+                                         : cudaLaunchKernelEx(&lc, xy_batch_persistent<8, 1>, p);
+    else e = b->p_minb == 2 ? cudaLaunchKernelEx(&lc, xy_batch_persistent<4, 2>, p)
+                            : cudaLaunchKernelEx(&lc, xy_batch_persistent<4, 1>, p);
+    cuda_check(e, "persistent batch segment");
+}
+
+// Picks the cluster size of the one-kernel segment by timing two segments of
+// each on the batch itself; every buffer a segment changes (field, holders,
+// slots, counters, swap count) is copied aside first and put back after.
+// The choice is cached in the process (and in UMC_TUNE_CACHE) per GPU, side
+// multiset, chain count and sweeps per exchange.
+void autotune_persistent(umc_batch* b)
+{
+    cudaDeviceProp prop{};
+    cuda_check(cudaGetDeviceProperties(&prop, b->device), "device properties");
+    std::string gpu = prop.name;
+    for (char& ch : gpu)
+        if (ch == ' ') ch = '_';
+    std::map<uint32_t, uint32_t> sides;
+    for (uint32_t c = 0; c < b->n_chains; ++c) sides[b->L[c]]++;
+    std::string key = gpu + "/xy_batch_persistent/s" + std::to_string(b->sweeps_per_exchange);
+    for (auto& [L, n] : sides) key += "/L" + std::to_string(L) + "x" + std::to_string(n);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        load_tune_file();
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            build_persistent(b, it->second.cpk);
+            b->p_minb = it->second.cpc;
+            return;
+        }
+    }
+    DevBuf keep_theta, keep_small;
+    keep_theta.alloc(b->theta.bytes, "tuning copy");
+    const size_t hb = b->holder_dev.bytes, sb = b->slot_dev.bytes, cb = sizeof(BatchCounters);
+    keep_small.alloc(hb + sb + cb + 8, "tuning copy");
+    auto save = [&](bool back) {
+        auto cp = [&](void* dst, void* src, size_t n) {
+            cuda_check(cudaMemcpyAsync(back ? src : dst, back ? dst : src, n, cudaMemcpyDeviceToDevice, b->stream), "copy");
+        };
+        uint8_t* k = static_cast<uint8_t*>(keep_small.p);
+        cp(keep_theta.p, b->theta.p, b->theta.bytes);
+        cp(k, b->holder_dev.p, hb);
+        cp(k + hb, b->slot_dev.p, sb);
+        cp(k + hb + sb, b->ctr.p, cb);
+        cp(k + hb + sb + cb, b->swaps.p, 8);
+    };
+    save(false);
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "event");
+    cuda_check(cudaEventCreate(&e1), "event");
+    uint32_t best = kPersistClusters[0], best_minb = 1;
+    float best_ms = 1e30f;
+    for (uint32_t cand = 0; cand < 4; ++cand) {
+        const uint32_t kc = kPersistClusters[cand & 1u], minb = 1 + (cand >> 1);
+        build_persistent(b, kc);
+        b->p_minb = minb;
+        launch_persistent(b, b->stream);  // warm
+        cuda_check(cudaEventRecord(e0, b->stream), "event");
+        launch_persistent(b, b->stream);
+        launch_persistent(b, b->stream);
+        cuda_check(cudaEventRecord(e1, b->stream), "event");
+        cuda_check(cudaEventSynchronize(e1), "tuning");
+        float ms = 0;
+        cuda_check(cudaEventElapsedTime(&ms, e0, e1), "tuning");
+        save(true);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = kc;
+            best_minb = minb;
+        }
+    }
+    cuda_check(cudaStreamSynchronize(b->stream), "tuning");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    build_persistent(b, best);
+    b->p_minb = best_minb;
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    GroupCfg cfg{best_minb, best, kPersistBlock};  // chains-per-CTA field holds CTAs per SM here
+    if (g_tune_cache.emplace(key, cfg).second) store_tune_file(key, cfg);
 }
 
 void build_graph(umc_batch* b)
@@ -903,7 +1002,7 @@ void create_batch(const umc_batch_desc* d, umc_batch* b)
     up(b->cpk_dev, b->cpk_of_chain.data(), b->cpk_of_chain.size() * 4, "cpk");
     cuda_check(cudaMemset(b->ctr.p, 0, sizeof(BatchCounters)), "counters");
     cuda_check(cudaMemcpy(&b->ctr.as<BatchCounters>()->capacity, &b->max_records, 8, cudaMemcpyHostToDevice), "capacity");
-    build_persistent(b);
+    autotune_persistent(b);
     build_graph(b);
 }
 
@@ -1190,12 +1289,15 @@ int umc_batch_set_persistent(umc_batch* b, int enable)
     });
 }
 
-int umc_batch_persistent_info(const umc_batch* b, int* enabled, uint32_t* grid, uint32_t* big_items, uint32_t* items)
+int umc_batch_persistent_info(const umc_batch* b, int* enabled, uint32_t* grid, uint32_t* big_items, uint32_t* items,
+                              uint32_t* cluster, uint32_t* ctas_per_sm)
 {
     return bguard([&] {
         if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
         if (enabled) *enabled = b->persistent ? 1 : 0;
         if (grid) *grid = b->p_grid;
+        if (cluster) *cluster = b->p_kc;
+        if (ctas_per_sm) *ctas_per_sm = b->p_minb;
         if (big_items) *big_items = b->p_big;
         if (items) *items = b->p_items;
     });
