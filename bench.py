@@ -478,12 +478,17 @@ class XYBatch:
     def describe(self):
         counts = {int(L): int((self.Ls_all == L).sum()) for L in sorted(set(self.Ls_all.tolist()))}
         info = self.b.persistent_info()
+        if info["enabled"]:
+            form = (f"one persistent kernel per step ({info['grid']} CTAs of 1024 threads in clusters of "
+                    f"{info['cluster']}, {info['ctas_per_sm']} per SM, {info['big_items']} cluster-swept chains, "
+                    f"{info['items']} work items)")
+        else:
+            shapes = {L: self.b.config(L) for L in sorted(set(int(x) for x in self.Ls))}
+            form = f"one kernel per side group + the exchange kernel, as one graph per step (shapes {shapes})"
         return (f"512 XY chains in 32 replica-exchange ladders of 16, L per ladder {counts} (ladders per L), "
                 f"FP32 angles, J=1, betas geometric on [0.8, 1.3], U1Shift 1.0, swaps every 10 sweeps; "
-                f"step = 10 sweeps of every chain + one exchange round, one persistent kernel per step "
-                f"({info['grid']} CTAs of 1024 threads in clusters of {info['cluster']}, {info['ctas_per_sm']} per SM, "
-                f"{info['big_items']} cluster-swept chains, "
-                f"{info['items']} work items)")
+                f"step = 10 sweeps of every chain + one exchange round, {form}; the faster form "
+                f"measured at creation")
 
     def enqueue(self, k):
         self.b.enqueue(k)

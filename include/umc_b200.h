@@ -345,17 +345,18 @@ int umc_batch_seeds(const umc_batch* b, uint64_t* chain_seeds, uint64_t* ladder_
 int umc_batch_config(const umc_batch* b, uint32_t L, uint32_t* chains_per_cta, uint32_t* ctas_per_chain,
                      uint32_t* block);
 int umc_batch_sites(const umc_batch* b, uint64_t* total_sites, uint64_t* kernel_launches);
-/* A segment runs as one persistent kernel by default (enable = 1): resident
- * CTAs of 1024 threads in clusters take work items largest first -- a chain
- * with at least 2 x 8192 sites per colour whose rows split into cluster-many
- * bands of at least 2 is swept by a whole cluster, smaller chains are packed
- * into CTA items of up to 8192 sites per colour -- and the CTA that completes
- * a ladder runs its exchange.  The cluster size (4 or 8) and the CTAs per SM
- * (1 or 2) are autotuned at creation by timing segments on the batch itself
- * (state restored), and cached like the group shapes.  enable = 0 selects one
- * kernel per lattice-size group (autotuned launch shapes, umc_batch_config)
- * plus an exchange kernel, as parallel branches of the segment's graph.  Both
- * run the same chains and exchanges. */
+/* A segment runs in one of two forms; both run the same chains and
+ * exchanges.  Persistent (enable = 1): one kernel whose resident CTAs of 1024
+ * threads in clusters take work items largest first -- a chain with at least
+ * 2 x 8192 sites per colour whose rows split into cluster-many bands of at
+ * least 2 is swept by a whole cluster, smaller chains are packed into CTA
+ * items of up to 8192 sites per colour -- and the CTA that completes a ladder
+ * runs its exchange; its cluster size (4 or 8) and CTAs per SM (1 or 2) are
+ * tuned.  Grouped (enable = 0): one kernel per lattice-size group (tuned
+ * launch shapes, umc_batch_config) plus an exchange kernel, as parallel
+ * branches of the segment's graph.  At creation both forms are timed on the
+ * batch itself (state restored) and the faster one is selected; the choice
+ * is cached like the group shapes.  This call overrides it. */
 int umc_batch_set_persistent(umc_batch* b, int enable);
 int umc_batch_persistent_info(const umc_batch* b, int* enabled, uint32_t* grid, uint32_t* big_items, uint32_t* items,
                               uint32_t* cluster, uint32_t* ctas_per_sm);

@@ -202,16 +202,18 @@ def test_sharded_u1batch_equals_the_whole_batch(umc):
 
 
 def test_persistent_segment_equals_grouped_segments(umc):
-    """The one-kernel segment (default: resident clusters taking work items,
-    a 256^2 chain swept by a cluster of four CTAs, small chains packed, the
-    exchanges run by whichever CTA completes a ladder) and the per-group
-    kernels run the same chains and exchanges: fields bit for bit, temperature
-    maps and records equal (energies to FP64 summation order)."""
+    """The one-kernel segment (resident clusters taking work items, a 256^2
+    chain swept by a cluster of CTAs, small chains packed, the exchanges run
+    by whichever CTA completes a ladder) and the per-group kernels run the
+    same chains and exchanges: fields bit for bit, temperature maps and
+    records equal (energies to FP64 summation order).  Creation selects the
+    form that measured faster; both are forced here."""
     Ls = np.array([256, 16, 64, 32, 256, 128, 16])
     R = 4
     betas = np.stack([_geometric(0.8, 1.3, R)] * len(Ls))
     a = umc.Batch(Ls, betas, width=1.0, sweeps_per_exchange=4, seed=5)
     b = umc.Batch(Ls, betas, width=1.0, sweeps_per_exchange=4, seed=5)
+    a.set_persistent(True)
     b.set_persistent(False)
     info = a.persistent_info()
     assert info["enabled"] and info["grid"] % info["cluster"] == 0 and info["cluster"] in (4, 8)
@@ -227,3 +229,29 @@ def test_persistent_segment_equals_grouped_segments(umc):
     for c in range(a.n_chains):
         np.testing.assert_array_equal(a.get_field(c), b.get_field(c))
     assert a.sites()[1] == 5  # one kernel per segment
+
+
+def _check_wrapped(got, th):
+    far = np.abs(th) > 8
+    np.testing.assert_array_equal(got[~far], th[~far])
+    assert np.all(np.abs(got[far]) <= np.pi + 1e-6)
+    d = np.angle(np.exp(1j * (got[far].astype(np.float64) - th[far].astype(np.float64))))
+    np.testing.assert_allclose(d, 0, atol=1e-6)
+
+
+def test_uploaded_angles_outside_the_sincos_domain_are_wrapped(umc):
+    """The FP32 XY decisions bound __sincosf's error for |angle| <= 8; an
+    uploaded angle beyond that is stored as the same angle in [-pi, pi], and
+    every other angle exactly as given (batched and single chains)."""
+    L = 8
+    th = np.random.default_rng(0).uniform(-7.9, 7.9, L * L).astype(np.float32)
+    th[:6] = np.float32([100.0, -50.5, 8.5, -8.0001, 1e6, 8.0])
+    b = umc.Batch([L], np.array([[1.0, 1.1]]), width=1.0, seed=2)
+    b.set_field(0, th)
+    _check_wrapped(b.get_field(0), th)
+    ch = umc.Chain(umc.MODEL_XY_ANGLE, graph=umc.square_lattice(L, L), coupling=1.0,
+                   proposal=umc.PROPOSAL_U1SHIFT, width=1.0, seed=4)
+    ch.set_field(th)
+    _check_wrapped(ch.get_field(), th)
+    ch.upload_async(th)
+    _check_wrapped(ch.get_field(), th)

@@ -99,7 +99,7 @@ def test_slabs_over_ranks_are_the_chain(umc, model, dims, world):
     import torch.multiprocessing as mp
 
     beta = 0.44 if model == "ising" else 0.693
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.start_processes(_worker, args=(world, _free_port(), model, dims, beta, 10, out), nprocs=world,
                            start_method="spawn", join=True)

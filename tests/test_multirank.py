@@ -42,7 +42,7 @@ def _worker(rank, world, port, out):
 
 def test_replicas_aggregate_over_two_gloo_ranks():
     world = 2
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.start_processes(_worker, args=(world, _free_port(), out), nprocs=world, start_method="spawn", join=True)
         res = dict(out)
@@ -99,7 +99,7 @@ def test_sharded_records_gather_in_rank_order_over_two_gloo_ranks():
     import numpy as np
 
     world = 2
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.start_processes(_gather_worker, args=(world, _free_port(), out), nprocs=world, start_method="spawn",
                            join=True)

@@ -995,8 +995,9 @@ class Batch:
         return t.value, k.value
 
     def set_persistent(self, enable: bool) -> None:
-        """One persistent kernel per segment (default) or one kernel per
-        lattice-size group plus an exchange kernel."""
+        """One persistent kernel per segment, or one kernel per lattice-size
+        group plus an exchange kernel.  Creation selects the form that
+        measured faster on this batch; this overrides it."""
         check(lib.umc_batch_set_persistent(self._h, int(enable)))
 
     def persistent_info(self):

@@ -1115,9 +1115,10 @@ int umc_chain_set_field(umc_chain* c, const void* host_field)
         const uint32_t g = grid_for(c, c->n);
         LaunchScope ls(c, UMC_KERNEL_OTHER);
         if (c->elem_bytes == 1)
-            scatter_field<int8_t><<<g, kBlock, 0, c->stream>>>(c->staging.as<int8_t>(), c->field.as<int8_t>(), uint32_t(c->n), 1, placement(c));
+            scatter_field<int8_t><<<g, kBlock, 0, c->stream>>>(c->staging.as<int8_t>(), c->field.as<int8_t>(), uint32_t(c->n), 1, placement(c), false);
         else
-            scatter_field<float><<<g, kBlock, 0, c->stream>>>(c->staging.as<float>(), c->field.as<float>(), uint32_t(c->n), c->comps, placement(c));
+            scatter_field<float><<<g, kBlock, 0, c->stream>>>(c->staging.as<float>(), c->field.as<float>(), uint32_t(c->n), c->comps, placement(c),
+                                                               c->model == UMC_MODEL_XY_ANGLE);
         launch_check("scatter field");
         // the caller's buffer is free once the copy has landed; the scatter
         // is stream-ordered before any later work on the chain
@@ -1256,10 +1257,11 @@ int umc_chain_upload_async(umc_chain* c, const void* host_field)
             LaunchScope ls(c, UMC_KERNEL_OTHER);
             if (c->elem_bytes == 1)
                 scatter_field<int8_t><<<g, kBlock, 0, c->stream>>>(c->up_staging[q].as<int8_t>(), c->field.as<int8_t>(),
-                                                                   uint32_t(c->n), 1, placement(c));
+                                                                   uint32_t(c->n), 1, placement(c), false);
             else
                 scatter_field<float><<<g, kBlock, 0, c->stream>>>(c->up_staging[q].as<float>(), c->field.as<float>(),
-                                                                  uint32_t(c->n), c->comps, placement(c));
+                                                                  uint32_t(c->n), c->comps, placement(c),
+                                                                  c->model == UMC_MODEL_XY_ANGLE);
             launch_check("scatter field");
         }
         cuda_check(cudaEventRecord(c->up_consumed[q], c->stream), "upload event");

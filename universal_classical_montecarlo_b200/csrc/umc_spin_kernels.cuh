@@ -16,8 +16,10 @@
 #pragma once
 
 #include <cmath>
+#include <type_traits>
 
 #include "umc_device.cuh"
+#include "umc_math64.cuh"
 
 namespace umc {
 
@@ -488,12 +490,24 @@ inline float vector_wolff_err(double beta, double J, int N)
 {
     return float(std::fabs(beta * J) * 0x1.0p-24 * (4.0 * N + 8.0));
 }
-// XY on angles over deg neighbours with __sincosf (each value within 2^-18 of
-// the exact one, generously, for angles within a few pi of zero):
-// beta |J| deg 2^-18 10.
+// XY on angles over d neighbours (xy_pass; the batched chains with d = 4):
+// lp = -beta J ((cos p - cos t) C + (sin p - sin t) S) from __sincosf values
+// within e = kSincosfAbsErr of the exact ones (every angle within
+// kSincosfDomain) and FP32 roundings of at most u = 2^-24 of each result:
+//   C, S (d values, sums up to d):          dC = d e + u (d (d + 1) / 2 - 1)
+//   cos p - cos t, sin p - sin t (<= 2):    da = 2 e + 2 u
+//   each product (<= 2 d, rounded):         dP = 2 dC + d da + 2 d u
+//   their sum (<= 4 d), J and beta (each rounded to FP32 and multiplied):
+//   beta |J| (2 dP + 4 d u (sum) + 8 d u (J) + 8 d u (beta)).
+// The factor 1 + 2^-10 covers the second-order terms.  For d = 4:
+// beta |J| (32 e + 148 u), about 4.8e-5 beta |J|.
 inline float xy_metropolis_err(double beta, double J, uint32_t deg)
 {
-    return float(std::fabs(beta * J) * double(deg) * 0x1.0p-18 * 10.0);
+    const double e = kSincosfAbsErr, u = 0x1.0p-24, d = double(deg);
+    const double dC = d * e + u * (d * (d + 1.0) / 2.0 - 1.0);
+    const double da = 2.0 * e + 2.0 * u;
+    const double dP = 2.0 * dC + d * da + 2.0 * d * u;
+    return float(std::fabs(beta * J) * (2.0 * dP + 20.0 * d * u) * (1.0 + 0x1.0p-10));
 }
 // The U(1) gauge passes (umc_gauge_kernels.cuh, and the plain batched U(1)
 // chains), deg = cells per link: a cell's staple angle sums three FP32 angles
@@ -620,12 +634,18 @@ struct XYArgs
 template <class Topo>
 __device__ __noinline__ double xy_log_ratio64(const XYArgs& a, Topo t, uint32_t k, float t0, float p)
 {
-    double d = 0.0;
+    // sum_j cos(x - t_j) = cos x C + sin x S, C and S the neighbours' sums
+    double C = 0.0, S = 0.0;
     t.neighbours(k, [&](uint32_t j, bool) {
-        const double tj = a.th[j];
-        d += -a.J64 * (cos(double(p) - tj) - cos(double(t0) - tj));
+        double sn, cs;
+        sincos_cw64(double(a.th[j]), sn, cs);
+        C += cs;
+        S += sn;
     });
-    return -a.beta64 * d;
+    double s0, c0, s1, c1;
+    sincos_cw64(double(t0), s0, c0);
+    sincos_cw64(double(p), s1, c1);
+    return a.beta64 * a.J64 * ((c1 - c0) * C + (s1 - s0) * S);
 }
 
 // (kBlock, 5): at most 48 registers (see vector_pass).
@@ -909,11 +929,17 @@ struct Placement
 
 // site-order AoS (the reference's data()) <-> colour-major SoA
 template <class T>
-__global__ void scatter_field(const T* src, T* dst, uint32_t n, uint32_t comps, Placement pl)
+__global__ void scatter_field(const T* src, T* dst, uint32_t n, uint32_t comps, Placement pl, bool angles)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t k = pl(i);
-        for (uint32_t c = 0; c < comps; ++c) dst[uint64_t(c) * n + k] = src[uint64_t(i) * comps + c];
+        for (uint32_t c = 0; c < comps; ++c) {
+            T v = src[uint64_t(i) * comps + c];
+            // XY angles: kept within the domain of the FP32 decisions' sincos bound
+            if constexpr (std::is_same_v<T, float>)
+                if (angles) v = wrap_angle(v);
+            dst[uint64_t(c) * n + k] = v;
+        }
     }
 }
 
