@@ -274,21 +274,28 @@ __global__ void __launch_bounds__(1024) xy_batch_segment(SegArgs a)
 // accepted updates, 0] for every temperature slot, then its exchange round:
 // slots (k, k+1), k of the round's parity, swap their chains iff
 // (beta_k - beta_{k+1})(E_k - E_{k+1}) >= 0 or log(u) < that product.  One
-// thread; part holds each chain's share partials (read through L2: another
-// CTA may have written them in this launch).
+// warp: lane q sums the energy of the ladder's chains q and q + 32, writes
+// the records of slots q and q + 32, and decides the pairs starting at
+// parity + 2 q (+ 64): the pairs of a round are disjoint, so their swaps
+// are independent.  Every sum runs over the shares in the same order as a
+// single thread would.  part holds each chain's share partials (read
+// through L2: another CTA may have written them in this launch); E is 64
+// doubles of shared memory for this warp.
 __device__ void exchange_ladder(uint32_t l, uint32_t R, unsigned long long round, unsigned long long rec, bool keep,
                                 uint32_t n_ladders, const uint32_t* cpk_of_chain, const double* part,
                                 const double* betas, uint32_t* holder, uint32_t* slot_of_chain,
-                                const unsigned long long* ladder_seed, double* records, unsigned long long* swaps)
+                                const unsigned long long* ladder_seed, double* records, unsigned long long* swaps,
+                                double* E)
 {
-    double E[kMaxRungs];
-    for (uint32_t q = 0; q < R; ++q) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t q = lane; q < R; q += 32) {
         const uint32_t c = l * R + q, k = cpk_of_chain[c];
         double e = 0.0;
         for (uint32_t r = 0; r < k; ++r) e += __ldcg(part + (uint64_t(c) * kMaxShares + r) * 4);
         E[q] = e;
     }
-    for (uint32_t k = 0; k < R && keep; ++k) {
+    __syncwarp();
+    for (uint32_t k = lane; k < R && keep; k += 32) {
         const uint32_t c = holder[l * R + k], nk = cpk_of_chain[c];
         double mx = 0.0, my = 0.0, acc = 0.0;
         for (uint32_t r = 0; r < nk; ++r) {
@@ -306,9 +313,10 @@ __device__ void exchange_ladder(uint32_t l, uint32_t R, unsigned long long round
         out[6] = acc;
         out[7] = 0.0;
     }
+    __syncwarp();  // every slot's holder read before any pair swaps
     const uint32_t parity = uint32_t(round & 1ull);
     const uint64_t kb = key_base(key_seed(ladder_seed[l], round, kTagSwap));
-    for (uint32_t k = parity; k + 1 < R; k += 2) {
+    for (uint32_t k = parity + 2 * lane; k + 1 < R; k += 64) {
         const uint32_t a = holder[l * R + k], b = holder[l * R + k + 1];
         const double delta = (betas[l * R + k] - betas[l * R + k + 1]) * (E[a - l * R] - E[b - l * R]);
         const bool acc = delta >= 0.0 || log(u_f64(first_draw(kb, k))) < delta;
@@ -321,6 +329,7 @@ __device__ void exchange_ladder(uint32_t l, uint32_t R, unsigned long long round
             atomicAdd(swaps, 1ull);
         }
     }
+    __syncwarp();
 }
 
 // The segment's bookkeeping once every ladder has exchanged: counters advance
@@ -334,19 +343,25 @@ __device__ __forceinline__ void close_segment(BatchCounters* ctr, unsigned long 
     else ctr->status |= kBatchErrRecords;
 }
 
-// One exchange round per ladder (one thread per ladder).
-__global__ void xy_batch_swap(BatchCounters* ctr, uint32_t n_ladders, uint32_t R, const uint32_t* cpk_of_chain,
-                              const double* part, const double* betas, uint32_t* holder, uint32_t* slot_of_chain,
-                              const unsigned long long* ladder_seed, double* records, unsigned long long* swaps,
-                              uint32_t sweeps)
+// One exchange round per ladder: one warp per ladder, up to 32 warps.
+constexpr uint32_t kSwapWarps = 32;
+__global__ void __launch_bounds__(kSwapWarps * 32) xy_batch_swap(BatchCounters* ctr, uint32_t n_ladders, uint32_t R,
+                                                                 const uint32_t* cpk_of_chain, const double* part,
+                                                                 const double* betas, uint32_t* holder,
+                                                                 uint32_t* slot_of_chain,
+                                                                 const unsigned long long* ladder_seed,
+                                                                 double* records, unsigned long long* swaps,
+                                                                 uint32_t sweeps)
 {
+    __shared__ double E[kSwapWarps][kMaxRungs];
     const unsigned long long round = ctr->round;
     const unsigned long long rec = ctr->rec;
     const bool keep = rec < ctr->capacity;
     __syncthreads();
-    for (uint32_t l = threadIdx.x; l < n_ladders; l += blockDim.x)
+    const uint32_t w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t l = w; l < n_ladders; l += nw)
         exchange_ladder(l, R, round, rec, keep, n_ladders, cpk_of_chain, part, betas, holder, slot_of_chain,
-                        ladder_seed, records, swaps);
+                        ladder_seed, records, swaps, E[w]);
     __syncthreads();
     if (threadIdx.x == 0) close_segment(ctr, round, rec, keep, sweeps);
 }
@@ -384,22 +399,28 @@ struct PersistArgs
 };
 
 // Counts the item's chain shares as done; the CTA that completes a ladder
-// exchanges it, and the one that completes the last ladder closes the segment.
-__device__ void complete_item(const PersistArgs& p, const uint32_t* chains, uint32_t chain_n, uint32_t shares)
+// exchanges it (its first warp), and the one that completes the last ladder
+// closes the segment.
+__device__ void complete_item(const PersistArgs& p, const uint32_t* chains, uint32_t chain_n, uint32_t shares,
+                              double* E)
 {
-    if (threadIdx.x != 0) return;
-    __threadfence();  // this CTA's partials before the counts that publish them
+    if (threadIdx.x >= 32) return;
+    const uint32_t lane = threadIdx.x;
+    if (lane == 0) __threadfence();  // this CTA's partials before the counts that publish them
     const SegArgs& a = p.seg;
     for (uint32_t ci = 0; ci < chain_n; ++ci) {
         const uint32_t l = chains[ci] / a.R;
-        if (atomicAdd(&p.ladder_done[l], 1u) + 1u != a.R * shares) continue;
+        unsigned last = 0;
+        if (lane == 0) last = atomicAdd(&p.ladder_done[l], 1u) + 1u == a.R * shares ? 1u : 0u;
+        if (!__shfl_sync(0xffffffffu, last, 0)) continue;
         __threadfence();
         const unsigned long long round = a.ctr->round, rec = a.ctr->rec;
         const bool keep = rec < a.ctr->capacity;
         exchange_ladder(l, a.R, round, rec, keep, p.n_ladders, p.cpk_of_chain, a.part, a.betas, p.holder,
-                        const_cast<uint32_t*>(a.slot_of_chain), p.ladder_seed, p.records, p.swaps);
-        __threadfence();
-        if (atomicAdd(&p.sched[2], 1u) + 1u == p.n_ladders)
+                        const_cast<uint32_t*>(a.slot_of_chain), p.ladder_seed, p.records, p.swaps, E);
+        __threadfence();  // every lane's writes before the count that ends the segment
+        __syncwarp();
+        if (lane == 0 && atomicAdd(&p.sched[2], 1u) + 1u == p.n_ladders)
             close_segment(const_cast<BatchCounters*>(a.ctr), round, rec, keep, a.sweeps);
     }
 }
@@ -411,6 +432,7 @@ __global__ void __launch_bounds__(kPersistBlock, MINB) xy_batch_persistent(Persi
 {
     __shared__ SegShared sh;
     __shared__ uint32_t item_sh;
+    __shared__ double E[kMaxRungs];  // the exchange's energies
     cg::cluster_group cl = cg::this_cluster();
     // big chains: the whole cluster, one band of rows per CTA
     for (;;) {
@@ -426,7 +448,7 @@ __global__ void __launch_bounds__(kPersistBlock, MINB) xy_batch_persistent(Persi
         a.half = w.z * w.z / 2;
         const uint32_t rows = w.z / KC, share = cl.block_rank();
         run_share<true>(a, sh, p.chains + w.x, 1, share * rows, rows, share);
-        complete_item(p, p.chains + w.x, 1, KC);
+        complete_item(p, p.chains + w.x, 1, KC, E);
     }
     // packed smaller chains, one CTA each
     for (;;) {
@@ -441,7 +463,7 @@ __global__ void __launch_bounds__(kPersistBlock, MINB) xy_batch_persistent(Persi
         a.H = w.z / 2;
         a.half = w.z * w.z / 2;
         run_share<false>(a, sh, p.chains + w.x, w.y, 0, w.z, 0);
-        complete_item(p, p.chains + w.x, w.y, 1);
+        complete_item(p, p.chains + w.x, w.y, 1, E);
     }
 }
 
@@ -922,7 +944,7 @@ void build_graph(umc_batch* b)
         cuda_check(cudaEventRecord(g.done, g.stream), "join");
         cuda_check(cudaStreamWaitEvent(b->stream, g.done, 0), "join wait");
     }
-    xy_batch_swap<<<1, 64, 0, b->stream>>>(b->ctr.as<BatchCounters>(), b->n_ladders, b->R, b->cpk_dev.as<uint32_t>(),
+    xy_batch_swap<<<1, std::min(b->n_ladders, kSwapWarps) * 32, 0, b->stream>>>(b->ctr.as<BatchCounters>(), b->n_ladders, b->R, b->cpk_dev.as<uint32_t>(),
                                              b->part.as<double>(), b->betas_dev.as<double>(), b->holder_dev.as<uint32_t>(),
                                              b->slot_dev.as<uint32_t>(), b->lseeds_dev.as<unsigned long long>(),
                                              b->records.as<double>(), b->swaps.as<unsigned long long>(),
