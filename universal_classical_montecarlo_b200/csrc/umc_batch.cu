@@ -105,9 +105,13 @@ __device__ __noinline__ double xy4_log_ratio64(double J64, double beta64, float 
 
 // One XY site update (the body of xy_pass in umc_spin_kernels.cuh) on chain
 // data `th`; neighbours through L1 inside one CTA, through L2 in a cluster.
+// In a cluster, rows [row_lo, row_lo + row_n) of both colours are written by
+// this CTA alone, so they are read through L1; the two halo rows belong to
+// other CTAs of the cluster and are read through L2.
 template <bool CLUSTER>
 __device__ __forceinline__ bool xy_update(const SegArgs& a, float* th, uint32_t colour, uint32_t y, uint32_t i,
-                                          uint64_t kbase, float beta, double beta64)
+                                          uint64_t kbase, float beta, double beta64, uint32_t row_lo,
+                                          uint32_t row_n)
 {
     const uint32_t L = a.L, H = a.H;
     const uint32_t p = (y + colour) & 1u;
@@ -115,8 +119,10 @@ __device__ __forceinline__ bool xy_update(const SegArgs& a, float* th, uint32_t 
     float* own = th + colour * a.half;
     const uint32_t ym = y == 0 ? L - 1 : y - 1, yp = y + 1 == L ? 0u : y + 1;
     const uint32_t i2 = p ? (i + 1 == H ? 0u : i + 1) : (i == 0 ? H - 1 : i - 1);
-    const float nb[4] = {ldf<CLUSTER>(other + y * H + i), ldf<CLUSTER>(other + y * H + i2),
-                         ldf<CLUSTER>(other + ym * H + i), ldf<CLUSTER>(other + yp * H + i)};
+    const bool l2m = CLUSTER && ym - row_lo >= row_n, l2p = CLUSTER && yp - row_lo >= row_n;
+    const float nb[4] = {other[y * H + i], other[y * H + i2],
+                         l2m ? __ldcg(other + ym * H + i) : other[ym * H + i],
+                         l2p ? __ldcg(other + yp * H + i) : other[yp * H + i]};
     float C = 0.f, S = 0.f;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -126,7 +132,7 @@ __device__ __forceinline__ bool xy_update(const SegArgs& a, float* th, uint32_t 
         S += sn;
     }
     const uint32_t k = colour * a.half + y * H + i;
-    const float t = ldf<CLUSTER>(own + y * H + i);
+    const float t = own[y * H + i];
     KeyedPcg g = KeyedPcg::open(kbase, k);
     const float prop = u1_shift(g, a.width, t);
     float so, co, sp, cp;
@@ -202,7 +208,8 @@ __device__ __forceinline__ void run_share(const SegArgs& a, SegShared& sh, const
                 uint32_t ci, y, i;
                 site_of(w, ci, y, i);
                 const bool acc =
-                    xy_update<CLUSTER>(a, a.theta + sh.off[ci], colour, y, i, sh.kb[ci], sh.beta[ci], sh.beta64[ci]);
+                    xy_update<CLUSTER>(a, a.theta + sh.off[ci], colour, y, i, sh.kb[ci], sh.beta[ci], sh.beta64[ci],
+                                       row_lo, row_n);
                 if (warp_chain) {
                     // the whole warp works on chain ci: one shared atomic per warp
                     const unsigned act = __activemask();
