@@ -185,18 +185,199 @@ struct U1Shift
 };
 
 // ---- SU(N) ---------------------------------------------------------------------
-// N x N row-major complex matrix (the reference's SULink<N> layout).
+// A complex number in the layout of std::complex<double> (real part, then
+// imaginary part) that device code can use, which std::complex cannot.  It
+// converts to and from std::complex on the host; conj, abs and norm are found
+// by argument-dependent lookup, and the arithmetic is the textbook one
+// ((a + bi)(c + di) = (ac - bd) + (ad + bc)i).
+struct Complex
+{
+    double re = 0.0, im = 0.0;
+
+    Complex() = default;
+    UMC_FACADE_HD constexpr Complex(double r, double i = 0.0) noexcept : re(r), im(i) {}
+    Complex(const std::complex<double>& z) noexcept : re(z.real()), im(z.imag()) {}
+    operator std::complex<double>() const noexcept { return {re, im}; }
+
+    UMC_FACADE_HD constexpr double real() const noexcept { return re; }
+    UMC_FACADE_HD constexpr double imag() const noexcept { return im; }
+
+    UMC_FACADE_HD constexpr Complex& operator+=(const Complex& z) noexcept
+    {
+        re += z.re;
+        im += z.im;
+        return *this;
+    }
+    UMC_FACADE_HD constexpr Complex& operator-=(const Complex& z) noexcept
+    {
+        re -= z.re;
+        im -= z.im;
+        return *this;
+    }
+    UMC_FACADE_HD constexpr Complex& operator*=(const Complex& z) noexcept
+    {
+        const double r = re * z.re - im * z.im, i = re * z.im + im * z.re;
+        re = r;
+        im = i;
+        return *this;
+    }
+    UMC_FACADE_HD constexpr Complex& operator*=(double x) noexcept
+    {
+        re *= x;
+        im *= x;
+        return *this;
+    }
+    UMC_FACADE_HD constexpr Complex& operator/=(double x) noexcept
+    {
+        re /= x;
+        im /= x;
+        return *this;
+    }
+    UMC_FACADE_HD friend constexpr Complex operator+(Complex a, const Complex& b) noexcept { return a += b; }
+    UMC_FACADE_HD friend constexpr Complex operator-(Complex a, const Complex& b) noexcept { return a -= b; }
+    UMC_FACADE_HD friend constexpr Complex operator*(Complex a, const Complex& b) noexcept { return a *= b; }
+    UMC_FACADE_HD friend constexpr Complex operator*(Complex a, double x) noexcept { return a *= x; }
+    UMC_FACADE_HD friend constexpr Complex operator*(double x, Complex a) noexcept { return a *= x; }
+    UMC_FACADE_HD friend constexpr Complex operator/(Complex a, double x) noexcept { return a /= x; }
+    UMC_FACADE_HD friend constexpr Complex operator-(const Complex& a) noexcept { return {-a.re, -a.im}; }
+    UMC_FACADE_HD friend constexpr bool operator==(const Complex& a, const Complex& b) noexcept
+    {
+        return a.re == b.re && a.im == b.im;
+    }
+    UMC_FACADE_HD friend constexpr Complex conj(const Complex& z) noexcept { return {z.re, -z.im}; }
+    UMC_FACADE_HD friend constexpr double norm(const Complex& z) noexcept { return z.re * z.re + z.im * z.im; }
+    UMC_FACADE_HD friend double abs(const Complex& z) noexcept { return std::hypot(z.re, z.im); }
+};
+static_assert(sizeof(Complex) == sizeof(std::complex<double>) && alignof(Complex) == alignof(std::complex<double>));
+
+// One SU(N) link: an N x N complex matrix, row-major (dof/sun.hpp:14-76), with
+// the reference's group operations.  Host and device code (nvcc builds) can
+// both use it, so a user's SU(N) term written against this interface runs on
+// the device unchanged.
 template <std::size_t N>
 struct SULink
 {
-    std::array<std::complex<double>, N * N> m{};
-    static SULink identity() noexcept
+    static_assert(N >= 2, "SU(N) needs N >= 2");
+    static constexpr std::size_t dim = N;
+    using Mat = std::array<Complex, N * N>;
+
+    Mat m{};
+
+    SULink() = default;
+    UMC_FACADE_HD explicit SULink(const Mat& mat) : m(mat) {}
+
+    UMC_FACADE_HD static SULink identity() noexcept
     {
         SULink u;
         for (std::size_t i = 0; i < N; ++i) u.m[i * N + i] = 1.0;
         return u;
     }
+    UMC_FACADE_HD SULink dagger() const noexcept
+    {
+        SULink u;
+        for (std::size_t i = 0; i < N; ++i)
+            for (std::size_t j = 0; j < N; ++j) u.m[i * N + j] = conj(m[j * N + i]);
+        return u;
+    }
+    // Re Tr U; the plaquette action divides it by N.
+    UMC_FACADE_HD double real_trace() const noexcept
+    {
+        double t = 0.0;
+        for (std::size_t i = 0; i < N; ++i) t += m[i * N + i].real();
+        return t;
+    }
+    // max_ij |(U^dagger U - I)_ij|
+    UMC_FACADE_HD double unitarity_error() const noexcept
+    {
+        const SULink u = dagger() * (*this);
+        double e = 0.0;
+        for (std::size_t i = 0; i < N; ++i)
+            for (std::size_t j = 0; j < N; ++j) {
+                const double d = abs(u.m[i * N + j] - Complex(i == j ? 1.0 : 0.0));
+                e = d > e ? d : e;
+            }
+        return e;
+    }
+    UMC_FACADE_HD friend SULink operator*(const SULink& a, const SULink& b) noexcept
+    {
+        SULink r;
+        for (std::size_t i = 0; i < N; ++i)
+            for (std::size_t j = 0; j < N; ++j) {
+                Complex s = 0.0;
+                for (std::size_t k = 0; k < N; ++k) s += a.m[i * N + k] * b.m[k * N + j];
+                r.m[i * N + j] = s;
+            }
+        return r;
+    }
 };
+
+// Re Tr(U0 U1 U2^dagger U3^dagger) / N, the oriented plaquette (dof/sun.hpp:78-84).
+template <std::size_t N>
+UMC_FACADE_HD double plaquette(const SULink<N>& u0, const SULink<N>& u1, const SULink<N>& u2,
+                               const SULink<N>& u3) noexcept
+{
+    return (u0 * u1 * u2.dagger() * u3.dagger()).real_trace() / double(N);
+}
+
+namespace sun_detail {
+template <std::size_t N>
+using Mat = std::array<Complex, N * N>;
+
+template <std::size_t N>
+UMC_FACADE_HD Mat<N> mul(const Mat<N>& a, const Mat<N>& b) noexcept
+{
+    Mat<N> r{};
+    for (std::size_t i = 0; i < N; ++i)
+        for (std::size_t j = 0; j < N; ++j) {
+            Complex s = 0.0;
+            for (std::size_t k = 0; k < N; ++k) s += a[i * N + k] * b[k * N + j];
+            r[i * N + j] = s;
+        }
+    return r;
+}
+
+// Largest absolute row sum (each entry's modulus).
+template <std::size_t N>
+UMC_FACADE_HD double norm_inf(const Mat<N>& a) noexcept
+{
+    double n = 0.0;
+    for (std::size_t i = 0; i < N; ++i) {
+        double row = 0.0;
+        for (std::size_t j = 0; j < N; ++j) row += abs(a[i * N + j]);
+        n = row > n ? row : n;
+    }
+    return n;
+}
+
+// exp(A) as dof/sun.hpp:118-146 computes it: halve A until its norm is at most
+// 1/2, sum the Taylor series until a term's norm drops below 1e-16 (at most 30
+// terms), square back.  The steps are kept so that a chain on the device
+// proposes what the reference proposes, to rounding.
+template <std::size_t N>
+UMC_FACADE_HD SULink<N> expm(const Mat<N>& a) noexcept
+{
+    double n = norm_inf<N>(a);
+    int squarings = 0;
+    while (n > 0.5) {
+        n *= 0.5;
+        ++squarings;
+    }
+    const double scale = std::ldexp(1.0, -squarings);
+    Mat<N> b = a;
+    for (auto& z : b) z *= scale;
+    Mat<N> result{}, term{};
+    for (std::size_t i = 0; i < N; ++i) result[i * N + i] = 1.0;
+    for (std::size_t i = 0; i < N; ++i) term[i * N + i] = 1.0;
+    for (std::size_t k = 1; k <= 30; ++k) {
+        term = mul<N>(term, b);
+        for (auto& z : term) z /= double(k);
+        for (std::size_t i = 0; i < N * N; ++i) result[i] += term[i];
+        if (norm_inf<N>(term) < 1e-16) break;
+    }
+    for (int k = 0; k < squarings; ++k) result = mul<N>(result, result);
+    return SULink<N>(result);
+}
+}  // namespace sun_detail
 
 template <std::size_t N>
 struct SUDof
@@ -205,12 +386,42 @@ struct SUDof
     static constexpr std::size_t size = 1;
 };
 
-// U -> U exp(i X), X traceless Hermitian of scale `width` (device only).
+// U -> U exp(i X), X traceless Hermitian with independent uniform entries of
+// scale `width` (dof/sun.hpp:160-204; the proposal is symmetric).  The draws
+// come in the reference's order: the N diagonal entries, then the real and
+// imaginary parts of each entry above the diagonal, row by row.  The engine's
+// own SU(N) chains only take the width from it; sample() runs for user
+// SU(N) terms (on the device in nvcc builds) and on the host.
 template <std::size_t N>
 struct SUShift
 {
-    double width = 0.2;
-    double log_ratio(const SULink<N>*, const SULink<N>*) const noexcept { return 0.0; }
+    static_assert(N >= 2, "SUShift needs N >= 2");
+    double width = 0.3;
+
+    template <class R>
+    UMC_FACADE_HD void sample(const SULink<N>* cur, R& rng, SULink<N>* out) const
+    {
+        sun_detail::Mat<N> x{};
+        double tr = 0.0;
+        for (std::size_t i = 0; i < N; ++i) {
+            const double d = width * (2.0 * rng.uni() - 1.0);
+            x[i * N + i] = d;
+            tr += d;
+        }
+        for (std::size_t i = 0; i < N; ++i)
+            for (std::size_t j = i + 1; j < N; ++j) {
+                const double a = width * (2.0 * rng.uni() - 1.0);
+                const double b = width * (2.0 * rng.uni() - 1.0);
+                x[i * N + j] = Complex(a, b);
+                x[j * N + i] = Complex(a, -b);
+            }
+        for (std::size_t i = 0; i < N; ++i) x[i * N + i] -= Complex(tr / double(N));
+        // A = i X is anti-Hermitian, so exp(A) is unitary
+        sun_detail::Mat<N> a{};
+        for (std::size_t k = 0; k < N * N; ++k) a[k] = Complex(-x[k].imag(), x[k].real());
+        *out = (*cur) * sun_detail::expm<N>(a);
+    }
+    UMC_FACADE_HD double log_ratio(const SULink<N>*, const SULink<N>*) const noexcept { return 0.0; }
 };
 
 // Engine extension: `hits` Metropolis hits per site and sweep with the inner

@@ -123,27 +123,7 @@ struct SUPlaquetteTerm
     static constexpr std::size_t arity = 4;
     double beta = 1.0;
 
-    static double real_plaquette(const dtype* const* l)
-    {
-        using C = std::complex<double>;
-        std::array<C, N * N> a{}, b{};
-        for (std::size_t i = 0; i < N; ++i)
-            for (std::size_t j = 0; j < N; ++j) {
-                C s = 0;
-                for (std::size_t k = 0; k < N; ++k) s += l[0]->m[i * N + k] * l[1]->m[k * N + j];
-                a[i * N + j] = s;
-            }
-        for (std::size_t i = 0; i < N; ++i)
-            for (std::size_t j = 0; j < N; ++j) {
-                C s = 0;
-                for (std::size_t k = 0; k < N; ++k) s += a[i * N + k] * std::conj(l[2]->m[j * N + k]);
-                b[i * N + j] = s;
-            }
-        double tr = 0.0;
-        for (std::size_t i = 0; i < N; ++i)
-            for (std::size_t k = 0; k < N; ++k) tr += (b[i * N + k] * std::conj(l[3]->m[i * N + k])).real();
-        return tr / double(N);
-    }
+    static double real_plaquette(const dtype* const* l) { return plaquette(*l[0], *l[1], *l[2], *l[3]); }
     energy_type energy(const dtype* const* links) const { return beta * (1.0 - real_plaquette(links)); }
     energy_type delta(std::size_t which, const dtype*, const dtype* nw, const dtype* const* links) const
     {
@@ -245,7 +225,7 @@ public:
 
     PairModel(G graph, Term term) : graph_(std::move(graph)), term_(std::move(term))
     {
-        this->host_.assign(graph_.sites() * DT::scalars, typename DT::HS(0));
+        this->host_.assign(graph_.sites() * DT::scalars, typename DT::HS{});
     }
 
     std::size_t sites() const noexcept { return graph_.sites(); }
@@ -329,7 +309,7 @@ public:
 
     CellModel(List list, Term term) : list_(std::move(list)), term_(std::move(term))
     {
-        this->host_.assign(list_.sites() * DT::scalars, typename DT::HS(0));
+        this->host_.assign(list_.sites() * DT::scalars, typename DT::HS{});
     }
 
     std::size_t sites() const noexcept { return list_.sites(); }

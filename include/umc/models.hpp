@@ -336,27 +336,7 @@ public:
 
 private:
     // ReTr(U0 U1 U2^dag U3^dag) / N
-    static double plaq(const SULink<N>* const l[4])
-    {
-        using C = std::complex<double>;
-        std::array<C, N * N> a{}, b{};
-        for (std::size_t i = 0; i < N; ++i)
-            for (std::size_t j = 0; j < N; ++j) {
-                C s = 0;
-                for (std::size_t k = 0; k < N; ++k) s += l[0]->m[i * N + k] * l[1]->m[k * N + j];
-                a[i * N + j] = s;
-            }
-        for (std::size_t i = 0; i < N; ++i)
-            for (std::size_t j = 0; j < N; ++j) {
-                C s = 0;
-                for (std::size_t k = 0; k < N; ++k) s += a[i * N + k] * std::conj(l[2]->m[j * N + k]);
-                b[i * N + j] = s;
-            }
-        double tr = 0.0;
-        for (std::size_t i = 0; i < N; ++i)
-            for (std::size_t k = 0; k < N; ++k) tr += (b[i * N + k] * std::conj(l[3]->m[i * N + k])).real();
-        return tr / double(N);
-    }
+    static double plaq(const SULink<N>* const l[4]) { return plaquette(*l[0], *l[1], *l[2], *l[3]); }
 
     CellComplex<4> cells_;
     double beta_;

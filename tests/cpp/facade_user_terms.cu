@@ -8,7 +8,8 @@
 // Writes to argv[1], in order: the XY start and end angles; the Ising start
 // spins, the spins after 12 flips, their cluster sizes, the spins after one
 // more Wolff sweep and the mean cluster size; the U(1) start and end angles;
-// the O(3) start and end spins.
+// the O(3) start and end spins; the SU(3) start and end links (18 doubles
+// each, the reference's data() layout).
 #include <umc/umc.hpp>
 
 #include <cmath>
@@ -96,8 +97,30 @@ struct MyHeisenbergTerm
     }
 };
 
+// S_p = beta (1 - Re Tr(U0 U1 U2^dag U3^dag) / 3) on SULink<3>, written
+// against the reference's SULink interface (plaquette, operator*, dagger).
+struct MySU3PlaquetteTerm
+{
+    using dtype = SULink<3>;
+    using energy_type = double;
+    static constexpr std::size_t arity = 4;
+    double beta = 1.0;
+
+    __host__ __device__ energy_type energy(const dtype* const* l) const
+    {
+        return beta * (1.0 - plaquette(*l[0], *l[1], *l[2], *l[3]));
+    }
+    __host__ __device__ energy_type delta(std::size_t which, const dtype*, const dtype* nw,
+                                          const dtype* const* l) const
+    {
+        const dtype* p[4] = {l[0], l[1], l[2], l[3]};
+        p[which] = nw;
+        return beta * (plaquette(*l[0], *l[1], *l[2], *l[3]) - plaquette(*p[0], *p[1], *p[2], *p[3]));
+    }
+};
+
 static_assert(CellTerm<XYAngleTerm, U1Dof> && CellTerm<MyIsingTerm, IsingDof> && CellTerm<MyPlaquetteTerm, U1Dof> &&
-              CellTerm<MyHeisenbergTerm, VectorDof<3>>);
+              CellTerm<MyHeisenbergTerm, VectorDof<3>> && CellTerm<MySU3PlaquetteTerm, SUDof<3>>);
 
 template <class T>
 static void put(std::FILE* f, const T* p, std::size_t n)
@@ -201,6 +224,35 @@ int main(int argc, char** argv)
         const std::vector<double> v1(o3.data(), o3.data() + 3 * o3.sites());
         put(out, v0.data(), v0.size());
         put(out, v1.data(), v1.size());
+
+        // SU(3): CellModel<SUDof<3>, user cell term, CellComplex<4>> on the 4^4
+        // plaquettes, the reference's SUShift<3>, 2 sweeps.  Start: each link
+        // the identity moved by four wide SUShift steps drawn on the host.
+        CellModel<SUDof<3>, MySU3PlaquetteTerm, CellComplex<4>> su(hypercubic_plaquettes(4), MySU3PlaquetteTerm{5.7});
+        for (std::size_t i = 0; i < su.sites(); ++i) {
+            SULink<3> u = SULink<3>::identity(), w;
+            for (int k = 0; k < 4; ++k) {
+                SUShift<3>{1.0}.sample(&u, init, &w);
+                u = w;
+            }
+            su.update(i, &u);
+        }
+        const auto* s0p = reinterpret_cast<const double*>(su.data());
+        const std::vector<double> su0(s0p, s0p + 18 * su.sites());
+        {
+            Metropolis metro(su, SUShift<3>{0.3}, Pcg32(33, 0), 1.0);
+            metro.run(2);
+        }
+        const auto* s1p = reinterpret_cast<const double*>(su.data());
+        const std::vector<double> su1(s1p, s1p + 18 * su.sites());
+        double worst = 0.0;
+        for (std::size_t i = 0; i < su.sites(); ++i) {
+            const double e = su.data()[i].unitarity_error();
+            worst = e > worst ? e : worst;
+        }
+        std::printf("SU(3) user cell term: S = %.6f, unitarity error %.2e\n", su.total_energy(), worst);
+        put(out, su0.data(), su0.size());
+        put(out, su1.data(), su1.size());
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());
         std::fclose(out);

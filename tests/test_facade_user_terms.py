@@ -5,7 +5,9 @@ GPU it fails loudly; on the GPU its fields equal the oracle's:
 - XY angles, 5 sweeps, to 1e-9;
 - Ising under Wolff, spins and cluster sizes bit for bit, flips and a sweep;
 - U(1) plaquettes, 2 sweeps, to 1e-9;
-- O(3) with LocalRotation, 2 sweeps, to 1e-9.
+- O(3) with LocalRotation, 2 sweeps, to 1e-9;
+- SU(3) links with a plaquette term written against SULink and the
+  reference's SUShift (expm on the device), 2 sweeps, to 1e-9.
 The oracle runs on the colour-major device numbering with the same keys."""
 import os
 import shutil
@@ -109,9 +111,26 @@ def test_user_term_program_matches_the_oracle(program, umc, oracle, tmp_path):
     n = 512
     pos, doff, dbonds, key = device_csr(g)
     v0, v1 = take(np.float64, 3 * n).reshape(n, 3), take(np.float64, 3 * n).reshape(n, 3)
-    assert at == len(raw)
     cm = np.empty((n, 3))
     cm[pos] = v0
     v_o, _, margin = oracle.vector_metropolis(3, doff, dbonds, 1.0, 0.693, 1, 0.6, 21, 0, 2, cm)
     assert np.abs(v1 - v_o[pos]).max() < 1e-9
     assert abs(np.linalg.norm(v1, axis=1) - 1).max() < 1e-12
+
+    # SU(3) with the user's plaquette term (SULink interface) and the
+    # reference's SUShift(0.3), 2 sweeps at beta 5.7, keys 33: the oracle's
+    # restatement of SUShift and expm (dof/sun.hpp) on the same links
+    cc = umc.hypercubic_plaquettes(4)
+    n = cc.sites()
+    _, _, pos = cc.colouring()
+    rcells = pos[cc.table()]
+    inc = oracle.cell_incidence(n, rcells)[1:]
+    s0 = take(np.float64, 18 * n).view(np.complex128).reshape(n, 3, 3)
+    s1 = take(np.float64, 18 * n).view(np.complex128).reshape(n, 3, 3)
+    assert at == len(raw)
+    cm = np.empty((n, 3, 3), np.complex128)
+    cm[pos] = s0
+    l_o, _, margin = oracle.su_metropolis(3, rcells, inc, 5.7, 1.0, 0.3, 1, 33, 0, 2, cm)
+    moved = np.abs(s1 - s0).max(axis=(1, 2)) > 0
+    assert 0.2 < moved.mean() < 0.95  # a Metropolis chain, not a frozen or free one
+    assert np.abs(s1 - l_o[pos]).max() < 1e-9
