@@ -351,13 +351,16 @@ int umc_batch_sites(const umc_batch* b, uint64_t* total_sites, uint64_t* kernel_
  * 2 x 8192 sites per colour whose rows split into cluster-many bands of at
  * least 2 is swept by a whole cluster, smaller chains are packed into CTA
  * items of up to 8192 sites per colour -- and the CTA that completes a ladder
- * runs its exchange; its cluster size (4 or 8) and CTAs per SM (1 or 2) are
- * tuned.  Grouped (enable = 0): one kernel per lattice-size group (tuned
+ * runs its exchange; its cluster size (1, 4 or 8: with 1 a big chain is one
+ * CTA's item) and CTAs per SM (1 or 2) are tuned.  Grouped (enable = 0): one kernel per lattice-size group (tuned
  * launch shapes, umc_batch_config) plus an exchange kernel, as parallel
  * branches of the segment's graph.  At creation both forms are timed on the
  * batch itself (state restored) and the faster one is selected; the choice
  * is cached like the group shapes.  This call overrides it. */
 int umc_batch_set_persistent(umc_batch* b, int enable);
+/* Selects the persistent form with a given cluster size (1, 4 or 8) and CTAs
+ * per SM (1 or 2) instead of the tuned ones. */
+int umc_batch_set_persistent_config(umc_batch* b, uint32_t cluster, uint32_t ctas_per_sm);
 int umc_batch_persistent_info(const umc_batch* b, int* enabled, uint32_t* grid, uint32_t* big_items, uint32_t* items,
                               uint32_t* cluster, uint32_t* ctas_per_sm);
 /* The stream the batch's segments run on (cudaStream_t). */

@@ -201,34 +201,38 @@ def test_sharded_u1batch_equals_the_whole_batch(umc):
             c += 1
 
 
-def test_persistent_segment_equals_grouped_segments(umc):
-    """The one-kernel segment (resident clusters taking work items, a 256^2
-    chain swept by a cluster of CTAs, small chains packed, the exchanges run
-    by whichever CTA completes a ladder) and the per-group kernels run the
-    same chains and exchanges: fields bit for bit, temperature maps and
-    records equal (energies to FP64 summation order).  Creation selects the
-    form that measured faster; both are forced here."""
+@pytest.mark.parametrize("cluster,ctas_per_sm", [(1, 1), (1, 2), (4, 1), (4, 2), (8, 1), (8, 2)])
+def test_persistent_segment_equals_grouped_segments(umc, cluster, ctas_per_sm):
+    """The one-kernel segment (resident CTAs taking work items, a 256^2 chain
+    swept by one CTA or a cluster of CTAs, small chains packed, the exchanges
+    run by whichever CTA completes a ladder) and the per-group kernels run
+    the same chains and exchanges: fields bit for bit, temperature maps and
+    records equal (energies to FP64 summation order), and both advance the
+    counters by every segment.  Creation selects the form that measured
+    faster; every persistent variant is forced here."""
     Ls = np.array([256, 16, 64, 32, 256, 128, 16])
-    R = 4
+    R, S, n = 4, 4, 5
     betas = np.stack([_geometric(0.8, 1.3, R)] * len(Ls))
-    a = umc.Batch(Ls, betas, width=1.0, sweeps_per_exchange=4, seed=5)
-    b = umc.Batch(Ls, betas, width=1.0, sweeps_per_exchange=4, seed=5)
-    a.set_persistent(True)
+    a = umc.Batch(Ls, betas, width=1.0, sweeps_per_exchange=S, seed=5)
+    b = umc.Batch(Ls, betas, width=1.0, sweeps_per_exchange=S, seed=5)
+    a.set_persistent_config(cluster, ctas_per_sm)
     b.set_persistent(False)
     info = a.persistent_info()
-    assert info["enabled"] and info["grid"] % info["cluster"] == 0 and info["cluster"] in (4, 8)
-    assert info["big_items"] == 2 * R and info["ctas_per_sm"] in (1, 2)
+    assert info["enabled"] and info["grid"] % info["cluster"] == 0
+    assert (info["cluster"], info["ctas_per_sm"]) == (cluster, ctas_per_sm)
+    assert info["big_items"] == 2 * R
     assert not b.persistent_info()["enabled"]
     for x in (a, b):
         x.randomize(6)
-    ra, rb = a.run(5), b.run(5)
+    ra, rb = a.run(n), b.run(n)
+    assert a.counters()[:2] == (n * S, n)
     np.testing.assert_array_equal(ra[..., 3], rb[..., 3])
     np.testing.assert_allclose(ra, rb, rtol=1e-12, atol=1e-9)
     np.testing.assert_array_equal(a.temperature_map(), b.temperature_map())
     assert a.counters() == b.counters()
     for c in range(a.n_chains):
         np.testing.assert_array_equal(a.get_field(c), b.get_field(c))
-    assert a.sites()[1] == 5  # one kernel per segment
+    assert a.sites()[1] == n  # one kernel per segment
 
 
 def _check_wrapped(got, th):

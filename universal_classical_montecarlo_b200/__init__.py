@@ -194,6 +194,7 @@ class BatchDesc(C.Structure):
 
 _decl("umc_batch_create", _int, C.POINTER(BatchDesc), C.POINTER(_vp))
 _decl("umc_batch_set_persistent", _int, _vp, _int)
+_decl("umc_batch_set_persistent_config", _int, _vp, _u32, _u32)
 _decl("umc_batch_persistent_info", _int, _vp, C.POINTER(_int), C.POINTER(_u32), C.POINTER(_u32), C.POINTER(_u32),
       C.POINTER(_u32), C.POINTER(_u32))
 _decl("umc_batch_destroy", _int, _vp)
@@ -999,6 +1000,11 @@ class Batch:
         group plus an exchange kernel.  Creation selects the form that
         measured faster on this batch; this overrides it."""
         check(lib.umc_batch_set_persistent(self._h, int(enable)))
+
+    def set_persistent_config(self, cluster: int, ctas_per_sm: int) -> None:
+        """The persistent form with this cluster size (1, 4, 8) and CTAs per
+        SM (1, 2) instead of the tuned ones."""
+        check(lib.umc_batch_set_persistent_config(self._h, cluster, ctas_per_sm))
 
     def persistent_info(self):
         e, g, nb, ni, kc, mb = _int(0), _u32(0), _u32(0), _u32(0), _u32(0), _u32(0)

@@ -375,9 +375,10 @@ __global__ void __launch_bounds__(kSwapWarps * 32) xy_batch_swap(BatchCounters* 
 
 // ---------------------------------------------------- one persistent kernel
 // The whole segment -- every chain's sweeps and every ladder's exchange -- in
-// one launch of resident CTAs grouped in clusters of KC (4 or 8).  Work
+// one launch of resident CTAs grouped in clusters of KC (1, 4 or 8).  Work
 // items, largest first: a "big" chain is swept by a whole cluster (one row
-// band per CTA, the cluster barrier between colour passes); smaller chains are
+// band per CTA, the cluster barrier between colour passes; with KC = 1 by one
+// CTA, as the grouped form sweeps it); smaller chains are
 // packed into CTA items of up to kPersistSites sites per colour.  CTAs take
 // items from two atomic counters (big, then small), so the long items start
 // first and the short ones fill the gaps.  The CTA that completes the last
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(kSwapWarps * 32) xy_batch_swap(BatchCounters* 
 // advances the counters.  No CTA ever waits for another: the scheduler is
 // atomics only, and the cluster barrier joins CTAs that are co-scheduled.
 // cluster sizes the autotuner chooses between (a big chain's bands)
-constexpr uint32_t kPersistClusters[2] = {4, 8};
+constexpr uint32_t kPersistClusters[3] = {1, 4, 8};
 constexpr uint32_t kPersistSites = 8192;   // sites per colour of a CTA item
 constexpr uint32_t kPersistBlock = 1024;
 
@@ -454,7 +455,8 @@ __global__ void __launch_bounds__(kPersistBlock, MINB) xy_batch_persistent(Persi
         a.H = w.z / 2;
         a.half = w.z * w.z / 2;
         const uint32_t rows = w.z / KC, share = cl.block_rank();
-        run_share<true>(a, sh, p.chains + w.x, 1, share * rows, rows, share);
+        if constexpr (KC == 1) run_share<false>(a, sh, p.chains + w.x, 1, 0, rows, 0);  // the whole chain
+        else run_share<true>(a, sh, p.chains + w.x, 1, share * rows, rows, share);
         complete_item(p, p.chains + w.x, 1, KC, E);
     }
     // packed smaller chains, one CTA each
@@ -609,30 +611,42 @@ SegArgs seg_args(umc_batch* b, umc_batch::Group& g, float* theta)
     return a;
 }
 
-void launch_segment(umc_batch* b, umc_batch::Group& g, const GroupCfg& cfg, float* theta, cudaStream_t st)
+// priority: a launch priority for the segment graph's kernel node (0: the
+// stream's own).  Larger sides get higher priority, so the longest chains
+// take SMs first and the short groups fill the rest.
+void launch_segment(umc_batch* b, umc_batch::Group& g, const GroupCfg& cfg, float* theta, cudaStream_t st,
+                    int priority = 0)
 {
     SegArgs a = seg_args(b, g, theta);
     a.cpc = cfg.cpc;
     a.cpk = cfg.cpk;
     const uint32_t nc = uint32_t(g.chains.size());
+    cudaLaunchConfig_t lc{};
+    lc.blockDim = dim3(cfg.block);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = st;
+    cudaLaunchAttribute attr[2];
+    unsigned n_attr = 0;
+    if (priority != 0) {
+        attr[n_attr].id = cudaLaunchAttributePriority;
+        attr[n_attr].val.priority = priority;
+        ++n_attr;
+    }
     if (cfg.cpk > 1) {
-        cudaLaunchConfig_t lc{};
         lc.gridDim = dim3(nc * cfg.cpk);
-        lc.blockDim = dim3(cfg.block);
-        lc.dynamicSmemBytes = 0;
-        lc.stream = st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = cfg.cpk;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
+        attr[n_attr].id = cudaLaunchAttributeClusterDimension;
+        attr[n_attr].val.clusterDim.x = cfg.cpk;
+        attr[n_attr].val.clusterDim.y = 1;
+        attr[n_attr].val.clusterDim.z = 1;
+        ++n_attr;
         lc.attrs = attr;
-        lc.numAttrs = 1;
+        lc.numAttrs = n_attr;
         cuda_check(cudaLaunchKernelEx(&lc, xy_batch_segment<true>, a), "batch segment (cluster)");
     } else {
-        const uint32_t grid = (nc + cfg.cpc - 1) / cfg.cpc;
-        xy_batch_segment<false><<<grid, cfg.block, 0, st>>>(a);
-        cuda_check(cudaGetLastError(), "batch segment");
+        lc.gridDim = dim3((nc + cfg.cpc - 1) / cfg.cpc);
+        lc.attrs = attr;
+        lc.numAttrs = n_attr;
+        cuda_check(cudaLaunchKernelEx(&lc, xy_batch_segment<false>, a), "batch segment");
     }
     b->launches++;
 }
@@ -761,11 +775,14 @@ void build_persistent(umc_batch* b, uint32_t kc)
     b->p_grid = 0;
 }
 
-// The four kernel variants by (cluster size, CTAs per SM).
+// The six kernel variants by (cluster size, CTAs per SM).
 const void* persistent_kernel(uint32_t kc, uint32_t minb)
 {
     if (kc == 8) return minb == 2 ? reinterpret_cast<const void*>(&xy_batch_persistent<8, 2>)
                                   : reinterpret_cast<const void*>(&xy_batch_persistent<8, 1>);
+    if (kc == 1) return minb == 2 ? reinterpret_cast<const void*>(&xy_batch_persistent<1, 2>)
+                                  : reinterpret_cast<const void*>(&xy_batch_persistent<1, 1>);
+    if (kc != 4) throw Error(UMC_ERR_UNSUPPORTED, "persistent batch: cluster size must be 1, 4 or 8");
     return minb == 2 ? reinterpret_cast<const void*>(&xy_batch_persistent<4, 2>)
                      : reinterpret_cast<const void*>(&xy_batch_persistent<4, 1>);
 }
@@ -826,10 +843,9 @@ void launch_persistent(umc_batch* b, cudaStream_t st)
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t lc = persistent_config(b->p_kc, b->p_grid, st, attr);
     cudaError_t e;
-    if (b->p_kc == 8) e = b->p_minb == 2 ? cudaLaunchKernelEx(&lc, xy_batch_persistent<8, 2>, p)
-                                         : cudaLaunchKernelEx(&lc, xy_batch_persistent<8, 1>, p);
-    else e = b->p_minb == 2 ? cudaLaunchKernelEx(&lc, xy_batch_persistent<4, 2>, p)
-                            : cudaLaunchKernelEx(&lc, xy_batch_persistent<4, 1>, p);
+    // the kernel variant from the one table that also sizes the grid
+    void* args[] = {&p};
+    e = cudaLaunchKernelExC(&lc, persistent_kernel(b->p_kc, b->p_minb), args);
     cuda_check(e, "persistent batch segment");
 }
 
@@ -883,8 +899,8 @@ void autotune_persistent(umc_batch* b)
     cuda_check(cudaEventCreate(&e1), "event");
     uint32_t best = kPersistClusters[0], best_minb = 1;
     float best_ms = 1e30f;
-    for (uint32_t cand = 0; cand < 4; ++cand) {
-        const uint32_t kc = kPersistClusters[cand & 1u], minb = 1 + (cand >> 1);
+    for (uint32_t cand = 0; cand < 6; ++cand) {
+        const uint32_t kc = kPersistClusters[cand % 3u], minb = 1 + cand / 3u;
         build_persistent(b, kc);
         b->p_minb = minb;
         launch_persistent(b, b->stream);  // warm
@@ -945,9 +961,15 @@ void build_graph(umc_batch* b)
     }
     cuda_check(cudaEventRecord(b->fork, b->stream), "fork");
     const uint64_t launches = b->launches;  // captured, not launched: replays are counted
+    int least = 0, greatest = 0;
+    cuda_check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "priority range");
     for (auto& g : b->groups) {
+        // rank of this group's side among the groups, largest first
+        int rank = 0;
+        for (const auto& o : b->groups) rank += o.L > g.L ? 1 : 0;
+        const int prio = std::min(least, greatest + rank);
         cuda_check(cudaStreamWaitEvent(g.stream, b->fork, 0), "fork wait");
-        launch_segment(b, g, g.cfg, b->theta.as<float>(), g.stream);
+        launch_segment(b, g, g.cfg, b->theta.as<float>(), g.stream, prio == least ? 0 : prio);
         cuda_check(cudaEventRecord(g.done, g.stream), "join");
         cuda_check(cudaStreamWaitEvent(b->stream, g.done, 0), "join wait");
     }
@@ -959,7 +981,7 @@ void build_graph(umc_batch* b)
     cuda_check(cudaGetLastError(), "swap kernel");
     b->launches = launches;
     cuda_check(cudaStreamEndCapture(b->stream, &graph), "end capture");
-    cuda_check(cudaGraphInstantiate(&b->graph, graph, 0), "instantiate graph");
+    cuda_check(cudaGraphInstantiate(&b->graph, graph, cudaGraphInstantiateFlagUseNodePriority), "instantiate graph");
     cudaGraphDestroy(graph);
 }
 
@@ -1344,6 +1366,22 @@ int umc_batch_set_persistent(umc_batch* b, int enable)
         batch_scope(b);
         cuda_check(cudaStreamSynchronize(b->stream), "sync");
         b->persistent = enable != 0;
+        build_graph(b);
+    });
+}
+
+int umc_batch_set_persistent_config(umc_batch* b, uint32_t cluster, uint32_t ctas_per_sm)
+{
+    return bguard([&] {
+        if (!b) throw Error(UMC_ERR_INVALID_ARGUMENT, "null batch");
+        if (cluster != 1 && cluster != 4 && cluster != 8)
+            throw Error(UMC_ERR_INVALID_ARGUMENT, "cluster size must be 1, 4 or 8");
+        if (ctas_per_sm != 1 && ctas_per_sm != 2) throw Error(UMC_ERR_INVALID_ARGUMENT, "CTAs per SM must be 1 or 2");
+        batch_scope(b);
+        cuda_check(cudaStreamSynchronize(b->stream), "sync");
+        build_persistent(b, cluster);
+        b->p_minb = ctas_per_sm;
+        b->persistent = true;
         build_graph(b);
     });
 }
