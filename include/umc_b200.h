@@ -407,6 +407,54 @@ int umc_slab_pass(umc_slab* s, void* field, double beta, uint64_t sweep, uint32_
  * to the single-GPU record.  Synchronises `stream`. */
 int umc_slab_record(umc_slab* s, double* out, void* stream);
 
+/* Gauge slabs: the U(1) and SU(N) link sweeps of a plaquette complex split
+ * over ranks (no reference counterpart, as above; the motivating case is an
+ * SU(3) lattice beyond one GPU).  The caller assigns every link to a rank
+ * (`owner`, in the reference's link numbering; for hypercubic_plaquettes a
+ * range of the slowest coordinate t per rank).  A rank keeps its owned links
+ * and the halo links that its owned links' plaquettes touch, in a
+ * caller-owned device array of comps planes x umc_gslab_info's n_local floats
+ * (comps = 1 for U(1) angles, 2N^2 for SU(N): plane q holds scalar q of every
+ * local link, the reference's data() scalars).  Local links are ordered as
+ * the single-GPU chain orders them (colour classes, then the halo); each link
+ * draws from the key of its global colour-major index and sums its
+ * plaquettes in the single-GPU order, so the ranks together run exactly the
+ * single-GPU chain.  A sweep: for each colour class c, umc_gslab_pass, then
+ * for every peer p the links of class c to send (umc_gslab_pack) and to
+ * receive (umc_gslab_unpack); after the last class umc_gslab_record. */
+typedef struct umc_gslab_desc {
+    int32_t model;            /* UMC_MODEL_U1 or UMC_MODEL_SU                    */
+    int32_t N;                /* SU(N): 2 or 3 (ignored for U(1))                 */
+    const umc_cells* cells;   /* the whole lattice's plaquettes (arity 4)         */
+    const uint32_t* owner;    /* owner rank of each link, n_sites entries         */
+    uint32_t rank, world;
+    double coupling;          /* the model's beta                                 */
+    double width;             /* U1Shift / SUShift width                          */
+    uint32_t hits;            /* Metropolis hits per link and sweep (>= 1)        */
+    uint64_t seed;            /* the chain's key seed (the same on every rank)    */
+    int32_t device;
+} umc_gslab_desc;
+typedef struct umc_gslab umc_gslab;
+int umc_gslab_create(const umc_gslab_desc* desc, umc_gslab** out);
+int umc_gslab_destroy(umc_gslab* s);
+/* Local links (owned first), owned links, colour classes, floats per link. */
+int umc_gslab_info(const umc_gslab* s, uint32_t* n_local, uint32_t* n_owned, uint32_t* n_classes, uint32_t* comps);
+/* The reference link id of every local link (n_local entries). */
+int umc_gslab_local_links(const umc_gslab* s, uint32_t* ref_ids);
+/* How many links of class `colour` go to `peer` and come from it. */
+int umc_gslab_exchange_counts(const umc_gslab* s, uint32_t peer, uint32_t colour, uint32_t* n_send,
+                              uint32_t* n_recv);
+/* Copies the class-`colour` links that `peer` holds as halo into buf (comps x
+ * n_send floats, device), or the ones it owns from buf into this rank's halo. */
+int umc_gslab_pack(umc_gslab* s, const float* field, uint32_t peer, uint32_t colour, float* buf, void* stream);
+int umc_gslab_unpack(umc_gslab* s, float* field, uint32_t peer, uint32_t colour, const float* buf, void* stream);
+/* Colour class `colour` of sweep `sweep` over the owned links. */
+int umc_gslab_pass(umc_gslab* s, float* field, double beta, uint64_t sweep, uint32_t colour, void* stream);
+/* Ends the sweep: the plaquettes whose first link this rank owns (all their
+ * links are local) into this rank's part of the record [S, <P>, Q, 0..,
+ * accepted]; the parts add up to the single-GPU record.  Synchronises. */
+int umc_gslab_record(umc_gslab* s, const float* field, double* out, void* stream);
+
 /* ================================================= allocation-free Wolff flip */
 
 /* No counterpart in the reference: an extra entry point for callers that cannot

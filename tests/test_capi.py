@@ -249,3 +249,38 @@ def test_slab_descriptions_are_checked(umc):
     assert create(model=umc.MODEL_U1) == umc.ERR_UNSUPPORTED
     assert create(model=umc.MODEL_VECTOR, components=3, proposal=umc.PROPOSAL_FLIP) == umc.ERR_UNSUPPORTED
     assert create(model=umc.MODEL_VECTOR, components=5, proposal=umc.PROPOSAL_SPHERE) == umc.ERR_UNSUPPORTED
+
+
+def test_gauge_slab_descriptions_are_checked(umc):
+    """umc_gslab_create refuses what the decomposition cannot run, before any
+    device work: missing tables or owners, a rank outside the world, no hits,
+    non-finite couplings, other models and SU(N) beyond N = 3; and the
+    slowest-axis owner split gives every rank a contiguous range."""
+    cc = umc.hypercubic_plaquettes(2)
+    owner = umc.slowest_axis_owner(cc, 2)
+    assert np.bincount(owner).tolist() == [32, 32]
+    t = (np.arange(cc.sites()) % 16) // 8
+    np.testing.assert_array_equal(owner, t)
+
+    def create(**kw):
+        d = umc.GaugeSlabDesc()
+        d.model, d.N, d.cells, d.owner = umc.MODEL_SU, 3, cc._h, owner.ctypes.data_as(umc._vp)
+        d.rank, d.world, d.coupling, d.width, d.hits, d.seed = 0, 2, 5.7, 0.3, 1, 1
+        for k, v in kw.items():
+            setattr(d, k, v)
+        h = umc._vp()
+        rc = umc.lib.umc_gslab_create(ctypes.byref(d), ctypes.byref(h))
+        if rc == umc.OK:
+            umc.lib.umc_gslab_destroy(h)
+        return rc
+
+    assert create(cells=None) == umc.ERR_INVALID_ARGUMENT
+    assert create(owner=None) == umc.ERR_INVALID_ARGUMENT
+    assert create(rank=2) == umc.ERR_INVALID_ARGUMENT
+    assert create(world=0, rank=0) == umc.ERR_INVALID_ARGUMENT
+    assert create(hits=0) == umc.ERR_INVALID_ARGUMENT
+    assert create(coupling=float("nan")) == umc.ERR_INVALID_ARGUMENT
+    assert create(N=4) == umc.ERR_UNSUPPORTED
+    assert create(model=umc.MODEL_ISING) == umc.ERR_UNSUPPORTED
+    with pytest.raises(ValueError):
+        umc.slowest_axis_owner(umc.CellComplex(5, [[0, 1, 2, 3]]), 2)

@@ -868,6 +868,189 @@ class SlabChain:
         return np.stack([self.sweep(beta) for _ in range(n)])
 
 
+class GaugeSlabDesc(C.Structure):
+    _fields_ = [
+        ("model", _i32),
+        ("N", _i32),
+        ("cells", _vp),
+        ("owner", _vp),
+        ("rank", _u32),
+        ("world", _u32),
+        ("coupling", _f64),
+        ("width", _f64),
+        ("hits", _u32),
+        ("seed", _u64),
+        ("device", _i32),
+    ]
+
+
+_decl("umc_gslab_create", _int, C.POINTER(GaugeSlabDesc), C.POINTER(_vp))
+_decl("umc_gslab_destroy", _int, _vp)
+_decl("umc_gslab_info", _int, _vp, C.POINTER(_u32), C.POINTER(_u32), C.POINTER(_u32), C.POINTER(_u32))
+_decl("umc_gslab_local_links", _int, _vp, _vp)
+_decl("umc_gslab_exchange_counts", _int, _vp, _u32, _u32, C.POINTER(_u32), C.POINTER(_u32))
+_decl("umc_gslab_pack", _int, _vp, _vp, _u32, _u32, _vp, _vp)
+_decl("umc_gslab_unpack", _int, _vp, _vp, _u32, _u32, _vp, _vp)
+_decl("umc_gslab_pass", _int, _vp, _vp, _f64, _u64, _u32, _vp)
+_decl("umc_gslab_record", _int, _vp, _vp, _vp, _vp)
+
+
+def slowest_axis_owner(cells, rank_count):
+    """Link -> rank for hypercubic_plaquettes(L) (4D: link mu*L^4 + site,
+    site = ((t L + z) L + y) L + x) or square_plaquettes(L) (2D: mu*L^2 + y L +
+    x): ranks take contiguous ranges of the slowest coordinate (t, or y in 2D),
+    sizes differing by at most one (shard_range)."""
+    n = cells.sites()
+    if n % 4 == 0 and round((n // 4) ** 0.25) ** 4 == n // 4:
+        L = round((n // 4) ** 0.25)
+        slow = (np.arange(n) % L**4) // L**3
+    else:
+        L = round((n // 2) ** 0.5)
+        if 2 * L * L != n:
+            raise ValueError("not a hypercubic or square plaquette complex")
+        slow = (np.arange(n) % (L * L)) // L
+    owner = np.zeros(n, np.uint32)
+    for r in range(rank_count):
+        lo, hi = shard_range(L, r, rank_count)
+        owner[(slow >= lo) & (slow < hi)] = r
+    return owner
+
+
+class GaugeSlab:
+    """One U(1) or SU(N) gauge chain split over the ranks of a
+    torch.distributed group (umc_gslab_*), one process per GPU.  `owner`
+    assigns every link (reference numbering) to a rank (slowest_axis_owner
+    cuts the slowest coordinate).  This rank's owned links and the halo links
+    their plaquettes touch live in a torch tensor on its GPU (comps planes x
+    n_local); after each colour class the links just updated go to the ranks
+    that hold them as halo (batch_isend_irecv: NCCL device to device, gloo
+    through host copies).  The ranks together run exactly the single-GPU
+    Chain of the same seed; records are summed over the ranks."""
+
+    def __init__(self, model, cells, owner, *, rank=0, world=1, group=None, N=3, coupling=1.0, width=0.3, hits=1,
+                 seed=1, device=0):
+        import torch
+
+        self.torch = torch
+        self.rank, self.world, self.group = rank, world, group
+        self.cells = cells
+        owner = np.ascontiguousarray(owner, np.uint32)
+        if owner.shape != (cells.sites(),):
+            raise ValueError("owner needs one rank per link")
+        d = GaugeSlabDesc()
+        d.model, d.N, d.cells, d.owner = model, N, cells._h, owner.ctypes.data_as(_vp)
+        d.rank, d.world, d.coupling, d.width, d.hits, d.seed, d.device = rank, world, coupling, width, hits, seed, device
+        h = _vp()
+        check(lib.umc_gslab_create(C.byref(d), C.byref(h)))
+        self._h = h
+        nl, no, nc, cp = _u32(0), _u32(0), _u32(0), _u32(0)
+        check(lib.umc_gslab_info(h, C.byref(nl), C.byref(no), C.byref(nc), C.byref(cp)))
+        self.n_local, self.n_owned, self.n_classes, self.comps = nl.value, no.value, nc.value, cp.value
+        self.local_ref = np.zeros(self.n_local, np.uint32)
+        check(lib.umc_gslab_local_links(h, _ptr(self.local_ref)))
+        self.device = torch.device("cuda", device)
+        self.field = torch.zeros(self.comps * self.n_local, dtype=torch.float32, device=self.device)
+        self.stream = torch.cuda.current_stream(self.device)
+        self.sweeps = 0
+        # (peer, class) -> (links to send, links to receive)
+        self.counts = {}
+        for p in range(world):
+            if p == rank:
+                continue
+            for c in range(self.n_classes):
+                ns, nr = _u32(0), _u32(0)
+                check(lib.umc_gslab_exchange_counts(h, p, c, C.byref(ns), C.byref(nr)))
+                if ns.value or nr.value:
+                    self.counts[(p, c)] = (ns.value, nr.value)
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h and lib is not None:
+            lib.umc_gslab_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_field(self, full):
+        """full: every link's scalars in the reference's layout, (links, comps);
+        every rank passes the same array."""
+        a = np.asarray(full, np.float32).reshape(-1, self.comps)
+        soa = np.ascontiguousarray(a[self.local_ref].T).reshape(-1)
+        self.field.copy_(self.torch.from_numpy(soa).to(self.device))
+
+    def get_owned(self):
+        """(reference ids, scalars) of this rank's owned links."""
+        loc = self.field.cpu().numpy().reshape(self.comps, self.n_local).T
+        return self.local_ref[: self.n_owned].copy(), loc[: self.n_owned].copy()
+
+    def gather_field(self):
+        """Every link's scalars (links, comps), on every rank."""
+        parts = [self.get_owned()]
+        if self.world > 1:
+            import torch.distributed as dist
+
+            parts = [None] * self.world
+            dist.all_gather_object(parts, self.get_owned(), group=self.group)
+        out = np.zeros((self.cells.sites(), self.comps), np.float32)
+        for ids, vals in parts:
+            out[ids] = vals
+        return out
+
+    def _exchange(self, colour):
+        if self.world == 1:
+            return
+        import torch.distributed as dist
+
+        cpu = dist.get_backend(self.group) == "gloo"
+        s = self.stream.cuda_stream
+        f = C.c_void_p(self.field.data_ptr())
+        ops, recvs = [], []
+        for p in range(self.world):
+            ns, nr = self.counts.get((p, colour), (0, 0))
+            if ns:
+                buf = self.torch.empty(self.comps * ns, dtype=self.torch.float32, device=self.device)
+                check(lib.umc_gslab_pack(self._h, f, p, colour, C.c_void_p(buf.data_ptr()), s))
+                self.stream.synchronize()
+                ops.append(dist.P2POp(dist.isend, buf.cpu() if cpu else buf, p, self.group, colour))
+            if nr:
+                buf = self.torch.empty(self.comps * nr, dtype=self.torch.float32, device="cpu" if cpu else self.device)
+                ops.append(dist.P2POp(dist.irecv, buf, p, self.group, colour))
+                recvs.append((p, buf))
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+        for p, buf in recvs:
+            b = buf.to(self.device)
+            check(lib.umc_gslab_unpack(self._h, f, p, colour, C.c_void_p(b.data_ptr()), s))
+        self.stream.synchronize()
+
+    def sweep(self, beta):
+        """One sweep of every colour class; its record summed over the ranks
+        ([S, <P>, Q, 0.., accepted])."""
+        s = self.stream.cuda_stream
+        f = C.c_void_p(self.field.data_ptr())
+        for c in range(self.n_classes):
+            check(lib.umc_gslab_pass(self._h, f, beta, self.sweeps, c, s))
+            self._exchange(c)
+        rec = np.zeros(OBS_STRIDE)
+        check(lib.umc_gslab_record(self._h, f, _ptr(rec), s))
+        self.sweeps += 1
+        if self.world > 1:
+            import torch.distributed as dist
+
+            t = self.torch.from_numpy(rec.copy())
+            if dist.get_backend(self.group) != "gloo":
+                t = t.to(self.device)
+            dist.all_reduce(t, group=self.group)
+            rec = t.cpu().numpy()
+        return rec
+
+    def metropolis(self, beta, n):
+        """n sweeps; their records (n x OBS_STRIDE)."""
+        return np.stack([self.sweep(beta) for _ in range(n)])
+
+
 class Batch:
     """Independent XY chains in replica-exchange ladders (umc_batch_*).
 

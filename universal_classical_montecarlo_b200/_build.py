@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++20", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", f"-I{INCLUDE}"]
 CXX_FLAGS = ["-std=c++23", "-O2", "-fPIC", "-Wall", "-Wextra", f"-I{INCLUDE}", f"-I{CUDA_HOME}/include"]
 
-CU_SOURCES = ["umc_chain.cu", "umc_gauge.cu", "umc_batch.cu", "umc_learn.cu", "umc_noalloc.cu", "umc_slab.cu"]
+CU_SOURCES = ["umc_chain.cu", "umc_gauge.cu", "umc_batch.cu", "umc_learn.cu", "umc_noalloc.cu", "umc_slab.cu", "umc_gslab.cu"]
 CXX_SOURCES = ["umc_tables.cpp", "umc_stats.cpp"]
 
 

@@ -140,9 +140,9 @@ void plaquettes(umc_chain* c, double* record, int pass, int n_passes)
     LaunchScope ls(c, UMC_KERNEL_OBSERVE);
     const uint4* cells = c->cells.as<uint4>();
     switch (c->N) {
-    case 1: plaquette_sum<1><<<g, kBlock, 0, c->stream>>>(c->field.as<float>(), uint32_t(c->n), cells, uint32_t(c->n_cells), c->J, o); break;
-    case 2: plaquette_sum<2><<<g, kBlock, 0, c->stream>>>(c->field.as<float>(), uint32_t(c->n), cells, uint32_t(c->n_cells), c->J, o); break;
-    default: plaquette_sum<3><<<g, kBlock, 0, c->stream>>>(c->field.as<float>(), uint32_t(c->n), cells, uint32_t(c->n_cells), c->J, o); break;
+    case 1: plaquette_sum<1><<<g, kBlock, 0, c->stream>>>(c->field.as<float>(), uint32_t(c->n), cells, uint32_t(c->n_cells), c->n_cells, c->J, o); break;
+    case 2: plaquette_sum<2><<<g, kBlock, 0, c->stream>>>(c->field.as<float>(), uint32_t(c->n), cells, uint32_t(c->n_cells), c->n_cells, c->J, o); break;
+    default: plaquette_sum<3><<<g, kBlock, 0, c->stream>>>(c->field.as<float>(), uint32_t(c->n), cells, uint32_t(c->n_cells), c->n_cells, c->J, o); break;
     }
     gcheck("plaquette reduction");
 }

@@ -418,6 +418,7 @@ struct GaugeArgs
     PassOut out;
     double model_beta64, driver_beta64;  // the couplings of the FP64 decisions
     float err;                           // u1_metropolis_err / su_metropolis_err
+    const uint32_t* gid;                 // key id of each link (null: its index), for a slab's local links
 };
 
 // Key base of hit h of this sweep (the same for every link): the first
@@ -441,7 +442,7 @@ __device__ __forceinline__ uint64_t hit_key(const uint64_t* keys, const GaugeArg
 // theta0 + theta1 - theta2 - theta3 (dof/u1.hpp:18-21) is +-(theta_k + phi)
 // with phi the sum of the cell's other three links.  Out of line and on plain
 // pointers: it runs only for decisions the FP32 test cannot call.
-__device__ __noinline__ double u1_delta64(const float* f, const uint32_t* inc_off, const uint32_t* inc,
+static __device__ __noinline__ double u1_delta64(const float* f, const uint32_t* inc_off, const uint32_t* inc,
                                           const uint4* cells, uint32_t k, float t, float p, double model_beta)
 {
     double d = 0.0;
@@ -470,6 +471,7 @@ static __global__ void __launch_bounds__(kBlock, 5) u1_pass(GaugeArgs a)
     double acc[kObs] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < a.count; q += gridDim.x * blockDim.x) {
         const uint32_t k = a.first + q;
+        const uint32_t kid = a.gid ? a.gid[k] : k;
         float Sr = 0.f, Si = 0.f;
         for (uint32_t e = a.inc_off[k]; e < a.inc_off[k + 1]; ++e) {
             const uint32_t w = a.inc[e];
@@ -492,7 +494,7 @@ static __global__ void __launch_bounds__(kBlock, 5) u1_pass(GaugeArgs a)
         sincosf(th, &so, &co);
         uint32_t accepted = 0;
         for (uint32_t h = 0; h < a.hits; ++h) {
-            KeyedPcg g = KeyedPcg::open(hit_key(keys, a, h), k);
+            KeyedPcg g = KeyedPcg::open(hit_key(keys, a, h), kid);
             const float p = u1_shift(g, a.width, th);
             float sp, cp;
             sincosf(p, &sp, &cp);
@@ -537,6 +539,7 @@ __global__ void __launch_bounds__(kBlock, 3) su_pass(GaugeArgs a)
     double acc[kObs] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < a.count; q += gridDim.x * blockDim.x) {
         const uint32_t k = a.first + q;
+        const uint32_t kid = a.gid ? a.gid[k] : k;
         Mat<N> A, B, T, u0, u1;
         mat_zero(A);
         for (uint32_t e = a.inc_off[k]; e < a.inc_off[k + 1]; ++e) {
@@ -581,7 +584,7 @@ __global__ void __launch_bounds__(kBlock, 3) su_pass(GaugeArgs a)
         uint32_t accepted = 0;
         const float coef = a.model_beta / float(N);
         for (uint32_t h = 0; h < a.hits; ++h) {
-            KeyedPcg g = KeyedPcg::open(hit_key(keys, a, h), k);
+            KeyedPcg g = KeyedPcg::open(hit_key(keys, a, h), kid);
             su_shift<N>(g, a.width, U, V);
             const float tr_new = re_tr_mul<N>(V, A);
             const float dE = coef * (tr_old - tr_new);
@@ -605,12 +608,15 @@ __global__ void __launch_bounds__(kBlock, 3) su_pass(GaugeArgs a)
 // Per cell: ReTr(U0 U1 U2^dag U3^dag)/N (dof/sun.hpp:78-84) or cos(theta_p)
 // (dof/u1.hpp:18-21), reduced in FP64 into [S, <P>, Q].  Q (the 2D U(1)
 // topological charge) sums remainder(theta_p, 2 pi) / 2 pi.
+// n_cells cells summed; <P> normalised by n_norm (a slab sums its share of
+// the lattice's cells).
 template <int N>
 __global__ void __launch_bounds__(kBlock) plaquette_sum(const float* f, uint32_t n, const uint4* cells,
-                                                        uint32_t n_cells, float model_beta, PassOut out)
+                                                        uint32_t n_cells, uint64_t n_norm, float model_beta,
+                                                        PassOut out)
 {
     double acc[kObs] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const double inv_cells = 1.0 / double(n_cells);
+    const double inv_cells = 1.0 / double(n_norm);
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cells; c += gridDim.x * blockDim.x) {
         const uint4 q = cells[c];
         double P, theta_p = 0.0;
