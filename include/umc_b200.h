@@ -381,7 +381,7 @@ void* umc_batch_stream(const umc_batch* b);
  * `planes` are the ones they need).  Sites draw from the keys of their global
  * colour-major index and sum neighbours in the single-GPU kernels' order, so
  * the ranks together run exactly the single-GPU chain (Ising bit for bit).
- * Wolff across slabs (a cross-rank union-find) is not provided. */
+ * Wolff flips across slabs: umc_slab_wolff_* below. */
 typedef struct umc_slab_desc {
     int32_t model;        /* UMC_MODEL_ISING (Flip) or UMC_MODEL_VECTOR       */
     int32_t components;   /* VectorSpin<N>: 1..4                              */
@@ -406,6 +406,31 @@ int umc_slab_pass(umc_slab* s, void* field, double beta, uint64_t sweep, uint32_
  * colour-1 end it owns), M_0..M_{N-1}, 0.., accepted]; the ranks' parts add up
  * to the single-GPU record.  Synchronises `stream`. */
 int umc_slab_record(umc_slab* s, double* out, void* stream);
+/* Wolff flip `flip` across slabs (the single-GPU flip of the same counter:
+ * the same seed, axis, bond keys and reflection).  1. umc_slab_wolff_local:
+ * decides every forward bond of the owned sites (the halos must be current)
+ * and labels the slab's clusters; 2. umc_slab_wolff_boundary: the root (a
+ * global natural site id) of every site of the first and last owned planes,
+ * and which last-plane sites have an activated bond into the next plane (the
+ * next rank's first); 3. umc_slab_wolff_seed: the seed site and, on the rank
+ * that owns it, its root (else 0xFFFFFFFF); 4. every rank gathers all ranks'
+ * boundaries (world x plane sites each, rank order) and the seed root, and
+ * umc_slab_wolff_merge picks this rank's roots in the seed's cluster (at most
+ * 2 x plane sites + 1); 5. umc_slab_wolff_flip reflects those clusters and
+ * counts this rank's flipped sites (the ranks' counts add up to the cluster
+ * size).  Then refresh the halos. */
+int umc_slab_wolff_local(umc_slab* s, void* field, double beta, uint64_t flip, void* stream);
+int umc_slab_wolff_boundary(umc_slab* s, uint32_t* first_roots, uint32_t* last_roots, uint8_t* last_up,
+                            void* stream);
+int umc_slab_wolff_seed(umc_slab* s, uint64_t flip, uint32_t* seed_nat, uint32_t* seed_root, void* stream);
+/* Host only.  first_roots, last_roots, last_up: world x plane_sites, rank r's
+ * at [r * plane_sites]; rank_roots_first/last and rank_seed_root: this
+ * rank's own (the seed root 0xFFFFFFFF where it does not own the seed). */
+int umc_slab_wolff_merge(uint32_t world, uint32_t plane_sites, const uint32_t* first_roots, const uint32_t* last_roots,
+                         const uint8_t* last_up, uint32_t seed_root, uint32_t rank, const uint32_t* rank_roots_first,
+                         const uint32_t* rank_roots_last, uint32_t rank_seed_root, uint32_t* roots, uint32_t* n_roots);
+int umc_slab_wolff_flip(umc_slab* s, void* field, uint64_t flip, const uint32_t* roots, uint32_t n_roots,
+                        uint64_t* flipped, void* stream);
 
 /* Gauge slabs: the U(1) and SU(N) link sweeps of a plaquette complex split
  * over ranks (no reference counterpart, as above; the motivating case is an

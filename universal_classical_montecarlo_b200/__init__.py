@@ -733,6 +733,11 @@ _decl("umc_slab_destroy", _int, _vp)
 _decl("umc_slab_local_sites", _u64, _vp)
 _decl("umc_slab_pass", _int, _vp, _vp, _f64, _u64, _u32, _vp)
 _decl("umc_slab_record", _int, _vp, _vp, _vp)
+_decl("umc_slab_wolff_local", _int, _vp, _vp, _f64, _u64, _vp)
+_decl("umc_slab_wolff_boundary", _int, _vp, _vp, _vp, _vp, _vp)
+_decl("umc_slab_wolff_seed", _int, _vp, _u64, C.POINTER(_u32), C.POINTER(_u32), _vp)
+_decl("umc_slab_wolff_merge", _int, _u32, _u32, _vp, _vp, _vp, _u32, _u32, _vp, _vp, _u32, _vp, C.POINTER(_u32))
+_decl("umc_slab_wolff_flip", _int, _vp, _vp, _u64, _vp, _u32, C.POINTER(_u64), _vp)
 
 
 class SlabChain:
@@ -776,6 +781,7 @@ class SlabChain:
         self.field = torch.zeros(self.N * self.nloc, dtype=dt, device=self.device)
         self.stream = torch.cuda.current_stream(self.device)
         self.sweeps = 0
+        self.flips = 0
 
     def close(self):
         h = getattr(self, "_h", None)
@@ -866,6 +872,54 @@ class SlabChain:
         """n sweeps; their records (n x OBS_STRIDE)."""
         self._exchange()
         return np.stack([self.sweep(beta) for _ in range(n)])
+
+    def wolff_flip(self, beta):
+        """One Wolff flip of the whole lattice (the single-GPU chain's flip of
+        the same counter); returns the cluster size (summed over the ranks)."""
+        h, s = self._h, self.stream.cuda_stream
+        f = C.c_void_p(self.field.data_ptr())
+        flip = self.flips
+        self._exchange()
+        check(lib.umc_slab_wolff_local(h, f, beta, flip, s))
+        P = self.P
+        first, last = np.zeros(P, np.uint32), np.zeros(P, np.uint32)
+        up = np.zeros(P, np.uint8)
+        check(lib.umc_slab_wolff_boundary(h, _ptr(first), _ptr(last), _ptr(up), s))
+        nat, root = _u32(0), _u32(0)
+        check(lib.umc_slab_wolff_seed(h, flip, C.byref(nat), C.byref(root), s))
+        mine = (first, last, up, root.value)
+        parts = [mine]
+        if self.world > 1:
+            import torch.distributed as dist
+
+            parts = [None] * self.world
+            dist.all_gather_object(parts, mine, group=self.group)
+        seed_root = next(p[3] for p in parts if p[3] != 0xFFFFFFFF)
+        firsts = np.ascontiguousarray(np.concatenate([p[0] for p in parts]))
+        lasts = np.ascontiguousarray(np.concatenate([p[1] for p in parts]))
+        ups = np.ascontiguousarray(np.concatenate([p[2] for p in parts]))
+        roots = np.zeros(2 * P + 1, np.uint32)
+        n_roots = _u32(0)
+        check(lib.umc_slab_wolff_merge(self.world, P, _ptr(firsts), _ptr(lasts), _ptr(ups), seed_root, self.rank,
+                                       _ptr(first), _ptr(last), root.value, _ptr(roots), C.byref(n_roots)))
+        flipped = _u64(0)
+        check(lib.umc_slab_wolff_flip(h, f, flip, _ptr(roots), n_roots.value, C.byref(flipped), s))
+        size = flipped.value
+        if self.world > 1:
+            import torch.distributed as dist
+
+            t = self.torch.tensor([size], dtype=self.torch.int64)
+            if dist.get_backend(self.group) != "gloo":
+                t = t.to(self.device)
+            dist.all_reduce(t, group=self.group)
+            size = int(t.item())
+        self.flips = flip + 1
+        self._exchange()
+        return size
+
+    def wolff(self, beta, n):
+        """n Wolff flips; their cluster sizes."""
+        return np.array([self.wolff_flip(beta) for _ in range(n)], np.uint64)
 
 
 class GaugeSlabDesc(C.Structure):

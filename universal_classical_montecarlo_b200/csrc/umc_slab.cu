@@ -22,8 +22,11 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <memory>
+#include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "umc_chain.hpp"
@@ -201,6 +204,188 @@ __global__ void __launch_bounds__(kBlock) slab_ising_pass(SlabArgs a)
     finish_pass<kObs>(v, a.out);
 }
 
+// ---------------------------------------------------------- Wolff across slabs
+// One Wolff flip of the whole lattice: each rank decides the forward bonds of
+// its owned sites (x+, y+, and z+ in 3D; the key of bond (site, direction) is
+// the single-GPU one, natural site id * directions + direction rank), unions
+// the ones inside its slab, and reports its boundary: the root of every site
+// of its first and last owned planes and which last-plane sites have an
+// activated bond into the next rank.  Every rank then merges all ranks'
+// boundaries on the host in the same way and flips the local roots whose
+// component holds the seed: the single-GPU flip's cluster.
+struct SlabWolffArgs
+{
+    void* field;
+    uint32_t Lx, Ly, Lz;
+    uint32_t along_z;
+    uint32_t first, planes, P, nloc, n, half;
+    uint64_t seed, flip;
+    float J, beta;
+    double J64, beta64;
+    float err;
+    unsigned long long cw[2];
+    uint32_t* lab;   // per owned site (planes * P): union-find, then the root's global natural id
+    uint8_t* up;     // per last-plane site: bond into the next plane activated
+    DevCtl* ctl;
+};
+
+template <int MODEL>
+__device__ __forceinline__ void slab_axis(const SlabWolffArgs& a, float* r, uint32_t* seed_nat)
+{
+    constexpr int N = MODEL == 0 ? 1 : MODEL;
+    KeyedPcg g = KeyedPcg::open_key(a.seed, a.flip, kTagAxis, 0);
+    if constexpr (MODEL == 0) r[0] = 1.0f;
+    else sphere_sample<MODEL>(g, r);
+    if (seed_nat) {
+        // the seed in colour-major order (as the single-GPU flip draws it), as a natural id
+        const uint32_t ks = uint32_t(u_f64(g.next()) * double(a.n));
+        const uint32_t c = ks >= a.half ? 1u : 0u, rank = ks - c * a.half;
+        uint32_t nat = 2 * rank;
+        const uint32_t x = nat % a.Lx, rr = nat / a.Lx, y = rr % a.Ly, z = rr / a.Ly;
+        if (((x + y + z) & 1u) != c) ++nat;
+        *seed_nat = nat;
+    }
+    (void)N;
+}
+
+template <int MODEL>
+__device__ __forceinline__ void slab_load(const SlabWolffArgs& a, uint32_t q, float* s)
+{
+    if constexpr (MODEL == 0) s[0] = float(static_cast<const int8_t*>(a.field)[q]);
+    else
+#pragma unroll
+        for (int c = 0; c < MODEL; ++c) s[c] = static_cast<const float*>(a.field)[c * a.nloc + q];
+}
+
+__global__ void slab_wolff_init(uint32_t* lab, uint32_t n_owned)
+{
+    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < n_owned; o += gridDim.x * blockDim.x) lab[o] = o;
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(kBlock) slab_wolff_bonds(SlabWolffArgs a)
+{
+    constexpr int N = MODEL == 0 ? 1 : MODEL;
+    __shared__ float r_sh[4];
+    if (threadIdx.x == 0) {
+        float r[N];
+        slab_axis<MODEL>(a, r, nullptr);
+        for (int c = 0; c < N; ++c) r_sh[c] = r[c];
+    }
+    __syncthreads();
+    float r[N];
+#pragma unroll
+    for (int c = 0; c < N; ++c) r[c] = r_sh[c];
+    const uint64_t kb = key_base(key_seed(a.seed, a.flip, kTagBond));
+    const uint32_t n_owned = a.planes * a.P;
+    const uint32_t ndir = 1u + (a.Ly > 1 ? 1u : 0u) + (a.Lz > 1 ? 1u : 0u);
+    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < n_owned; o += gridDim.x * blockDim.x) {
+        const uint32_t lp = o / a.P, pos = o - lp * a.P;  // owned plane (0 = the first), position in it
+        const uint32_t q = o + a.P;                        // local index (plane lp + 1)
+        const uint32_t x = pos % a.Lx;
+        const uint32_t gplane = a.first + lp;
+        const uint32_t nat = gplane * a.P + pos;
+        float si[N];
+        slab_load<MODEL>(a, q, si);
+        // neighbours in direction order x, y (3D only, in-plane), then the cut axis
+        uint32_t nbq[3], nbo[3];
+        bool cross[3];
+        uint32_t nd = 0;
+        {
+            const uint32_t xj = x + 1 == a.Lx ? 0u : x + 1;
+            const uint32_t pj = pos - x + xj;
+            nbq[nd] = lp * a.P + pj + a.P;
+            nbo[nd] = lp * a.P + pj;
+            cross[nd++] = false;
+        }
+        if (a.along_z && a.Ly > 1) {
+            const uint32_t y = pos / a.Lx;
+            const uint32_t yj = y + 1 == a.Ly ? 0u : y + 1;
+            const uint32_t pj = yj * a.Lx + x;
+            nbq[nd] = lp * a.P + pj + a.P;
+            nbo[nd] = lp * a.P + pj;
+            cross[nd++] = false;
+        }
+        if (a.along_z ? a.Lz > 1 : a.Ly > 1) {
+            nbq[nd] = q + a.P;  // the next plane: owned, or the halo after the last one
+            nbo[nd] = o + a.P;
+            cross[nd++] = lp + 1 == a.planes;
+        }
+        for (uint32_t d = 0; d < nd; ++d) {
+            float sj[N];
+            slab_load<MODEL>(a, nbq[d], sj);
+            const uint32_t k = first_draw(kb, nat * ndir + d);
+            bool on;
+            if constexpr (MODEL == 0) on = ising_bond_active(a.cw, int(si[0]), int(sj[0]), k);
+            else on = vector_bond_active<N>(a.J, a.beta, a.J64, a.beta64, a.err, si, sj, r, k);
+            if (cross[d]) a.up[pos] = on ? 1 : 0;
+            else if (on) uf_union(a.lab, o, nbo[d], n_owned + 1, &a.ctl->status);
+        }
+    }
+}
+
+// every owned site's label becomes its root's global natural id
+__global__ void __launch_bounds__(kBlock) slab_wolff_roots(SlabWolffArgs a, uint32_t* glab)
+{
+    const uint32_t n_owned = a.planes * a.P;
+    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < n_owned; o += gridDim.x * blockDim.x) {
+        const uint32_t root = uf_find(a.lab, o, n_owned + 1, &a.ctl->status);
+        glab[o] = (a.first + root / a.P) * a.P + root % a.P;
+    }
+}
+
+template <int MODEL>
+__global__ void slab_wolff_seed(SlabWolffArgs a, uint32_t* seed_nat)
+{
+    float r[MODEL == 0 ? 1 : MODEL];
+    slab_axis<MODEL>(a, r, seed_nat);
+}
+
+// mark[root - first * P] = 1 for the roots to flip
+__global__ void slab_wolff_mark(const uint32_t* roots, uint32_t n_roots, uint32_t base, uint8_t* mark)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_roots; i += gridDim.x * blockDim.x)
+        mark[roots[i] - base] = 1;
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(kBlock) slab_wolff_flip(SlabWolffArgs a, const uint32_t* glab, const uint8_t* mark,
+                                                         unsigned long long* flipped)
+{
+    constexpr int N = MODEL == 0 ? 1 : MODEL;
+    __shared__ float r_sh[4];
+    if (threadIdx.x == 0) {
+        float r[N];
+        slab_axis<MODEL>(a, r, nullptr);
+        for (int c = 0; c < N; ++c) r_sh[c] = r[c];
+    }
+    __syncthreads();
+    float r[N];
+#pragma unroll
+    for (int c = 0; c < N; ++c) r[c] = r_sh[c];
+    const uint32_t n_owned = a.planes * a.P, base = a.first * a.P;
+    double cnt[1] = {0.0};
+    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < n_owned; o += gridDim.x * blockDim.x) {
+        if (!mark[glab[o] - base]) continue;
+        cnt[0] += 1.0;
+        const uint32_t q = o + a.P;
+        if constexpr (MODEL == 0) {
+            int8_t* s = static_cast<int8_t*>(a.field);
+            s[q] = int8_t(-s[q]);
+        } else {
+            float* f = static_cast<float*>(a.field);
+            float si[N];
+#pragma unroll
+            for (int c = 0; c < N; ++c) si[c] = f[c * a.nloc + q];
+            reflect<N>(si, r);
+#pragma unroll
+            for (int c = 0; c < N; ++c) f[c * a.nloc + q] = si[c];
+        }
+    }
+    block_sum<1>(cnt);
+    if (threadIdx.x == 0 && cnt[0] > 0.0) atomicAdd(flipped, (unsigned long long)cnt[0]);
+}
+
 }  // namespace
 }  // namespace umc
 
@@ -213,6 +398,7 @@ struct umc_slab
     int device = 0;
     uint32_t grid = 0;
     DevBuf ctl, partials, record, tm1;
+    DevBuf w_lab, w_glab, w_up, w_mark, w_roots, w_slot;  // Wolff work buffers (first Wolff call)
     std::vector<uint32_t> h_tm1;
     double tm1_beta = std::nan("");
     int32_t J_int = 0;
@@ -241,6 +427,56 @@ void launch_vector(const umc_slab* s, const SlabArgs& a, cudaStream_t st)
 {
     if (s->desc.proposal == UMC_PROPOSAL_ROTATION) slab_vector_pass<N, kPropRotation><<<s->grid, kBlock, 0, st>>>(a);
     else slab_vector_pass<N, kPropSphere><<<s->grid, kBlock, 0, st>>>(a);
+}
+
+SlabWolffArgs wolff_args(umc_slab* s, void* field, double beta, uint64_t flip)
+{
+    const umc_slab_desc& d = s->desc;
+    SlabWolffArgs a{};
+    a.field = field;
+    a.Lx = d.Lx;
+    a.Ly = d.Ly;
+    a.Lz = d.Lz;
+    a.along_z = s->along_z;
+    a.first = d.first_plane;
+    a.planes = d.planes;
+    a.P = s->P;
+    a.nloc = s->nloc;
+    a.n = uint32_t(uint64_t(d.Lx) * d.Ly * d.Lz);
+    a.half = s->half;
+    a.seed = d.seed;
+    a.flip = flip;
+    a.J = float(d.coupling);
+    a.beta = float(beta);
+    a.J64 = d.coupling;
+    a.beta64 = beta;
+    a.err = vector_wolff_err(beta, d.coupling, d.components);
+    if (d.model == UMC_MODEL_ISING) ising_wolff_thresholds(s->J_int, beta, a.cw);
+    const size_t n_owned = size_t(d.planes) * s->P;
+    if (!s->w_lab.p) {
+        s->w_lab.alloc(n_owned * 4, "slab Wolff labels");
+        s->w_glab.alloc(n_owned * 4, "slab Wolff roots");
+        s->w_up.alloc(s->P, "slab Wolff boundary bonds");
+        s->w_mark.alloc(n_owned, "slab Wolff marks");
+        s->w_roots.alloc((2 * size_t(s->P) + 1) * 4, "slab Wolff flip roots");
+        s->w_slot.alloc(16, "slab Wolff slots");
+    }
+    a.lab = s->w_lab.as<uint32_t>();
+    a.up = s->w_up.as<uint8_t>();
+    a.ctl = s->ctl.as<DevCtl>();
+    return a;
+}
+
+template <class F>
+void by_model(const umc_slab* s, F&& f)
+{
+    if (s->desc.model == UMC_MODEL_ISING) return f(std::integral_constant<int, 0>{});
+    switch (s->desc.components) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    default: return f(std::integral_constant<int, 4>{});
+    }
 }
 
 }  // namespace
@@ -369,6 +605,156 @@ int umc_slab_record(umc_slab* s, double* out, void* stream)
         cuda_check(cudaMemcpy(&status, &s->ctl.as<DevCtl>()->status, sizeof status, cudaMemcpyDeviceToHost),
                    "slab status");
         if (status) throw Error(UMC_ERR_DEVICE_TIMEOUT, "slab pass reported a device error");
+    });
+}
+
+int umc_slab_wolff_local(umc_slab* s, void* field, double beta, uint64_t flip, void* stream)
+{
+    return slab_guard([&] {
+        NvtxRange range("umc_slab_wolff_local");
+        if (!s || !field) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (!std::isfinite(beta)) throw Error(UMC_ERR_INVALID_ARGUMENT, "beta must be finite");
+        if (s->desc.model == UMC_MODEL_VECTOR && s->desc.components > 4)
+            throw Error(UMC_ERR_UNSUPPORTED, "VectorSpin<N>: N must be 1..4");
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        SlabWolffArgs a = wolff_args(s, field, beta, flip);
+        const uint32_t n_owned = s->desc.planes * s->P;
+        slab_wolff_init<<<s->grid, kBlock, 0, st>>>(a.lab, n_owned);
+        by_model(s, [&](auto m) { slab_wolff_bonds<decltype(m)::value><<<s->grid, kBlock, 0, st>>>(a); });
+        slab_wolff_roots<<<s->grid, kBlock, 0, st>>>(a, s->w_glab.as<uint32_t>());
+        cuda_check(cudaGetLastError(), "slab Wolff labels");
+    });
+}
+
+int umc_slab_wolff_boundary(umc_slab* s, uint32_t* first_roots, uint32_t* last_roots, uint8_t* last_up,
+                            void* stream)
+{
+    return slab_guard([&] {
+        if (!s || !first_roots || !last_roots || !last_up) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (!s->w_glab.p) throw Error(UMC_ERR_STATE, "umc_slab_wolff_local has not run");
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        const uint32_t* g = s->w_glab.as<uint32_t>();
+        const size_t P = s->P;
+        cuda_check(cudaMemcpyAsync(first_roots, g, P * 4, cudaMemcpyDeviceToHost, st), "slab Wolff boundary");
+        cuda_check(cudaMemcpyAsync(last_roots, g + size_t(s->desc.planes - 1) * P, P * 4, cudaMemcpyDeviceToHost, st),
+                   "slab Wolff boundary");
+        cuda_check(cudaMemcpyAsync(last_up, s->w_up.p, P, cudaMemcpyDeviceToHost, st), "slab Wolff boundary");
+        cuda_check(cudaStreamSynchronize(st), "slab Wolff boundary");
+        unsigned status = 0;
+        cuda_check(cudaMemcpy(&status, &s->ctl.as<DevCtl>()->status, sizeof status, cudaMemcpyDeviceToHost),
+                   "slab status");
+        if (status) throw Error(UMC_ERR_DEVICE_TIMEOUT, "slab Wolff labelling reported a device error");
+    });
+}
+
+int umc_slab_wolff_seed(umc_slab* s, uint64_t flip, uint32_t* seed_nat, uint32_t* seed_root, void* stream)
+{
+    return slab_guard([&] {
+        if (!s || !seed_nat || !seed_root) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        SlabWolffArgs a = wolff_args(s, nullptr, 1.0, flip);
+        uint32_t* slot = s->w_slot.as<uint32_t>();
+        by_model(s, [&](auto m) { slab_wolff_seed<decltype(m)::value><<<1, 1, 0, st>>>(a, slot); });
+        cuda_check(cudaGetLastError(), "slab Wolff seed");
+        cuda_check(cudaMemcpyAsync(seed_nat, slot, 4, cudaMemcpyDeviceToHost, st), "slab Wolff seed");
+        cuda_check(cudaStreamSynchronize(st), "slab Wolff seed");
+        *seed_root = 0xFFFFFFFFu;
+        const uint64_t plane = *seed_nat / s->P;
+        if (plane >= s->desc.first_plane && plane < uint64_t(s->desc.first_plane) + s->desc.planes) {
+            if (!s->w_glab.p) throw Error(UMC_ERR_STATE, "umc_slab_wolff_local has not run");
+            const size_t o = *seed_nat - size_t(s->desc.first_plane) * s->P;
+            cuda_check(cudaMemcpy(seed_root, s->w_glab.as<uint32_t>() + o, 4, cudaMemcpyDeviceToHost), "slab Wolff seed");
+        }
+    });
+}
+
+int umc_slab_wolff_merge(uint32_t world, uint32_t plane_sites, const uint32_t* first_roots, const uint32_t* last_roots,
+                         const uint8_t* last_up, uint32_t seed_root, uint32_t rank, const uint32_t* rank_roots_first,
+                         const uint32_t* rank_roots_last, uint32_t rank_seed_root, uint32_t* roots, uint32_t* n_roots)
+{
+    return slab_guard([&] {
+        if (!first_roots || !last_roots || !last_up || !rank_roots_first || !rank_roots_last || !roots || !n_roots)
+            throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (world == 0 || rank >= world) throw Error(UMC_ERR_INVALID_ARGUMENT, "rank outside the world");
+        const size_t P = plane_sites;
+        // union-find over the boundary labels (global natural ids of local roots)
+        std::unordered_map<uint32_t, uint32_t> parent;
+        auto find = [&](uint32_t x) {
+            auto it = parent.find(x);
+            while (it != parent.end() && it->second != x) {
+                const uint32_t p = it->second;
+                auto pit = parent.find(p);
+                if (pit != parent.end() && pit->second != p) it->second = pit->second;  // path halving
+                x = it->second;
+                it = parent.find(x);
+            }
+            return x;
+        };
+        auto unite = [&](uint32_t a, uint32_t b) {
+            parent.emplace(a, a);
+            parent.emplace(b, b);
+            a = find(a);
+            b = find(b);
+            if (a == b) return;
+            if (a > b) std::swap(a, b);
+            parent[b] = a;  // the smaller id is the root: the same on every rank
+        };
+        for (uint32_t r = 0; r < world; ++r) {
+            const uint32_t nx = (r + 1) % world;
+            for (size_t q = 0; q < P; ++q)
+                if (last_up[r * P + q]) unite(last_roots[r * P + q], first_roots[nx * P + q]);
+        }
+        const uint32_t g = find(seed_root);
+        std::vector<uint32_t> out;
+        auto take = [&](uint32_t L) {
+            if (find(L) == g) out.push_back(L);
+        };
+        for (size_t q = 0; q < P; ++q) {
+            take(rank_roots_first[q]);
+            take(rank_roots_last[q]);
+        }
+        if (rank_seed_root != 0xFFFFFFFFu) take(rank_seed_root);
+        std::sort(out.begin(), out.end());
+        out.erase(std::unique(out.begin(), out.end()), out.end());
+        std::copy(out.begin(), out.end(), roots);
+        *n_roots = uint32_t(out.size());
+    });
+}
+
+int umc_slab_wolff_flip(umc_slab* s, void* field, uint64_t flip, const uint32_t* roots, uint32_t n_roots,
+                        uint64_t* flipped, void* stream)
+{
+    return slab_guard([&] {
+        NvtxRange range("umc_slab_wolff_flip");
+        if (!s || !field || !flipped || (n_roots && !roots)) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (!s->w_glab.p) throw Error(UMC_ERR_STATE, "umc_slab_wolff_local has not run");
+        if (n_roots > 2 * s->P + 1) throw Error(UMC_ERR_INVALID_ARGUMENT, "more roots than the boundary holds");
+        const uint32_t base = s->desc.first_plane * s->P, n_owned = s->desc.planes * s->P;
+        for (uint32_t i = 0; i < n_roots; ++i)
+            if (roots[i] < base || roots[i] - base >= n_owned) throw Error(UMC_ERR_OUT_OF_RANGE, "root outside the slab");
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        SlabWolffArgs a = wolff_args(s, field, 1.0, flip);
+        cuda_check(cudaMemsetAsync(s->w_mark.p, 0, n_owned, st), "slab Wolff marks");
+        unsigned long long* count = reinterpret_cast<unsigned long long*>(s->w_slot.as<uint8_t>() + 8);
+        cuda_check(cudaMemsetAsync(count, 0, 8, st), "slab Wolff count");
+        if (n_roots) {
+            cuda_check(cudaMemcpyAsync(s->w_roots.p, roots, size_t(n_roots) * 4, cudaMemcpyHostToDevice, st),
+                       "slab Wolff roots");
+            slab_wolff_mark<<<1, kBlock, 0, st>>>(s->w_roots.as<uint32_t>(), n_roots, base, s->w_mark.as<uint8_t>());
+            by_model(s, [&](auto m) {
+                slab_wolff_flip<decltype(m)::value><<<s->grid, kBlock, 0, st>>>(a, s->w_glab.as<uint32_t>(),
+                                                                                  s->w_mark.as<uint8_t>(), count);
+            });
+        }
+        cuda_check(cudaGetLastError(), "slab Wolff flip");
+        unsigned long long c = 0;
+        cuda_check(cudaMemcpyAsync(&c, count, 8, cudaMemcpyDeviceToHost, st), "slab Wolff count");
+        cuda_check(cudaStreamSynchronize(st), "slab Wolff count");
+        *flipped = c;
     });
 }
 
