@@ -323,7 +323,7 @@ class ObsStream:
         self.close()
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:  # the library may be gone at interpreter exit
             lib.umc_obs_stream_close(self._h)
             self._h = None
 
@@ -396,7 +396,7 @@ class PairGraph:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:  # the library may be gone at interpreter exit
             lib.umc_graph_destroy(h)
             self._h = None
 
@@ -454,7 +454,7 @@ class CellComplex:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:  # the library may be gone at interpreter exit
             lib.umc_cells_destroy(h)
             self._h = None
 
