@@ -61,7 +61,7 @@ def test_single_rank_defaults(monkeypatch):
     assert _bench().rank_info() == (1, 0, 0)
 
 
-# ------------------------------------------------ sharded batches
+# ----------------------------------- sharded batches (ladders or chains over ranks)
 def test_shard_ranges_partition_the_units():
     import universal_classical_montecarlo_b200 as umc
 
