@@ -178,9 +178,6 @@ __device__ __forceinline__ void run_share(const SegArgs& a, SegShared& sh, const
     // integer divisions (uniform branch)
     const bool pow2 = (H & (H - 1)) == 0 && (per_chain & (per_chain - 1)) == 0;
     const uint32_t hs = __ffs(H) - 1, ps = __ffs(per_chain) - 1;
-    // every warp's items lie in one chain when a chain's share is a multiple
-    // of 32 items and the block a multiple of 32 threads
-    const bool warp_chain = (per_chain & 31u) == 0 && (blockDim.x & 31u) == 0;
     for (uint32_t s = 0; s < a.sweeps; ++s) {
         for (uint32_t ci = threadIdx.x; ci < chain_n; ci += blockDim.x) {
             const uint32_t chain = chains[ci];
@@ -204,21 +201,24 @@ __device__ __forceinline__ void run_share(const SegArgs& a, SegShared& sh, const
             }
         };
         for (uint32_t colour = 0; colour < 2; ++colour) {
+            // accepted updates counted in a register while the thread stays
+            // on one chain (its items change chain every per_chain / blockDim
+            // iterations at most), added to the chain's count on a change
+            uint32_t cur = 0xFFFFFFFFu, cnt = 0;
             for (uint32_t w = threadIdx.x; w < work; w += blockDim.x) {
                 uint32_t ci, y, i;
                 site_of(w, ci, y, i);
                 const bool acc =
                     xy_update<CLUSTER>(a, a.theta + sh.off[ci], colour, y, i, sh.kb[ci], sh.beta[ci], sh.beta64[ci],
                                        row_lo, row_n);
-                if (warp_chain) {
-                    // the whole warp works on chain ci: one shared atomic per warp
-                    const unsigned act = __activemask();
-                    const unsigned bal = __ballot_sync(act, acc);
-                    if ((threadIdx.x & 31u) == uint32_t(__ffs(act) - 1) && bal) atomicAdd(&sh.accepted[ci], __popc(bal));
-                } else if (acc) {
-                    atomicAdd(&sh.accepted[ci], 1u);
+                if (ci != cur) {
+                    if (cnt) atomicAdd(&sh.accepted[cur], cnt);
+                    cur = ci;
+                    cnt = 0;
                 }
+                cnt += acc ? 1u : 0u;
             }
+            if (cnt) atomicAdd(&sh.accepted[cur], cnt);
             if constexpr (CLUSTER) cg::this_cluster().sync();
             else __syncthreads();
         }
