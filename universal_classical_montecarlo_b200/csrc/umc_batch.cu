@@ -204,19 +204,25 @@ __device__ __forceinline__ void run_share(const SegArgs& a, SegShared& sh, const
             // accepted updates counted in a register while the thread stays
             // on one chain (its items change chain every per_chain / blockDim
             // iterations at most), added to the chain's count on a change
+            // (the chain's field, key base and betas likewise stay in registers)
             uint32_t cur = 0xFFFFFFFFu, cnt = 0;
+            float* th = nullptr;
+            uint64_t kb = 0;
+            float beta = 0.f;
+            double beta64 = 0.0;
             for (uint32_t w = threadIdx.x; w < work; w += blockDim.x) {
                 uint32_t ci, y, i;
                 site_of(w, ci, y, i);
-                const bool acc =
-                    xy_update<CLUSTER>(a, a.theta + sh.off[ci], colour, y, i, sh.kb[ci], sh.beta[ci], sh.beta64[ci],
-                                       row_lo, row_n);
                 if (ci != cur) {
                     if (cnt) atomicAdd(&sh.accepted[cur], cnt);
                     cur = ci;
                     cnt = 0;
+                    th = a.theta + sh.off[ci];
+                    kb = sh.kb[ci];
+                    beta = sh.beta[ci];
+                    beta64 = sh.beta64[ci];
                 }
-                cnt += acc ? 1u : 0u;
+                cnt += xy_update<CLUSTER>(a, th, colour, y, i, kb, beta, beta64, row_lo, row_n) ? 1u : 0u;
             }
             if (cnt) atomicAdd(&sh.accepted[cur], cnt);
             if constexpr (CLUSTER) cg::this_cluster().sync();
