@@ -108,15 +108,15 @@ __device__ __noinline__ double xy4_log_ratio64(double J64, double beta64, float 
 // In a cluster, rows [row_lo, row_lo + row_n) of both colours are written by
 // this CTA alone, so they are read through L1; the two halo rows belong to
 // other CTAs of the cluster and are read through L2.
+// other / own: the chain's two colour classes (the one read, the one
+// updated); err: beta * err_per_beta, the FP32 test's bound at this beta.
 template <bool CLUSTER>
-__device__ __forceinline__ bool xy_update(const SegArgs& a, float* th, uint32_t colour, uint32_t y, uint32_t i,
-                                          uint64_t kbase, float beta, double beta64, uint32_t row_lo,
-                                          uint32_t row_n)
+__device__ __forceinline__ bool xy_update(const SegArgs& a, const float* other, float* own, uint32_t colour,
+                                          uint32_t y, uint32_t i, uint64_t kbase, float beta, double beta64,
+                                          float err, uint32_t row_lo, uint32_t row_n)
 {
     const uint32_t L = a.L, H = a.H;
     const uint32_t p = (y + colour) & 1u;
-    const float* other = th + (1u - colour) * a.half;
-    float* own = th + colour * a.half;
     const uint32_t ym = y == 0 ? L - 1 : y - 1, yp = y + 1 == L ? 0u : y + 1;
     const uint32_t i2 = p ? (i + 1 == H ? 0u : i + 1) : (i == 0 ? H - 1 : i - 1);
     const bool l2m = CLUSTER && ym - row_lo >= row_n, l2p = CLUSTER && yp - row_lo >= row_n;
@@ -139,7 +139,7 @@ __device__ __forceinline__ bool xy_update(const SegArgs& a, float* th, uint32_t 
     __sincosf(t, &so, &co);
     __sincosf(prop, &sp, &cp);
     const float dE = -a.J * ((cp - co) * C + (sp - so) * S);
-    const bool ok = metropolis_accept(g, -beta * dE, beta * a.err_per_beta, [&] {
+    const bool ok = metropolis_accept(g, -beta * dE, err, [&] {
         return xy4_log_ratio64(a.J64, beta64, t, prop, nb[0], nb[1], nb[2], nb[3]);
     });
     if (!ok) return false;
@@ -206,9 +206,10 @@ __device__ __forceinline__ void run_share(const SegArgs& a, SegShared& sh, const
             // iterations at most), added to the chain's count on a change
             // (the chain's field, key base and betas likewise stay in registers)
             uint32_t cur = 0xFFFFFFFFu, cnt = 0;
-            float* th = nullptr;
+            const float* other = nullptr;
+            float* own = nullptr;
             uint64_t kb = 0;
-            float beta = 0.f;
+            float beta = 0.f, err = 0.f;
             double beta64 = 0.0;
             for (uint32_t w = threadIdx.x; w < work; w += blockDim.x) {
                 uint32_t ci, y, i;
@@ -217,12 +218,15 @@ __device__ __forceinline__ void run_share(const SegArgs& a, SegShared& sh, const
                     if (cnt) atomicAdd(&sh.accepted[cur], cnt);
                     cur = ci;
                     cnt = 0;
-                    th = a.theta + sh.off[ci];
+                    float* th = a.theta + sh.off[ci];
+                    other = th + (1u - colour) * half;
+                    own = th + colour * half;
                     kb = sh.kb[ci];
                     beta = sh.beta[ci];
                     beta64 = sh.beta64[ci];
+                    err = beta * a.err_per_beta;
                 }
-                cnt += xy_update<CLUSTER>(a, th, colour, y, i, kb, beta, beta64, row_lo, row_n) ? 1u : 0u;
+                cnt += xy_update<CLUSTER>(a, other, own, colour, y, i, kb, beta, beta64, err, row_lo, row_n) ? 1u : 0u;
             }
             if (cnt) atomicAdd(&sh.accepted[cur], cnt);
             if constexpr (CLUSTER) cg::this_cluster().sync();

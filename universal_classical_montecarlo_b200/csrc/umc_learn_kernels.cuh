@@ -656,7 +656,7 @@ __global__ void __launch_bounds__(256) u1_plain_batch(U1BatchArgs a)
         __syncthreads();
         for (uint32_t s = 0; s < a.n_sweeps; ++s) {
             const uint64_t kbase = key_base(key_seed(a.chain_seed[c], a.sweep0 + s, tag_site(0)));
-            double acc = 0.0;
+            uint32_t acc = 0;
             for (uint32_t cls = 0; cls < 4; ++cls) {
                 for (uint32_t q = threadIdx.x; q < g.half; q += blockDim.x) {
                     float Sr, Si;
@@ -675,12 +675,12 @@ __global__ void __launch_bounds__(256) u1_plain_batch(U1BatchArgs a)
                     });
                     if (ok) {
                         th[k] = p;
-                        acc += 1.0;
+                        ++acc;
                     }
                 }
                 __syncthreads();
             }
-            chain_record(a, th, g, c, s, acc);
+            chain_record(a, th, g, c, s, double(acc));
         }
         for (uint32_t i = threadIdx.x; i < nl; i += blockDim.x) gth[i] = th[i];
         __syncthreads();
