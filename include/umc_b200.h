@@ -399,6 +399,11 @@ int umc_slab_create(const umc_slab_desc* desc, umc_slab** out);
 int umc_slab_destroy(umc_slab* s);
 /* (planes + 2) x plane sites: halo, owned planes, halo. */
 uint64_t umc_slab_local_sites(const umc_slab* s);
+/* 1 when each row is stored split by colour instead of in x order: 2D Ising
+ * with Lx / 2 a multiple of 16 (the packed 16-sites-per-thread pass).  Row y
+ * then holds its colour-0 sites, x in increasing order, then its colour-1
+ * sites; the site at x has colour (x + y) & 1 and sits at x / 2 in its half. */
+uint32_t umc_slab_row_split(const umc_slab* s);
 /* Colour pass `colour` (0 then 1 make sweep `sweep`) of the owned sites of
  * `field` (device pointer) on `stream` (cudaStream_t, NULL = default). */
 int umc_slab_pass(umc_slab* s, void* field, double beta, uint64_t sweep, uint32_t colour, void* stream);

@@ -731,6 +731,7 @@ class SlabDesc(C.Structure):
 _decl("umc_slab_create", _int, C.POINTER(SlabDesc), C.POINTER(_vp))
 _decl("umc_slab_destroy", _int, _vp)
 _decl("umc_slab_local_sites", _u64, _vp)
+_decl("umc_slab_row_split", _u32, _vp)
 _decl("umc_slab_pass", _int, _vp, _vp, _f64, _u64, _u32, _vp)
 _decl("umc_slab_record", _int, _vp, _vp, _vp)
 _decl("umc_slab_wolff_local", _int, _vp, _vp, _f64, _u64, _vp)
@@ -776,6 +777,8 @@ class SlabChain:
         check(lib.umc_slab_create(C.byref(d), C.byref(h)))
         self._h = h
         self.nloc = int(lib.umc_slab_local_sites(h))
+        # 2D Ising with Lx / 2 a multiple of 16: each row stored split by colour
+        self.row_split = bool(lib.umc_slab_row_split(h))
         self.device = torch.device("cuda", device)
         dt = torch.int8 if model == MODEL_ISING else torch.float32
         self.field = torch.zeros(self.N * self.nloc, dtype=dt, device=self.device)
@@ -802,14 +805,28 @@ class SlabChain:
         shape (sites,) or (sites, N); every rank passes the same array."""
         a = np.asarray(full).reshape(-1, self.N)
         planes = self._local_planes()
-        loc = np.concatenate([a[p * self.P:(p + 1) * self.P] for p in planes])  # (nloc, N)
+        if self.row_split:  # row y: its (x + y) even sites, then the odd ones
+            loc = np.concatenate([np.concatenate([a[p * self.P + (p & 1)::2][: self.P // 2],
+                                                  a[p * self.P + 1 - (p & 1)::2][: self.P // 2]]) for p in planes])
+        else:
+            loc = np.concatenate([a[p * self.P:(p + 1) * self.P] for p in planes])  # (nloc, N)
         soa = np.ascontiguousarray(loc.T).reshape(-1).astype(np.int8 if self.model == MODEL_ISING else np.float32)
         self.field.copy_(self.torch.from_numpy(soa).to(self.device))
 
     def get_field(self):
         """This rank's planes in natural order: (planes * plane sites, N)."""
         loc = self.field.cpu().numpy().reshape(self.N, self.nloc).T
-        return loc[self.P:(self.planes + 1) * self.P].copy()
+        own = loc[self.P:(self.planes + 1) * self.P].copy()
+        if self.row_split:  # back to x order
+            lo = self.planes_range[0]
+            h = self.P // 2
+            out = np.empty_like(own)
+            for r in range(self.planes):
+                row, par = own[r * self.P:(r + 1) * self.P], (lo + r) & 1
+                out[r * self.P + par:(r + 1) * self.P:2] = row[:h]
+                out[r * self.P + 1 - par:(r + 1) * self.P:2] = row[h:]
+            own = out
+        return own
 
     def gather_field(self):
         """The whole lattice (natural order), on every rank."""

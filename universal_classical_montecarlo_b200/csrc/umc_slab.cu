@@ -180,6 +180,77 @@ __global__ void __launch_bounds__(kBlock, 4) slab_vector_pass(SlabArgs a)
     finish_pass<kObs>(acc, a.out);
 }
 
+// 2D Ising with the rows split by colour (local row r holds the class-0 sites
+// of its row at r * Lx + [0, H), the class-1 sites at r * Lx + H + [0, H), in
+// x order; row y's class-c sites sit at x = 2i + ((y + c) & 1)): the pass of
+// ising_packed_pass (umc_spin_kernels.cuh) -- 16 sites of a row per thread,
+// one 16-byte load of the own class and three of the other class (rows y-1,
+// y, y+1, the outer two possibly halo rows), the 16 consecutive outputs of the
+// stream of the vector's global colour-major index / 16 -- so each site takes
+// the draw, the threshold and the update of the single-GPU pass.  Needs H a
+// multiple of 16.
+__global__ void __launch_bounds__(kBlock) slab_ising_row_pass(SlabArgs a)
+{
+    __shared__ uint32_t tm1[5];
+    // the slab's table is indexed by s h + D (D = 4); this pass by (s h + 4) / 2
+    if (threadIdx.x < 5) tm1[threadIdx.x] = a.tm1[2 * threadIdx.x];
+    __syncthreads();
+    int64_t e_acc = 0, m_acc = 0, n_acc = 0;
+    int8_t* sp = static_cast<int8_t*>(a.field);
+    const uint32_t H = a.Lx / 2, vpr = H >> 4;
+    const uint32_t nvec = a.planes * vpr;
+    const uint32_t oc = (1u - a.colour) * H, cc = a.colour * H;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nvec; v += gridDim.x * blockDim.x) {
+        const uint32_t pl = v / vpr, i0 = (v - pl * vpr) << 4;
+        const uint32_t lr = pl + 1, gy = a.first + pl;  // local and global row
+        const uint32_t p = (gy + a.colour) & 1u;
+        int8_t* own = sp + size_t(lr) * a.Lx + cc;
+        const int8_t* mid = sp + size_t(lr) * a.Lx + oc;
+        const uint4 s4 = *reinterpret_cast<const uint4*>(own + i0);
+        const uint4 m4 = *reinterpret_cast<const uint4*>(mid + i0);
+        const uint4 u4 = *reinterpret_cast<const uint4*>(sp + size_t(lr + 1) * a.Lx + oc + i0);
+        const uint4 d4 = *reinterpret_cast<const uint4*>(sp + size_t(lr - 1) * a.Lx + oc + i0);
+        const uint32_t xe = p ? (i0 + 16 == H ? 0u : i0 + 16) : (i0 == 0 ? H - 1 : i0 - 1);
+        const uint32_t extra = uint32_t(uint8_t(mid[xe]));
+        const uint32_t sw[4] = {s4.x, s4.y, s4.z, s4.w};
+        const uint32_t mw[4] = {m4.x, m4.y, m4.z, m4.w};
+        const uint32_t uw[4] = {u4.x, u4.y, u4.z, u4.w};
+        const uint32_t dw[4] = {d4.x, d4.y, d4.z, d4.w};
+        uint32_t out[4];
+        KeyedPcg rng = KeyedPcg::open(a.kbase, (a.colour * a.half + gy * H + i0) / kGroupSites);
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            // second horizontal neighbour: byte k-1 (p == 0) or k+1 (p == 1)
+            const uint32_t h2 = p ? __byte_perm(mw[w], w == 3 ? extra : mw[w + 1], 0x4321)
+                                  : __byte_perm(w == 0 ? (extra << 24) : mw[w - 1], mw[w], 0x6543);
+            const uint32_t nd = down_bits(uw[w]) + down_bits(dw[w]) + down_bits(mw[w]) + down_bits(h2);
+            const uint32_t di = down_bits(sw[w]);
+            const uint32_t mask = di * 0xFFu;
+            const uint32_t t = (nd & mask) | ((0x04040404u - nd) & ~mask);
+            uint32_t fm = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const uint32_t tb = (t >> (8 * b)) & 0xFFu;
+                const uint32_t r = rng.next();
+                fm |= (r <= tm1[tb] ? 0xFEu : 0u) << (8 * b);
+            }
+            const uint32_t ns = sw[w] ^ fm;
+            out[w] = ns;
+            const uint32_t dn = down_bits(ns);
+            const int32_t ndown = __popc(dn);
+            m_acc += 4 - 2 * ndown;
+            n_acc += __popc(fm) / 7;
+            const int32_t sh = 16 - 2 * int32_t(byte_sum(nd)) - 8 * ndown + 4 * int32_t(byte_sum(nd & (dn * 0xFFu)));
+            e_acc += sh;
+        }
+        *reinterpret_cast<uint4*>(own + i0) = make_uint4(out[0], out[1], out[2], out[3]);
+    }
+    // every bond joins the two classes: count it once, in the pass of class 1
+    double v[kObs] = {a.colour == 1u ? double(-int64_t(a.Jint) * e_acc) : 0.0, double(m_acc), 0, 0, 0, 0, 0,
+                      double(n_acc)};
+    finish_pass<kObs>(v, a.out);
+}
+
 __global__ void __launch_bounds__(kBlock) slab_ising_pass(SlabArgs a)
 {
     int64_t e_acc = 0, m_acc = 0, n_acc = 0;
@@ -224,6 +295,7 @@ struct SlabWolffArgs
     double J64, beta64;
     float err;
     unsigned long long cw[2];
+    uint32_t row_split;  // 2D Ising rows stored split by colour (slab_ising_row_pass)
     uint32_t* lab;   // per owned site (planes * P): union-find, then the root's global natural id
     uint8_t* up;     // per last-plane site: bond into the next plane activated
     DevCtl* ctl;
@@ -248,10 +320,18 @@ __device__ __forceinline__ void slab_axis(const SlabWolffArgs& a, float* r, uint
     (void)N;
 }
 
+// Natural local index q (local plane * P + position) -> the storage index.
+__device__ __forceinline__ uint32_t slab_store_index(const SlabWolffArgs& a, uint32_t q)
+{
+    if (!a.row_split) return q;
+    const uint32_t lr = q / a.P, x = q - lr * a.P;
+    return lr * a.P + ((x + a.first + lr - 1u) & 1u) * (a.P / 2) + x / 2;
+}
+
 template <int MODEL>
 __device__ __forceinline__ void slab_load(const SlabWolffArgs& a, uint32_t q, float* s)
 {
-    if constexpr (MODEL == 0) s[0] = float(static_cast<const int8_t*>(a.field)[q]);
+    if constexpr (MODEL == 0) s[0] = float(static_cast<const int8_t*>(a.field)[slab_store_index(a, q)]);
     else
 #pragma unroll
         for (int c = 0; c < MODEL; ++c) s[c] = static_cast<const float*>(a.field)[c * a.nloc + q];
@@ -371,7 +451,8 @@ __global__ void __launch_bounds__(kBlock) slab_wolff_flip(SlabWolffArgs a, const
         const uint32_t q = o + a.P;
         if constexpr (MODEL == 0) {
             int8_t* s = static_cast<int8_t*>(a.field);
-            s[q] = int8_t(-s[q]);
+            const uint32_t qi = slab_store_index(a, q);
+            s[qi] = int8_t(-s[qi]);
         } else {
             float* f = static_cast<float*>(a.field);
             float si[N];
@@ -399,6 +480,8 @@ struct umc_slab
     uint32_t grid = 0;
     DevBuf ctl, partials, record, tm1;
     DevBuf w_lab, w_glab, w_up, w_mark, w_roots, w_slot;  // Wolff work buffers (first Wolff call)
+    uint32_t row_split = 0;  // 2D Ising, Lx / 2 a multiple of 16: rows split by colour
+    uint32_t row_grid = 0;
     std::vector<uint32_t> h_tm1;
     double tm1_beta = std::nan("");
     int32_t J_int = 0;
@@ -461,6 +544,7 @@ SlabWolffArgs wolff_args(umc_slab* s, void* field, double beta, uint64_t flip)
         s->w_roots.alloc((2 * size_t(s->P) + 1) * 4, "slab Wolff flip roots");
         s->w_slot.alloc(16, "slab Wolff slots");
     }
+    a.row_split = s->row_split;
     a.lab = s->w_lab.as<uint32_t>();
     a.up = s->w_up.as<uint8_t>();
     a.ctl = s->ctl.as<DevCtl>();
@@ -521,6 +605,9 @@ int umc_slab_create(const umc_slab_desc* d, umc_slab** out)
         cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device), "SM count");
         const uint64_t work = (uint64_t(d->planes) * s->P / 2 + kBlock - 1) / kBlock;
         s->grid = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(work, uint64_t(sms) * 8)));
+        s->row_split = d->model == UMC_MODEL_ISING && !s->along_z && (Lx / 2) % 16 == 0 ? 1u : 0u;
+        const uint64_t row_work = (uint64_t(d->planes) * (Lx / 2) / 16 + kBlock - 1) / kBlock;
+        s->row_grid = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(row_work, s->grid)));
         s->ctl.alloc(sizeof(DevCtl), "slab control");
         cuda_check(cudaMemset(s->ctl.p, 0, sizeof(DevCtl)), "slab control");
         s->partials.alloc(size_t(s->grid) * kObs * sizeof(double), "slab partials");
@@ -536,6 +623,8 @@ int umc_slab_destroy(umc_slab* s)
 }
 
 uint64_t umc_slab_local_sites(const umc_slab* s) { return s ? s->nloc : 0; }
+
+uint32_t umc_slab_row_split(const umc_slab* s) { return s ? s->row_split : 0u; }
 
 int umc_slab_pass(umc_slab* s, void* field, double beta, uint64_t sweep, uint32_t colour, void* stream)
 {
@@ -579,7 +668,8 @@ int umc_slab_pass(umc_slab* s, void* field, double beta, uint64_t sweep, uint32_
             a.tm1 = s->tm1.as<uint32_t>();
             a.D = int32_t(s->deg);
             a.Jint = s->J_int;
-            slab_ising_pass<<<s->grid, kBlock, 0, st>>>(a);
+            if (s->row_split) slab_ising_row_pass<<<s->row_grid, kBlock, 0, st>>>(a);
+            else slab_ising_pass<<<s->grid, kBlock, 0, st>>>(a);
         } else {
             a.err = vector_metropolis_err(beta, d.coupling, d.components, s->deg);
             switch (d.components) {
