@@ -374,8 +374,9 @@ void* umc_batch_stream(const umc_batch* b);
  * (Lz = 1 in 2D; Lx, Ly even, Lz 1 or even) is cut along z in 3D, along y in
  * 2D, into planes; a rank holds planes [first_plane, first_plane + planes)
  * plus a halo plane on each side in a caller-owned device array (natural
- * order, x fastest; Ising int8, VectorSpin<N> one float array per component
- * with stride umc_slab_local_sites).  umc_slab_pass runs one checkerboard
+ * order, x fastest, except the rows of 2D Ising slabs that umc_slab_row_split
+ * reports split by colour; Ising int8, VectorSpin<N> one float array per
+ * component with stride umc_slab_local_sites).  umc_slab_pass runs one checkerboard
  * colour over the owned planes; the caller refreshes both halos from the
  * neighbouring ranks after each pass (the planes at local index 1 and
  * `planes` are the ones they need).  Sites draw from the keys of their global
