@@ -421,6 +421,19 @@ __global__ void slab_wolff_seed(SlabWolffArgs a, uint32_t* seed_nat)
     slab_axis<MODEL>(a, r, seed_nat);
 }
 
+// slot[0] = the seed's natural id, slot[1] = its root where this slab owns
+// it (else 0xFFFFFFFF): read back with the boundary, in the same copy batch.
+template <int MODEL>
+__global__ void slab_wolff_seed_root(SlabWolffArgs a, const uint32_t* glab, uint32_t* slot)
+{
+    float r[MODEL == 0 ? 1 : MODEL];
+    uint32_t nat = 0;
+    slab_axis<MODEL>(a, r, &nat);
+    const uint32_t plane = nat / a.P;
+    slot[0] = nat;
+    slot[1] = plane >= a.first && plane - a.first < a.planes ? glab[nat - a.first * a.P] : 0xFFFFFFFFu;
+}
+
 // mark[root - first * P] = 1 for the roots to flip
 __global__ void slab_wolff_mark(const uint32_t* roots, uint32_t n_roots, uint32_t base, uint8_t* mark)
 {
@@ -481,6 +494,9 @@ struct umc_slab
     DevBuf ctl, partials, record, tm1;
     DevBuf w_lab, w_glab, w_up, w_mark, w_roots, w_slot;  // Wolff work buffers (first Wolff call)
     uint32_t row_split = 0;  // 2D Ising, Lx / 2 a multiple of 16: rows split by colour
+    uint32_t seed_host[2] = {0, 0};  // seed site and its root of flip seed_flip, read with the boundary
+    uint64_t seed_flip = 0;
+    bool seed_valid = false;
     uint32_t row_grid = 0;
     std::vector<uint32_t> h_tm1;
     double tm1_beta = std::nan("");
@@ -713,7 +729,12 @@ int umc_slab_wolff_local(umc_slab* s, void* field, double beta, uint64_t flip, v
         slab_wolff_init<<<s->grid, kBlock, 0, st>>>(a.lab, n_owned);
         by_model(s, [&](auto m) { slab_wolff_bonds<decltype(m)::value><<<s->grid, kBlock, 0, st>>>(a); });
         slab_wolff_roots<<<s->grid, kBlock, 0, st>>>(a, s->w_glab.as<uint32_t>());
+        by_model(s, [&](auto m) {
+            slab_wolff_seed_root<decltype(m)::value><<<1, 1, 0, st>>>(a, s->w_glab.as<uint32_t>(), s->w_slot.as<uint32_t>());
+        });
         cuda_check(cudaGetLastError(), "slab Wolff labels");
+        s->seed_flip = flip;
+        s->seed_valid = false;
     });
 }
 
@@ -731,11 +752,15 @@ int umc_slab_wolff_boundary(umc_slab* s, uint32_t* first_roots, uint32_t* last_r
         cuda_check(cudaMemcpyAsync(last_roots, g + size_t(s->desc.planes - 1) * P, P * 4, cudaMemcpyDeviceToHost, st),
                    "slab Wolff boundary");
         cuda_check(cudaMemcpyAsync(last_up, s->w_up.p, P, cudaMemcpyDeviceToHost, st), "slab Wolff boundary");
-        cuda_check(cudaStreamSynchronize(st), "slab Wolff boundary");
+        // the seed and its root (umc_slab_wolff_local computed them) and the
+        // status word ride in the same batch of copies: one synchronisation
         unsigned status = 0;
-        cuda_check(cudaMemcpy(&status, &s->ctl.as<DevCtl>()->status, sizeof status, cudaMemcpyDeviceToHost),
+        cuda_check(cudaMemcpyAsync(s->seed_host, s->w_slot.p, 8, cudaMemcpyDeviceToHost, st), "slab Wolff seed");
+        cuda_check(cudaMemcpyAsync(&status, &s->ctl.as<DevCtl>()->status, sizeof status, cudaMemcpyDeviceToHost, st),
                    "slab status");
+        cuda_check(cudaStreamSynchronize(st), "slab Wolff boundary");
         if (status) throw Error(UMC_ERR_DEVICE_TIMEOUT, "slab Wolff labelling reported a device error");
+        s->seed_valid = true;
     });
 }
 
@@ -743,6 +768,11 @@ int umc_slab_wolff_seed(umc_slab* s, uint64_t flip, uint32_t* seed_nat, uint32_t
 {
     return slab_guard([&] {
         if (!s || !seed_nat || !seed_root) throw Error(UMC_ERR_INVALID_ARGUMENT, "null argument");
+        if (s->seed_valid && s->seed_flip == flip) {  // read back with the boundary
+            *seed_nat = s->seed_host[0];
+            *seed_root = s->seed_host[1];
+            return;
+        }
         cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         SlabWolffArgs a = wolff_args(s, nullptr, 1.0, flip);
