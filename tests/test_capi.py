@@ -284,3 +284,33 @@ def test_gauge_slab_descriptions_are_checked(umc):
     assert create(model=umc.MODEL_ISING) == umc.ERR_UNSUPPORTED
     with pytest.raises(ValueError):
         umc.slowest_axis_owner(umc.CellComplex(5, [[0, 1, 2, 3]]), 2)
+
+
+def test_slab_wolff_boundary_merge(umc):
+    """The host merge of the slab Wolff flip (umc_slab_wolff_merge, no GPU):
+    every rank joins the boundary labels along the activated bonds from each
+    rank's last plane into the next rank's first plane (periodic), finds the
+    seed's component, and keeps its own labels in it."""
+    P, world = 4, 2
+    first = np.array([[100, 101, 102, 103], [200, 201, 202, 203]], np.uint32)
+    last = np.array([[110, 110, 112, 113], [210, 211, 212, 213]], np.uint32)
+    up = np.array([[1, 0, 0, 1], [0, 1, 0, 0]], np.uint8)  # 110-200, 113-203, 211-101
+
+    def merge(seed_root, rank, rank_seed_root=0xFFFFFFFF):
+        out = np.zeros(2 * P + 1, np.uint32)
+        n = umc._u32(0)
+        rc = umc.lib.umc_slab_wolff_merge(world, P, umc._ptr(first.ravel()), umc._ptr(last.ravel()),
+                                          umc._ptr(up.ravel()), seed_root, rank, umc._ptr(first[rank]),
+                                          umc._ptr(last[rank]), rank_seed_root, umc._ptr(out), ctypes.byref(n))
+        assert rc == umc.OK
+        return out[: n.value].tolist()
+
+    assert merge(200, 0) == [110] and merge(200, 1, 200) == [200]
+    assert merge(203, 0) == [113] and merge(203, 1, 203) == [203]
+    assert merge(101, 0) == [101] and merge(101, 1) == [211]
+    # a seed whose cluster touches no boundary: only its own rank flips it
+    assert merge(999, 0, 999) == [999] and merge(999, 1) == []
+    # labels on both boundaries of one rank (110 is in its last plane twice)
+    assert merge(110, 0, 110) == [110] and merge(110, 1) == [200]
+    bad = umc.lib.umc_slab_wolff_merge(world, P, None, None, None, 0, 0, None, None, 0, None, None)
+    assert bad == umc.ERR_INVALID_ARGUMENT
