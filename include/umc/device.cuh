@@ -129,6 +129,47 @@ private:
     std::size_t n_ = 0;
 };
 
+// Field<T, N> of model.hpp:9-41: the owning buffer of one lattice, N values,
+// allocated once, moved but never copied; here in device memory.
+template <class T, std::size_t N>
+class Field : public Buffer<T>
+{
+public:
+    Field() : Buffer<T>(N) {}
+};
+
+// Model<T, Sites, Dof> of model.hpp:47-61: sites(), data() and the write-back
+// update() of a model whose state is one field of Sites sites with Dof values
+// each, so that a model only writes its energy terms.  The reference's Model
+// owns its Field; a model driven by a kernel must be trivially copyable, so
+// this one points at a Field<T, Sites * Dof> (or any device array of that
+// many T) that the caller owns and passes at construction.
+template <class T, std::size_t Sites, std::size_t Dof>
+class Model
+{
+public:
+    Model() = default;
+    explicit Model(T* field) : field_(field) {}
+    template <std::size_t N>
+        requires(N == Sites * Dof)
+    explicit Model(Field<T, N>& f) : field_(f.data())
+    {
+    }
+
+    UMC_HD std::size_t sites() const noexcept { return Sites; }
+    UMC_HD const T* data() const noexcept { return field_; }
+    UMC_HD T* data() noexcept { return field_; }
+
+    // Writes proposal into loc, leaving every other site untouched.
+    UMC_HD void update(std::size_t loc, const T* proposal)
+    {
+        for (std::size_t c = 0; c < Dof; ++c) field_[loc * Dof + c] = proposal[c];
+    }
+
+private:
+    T* field_ = nullptr;
+};
+
 // ------------------------------------------------------------------ random numbers
 
 // The proposal's rng argument: one counter-keyed reference Pcg32.

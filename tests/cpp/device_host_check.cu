@@ -3,7 +3,7 @@
 // construction, the checkerboard colouring, Classes::from_colours, the Rng
 // against a sequential reference Pcg32 seeded the keyed way, and
 // PlaquetteLattice's numbering, cells and incidence against the library's
-// plaquette complexes.  Prints "ok".
+// plaquette complexes, and a model written on the Model base.  Prints "ok".
 #include <umc/device.cuh>
 
 #include <algorithm>
@@ -243,8 +243,44 @@ static void check_plaquettes(std::uint32_t L, std::uint32_t dim)
     }
 }
 
+// A model written on the Model base (model.hpp:47-61): a Heisenberg ring of
+// six sites, neighbours i - 1 and i + 1.
+struct Ring : Model<double, 6, 3>
+{
+    using value_type = double;
+    static constexpr std::size_t size = 3;
+    using Model::Model;
+    UMC_HD double energy_diff_at(std::size_t i, const double* p) const
+    {
+        const double* s = data();
+        const std::size_t l = (i + 5) % 6, r = (i + 1) % 6;
+        double d = 0.0;
+        for (int c = 0; c < 3; ++c) d -= (p[c] - s[3 * i + c]) * (s[3 * l + c] + s[3 * r + c]);
+        return d;
+    }
+};
+static_assert(ModelLike<Ring>);
+static_assert(std::is_trivially_copyable_v<Ring>);
+static_assert(std::is_constructible_v<Ring, Field<double, 18>&>);
+static_assert(!std::is_constructible_v<Ring, Field<double, 17>&>);
+
+void check_model_base()
+{
+    std::vector<double> f(18);
+    for (std::size_t k = 0; k < f.size(); ++k) f[k] = double(k);
+    Ring m(f.data());
+    CHECK(m.sites() == 6 && m.data() == f.data());
+    const double p[3] = {-1.0, -2.0, -3.0};
+    // site 2 holds (6, 7, 8), its neighbours 1 and 3 hold (3, 4, 5) and (9, 10, 11)
+    const double want = -((-1.0 - 6.0) * (3.0 + 9.0) + (-2.0 - 7.0) * (4.0 + 10.0) + (-3.0 - 8.0) * (5.0 + 11.0));
+    CHECK(m.energy_diff_at(2, p) == want);
+    m.update(2, p);
+    for (std::size_t k = 0; k < f.size(); ++k) CHECK(f[k] == (k / 3 == 2 ? p[k % 3] : double(k)));
+}
+
 int main()
 {
+    check_model_base();
     check_fast_div();
     const std::uint32_t dims[][3] = {{2, 2, 1}, {4, 2, 1}, {8, 8, 1}, {6, 4, 2}, {10, 6, 4}, {2, 1, 1},
                                      {8, 1, 1}, {4, 1, 6}, {12, 4, 10}, {16, 6, 1}, {2, 2, 2}};
