@@ -351,7 +351,24 @@ struct CubicHeisenberg
     }
 };
 
+// The same O(3) model written on the Model base (model.hpp:47-61), whose size
+// is fixed at compile time: 8 x 8 x 8 sites.  The base holds the field and
+// its write-back; the energy terms are CubicHeisenberg's on that field.
+struct Heisenberg8 : Model<double, 512, 3>
+{
+    using value_type = double;
+    static constexpr std::size_t size = 3;
+    double J = 1.0;
+
+    Heisenberg8(Field<double, 1536>& f, double J_) : Model(f), J(J_) {}
+    // CubicHeisenberg only reads through its pointer in these two members
+    UMC_HD CubicHeisenberg terms() const { return {const_cast<double*>(data()), 8, 8, 8, J}; }
+    UMC_HD double energy_diff_at(std::size_t i, const double* p) const { return terms().energy_diff_at(i, p); }
+    UMC_HD double energy_at(std::size_t i) const { return terms().energy_at(i); }
+};
+
 static_assert(ModelLike<CubicHeisenberg> && EnergyModel<CubicHeisenberg>);
+static_assert(ModelLike<Heisenberg8> && EnergyModel<Heisenberg8>);
 static_assert(WolffModel<PairModel<Vec<3>, DotTerm<3>>> && WolffModel<PairModel<Spin, IsingBondTerm>>);
 static_assert(Axis<UpAxis, std::int8_t> && Axis<Sphere3, double>);
 static_assert(WolffModel<LatticePairModel<Vec<3>, DotTerm<3>>> && EnergyModel<LatticePairModel<Vec<3>, DotTerm<3>>>);
@@ -495,6 +512,27 @@ int um_heisenberg_cubic(std::uint32_t Lx, std::uint32_t Ly, std::uint32_t Lz, do
         field.upload(spins);
         CubicHeisenberg model{field.data(), Lx, Ly, Lz, J};
         Metropolis<CubicHeisenberg, Sphere3> mc(model, Sphere3{}, classes, seed, beta);
+        mc.set_sweeps(sweep0);
+        mc.run(n_sweeps);
+        *energy = mc.energy_at_sum();
+        field.download(spins);
+    });
+}
+
+// Heisenberg8 (the Model base) from the same state and keys: the chain of
+// um_heisenberg_cubic(8, 8, 8, ...).
+int um_heisenberg_cubic8_base(double J, double beta, std::uint64_t seed, std::uint64_t sweep0, std::uint32_t n_sweeps,
+                              double* spins, double* energy)
+{
+    return guarded([&] {
+        constexpr std::size_t n = 512;
+        std::vector<std::uint32_t> colour(n);
+        for (std::size_t i = 0; i < n; ++i) colour[i] = std::uint32_t((i % 8 + (i / 8) % 8 + i / 64) & 1u);
+        ClassTable classes(Classes::from_colours(colour, 2));
+        Field<double, 3 * n> field;
+        field.upload(spins);
+        Heisenberg8 model(field, J);
+        Metropolis<Heisenberg8, Sphere3> mc(model, Sphere3{}, classes, seed, beta);
         mc.set_sweeps(sweep0);
         mc.run(n_sweeps);
         *energy = mc.energy_at_sum();
