@@ -155,8 +155,10 @@ protected:
             std::vector<DevT> dev(host_.size());
             check(umc_chain_get_field(owner_, dev.data()));
             for (std::size_t k = 0; k < host_.size(); ++k) host_[k] = static_cast<HS>(dev[k]);
+            downloaded_ = true;
         } else if (copy_) {
             copy_->pull(host_.data());
+            downloaded_ = true;
         }
         host_valid_ = true;
     }
@@ -171,6 +173,8 @@ protected:
     mutable umc_chain* owner_ = nullptr;
     mutable DeviceCopy* copy_ = nullptr;
     mutable bool host_valid_ = true;
+    // set by each read-back from the device (a model may post-process it)
+    mutable bool downloaded_ = false;
 };
 
 }  // namespace umc::gpu::detail

@@ -185,11 +185,15 @@ struct U1Shift
 };
 
 // ---- SU(N) ---------------------------------------------------------------------
-// A complex number in the layout of std::complex<double> (real part, then
-// imaginary part) that device code can use, which std::complex cannot.  It
-// converts to and from std::complex on the host; conj, abs and norm are found
-// by argument-dependent lookup, and the arithmetic is the textbook one
-// ((a + bi)(c + di) = (ac - bd) + (ad + bc)i).
+// The entries of an SU(N) link.  In a g++ translation unit, which has no
+// device code, they are the reference's own std::complex<double>, so that host
+// code such as std::abs(u.m[k] - v.m[k]) compiles unchanged.  In an nvcc
+// translation unit they are Complex below: the layout of std::complex<double>
+// (real part, then imaginary part) in a type that device code can use, which
+// std::complex cannot.  It converts to and from std::complex on the host;
+// conj, abs and norm are found by argument-dependent lookup, and the
+// arithmetic is the textbook one ((a + bi)(c + di) = (ac - bd) + (ad + bc)i).
+#if defined(__CUDACC__)
 struct Complex
 {
     double re = 0.0, im = 0.0;
@@ -248,6 +252,9 @@ struct Complex
     UMC_FACADE_HD friend constexpr double norm(const Complex& z) noexcept { return z.re * z.re + z.im * z.im; }
     UMC_FACADE_HD friend double abs(const Complex& z) noexcept { return std::hypot(z.re, z.im); }
 };
+#else
+using Complex = std::complex<double>;
+#endif
 static_assert(sizeof(Complex) == sizeof(std::complex<double>) && alignof(Complex) == alignof(std::complex<double>));
 
 // One SU(N) link: an N x N complex matrix, row-major (dof/sun.hpp:14-76), with
@@ -317,6 +324,46 @@ UMC_FACADE_HD double plaquette(const SULink<N>& u0, const SULink<N>& u1, const S
                                const SULink<N>& u3) noexcept
 {
     return (u0 * u1 * u2.dagger() * u3.dagger()).real_trace() / double(N);
+}
+
+// The nearest-by-construction SU(N) matrix to a link that is unitary only to
+// a few ulp of FP32, in FP64 on the host: Gram-Schmidt over the rows (each row
+// minus its projections on the rows before it, then normalised), then the
+// last row multiplied by conj(det) / |det| so that det U = 1.  A link already
+// in SU(N) to FP64 rounding moves by a few ulp.
+template <std::size_t N>
+void su_project(SULink<N>& u)
+{
+    for (std::size_t r = 0; r < N; ++r) {
+        for (std::size_t q = 0; q < r; ++q) {
+            Complex c(0.0);
+            for (std::size_t k = 0; k < N; ++k) c += conj(u.m[q * N + k]) * u.m[r * N + k];
+            for (std::size_t k = 0; k < N; ++k) u.m[r * N + k] -= c * u.m[q * N + k];
+        }
+        double s = 0.0;
+        for (std::size_t k = 0; k < N; ++k) s += norm(u.m[r * N + k]);
+        const double inv = 1.0 / std::sqrt(s);
+        for (std::size_t k = 0; k < N; ++k) u.m[r * N + k] *= inv;
+    }
+    // det by Gaussian elimination with partial pivoting on a copy
+    std::array<Complex, N * N> a = u.m;
+    Complex det(1.0);
+    for (std::size_t c = 0; c < N; ++c) {
+        std::size_t p = c;
+        for (std::size_t r = c + 1; r < N; ++r)
+            if (abs(a[r * N + c]) > abs(a[p * N + c])) p = r;
+        if (p != c) {
+            for (std::size_t k = 0; k < N; ++k) std::swap(a[c * N + k], a[p * N + k]);
+            det = -det;
+        }
+        det *= a[c * N + c];
+        for (std::size_t r = c + 1; r < N; ++r) {
+            const Complex f = a[r * N + c] * conj(a[c * N + c]) / norm(a[c * N + c]);
+            for (std::size_t k = c; k < N; ++k) a[r * N + k] -= f * a[c * N + k];
+        }
+    }
+    const Complex phase = conj(det) / abs(det);
+    for (std::size_t k = 0; k < N; ++k) u.m[(N - 1) * N + k] *= phase;
 }
 
 namespace sun_detail {

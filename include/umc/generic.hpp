@@ -316,7 +316,7 @@ public:
     std::size_t cells() const noexcept { return list_.cells(); }
     const dtype* data() const
     {
-        this->ensure_host();
+        host_view();
         return reinterpret_cast<const dtype*>(this->host_.data());
     }
     const Term& term() const noexcept { return term_; }
@@ -348,7 +348,7 @@ public:
     }
     void update(std::size_t i, const dtype* p)
     {
-        this->ensure_host();
+        host_view();
         const auto* s = reinterpret_cast<const typename DT::HS*>(p);
         for (std::size_t k = 0; k < DT::scalars; ++k) this->host_[i * DT::scalars + k] = s[k];
         this->host_written();
@@ -370,6 +370,21 @@ private:
         std::array<const dtype*, arity> l{};
         for (std::size_t k = 0; k < arity; ++k) l[k] = f + s[k] * size;
         return l;
+    }
+    // The host copy.  The built-in SU(N) term keeps its links in FP32 on the
+    // device; after a read-back the host copy holds their FP64 projections
+    // onto SU(N) (su_project), as SUGauge's does.
+    void host_view() const
+    {
+        this->ensure_host();
+        if constexpr (DT::ok) {
+            if constexpr (DT::model == UMC_MODEL_SU) {
+                if (!this->downloaded_) return;
+                auto* u = reinterpret_cast<dtype*>(this->host_.data());
+                for (std::size_t l = 0; l < list_.sites(); ++l) su_project(u[l]);
+                this->downloaded_ = false;
+            }
+        }
     }
 
     List list_;

@@ -289,12 +289,12 @@ public:
     std::size_t length() const noexcept { return L_; }
     const SULink<N>* data() const
     {
-        ensure_host();
+        host_links();
         return reinterpret_cast<const SULink<N>*>(host_.data());
     }
     void update(std::size_t i, const SULink<N>* p)
     {
-        ensure_host();
+        host_links();
         const double* s = reinterpret_cast<const double*>(p->m.data());
         for (std::size_t k = 0; k < kScalars; ++k) host_[i * kScalars + k] = s[k];
         host_written();
@@ -338,9 +338,26 @@ private:
     // ReTr(U0 U1 U2^dag U3^dag) / N
     static double plaq(const SULink<N>* const l[4]) { return plaquette(*l[0], *l[1], *l[2], *l[3]); }
 
+    // The host copy of the links.  The device holds them in FP32, unitary to
+    // about 1e-7; after a read-back each link is replaced by its projection
+    // onto SU(N) in FP64 (su_project), so that the host sees links as unitary
+    // as the reference's FP64 chain keeps them.
+    void host_links() const
+    {
+        ensure_host();
+        if (!downloaded_) return;
+        auto* u = reinterpret_cast<SULink<N>*>(host_.data());
+        for (std::size_t l = 0; l < cells_.sites(); ++l) su_project(u[l]);
+        downloaded_ = false;
+    }
+
     CellComplex<4> cells_;
     double beta_;
     std::size_t L_ = 0;
 };
+
+// example/sun_gauge.hpp:85-86
+using SU2Gauge = SUGauge<2>;
+using SU3Gauge = SUGauge<3>;
 
 }  // namespace umc::gpu

@@ -52,6 +52,8 @@ using umc::gpu::Proposal;
 using umc::gpu::square_lattice;
 using umc::gpu::square_plaquettes;
 using umc::gpu::SUDof;
+using umc::gpu::SU2Gauge;
+using umc::gpu::SU3Gauge;
 using umc::gpu::SUGauge;
 using umc::gpu::SULink;
 using umc::gpu::SUPlaquetteTerm;

@@ -5,8 +5,10 @@
 // character expansion).  Prints "ok" and exits 0 on success.
 #include <umc/umc.hpp>
 
+#include <algorithm>
 #include <array>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <string>
 #include <cstdlib>
@@ -131,10 +133,50 @@ void check_weighted_graph()
     CHECK(directed.degree(0) == 1 && directed.degree(1) == 0 && directed.bonds(0)[0].c == 0.25);
 }
 
+// su_project on links rounded to FP32, as the device stores them: the result
+// is unitary with det 1 to FP64 rounding and within FP32 rounding of the link.
+template <std::size_t N>
+void check_su_project()
+{
+    Pcg32 rng(5 + N, 1);
+    SULink<N> u = SULink<N>::identity();
+    for (int k = 0; k < 200; ++k) {
+        SUShift<N>{0.8}.sample(&u, rng, &u);
+        SULink<N> v = u;
+        for (auto& z : v.m) z = std::complex<double>(double(float(z.real())), double(float(z.imag())));
+        CHECK(v.unitarity_error() > 1e-12);
+        umc::gpu::su_project(v);
+        CHECK(v.unitarity_error() < 1e-14);
+        double d = 0.0;
+        for (std::size_t q = 0; q < N * N; ++q) d = std::max(d, std::abs(v.m[q] - u.m[q]));
+        CHECK(d < 1e-6);
+        // det 1: the product of the pivots of v equals that of u (1) to rounding
+        std::array<std::complex<double>, N * N> a = v.m;
+        std::complex<double> det(1.0);
+        for (std::size_t c = 0; c < N; ++c) {
+            std::size_t p = c;
+            for (std::size_t r = c + 1; r < N; ++r)
+                if (std::abs(a[r * N + c]) > std::abs(a[p * N + c])) p = r;
+            if (p != c) {
+                for (std::size_t q = 0; q < N; ++q) std::swap(a[c * N + q], a[p * N + q]);
+                det = -det;
+            }
+            det *= a[c * N + c];
+            for (std::size_t r = c + 1; r < N; ++r) {
+                const std::complex<double> f = a[r * N + c] / a[c * N + c];
+                for (std::size_t q = c; q < N; ++q) a[r * N + q] -= f * a[c * N + q];
+            }
+        }
+        CHECK(std::abs(det - std::complex<double>(1.0)) < 1e-14);
+    }
+}
+
 int main(int argc, char** argv)
 {
-    // ---- host-side tables (no GPU needed)
+    // ---- host-side tables and link algebra (no GPU needed)
     check_weighted_graph();
+    check_su_project<2>();
+    check_su_project<3>();
     if (argc > 1 && std::string(argv[1]) == "tables") {
         std::puts("facade_check tables: ok");
         return 0;
