@@ -39,6 +39,23 @@ concept Proposal = requires(const Q& q, const T* cur, T* out, R& rng) {
 // ---- Ising ---------------------------------------------------------------
 using IsingSpin = std::int8_t;
 
+// dof/ising.hpp:20-24: the bilinear s_i s_j of two Ising spins.
+UMC_FACADE_HD constexpr std::int32_t dot(IsingSpin a, IsingSpin b) noexcept
+{
+    return std::int32_t(a) * std::int32_t(b);
+}
+
+// dof/vector.hpp:23-31: the dot product of two N-component vectors, summed in
+// component order.
+template <std::size_t N>
+UMC_FACADE_HD constexpr double dot(const double* a, const double* b) noexcept
+{
+    static_assert(N >= 1, "dot needs at least one component");
+    double s = 0.0;
+    for (std::size_t k = 0; k < N; ++k) s += a[k] * b[k];
+    return s;
+}
+
 struct IsingDof
 {
     using dtype = IsingSpin;

@@ -105,7 +105,18 @@ std::unique_ptr<UserRunner> make_user_metropolis(M& model, const Q& proposal, st
 template <class M, class A>
 std::unique_ptr<UserRunner> make_user_wolff(M& model, const A& axis, std::uint64_t key, double beta);
 
+// A model the engine runs itself: the example models and the PairModel /
+// CellModel of the built-in terms describe their chain.
+template <class M>
+concept EngineModel = requires(const M& m) { m.chain_desc(); };
+
 }  // namespace detail
+
+#define UMC_DRIVER_MODEL_CHECK(M)                                                                          \
+    static_assert(detail::EngineModel<M> || detail::UserTermModel<M>,                                     \
+                  "the facade's drivers run the engine's models and PairModel / CellModel with any term; " \
+                  "a model type of your own runs on the device through umc/device.cuh "                   \
+                  "(umc::gpu::device::Metropolis / Wolff, built by nvcc)")
 
 template <class M, class Q, class R>
 class Metropolis
@@ -114,6 +125,7 @@ public:
     Metropolis(M& model, Q proposal, R rng, double beta)
         : model_(model), proposal_(std::move(proposal)), rng_(std::move(rng)), beta_(beta)
     {
+        UMC_DRIVER_MODEL_CHECK(M);
         if constexpr (detail::UserTermModel<M>) {
             user_ = detail::make_user_metropolis(model_, proposal_, detail::key_of(rng_), beta_);
         } else {
@@ -190,6 +202,7 @@ public:
     Wolff(M& model, A axis, R rng, double beta) : model_(model), axis_(std::move(axis)), rng_(std::move(rng)), beta_(beta)
     {
         static_assert(WolffModel<M>, "Wolff needs a pair model (degree, bonds, energy_diff_bond)");
+        UMC_DRIVER_MODEL_CHECK(M);
         if constexpr (detail::UserTermModel<M>) {
             user_ = detail::make_user_wolff(model_, axis_, detail::key_of(rng_), beta_);
         } else {
@@ -291,3 +304,5 @@ private:
 };
 
 }  // namespace umc::gpu
+
+#undef UMC_DRIVER_MODEL_CHECK

@@ -67,6 +67,19 @@ def build(reference_root: str | None = None) -> None:
         subprocess.run(["make", "-s", "-C", HERE, "ref-if-present"], check=True)
 
 
+def reference_root() -> str | None:
+    """The reference tree: $UMC_REFERENCE_ROOT, else oracle/Makefile's REF
+    default; None where no tree is there."""
+    root = os.environ.get("UMC_REFERENCE_ROOT")
+    if not root:
+        with open(os.path.join(HERE, "Makefile")) as f:
+            for line in f:
+                if line.startswith("REF ?="):
+                    root = line.split("=", 1)[1].strip()
+                    break
+    return root if root and os.path.isfile(os.path.join(root, "driver.hpp")) else None
+
+
 def _ptr(a):
     return None if a is None else a.ctypes.data_as(_vp)
 
