@@ -8,6 +8,7 @@
 // and SUShift only parameterise the device update.
 #pragma once
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <complex>
@@ -16,6 +17,9 @@
 #include <cstdint>
 #include <limits>
 #include <numbers>
+#include <system_error>
+#include <thread>
+#include <vector>
 
 #include "detail.hpp"
 
@@ -381,6 +385,37 @@ void su_project(SULink<N>& u)
     }
     const Complex phase = conj(det) / abs(det);
     for (std::size_t k = 0; k < N; ++k) u.m[(N - 1) * N + k] *= phase;
+}
+
+// su_project of n links, split into contiguous ranges over the host's
+// hardware threads when n is large; every link is projected on its own, so
+// the result does not depend on the split.  A thread that cannot be started
+// leaves its range to the calling thread.
+template <std::size_t N>
+void su_project_all(SULink<N>* u, std::size_t n)
+{
+    constexpr std::size_t kMinPerThread = 16384;
+    const std::size_t hw = std::max<std::size_t>(1, std::thread::hardware_concurrency());
+    const std::size_t parts = std::min<std::size_t>(hw, (n + kMinPerThread - 1) / kMinPerThread);
+    const auto range = [u, n, parts](std::size_t p) {
+        for (std::size_t i = n * p / parts; i < n * (p + 1) / parts; ++i) su_project(u[i]);
+    };
+    if (parts <= 1) {
+        for (std::size_t i = 0; i < n; ++i) su_project(u[i]);
+        return;
+    }
+    std::vector<std::thread> threads;
+    std::vector<std::size_t> left;
+    for (std::size_t p = 1; p < parts; ++p) {
+        try {
+            threads.emplace_back(range, p);
+        } catch (const std::system_error&) {
+            left.push_back(p);
+        }
+    }
+    range(0);
+    for (std::size_t p : left) range(p);
+    for (auto& t : threads) t.join();
 }
 
 namespace sun_detail {

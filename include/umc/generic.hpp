@@ -373,15 +373,14 @@ private:
     }
     // The host copy.  The built-in SU(N) term keeps its links in FP32 on the
     // device; after a read-back the host copy holds their FP64 projections
-    // onto SU(N) (su_project), as SUGauge's does.
+    // onto SU(N) (su_project_all), as SUGauge's does.
     void host_view() const
     {
         this->ensure_host();
         if constexpr (DT::ok) {
             if constexpr (DT::model == UMC_MODEL_SU) {
                 if (!this->downloaded_) return;
-                auto* u = reinterpret_cast<dtype*>(this->host_.data());
-                for (std::size_t l = 0; l < list_.sites(); ++l) su_project(u[l]);
+                su_project_all(reinterpret_cast<dtype*>(this->host_.data()), list_.sites());
                 this->downloaded_ = false;
             }
         }

@@ -340,14 +340,13 @@ private:
 
     // The host copy of the links.  The device holds them in FP32, unitary to
     // about 1e-7; after a read-back each link is replaced by its projection
-    // onto SU(N) in FP64 (su_project), so that the host sees links as unitary
+    // onto SU(N) in FP64 (su_project_all), so that the host sees links as unitary
     // as the reference's FP64 chain keeps them.
     void host_links() const
     {
         ensure_host();
         if (!downloaded_) return;
-        auto* u = reinterpret_cast<SULink<N>*>(host_.data());
-        for (std::size_t l = 0; l < cells_.sites(); ++l) su_project(u[l]);
+        su_project_all(reinterpret_cast<SULink<N>*>(host_.data()), cells_.sites());
         downloaded_ = false;
     }
 
