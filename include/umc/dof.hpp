@@ -448,6 +448,13 @@ UMC_FACADE_HD double norm_inf(const Mat<N>& a) noexcept
     return n;
 }
 
+// The same norm under its dof/sun.hpp:104-114 name.
+template <std::size_t N>
+UMC_FACADE_HD double norm(const Mat<N>& a) noexcept
+{
+    return norm_inf<N>(a);
+}
+
 // exp(A) as dof/sun.hpp:118-146 computes it: halve A until its norm is at most
 // 1/2, sum the Taylor series until a term's norm drops below 1e-16 (at most 30
 // terms), square back.  The steps are kept so that a chain on the device

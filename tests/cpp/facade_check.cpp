@@ -169,6 +169,16 @@ void check_su_project()
         }
         CHECK(std::abs(det - std::complex<double>(1.0)) < 1e-14);
     }
+    // sun_detail::norm (the reference's name): the largest absolute row sum
+    umc::gpu::sun_detail::Mat<N> m{};
+    for (std::size_t q = 0; q < N * N; ++q) m[q] = std::complex<double>(double(q % N) - 1.0, q == 0 ? 3.0 : 0.0);
+    double want = 0.0;
+    for (std::size_t r = 0; r < N; ++r) {
+        double row = 0.0;
+        for (std::size_t c = 0; c < N; ++c) row += std::abs(m[r * N + c]);
+        want = std::max(want, row);
+    }
+    CHECK(umc::gpu::sun_detail::norm<N>(m) == want);
 }
 
 int main(int argc, char** argv)
