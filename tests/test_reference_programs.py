@@ -56,3 +56,23 @@ def test_reference_host_model_is_refused_with_the_drivers_message(ref_tests, umc
     r = _build(os.path.join(ref_tests, "graph_check.cpp"), str(tmp_path / "graph_check"))
     assert r.returncode != 0
     assert "runs on the device through umc/device.cuh" in r.stderr
+
+
+def test_every_reference_header_has_a_compat_header(ref_tests):
+    """include/umc/compat holds a header at each of the reference's include
+    paths, and each one alone compiles (with the names it declares)."""
+    root = os.path.dirname(ref_tests)
+    compat = os.path.join(INC, "umc", "compat")
+    paths = []
+    for d, _, files in os.walk(root):
+        if os.path.relpath(d, root).split(os.sep)[0] == "test":
+            continue
+        paths += [os.path.relpath(os.path.join(d, f), root) for f in files if f.endswith(".hpp")]
+    assert paths
+    missing = [p for p in paths if not os.path.isfile(os.path.join(compat, p))]
+    assert not missing, missing
+    for p in sorted(paths):
+        r = subprocess.run(["g++", "-std=c++23", "-fsyntax-only", "-Wall", "-Wextra", "-Werror", f"-I{INC}",
+                            f"-I{compat}", "-x", "c++", "-"], input=f"#include <{p}>\n", capture_output=True,
+                           text=True)
+        assert r.returncode == 0, (p, r.stderr)
